@@ -1,0 +1,85 @@
+"""ctypes binding of include/adamantine_b200.h (libadamantine_b200.so).
+
+The library is the only compute path: if it is missing or fails to load, the
+package raises instead of falling back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+from .config import ConfigStruct, SourceStruct
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libadamantine_b200.so")
+
+_VP = ctypes.c_void_p
+_D = ctypes.POINTER(ctypes.c_double)
+_U8 = ctypes.POINTER(ctypes.c_uint8)
+_I64 = ctypes.POINTER(ctypes.c_int64)
+_I32 = ctypes.POINTER(ctypes.c_int32)
+
+# name -> argtypes (every function returns int)
+SIGNATURES = {
+    "adm_create": [ctypes.POINTER(ConfigStruct), ctypes.c_int, _VP, ctypes.POINTER(_VP)],
+    "adm_destroy": [_VP],
+    "adm_set_cells": [_VP, _U8, _U8, _U8, _D, _D],
+    "adm_setup": [_VP],
+    "adm_n_nodes": [_VP, _I64],
+    "adm_n_cells": [_VP, _I64],
+    "adm_node_layout": [_VP, _I64, _I64],
+    "adm_set_time": [_VP, ctypes.c_double],
+    "adm_vmult": [_VP, _VP, _VP],
+    "adm_vmult_add": [_VP, _VP, _VP],
+    "adm_vmult_host": [_VP, _D, _D],
+    "adm_compute_inverse_mass_matrix": [_VP],
+    "adm_get_inverse_mass_matrix": [_VP, _VP],
+    "adm_evolve_one_time_step": [_VP, ctypes.c_double, ctypes.c_double, _VP, _D],
+    "adm_evolve_one_time_step_host": [_VP, ctypes.c_double, ctypes.c_double, _D, _D],
+    "adm_evolve_n_steps": [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_int32, _VP, _D],
+    "adm_evaluate_material_properties": [_VP, _VP, _VP],
+    "adm_set_state_to_material_properties": [_VP],
+    "adm_get_state_from_material_properties": [_VP],
+    "adm_get_cell_state": [_VP, _D],
+    "adm_set_cell_state": [_VP, _D],
+    "adm_get_qp_powder": [_VP, _D],
+    "adm_mark_has_melted": [_VP, ctypes.c_double, _VP, _U8],
+    "adm_activate_cells": [_VP, _I64, ctypes.c_int64, ctypes.c_double, _D, _D, _VP],
+    "adm_update_beam": [_VP, ctypes.c_int32, ctypes.POINTER(SourceStruct)],
+    "adm_device_error": [_VP, _I32],
+    "adm_synchronize": [_VP],
+}
+
+_lib = None
+
+
+class AdmError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"adamantine_b200 error {code}: {msg}")
+        self.code = code
+
+
+def load():
+    """Load the CUDA library (building it first if it is absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        from . import build
+
+        build.build()
+    L = ctypes.CDLL(LIB_PATH)
+    for name, argtypes in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.argtypes = argtypes
+        fn.restype = ctypes.c_int
+    L.adm_last_error.restype = ctypes.c_char_p
+    L.adm_last_error.argtypes = []
+    _lib = L
+    return L
+
+
+def check(rc: int):
+    if rc != 0:
+        msg = load().adm_last_error().decode(errors="replace")
+        raise AdmError(rc, msg)

@@ -1,0 +1,461 @@
+// Small kernels around the tile kernel: stage preparation (heat-source state
+// from the scan path on the device), lumped inverse mass, cell averages and
+// material update, state averaging/broadcast, activation.
+#pragma once
+
+#include "device_types.cuh"
+
+#include <cuda_runtime.h>
+
+namespace adm
+{
+
+// Set the stage clock of members [0, n): t and dt.
+__global__ void set_clock_kernel(MemberData *members, int n, double t, double dt)
+{
+  int const m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m < n)
+  {
+    members[m].clock[0] = t;
+    members[m].clock[1] = dt;
+  }
+}
+
+// clock[0] += clock[1] (end of a captured time step).
+__global__ void advance_clock_kernel(MemberData *members, int n)
+{
+  int const m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m < n)
+    members[m].clock[0] = members[m].clock[0] + members[m].clock[1];
+}
+
+// Heat-source state at t = clock[0] + c * clock[1] for every member and beam:
+// ScanPath::value / get_power_modifier (source/ScanPath.cc:197-275) and
+// GoldakHeatSource / ElectronBeamHeatSource / CubeHeatSource::update_time
+// (source/GoldakHeatSource.cc:24-44, source/ElectronBeamHeatSource.cc:24-45,
+// source/CubeHeatSource.cc:45-49). One block per member, one thread per beam.
+__global__ void stage_prepare_kernel(MemberData *members, int n_members, double c)
+{
+  int const m = blockIdx.x;
+  int const b = threadIdx.x;
+  if (m >= n_members)
+    return;
+  MemberData const &md = members[m];
+  if (b >= md.n_beams)
+    return;
+  double const t = md.clock[0] + c * md.clock[1];
+  BeamDesc const &bd = md.beams[b];
+  BeamState st;
+  st.type = bd.type;
+  st.depth = bd.depth;
+  st.radius_squared = bd.radius_squared;
+  st.five_r2 = 5. * bd.radius_squared;
+  st.inv_r2 = 0.0;
+  st.inv_d2 = 0.0;
+  st.inv_d = 0.0;
+  st.log01 = md.log_01;
+  st.alpha = 0.0;
+  for (int d = 0; d < 3; ++d)
+  {
+    st.cube_min[d] = bd.cube_min[d];
+    st.cube_max[d] = bd.cube_max[d];
+    st.center[d] = 0.0;
+  }
+  st.cube_value = bd.cube_value;
+  if (bd.type == 2)
+  {
+    st.on = (t > bd.cube_start_time) && (t < bd.cube_end_time);
+  }
+  else
+  {
+    int const n = bd.n_segments;
+    double const *sg = bd.segments;
+    double pmod = 0.0;
+    if (n == 0 || t > sg[(n - 1) * 5])
+    {
+      double const low = -1.7976931348623157e308;
+      st.center[0] = st.center[1] = st.center[2] = low;
+    }
+    else
+    {
+      // first segment whose end time is >= t (end times are non-decreasing)
+      int lo = 0, hi = n - 1;
+      while (lo < hi)
+      {
+        int const mid = (lo + hi) / 2;
+        if (t > sg[mid * 5])
+          lo = mid + 1;
+        else
+          hi = mid;
+      }
+      int const cur = lo;
+      double st_t, sp[3];
+      if (cur > 0)
+      {
+        st_t = sg[(cur - 1) * 5];
+        for (int d = 0; d < 3; ++d)
+          sp[d] = sg[(cur - 1) * 5 + 2 + d];
+      }
+      else
+      {
+        st_t = 0.0;
+        for (int d = 0; d < 3; ++d)
+          sp[d] = sg[cur * 5 + 2 + d];
+      }
+      double const et = sg[cur * 5];
+      for (int d = 0; d < 3; ++d)
+        st.center[d] = sp[d] + (sg[cur * 5 + 2 + d] - sp[d]) / (et - st_t) * (t - st_t);
+      pmod = sg[cur * 5 + 1];
+    }
+    st.on = pmod > 0.0;
+    if (bd.type == 0)
+    {
+      st.alpha = 2.0 * bd.absorption_efficiency * bd.max_power * pmod /
+                 (bd.radius_squared * bd.depth * md.pi_over_3_to_1p5);
+      st.inv_r2 = 1.0 / bd.radius_squared;
+      st.inv_d2 = 1.0 / (bd.depth * bd.depth);
+    }
+    else
+    {
+      st.alpha = -bd.absorption_efficiency * bd.max_power * pmod * md.log_01 /
+                 (3.14159265358979323846 * bd.radius_squared * bd.depth);
+      st.inv_d = 1.0 / bd.depth;
+      st.inv_r2 = 1.0 / bd.radius_squared;
+    }
+  }
+  md.beam_state[b] = st;
+}
+
+// Per-direction cells touching node i: (cell index, local node index).
+__device__ __forceinline__ int node_cells(int i, int deg, int nc, int *cell, int *loc)
+{
+  int n = 0;
+  if (deg == 2)
+  {
+    if (i & 1)
+    {
+      cell[n] = (i - 1) / 2;
+      loc[n++] = 1;
+    }
+    else
+    {
+      if (i / 2 - 1 >= 0)
+      {
+        cell[n] = i / 2 - 1;
+        loc[n++] = 2;
+      }
+      if (i / 2 < nc)
+      {
+        cell[n] = i / 2;
+        loc[n++] = 0;
+      }
+    }
+  }
+  else
+  {
+    if (i - 1 >= 0)
+    {
+      cell[n] = i - 1;
+      loc[n++] = 1;
+    }
+    if (i < nc)
+    {
+      cell[n] = i;
+      loc[n++] = 0;
+    }
+  }
+  return n;
+}
+
+struct GridArgs
+{
+  int nc[3], nn[3], pitch, deg;
+  double vol;
+  double glw[3]; // Gauss-Lobatto weights (lumped mass)
+};
+
+// compute_inverse_mass_matrix (source/ThermalOperator.templates.hh:118-164):
+// Gauss-Lobatto lumped mass of the active cells, inverted on DoFs, 0 elsewhere.
+__global__ void inverse_mass_kernel(GridArgs g, uint32_t const *cell_info,
+                                    double *inv_mass, size_t n_total)
+{
+  size_t const idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (idx >= n_total)
+    return;
+  int const i = idx % g.pitch;
+  size_t const r = idx / g.pitch;
+  int const j = r % g.nn[1], k = r / g.nn[1];
+  if (i >= g.nn[0])
+  {
+    inv_mass[idx] = 0.0;
+    return;
+  }
+  int cx[2], ax[2], cy[2], ay[2], cz[2], az[2];
+  int const nx = node_cells(i, g.deg, g.nc[0], cx, ax);
+  int const ny = node_cells(j, g.deg, g.nc[1], cy, ay);
+  int const nz = node_cells(k, g.deg, g.nc[2], cz, az);
+  double m = 0.0;
+  for (int c = 0; c < nz; ++c)
+    for (int b = 0; b < ny; ++b)
+      for (int a = 0; a < nx; ++a)
+      {
+        size_t const cell = cx[a] + (size_t)g.nc[0] * (cy[b] + (size_t)g.nc[1] * cz[c]);
+        if (cell_info[cell] & CI_ACTIVE)
+          m += g.vol * g.glw[ax[a]] * g.glw[ay[b]] * g.glw[az[c]];
+      }
+  inv_mass[idx] = m > 0.0 ? 1.0 / m : 0.0;
+}
+
+// New DoFs of an activation get new_temperature: nodes of the cells in the
+// list that no previously active cell touches (cell_info is the old one).
+__global__ void activate_nodes_kernel(GridArgs g, uint32_t const *cell_info,
+                                      int64_t const *cells, int64_t n_cells,
+                                      double new_temperature, double *y)
+{
+  int64_t const w = blockIdx.x;
+  if (w >= n_cells)
+    return;
+  int const deg = g.deg, np = deg + 1;
+  int64_t const c = cells[w];
+  int const ccx = c % g.nc[0];
+  int const ccy = (c / g.nc[0]) % g.nc[1];
+  int const ccz = c / ((int64_t)g.nc[0] * g.nc[1]);
+  for (int l = threadIdx.x; l < np * np * np; l += blockDim.x)
+  {
+    int const i = deg * ccx + l % np, j = deg * ccy + (l / np) % np,
+              k = deg * ccz + l / (np * np);
+    int cx[2], ax[2], cy[2], ay[2], cz[2], az[2];
+    int const nx = node_cells(i, deg, g.nc[0], cx, ax);
+    int const ny = node_cells(j, deg, g.nc[1], cy, ay);
+    int const nz = node_cells(k, deg, g.nc[2], cz, az);
+    bool old = false;
+    for (int c3 = 0; c3 < nz; ++c3)
+      for (int b = 0; b < ny; ++b)
+        for (int a = 0; a < nx; ++a)
+        {
+          size_t const cell = cx[a] + (size_t)g.nc[0] * (cy[b] + (size_t)g.nc[1] * cz[c3]);
+          if (cell_info[cell] & CI_ACTIVE)
+            old = true;
+        }
+    if (!old)
+      y[i + (size_t)g.pitch * (j + (size_t)g.nn[1] * k)] = new_temperature;
+  }
+}
+
+struct AvgArgs
+{
+  GridArgs g;
+  int nq;        // points per direction
+  double S[3][3]; // basis at the points
+  double w[3];    // weights on [0,1]
+};
+
+// Cell-average temperature: sum_q sum_i phi_i(q) T_i JxW / sum_q sum_i phi_i(q) JxW
+// (compute_average, source/MaterialProperty.templates.hh:33-73).
+__device__ double cell_average(AvgArgs const &a, double const *T, int cx, int cy, int cz)
+{
+  int const deg = a.g.deg, np = deg + 1, nq = a.nq;
+  double volume = 0.0, avg = 0.0;
+  for (int q = 0; q < nq * nq * nq; ++q)
+  {
+    int const qa = q % nq, qb = (q / nq) % nq, qc = q / (nq * nq);
+    double const JxW = a.g.vol * a.w[qa] * a.w[qb] * a.w[qc];
+    for (int l = 0; l < np * np * np; ++l)
+    {
+      int const la = l % np, lb = (l / np) % np, lc = l / (np * np);
+      double const phi = a.S[qa][la] * a.S[qb][lb] * a.S[qc][lc];
+      size_t const node = (deg * cx + la) +
+                          (size_t)a.g.pitch * ((deg * cy + lb) + (size_t)a.g.nn[1] * (deg * cz + lc));
+      volume += phi * JxW;
+      avg += phi * T[node] * JxW;
+    }
+  }
+  return avg / volume;
+}
+
+// MaterialProperty::update (source/MaterialProperty.templates.hh:244-437).
+__global__ void material_update_kernel(AvgArgs a, uint32_t const *cell_info,
+                                       MaterialDesc const *gm, double const *T,
+                                       double *state, double *pv, size_t C)
+{
+  size_t const c = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (c >= C)
+    return;
+  int const cx = c % a.g.nc[0], cy = (c / a.g.nc[0]) % a.g.nc[1],
+            cz = c / ((size_t)a.g.nc[0] * a.g.nc[1]);
+  uint32_t const info = cell_info[c];
+  double const Tavg = (info & CI_ACTIVE) ? cell_average(a, T, cx, cy, cz) : 0.0;
+  int const mat = (info >> CI_MAT_SHIFT) & 15;
+  int const ns = gm->n_states;
+  double const solidus = gm->props[mat][Q_SOLIDUS];
+  double const liquidus = gm->props[mat][Q_LIQUIDUS];
+  double solid_ratio = 1.0, liquid_ratio = 0.0;
+  if (ns > 1)
+  {
+    if (Tavg < solidus)
+      liquid_ratio = 0.0;
+    else if (Tavg > liquidus)
+      liquid_ratio = 1.0;
+    else
+      liquid_ratio = (Tavg - solidus) / (liquidus - solidus);
+    if (ns == 2)
+      solid_ratio = 1.0 - liquid_ratio;
+    else
+    {
+      double const p_old = state[2 * C + c];
+      double const oml = 1.0 - liquid_ratio;
+      double const p = (p_old < oml) ? p_old : oml;
+      solid_ratio = 1.0 - liquid_ratio - p;
+      state[2 * C + c] = p;
+    }
+    state[C + c] = liquid_ratio;
+  }
+  state[c] = solid_ratio;
+  for (int p = 0; p < kNStateProps; ++p)
+  {
+    double v = 0.0;
+    for (int s = 0; s < ns; ++s)
+    {
+      double const ratio = state[s * C + c];
+      if (gm->use_table)
+      {
+        double const(*t)[2] = gm->table[mat][p][s];
+        double val;
+        if (Tavg <= t[0][0])
+          val = t[0][1];
+        else
+        {
+          int i = 0;
+          for (; i < kTableSize; ++i)
+            if (Tavg < t[i][0])
+              break;
+          if (i >= kTableSize - 1)
+            val = t[kTableSize - 1][1];
+          else
+            val = t[i - 1][1] + (Tavg - t[i - 1][0]) * (t[i][1] - t[i - 1][1]) /
+                                    (t[i][0] - t[i - 1][0]);
+        }
+        v += ratio * val;
+      }
+      else
+      {
+        double tp = 1.0;
+        for (int i = 0; i <= gm->p_order; ++i)
+        {
+          v += ratio * gm->poly[mat][p][s][i] * tp;
+          tp *= Tavg;
+        }
+      }
+    }
+    pv[p * C + c] = v;
+  }
+  if (ns > 1 && liquid_ratio > 0.0 && liquid_ratio < 1.0)
+    for (int s = 0; s < ns; ++s)
+      pv[P_SPECIFIC_HEAT * C + c] += state[s * C + c] * gm->props[mat][Q_LATENT] / (liquidus - solidus);
+  double const T_inf = gm->props[mat][Q_RAD_TINF];
+  if (T_inf != 1.7976931348623157e308)
+    pv[P_RAD_COEF * C + c] = pv[P_EMISSIVITY * C + c] * 5.670374419e-8 *
+                             (Tavg + T_inf) * (Tavg * Tavg + T_inf * T_inf);
+}
+
+// ThermalPhysics::mark_has_melted (source/ThermalPhysics.templates.hh:537-593)
+__global__ void has_melted_kernel(AvgArgs a, uint32_t const *cell_info,
+                                  double const *T, double threshold,
+                                  uint8_t *has_melted, size_t C)
+{
+  size_t const c = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (c >= C)
+    return;
+  if (!(cell_info[c] & CI_ACTIVE) || has_melted[c])
+    return;
+  int const cx = c % a.g.nc[0], cy = (c / a.g.nc[0]) % a.g.nc[1],
+            cz = c / ((size_t)a.g.nc[0] * a.g.nc[1]);
+  if (cell_average(a, T, cx, cy, cz) > threshold)
+    has_melted[c] = 1;
+}
+
+// set_state_to_material_properties -> MaterialProperty::set_state
+// (source/MaterialProperty.templates.hh:537-621): arithmetic means over the
+// cell's quadrature points; inactive cells keep their state.
+__global__ void set_state_kernel(uint32_t const *cell_info, int ns, int NN,
+                                 double const *liquid_sum, uint8_t const *pmode,
+                                 double const *pcell, double const *pq,
+                                 double *state, size_t C)
+{
+  size_t const c = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (c >= C)
+    return;
+  if (ns == 1)
+  {
+    state[c] = 1.0;
+    return;
+  }
+  if (!(cell_info[c] & CI_ACTIVE))
+    return;
+  double const l = liquid_sum[c] / NN;
+  state[C + c] = l;
+  if (ns == 2)
+  {
+    state[c] = 1.0 - l;
+    return;
+  }
+  double ps = 0.0;
+  int const mode = pmode[c];
+  if (mode == 2)
+    for (int q = 0; q < NN; ++q)
+      ps += pq[c * NN + q];
+  else if (mode == 1)
+    for (int q = 0; q < NN; ++q)
+      ps += pcell[c];
+  double const p = ps / NN;
+  state[2 * C + c] = p;
+  state[c] = 1.0 - l - p;
+}
+
+// get_state_from_material_properties (source/ThermalOperator.templates.hh:753-884):
+// broadcast the cell state to the quadrature-point (and face) tables.
+__global__ void get_state_kernel(uint32_t const *cell_info, int ns, int NN, int NF,
+                                 double const *state, double *liquid_sum,
+                                 uint8_t *pmode, double *pcell,
+                                 int32_t const *face_slot, double *face_powder,
+                                 size_t C)
+{
+  size_t const c = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (c >= C)
+    return;
+  if (!(cell_info[c] & CI_ACTIVE) || ns == 1)
+    return;
+  double const l = state[C + c];
+  double ls = 0.0;
+  for (int q = 0; q < NN; ++q)
+    ls += l;
+  liquid_sum[c] = ls;
+  if (ns == 3)
+  {
+    double const p = state[2 * C + c];
+    pmode[c] = p == 0.0 ? 0 : 1;
+    pcell[c] = p;
+    if (face_slot)
+    {
+      int const slot = face_slot[c];
+      if (slot >= 0)
+        for (int i = 0; i < 6 * NF; ++i)
+          face_powder[(size_t)slot * 6 * NF + i] = p;
+    }
+  }
+}
+
+// Expand the powder representation to [C][NN] values (diagnostics).
+__global__ void expand_powder_kernel(uint32_t const *cell_info, int NN,
+                                     uint8_t const *pmode, double const *pcell,
+                                     double const *pq, double *out, size_t C)
+{
+  size_t const idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (idx >= C * NN)
+    return;
+  size_t const c = idx / NN;
+  int const mode = pmode[c];
+  out[idx] = mode == 2 ? pq[idx] : (mode == 1 ? pcell[c] : 0.0);
+}
+
+} // namespace adm

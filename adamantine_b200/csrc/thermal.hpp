@@ -1,0 +1,216 @@
+// Host-side C++ layer of the B200 thermal hot path.
+//
+// adm::Thermal keeps the method names and meaning of the reference's
+// ThermalOperatorBase (source/ThermalOperatorBase.hh:14-85) and
+// ThermalPhysicsInterface (source/ThermalPhysicsInterface.hh:28-189) over
+// project-owned data: a structured box mesh with a fixed full-grid node
+// numbering, a per-cell active mask instead of FE_Nothing, device FP64
+// vectors and the material/source tables of adm_config. All numerical work is
+// done by the kernels of tile_kernel.cuh and aux_kernels.cuh; there is no CPU
+// fallback.
+#pragma once
+
+#include "../../include/adamantine_b200.h"
+#include "device_types.cuh"
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace adm
+{
+
+struct Error : std::runtime_error
+{
+  int code;
+  Error(int c, std::string const &m) : std::runtime_error(m), code(c) {}
+};
+
+void check_cuda(cudaError_t e, char const *what, char const *file, int line);
+#define ADM_CK(x) ::adm::check_cuda((x), #x, __FILE__, __LINE__)
+
+template <class T>
+struct DevBuf
+{
+  T *p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(DevBuf const &) = delete;
+  DevBuf &operator=(DevBuf const &) = delete;
+  ~DevBuf() { release(); }
+  void release()
+  {
+    if (p)
+      cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count)
+  {
+    if (count == n && p)
+      return;
+    release();
+    if (count == 0)
+      return;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e != cudaSuccess)
+    {
+      p = nullptr;
+      (void)cudaGetLastError();
+      throw Error(ADM_ERR_ALLOC, "cudaMalloc of " + std::to_string(count * sizeof(T)) +
+                                     " bytes failed: " + cudaGetErrorString(e));
+    }
+    n = count;
+  }
+};
+
+// 1D tables of one quadrature rule for FE_Q(deg) on Gauss-Lobatto nodes.
+struct Rule1D
+{
+  int n = 0;
+  double x[3] = {0, 0, 0}, w[3] = {0, 0, 0};
+  double S[3][3] = {};   // S[q][i] = phi_i(x_q)
+  double D[3][3] = {};   // collocation derivative at the points
+  double G[3][3] = {};   // G[q][i] = phi_i'(x_q)
+};
+
+// Geometry and cell arrays shared by the single-problem and ensemble paths.
+struct Mesh
+{
+  int deg = 1;
+  int nc[3] = {0, 0, 0}, nn[3] = {0, 0, 0}, nt[3] = {0, 0, 0};
+  int pitch = 0;
+  double h[3] = {0, 0, 0}, origin[3] = {0, 0, 0};
+  size_t n_nodes = 0, n_cells = 0, n_tiles = 0;
+  int tx = 8, ty = 8, tz = 4;
+  Rule1D quad, gauss;
+  double glw[3] = {0, 0, 0};
+  void init(adm_config const &cfg);
+  size_t cell_index(int x, int y, int z) const
+  {
+    return x + (size_t)nc[0] * (y + (size_t)nc[1] * z);
+  }
+};
+
+// Host mirror of one member's physics description.
+MaterialDesc make_material(adm_config const &cfg);
+void check_config(adm_config const &cfg);
+
+// Per-cell info bits, tile masks and colour work lists for a set of members
+// sharing one mesh.
+struct CellTopology
+{
+  std::vector<uint32_t> cell_info;
+  std::vector<uint32_t> tile_nbr;
+  std::vector<uint8_t> tile_active;
+  std::vector<int32_t> face_slot;
+  int n_slots = 0;
+  bool all_tiles_active = true;
+};
+CellTopology build_topology(Mesh const &mesh, std::vector<uint8_t> const &active,
+                            std::vector<uint8_t> const &matid, bool need_slots);
+
+class Thermal
+{
+public:
+  Thermal(adm_config const &cfg, int device, cudaStream_t stream);
+  ~Thermal();
+  Thermal(Thermal const &) = delete;
+  Thermal &operator=(Thermal const &) = delete;
+
+  // ---- set-up (ThermalPhysics ctor / setup / reinit)
+  void set_cells(uint8_t const *active, uint8_t const *material_id,
+                 uint8_t const *initial_state, double const *cosv,
+                 double const *sinv);
+  void setup();
+
+  // ---- ThermalOperatorBase
+  size_t m() const { return mesh_.n_nodes; }
+  size_t n_cells() const { return mesh_.n_cells; }
+  Mesh const &mesh() const { return mesh_; }
+  void set_time(double t);
+  void vmult(double *dst, double const *src, bool add);
+  void compute_inverse_mass_matrix();
+  double const *inverse_mass_matrix() const { return inv_mass_.p; }
+  void get_state_from_material_properties();
+  void set_state_to_material_properties();
+
+  // ---- ThermalPhysicsInterface
+  double evolve_one_time_step(double t, double dt, double *solution);
+  double evolve_n_steps(double t, double dt, int n, double *solution);
+  void evaluate_material_properties(double const *temperature, double *pv);
+  void get_cell_state(double *host);
+  void set_cell_state(double const *host);
+  void get_qp_powder(double *host);
+  void mark_has_melted(double threshold, double const *temperature, uint8_t *host);
+  void activate_cells(int64_t const *cells, int64_t n, double new_temperature,
+                      double const *cos_new, double const *sin_new, double *solution);
+  void update_beam(int i, adm_source const &beam);
+  // host-buffer variants through persistent device staging vectors
+  void vmult_host(double *dst_host, double const *src_host);
+  double evolve_one_time_step_host(double t, double dt, double *solution_host);
+  int32_t device_error();
+  cudaStream_t stream() const { return stream_; }
+  void synchronize();
+
+  // stage schedule (Butcher tableau of the configured method)
+  struct Tableau
+  {
+    int s;
+    double a[4][4], b[4], c[4];
+  };
+  static Tableau tableau(int method);
+
+private:
+  void rebuild();
+  void upload_member();
+  KernelArgs base_args() const;
+  void launch_pass(KernelArgs args, double const *src);
+  void launch_step(double *solution);
+  void prepare_stage(double c);
+  void set_clock(double t, double dt);
+
+  adm_config cfg_;
+  std::vector<std::vector<double>> segments_;
+  Mesh mesh_;
+  int ns_ = 1;
+  int poly_p_ = 2;
+  int device_ = 0;
+  cudaStream_t stream_ = nullptr;
+  cudaStream_t graph_stream_ = nullptr; // capture/replay stream of evolve_n_steps
+  cudaEvent_t ev_a_ = nullptr, ev_b_ = nullptr;
+  bool adiabatic_only_ = true;
+  bool has_rotation_ = false;
+  bool setup_done_ = false;
+  double op_time_ = 0.0;
+  Tableau tab_;
+
+  std::vector<uint8_t> active_, matid_, init_state_, has_melted_;
+  std::vector<double> cos_, sin_;
+  CellTopology topo_;
+  std::vector<TileWork> work_;
+  int colour_off_[9] = {0};
+
+  DevBuf<double> za_, zb_, s_, f0_, acc_, inv_mass_;
+  DevBuf<double> stage_in_, stage_out_;
+  DevBuf<double> powder_cell_, powder_q_, liquid_sum_, face_powder_;
+  DevBuf<double> cos_d_, sin_d_, state_d_, clock_, segs_;
+  DevBuf<uint32_t> cell_info_d_, tile_nbr_d_;
+  DevBuf<uint8_t> powder_mode_, has_melted_d_;
+  DevBuf<int32_t> face_slot_d_, error_d_;
+  DevBuf<int64_t> cells_d_;
+  DevBuf<MaterialDesc> mat_d_;
+  DevBuf<BeamState> beam_state_d_;
+  DevBuf<MemberData> member_d_;
+  DevBuf<TileWork> work_d_;
+  MemberData md_{};
+
+  // captured step graph for evolve_n_steps
+  cudaGraphExec_t step_graph_ = nullptr;
+  double *graph_solution_ = nullptr;
+};
+
+} // namespace adm

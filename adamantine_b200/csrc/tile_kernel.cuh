@@ -1,0 +1,1042 @@
+// Fused cell-tile kernel of the B200 thermal hot path.
+//
+// One CTA owns a tile of TX x TY x TZ hex cells (one thread per cell) and
+// its brick of (DEG*TX+1) x (DEG*TY+1) x (DEG*TZ+1) nodes. Per launch the
+// kernel processes the tiles of one colour (tile-index parity in x, y, z), so
+// no two CTAs of a launch share a node and no atomics are needed:
+//  1. the node brick of the stage input is staged in shared memory;
+//  2. each thread gathers its cell's nodal values and does the sum-factorized
+//     interpolation to the Gauss points and the collocation gradients in
+//     registers (FP64, CUDA cores: the 2x2 and 3x3 contractions are far too
+//     small for tensor cores);
+//  3. at every quadrature point it updates the solid/liquid/powder ratios,
+//     evaluates the temperature-dependent density, specific heat (with the
+//     latent-heat term) and conductivity, and the Goldak / electron-beam /
+//     cube source, then integrates back in registers;
+//  4. active-boundary faces add the convective / radiative terms;
+//  5. the CTA sums the per-cell results per node and writes each node: the
+//     first tile (in colour order) that touches a node writes it, later ones
+//     add, and the last one finalizes it -- for a time step this applies the
+//     inverse lumped mass and the explicit Runge-Kutta stage update in place.
+//
+// The arithmetic restates source/ThermalOperator.templates.hh:227-751 and
+// source/MaterialProperty.hh:529-846 of the reference (adamantine v1.1.9).
+#pragma once
+
+#include "device_types.cuh"
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+namespace adm
+{
+
+template <int DEG>
+struct TileShape;
+template <>
+struct TileShape<1>
+{
+  static constexpr int TX = 8, TY = 4, TZ = 4;
+};
+template <>
+struct TileShape<2>
+{
+  static constexpr int TX = 8, TY = 4, TZ = 2;
+};
+
+template <int DEG>
+struct TD
+{
+  static constexpr int N = DEG + 1; // nodes / Gauss points per direction
+  static constexpr int TX = TileShape<DEG>::TX, TY = TileShape<DEG>::TY,
+                       TZ = TileShape<DEG>::TZ;
+  static constexpr int NCELL = TX * TY * TZ;
+  // N threads per cell: thread (slab s, cell c) owns the Gauss points and the
+  // nodes of z-level s of cell c
+  static constexpr int NT = NCELL * N;
+  static constexpr int MINB = 2; // resident CTAs per SM the register budget targets
+  static constexpr int BX = DEG * TX + 1, BY = DEG * TY + 1, BZ = DEG * TZ + 1;
+  // x extent of the TMA box: a multiple of 16 bytes
+  static constexpr int BXP = (BX + 1) / 2 * 2;
+  static constexpr int BRICK = BX * BY * BZ;
+  // one staged brick (TMA box), rounded to 128 bytes
+  static constexpr int BRICKP = (BXP * BY * BZ + 15) / 16 * 16;
+  static constexpr int NN = N * N * N;
+  static constexpr int NQS = N * N; // Gauss points (and nodes) per slab
+  static constexpr int NF = N * N;
+  // nodes each thread writes back
+  static constexpr int WIT = (BRICK + NT - 1) / NT;
+  // dynamic shared memory: two staged bricks, the level exchange / per-cell
+  // result buffer [NN][NCELL], the flux exchange [2][NN][NCELL], per-cell
+  // liquid partial sums [N][NCELL] and powder-change flags [NCELL]
+  static constexpr size_t SMEM =
+      sizeof(double) * (2 * BRICKP + 3 * NN * NCELL + N * NCELL) + sizeof(int) * NCELL;
+};
+
+// ------------------------------------------------------------ TMA + mbarrier
+__device__ __forceinline__ uint32_t smem_addr(void const *p)
+{
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
+{
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init()
+{
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async()
+{
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
+{
+  uint32_t ok;
+  asm volatile("{\n\t.reg .pred p;\n\t"
+               "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+               "selp.u32 %0, 1, 0, p;\n\t}"
+               : "=r"(ok)
+               : "r"(smem_addr(bar)), "r"(parity)
+               : "memory");
+  return ok != 0;
+}
+// 3D tiled TMA load of one node brick (no multicast).
+__device__ __forceinline__ void tma_load_brick(void *dst, CUtensorMap const *map, int x, int y, int z,
+                                               uint64_t *bar)
+{
+  asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+               " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(dst)),
+               "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+               : "memory");
+}
+// Bounded wait on an mbarrier phase: false after ~kSpinLimit polls (the
+// caller then reports DERR_TMA_TIMEOUT instead of hanging).
+constexpr long long kSpinLimit = 1ll << 26;
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity)
+{
+  for (long long i = 0; i < kSpinLimit; ++i)
+    if (mbar_try_wait(bar, parity))
+      return true;
+  return false;
+}
+
+struct SmemPhys
+{
+  double poly[kMaxMaterials][kNStateProps][kMaxStates][kMaxPoly];
+  double props[kMaxMaterials][kNProps];
+  double latent_term[kMaxMaterials]; // L / (T_l - T_s)
+  BeamState beams[kMaxBeams];
+  int prop_deg[kNStateProps];
+  int n_materials, use_table, isotropic, n_beams;
+  int has_rotation, sources_here;
+  int member;
+  int role[27];
+};
+
+// ------------------------------------------------------------ properties
+__device__ __forceinline__ double table_lookup(MaterialDesc const *gm, int mat,
+                                               int prop, int s, double T)
+{
+  // MaterialProperty::compute_property_from_table
+  // (source/MaterialProperty.templates.hh:1158-1212)
+  double const(*t)[2] = gm->table[mat][prop][s];
+  if (T <= t[0][0])
+    return t[0][1];
+  int i = 0;
+  for (; i < kTableSize; ++i)
+    if (T < t[i][0])
+      break;
+  if (i >= kTableSize - 1)
+    return t[kTableSize - 1][1];
+  return t[i - 1][1] + (T - t[i - 1][0]) * (t[i][1] - t[i - 1][1]) /
+                           (t[i][0] - t[i - 1][0]);
+}
+
+// Horner evaluation of sum_i c[i] T^i up to degree deg (uniform branch).
+__device__ __forceinline__ double horner(double const *c, int deg, double T)
+{
+  switch (deg)
+  {
+  case 0:
+    return c[0];
+  case 1:
+    return fma(c[1], T, c[0]);
+  case 2:
+    return fma(fma(c[2], T, c[1]), T, c[0]);
+  case 3:
+    return fma(fma(fma(c[3], T, c[2]), T, c[1]), T, c[0]);
+  default:
+    return fma(fma(fma(fma(c[4], T, c[3]), T, c[2]), T, c[1]), T, c[0]);
+  }
+}
+
+// Horner evaluation with a compile-time degree (higher coefficients are zero).
+template <int P>
+__device__ __forceinline__ double horner_fixed(double const *c, double T)
+{
+  double acc = c[P];
+#pragma unroll
+  for (int i = P - 1; i >= 0; --i)
+    acc = fma(acc, T, c[i]);
+  return acc;
+}
+
+// 1/x by Newton-Raphson iteration on the hardware reciprocal estimate
+// (PTX rcp.approx.ftz.f64). Each step y <- y + y (1 - x y) squares the
+// relative error of the estimate, so two steps bring it to the rounding
+// level of double precision for normal, finite x.
+__device__ __forceinline__ double recip(double x)
+{
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
+}
+
+// MaterialProperty::compute_material_property (source/MaterialProperty.hh:529-800):
+// sum over states of ratio_s * property_s(T). pure >= 0 names the only state
+// with a nonzero ratio (that ratio is exactly 1).
+template <int NS>
+__device__ __forceinline__ double property(SmemPhys const &sp,
+                                           MaterialDesc const *gm, int prop,
+                                           int mat, double const *r, int pure,
+                                           double T)
+{
+  if (sp.use_table)
+  {
+    double v = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s)
+      v += r[s] * table_lookup(gm, mat, prop, s, T);
+    return v;
+  }
+  int const deg = sp.prop_deg[prop];
+  double const *c = &sp.poly[mat][prop][0][0];
+  if (NS == 1 || pure >= 0)
+    return horner(c + (NS == 1 ? 0 : pure) * kMaxPoly, deg, T);
+  double m[kMaxPoly];
+#pragma unroll
+  for (int i = 0; i < kMaxPoly; ++i)
+  {
+    double a = r[0] * c[i];
+#pragma unroll
+    for (int s = 1; s < NS; ++s)
+      a = fma(r[s], c[s * kMaxPoly + i], a);
+    m[i] = a;
+  }
+  return horner(m, deg, T);
+}
+
+// update_state_ratios (source/ThermalOperator.templates.hh:227-317), scalar
+// semantics for every quadrature point. Returns the pure state or -1.
+template <int NS>
+__device__ __forceinline__ int state_ratios(SmemPhys const &sp, int mat,
+                                            double T, double p_old, double *r,
+                                            double &liquid, double &p_new)
+{
+  if (NS == 1)
+  {
+    r[0] = 1.0;
+    liquid = 0.0;
+    return 0;
+  }
+  double const solidus = sp.props[mat][Q_SOLIDUS];
+  double const liquidus = sp.props[mat][Q_LIQUIDUS];
+  double l;
+  if (T < solidus)
+    l = 0.0;
+  else if (T > liquidus)
+    l = 1.0;
+  else
+    l = (T - solidus) / (liquidus - solidus);
+  liquid = l;
+  r[1] = l;
+  if (NS == 2)
+  {
+    r[0] = 1.0 - l;
+    if (l == 0.0)
+      return 0;
+    if (l == 1.0)
+      return 1;
+    return -1;
+  }
+  double const one_minus_l = 1.0 - l;
+  double const p = (p_old < one_minus_l) ? p_old : one_minus_l; // std::min
+  p_new = p;
+  r[2] = p;
+  r[0] = 1.0 - l - p;
+  if (l == 0.0)
+  {
+    if (p == 0.0)
+      return 0;
+    if (p == 1.0)
+      return 2;
+    return -1;
+  }
+  if (l == 1.0)
+    return 1; // p = min(0, p_old) = 0, s = 0
+  return -1;
+}
+
+// get_inv_rho_cp (source/ThermalOperator.templates.hh:415-477), CPU latent
+// heat rule liquid * solid > 0.
+template <int NS>
+__device__ __forceinline__ double inv_rho_cp(SmemPhys const &sp,
+                                             MaterialDesc const *gm, int mat,
+                                             double const *r, int pure,
+                                             double T)
+{
+  double const rho = property<NS>(sp, gm, P_DENSITY, mat, r, pure, T);
+  double cp = property<NS>(sp, gm, P_SPECIFIC_HEAT, mat, r, pure, T);
+  if (NS > 1 && pure < 0)
+    if (r[1] * r[0] > 0.0)
+      cp += sp.latent_term[mat];
+  return 1.0 / (rho * cp);
+}
+
+// Conductivity tensor and 1/(rho c_p) at one Gauss point.
+struct QpCoef
+{
+  double inv, kxx, kxy, kyy, kzz;
+};
+
+// General material evaluation (tables, mixed states, anisotropy, rotation);
+// kept out of line so that the common path stays compact.
+template <int NS>
+__device__ __noinline__ void qp_general(SmemPhys const &sp, MaterialDesc const *gm, int mat, double r0,
+                                        double r1, double r2, int pure, double T, double cs, double sn,
+                                        QpCoef &out)
+{
+  double const rat[3] = {r0, r1, r2};
+  out.inv = inv_rho_cp<NS>(sp, gm, mat, rat, pure, T);
+  double const kx = property<NS>(sp, gm, P_KX, mat, rat, pure, T);
+  double const ky = sp.isotropic ? kx : property<NS>(sp, gm, P_KY, mat, rat, pure, T);
+  double const kz = sp.isotropic ? kx : property<NS>(sp, gm, P_KZ, mat, rat, pure, T);
+  // rotation by the deposition angle (source/ThermalOperator.templates.hh:552-594)
+  out.kxx = kx * cs * cs + ky * sn * sn;
+  out.kxy = (kx - ky) * sn * cs;
+  out.kyy = kx * sn * sn + ky * cs * cs;
+  out.kzz = kz;
+}
+
+// Scalar GoldakHeatSource::value / ElectronBeamHeatSource::value /
+// CubeHeatSource::value (source/GoldakHeatSource.cc:46-89,
+// source/ElectronBeamHeatSource.cc:47-93, source/CubeHeatSource.cc:51-71).
+__device__ __forceinline__ double beam_value(BeamState const &b, double px,
+                                             double py, double pz)
+{
+  if (b.type == 2)
+  {
+    if (!b.on)
+      return 0.0;
+    if (px < b.cube_min[0] || px > b.cube_max[0] || py < b.cube_min[1] ||
+        py > b.cube_max[1] || pz < b.cube_min[2] || pz > b.cube_max[2])
+      return 0.0;
+    return b.cube_value;
+  }
+  double const z = pz - b.center[2];
+  if (z + b.depth < 0.0)
+    return 0.0;
+  double const dx = px - b.center[0], dy = py - b.center[1];
+  double const xpy = dx * dx + dy * dy;
+  if (xpy > b.five_r2)
+    return 0.0;
+  if (b.type == 0)
+    return b.alpha * exp(-3.0 * xpy * b.inv_r2 + -3.0 * (z * z) * b.inv_d2);
+  double const z_rel = z * b.inv_d;
+  double const dist_z = -3.0 * (z_rel * z_rel) - 2.0 * z_rel + 1.0;
+  return b.alpha * exp(b.log01 * xpy * b.inv_r2) * dist_z;
+}
+
+// Sum of all heat sources at a point (out of line: only tiles near a beam
+// call it).
+static __device__ __noinline__ double beam_sum(SmemPhys const &sp, double px, double py, double pz)
+{
+  double qs = 0.0;
+  for (int b = 0; b < sp.n_beams; ++b)
+    qs += beam_value(sp.beams[b], px, py, pz);
+  return qs;
+}
+
+// ------------------------------------------------------------ the kernel
+// Loads the physics constants of a member into shared memory.
+template <int NT>
+__device__ __forceinline__ void load_member_constants(SmemPhys &sp, MemberData const &md, int tid)
+{
+  MaterialDesc const *gm = md.mat;
+  int const nm = gm->n_materials;
+  double const *gp = &gm->poly[0][0][0][0];
+  double *spp = &sp.poly[0][0][0][0];
+  int const npoly = nm * kNStateProps * kMaxStates * kMaxPoly;
+  for (int i = tid; i < npoly; i += NT)
+    spp[i] = gp[i];
+  for (int i = tid; i < nm * kNProps; i += NT)
+    (&sp.props[0][0])[i] = (&gm->props[0][0])[i];
+  if (tid < nm)
+  {
+    double const Tl = gm->props[tid][Q_LIQUIDUS], Ts = gm->props[tid][Q_SOLIDUS];
+    sp.latent_term[tid] = gm->props[tid][Q_LATENT] / (Tl - Ts);
+  }
+  if (tid < kNStateProps)
+    sp.prop_deg[tid] = gm->prop_deg[tid];
+  if (tid < md.n_beams)
+    sp.beams[tid] = md.beam_state[tid];
+  if (tid == 0)
+  {
+    sp.n_materials = nm;
+    sp.use_table = gm->use_table;
+    sp.isotropic = gm->isotropic;
+    sp.n_beams = md.n_beams;
+    sp.has_rotation = md.has_rotation;
+  }
+}
+
+// The persistent tile loop: CTA b processes work items b, b + grid, ... of
+// one colour. The node brick of the next item is fetched by TMA into the
+// other buffer while the current item is computed.
+template <int DEG, int NS, int P>
+__global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
+    tile_kernel(const __grid_constant__ CUtensorMap tmap, KernelArgs const args, int n_items)
+{
+  using T_ = TD<DEG>;
+  constexpr int N = T_::N, NN = T_::NN, NT = T_::NT, NCELL = T_::NCELL, NQS = T_::NQS;
+  constexpr int TX = T_::TX, TY = T_::TY, TZ = T_::TZ;
+  constexpr int BX = T_::BX, BY = T_::BY, BZ = T_::BZ, BXP = T_::BXP;
+  constexpr int WIT = T_::WIT;
+  constexpr unsigned kBoxBytes = sizeof(double) * BXP * BY * BZ;
+  extern __shared__ __align__(128) double smem[];
+  double *const xbuf = smem + 2 * T_::BRICKP;  // [NN][NCELL]: levels, then results
+  double *const pzbuf = xbuf + NN * NCELL;     // [2][NN][NCELL]: flux exchange
+  double *const lsum = pzbuf + 2 * NN * NCELL; // [N][NCELL]
+  int *const changed = reinterpret_cast<int *>(lsum + N * NCELL); // [NCELL]
+  __shared__ SmemPhys sp;
+  __shared__ __align__(8) uint64_t bars[2];
+
+  int const tid = threadIdx.x;
+  int const slab = tid / NCELL, cl = tid % NCELL;
+  int const lx = cl % TX, ly = (cl / TX) % TY, lz = cl / (TX * TY);
+  int const nt0 = args.nt[0], nt1 = args.nt[1];
+  int const pitch = args.pitch, nn1 = args.nn[1];
+
+  auto issue = [&](int buf, int item) {
+    int const tile = args.work[item].tile;
+    int const tix = tile % nt0, tiy = (tile / nt0) % nt1, tiz = tile / (nt0 * nt1);
+    mbar_arrive_expect_tx(&bars[buf], kBoxBytes);
+    tma_load_brick(smem + buf * T_::BRICKP, &tmap, DEG * TX * tix, DEG * TY * tiy, DEG * TZ * tiz,
+                   &bars[buf]);
+  };
+
+  if (tid == 0)
+  {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    fence_mbar_init();
+    sp.member = -1;
+  }
+  __syncthreads();
+  if (tid == 0 && (int)blockIdx.x < n_items)
+    issue(0, blockIdx.x);
+
+  int it = 0;
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x, ++it)
+  {
+    int const buf = it & 1;
+    double const *brick = smem + buf * T_::BRICKP;
+    TileWork const w = args.work[item];
+    MemberData const &md = args.members[w.member];
+    MaterialDesc const *gm = md.mat;
+    int const tile = w.tile;
+    int const tix = tile % nt0, tiy = (tile / nt0) % nt1, tiz = tile / (nt0 * nt1);
+    int const colour = (tix & 1) | ((tiy & 1) << 1) | ((tiz & 1) << 2);
+    int const ncx0 = TX * tix, ncy0 = TY * tiy, ncz0 = TZ * tiz;      // first cell
+    int const nx0 = DEG * ncx0, ny0 = DEG * ncy0, nz0 = DEG * ncz0; // first node
+    double *const y = args.y_override ? args.y_override : md.y;
+
+    // prefetch the next item's brick into the other buffer (its previous
+    // contents were consumed before the barrier that ended the last item)
+    if (tid == 0 && item + (int)gridDim.x < n_items)
+    {
+      fence_proxy_async();
+      issue(buf ^ 1, item + gridDim.x);
+    }
+    if (sp.member != w.member)
+    {
+      load_member_constants<NT>(sp, md, tid);
+      __syncthreads();
+      if (tid == 0)
+        sp.member = w.member;
+    }
+    if (tid < 27)
+    {
+      // first/last toucher role of a node whose per-direction sharing state
+      // is (tid % 3, tid / 3 % 3, tid / 9): 0 not shared, 1 shared with the
+      // lower neighbour tile, 2 with the upper one.
+      uint32_t const nbr = md.tile_nbr[tile];
+      int const s0 = tid % 3, s1 = (tid / 3) % 3, s2 = tid / 9;
+      int cmin = 8, cmax = -1;
+#pragma unroll
+      for (int m = 0; m < 8; ++m)
+      {
+        int const b0 = m & 1, b1 = (m >> 1) & 1, b2 = (m >> 2) & 1;
+        if ((b0 && s0 == 0) || (b1 && s1 == 0) || (b2 && s2 == 0))
+          continue;
+        int const o0 = b0 ? (s0 == 1 ? -1 : 1) : 0;
+        int const o1 = b1 ? (s1 == 1 ? -1 : 1) : 0;
+        int const o2 = b2 ? (s2 == 1 ? -1 : 1) : 0;
+        int const bit = (o0 + 1) + 3 * (o1 + 1) + 9 * (o2 + 1);
+        if (!((nbr >> bit) & 1u))
+          continue;
+        int const c = colour ^ (b0 | (b1 << 1) | (b2 << 2));
+        cmin = c < cmin ? c : cmin;
+        cmax = c > cmax ? c : cmax;
+      }
+      sp.role[tid] = (colour == cmin ? 1 : 0) | (colour == cmax ? 2 : 0);
+    }
+    if (slab == 0)
+      changed[cl] = 0;
+    // wait for this item's brick (bounded; every thread polls); the barrier
+    // also publishes the role table and the cleared flags
+    bool const arrived = mbar_wait(&bars[buf], (unsigned)((it >> 1) & 1));
+    if (__syncthreads_or(!arrived))
+    {
+      if (tid == 0)
+      {
+        atomicCAS(md.error, 0, (int)DERR_TMA_TIMEOUT);
+        // let a prefetch still in flight land before the CTA leaves
+        if (item + (int)gridDim.x < n_items)
+          mbar_wait(&bars[buf ^ 1], (unsigned)(((it + 1) >> 1) & 1));
+      }
+      return;
+    }
+
+    // Tile-level source culling, evaluated by every thread (exact: it skips
+    // only points where every source is zero by its own cutoff rules).
+    bool do_src = false;
+    {
+      double const x0 = args.origin[0] + ncx0 * args.h[0];
+      double const y0 = args.origin[1] + ncy0 * args.h[1];
+      double const z0 = args.origin[2] + ncz0 * args.h[2];
+      double const x1 = x0 + TX * args.h[0], y1 = y0 + TY * args.h[1], z1 = z0 + TZ * args.h[2];
+      for (int b = 0; b < sp.n_beams; ++b)
+      {
+        BeamState const &bs = sp.beams[b];
+        if (!bs.on)
+          continue;
+        if (bs.type == 2)
+        {
+          if (x1 >= bs.cube_min[0] && x0 <= bs.cube_max[0] && y1 >= bs.cube_min[1] &&
+              y0 <= bs.cube_max[1] && z1 >= bs.cube_min[2] && z0 <= bs.cube_max[2])
+            do_src = true;
+          continue;
+        }
+        if ((z1 - bs.center[2]) + bs.depth < 0.0)
+          continue;
+        double const qx = fmin(fmax(bs.center[0], x0), x1);
+        double const qy = fmin(fmax(bs.center[1], y0), y1);
+        double const dx = qx - bs.center[0], dy = qy - bs.center[1];
+        if (dx * dx + dy * dy > bs.five_r2 * (1.0 + 1e-9))
+          continue;
+        do_src = true;
+      }
+    }
+
+    // ---- the cell: thread (slab, cl) handles Gauss-point level qc = slab
+    int const cx = ncx0 + lx, cy = ncy0 + ly, cz = ncz0 + lz;
+    bool const in_domain = cx < args.nc[0] && cy < args.nc[1] && cz < args.nc[2];
+    size_t const c = in_domain ? cx + (size_t)args.nc[0] * (cy + (size_t)args.nc[1] * cz) : 0;
+    uint32_t const info = in_domain ? md.cell_info[c] : 0u;
+    bool const active = (info & CI_ACTIVE) != 0;
+    int const mat = (info >> CI_MAT_SHIFT) & 15;
+    // 1. x/y interpolation of the nodes of z-level `slab` (in registers)
+    double wv[NQS];
+    {
+#pragma unroll
+      for (int j = 0; j < N; ++j)
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+          wv[i + N * j] = brick[(DEG * lx + i) + BXP * ((DEG * ly + j) + BY * (DEG * lz + slab))];
+#pragma unroll
+      for (int j = 0; j < N; ++j)
+      {
+        double t[N];
+#pragma unroll
+        for (int q = 0; q < N; ++q)
+        {
+          double acc = args.S[q][0] * wv[N * j];
+#pragma unroll
+          for (int k = 1; k < N; ++k)
+            acc = fma(args.S[q][k], wv[k + N * j], acc);
+          t[q] = acc;
+        }
+#pragma unroll
+        for (int q = 0; q < N; ++q)
+          wv[q + N * j] = t[q];
+      }
+#pragma unroll
+      for (int i = 0; i < N; ++i)
+      {
+        double t[N];
+#pragma unroll
+        for (int q = 0; q < N; ++q)
+        {
+          double acc = args.S[q][0] * wv[i];
+#pragma unroll
+          for (int k = 1; k < N; ++k)
+            acc = fma(args.S[q][k], wv[i + N * k], acc);
+          t[q] = acc;
+        }
+#pragma unroll
+        for (int q = 0; q < N; ++q)
+          wv[i + N * q] = t[q];
+      }
+    }
+    // 2. exchange the levels: values T and z-gradients gz (G = D S) at this
+    //    thread's Gauss-point level
+#pragma unroll
+    for (int i = 0; i < NQS; ++i)
+      xbuf[(i + NQS * slab) * NCELL + cl] = wv[i];
+    __syncthreads();
+    double Tq[NQS], az[NQS];
+#pragma unroll
+    for (int i = 0; i < NQS; ++i)
+    {
+      double tv = 0.0, gz = 0.0;
+#pragma unroll
+      for (int m = 0; m < N; ++m)
+      {
+        double const wm = (m == slab) ? wv[i] : xbuf[(i + NQS * m) * NCELL + cl];
+        tv = fma(args.S[slab][m], wm, tv);
+        gz = fma(args.G[slab][m], wm, gz);
+      }
+      Tq[i] = tv;
+      az[i] = gz;
+    }
+    // 3. physics at the NQS Gauss points of this level; axy accumulates the
+    //    x/y flux contributions (collocation D^T) and the source, az ends
+    //    up holding the z fluxes
+    double axy[NQS];
+#pragma unroll
+    for (int i = 0; i < NQS; ++i)
+      axy[i] = 0.0;
+    double liquid_acc = 0.0;
+    uint32_t changed_mask = 0;
+    int pmode = 0;
+    double pu = 0.0;
+    if (active)
+    {
+      size_t const pbase = c * NN + (size_t)NQS * slab;
+      if (NS == 3)
+      {
+        pmode = md.powder_mode[c];
+        if (pmode == 1)
+          pu = md.powder_cell[c];
+      }
+      double cs = 1.0, sn = 0.0;
+      if (sp.has_rotation)
+      {
+        cs = md.cosv[c];
+        sn = md.sinv[c];
+      }
+      bool const fast_ok = !sp.use_table && sp.isotropic && !sp.has_rotation;
+      double const Wz = args.qw[slab];
+#pragma unroll
+      for (int i = 0; i < NQS; ++i)
+      {
+        int const qa = i % N, qb = i / N;
+        double const T = Tq[i];
+        double gx = 0.0, gy = 0.0;
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+        {
+          gx = fma(args.D[qa][k], Tq[k + N * qb], gx);
+          gy = fma(args.D[qb][k], Tq[qa + N * k], gy);
+        }
+        double const gz = az[i];
+        double p_old = 0.0;
+        if (NS == 3)
+          p_old = (pmode == 2) ? md.powder_q[pbase + i] : pu;
+        double rat[NS > 1 ? NS : 1];
+        double liquid = 0.0, p_new = p_old;
+        int const pure = state_ratios<NS>(sp, mat, T, p_old, rat, liquid, p_new);
+        if (NS > 1)
+          liquid_acc += liquid;
+        if (NS == 3 && p_new != p_old)
+        {
+          md.powder_q[pbase + i] = p_new;
+          changed_mask |= 1u << i;
+        }
+        QpCoef k;
+        if (fast_ok && pure >= 0)
+        {
+          // one state, polynomial, isotropic: Horner in that state only
+          double const *cc = &sp.poly[mat][0][NS == 1 ? 0 : pure][0];
+          constexpr int PS = kMaxStates * kMaxPoly; // stride between properties
+          double const rho = horner_fixed<P>(cc + P_DENSITY * PS, T);
+          double const cp = horner_fixed<P>(cc + P_SPECIFIC_HEAT * PS, T);
+          k.inv = recip(rho * cp);
+          k.kxx = horner_fixed<P>(cc + P_KX * PS, T);
+          k.kyy = k.kxx;
+          k.kzz = k.kxx;
+          k.kxy = 0.0;
+        }
+        else
+        {
+          qp_general<NS>(sp, gm, mat, rat[0], NS > 1 ? rat[1] : 0.0, NS > 2 ? rat[2] : 0.0, pure, T,
+                         cs, sn, k);
+        }
+        double const W = args.qw[qa] * args.qw[qb] * Wz;
+        double const grx = gx * args.inv_h[0], gry = gy * args.inv_h[1];
+        double const cf = -k.inv * W;
+        double const fx = cf * (k.kxx * grx + k.kxy * gry) * args.vol_over_h[0];
+        double const fy = cf * (k.kxy * grx + k.kyy * gry) * args.vol_over_h[1];
+        az[i] = cf * k.kzz * gz * args.vol_over_h2[2];
+#pragma unroll
+        for (int m = 0; m < N; ++m)
+        {
+          axy[m + N * qb] = fma(args.D[qa][m], fx, axy[m + N * qb]);
+          axy[qa + N * m] = fma(args.D[qb][m], fy, axy[qa + N * m]);
+        }
+        if (do_src)
+        {
+          double const px = (args.origin[0] + cx * args.h[0]) + args.qx[qa] * args.h[0];
+          double const py = (args.origin[1] + cy * args.h[1]) + args.qx[qb] * args.h[1];
+          double const pz = (args.origin[2] + cz * args.h[2]) + args.qx[slab] * args.h[2];
+          axy[i] += beam_sum(sp, px, py, pz) * k.inv * (W * args.vol);
+        }
+      }
+      if (NS == 3 && pmode != 2 && changed_mask)
+        changed[cl] = 1;
+    }
+    // 4. in-slab S^T in x and y of both contributions
+#pragma unroll
+    for (int pass = 0; pass < 2; ++pass)
+    {
+      double *a = pass == 0 ? axy : az;
+#pragma unroll
+      for (int j = 0; j < N; ++j)
+      {
+        double t[N];
+#pragma unroll
+        for (int n = 0; n < N; ++n)
+        {
+          double acc = args.S[0][n] * a[N * j];
+#pragma unroll
+          for (int q = 1; q < N; ++q)
+            acc = fma(args.S[q][n], a[q + N * j], acc);
+          t[n] = acc;
+        }
+#pragma unroll
+        for (int n = 0; n < N; ++n)
+          a[n + N * j] = t[n];
+      }
+#pragma unroll
+      for (int i = 0; i < N; ++i)
+      {
+        double t[N];
+#pragma unroll
+        for (int n = 0; n < N; ++n)
+        {
+          double acc = args.S[0][n] * a[i];
+#pragma unroll
+          for (int q = 1; q < N; ++q)
+            acc = fma(args.S[q][n], a[i + N * q], acc);
+          t[n] = acc;
+        }
+#pragma unroll
+        for (int n = 0; n < N; ++n)
+          a[i + N * n] = t[n];
+      }
+    }
+    if (NS > 1)
+      lsum[slab * NCELL + cl] = liquid_acc;
+    // 5. z-direction: node level `slab` gathers S^T (values, x/y fluxes) and
+    //    G^T (z fluxes) from every Gauss-point level
+#pragma unroll
+    for (int i = 0; i < NQS; ++i)
+    {
+      pzbuf[(i + NQS * slab) * NCELL + cl] = axy[i];
+      pzbuf[(NN + i + NQS * slab) * NCELL + cl] = az[i];
+    }
+    __syncthreads();
+    double res[NQS];
+#pragma unroll
+    for (int i = 0; i < NQS; ++i)
+    {
+      double acc = 0.0;
+#pragma unroll
+      for (int q = 0; q < N; ++q)
+      {
+        double const vp = (q == slab) ? axy[i] : pzbuf[(i + NQS * q) * NCELL + cl];
+        double const vz = (q == slab) ? az[i] : pzbuf[(NN + i + NQS * q) * NCELL + cl];
+        acc = fma(args.S[q][slab], vp, acc);
+        acc = fma(args.G[q][slab], vz, acc);
+      }
+      res[i] = active ? acc : 0.0;
+    }
+
+    // ---- face terms of this node level (face_local_apply,
+    // source/ThermalOperator.templates.hh:619-751); every slab thread of a
+    // cell evaluates the face quadrature and keeps the test functions of its
+    // own node level
+    if (args.faces && active && ((info >> CI_FACE_SHIFT) & 63u))
+    {
+      int const slot = (NS == 3) ? md.face_slot[c] : -1;
+      for (int f = 0; f < 6; ++f)
+      {
+        if (!((info >> (CI_FACE_SHIFT + f)) & 1u))
+          continue;
+        int const d = f / 2, side = f % 2;
+        if (d == 2 && slab != (side ? N - 1 : 0))
+          continue; // a z face only touches one node level
+        int const t0 = d == 0 ? 1 : 0, t1 = d == 2 ? 1 : 2;
+        int const btype =
+            ((info >> (CI_INTERFACE_SHIFT + f)) & 1u) ? args.interface_type : args.boundary_type[f];
+        double const ht0 = args.h[t0], ht1 = args.h[t1];
+        for (int fq = 0; fq < N * N; ++fq)
+        {
+          int const qa = fq % N, qb = fq / N;
+          double T = 0.0;
+          for (int j = 0; j < N; ++j)
+            for (int i = 0; i < N; ++i)
+            {
+              int loc[3];
+              loc[d] = side ? N - 1 : 0;
+              loc[t0] = i;
+              loc[t1] = j;
+              double const u =
+                  brick[(DEG * lx + loc[0]) + BXP * ((DEG * ly + loc[1]) + BY * (DEG * lz + loc[2]))];
+              T += args.S[qa][i] * args.S[qb][j] * u;
+            }
+          double rat[NS > 1 ? NS : 1];
+          double liquid = 0.0, p_old = 0.0, p_new = 0.0;
+          double *ph = nullptr;
+          if (NS == 3 && slot >= 0)
+          {
+            ph = &md.face_powder[((size_t)slot * 6 + f) * (N * N) + fq];
+            p_old = *ph;
+          }
+          int const pure = state_ratios<NS>(sp, mat, T, p_old, rat, liquid, p_new);
+          // p_new = min(1 - l, p_old) is idempotent, so the other level
+          // threads of this cell compute the same value whether they read
+          // the history before or after this store
+          if (ph && (d == 2 || slab == 0) && p_new != p_old)
+            *ph = p_new;
+          double const inv = inv_rho_cp<NS>(sp, gm, mat, rat, pure, T);
+          double conv_tinf = 0.0, conv_h = 0.0, rad_tinf = 0.0, rad_h = 0.0;
+          if (btype & B_CONVECTIVE)
+          {
+            conv_tinf = sp.props[mat][Q_CONV_TINF];
+            conv_h = property<NS>(sp, gm, P_CONV_COEF, mat, rat, pure, T);
+          }
+          if (btype & B_RADIATIVE)
+          {
+            rad_tinf = sp.props[mat][Q_RAD_TINF];
+            rad_h = property<NS>(sp, gm, P_EMISSIVITY, mat, rat, pure, T) * 5.670374419e-8 *
+                    (T + rad_tinf) * (T * T + rad_tinf * rad_tinf);
+          }
+          double const bval = -inv * (conv_h * (T - conv_tinf) + rad_h * (T - rad_tinf));
+          double const JxW = args.qw[qa] * ht0 * args.qw[qb] * ht1;
+#pragma unroll
+          for (int j = 0; j < N; ++j)
+#pragma unroll
+            for (int i = 0; i < N; ++i)
+            {
+              // node (loc) of this face; keep it if it is on level `slab`
+              int la, lb, lc;
+              if (d == 0)
+              {
+                la = side ? N - 1 : 0;
+                lb = i;
+                lc = j;
+              }
+              else if (d == 1)
+              {
+                la = i;
+                lb = side ? N - 1 : 0;
+                lc = j;
+              }
+              else
+              {
+                la = i;
+                lb = j;
+                lc = side ? N - 1 : 0;
+              }
+              if (lc != slab)
+                continue;
+              double const add = bval * (args.S[qa][i] * args.S[qb][j]) * JxW;
+#pragma unroll
+              for (int e = 0; e < NQS; ++e)
+                if (e == la + N * lb)
+                  res[e] += add;
+            }
+        }
+      }
+    }
+    // ---- per-node sums: a warp holds one 8 x 4 layer of cells (lane =
+    // lx + 8 ly), so the nodes shared in x and y are summed with shuffles
+    // into the cell that owns them (the lower one); nodes shared in z go
+    // through one shared-memory exchange between the level threads.
+    static_assert(TX == 8 && TY == 4, "the node merge assumes 8 x 4 cell layers per warp");
+    unsigned const full = 0xffffffffu;
+#pragma unroll
+    for (int j = 0; j < N; ++j)
+    {
+      double const v = __shfl_down_sync(full, res[0 + N * j], 1);
+      if (lx < TX - 1)
+        res[DEG + N * j] += v;
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+    {
+      double const v = __shfl_down_sync(full, res[i], TX);
+      if (ly < TY - 1)
+        res[i + N * DEG] += v;
+    }
+    if (slab == 0 && lz > 0)
+    {
+#pragma unroll
+      for (int i = 0; i < NQS; ++i)
+        xbuf[i * NCELL + cl] = res[i];
+    }
+    __syncthreads();
+    if (slab == DEG && lz < TZ - 1)
+    {
+#pragma unroll
+      for (int i = 0; i < NQS; ++i)
+        res[i] += xbuf[i * NCELL + cl + TX * TY];
+    }
+
+    // ---- state write-back
+    if (slab == 0 && active)
+    {
+      if (NS > 1)
+      {
+        double l = 0.0;
+        for (int s = 0; s < N; ++s)
+          l += lsum[s * NCELL + cl];
+        md.liquid_sum[c] = l;
+      }
+      if (NS == 3 && changed[cl])
+        md.powder_mode[c] = 2;
+    }
+    if (NS == 3 && active && pmode != 2 && changed[cl])
+    {
+      // the cell switches to per-point powder storage: write this level's
+      // points that kept the uniform value
+      size_t const pbase = c * NN + (size_t)NQS * slab;
+      for (int i = 0; i < NQS; ++i)
+        if (!((changed_mask >> i) & 1u))
+          md.powder_q[pbase + i] = pu;
+    }
+
+    // ---- colour-ordered write-out of the nodes this thread owns: the
+    // first tile (in colour order) that touches a node writes it, later
+    // ones add, the last one finalizes it. All loads first, then stores.
+    double const dt = (args.mode == 2) ? md.clock[1] : 0.0;
+    double *const znext = args.dst_sel == 1 ? md.za : md.zb;
+    bool const own_k = slab > 0 || lz == 0;
+    int const Z = DEG * lz + slab;
+    int const gz = nz0 + Z;
+    int const sz = (Z == 0 && tiz > 0) ? 1 : ((Z == DEG * TZ && tiz < args.nt[2] - 1) ? 2 : 0);
+    int rl[NQS];
+    size_t gidx[NQS];
+#pragma unroll
+    for (int i = 0; i < NQS; ++i)
+    {
+      int const a = i % N, bb = i / N;
+      int const X = DEG * lx + a, Y = DEG * ly + bb;
+      int const gx = nx0 + X, gy = ny0 + Y;
+      bool const own = own_k && (a > 0 || lx == 0) && (bb > 0 || ly == 0);
+      bool const inside = gx < args.nn[0] && gy < nn1 && gz < args.nn[2];
+      int const sx = (X == 0 && tix > 0) ? 1 : ((X == DEG * TX && tix < nt0 - 1) ? 2 : 0);
+      int const sy = (Y == 0 && tiy > 0) ? 1 : ((Y == DEG * TY && tiy < nt1 - 1) ? 2 : 0);
+      rl[i] = (own && inside) ? (sp.role[sx + 3 * sy + 9 * sz] | 4) : 0;
+      gidx[i] = gx + (size_t)pitch * (gy + (size_t)nn1 * gz);
+    }
+    if (args.mode == 0 || args.mode == 1)
+    {
+      double old[NQS];
+#pragma unroll
+      for (int i = 0; i < NQS; ++i)
+        old[i] = ((rl[i] & 4) && (args.mode == 1 || !(rl[i] & 1))) ? args.vdst[gidx[i]] : 0.0;
+#pragma unroll
+      for (int i = 0; i < NQS; ++i)
+        if (rl[i] & 4)
+          args.vdst[gidx[i]] = old[i] + res[i];
+    }
+    else
+    {
+      double pa[NQS], im[NQS], yv[NQS], sv[NQS], fv[NQS];
+#pragma unroll
+      for (int i = 0; i < NQS; ++i)
+      {
+        bool const valid = rl[i] & 4, first = rl[i] & 1, last = rl[i] & 2;
+        size_t const g = gidx[i];
+        pa[i] = (valid && !first) ? md.acc[g] : 0.0;
+        im[i] = (valid && last) ? md.inv_mass[g] : 0.0;
+        yv[i] = (valid && last) ? y[g] : 0.0;
+        sv[i] = (valid && last && args.n_stages > 1 && (args.stage > 0)) ? md.s[g] : 0.0;
+        fv[i] = (valid && last && args.has_f0) ? md.f0[g] : 0.0;
+      }
+#pragma unroll
+      for (int i = 0; i < NQS; ++i)
+      {
+        if (!(rl[i] & 4))
+          continue;
+        size_t const g = gidx[i];
+        double const total = pa[i] + res[i];
+        if (!(rl[i] & 2))
+        {
+          md.acc[g] = total;
+          continue;
+        }
+        double const f = im[i] * total;
+        if (!isfinite(f))
+          atomicCAS(md.error, 0, (int)DERR_NONFINITE);
+        if (args.n_stages == 1)
+        {
+          y[g] = yv[i] + dt * f;
+        }
+        else if (!args.last)
+        {
+          double zn = yv[i];
+          if (args.has_f0)
+            zn = zn + (dt * args.a_next_f0) * fv[i];
+          zn = zn + (dt * args.a_next) * f;
+          znext[g] = zn;
+          double const sb = (dt * args.b_i) * f;
+          md.s[g] = args.stage == 0 ? sb : sv[i] + sb;
+          if (args.store_f0)
+            md.f0[g] = f;
+        }
+        else
+        {
+          y[g] = yv[i] + (sv[i] + (dt * args.b_i) * f);
+        }
+      }
+    }
+    // vmult writes zeros into the row padding of the node layout
+    if (args.mode == 0 && tix == nt0 - 1 && pitch > args.nn[0])
+    {
+      int const npad = pitch - args.nn[0];
+      for (int i = tid; i < npad * BY * BZ; i += NT)
+      {
+        int const X = i % npad, Y = (i / npad) % BY, Z = i / (npad * BY);
+        int const gy = ny0 + Y, gz = nz0 + Z;
+        if (gy < nn1 && gz < args.nn[2])
+          args.vdst[args.nn[0] + X + (size_t)pitch * (gy + (size_t)nn1 * gz)] = 0.0;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+} // namespace adm

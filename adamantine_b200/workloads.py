@@ -1,0 +1,141 @@
+"""Seeded synthetic workloads of the hot-path benchmark and tests.
+
+The reference publishes no benchmark suite for this path; these builders
+create problems with the shapes, sizes and value ranges of the five benchmark
+configurations (mesh, FE degree, material model, source and time stepping),
+with every random quantity drawn from a named, seeded numpy stream.
+"""
+from __future__ import annotations
+
+import zlib
+
+import numpy as np
+
+from .config import Boundary, Geometry, Material, Source, ThermalConfig
+
+SEED = 20261203
+
+
+def rng_for(name: str, seed: int = SEED) -> np.random.Generator:
+    return np.random.default_rng([seed, zlib.crc32(name.encode())])
+
+
+# --------------------------------------------------------------- materials
+def steel_solid_material() -> Material:
+    """Solid only: rho 7904 kg/m^3, c_p 714 J/kg/K, k 31.4 W/m/K, h_conv 10."""
+    db = {
+        "property_format": "polynomial",
+        "n_materials": 1,
+        "material_0.solid.density": 7904.0,
+        "material_0.solid.specific_heat": 714.0,
+        "material_0.solid.thermal_conductivity_x": 31.4,
+        "material_0.solid.thermal_conductivity_y": 31.4,
+        "material_0.solid.thermal_conductivity_z": 31.4,
+        "material_0.solid.convection_heat_transfer_coef": 10.0,
+        "material_0.convection_temperature_infty": 300.0,
+    }
+    return Material.from_database(db, n_states=1, p_order=0)
+
+
+def phase_change_material(rng=None, k_scale: float = 1.0, cp_scale: float = 1.0) -> Material:
+    """Solid / liquid / powder; solidus 1648 K, liquidus 1673 K, L = 2.9e5 J/kg.
+
+    k_solid(T): seeded quadratic with k(300) = 10 and k(1700) = 35 W/m/K,
+    monotone on [300, 1700]; k_powder = 0.5% of k_solid; k_liquid = 35.
+    c_p: seeded linear function (about 500 J/kg/K at 300 K).  rho = 7904.
+    k_scale and cp_scale multiply every conductivity / specific-heat
+    coefficient (the perturbed parameters of the ensemble and the adjoint).
+    """
+    rng = rng if rng is not None else rng_for("phase_change_material")
+    t0, t1 = 300.0, 1700.0
+    c = rng.uniform(-5e-6, 5e-6)
+    b = (35.0 - 10.0) / (t1 - t0) - c * (t0 + t1)
+    a = 10.0 - b * t0 - c * t0 * t0
+    cp0 = rng.uniform(440.0, 480.0)
+    cp1 = rng.uniform(0.15, 0.25)
+    ks = np.array([a, b, c]) * k_scale
+    db = {"property_format": "polynomial", "n_materials": 1,
+          "material_0.solidus": 1648.0, "material_0.liquidus": 1673.0, "material_0.latent_heat": 2.9e5}
+    for s, kk in (("solid", ks), ("powder", 0.005 * ks), ("liquid", np.array([35.0 * k_scale, 0.0, 0.0]))):
+        db[f"material_0.{s}.density"] = 7904.0
+        db[f"material_0.{s}.specific_heat"] = f"{cp0 * cp_scale!r}, {cp1 * cp_scale!r}"
+        for ax in ("x", "y", "z"):
+            db[f"material_0.{s}.thermal_conductivity_{ax}"] = ", ".join(repr(float(v)) for v in kk)
+    return Material.from_database(db, n_states=3, p_order=2)
+
+
+# --------------------------------------------------------------- scan paths
+def line_segments(x0, x1, y, z, speed, t0=1e-9):
+    """A point segment then one line along x at `speed`."""
+    return np.array([[t0, 0.0, x0, y, z], [t0 + abs(x1 - x0) / speed, 1.0, x1, y, z]])
+
+
+def serpentine_segments(rng, x0, x1, y0, z, n_passes, hatch, speed):
+    """Seeded serpentine: n_passes lines along x, hatch apart, joined by
+    power-off moves (end_time, power_modifier, x, y, z rows)."""
+    jitter = rng.uniform(-0.1, 0.1) * hatch
+    rows = [[1e-9, 0.0, x0, y0 + jitter, z]]
+    t = rows[0][0]
+    x, y = x0, y0 + jitter
+    for p in range(n_passes):
+        xe = x1 if p % 2 == 0 else x0
+        t += abs(xe - x) / speed
+        rows.append([t, 1.0, xe, y, z])
+        x = xe
+        if p + 1 < n_passes:
+            y += hatch
+            t += hatch / speed
+            rows.append([t, 0.0, x, y, z])
+    return np.array(rows)
+
+
+# --------------------------------------------------------------- configs
+def solid_q1_small() -> ThermalConfig:
+    """10x10x5 mm, 32x32x16 Q1, Gauss 2, solid, convective top (h = 10,
+    T_inf = 300), Goldak 200 W / 0.3 / R = d = 50 um along +x at 1 m/s on the
+    top mid-line; forward Euler, dt = 1e-6."""
+    geo = Geometry(dim=3, n_cells=(32, 32, 16), extent=(10e-3, 10e-3, 5e-3))
+    bnd = Boundary.from_database({"type": "adiabatic", "boundary_5.type": "convective"}, 3)
+    src = Source(type="goldak", depth=50e-6, absorption_efficiency=0.3, diameter=100e-6, max_power=200.0,
+                 segments=line_segments(0.0, 10e-3, 5e-3, 5e-3, 1.0))
+    return ThermalConfig(geometry=geo, material=steel_solid_material(), boundary=bnd, sources=[src], degree=1,
+                         time_method="forward_euler")
+
+
+def phase_change_q2(n_cells=(128, 128, 64), extent=(20e-3, 20e-3, 10e-3), powder_layers=16,
+                    method="rk_fourth_order", k_scale=1.0, cp_scale=1.0, absorptivity=0.35,
+                    power=400.0) -> ThermalConfig:
+    """20x20x10 mm, 128x128x64 Q2, Gauss 3, solid/liquid/powder with powder in
+    the top 16 cell layers, Goldak 400 W / 0.35 (R = d = 50 um) on a seeded
+    10-pass serpentine (hatch 200 um, 1 m/s); adiabatic; RK4."""
+    nz = n_cells[2]
+    hz = extent[2] / nz
+    geo = Geometry(dim=3, n_cells=n_cells, extent=extent, material_height=extent[2] + 0.5 * hz,
+                   use_powder=True, powder_layer=powder_layers * hz + 0.5 * hz)
+    bnd = Boundary.from_database({"type": "adiabatic"}, 3)
+    rng = rng_for("phase_change_q2-scan")
+    seg = serpentine_segments(rng, 0.25 * extent[0], 0.75 * extent[0], 0.45 * extent[1], extent[2], 10,
+                              200e-6, 1.0)
+    src = Source(type="goldak", depth=50e-6, absorption_efficiency=absorptivity, diameter=100e-6,
+                 max_power=power, segments=seg)
+    mat = phase_change_material(k_scale=k_scale, cp_scale=cp_scale)
+    return ThermalConfig(geometry=geo, material=mat, boundary=bnd, sources=[src], degree=2, time_method=method)
+
+
+def initial_temperature(cfg: ThermalConfig, name: str, melt_pool: bool = True) -> np.ndarray:
+    """300 K + U(-1, 1) noise on the (nz, ny, nx) node grid; with melt_pool a
+    seeded 2000 K Gaussian spot under the scan-path start so that liquid,
+    mushy and powder-to-liquid points exist."""
+    geo = cfg.geometry
+    rng = rng_for("initial-" + name)
+    shape = geo.node_shape(cfg.degree)[::-1]
+    T = 300.0 + rng.uniform(-1.0, 1.0, shape)
+    if melt_pool and cfg.sources:
+        seg = cfg.sources[0].segments
+        cx, cy, cz = seg[0, 2], seg[0, 3], seg[0, 4]
+        zs = np.linspace(geo.origin[2], geo.origin[2] + geo.extent[2], shape[0])
+        ys = np.linspace(geo.origin[1], geo.origin[1] + geo.extent[1], shape[1])
+        xs = np.linspace(geo.origin[0], geo.origin[0] + geo.extent[0], shape[2])
+        r2 = ((xs[None, None, :] - cx) ** 2 + (ys[None, :, None] - cy) ** 2 + (zs[:, None, None] - cz) ** 2)
+        T += 1700.0 * np.exp(-r2 / (0.4e-3) ** 2)
+    return T

@@ -1,0 +1,24 @@
+/*
+ * adamantine_b200 -- diagnostic entry points (no counterpart in the
+ * reference). They exist so that tests can check building blocks of the
+ * kernels on the GPU.
+ */
+#ifndef ADAMANTINE_B200_DIAG_H
+#define ADAMANTINE_B200_DIAG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* y[i] = reciprocal of x[i] as computed by the tile kernel (Newton-Raphson on
+ * the hardware estimate), and y_ref[i] = 1.0 / x[i] (IEEE division); device
+ * pointers, n values, on the CUDA default stream; synchronizes. */
+int adm_diag_reciprocal(double const *x, double *y, double *y_ref, int64_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
