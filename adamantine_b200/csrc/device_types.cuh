@@ -171,6 +171,9 @@ struct KernelArgs
   double G[3][3];        // G = D S: nodal-basis derivative at the quadrature points
   double qw[3];          // 1D quadrature weights on [0,1]
   double qx[3];          // 1D quadrature points on [0,1]
+  // per Gauss point q (lexicographic, up to 27): W_q vol / h_x^2,
+  // W_q vol / h_y^2, W_q vol / h_z^2, W_q vol, with W_q the product weight
+  double cw[27][4];
 };
 
 } // namespace adm

@@ -670,6 +670,14 @@ KernelArgs Thermal::base_args() const
   std::memcpy(a.G, r.G, sizeof(a.G));
   std::memcpy(a.qw, r.w, sizeof(a.qw));
   std::memcpy(a.qx, r.x, sizeof(a.qx));
+  int const n = r.n;
+  for (int q = 0; q < n * n * n; ++q)
+  {
+    double const W = r.w[q % n] * r.w[(q / n) % n] * r.w[q / (n * n)];
+    for (int d = 0; d < 3; ++d)
+      a.cw[q][d] = W * a.vol_over_h2[d];
+    a.cw[q][3] = W * vol;
+  }
   return a;
 }
 

@@ -404,7 +404,7 @@ __device__ __forceinline__ void load_member_constants(SmemPhys &sp, MemberData c
 // other buffer while the current item is computed.
 template <int DEG, int NS, int P>
 __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
-    tile_kernel(const __grid_constant__ CUtensorMap tmap, KernelArgs const args, int n_items)
+    tile_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ KernelArgs args, int n_items)
 {
   using T_ = TD<DEG>;
   constexpr int N = T_::N, NN = T_::NN, NT = T_::NT, NCELL = T_::NCELL, NQS = T_::NQS;
@@ -646,7 +646,25 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
         sn = md.sinv[c];
       }
       bool const fast_ok = !sp.use_table && sp.isotropic && !sp.has_rotation;
-      double const Wz = args.qw[slab];
+      // Below the solidus the liquid ratio is 0 and the powder ratio keeps
+      // its value (min(1, p) = p), so a cell whose powder ratio is uniformly
+      // 0 or 1 is in one pure state there: `cold` names it (or -1).
+      double const solidus = sp.props[mat][Q_SOLIDUS];
+      int cold = -1;
+      if (fast_ok)
+      {
+        if (NS == 1)
+          cold = 0;
+        else if (NS == 2)
+          cold = 0;
+        else if (pmode == 0)
+          cold = 0;
+        else if (pmode == 1 && pu == 1.0)
+          cold = 2;
+      }
+      constexpr int PS = kMaxStates * kMaxPoly; // stride between properties
+      double const *cold_c = &sp.poly[mat][0][cold < 0 ? 0 : cold][0];
+      double const *cw = &args.cw[NQS * slab][0];
 #pragma unroll
       for (int i = 0; i < NQS; ++i)
       {
@@ -660,44 +678,73 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
           gy = fma(args.D[qb][k], Tq[qa + N * k], gy);
         }
         double const gz = az[i];
-        double p_old = 0.0;
-        if (NS == 3)
-          p_old = (pmode == 2) ? md.powder_q[pbase + i] : pu;
-        double rat[NS > 1 ? NS : 1];
-        double liquid = 0.0, p_new = p_old;
-        int const pure = state_ratios<NS>(sp, mat, T, p_old, rat, liquid, p_new);
-        if (NS > 1)
-          liquid_acc += liquid;
-        if (NS == 3 && p_new != p_old)
+        double inv, fx, fy, fz;
+        if (cold >= 0 && (NS == 1 || T < solidus))
         {
-          md.powder_q[pbase + i] = p_new;
-          changed_mask |= 1u << i;
-        }
-        QpCoef k;
-        if (fast_ok && pure >= 0)
-        {
-          // one state, polynomial, isotropic: Horner in that state only
-          double const *cc = &sp.poly[mat][0][NS == 1 ? 0 : pure][0];
-          constexpr int PS = kMaxStates * kMaxPoly; // stride between properties
-          double const rho = horner_fixed<P>(cc + P_DENSITY * PS, T);
-          double const cp = horner_fixed<P>(cc + P_SPECIFIC_HEAT * PS, T);
-          k.inv = recip(rho * cp);
-          k.kxx = horner_fixed<P>(cc + P_KX * PS, T);
-          k.kyy = k.kxx;
-          k.kzz = k.kxx;
-          k.kxy = 0.0;
+          // one state, polynomial, isotropic: Horner in that state only;
+          // cw holds W_q * vol / h_d^2 and W_q * vol for this point
+          double const rho = horner_fixed<P>(cold_c + P_DENSITY * PS, T);
+          double const cp = horner_fixed<P>(cold_c + P_SPECIFIC_HEAT * PS, T);
+          inv = recip(rho * cp);
+          double const cf = -inv * horner_fixed<P>(cold_c + P_KX * PS, T);
+          fx = (cf * cw[4 * i + 0]) * gx;
+          fy = (cf * cw[4 * i + 1]) * gy;
+          fz = (cf * cw[4 * i + 2]) * gz;
         }
         else
         {
-          qp_general<NS>(sp, gm, mat, rat[0], NS > 1 ? rat[1] : 0.0, NS > 2 ? rat[2] : 0.0, pure, T,
-                         cs, sn, k);
+          double p_old = 0.0;
+          if (NS == 3)
+            p_old = (pmode == 2) ? md.powder_q[pbase + i] : pu;
+          double r0, r1 = 0.0, r2 = 0.0;
+          double liquid = 0.0, p_new = p_old;
+          int pure;
+          {
+            double rat[NS > 1 ? NS : 1];
+            pure = state_ratios<NS>(sp, mat, T, p_old, rat, liquid, p_new);
+            r0 = rat[0];
+            if (NS > 1)
+              r1 = rat[1];
+            if (NS > 2)
+              r2 = rat[NS > 2 ? 2 : 0];
+          }
+          if (NS > 1)
+            liquid_acc += liquid;
+          if (NS == 3 && p_new != p_old)
+          {
+            md.powder_q[pbase + i] = p_new;
+            changed_mask |= 1u << i;
+          }
+          double kxx, kxy, kyy, kzz;
+          if (fast_ok && pure >= 0)
+          {
+            double const *cc = &sp.poly[mat][0][NS == 1 ? 0 : pure][0];
+            double const rho = horner_fixed<P>(cc + P_DENSITY * PS, T);
+            double const cp = horner_fixed<P>(cc + P_SPECIFIC_HEAT * PS, T);
+            inv = recip(rho * cp);
+            kxx = horner_fixed<P>(cc + P_KX * PS, T);
+            kyy = kxx;
+            kzz = kxx;
+            kxy = 0.0;
+          }
+          else
+          {
+            QpCoef kk;
+            qp_general<NS>(sp, gm, mat, r0, r1, r2, pure, T, cs, sn, kk);
+            inv = kk.inv;
+            kxx = kk.kxx;
+            kxy = kk.kxy;
+            kyy = kk.kyy;
+            kzz = kk.kzz;
+          }
+          double const W = args.qw[qa] * args.qw[qb] * args.qw[slab];
+          double const grx = gx * args.inv_h[0], gry = gy * args.inv_h[1];
+          double const cf = -inv * W;
+          fx = cf * (kxx * grx + kxy * gry) * args.vol_over_h[0];
+          fy = cf * (kxy * grx + kyy * gry) * args.vol_over_h[1];
+          fz = cf * kzz * gz * args.vol_over_h2[2];
         }
-        double const W = args.qw[qa] * args.qw[qb] * Wz;
-        double const grx = gx * args.inv_h[0], gry = gy * args.inv_h[1];
-        double const cf = -k.inv * W;
-        double const fx = cf * (k.kxx * grx + k.kxy * gry) * args.vol_over_h[0];
-        double const fy = cf * (k.kxy * grx + k.kyy * gry) * args.vol_over_h[1];
-        az[i] = cf * k.kzz * gz * args.vol_over_h2[2];
+        az[i] = fz;
 #pragma unroll
         for (int m = 0; m < N; ++m)
         {
@@ -709,7 +756,7 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
           double const px = (args.origin[0] + cx * args.h[0]) + args.qx[qa] * args.h[0];
           double const py = (args.origin[1] + cy * args.h[1]) + args.qx[qb] * args.h[1];
           double const pz = (args.origin[2] + cz * args.h[2]) + args.qx[slab] * args.h[2];
-          axy[i] += beam_sum(sp, px, py, pz) * k.inv * (W * args.vol);
+          axy[i] += beam_sum(sp, px, py, pz) * inv * cw[4 * i + 3];
         }
       }
       if (NS == 3 && pmode != 2 && changed_mask)
