@@ -46,6 +46,7 @@ SIGNATURES = {
     "adm_mark_has_melted": [_VP, ctypes.c_double, _VP, _U8],
     "adm_activate_cells": [_VP, _I64, ctypes.c_int64, ctypes.c_double, _D, _D, _VP],
     "adm_update_beam": [_VP, ctypes.c_int32, ctypes.POINTER(SourceStruct)],
+    "adm_vmult_host_static": [_VP, _D, _D],
     "adm_device_error": [_VP, _I32],
     "adm_synchronize": [_VP],
 }

@@ -53,6 +53,13 @@ adm::Thermal const *as(adm_thermal const *h)
   } while (0)
 } // namespace
 
+namespace adm
+{
+// Records a failure message for adm_last_error() (used by entry points
+// defined in other translation units).
+void set_last_error(std::string const &msg) { g_last_error = msg; }
+} // namespace adm
+
 extern "C" {
 
 const char *adm_last_error(void) { return g_last_error.c_str(); }

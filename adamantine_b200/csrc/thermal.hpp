@@ -154,6 +154,7 @@ public:
   double evolve_one_time_step_host(double t, double dt, double *solution_host);
   int32_t device_error();
   cudaStream_t stream() const { return stream_; }
+  int device() const { return device_; }
   void synchronize();
 
   // stage schedule (Butcher tableau of the configured method)

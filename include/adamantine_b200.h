@@ -191,6 +191,27 @@ int adm_activate_cells(adm_thermal *h, int64_t const *cells, int64_t n,
  * radius and power for source i (segments are ignored). */
 int adm_update_beam(adm_thermal *h, int32_t i, adm_source const *beam);
 
+/* Largest node vector (adm_n_nodes) that adm_vmult_host_static accepts. */
+#define ADM_STATIC_SCRATCH_MAX_NODES 1310720
+
+/* vmult on host buffers that allocates nothing (no counterpart in the
+ * reference). For callers that hold their vectors in host memory and cannot
+ * allocate device memory at the point of the call -- for example code that
+ * runs while another part of the program is capturing a CUDA graph (a
+ * cudaMalloc there breaks the capture) or a process whose device memory
+ * budget is fixed up front. adm_vmult_host allocates its device staging
+ * vectors on first use; this entry point stages src and dst in one static
+ * device array of 2 x ADM_STATIC_SCRATCH_MAX_NODES doubles (20 MiB, held by
+ * every GPU that loads the library until the process exits) and calls no
+ * cudaMalloc or cudaFree. The first call on a device looks up that array's
+ * device address; make that first call before any stream capture. Vectors
+ * longer than the maximum are rejected with ADM_ERR_INVALID. The staged dst
+ * is rewritten completely by every call (nodes no active cell touches are
+ * cleared to zero). All calls on a device share the array, so calls that
+ * overlap on the GPU (other threads, other streams) race; serialize them.
+ * Synchronizes the handle's stream. */
+int adm_vmult_host_static(adm_thermal *h, double *dst_host, double const *src_host);
+
 /* Sticky device error word: 0 if no kernel reported a fault. Synchronizes. */
 int adm_device_error(adm_thermal *h, int32_t *code);
 /* Wait for the handle's stream. */
