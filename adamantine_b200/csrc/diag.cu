@@ -27,3 +27,66 @@ extern "C" int adm_diag_reciprocal(double const *x, double *y, double *y_ref, in
     return ADM_ERR_CUDA;
   return ADM_OK;
 }
+
+namespace
+{
+// Eight independent FMA chains per thread, so that the FP64 pipe, not the
+// dependent-issue latency, bounds the rate.
+__global__ void __launch_bounds__(256) fma_rate_kernel(double b, double c, int iters, double *out)
+{
+  double a[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    a[k] = threadIdx.x * 1e-3 + k;
+  for (int it = 0; it < iters; ++it)
+  {
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      a[k] = fma(a[k], b, c);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    s += a[k];
+  out[blockIdx.x * (int64_t)blockDim.x + threadIdx.x] = s;
+}
+} // namespace
+
+extern "C" int adm_diag_fp64_fma_rate(int device, double *tflops)
+{
+  if (!tflops)
+    return ADM_ERR_INVALID;
+  *tflops = 0.0;
+  if (cudaSetDevice(device) != cudaSuccess)
+    return ADM_ERR_CUDA;
+  int n_sm = 0;
+  if (cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+    return ADM_ERR_CUDA;
+  int const blocks = n_sm * 8, threads = 256, iters = 4096;
+  double *out = nullptr;
+  if (cudaMalloc(&out, sizeof(double) * blocks * threads) != cudaSuccess)
+    return ADM_ERR_ALLOC;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 0.f;
+  int rc = ADM_OK;
+  for (int rep = 0; rep < 6 && rc == ADM_OK; ++rep)
+  {
+    cudaEventRecord(e0);
+    fma_rate_kernel<<<blocks, threads>>>(0.999999, 1e-6, iters, out);
+    cudaEventRecord(e1);
+    if (cudaGetLastError() != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess)
+      rc = ADM_ERR_CUDA;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (rep > 0 && (best == 0.f || ms < best))
+      best = ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  if (rc == ADM_OK && best > 0.f)
+    *tflops = 2.0 * 8.0 * iters * (double)blocks * threads / (best * 1e-3) / 1e12;
+  return rc;
+}

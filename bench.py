@@ -35,6 +35,34 @@ METRIC = "heat vmult GDoF/s (FP64 Q2) & %HBM peak; batched-ensemble vs looped st
 WORKLOAD = "phase_change_q2_128x128x64_vmult"
 
 
+# FP64 work of one Q2 cell of this workload: 1257 DFMA + 379 DMUL + 41 DADD
+# thread instructions per cell (ncu sm__sass_thread_inst_executed_op_d*
+# counts of tile_kernel<2,3,2> on the 128x128x32 case) = 2934 FLOP.
+FP64_FLOP_PER_Q2_CELL = 2934
+
+# DRAM bytes (read + write) of one vmult of the 128x128x64 workload: sum of
+# dram__bytes_read.sum + dram__bytes_write.sum over the 8 colour launches of
+# the tile kernel in one ncu capture (L2 flushed before every launch, so the
+# halo and partial-sum re-reads that stay in L2 in the timed loop are counted).
+DRAM_BYTES_PER_VMULT_FULL = 327.0e6
+
+
+def fp64_fma_peak(device):
+    """Measured FP64 FMA throughput (TFLOP/s) of the GPU, from the library's
+    diagnostic microbenchmark."""
+    import ctypes
+
+    from adamantine_b200 import _lib
+
+    L = _lib.load()
+    fn = L.adm_diag_fp64_fma_rate
+    fn.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    fn.restype = ctypes.c_int
+    out = ctypes.c_double(0.0)
+    _lib.check(fn(device, ctypes.byref(out)))
+    return out.value
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -230,6 +258,7 @@ def run_ours(args, rank, world, local_rank):
     del src_h
 
     peak, peak_kind = measured_peaks()
+    fp64_peak = fp64_fma_peak(local_rank)
     # algorithmic bytes of one vmult: read src, write dst (8 B per node each),
     # cell info (4 B per cell), per-cell powder mode (1 B) and liquid sums
     # (8 B) and the per-qp powder of cells whose powder varies inside the
@@ -239,6 +268,8 @@ def run_ours(args, rank, world, local_rank):
     mixed = int(np.sum(np.any(powder != powder[:, :1], axis=1)))
     alg_bytes = 16 * g.m() + 4 * C + 1 * C + 8 * C + 16 * 27 * mixed
     achieved = alg_bytes / (ms_per_step * 1e-3) / 1e9
+    fp64_flop = FP64_FLOP_PER_Q2_CELL * C
+    fp64_achieved = fp64_flop / (ms_per_step * 1e-3) / 1e12
 
     line = {
         "metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
@@ -249,9 +280,17 @@ def run_ours(args, rank, world, local_rank):
                    "states": "solid/liquid/powder", "source": "Goldak 400 W", "parallelism": f"replicas x{world}",
                    "l2": "two src/dst pairs alternate (272 MB working set > 126 MB L2)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "peak_kind": f"{peak_kind} hbm_gbs",
+                     "frac": achieved / peak,
+                     "traffic": DRAM_BYTES_PER_VMULT_FULL if args.size == "full" else None,
+                     "traffic_note": "ncu, L2 flushed before each of the 8 colour launches", "peak_kind": f"{peak_kind} hbm_gbs",
                      "kernel": "adm::tile_kernel<2,3> (8 colour launches per vmult)",
                      "algorithmic_bytes_per_vmult": alg_bytes},
+        # the operator is FP64-issue bound (per-qp physics plus sum
+        # factorization), so the FP64 roofline is the binding one
+        "roofline_fp64": {"bound": "fp64", "achieved": fp64_achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                          "frac": fp64_achieved / fp64_peak if fp64_peak else None,
+                          "flop_per_vmult": fp64_flop,
+                          "peak_kind": "measured FP64 FMA rate (adm_diag_fp64_fma_rate) on this GPU"},
         "e2e": {"value": e2e_val, "unit": "GDoF/s", "h2d_bytes_per_step": 8 * g.m(),
                 "d2h_bytes_per_step": 8 * g.m(), "path": "adm_vmult_host (pinned host buffers)"},
         "gpu_launches": args.steps * 9,

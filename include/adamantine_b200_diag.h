@@ -17,6 +17,11 @@ extern "C" {
  * pointers, n values, on the CUDA default stream; synchronizes. */
 int adm_diag_reciprocal(double const *x, double *y, double *y_ref, int64_t n);
 
+/* FP64 FMA throughput of the device in TFLOP/s (2 FLOP per FMA), measured
+ * with independent FMA chains on every SM; the FP64 roofline denominator.
+ * Best of five timed launches after one warm-up; synchronizes. */
+int adm_diag_fp64_fma_rate(int device, double *tflops);
+
 #ifdef __cplusplus
 }
 #endif
