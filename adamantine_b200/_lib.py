@@ -49,6 +49,26 @@ SIGNATURES = {
     "adm_vmult_host_static": [_VP, _D, _D],
     "adm_device_error": [_VP, _I32],
     "adm_synchronize": [_VP],
+    # include/adamantine_b200_ensemble.h
+    "adm_ensemble_create": [ctypes.POINTER(ConfigStruct), ctypes.c_int32, ctypes.c_int, _VP, ctypes.POINTER(_VP)],
+    "adm_ensemble_destroy": [_VP],
+    "adm_ensemble_set_cells": [_VP, ctypes.c_int32, _U8, _U8, _U8, _D, _D],
+    "adm_ensemble_setup": [_VP],
+    "adm_ensemble_stride": [_VP, _I64],
+    "adm_ensemble_n_work_items": [_VP, _I64],
+    "adm_ensemble_evolve_one_time_step": [_VP, ctypes.c_double, ctypes.c_double, _VP, _D],
+    "adm_ensemble_evolve_looped": [_VP, ctypes.c_double, ctypes.c_double, _VP, _D],
+    "adm_ensemble_evolve_n_steps": [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_int32, _VP, _D],
+    "adm_ensemble_update_beam": [_VP, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(SourceStruct)],
+    "adm_ensemble_update_material": [_VP, ctypes.c_int32, ctypes.POINTER(ConfigStruct)],
+    "adm_ensemble_get_cell_state": [_VP, ctypes.c_int32, _D],
+    "adm_ensemble_get_inverse_mass_matrix": [_VP, ctypes.c_int32, _VP],
+    "adm_ensemble_device_error": [_VP, _I32],
+    "adm_ensemble_synchronize": [_VP],
+    "adm_enkf_create": [ctypes.c_int, _VP, ctypes.POINTER(_VP)],
+    "adm_enkf_destroy": [_VP],
+    "adm_enkf_analysis": [_VP, ctypes.c_int32, _VP, ctypes.c_int64, ctypes.c_int64, _VP, ctypes.c_int32,
+                          ctypes.c_int32, _VP, _VP, _VP, _VP, _VP, _VP],
 }
 
 _lib = None

@@ -1,7 +1,7 @@
 // extern "C" entry points of include/adamantine_b200.h over adm::Thermal.
 // No C++ exception crosses the ABI: each call returns a status code and keeps
 // the message for adm_last_error().
-#include "thermal.hpp"
+#include "capi_common.hpp"
 
 #include <string>
 
@@ -9,54 +9,17 @@ namespace
 {
 thread_local std::string g_last_error;
 
-template <class F>
-int guard(F &&f)
-{
-  try
-  {
-    f();
-    return ADM_OK;
-  }
-  catch (adm::Error const &e)
-  {
-    g_last_error = e.what();
-    return e.code;
-  }
-  catch (std::bad_alloc const &)
-  {
-    g_last_error = "host allocation failed";
-    return ADM_ERR_ALLOC;
-  }
-  catch (std::exception const &e)
-  {
-    g_last_error = e.what();
-    return ADM_ERR_INVALID;
-  }
-  catch (...)
-  {
-    g_last_error = "unknown error";
-    return ADM_ERR_INVALID;
-  }
-}
-
 adm::Thermal *as(adm_thermal *h) { return reinterpret_cast<adm::Thermal *>(h); }
 adm::Thermal const *as(adm_thermal const *h)
 {
   return reinterpret_cast<adm::Thermal const *>(h);
 }
-
-#define ADM_REQUIRE(cond, msg)                                                 \
-  do                                                                           \
-  {                                                                            \
-    if (!(cond))                                                               \
-      throw adm::Error(ADM_ERR_INVALID, msg);                                  \
-  } while (0)
 } // namespace
 
 namespace adm
 {
-// Records a failure message for adm_last_error() (used by entry points
-// defined in other translation units).
+// Records a failure message for adm_last_error() (also used by the entry
+// points defined in other translation units).
 void set_last_error(std::string const &msg) { g_last_error = msg; }
 } // namespace adm
 
@@ -66,7 +29,7 @@ const char *adm_last_error(void) { return g_last_error.c_str(); }
 
 int adm_create(adm_config const *cfg, int device, void *stream, adm_thermal **out)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(cfg && out, "null argument");
     *out = nullptr;
     auto *t = new adm::Thermal(*cfg, device, reinterpret_cast<cudaStream_t>(stream));
@@ -76,14 +39,14 @@ int adm_create(adm_config const *cfg, int device, void *stream, adm_thermal **ou
 
 int adm_destroy(adm_thermal *h)
 {
-  return guard([&] { delete as(h); });
+  return adm::guard([&] { delete as(h); });
 }
 
 int adm_set_cells(adm_thermal *h, uint8_t const *active, uint8_t const *material_id,
                   uint8_t const *initial_state, double const *deposition_cos,
                   double const *deposition_sin)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(h, "null handle");
     as(h)->set_cells(active, material_id, initial_state, deposition_cos, deposition_sin);
   });
@@ -91,7 +54,7 @@ int adm_set_cells(adm_thermal *h, uint8_t const *active, uint8_t const *material
 
 int adm_setup(adm_thermal *h)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(h, "null handle");
     as(h)->setup();
   });
@@ -99,7 +62,7 @@ int adm_setup(adm_thermal *h)
 
 int adm_n_nodes(adm_thermal const *h, int64_t *n)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(h && n, "null argument");
     *n = (int64_t)as(h)->m();
   });
@@ -107,7 +70,7 @@ int adm_n_nodes(adm_thermal const *h, int64_t *n)
 
 int adm_n_cells(adm_thermal const *h, int64_t *n)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(h && n, "null argument");
     *n = (int64_t)as(h)->n_cells();
   });
@@ -115,7 +78,7 @@ int adm_n_cells(adm_thermal const *h, int64_t *n)
 
 int adm_node_layout(adm_thermal const *h, int64_t nodes[3], int64_t *pitch)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(h && nodes && pitch, "null argument");
     adm::Mesh const &m = as(h)->mesh();
     for (int d = 0; d < 3; ++d)
@@ -126,7 +89,7 @@ int adm_node_layout(adm_thermal const *h, int64_t nodes[3], int64_t *pitch)
 
 int adm_set_time(adm_thermal *h, double t)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(h, "null handle");
     as(h)->set_time(t);
   });
@@ -134,7 +97,7 @@ int adm_set_time(adm_thermal *h, double t)
 
 int adm_vmult(adm_thermal *h, double *dst, double const *src)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(h && dst && src, "null argument");
     ADM_REQUIRE(dst != src, "vmult needs distinct src and dst");
     as(h)->vmult(dst, src, false);
@@ -143,7 +106,7 @@ int adm_vmult(adm_thermal *h, double *dst, double const *src)
 
 int adm_vmult_add(adm_thermal *h, double *dst, double const *src)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(h && dst && src, "null argument");
     ADM_REQUIRE(dst != src, "vmult_add needs distinct src and dst");
     as(h)->vmult(dst, src, true);
@@ -152,7 +115,7 @@ int adm_vmult_add(adm_thermal *h, double *dst, double const *src)
 
 int adm_vmult_host(adm_thermal *h, double *dst_host, double const *src_host)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(h && dst_host && src_host, "null argument");
     as(h)->vmult_host(dst_host, src_host);
   });
@@ -160,7 +123,7 @@ int adm_vmult_host(adm_thermal *h, double *dst_host, double const *src_host)
 
 int adm_compute_inverse_mass_matrix(adm_thermal *h)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(h, "null handle");
     as(h)->compute_inverse_mass_matrix();
   });
@@ -168,7 +131,7 @@ int adm_compute_inverse_mass_matrix(adm_thermal *h)
 
 int adm_get_inverse_mass_matrix(adm_thermal *h, double *dst)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(h && dst, "null argument");
     adm::Thermal *t = as(h);
     ADM_CK(cudaMemcpyAsync(dst, t->inverse_mass_matrix(), t->m() * sizeof(double),
@@ -179,7 +142,7 @@ int adm_get_inverse_mass_matrix(adm_thermal *h, double *dst)
 int adm_evolve_one_time_step(adm_thermal *h, double t, double dt, double *solution,
                              double *t_out)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(h && solution, "null argument");
     double const tn = as(h)->evolve_one_time_step(t, dt, solution);
     if (t_out)
@@ -190,7 +153,7 @@ int adm_evolve_one_time_step(adm_thermal *h, double t, double dt, double *soluti
 int adm_evolve_one_time_step_host(adm_thermal *h, double t, double dt,
                                   double *solution_host, double *t_out)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(h && solution_host, "null argument");
     double const tn = as(h)->evolve_one_time_step_host(t, dt, solution_host);
     if (t_out)
@@ -201,7 +164,7 @@ int adm_evolve_one_time_step_host(adm_thermal *h, double t, double dt,
 int adm_evolve_n_steps(adm_thermal *h, double t, double dt, int32_t n_steps,
                        double *solution, double *t_out)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(h && solution, "null argument");
     ADM_REQUIRE(n_steps >= 0, "n_steps must be non-negative");
     double const tn = as(h)->evolve_n_steps(t, dt, n_steps, solution);
@@ -213,7 +176,7 @@ int adm_evolve_n_steps(adm_thermal *h, double t, double dt, int32_t n_steps,
 int adm_evaluate_material_properties(adm_thermal *h, double const *temperature,
                                      double *property_values)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(h && temperature && property_values, "null argument");
     as(h)->evaluate_material_properties(temperature, property_values);
   });
@@ -221,7 +184,7 @@ int adm_evaluate_material_properties(adm_thermal *h, double const *temperature,
 
 int adm_set_state_to_material_properties(adm_thermal *h)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(h, "null handle");
     as(h)->set_state_to_material_properties();
   });
@@ -229,7 +192,7 @@ int adm_set_state_to_material_properties(adm_thermal *h)
 
 int adm_get_state_from_material_properties(adm_thermal *h)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(h, "null handle");
     as(h)->get_state_from_material_properties();
   });
@@ -237,7 +200,7 @@ int adm_get_state_from_material_properties(adm_thermal *h)
 
 int adm_get_cell_state(adm_thermal *h, double *state_host)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(h && state_host, "null argument");
     as(h)->get_cell_state(state_host);
   });
@@ -245,7 +208,7 @@ int adm_get_cell_state(adm_thermal *h, double *state_host)
 
 int adm_set_cell_state(adm_thermal *h, double const *state_host)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(h && state_host, "null argument");
     as(h)->set_cell_state(state_host);
   });
@@ -253,7 +216,7 @@ int adm_set_cell_state(adm_thermal *h, double const *state_host)
 
 int adm_get_qp_powder(adm_thermal *h, double *powder_host)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(h && powder_host, "null argument");
     as(h)->get_qp_powder(powder_host);
   });
@@ -262,7 +225,7 @@ int adm_get_qp_powder(adm_thermal *h, double *powder_host)
 int adm_mark_has_melted(adm_thermal *h, double threshold, double const *temperature,
                         uint8_t *has_melted_host)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(h && temperature, "null argument");
     as(h)->mark_has_melted(threshold, temperature, has_melted_host);
   });
@@ -272,7 +235,7 @@ int adm_activate_cells(adm_thermal *h, int64_t const *cells, int64_t n,
                        double new_temperature, double const *cos_new,
                        double const *sin_new, double *solution)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(h && solution && (n == 0 || cells), "null argument");
     ADM_REQUIRE(n >= 0, "negative cell count");
     as(h)->activate_cells(cells, n, new_temperature, cos_new, sin_new, solution);
@@ -281,7 +244,7 @@ int adm_activate_cells(adm_thermal *h, int64_t const *cells, int64_t n,
 
 int adm_update_beam(adm_thermal *h, int32_t i, adm_source const *beam)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(h && beam, "null argument");
     as(h)->update_beam(i, *beam);
   });
@@ -289,7 +252,7 @@ int adm_update_beam(adm_thermal *h, int32_t i, adm_source const *beam)
 
 int adm_device_error(adm_thermal *h, int32_t *code)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(h && code, "null argument");
     *code = as(h)->device_error();
   });
@@ -297,7 +260,7 @@ int adm_device_error(adm_thermal *h, int32_t *code)
 
 int adm_synchronize(adm_thermal *h)
 {
-  return guard([&] {
+  return adm::guard([&] {
     ADM_REQUIRE(h, "null handle");
     as(h)->synchronize();
   });

@@ -370,7 +370,7 @@ Thermal::Tableau Thermal::tableau(int method)
 }
 
 // ------------------------------------------------------------ Thermal
-Thermal::Thermal(adm_config const &cfg, int device, cudaStream_t stream)
+Thermal::Thermal(adm_config const &cfg, int device, cudaStream_t stream, bool own_stage_vectors)
 {
   check_config(cfg);
   cfg_ = cfg;
@@ -398,14 +398,25 @@ Thermal::Thermal(adm_config const &cfg, int device, cudaStream_t stream)
 
   size_t const N = mesh_.n_nodes, C = mesh_.n_cells;
   int const NN = (mesh_.deg + 1) * (mesh_.deg + 1) * (mesh_.deg + 1);
-  za_.alloc(N);
-  zb_.alloc(N);
-  acc_.alloc(N);
   inv_mass_.alloc(N);
-  if (tab_.s > 1)
-    s_.alloc(N);
-  if (cfg_.time_method == 2)
-    f0_.alloc(N);
+  if (own_stage_vectors)
+  {
+    za_.alloc(N);
+    zb_.alloc(N);
+    acc_.alloc(N);
+    if (tab_.s > 1)
+      s_.alloc(N);
+    if (cfg_.time_method == 2)
+      f0_.alloc(N);
+    za_p_ = za_.p;
+    zb_p_ = zb_.p;
+    acc_p_ = acc_.p;
+    s_p_ = s_.p;
+    f0_p_ = f0_.p;
+    ADM_CK(cudaMemset(acc_.p, 0, N * sizeof(double)));
+    ADM_CK(cudaMemset(za_.p, 0, N * sizeof(double)));
+    ADM_CK(cudaMemset(zb_.p, 0, N * sizeof(double)));
+  }
   if (ns_ > 1)
     liquid_sum_.alloc(C);
   if (ns_ == 3)
@@ -447,9 +458,6 @@ Thermal::Thermal(adm_config const &cfg, int device, cudaStream_t stream)
   double const clk[2] = {0.0, 0.0};
   ADM_CK(cudaMemcpy(clock_.p, clk, sizeof(clk), cudaMemcpyHostToDevice));
   ADM_CK(cudaMemset(error_d_.p, 0, sizeof(int32_t)));
-  ADM_CK(cudaMemset(acc_.p, 0, N * sizeof(double)));
-  ADM_CK(cudaMemset(za_.p, 0, N * sizeof(double)));
-  ADM_CK(cudaMemset(zb_.p, 0, N * sizeof(double)));
   // defaults: every cell active, material 0, solid, no rotation
   set_cells(nullptr, nullptr, nullptr, nullptr, nullptr);
 }
@@ -564,11 +572,11 @@ void Thermal::upload_member()
   MemberData &md = md_;
   std::memset(&md, 0, sizeof(md));
   md.y = nullptr;
-  md.za = za_.p;
-  md.zb = zb_.p;
-  md.s = s_.p;
-  md.f0 = f0_.p;
-  md.acc = acc_.p;
+  md.za = za_p_;
+  md.zb = zb_p_;
+  md.s = s_p_;
+  md.f0 = f0_p_;
+  md.acc = acc_p_;
   md.inv_mass = inv_mass_.p;
   md.cell_info = cell_info_d_.p;
   md.powder_mode = powder_mode_.p;
@@ -757,18 +765,25 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
   return fn;
 }
 
-// Tensor map of a node vector for the TMA brick loads: a 3D box of
-// (BXP, BY, BZ) nodes over the (nn0, nn1, nn2) grid with row pitch `pitch`.
-CUtensorMap brick_map(Mesh const &m, double const *base)
+// Tensor map of node vectors for the TMA brick loads: a 4D box of
+// (BXP, BY, BZ, 1) nodes over the (nn0, nn1, nn2, members) array with row
+// pitch `pitch` and member_stride doubles between members.
+CUtensorMap brick_map(Mesh const &m, double const *base, int n_members, size_t member_stride)
 {
   CUtensorMap map;
   std::memset(&map, 0, sizeof(map));
   if ((reinterpret_cast<uintptr_t>(base) & 15u) != 0)
     throw Error(ADM_ERR_INVALID, "node vectors must be 16-byte aligned");
-  cuuint64_t const dims[3] = {(cuuint64_t)m.nn[0], (cuuint64_t)m.nn[1], (cuuint64_t)m.nn[2]};
-  cuuint64_t const strides[2] = {(cuuint64_t)m.pitch * sizeof(double),
-                                 (cuuint64_t)m.pitch * m.nn[1] * sizeof(double)};
-  cuuint32_t box[3];
+  if (n_members < 1 || (n_members > 1 && (member_stride * sizeof(double)) % 16 != 0) ||
+      member_stride < m.n_nodes)
+    throw Error(ADM_ERR_INVALID, "member stride must cover a node vector and be a multiple of 2 doubles");
+  cuuint64_t const dims[4] = {(cuuint64_t)m.nn[0], (cuuint64_t)m.nn[1], (cuuint64_t)m.nn[2],
+                              (cuuint64_t)n_members};
+  cuuint64_t const strides[3] = {(cuuint64_t)m.pitch * sizeof(double),
+                                 (cuuint64_t)m.pitch * m.nn[1] * sizeof(double),
+                                 (cuuint64_t)member_stride * sizeof(double)};
+  cuuint32_t box[4];
+  box[3] = 1;
   if (m.deg == 1)
   {
     box[0] = TD<1>::BXP;
@@ -781,8 +796,8 @@ CUtensorMap brick_map(Mesh const &m, double const *base)
     box[1] = TD<2>::BY;
     box[2] = TD<2>::BZ;
   }
-  cuuint32_t const elem[3] = {1, 1, 1};
-  CUresult const r = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(base), dims,
+  cuuint32_t const elem[4] = {1, 1, 1, 1};
+  CUresult const r = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double *>(base), dims,
                                  strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS)
@@ -792,7 +807,7 @@ CUtensorMap brick_map(Mesh const &m, double const *base)
 
 void Thermal::launch_pass(KernelArgs a, double const *src)
 {
-  CUtensorMap const map = brick_map(mesh_, src);
+  CUtensorMap const map = brick_map(mesh_, src, 1, mesh_.n_nodes);
   for (int col = 0; col < 8; ++col)
   {
     int const count = colour_off_[col + 1] - colour_off_[col];
@@ -802,6 +817,24 @@ void Thermal::launch_pass(KernelArgs a, double const *src)
     launch_tile(mesh_.deg, ns_, poly_p_, map, a, count, stream_);
     ADM_CK(cudaGetLastError());
   }
+}
+
+void launch_set_clock(MemberData *members, int n, double t, double dt, cudaStream_t stream)
+{
+  set_clock_kernel<<<(n + 31) / 32, 32, 0, stream>>>(members, n, t, dt);
+  ADM_CK(cudaGetLastError());
+}
+
+void launch_advance_clock(MemberData *members, int n, cudaStream_t stream)
+{
+  advance_clock_kernel<<<(n + 31) / 32, 32, 0, stream>>>(members, n);
+  ADM_CK(cudaGetLastError());
+}
+
+void launch_stage_prepare(MemberData *members, int n, double c, cudaStream_t stream)
+{
+  stage_prepare_kernel<<<n, 32, 0, stream>>>(members, n, c);
+  ADM_CK(cudaGetLastError());
 }
 
 void Thermal::set_clock(double t, double dt)
@@ -840,35 +873,43 @@ void Thermal::vmult(double *dst, double const *src, bool add)
   launch_pass(a, src);
 }
 
+// Kernel arguments of RK stage i: stage input y (i == 0) or the stage vector
+// the previous stage wrote; za/zb alternate as stage outputs.
+KernelArgs Thermal::stage_args(int i) const
+{
+  KernelArgs a = base_args();
+  a.mode = 2;
+  a.stage = i;
+  a.n_stages = tab_.s;
+  a.last = i == tab_.s - 1;
+  a.src_sel = i == 0 ? 0 : ((i & 1) ? 1 : 2);
+  a.dst_sel = (i & 1) ? 2 : 1;
+  a.c_stage = tab_.c[i];
+  a.b_i = tab_.b[i];
+  if (i + 1 < tab_.s)
+  {
+    a.a_next = tab_.a[i + 1][i];
+    if (i >= 1 && tab_.a[i + 1][0] != 0.0)
+    {
+      a.has_f0 = 1;
+      a.a_next_f0 = tab_.a[i + 1][0];
+    }
+  }
+  if (i == 0)
+    for (int k = 2; k < tab_.s; ++k)
+      if (tab_.a[k][0] != 0.0)
+        a.store_f0 = 1;
+  return a;
+}
+
 void Thermal::launch_step(double *solution)
 {
   for (int i = 0; i < tab_.s; ++i)
   {
     prepare_stage(tab_.c[i]);
-    KernelArgs a = base_args();
-    a.mode = 2;
-    a.stage = i;
-    a.n_stages = tab_.s;
-    a.last = i == tab_.s - 1;
-    a.src_sel = i == 0 ? 0 : ((i & 1) ? 1 : 2);
-    a.dst_sel = (i & 1) ? 2 : 1;
-    a.c_stage = tab_.c[i];
-    a.b_i = tab_.b[i];
-    if (i + 1 < tab_.s)
-    {
-      a.a_next = tab_.a[i + 1][i];
-      if (i >= 1 && tab_.a[i + 1][0] != 0.0)
-      {
-        a.has_f0 = 1;
-        a.a_next_f0 = tab_.a[i + 1][0];
-      }
-    }
-    if (i == 0)
-      for (int k = 2; k < tab_.s; ++k)
-        if (tab_.a[k][0] != 0.0)
-          a.store_f0 = 1;
+    KernelArgs a = stage_args(i);
     a.y_override = solution;
-    launch_pass(a, i == 0 ? solution : (a.src_sel == 1 ? za_.p : zb_.p));
+    launch_pass(a, i == 0 ? solution : (a.src_sel == 1 ? za_p_ : zb_p_));
   }
 }
 
@@ -1106,6 +1147,34 @@ void Thermal::update_beam(int i, adm_source const &beam)
   upload_member();
 }
 
+void Thermal::update_material(adm_config const &cfg)
+{
+  if (cfg.n_materials != cfg_.n_materials || cfg.n_states != cfg_.n_states ||
+      cfg.use_table != cfg_.use_table)
+    throw Error(ADM_ERR_INVALID, "update_material: the number of materials and states and the "
+                                 "table/polynomial choice must not change");
+  if (cfg.p_order < 0 || cfg.p_order > 4)
+    throw Error(ADM_ERR_INVALID, "p_order must be in [0, 4]");
+  ADM_CK(cudaSetDevice(device_));
+  cfg_.p_order = cfg.p_order;
+  std::memcpy(cfg_.poly, cfg.poly, sizeof(cfg_.poly));
+  std::memcpy(cfg_.table, cfg.table, sizeof(cfg_.table));
+  std::memcpy(cfg_.props, cfg.props, sizeof(cfg_.props));
+  MaterialDesc const m = make_material(cfg_);
+  ADM_CK(cudaMemcpyAsync(mat_d_.p, &m, sizeof(m), cudaMemcpyHostToDevice, stream_));
+  ADM_CK(cudaStreamSynchronize(stream_));
+  int pmax = 0;
+  for (int p : {(int)P_DENSITY, (int)P_SPECIFIC_HEAT, (int)P_KX, (int)P_KY, (int)P_KZ})
+    pmax = std::max(pmax, m.prop_deg[p]);
+  int const p_new = pmax <= 2 ? 2 : 4;
+  if (p_new != poly_p_ && step_graph_)
+  {
+    cudaGraphExecDestroy(step_graph_);
+    step_graph_ = nullptr;
+  }
+  poly_p_ = p_new;
+}
+
 int32_t Thermal::device_error()
 {
   int32_t e = 0;
@@ -1115,6 +1184,21 @@ int32_t Thermal::device_error()
 }
 
 void Thermal::synchronize() { ADM_CK(cudaStreamSynchronize(stream_)); }
+
+void Thermal::bind_stage_vectors(double *za, double *zb, double *s, double *f0, double *acc)
+{
+  za_p_ = za;
+  zb_p_ = zb;
+  s_p_ = s;
+  f0_p_ = f0;
+  acc_p_ = acc;
+  if (step_graph_)
+  {
+    cudaGraphExecDestroy(step_graph_);
+    step_graph_ = nullptr;
+  }
+  upload_member();
+}
 
 void Thermal::vmult_host(double *dst_host, double const *src_host)
 {

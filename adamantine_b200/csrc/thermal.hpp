@@ -13,6 +13,7 @@
 #include "../../include/adamantine_b200.h"
 #include "device_types.cuh"
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -113,10 +114,28 @@ struct CellTopology
 CellTopology build_topology(Mesh const &mesh, std::vector<uint8_t> const &active,
                             std::vector<uint8_t> const &matid, bool need_slots);
 
+// Tensor map of n_members node vectors laid out member after member,
+// member_stride doubles apart (1 member: one vector), for the 4D TMA brick
+// loads of the tile kernel.
+CUtensorMap brick_map(Mesh const &m, double const *base, int n_members, size_t member_stride);
+// Tile kernel launch for one colour's work list.
+void launch_tile(int deg, int ns, int p, CUtensorMap const &map, KernelArgs const &a, int n_items,
+                 cudaStream_t stream);
+
+// Per-member clock and heat-source-state kernels over a member table.
+void launch_set_clock(MemberData *members, int n, double t, double dt, cudaStream_t stream);
+void launch_advance_clock(MemberData *members, int n, cudaStream_t stream);
+void launch_stage_prepare(MemberData *members, int n, double c, cudaStream_t stream);
+
+class Ensemble;
+
 class Thermal
 {
 public:
-  Thermal(adm_config const &cfg, int device, cudaStream_t stream);
+  // own_stage_vectors = false: the RK stage vectors and partial sums are
+  // supplied by bind_stage_vectors (the ensemble keeps all members' vectors
+  // in shared arrays).
+  Thermal(adm_config const &cfg, int device, cudaStream_t stream, bool own_stage_vectors = true);
   ~Thermal();
   Thermal(Thermal const &) = delete;
   Thermal &operator=(Thermal const &) = delete;
@@ -149,6 +168,9 @@ public:
   void activate_cells(int64_t const *cells, int64_t n, double new_temperature,
                       double const *cos_new, double const *sin_new, double *solution);
   void update_beam(int i, adm_source const &beam);
+  // new material tables of the same shape (ensemble analysis of a
+  // material parameter); no counterpart in the reference
+  void update_material(adm_config const &cfg);
   // host-buffer variants through persistent device staging vectors
   void vmult_host(double *dst_host, double const *src_host);
   double evolve_one_time_step_host(double t, double dt, double *solution_host);
@@ -156,6 +178,7 @@ public:
   cudaStream_t stream() const { return stream_; }
   int device() const { return device_; }
   void synchronize();
+  void bind_stage_vectors(double *za, double *zb, double *s, double *f0, double *acc);
 
   // stage schedule (Butcher tableau of the configured method)
   struct Tableau
@@ -166,9 +189,11 @@ public:
   static Tableau tableau(int method);
 
 private:
+  friend class Ensemble;
   void rebuild();
   void upload_member();
   KernelArgs base_args() const;
+  KernelArgs stage_args(int i) const;
   void launch_pass(KernelArgs args, double const *src);
   void launch_step(double *solution);
   void prepare_stage(double c);
@@ -196,6 +221,8 @@ private:
   int colour_off_[9] = {0};
 
   DevBuf<double> za_, zb_, s_, f0_, acc_, inv_mass_;
+  // the stage vectors in use: za_ .. acc_ or the bound external ones
+  double *za_p_ = nullptr, *zb_p_ = nullptr, *s_p_ = nullptr, *f0_p_ = nullptr, *acc_p_ = nullptr;
   DevBuf<double> stage_in_, stage_out_;
   DevBuf<double> powder_cell_, powder_q_, liquid_sum_, face_powder_;
   DevBuf<double> cos_d_, sin_d_, state_d_, clock_, segs_;

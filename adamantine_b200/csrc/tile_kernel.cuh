@@ -106,13 +106,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
                : "memory");
   return ok != 0;
 }
-// 3D tiled TMA load of one node brick (no multicast).
+// 4D tiled TMA load of one node brick of member m (no multicast).
 __device__ __forceinline__ void tma_load_brick(void *dst, CUtensorMap const *map, int x, int y, int z,
-                                               uint64_t *bar)
+                                               int m, uint64_t *bar)
 {
-  asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-               " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(dst)),
-               "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+  asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+               " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_addr(dst)),
+               "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(m), "r"(smem_addr(bar))
                : "memory");
 }
 // Bounded wait on an mbarrier phase: false after ~kSpinLimit polls (the
@@ -427,11 +427,12 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
   int const pitch = args.pitch, nn1 = args.nn[1];
 
   auto issue = [&](int buf, int item) {
-    int const tile = args.work[item].tile;
+    TileWork const wi = args.work[item];
+    int const tile = wi.tile;
     int const tix = tile % nt0, tiy = (tile / nt0) % nt1, tiz = tile / (nt0 * nt1);
     mbar_arrive_expect_tx(&bars[buf], kBoxBytes);
     tma_load_brick(smem + buf * T_::BRICKP, &tmap, DEG * TX * tix, DEG * TY * tiy, DEG * TZ * tiz,
-                   &bars[buf]);
+                   wi.member, &bars[buf]);
   };
 
   if (tid == 0)

@@ -139,3 +139,53 @@ def initial_temperature(cfg: ThermalConfig, name: str, melt_pool: bool = True) -
         r2 = ((xs[None, None, :] - cx) ** 2 + (ys[None, :, None] - cy) ** 2 + (zs[:, None, None] - cz) ** 2)
         T += 1700.0 * np.exp(-r2 / (0.4e-3) ** 2)
     return T
+
+
+def ensemble_q1(n_members=32, n_cells=(64, 64, 32), extent=(20e-3, 20e-3, 10e-3), min_layers=20,
+                max_layers=32, powder_layers=4, method="rk_fourth_order", name="ensemble_q1"):
+    """Batched EnKF ensemble: n_members problems on one 64x64x32 Q1 mesh
+    (20x20x10 mm, Gauss 2) with the phase-change material of phase_change_q2.
+
+    Per member (seeded): conductivity scale and absorptivity factor drawn
+    from log-normal(0, 0.1) (absorptivity = 0.35 x factor), and a deposited
+    height of min_layers..max_layers cell layers (uniform), the top
+    powder_layers of it powder, so the active cell counts differ. Goldak
+    400 W with R = 250 um, d = 300 um (resolved by the 312.5 um cells) on the
+    seeded serpentine at the member's top surface; adiabatic; RK4.
+
+    Returns (configs, params) with params[k] = (k_scale, absorptivity,
+    n_layers).
+    """
+    rng = rng_for(name + "-params")
+    k_scale = np.exp(rng.normal(0.0, 0.1, n_members))
+    absorb = 0.35 * np.exp(rng.normal(0.0, 0.1, n_members))
+    layers = rng.integers(min_layers, max_layers + 1, n_members)
+    seg_rng_state = rng_for(name + "-scan")
+    hz = extent[2] / n_cells[2]
+    base_seg = serpentine_segments(seg_rng_state, 0.25 * extent[0], 0.75 * extent[0], 0.45 * extent[1], 0.0, 10,
+                                   200e-6, 1.0)
+    bnd = Boundary.from_database({"type": "adiabatic"}, 3)
+    configs, params = [], []
+    for k in range(n_members):
+        top = layers[k] * hz
+        geo = Geometry(dim=3, n_cells=n_cells, extent=extent, material_height=top, use_powder=True,
+                       powder_layer=powder_layers * hz)
+        seg = base_seg.copy()
+        seg[:, 4] = top
+        src = Source(type="goldak", depth=300e-6, absorption_efficiency=float(absorb[k]), diameter=500e-6,
+                     max_power=400.0, segments=seg)
+        mat = phase_change_material(k_scale=float(k_scale[k]))
+        configs.append(ThermalConfig(geometry=geo, material=mat, boundary=bnd, sources=[src], degree=1,
+                                     time_method=method))
+        params.append((float(k_scale[k]), float(absorb[k]), int(layers[k])))
+    return configs, params
+
+
+def surface_observations(n_nodes_xy, layers, n_obs=2000, sigma=5.0, name="ensemble_q1-obs"):
+    """2000 seeded observation points on the top surface: distinct (i, j)
+    node columns, and for each member the node index (i, j, layers[k]) of
+    its own top surface (Q1). Returns (ij, sigma)."""
+    rng = rng_for(name)
+    nx, ny = n_nodes_xy
+    flat = rng.choice(nx * ny, size=n_obs, replace=False)
+    return np.stack([flat % nx, flat // nx], axis=1), sigma

@@ -1,0 +1,108 @@
+/*
+ * adamantine_b200 -- batched ensemble and EnKF analysis (C ABI).
+ *
+ * The reference runs its data-assimilation ensemble as a loop over
+ * independent ThermalPhysics objects (application/adamantine.hh:2137-2142)
+ * and updates it with DataAssimilator::update_ensemble
+ * (source/DataAssimilator.cc:95-189). Here all members of an ensemble advance
+ * together in one launch per colour and stage, and the analysis runs on the
+ * GPU in FP64. Conventions are those of adamantine_b200.h (status codes,
+ * adm_last_error, one stream per handle, device pointers).
+ *
+ * Ensemble vectors: member k's node vector (same layout as adm_n_nodes /
+ * adm_node_layout of a single problem) starts at solutions + k * stride
+ * (adm_ensemble_stride, in doubles); the array must be 16-byte aligned.
+ */
+#ifndef ADAMANTINE_B200_ENSEMBLE_H
+#define ADAMANTINE_B200_ENSEMBLE_H
+
+#include "adamantine_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct adm_ensemble adm_ensemble;
+typedef struct adm_enkf adm_enkf;
+
+/* create_database_ensemble + one ThermalPhysics per member
+ * (source/ensemble_management.cc:213-277, application/adamantine.hh:1663-1730).
+ * cfgs: n_members configurations that agree on the mesh, element, quadrature,
+ * material states, table/polynomial choice, boundary types, time method and
+ * source kinds; material and source values may differ per member. */
+int adm_ensemble_create(adm_config const *cfgs, int32_t n_members, int device, void *stream,
+                        adm_ensemble **out);
+int adm_ensemble_destroy(adm_ensemble *e);
+/* adm_set_cells for member k (its own active cells, materials, states). */
+int adm_ensemble_set_cells(adm_ensemble *e, int32_t member, uint8_t const *active,
+                           uint8_t const *material_id, uint8_t const *initial_state,
+                           double const *deposition_cos, double const *deposition_sin);
+/* adm_setup of every member, then the batched work list. */
+int adm_ensemble_setup(adm_ensemble *e);
+/* Doubles between consecutive members' vectors. */
+int adm_ensemble_stride(adm_ensemble const *e, int64_t *stride);
+/* Number of (member, tile) work items of one batched colour sweep. */
+int adm_ensemble_n_work_items(adm_ensemble const *e, int64_t *n);
+
+/* ThermalPhysicsInterface::evolve_one_time_step (source/ThermalPhysics.templates.hh:854-888)
+ * for every member: one launch per colour and stage over all members. */
+int adm_ensemble_evolve_one_time_step(adm_ensemble *e, double t, double dt, double *solutions,
+                                      double *t_out);
+/* The same step as the reference's loop over members (each member through
+ * its own single-problem launches); the batched step's baseline. */
+int adm_ensemble_evolve_looped(adm_ensemble *e, double t, double dt, double *solutions,
+                               double *t_out);
+/* n_steps batched steps replayed from one captured CUDA graph. */
+int adm_ensemble_evolve_n_steps(adm_ensemble *e, double t, double dt, int32_t n_steps,
+                                double *solutions, double *t_out);
+
+/* ThermalPhysics::update_physics_parameters (source/ThermalPhysics.templates.hh:827-852)
+ * for member k: new depth, efficiency, radius and power of source i. */
+int adm_ensemble_update_beam(adm_ensemble *e, int32_t member, int32_t i, adm_source const *beam);
+/* New material tables for member k (same shape as at creation); no
+ * counterpart in the reference, which augments only beam parameters. */
+int adm_ensemble_update_material(adm_ensemble *e, int32_t member, adm_config const *cfg);
+/* MaterialProperty::get_state of member k: [n_states][n_cells], host. */
+int adm_ensemble_get_cell_state(adm_ensemble *e, int32_t member, double *state_host);
+/* Inverse lumped mass of member k into a device vector. */
+int adm_ensemble_get_inverse_mass_matrix(adm_ensemble *e, int32_t member, double *dst);
+/* First non-zero sticky device error word over the members (synchronizes). */
+int adm_ensemble_device_error(adm_ensemble *e, int32_t *code);
+int adm_ensemble_synchronize(adm_ensemble *e);
+
+/* Analysis workspace on a device and stream (NULL: default stream). */
+int adm_enkf_create(int device, void *stream, adm_enkf **out);
+int adm_enkf_destroy(adm_enkf *e);
+/* DataAssimilator::update_ensemble (source/DataAssimilator.cc:95-189) with
+ * localization "none" (every state entry correlates with every observation),
+ * in FP64 on the device, dense Cholesky of H P H^T + R instead of GMRES:
+ *   x_k += P H^T (H P H^T + R)^-1 (obs + perturbations_k - H_k x_k)
+ * for the augmented states [x_k; p_k], P their sample covariance (divided
+ * by N - 1). All arrays are device memory:
+ *   states        N vectors, member k at states + k * stride, n_state entries
+ *                 each (updated in place)
+ *   params        [N][n_params] augmented parameters (updated; may be NULL
+ *                 when n_params == 0)
+ *   obs_index     [N][n_obs] state index of observation j for member k
+ *                 (calc_Hx with a member-specific map: ragged members see
+ *                 the same point at different nodes)
+ *   obs           [n_obs] observed values
+ *   obs_var       [n_obs] diagonal of R, or NULL when obs_cov is given
+ *   obs_cov       [n_obs][n_obs] dense R (row-major), or NULL
+ *   perturbations [N][n_obs] the draws e_k ~ N(0, R) of fill_noise_vector
+ *                 (:630-670), supplied by the caller
+ *   update_mask   [N][n_state] 1 where member k's entry is updated, or NULL
+ * 2 <= N <= 64, 1 <= n_obs <= 16384. Synchronizes. Nothing is updated
+ * when H P H^T + R is not positive definite (ADM_ERR_DEVICE) or an index is
+ * outside [0, n_state) (ADM_ERR_INVALID). */
+int adm_enkf_analysis(adm_enkf *e, int32_t n_members, double *states, int64_t stride,
+                      int64_t n_state, double *params, int32_t n_params, int32_t n_obs,
+                      int64_t const *obs_index, double const *obs, double const *obs_var,
+                      double const *obs_cov, double const *perturbations,
+                      uint8_t const *update_mask);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

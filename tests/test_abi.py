@@ -13,22 +13,26 @@ from adamantine_b200.config import ConfigStruct, SourceStruct
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def header_functions():
-    text = open(os.path.join(ROOT, "include", "adamantine_b200.h")).read()
+def header_functions(header="adamantine_b200.h"):
+    text = open(os.path.join(ROOT, "include", header)).read()
     return sorted(set(re.findall(r"\b(adm_[a-z0-9_]+)\s*\(", text)))
+
+
+def all_headers():
+    return sorted(f for f in os.listdir(os.path.join(ROOT, "include")) if f.endswith(".h"))
 
 
 def test_library_exports_every_declared_symbol():
     L = _lib.load()
-    names = header_functions()
-    assert len(names) >= 25
+    names = [n for h in all_headers() for n in header_functions(h)]
+    assert len(names) >= 27
     missing = [n for n in names if not hasattr(L, n)]
     assert not missing, missing
 
 
 def test_python_binding_covers_header():
-    names = set(header_functions()) - {"adm_last_error"}
-    assert names == set(_lib.SIGNATURES)
+    names = set(header_functions()) | set(header_functions("adamantine_b200_ensemble.h"))
+    assert names - {"adm_last_error"} == set(_lib.SIGNATURES)
 
 
 def test_config_layout_matches_oracle_header():
