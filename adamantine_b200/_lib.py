@@ -47,6 +47,7 @@ SIGNATURES = {
     "adm_activate_cells": [_VP, _I64, ctypes.c_int64, ctypes.c_double, _D, _D, _VP],
     "adm_update_beam": [_VP, ctypes.c_int32, ctypes.POINTER(SourceStruct)],
     "adm_vmult_host_static": [_VP, _D, _D],
+    "adm_update_material": [_VP, ctypes.POINTER(ConfigStruct)],
     "adm_device_error": [_VP, _I32],
     "adm_synchronize": [_VP],
     # include/adamantine_b200_ensemble.h
@@ -67,6 +68,14 @@ SIGNATURES = {
     "adm_ensemble_synchronize": [_VP],
     "adm_enkf_create": [ctypes.c_int, _VP, ctypes.POINTER(_VP)],
     "adm_enkf_destroy": [_VP],
+    # include/adamantine_b200_adjoint.h
+    "adm_adjoint_create": [_VP, ctypes.POINTER(_VP)],
+    "adm_adjoint_destroy": [_VP],
+    "adm_adjoint_set_observations": [_VP, ctypes.c_int32, _I32, ctypes.c_int32, _I64, _D],
+    "adm_adjoint_objective": [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_int32, _VP, _D, _VP],
+    "adm_adjoint_gradient": [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_int32, _VP, _D, _D,
+                             _VP],
+    "adm_adjoint_vmult_transpose": [_VP, _VP, _VP, _VP, _D],
     "adm_enkf_analysis": [_VP, ctypes.c_int32, _VP, ctypes.c_int64, ctypes.c_int64, _VP, ctypes.c_int32,
                           ctypes.c_int32, _VP, _VP, _VP, _VP, _VP, _VP],
 }

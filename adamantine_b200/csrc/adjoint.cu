@@ -1,0 +1,557 @@
+// Hand-written adjoint of the explicit time step (no counterpart in the
+// reference, which only runs the forward problem).
+//
+// Objective: J = sum over observation steps n and points p of
+// (T_n[node_p] - target_{n,p})^2, T_n the temperature after n steps of the
+// configured explicit Runge-Kutta method (source/ThermalPhysics.templates.hh:854-888).
+// The gradient with respect to the logarithms of the conductivity scale, the
+// specific-heat scale and the source strength comes from the discrete
+// adjoint of the forward stages, including the phase history
+// s' = min(1 - l(T), s) of every Gauss point:
+//   forward stage i: Y_i = y + dt sum_j a_ij k_j,  (k_i, s_{i+1}) = (M^-1 r(Y_i, s_i), s'(Y_i, s_i))
+//   step:            y_new = y + dt sum_i b_i k_i
+//   adjoint, i = s-1 .. 0:
+//     lambda_k_i = dt b_i lambda_y_new + sum_{l > i} dt a_li lambda_Y_l
+//     (lambda_Y_i, lambda_s_i) = transpose of stage i applied to (M^-1 lambda_k_i, lambda_s_{i+1})
+//   lambda_y = lambda_y_new + sum_i lambda_Y_i
+// The forward states are checkpointed every K steps (temperature and the
+// sparse powder history) and each K-step segment is recomputed, stage by
+// stage, right before its backward sweep.
+#include "adjoint_kernel.cuh"
+#include "capi_common.hpp"
+#include "../../include/adamantine_b200_adjoint.h"
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+namespace adm
+{
+namespace
+{
+template <int DEG, int NS>
+void launch_adj(AdjArgs const &a, int n_items, cudaStream_t stream)
+{
+  using T_ = TD<DEG>;
+  size_t const smem = sizeof(double) * (2 * T_::BRICKP + 4 * T_::NN * T_::NCELL);
+  static bool attr = false;
+  if (!attr)
+  {
+    ADM_CK(cudaFuncSetAttribute(adjoint_kernel<DEG, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr = true;
+  }
+  adjoint_kernel<DEG, NS><<<n_items, T_::NT, smem, stream>>>(a);
+}
+
+void launch_adjoint(int deg, int ns, AdjArgs const &a, int n_items, cudaStream_t stream)
+{
+  switch (deg * 10 + ns)
+  {
+  case 11:
+    launch_adj<1, 1>(a, n_items, stream);
+    break;
+  case 12:
+    launch_adj<1, 2>(a, n_items, stream);
+    break;
+  case 13:
+    launch_adj<1, 3>(a, n_items, stream);
+    break;
+  case 21:
+    launch_adj<2, 1>(a, n_items, stream);
+    break;
+  case 22:
+    launch_adj<2, 2>(a, n_items, stream);
+    break;
+  case 23:
+    launch_adj<2, 3>(a, n_items, stream);
+    break;
+  default:
+    throw Error(ADM_ERR_INVALID, "no adjoint kernel for this degree / state count");
+  }
+}
+
+// resid[p] = y[idx[p]] - target[p]; *J += sum_p resid[p]^2 (one block, fixed
+// summation order).
+__global__ void misfit_kernel(double const *y, int64_t const *idx, double const *target, int n, double *resid,
+                              double *J)
+{
+  __shared__ double part[256];
+  double s = 0.0;
+  for (int p = threadIdx.x; p < n; p += blockDim.x)
+  {
+    double const r = y[idx[p]] - target[p];
+    resid[p] = r;
+    s += r * r;
+  }
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1)
+  {
+    if ((int)threadIdx.x < o)
+      part[threadIdx.x] += part[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    *J += part[0];
+}
+
+// lambda[idx[p]] += 2 resid[p] (points may repeat a node)
+__global__ void inject_kernel(double *lam, int64_t const *idx, double const *resid, int n)
+{
+  int const p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n)
+    atomicAdd(&lam[idx[p]], 2.0 * resid[p]);
+}
+
+struct LamTerms
+{
+  double const *v[4];
+  double c[4];
+  int n;
+};
+
+// mu = inv_mass * (cb * lam_new + sum_l c_l lam_Y_l)
+__global__ void lamk_kernel(double *mu, double const *inv_mass, double const *lam_new, double cb, LamTerms t,
+                            size_t n)
+{
+  size_t const i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  double s = cb * lam_new[i];
+  for (int l = 0; l < t.n; ++l)
+    s = fma(t.c[l], t.v[l][i], s);
+  mu[i] = inv_mass[i] * s;
+}
+
+// lam += sum_l lam_Y_l
+__global__ void sum_kernel(double *lam, LamTerms t, size_t n)
+{
+  size_t const i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  double s = lam[i];
+  for (int l = 0; l < t.n; ++l)
+    s += t.v[l][i];
+  lam[i] = s;
+}
+
+unsigned blocks(size_t n) { return (unsigned)((n + 255) / 256); }
+} // namespace
+
+class Adjoint
+{
+public:
+  explicit Adjoint(Thermal &t) : th_(t)
+  {
+    if (t.cfg_.use_table)
+      throw Error(ADM_ERR_UNSUPPORTED, "the adjoint supports polynomial material properties only");
+    if (t.has_rotation_)
+      throw Error(ADM_ERR_UNSUPPORTED, "the adjoint does not support deposition-angle rotation");
+    if (!t.adiabatic_only_)
+      throw Error(ADM_ERR_UNSUPPORTED, "the adjoint supports adiabatic boundaries only");
+    if (!t.setup_done_)
+      throw Error(ADM_ERR_INVALID, "setup() has not been called");
+    ADM_CK(cudaSetDevice(t.device_));
+    C_ = t.mesh_.n_cells;
+    NN_ = (t.mesh_.deg + 1) * (t.mesh_.deg + 1) * (t.mesh_.deg + 1);
+    n_ = t.mesh_.n_nodes;
+    save_phase(init_mode_, init_cell_, init_q_);
+  }
+
+  void set_observations(int n_obs_steps, int32_t const *steps, int n_points, int64_t const *index,
+                        double const *targets)
+  {
+    if (n_obs_steps < 0 || n_points < 0 || (n_obs_steps > 0 && (!steps || !targets)) ||
+        (n_points > 0 && !index))
+      throw Error(ADM_ERR_INVALID, "invalid observation arguments");
+    for (int p = 0; p < n_points; ++p)
+      if (index[p] < 0 || (size_t)index[p] >= n_)
+        throw Error(ADM_ERR_INVALID, "observation node index out of range");
+    obs_steps_.assign(steps, steps + n_obs_steps);
+    n_points_ = n_points;
+    idx_.alloc(std::max(1, n_points));
+    tgt_.alloc(std::max<size_t>(1, (size_t)n_obs_steps * n_points));
+    resid_.alloc(std::max<size_t>(1, (size_t)n_obs_steps * n_points));
+    Jd_.alloc(1);
+    if (n_points > 0)
+      ADM_CK(cudaMemcpy(idx_.p, index, n_points * sizeof(int64_t), cudaMemcpyHostToDevice));
+    if (n_obs_steps > 0 && n_points > 0)
+      ADM_CK(cudaMemcpy(tgt_.p, targets, (size_t)n_obs_steps * n_points * sizeof(double),
+                        cudaMemcpyHostToDevice));
+  }
+
+  // Forward run from the captured initial phase state: J and the final field.
+  double objective(double t0, double dt, int n_steps, double const *y0, double *y_final)
+  {
+    check_run(n_steps, 1);
+    forward(t0, dt, n_steps, y0, 0);
+    double J = 0.0;
+    ADM_CK(cudaMemcpyAsync(&J, Jd_.p, sizeof(double), cudaMemcpyDeviceToHost, th_.stream_));
+    if (y_final)
+      ADM_CK(cudaMemcpyAsync(y_final, y_.p, n_ * sizeof(double), cudaMemcpyDeviceToDevice, th_.stream_));
+    ADM_CK(cudaStreamSynchronize(th_.stream_));
+    return J;
+  }
+
+  double gradient(double t0, double dt, int n_steps, int K, double const *y0, double *grad, double *y_final)
+  {
+    check_run(n_steps, K);
+    Thermal &t = th_;
+    cudaStream_t const st = t.stream_;
+    int const S = t.tab_.s;
+    forward(t0, dt, n_steps, y0, K);
+    double J = 0.0;
+    ADM_CK(cudaMemcpyAsync(&J, Jd_.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (y_final)
+      ADM_CK(cudaMemcpyAsync(y_final, y_.p, n_ * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    // final phase state of the forward run, restored at the end
+    save_phase(fin_mode_, fin_cell_, fin_q_);
+
+    bool const ns3 = t.ns_ == 3;
+    size_t const qn = C_ * NN_;
+    lam_.alloc(n_);
+    mu_.alloc(n_);
+    lamY_.alloc(n_ * S);
+    ADM_CK(cudaMemsetAsync(lam_.p, 0, n_ * sizeof(double), st));
+    if (ns3)
+    {
+      ls_a_.alloc(qn);
+      ls_b_.alloc(qn);
+      ADM_CK(cudaMemsetAsync(ls_a_.p, 0, qn * sizeof(double), st));
+      ADM_CK(cudaMemsetAsync(ls_b_.p, 0, qn * sizeof(double), st));
+    }
+    grad_d_.alloc(3);
+    ADM_CK(cudaMemsetAsync(grad_d_.p, 0, 3 * sizeof(double), st));
+    // per step of a segment: the S stage inputs and (3 states) S phase states
+    Ystore_.alloc((size_t)K * S * n_);
+    if (ns3)
+      Sstore_.alloc((size_t)K * S * qn);
+    int const n_seg = (n_steps + K - 1) / K;
+    for (int seg = n_seg - 1; seg >= 0; --seg)
+    {
+      int const n0 = seg * K, n1 = std::min(n_steps, n0 + K);
+      // recompute the segment from its checkpoint, recording the stages
+      ADM_CK(cudaMemcpyAsync(y_.p, ck_y_.p + (size_t)seg * n_, n_ * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      if (ns3)
+        restore_phase(seg);
+      for (int n = n0; n < n1; ++n)
+      {
+        t.set_clock(times_[n], dt);
+        for (int i = 0; i < S; ++i)
+        {
+          t.prepare_stage(t.tab_.c[i]);
+          KernelArgs a = t.stage_args(i);
+          a.y_override = y_.p;
+          double const *src = i == 0 ? y_.p : (a.src_sel == 1 ? t.za_p_ : t.zb_p_);
+          size_t const slot = (size_t)(n - n0) * S + i;
+          ADM_CK(cudaMemcpyAsync(Ystore_.p + slot * n_, src, n_ * sizeof(double), cudaMemcpyDeviceToDevice, st));
+          if (ns3)
+            launch_expand_powder(t.cell_info_d_.p, NN_, t.powder_mode_.p, t.powder_cell_.p, t.powder_q_.p,
+                                 Sstore_.p + slot * qn, C_, st);
+          t.launch_pass(a, src);
+        }
+      }
+      // backward sweep over the segment
+      for (int n = n1 - 1; n >= n0; --n)
+      {
+        inject(n + 1);
+        t.set_clock(times_[n], dt);
+        for (int i = S - 1; i >= 0; --i)
+        {
+          LamTerms lt{};
+          lt.n = 0;
+          for (int l = i + 1; l < S; ++l)
+            if (t.tab_.a[l][i] != 0.0)
+            {
+              lt.v[lt.n] = lamY_.p + (size_t)l * n_;
+              lt.c[lt.n] = dt * t.tab_.a[l][i];
+              ++lt.n;
+            }
+          lamk_kernel<<<blocks(n_), 256, 0, st>>>(mu_.p, t.inv_mass_.p, lam_.p, dt * t.tab_.b[i], lt, n_);
+          ADM_CK(cudaGetLastError());
+          double *lamYi = lamY_.p + (size_t)i * n_;
+          ADM_CK(cudaMemsetAsync(lamYi, 0, n_ * sizeof(double), st));
+          t.prepare_stage(t.tab_.c[i]);
+          size_t const slot = (size_t)(n - n0) * S + i;
+          AdjArgs A;
+          std::memset(&A, 0, sizeof(A));
+          A.k = t.base_args();
+          A.yv = Ystore_.p + slot * n_;
+          A.mu = mu_.p;
+          if (ns3)
+          {
+            A.s_in = Sstore_.p + slot * qn;
+            A.lam_s_out = ls_a_.p;
+            A.lam_s_in = ls_b_.p;
+          }
+          A.lam_y = lamYi;
+          A.grad = grad_d_.p;
+          for (int col = 0; col < 8; ++col)
+          {
+            int const count = t.colour_off_[col + 1] - t.colour_off_[col];
+            if (count == 0)
+              continue;
+            A.k.work = t.work_d_.p + t.colour_off_[col];
+            launch_adjoint(t.mesh_.deg, t.ns_, A, count, st);
+            ADM_CK(cudaGetLastError());
+          }
+          if (ns3)
+            std::swap(ls_a_.p, ls_b_.p);
+        }
+        LamTerms all{};
+        all.n = S;
+        for (int i = 0; i < S; ++i)
+          all.v[i] = lamY_.p + (size_t)i * n_;
+        sum_kernel<<<blocks(n_), 256, 0, st>>>(lam_.p, all, n_);
+        ADM_CK(cudaGetLastError());
+      }
+    }
+    double g[3] = {0, 0, 0};
+    ADM_CK(cudaMemcpyAsync(g, grad_d_.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    // the handle ends with the phase state of the forward run
+    if (ns3)
+    {
+      ADM_CK(cudaMemcpyAsync(t.powder_mode_.p, fin_mode_.p, C_, cudaMemcpyDeviceToDevice, st));
+      ADM_CK(cudaMemcpyAsync(t.powder_cell_.p, fin_cell_.p, C_ * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      ADM_CK(cudaMemcpyAsync(t.powder_q_.p, fin_q_.p, qn * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    }
+    ADM_CK(cudaStreamSynchronize(st));
+    grad[0] = g[0];
+    grad[1] = g[1];
+    grad[2] = g[2];
+    grad[3] = g[2];
+    return J;
+  }
+
+  // lambda = (dr/dT)^T mu at the field y with the handle's current phase
+  // state held fixed (no powder-history chain): the transpose operator.
+  void vmult_transpose(double *lam, double const *y, double const *mu, double *grad)
+  {
+    Thermal &t = th_;
+    cudaStream_t const st = t.stream_;
+    ADM_CK(cudaSetDevice(t.device_));
+    bool const ns3 = t.ns_ == 3;
+    size_t const qn = C_ * NN_;
+    ADM_CK(cudaMemsetAsync(lam, 0, n_ * sizeof(double), st));
+    grad_d_.alloc(3);
+    ADM_CK(cudaMemsetAsync(grad_d_.p, 0, 3 * sizeof(double), st));
+    t.prepare_stage(0.0);
+    AdjArgs A;
+    std::memset(&A, 0, sizeof(A));
+    A.k = t.base_args();
+    A.yv = y;
+    A.mu = mu;
+    if (ns3)
+    {
+      ls_a_.alloc(qn);
+      ls_b_.alloc(qn);
+      Sstore_.alloc(qn);
+      ADM_CK(cudaMemsetAsync(ls_a_.p, 0, qn * sizeof(double), st));
+      launch_expand_powder(t.cell_info_d_.p, NN_, t.powder_mode_.p, t.powder_cell_.p, t.powder_q_.p, Sstore_.p,
+                           C_, st);
+      A.s_in = Sstore_.p;
+      A.lam_s_out = ls_a_.p;
+      A.lam_s_in = ls_b_.p;
+    }
+    A.lam_y = lam;
+    A.grad = grad_d_.p;
+    for (int col = 0; col < 8; ++col)
+    {
+      int const count = t.colour_off_[col + 1] - t.colour_off_[col];
+      if (count == 0)
+        continue;
+      A.k.work = t.work_d_.p + t.colour_off_[col];
+      launch_adjoint(t.mesh_.deg, t.ns_, A, count, st);
+      ADM_CK(cudaGetLastError());
+    }
+    double g[3];
+    ADM_CK(cudaMemcpyAsync(g, grad_d_.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    ADM_CK(cudaStreamSynchronize(st));
+    if (grad)
+      for (int k = 0; k < 3; ++k)
+        grad[k] = g[k];
+  }
+
+private:
+  void check_run(int n_steps, int K)
+  {
+    if (n_steps < 1)
+      throw Error(ADM_ERR_INVALID, "n_steps must be positive");
+    if (K < 1)
+      throw Error(ADM_ERR_INVALID, "checkpoint interval must be positive");
+    for (int s : obs_steps_)
+      if (s < 0 || s > n_steps)
+        throw Error(ADM_ERR_INVALID, "observation step outside [0, n_steps]");
+    ADM_CK(cudaSetDevice(th_.device_));
+  }
+
+  void save_phase(DevBuf<uint8_t> &mode, DevBuf<double> &cell, DevBuf<double> &q)
+  {
+    Thermal &t = th_;
+    if (t.ns_ != 3)
+      return;
+    cudaStream_t const st = t.stream_;
+    mode.alloc(C_);
+    cell.alloc(C_);
+    q.alloc(C_ * NN_);
+    ADM_CK(cudaMemcpyAsync(mode.p, t.powder_mode_.p, C_, cudaMemcpyDeviceToDevice, st));
+    ADM_CK(cudaMemcpyAsync(cell.p, t.powder_cell_.p, C_ * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    ADM_CK(cudaMemcpyAsync(q.p, t.powder_q_.p, C_ * NN_ * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  }
+
+  void restore_phase(int seg)
+  {
+    Thermal &t = th_;
+    cudaStream_t const st = t.stream_;
+    ADM_CK(cudaMemcpyAsync(t.powder_mode_.p, ck_mode_.p + (size_t)seg * C_, C_, cudaMemcpyDeviceToDevice, st));
+    ADM_CK(cudaMemcpyAsync(t.powder_cell_.p, ck_cell_.p + (size_t)seg * C_, C_ * sizeof(double),
+                           cudaMemcpyDeviceToDevice, st));
+    ADM_CK(cudaMemcpyAsync(t.powder_q_.p, ck_q_.p + (size_t)seg * C_ * NN_, C_ * NN_ * sizeof(double),
+                           cudaMemcpyDeviceToDevice, st));
+  }
+
+  void checkpoint(int seg)
+  {
+    Thermal &t = th_;
+    cudaStream_t const st = t.stream_;
+    ADM_CK(cudaMemcpyAsync(ck_y_.p + (size_t)seg * n_, y_.p, n_ * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    if (t.ns_ == 3)
+    {
+      ADM_CK(cudaMemcpyAsync(ck_mode_.p + (size_t)seg * C_, t.powder_mode_.p, C_, cudaMemcpyDeviceToDevice, st));
+      ADM_CK(cudaMemcpyAsync(ck_cell_.p + (size_t)seg * C_, t.powder_cell_.p, C_ * sizeof(double),
+                             cudaMemcpyDeviceToDevice, st));
+      ADM_CK(cudaMemcpyAsync(ck_q_.p + (size_t)seg * C_ * NN_, t.powder_q_.p, C_ * NN_ * sizeof(double),
+                             cudaMemcpyDeviceToDevice, st));
+    }
+  }
+
+  void observe(int n)
+  {
+    for (size_t k = 0; k < obs_steps_.size(); ++k)
+      if (obs_steps_[k] == n && n_points_ > 0)
+      {
+        misfit_kernel<<<1, 256, 0, th_.stream_>>>(y_.p, idx_.p, tgt_.p + k * n_points_, n_points_,
+                                                  resid_.p + k * n_points_, Jd_.p);
+        ADM_CK(cudaGetLastError());
+      }
+  }
+
+  void inject(int n)
+  {
+    for (size_t k = 0; k < obs_steps_.size(); ++k)
+      if (obs_steps_[k] == n && n_points_ > 0)
+      {
+        inject_kernel<<<blocks(n_points_), 256, 0, th_.stream_>>>(lam_.p, idx_.p, resid_.p + k * n_points_,
+                                                                  n_points_);
+        ADM_CK(cudaGetLastError());
+      }
+  }
+
+  // Forward run from the initial phase state; K > 0 checkpoints every K steps.
+  void forward(double t0, double dt, int n_steps, double const *y0, int K)
+  {
+    Thermal &t = th_;
+    cudaStream_t const st = t.stream_;
+    if (obs_steps_.empty() && n_points_ == 0)
+      Jd_.alloc(1);
+    y_.alloc(n_);
+    ADM_CK(cudaMemcpyAsync(y_.p, y0, n_ * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    if (t.ns_ == 3)
+    {
+      ADM_CK(cudaMemcpyAsync(t.powder_mode_.p, init_mode_.p, C_, cudaMemcpyDeviceToDevice, st));
+      ADM_CK(cudaMemcpyAsync(t.powder_cell_.p, init_cell_.p, C_ * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      ADM_CK(cudaMemcpyAsync(t.powder_q_.p, init_q_.p, C_ * NN_ * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    }
+    ADM_CK(cudaMemsetAsync(Jd_.p, 0, sizeof(double), st));
+    if (K > 0)
+    {
+      int const n_seg = (n_steps + K - 1) / K;
+      ck_y_.alloc((size_t)n_seg * n_);
+      if (t.ns_ == 3)
+      {
+        ck_mode_.alloc((size_t)n_seg * C_);
+        ck_cell_.alloc((size_t)n_seg * C_);
+        ck_q_.alloc((size_t)n_seg * C_ * NN_);
+      }
+    }
+    times_.assign(n_steps + 1, 0.0);
+    double tt = t0;
+    observe(0);
+    for (int n = 0; n < n_steps; ++n)
+    {
+      if (K > 0 && n % K == 0)
+        checkpoint(n / K);
+      times_[n] = tt;
+      tt = t.evolve_one_time_step(tt, dt, y_.p);
+      observe(n + 1);
+    }
+    times_[n_steps] = tt;
+  }
+
+  Thermal &th_;
+  size_t C_ = 0, n_ = 0;
+  int NN_ = 0;
+  std::vector<int32_t> obs_steps_;
+  int n_points_ = 0;
+  std::vector<double> times_;
+  DevBuf<int64_t> idx_;
+  DevBuf<double> tgt_, resid_, Jd_, y_, lam_, mu_, lamY_, ls_a_, ls_b_, grad_d_, Ystore_, Sstore_;
+  DevBuf<double> ck_y_, ck_cell_, ck_q_, init_cell_, init_q_, fin_cell_, fin_q_;
+  DevBuf<uint8_t> ck_mode_, init_mode_, fin_mode_;
+};
+
+} // namespace adm
+
+extern "C" {
+
+int adm_adjoint_create(adm_thermal *h, adm_adjoint **out)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && out, "null argument");
+    *out = nullptr;
+    auto *a = new adm::Adjoint(*reinterpret_cast<adm::Thermal *>(h));
+    *out = reinterpret_cast<adm_adjoint *>(a);
+  });
+}
+
+int adm_adjoint_destroy(adm_adjoint *a)
+{
+  return adm::guard([&] { delete reinterpret_cast<adm::Adjoint *>(a); });
+}
+
+int adm_adjoint_set_observations(adm_adjoint *a, int32_t n_obs_steps, int32_t const *obs_steps,
+                                 int32_t n_points, int64_t const *node_index, double const *targets)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(a, "null handle");
+    reinterpret_cast<adm::Adjoint *>(a)->set_observations(n_obs_steps, obs_steps, n_points, node_index, targets);
+  });
+}
+
+int adm_adjoint_objective(adm_adjoint *a, double t0, double dt, int32_t n_steps, double const *y0, double *J,
+                          double *y_final)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(a && y0 && J, "null argument");
+    *J = reinterpret_cast<adm::Adjoint *>(a)->objective(t0, dt, n_steps, y0, y_final);
+  });
+}
+
+int adm_adjoint_gradient(adm_adjoint *a, double t0, double dt, int32_t n_steps, int32_t checkpoint_every,
+                         double const *y0, double *J, double *grad, double *y_final)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(a && y0 && J && grad, "null argument");
+    *J = reinterpret_cast<adm::Adjoint *>(a)->gradient(t0, dt, n_steps, checkpoint_every, y0, grad, y_final);
+  });
+}
+
+int adm_adjoint_vmult_transpose(adm_adjoint *a, double *dst, double const *y, double const *mu, double *grad)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(a && dst && y && mu, "null argument");
+    reinterpret_cast<adm::Adjoint *>(a)->vmult_transpose(dst, y, mu, grad);
+  });
+}
+
+} // extern "C"

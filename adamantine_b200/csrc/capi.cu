@@ -242,6 +242,14 @@ int adm_activate_cells(adm_thermal *h, int64_t const *cells, int64_t n,
   });
 }
 
+int adm_update_material(adm_thermal *h, adm_config const *cfg)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && cfg, "null argument");
+    as(h)->update_material(*cfg);
+  });
+}
+
 int adm_update_beam(adm_thermal *h, int32_t i, adm_source const *beam)
 {
   return adm::guard([&] {

@@ -837,6 +837,14 @@ void launch_stage_prepare(MemberData *members, int n, double c, cudaStream_t str
   ADM_CK(cudaGetLastError());
 }
 
+void launch_expand_powder(uint32_t const *cell_info, int NN, uint8_t const *pmode, double const *pcell,
+                          double const *pq, double *out, size_t C, cudaStream_t stream)
+{
+  expand_powder_kernel<<<(unsigned)((C * NN + 255) / 256), 256, 0, stream>>>(cell_info, NN, pmode, pcell, pq,
+                                                                            out, C);
+  ADM_CK(cudaGetLastError());
+}
+
 void Thermal::set_clock(double t, double dt)
 {
   set_clock_kernel<<<1, 32, 0, stream_>>>(member_d_.p, 1, t, dt);

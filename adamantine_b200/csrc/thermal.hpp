@@ -126,8 +126,12 @@ void launch_tile(int deg, int ns, int p, CUtensorMap const &map, KernelArgs cons
 void launch_set_clock(MemberData *members, int n, double t, double dt, cudaStream_t stream);
 void launch_advance_clock(MemberData *members, int n, cudaStream_t stream);
 void launch_stage_prepare(MemberData *members, int n, double c, cudaStream_t stream);
+// Per-Gauss-point powder ratios [C][NN] from the sparse powder history.
+void launch_expand_powder(uint32_t const *cell_info, int NN, uint8_t const *pmode, double const *pcell,
+                          double const *pq, double *out, size_t C, cudaStream_t stream);
 
 class Ensemble;
+class Adjoint;
 
 class Thermal
 {
@@ -190,6 +194,7 @@ public:
 
 private:
   friend class Ensemble;
+  friend class Adjoint;
   void rebuild();
   void upload_member();
   KernelArgs base_args() const;

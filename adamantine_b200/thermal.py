@@ -222,6 +222,11 @@ class ThermalPhysics:
         s.max_power = max_power
         _lib.check(self._L.adm_update_beam(self._h, int(i), ctypes.byref(s)))
 
+    def update_material(self, config: ThermalConfig):
+        """New material tables (same shape) from config."""
+        st = config.to_struct()
+        _lib.check(self._L.adm_update_material(self._h, ctypes.byref(st)))
+
     def device_error(self) -> int:
         code = ctypes.c_int32()
         _lib.check(self._L.adm_device_error(self._h, ctypes.byref(code)))

@@ -189,3 +189,41 @@ def surface_observations(n_nodes_xy, layers, n_obs=2000, sigma=5.0, name="ensemb
     nx, ny = n_nodes_xy
     flat = rng.choice(nx * ny, size=n_obs, replace=False)
     return np.stack([flat % nx, flat // nx], axis=1), sigma
+
+
+def adjoint_q2(n_cells=(64, 64, 32), extent=(20e-3, 20e-3, 10e-3), powder_layers=8, method="rk_second_order",
+               k_scale=1.0, cp_scale=1.0, absorptivity=0.35, power=400.0, name="adjoint_q2"):
+    """Adjoint workload: 64x64x32 Q2 (Gauss 3) over 20x20x10 mm with the
+    phase-change material (powder in the top 8 cell layers), Goldak 400 W /
+    0.35 with R = 250 um, d = 300 um (resolved by the 312.5 um cells) on the
+    seeded serpentine at the top surface; adiabatic; explicit RK2."""
+    nz = n_cells[2]
+    hz = extent[2] / nz
+    geo = Geometry(dim=3, n_cells=n_cells, extent=extent, material_height=extent[2] + 0.5 * hz,
+                   use_powder=True, powder_layer=powder_layers * hz + 0.5 * hz)
+    bnd = Boundary.from_database({"type": "adiabatic"}, 3)
+    seg = serpentine_segments(rng_for(name + "-scan"), 0.25 * extent[0], 0.75 * extent[0], 0.45 * extent[1],
+                              extent[2], 10, 200e-6, 1.0)
+    src = Source(type="goldak", depth=300e-6, absorption_efficiency=absorptivity, diameter=500e-6,
+                 max_power=power, segments=seg)
+    mat = phase_change_material(k_scale=k_scale, cp_scale=cp_scale)
+    return ThermalConfig(geometry=geo, material=mat, boundary=bnd, sources=[src], degree=2, time_method=method)
+
+
+def interior_points(cfg: ThermalConfig, n_points=500, radius=1.0e-3, depth=1.0e-3, name="adjoint-points"):
+    """n_points distinct seeded interior nodes (i, j, k) within `radius` (in
+    x and y) of the scan-path start and `depth` below the top surface, none
+    on the domain boundary."""
+    rng = rng_for(name)
+    geo = cfg.geometry
+    nx, ny, nz = geo.node_shape(cfg.degree)
+    h = [geo.extent[d] / (nx - 1 if d == 0 else (ny - 1 if d == 1 else nz - 1)) for d in range(3)]
+    seg = cfg.sources[0].segments
+    cx, cy, top = seg[0, 2], seg[0, 3], seg[0, 4]
+    i0, i1 = max(1, int((cx - radius) / h[0])), min(nx - 2, int((cx + radius) / h[0]))
+    j0, j1 = max(1, int((cy - radius) / h[1])), min(ny - 2, int((cy + radius) / h[1]))
+    k1 = min(nz - 2, int(round(top / h[2])) - 1)
+    k0 = max(1, k1 - int(depth / h[2]))
+    cand = np.array([(i, j, k) for k in range(k0, k1 + 1) for j in range(j0, j1 + 1) for i in range(i0, i1 + 1)])
+    pick = rng.choice(len(cand), size=min(n_points, len(cand)), replace=False)
+    return cand[np.sort(pick)]

@@ -191,6 +191,13 @@ int adm_activate_cells(adm_thermal *h, int64_t const *cells, int64_t n,
  * radius and power for source i (segments are ignored). */
 int adm_update_beam(adm_thermal *h, int32_t i, adm_source const *beam);
 
+/* New material tables of the same shape (number of materials and states,
+ * table or polynomial) for the handle: polynomial coefficients, tables and
+ * the state-independent properties are taken from cfg, nothing else. No
+ * counterpart in the reference (whose data assimilation changes beam
+ * parameters only); used to perturb material parameters. */
+int adm_update_material(adm_thermal *h, adm_config const *cfg);
+
 /* Largest node vector (adm_n_nodes) that adm_vmult_host_static accepts. */
 #define ADM_STATIC_SCRATCH_MAX_NODES 1310720
 
