@@ -30,40 +30,47 @@ namespace adm
 namespace
 {
 template <int DEG, int NS>
-void launch_adj(AdjArgs const &a, int n_items, cudaStream_t stream)
+void launch_adj(CUtensorMap const &ymap, CUtensorMap const &mmap, AdjArgs const &a, int n_items,
+                cudaStream_t stream)
 {
   using T_ = TD<DEG>;
-  size_t const smem = sizeof(double) * (2 * T_::BRICKP + 4 * T_::NN * T_::NCELL);
-  static bool attr = false;
-  if (!attr)
+  size_t const smem = sizeof(double) * (4 * T_::BRICKP + 4 * T_::NN * T_::NCELL);
+  static int grid_cap = 0;
+  if (grid_cap == 0)
   {
     ADM_CK(cudaFuncSetAttribute(adjoint_kernel<DEG, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = true;
+    int dev = 0, sms = 0, per_sm = 0;
+    ADM_CK(cudaGetDevice(&dev));
+    ADM_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    ADM_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_kernel<DEG, NS>, T_::NT, smem));
+    grid_cap = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
   }
-  adjoint_kernel<DEG, NS><<<n_items, T_::NT, smem, stream>>>(a);
+  int const grid = n_items < grid_cap ? n_items : grid_cap;
+  adjoint_kernel<DEG, NS><<<grid, T_::NT, smem, stream>>>(ymap, mmap, a, n_items);
 }
 
-void launch_adjoint(int deg, int ns, AdjArgs const &a, int n_items, cudaStream_t stream)
+void launch_adjoint(int deg, int ns, CUtensorMap const &ym, CUtensorMap const &mm, AdjArgs const &a, int n_items,
+                    cudaStream_t stream)
 {
   switch (deg * 10 + ns)
   {
   case 11:
-    launch_adj<1, 1>(a, n_items, stream);
+    launch_adj<1, 1>(ym, mm, a, n_items, stream);
     break;
   case 12:
-    launch_adj<1, 2>(a, n_items, stream);
+    launch_adj<1, 2>(ym, mm, a, n_items, stream);
     break;
   case 13:
-    launch_adj<1, 3>(a, n_items, stream);
+    launch_adj<1, 3>(ym, mm, a, n_items, stream);
     break;
   case 21:
-    launch_adj<2, 1>(a, n_items, stream);
+    launch_adj<2, 1>(ym, mm, a, n_items, stream);
     break;
   case 22:
-    launch_adj<2, 2>(a, n_items, stream);
+    launch_adj<2, 2>(ym, mm, a, n_items, stream);
     break;
   case 23:
-    launch_adj<2, 3>(a, n_items, stream);
+    launch_adj<2, 3>(ym, mm, a, n_items, stream);
     break;
   default:
     throw Error(ADM_ERR_INVALID, "no adjoint kernel for this degree / state count");
@@ -199,6 +206,10 @@ public:
     Thermal &t = th_;
     cudaStream_t const st = t.stream_;
     int const S = t.tab_.s;
+    // per step of a segment: the S stage inputs and (3 states) S phase states
+    Ystore_.alloc((size_t)K * S * n_);
+    if (t.ns_ == 3)
+      Sstore_.alloc((size_t)K * S * C_ * NN_);
     forward(t0, dt, n_steps, y0, K);
     double J = 0.0;
     ADM_CK(cudaMemcpyAsync(&J, Jd_.p, sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -222,34 +233,20 @@ public:
     }
     grad_d_.alloc(3);
     ADM_CK(cudaMemsetAsync(grad_d_.p, 0, 3 * sizeof(double), st));
-    // per step of a segment: the S stage inputs and (3 states) S phase states
-    Ystore_.alloc((size_t)K * S * n_);
-    if (ns3)
-      Sstore_.alloc((size_t)K * S * qn);
     int const n_seg = (n_steps + K - 1) / K;
     for (int seg = n_seg - 1; seg >= 0; --seg)
     {
       int const n0 = seg * K, n1 = std::min(n_steps, n0 + K);
-      // recompute the segment from its checkpoint, recording the stages
-      ADM_CK(cudaMemcpyAsync(y_.p, ck_y_.p + (size_t)seg * n_, n_ * sizeof(double), cudaMemcpyDeviceToDevice, st));
-      if (ns3)
-        restore_phase(seg);
-      for (int n = n0; n < n1; ++n)
+      // recompute the segment from its checkpoint, recording the stages (the
+      // forward run recorded the last segment already)
+      if (seg != n_seg - 1)
       {
-        t.set_clock(times_[n], dt);
-        for (int i = 0; i < S; ++i)
-        {
-          t.prepare_stage(t.tab_.c[i]);
-          KernelArgs a = t.stage_args(i);
-          a.y_override = y_.p;
-          double const *src = i == 0 ? y_.p : (a.src_sel == 1 ? t.za_p_ : t.zb_p_);
-          size_t const slot = (size_t)(n - n0) * S + i;
-          ADM_CK(cudaMemcpyAsync(Ystore_.p + slot * n_, src, n_ * sizeof(double), cudaMemcpyDeviceToDevice, st));
-          if (ns3)
-            launch_expand_powder(t.cell_info_d_.p, NN_, t.powder_mode_.p, t.powder_cell_.p, t.powder_q_.p,
-                                 Sstore_.p + slot * qn, C_, st);
-          t.launch_pass(a, src);
-        }
+        ADM_CK(cudaMemcpyAsync(y_.p, ck_y_.p + (size_t)seg * n_, n_ * sizeof(double), cudaMemcpyDeviceToDevice,
+                               st));
+        if (ns3)
+          restore_phase(seg);
+        for (int n = n0; n < n1; ++n)
+          record_step(n, n0, dt);
       }
       // backward sweep over the segment
       for (int n = n1 - 1; n >= n0; --n)
@@ -286,15 +283,7 @@ public:
           }
           A.lam_y = lamYi;
           A.grad = grad_d_.p;
-          for (int col = 0; col < 8; ++col)
-          {
-            int const count = t.colour_off_[col + 1] - t.colour_off_[col];
-            if (count == 0)
-              continue;
-            A.k.work = t.work_d_.p + t.colour_off_[col];
-            launch_adjoint(t.mesh_.deg, t.ns_, A, count, st);
-            ADM_CK(cudaGetLastError());
-          }
+          run_kernel(A);
           if (ns3)
             std::swap(ls_a_.p, ls_b_.p);
         }
@@ -355,15 +344,7 @@ public:
     }
     A.lam_y = lam;
     A.grad = grad_d_.p;
-    for (int col = 0; col < 8; ++col)
-    {
-      int const count = t.colour_off_[col + 1] - t.colour_off_[col];
-      if (count == 0)
-        continue;
-      A.k.work = t.work_d_.p + t.colour_off_[col];
-      launch_adjoint(t.mesh_.deg, t.ns_, A, count, st);
-      ADM_CK(cudaGetLastError());
-    }
+    run_kernel(A);
     double g[3];
     ADM_CK(cudaMemcpyAsync(g, grad_d_.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
     ADM_CK(cudaStreamSynchronize(st));
@@ -373,6 +354,21 @@ public:
   }
 
 private:
+  // one launch over the work items of every colour (atomics merge the nodes
+  // that tiles share)
+  void run_kernel(AdjArgs &A)
+  {
+    Thermal &t = th_;
+    int const count = t.colour_off_[8];
+    if (count == 0)
+      return;
+    A.k.work = t.work_d_.p;
+    CUtensorMap const ym = brick_map(t.mesh_, A.yv, 1, n_);
+    CUtensorMap const mm = brick_map(t.mesh_, A.mu, 1, n_);
+    launch_adjoint(t.mesh_.deg, t.ns_, ym, mm, A, count, t.stream_);
+    ADM_CK(cudaGetLastError());
+  }
+
   void check_run(int n_steps, int K)
   {
     if (n_steps < 1)
@@ -422,6 +418,31 @@ private:
                              cudaMemcpyDeviceToDevice, st));
       ADM_CK(cudaMemcpyAsync(ck_q_.p + (size_t)seg * C_ * NN_, t.powder_q_.p, C_ * NN_ * sizeof(double),
                              cudaMemcpyDeviceToDevice, st));
+    }
+  }
+
+  // One step n of the forward run, stage by stage as Thermal::launch_step
+  // does it, recording each stage's input field and phase state in slot
+  // (n - n0) of the segment store.
+  void record_step(int n, int n0, double dt)
+  {
+    Thermal &t = th_;
+    cudaStream_t const st = t.stream_;
+    int const S = t.tab_.s;
+    size_t const qn = C_ * NN_;
+    t.set_clock(times_[n], dt);
+    for (int i = 0; i < S; ++i)
+    {
+      t.prepare_stage(t.tab_.c[i]);
+      KernelArgs a = t.stage_args(i);
+      a.y_override = y_.p;
+      double const *src = i == 0 ? y_.p : (a.src_sel == 1 ? t.za_p_ : t.zb_p_);
+      size_t const slot = (size_t)(n - n0) * S + i;
+      ADM_CK(cudaMemcpyAsync(Ystore_.p + slot * n_, src, n_ * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      if (t.ns_ == 3)
+        launch_expand_powder(t.cell_info_d_.p, NN_, t.powder_mode_.p, t.powder_cell_.p, t.powder_q_.p,
+                             Sstore_.p + slot * qn, C_, st);
+      t.launch_pass(a, src);
     }
   }
 
@@ -477,12 +498,20 @@ private:
     times_.assign(n_steps + 1, 0.0);
     double tt = t0;
     observe(0);
+    int const last0 = K > 0 ? ((n_steps - 1) / K) * K : n_steps;
     for (int n = 0; n < n_steps; ++n)
     {
       if (K > 0 && n % K == 0)
         checkpoint(n / K);
       times_[n] = tt;
-      tt = t.evolve_one_time_step(tt, dt, y_.p);
+      if (n >= last0)
+      {
+        // last segment: record the stages now instead of recomputing them
+        record_step(n, last0, dt);
+        tt = tt + dt;
+      }
+      else
+        tt = t.evolve_one_time_step(tt, dt, y_.p);
       observe(n + 1);
     }
     times_[n_steps] = tt;

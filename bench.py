@@ -249,6 +249,53 @@ def run_ensemble(args, dist, local_rank):
     }
 
 
+ADJOINT_WORKLOAD = "adjoint_q2_64x64x32_rk2_200steps"
+
+
+def run_adjoint(args, local_rank):
+    """Adjoint gradient of the misfit at 500 interior points after steps
+    50/100/150/200 (RK2, dt = 1e-6, 64x64x32 Q2) with respect to conductivity
+    scale, specific-heat scale, absorptivity and power, checkpointed every 20
+    steps: time of one gradient over the time of one forward run, and the
+    agreement with central differences (h = 1e-5 relative) of the forward."""
+    import torch
+
+    from adamantine_b200.adjoint import AdjointProblem
+    from adamantine_b200.workloads import adjoint_q2, initial_temperature, interior_points, rng_for
+
+    cfg = adjoint_q2()
+    T0 = initial_temperature(cfg, "adjoint")
+    pts = interior_points(cfg, n_points=500)
+    obs = [50, 100, 150, 200]
+    prob = AdjointProblem(cfg, T0, 0.0, 1e-6, 200, obs, pts, device=local_rank, checkpoint_every=20)
+    truth = (1.0, 1.0, 0.35, 400.0)
+    prob.set_targets(prob.observe(truth))
+    f = np.exp(rng_for("adjoint-perturbation").uniform(np.log(0.9), np.log(1.1), 4))
+    theta = tuple(float(a * b) for a, b in zip(truth, f))
+    prob.objective(theta)  # warm-up
+    prob.gradient(theta)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    J = prob.objective(theta)
+    t1 = time.perf_counter()
+    Jg, grad = prob.gradient(theta)
+    t2 = time.perf_counter()
+    fd = np.zeros(4)
+    h = 1e-5
+    for k in range(4):
+        tp, tm = list(theta), list(theta)
+        tp[k] *= 1 + h
+        tm[k] *= 1 - h
+        fd[k] = (prob.objective(tp) - prob.objective(tm)) / (2 * h * theta[k])
+    rel = np.abs(grad - fd) / np.maximum(np.abs(fd), 1e-300)
+    return {
+        "workload": ADJOINT_WORKLOAD, "theta": list(theta), "J": J, "gradient": grad.tolist(),
+        "fd_gradient": fd.tolist(), "fd_max_rel_err": float(rel.max()), "fd_h": h,
+        "forward_ms": 1e3 * (t1 - t0), "gradient_ms": 1e3 * (t2 - t1),
+        "cost_ratio": (t2 - t1) / (t1 - t0), "checkpoint_every": 20, "timing": "host wall clock, synchronized",
+    }
+
+
 def run_reference(args, rank, world):
     """--impl reference: the oracle's vmult on all host cores (rank 0 only)."""
     if rank != 0:
@@ -382,6 +429,8 @@ def run_ours(args, rank, world, local_rank):
     }
     if not args.no_ensemble:
         line["ensemble"] = run_ensemble(args, dist, local_rank)
+    if not args.no_adjoint:
+        line["adjoint"] = run_adjoint(args, local_rank)
     if rank == 0 and not args.no_cpu_baseline:
         rate, med, n = cpu_vmult_rate(build_workload(args.size)[0], T, os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": rate, "unit": "GDoF/s", "cores": os.cpu_count() or 1, "kind": "port",
@@ -402,6 +451,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--size", default="full", choices=sorted(SIZES))
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
