@@ -68,6 +68,14 @@ SIGNATURES = {
     "adm_ensemble_synchronize": [_VP],
     "adm_enkf_create": [ctypes.c_int, _VP, ctypes.POINTER(_VP)],
     "adm_enkf_destroy": [_VP],
+    # include/adamantine_b200_deposition.h
+    "adm_deposition_boxes": [ctypes.POINTER(SourceStruct), ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                             ctypes.c_double, ctypes.c_double, ctypes.c_int64, _D, _D, _D, _D, _D, _I64],
+    "adm_deposition_create": [_VP, ctypes.c_int64, _D, _D, _D, _D, _D, ctypes.c_double, ctypes.c_double,
+                              ctypes.POINTER(_VP)],
+    "adm_deposition_destroy": [_VP],
+    "adm_deposition_activate_range": [_VP, ctypes.c_int64, ctypes.c_int64, ctypes.c_double, _VP, _I64],
+    "adm_deposition_step": [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_double, _VP, _I64],
     # include/adamantine_b200_adjoint.h
     "adm_adjoint_create": [_VP, ctypes.POINTER(_VP)],
     "adm_adjoint_destroy": [_VP],

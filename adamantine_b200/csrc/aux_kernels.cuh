@@ -176,6 +176,25 @@ struct GridArgs
 
 // compute_inverse_mass_matrix (source/ThermalOperator.templates.hh:118-164):
 // Gauss-Lobatto lumped mass of the active cells, inverted on DoFs, 0 elsewhere.
+// Inverse lumped mass of node (i, j, k) from the active cells around it.
+__device__ __forceinline__ double node_inv_mass(GridArgs const &g, uint32_t const *cell_info, int i, int j, int k)
+{
+  int cx[2], ax[2], cy[2], ay[2], cz[2], az[2];
+  int const nx = node_cells(i, g.deg, g.nc[0], cx, ax);
+  int const ny = node_cells(j, g.deg, g.nc[1], cy, ay);
+  int const nz = node_cells(k, g.deg, g.nc[2], cz, az);
+  double m = 0.0;
+  for (int c = 0; c < nz; ++c)
+    for (int b = 0; b < ny; ++b)
+      for (int a = 0; a < nx; ++a)
+      {
+        size_t const cell = cx[a] + (size_t)g.nc[0] * (cy[b] + (size_t)g.nc[1] * cz[c]);
+        if (cell_info[cell] & CI_ACTIVE)
+          m += g.vol * g.glw[ax[a]] * g.glw[ay[b]] * g.glw[az[c]];
+      }
+  return m > 0.0 ? 1.0 / m : 0.0;
+}
+
 __global__ void inverse_mass_kernel(GridArgs g, uint32_t const *cell_info,
                                     double *inv_mass, size_t n_total)
 {
@@ -190,20 +209,169 @@ __global__ void inverse_mass_kernel(GridArgs g, uint32_t const *cell_info,
     inv_mass[idx] = 0.0;
     return;
   }
-  int cx[2], ax[2], cy[2], ay[2], cz[2], az[2];
-  int const nx = node_cells(i, g.deg, g.nc[0], cx, ax);
-  int const ny = node_cells(j, g.deg, g.nc[1], cy, ay);
-  int const nz = node_cells(k, g.deg, g.nc[2], cz, az);
-  double m = 0.0;
-  for (int c = 0; c < nz; ++c)
-    for (int b = 0; b < ny; ++b)
-      for (int a = 0; a < nx; ++a)
+  inv_mass[idx] = node_inv_mass(g, cell_info, i, j, k);
+}
+
+// ------------------------------------------------------------ deposition
+// Boxes of material deposition against the cells of the structured mesh.
+// Cell (i, j, k) spans [origin + i h, origin + (i + 1) h] per direction (the
+// vertices of a subdivided hyper-rectangle); a cell and a box intersect when
+// the closed intervals overlap in every direction (touching counts), as the
+// bounding-box search of get_elements_to_activate
+// (source/material_deposition.cc:374-438) decides.
+struct BoxArgs
+{
+  int nc[3];
+  double origin[3], h[3];
+  double const *lo; // [n][3]
+  double const *hi; // [n][3]
+  int64_t b0;       // first box of the launch (block b handles box b0 + b)
+};
+
+__device__ __forceinline__ double vertex_coord(double origin, int i, double h)
+{
+  // no contraction into an FMA: the vertex is origin + (i * h) rounded twice
+  return __dadd_rn(origin, __dmul_rn((double)i, h));
+}
+
+// Index range [i0, i1] of the cells whose closed extent meets [lo, hi].
+__device__ __forceinline__ void box_range(double lo, double hi, double origin, double h, int n, int &i0,
+                                          int &i1)
+{
+  double const fa = floor((lo - origin) / h) - 1.0, fb = floor((hi - origin) / h) + 1.0;
+  int a = fa < 0.0 ? 0 : (fa > n - 1 ? n : (int)fa);
+  int b = fb < 0.0 ? -1 : (fb > n - 1 ? n - 1 : (int)fb);
+  while (a <= b && vertex_coord(origin, a + 1, h) < lo)
+    ++a;
+  while (b >= a && vertex_coord(origin, b, h) > hi)
+    --b;
+  i0 = a;
+  i1 = b;
+}
+
+// Every inactive cell a box meets records the largest such box index (the
+// last box of the window sets its deposition direction).
+__global__ void box_mark_kernel(BoxArgs a, uint32_t const *cell_info, int32_t *last_box)
+{
+  int64_t const b = a.b0 + blockIdx.x;
+  int r0[3], r1[3];
+  for (int d = 0; d < 3; ++d)
+    box_range(a.lo[3 * b + d], a.hi[3 * b + d], a.origin[d], a.h[d], a.nc[d], r0[d], r1[d]);
+  int64_t const ex = r1[0] - r0[0] + 1, ey = r1[1] - r0[1] + 1, ez = r1[2] - r0[2] + 1;
+  if (ex <= 0 || ey <= 0 || ez <= 0)
+    return;
+  int64_t const total = ex * ey * ez;
+  for (int64_t e = threadIdx.x; e < total; e += blockDim.x)
+  {
+    int const x = r0[0] + (int)(e % ex), y = r0[1] + (int)((e / ex) % ey), z = r0[2] + (int)(e / (ex * ey));
+    size_t const c = x + (size_t)a.nc[0] * (y + (size_t)a.nc[1] * z);
+    if (!(cell_info[c] & CI_ACTIVE))
+      atomicMax(&last_box[c], (int32_t)b);
+  }
+}
+
+// Appends each marked cell once (by the box that marked it last) to the
+// activation list.
+__global__ void box_collect_kernel(BoxArgs a, int32_t const *last_box, int64_t *list, int32_t *list_box,
+                                   unsigned long long *count, unsigned long long capacity)
+{
+  int64_t const b = a.b0 + blockIdx.x;
+  int r0[3], r1[3];
+  for (int d = 0; d < 3; ++d)
+    box_range(a.lo[3 * b + d], a.hi[3 * b + d], a.origin[d], a.h[d], a.nc[d], r0[d], r1[d]);
+  int64_t const ex = r1[0] - r0[0] + 1, ey = r1[1] - r0[1] + 1, ez = r1[2] - r0[2] + 1;
+  if (ex <= 0 || ey <= 0 || ez <= 0)
+    return;
+  int64_t const total = ex * ey * ez;
+  for (int64_t e = threadIdx.x; e < total; e += blockDim.x)
+  {
+    int const x = r0[0] + (int)(e % ex), y = r0[1] + (int)((e / ex) % ey), z = r0[2] + (int)(e / (ex * ey));
+    size_t const c = x + (size_t)a.nc[0] * (y + (size_t)a.nc[1] * z);
+    if (last_box[c] == (int32_t)b)
+    {
+      unsigned long long const slot = atomicAdd(count, 1ull);
+      if (slot < capacity)
       {
-        size_t const cell = cx[a] + (size_t)g.nc[0] * (cy[b] + (size_t)g.nc[1] * cz[c]);
-        if (cell_info[cell] & CI_ACTIVE)
-          m += g.vol * g.glw[ax[a]] * g.glw[ay[b]] * g.glw[az[c]];
+        list[slot] = (int64_t)c;
+        list_box[slot] = (int32_t)b;
       }
-  inv_mass[idx] = m > 0.0 ? 1.0 / m : 0.0;
+    }
+  }
+}
+
+// New cells become active (material id from matid), take their box's
+// deposition direction, count as melted before (the reference's transfer of
+// the inactive cells' data), and leave the mark array clean.
+__global__ void activate_list_kernel(int64_t const *list, int32_t const *list_box, int64_t n, uint8_t const *matid,
+                                     double const *box_cos, double const *box_sin, uint32_t *cell_info,
+                                     double *cosv, double *sinv, uint8_t *has_melted, int32_t *last_box)
+{
+  int64_t const w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (w >= n)
+    return;
+  int64_t const c = list[w];
+  int const b = list_box[w];
+  cell_info[c] = CI_ACTIVE | ((uint32_t)(matid[c] & 15) << CI_MAT_SHIFT);
+  if (cosv)
+  {
+    cosv[c] = box_cos[b];
+    sinv[c] = box_sin[b];
+  }
+  has_melted[c] = 1;
+  last_box[c] = -1;
+}
+
+// Face bits (active boundary / interface) of the listed cells and of their
+// six neighbours, from the activity after the activation.
+__global__ void face_bits_kernel(int64_t const *list, int64_t n, int nc0, int nc1, int nc2, uint32_t *cell_info)
+{
+  int64_t const w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (w >= n * 7)
+    return;
+  int64_t const c0 = list[w / 7];
+  int const which = (int)(w % 7);
+  int const nc[3] = {nc0, nc1, nc2};
+  int cc[3] = {(int)(c0 % nc0), (int)((c0 / nc0) % nc1), (int)(c0 / ((int64_t)nc0 * nc1))};
+  if (which > 0)
+  {
+    int const d = (which - 1) / 2;
+    cc[d] += ((which - 1) % 2) ? 1 : -1;
+    if (cc[d] < 0 || cc[d] >= nc[d])
+      return;
+  }
+  size_t const c = cc[0] + (size_t)nc0 * (cc[1] + (size_t)nc1 * cc[2]);
+  uint32_t const info = cell_info[c];
+  if (!(info & CI_ACTIVE))
+    return;
+  uint32_t out = info & (CI_ACTIVE | (15u << CI_MAT_SHIFT));
+  for (int f = 0; f < 6; ++f)
+  {
+    int const d = f / 2;
+    int nb[3] = {cc[0], cc[1], cc[2]};
+    nb[d] += (f % 2) ? 1 : -1;
+    if (nb[d] < 0 || nb[d] >= nc[d])
+      out |= 1u << (CI_FACE_SHIFT + f);
+    else if (!(cell_info[nb[0] + (size_t)nc0 * (nb[1] + (size_t)nc1 * nb[2])] & CI_ACTIVE))
+      out |= (1u << (CI_FACE_SHIFT + f)) | (1u << (CI_INTERFACE_SHIFT + f));
+  }
+  cell_info[c] = out;
+}
+
+// Inverse lumped mass of the nodes of the listed cells (after activation).
+__global__ void inverse_mass_cells_kernel(GridArgs g, uint32_t const *cell_info, int64_t const *list, int64_t n,
+                                          double *inv_mass)
+{
+  int64_t const w = blockIdx.x;
+  if (w >= n)
+    return;
+  int const deg = g.deg, np = deg + 1;
+  int64_t const c = list[w];
+  int const ccx = c % g.nc[0], ccy = (c / g.nc[0]) % g.nc[1], ccz = c / ((int64_t)g.nc[0] * g.nc[1]);
+  for (int l = threadIdx.x; l < np * np * np; l += blockDim.x)
+  {
+    int const i = deg * ccx + l % np, j = deg * ccy + (l / np) % np, k = deg * ccz + l / (np * np);
+    inv_mass[i + (size_t)g.pitch * (j + (size_t)g.nn[1] * k)] = node_inv_mass(g, cell_info, i, j, k);
+  }
 }
 
 // New DoFs of an activation get new_temperature: nodes of the cells in the

@@ -1143,6 +1143,180 @@ void Thermal::activate_cells(int64_t const *cells, int64_t n, double new_tempera
   get_state_from_material_properties();
 }
 
+int64_t Thermal::activate_in_boxes(DeviceBoxes const &boxes, int64_t b0, int64_t b1, double new_temperature,
+                                   double *solution)
+{
+  if (!setup_done_)
+    throw Error(ADM_ERR_INVALID, "setup() has not been called");
+  if (b0 < 0 || b1 > boxes.n || b0 > b1)
+    throw Error(ADM_ERR_INVALID, "box range out of bounds");
+  if (b0 == b1)
+    return 0;
+  ADM_CK(cudaSetDevice(device_));
+  size_t const C = mesh_.n_cells;
+  if (last_box_d_.n != C)
+  {
+    last_box_d_.alloc(C);
+    ADM_CK(cudaMemsetAsync(last_box_d_.p, 0xff, C * sizeof(int32_t), stream_)); // -1
+    list_d_.alloc(C);
+    list_box_d_.alloc(C);
+    count_d_.alloc(1);
+    matid_d_.alloc(C);
+  }
+  ADM_CK(cudaMemcpyAsync(matid_d_.p, matid_.data(), C, cudaMemcpyHostToDevice, stream_));
+  ADM_CK(cudaMemsetAsync(count_d_.p, 0, sizeof(unsigned long long), stream_));
+  BoxArgs ba;
+  for (int d = 0; d < 3; ++d)
+  {
+    ba.nc[d] = mesh_.nc[d];
+    ba.origin[d] = mesh_.origin[d];
+    ba.h[d] = mesh_.h[d];
+  }
+  ba.lo = boxes.lo;
+  ba.hi = boxes.hi;
+  ba.b0 = b0;
+  unsigned const nb = (unsigned)(b1 - b0);
+  box_mark_kernel<<<nb, 256, 0, stream_>>>(ba, cell_info_d_.p, last_box_d_.p);
+  ADM_CK(cudaGetLastError());
+  box_collect_kernel<<<nb, 256, 0, stream_>>>(ba, last_box_d_.p, list_d_.p, list_box_d_.p, count_d_.p,
+                                              (unsigned long long)C);
+  ADM_CK(cudaGetLastError());
+  unsigned long long cnt = 0;
+  ADM_CK(cudaMemcpyAsync(&cnt, count_d_.p, sizeof(cnt), cudaMemcpyDeviceToHost, stream_));
+  ADM_CK(cudaStreamSynchronize(stream_));
+  int64_t const n = (int64_t)cnt;
+  if (n == 0)
+    return 0;
+  std::vector<int64_t> list(n);
+  std::vector<int32_t> lbox(n);
+  ADM_CK(cudaMemcpyAsync(list.data(), list_d_.p, n * sizeof(int64_t), cudaMemcpyDeviceToHost, stream_));
+  ADM_CK(cudaMemcpyAsync(lbox.data(), list_box_d_.p, n * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
+  ADM_CK(cudaStreamSynchronize(stream_));
+  std::vector<double> cn(n), sn(n);
+  bool rotation = false;
+  for (int64_t k = 0; k < n; ++k)
+  {
+    cn[k] = boxes.cos_host[lbox[k]];
+    sn[k] = boxes.sin_host[lbox[k]];
+    rotation = rotation || cn[k] != 1.0 || sn[k] != 0.0;
+  }
+  bool const need_slots = (ns_ == 3) && !adiabatic_only_;
+  if (need_slots)
+  {
+    // the per-face powder slots are laid out on the host: full rebuild
+    ADM_CK(cudaMemsetAsync(last_box_d_.p, 0xff, C * sizeof(int32_t), stream_));
+    activate_cells(list.data(), n, new_temperature, cn.data(), sn.data(), solution);
+    return n;
+  }
+  // add_material_start: the phase state goes to the cells
+  set_state_to_material_properties();
+  GridArgs g;
+  for (int d = 0; d < 3; ++d)
+  {
+    g.nc[d] = mesh_.nc[d];
+    g.nn[d] = mesh_.nn[d];
+  }
+  g.pitch = mesh_.pitch;
+  g.deg = mesh_.deg;
+  g.vol = mesh_.h[0] * mesh_.h[1] * mesh_.h[2];
+  for (int i = 0; i < 3; ++i)
+    g.glw[i] = mesh_.glw[i];
+  // new DoFs get the new-material temperature (old cell info)
+  activate_nodes_kernel<<<(unsigned)n, 32, 0, stream_>>>(g, cell_info_d_.p, list_d_.p, n, new_temperature,
+                                                         solution);
+  ADM_CK(cudaGetLastError());
+  // host bookkeeping of the activity and directions
+  for (int64_t k = 0; k < n; ++k)
+  {
+    size_t const c = (size_t)list[k];
+    active_[c] = 1;
+    cos_[c] = cn[k];
+    sin_[c] = sn[k];
+    has_melted_[c] = 1;
+  }
+  bool const rotation_added = rotation && !has_rotation_;
+  if (rotation_added)
+  {
+    cos_d_.alloc(C);
+    sin_d_.alloc(C);
+    ADM_CK(cudaMemcpyAsync(cos_d_.p, cos_.data(), C * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    ADM_CK(cudaMemcpyAsync(sin_d_.p, sin_.data(), C * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    has_rotation_ = true;
+  }
+  unsigned const blk = (unsigned)((n + 255) / 256);
+  activate_list_kernel<<<blk, 256, 0, stream_>>>(list_d_.p, list_box_d_.p, n, matid_d_.p, boxes.cosv, boxes.sinv,
+                                                 cell_info_d_.p, has_rotation_ ? cos_d_.p : nullptr,
+                                                 has_rotation_ ? sin_d_.p : nullptr, has_melted_d_.p,
+                                                 last_box_d_.p);
+  ADM_CK(cudaGetLastError());
+  face_bits_kernel<<<(unsigned)((7 * n + 255) / 256), 256, 0, stream_>>>(list_d_.p, n, mesh_.nc[0], mesh_.nc[1],
+                                                                         mesh_.nc[2], cell_info_d_.p);
+  ADM_CK(cudaGetLastError());
+  inverse_mass_cells_kernel<<<(unsigned)n, 32, 0, stream_>>>(g, cell_info_d_.p, list_d_.p, n, inv_mass_.p);
+  ADM_CK(cudaGetLastError());
+  // tiles: activity, neighbour masks and colour work lists (host, per tile)
+  std::vector<uint8_t> &ta = topo_.tile_active;
+  for (int64_t k = 0; k < n; ++k)
+  {
+    size_t const c = (size_t)list[k];
+    int const x = c % mesh_.nc[0], y = (c / mesh_.nc[0]) % mesh_.nc[1], z = c / ((size_t)mesh_.nc[0] * mesh_.nc[1]);
+    ta[(x / mesh_.tx) + (size_t)mesh_.nt[0] * ((y / mesh_.ty) + (size_t)mesh_.nt[1] * (z / mesh_.tz))] = 1;
+  }
+  topo_.all_tiles_active = true;
+  for (int tz = 0; tz < mesh_.nt[2]; ++tz)
+    for (int ty = 0; ty < mesh_.nt[1]; ++ty)
+      for (int tx = 0; tx < mesh_.nt[0]; ++tx)
+      {
+        size_t const tile = tx + (size_t)mesh_.nt[0] * (ty + (size_t)mesh_.nt[1] * tz);
+        if (!ta[tile])
+        {
+          topo_.all_tiles_active = false;
+          continue;
+        }
+        uint32_t mask = 0;
+        for (int oz = -1; oz <= 1; ++oz)
+          for (int oy = -1; oy <= 1; ++oy)
+            for (int ox = -1; ox <= 1; ++ox)
+            {
+              int const ax = tx + ox, ay = ty + oy, az = tz + oz;
+              if (ax < 0 || ay < 0 || az < 0 || ax >= mesh_.nt[0] || ay >= mesh_.nt[1] || az >= mesh_.nt[2])
+                continue;
+              if (ta[ax + (size_t)mesh_.nt[0] * (ay + (size_t)mesh_.nt[1] * az)])
+                mask |= 1u << ((ox + 1) + 3 * (oy + 1) + 9 * (oz + 1));
+            }
+        topo_.tile_nbr[tile] = mask;
+      }
+  work_.clear();
+  for (int col = 0; col < 8; ++col)
+  {
+    colour_off_[col] = (int)work_.size();
+    for (int tz = (col >> 2) & 1; tz < mesh_.nt[2]; tz += 2)
+      for (int ty = (col >> 1) & 1; ty < mesh_.nt[1]; ty += 2)
+        for (int tx = col & 1; tx < mesh_.nt[0]; tx += 2)
+        {
+          size_t const tile = tx + (size_t)mesh_.nt[0] * (ty + (size_t)mesh_.nt[1] * tz);
+          if (ta[tile])
+            work_.push_back(TileWork{0, (int32_t)tile});
+        }
+  }
+  colour_off_[8] = (int)work_.size();
+  work_d_.alloc(std::max<size_t>(1, work_.size()));
+  ADM_CK(cudaMemcpyAsync(work_d_.p, work_.data(), work_.size() * sizeof(TileWork), cudaMemcpyHostToDevice, stream_));
+  ADM_CK(cudaMemcpyAsync(tile_nbr_d_.p, topo_.tile_nbr.data(), mesh_.n_tiles * sizeof(uint32_t),
+                         cudaMemcpyHostToDevice, stream_));
+  // add_material_end: the cell state goes back to the quadrature points
+  get_state_from_material_properties();
+  ADM_CK(cudaStreamSynchronize(stream_));
+  if (step_graph_)
+  {
+    cudaGraphExecDestroy(step_graph_);
+    step_graph_ = nullptr;
+  }
+  if (rotation_added)
+    upload_member();
+  return n;
+}
+
 void Thermal::update_beam(int i, adm_source const &beam)
 {
   if (i < 0 || i >= cfg_.n_sources)

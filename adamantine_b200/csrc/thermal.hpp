@@ -133,6 +133,15 @@ void launch_expand_powder(uint32_t const *cell_info, int NN, uint8_t const *pmod
 class Ensemble;
 class Adjoint;
 
+// Material-deposition boxes on the device ([n][3] corners) with host copies
+// of the directions (for the host fallback of the activation).
+struct DeviceBoxes
+{
+  int64_t n = 0;
+  double const *lo = nullptr, *hi = nullptr, *cosv = nullptr, *sinv = nullptr;
+  std::vector<double> cos_host, sin_host;
+};
+
 class Thermal
 {
 public:
@@ -172,6 +181,11 @@ public:
   void activate_cells(int64_t const *cells, int64_t n, double new_temperature,
                       double const *cos_new, double const *sin_new, double *solution);
   void update_beam(int i, adm_source const &beam);
+  // add_material_start/end for the inactive cells that boxes [b0, b1) meet,
+  // found and activated on the device (append list, no renumbering);
+  // returns the number of activated cells
+  int64_t activate_in_boxes(DeviceBoxes const &boxes, int64_t b0, int64_t b1, double new_temperature,
+                            double *solution);
   // new material tables of the same shape (ensemble analysis of a
   // material parameter); no counterpart in the reference
   void update_material(adm_config const &cfg);
@@ -235,6 +249,11 @@ private:
   DevBuf<uint8_t> powder_mode_, has_melted_d_;
   DevBuf<int32_t> face_slot_d_, error_d_;
   DevBuf<int64_t> cells_d_;
+  // deposition: per-cell mark, append list, material ids
+  DevBuf<int32_t> last_box_d_, list_box_d_;
+  DevBuf<int64_t> list_d_;
+  DevBuf<unsigned long long> count_d_;
+  DevBuf<uint8_t> matid_d_;
   DevBuf<MaterialDesc> mat_d_;
   DevBuf<BeamState> beam_state_d_;
   DevBuf<MemberData> member_d_;

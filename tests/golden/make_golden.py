@@ -7,6 +7,12 @@ Run in a container where the reference is mounted at /root/reference:
 * convective_bc_gold.npy -- tests/data/convective_bc_gold.txt of the reference
   (the 1809 nodal temperatures of test_thermal_physics.hh:513-625, deal.II DoF
   order), stored as float64.
+* deposition_inputs.npz -- the inputs of test_material_deposition.cc:
+  scan_path.txt and scan_path_L.txt as (end_time, power_modifier, x, y, z)
+  segment rows (ScanPath "segment" format: mode 1 = point held for `param`
+  seconds, mode 0 = line at `param` m/s), and the box file
+  material_path_test_material_deposition.txt as rows (center[3], size[3],
+  time, angle).
 """
 import os
 import sys
@@ -25,6 +31,34 @@ def main():
     assert vals.size == 1809, vals.size
     np.save(os.path.join(HERE, "convective_bc_gold.npy"), vals)
     print("wrote convective_bc_gold.npy", vals.size)
+
+    data = os.path.join(REF, "tests", "data")
+    out = {}
+    for name in ("scan_path", "scan_path_L"):
+        out[name] = segments(open(os.path.join(data, name + ".txt")).read())
+    lines = open(os.path.join(data, "material_path_test_material_deposition.txt")).read().split("\n")
+    assert int(lines[0]) == 3
+    out["material_path"] = np.array([[float(v) for v in ln.split()] for ln in lines[1:] if ln.strip()])
+    np.savez(os.path.join(HERE, "deposition_inputs.npz"), **out)
+    print("wrote deposition_inputs.npz", {k: v.shape for k, v in out.items()})
+
+
+def segments(text):
+    """ScanPath segment-format text -> (end_time, power_modifier, x, y, z) rows
+    (the first row is the start point)."""
+    rows = [ln.split() for ln in text.split("\n")[3:] if ln.strip()]
+    out = []
+    t = 0.0
+    prev = None
+    for r in rows:
+        mode, x, y, z, pmod, param = int(r[0]), float(r[1]), float(r[2]), float(r[3]), float(r[4]), float(r[5])
+        if mode == 1 or prev is None:
+            t = t + param
+        else:
+            t = t + float(np.sqrt((x - prev[0]) ** 2 + (y - prev[1]) ** 2 + (z - prev[2]) ** 2)) / param
+        out.append([t, pmod, x, y, z])
+        prev = (x, y, z)
+    return np.array(out)
 
 
 if __name__ == "__main__":
