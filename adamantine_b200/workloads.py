@@ -227,3 +227,28 @@ def interior_points(cfg: ThermalConfig, n_points=500, radius=1.0e-3, depth=1.0e-
     cand = np.array([(i, j, k) for k in range(k0, k1 + 1) for j in range(j0, j1 + 1) for i in range(i0, i1 + 1)])
     pick = rng.choice(len(cand), size=min(n_points, len(cand)), replace=False)
     return cand[np.sort(pick)]
+
+
+def deposition_q2(n_cells=(256, 256, 128), extent=(40e-3, 40e-3, 20e-3), initial_layers=100, powder_layers=16,
+                  n_passes=40, speed=1.2, power=400.0, name="deposition_q2"):
+    """Largest single-GPU workload with deposition: 256x256x128 Q2 (Gauss 3)
+    over 40x40x20 mm (67.6 M nodes), the phase-change material with powder in
+    the top 16 of the initially active 100 cell layers, Goldak 400 W / 0.35
+    (R = d = 50 um) on a seeded 40-pass raster (x passes from 5 to 35 mm,
+    hatch 0.75 mm, 1.2 m/s) at the top surface; adiabatic; RK4. Returns the
+    configuration and the deposition boxes (50 um long, 50 um high, 100 um
+    wide) along the path, which activate the cell layer above the surface."""
+    from .deposition import deposition_boxes
+
+    hz = extent[2] / n_cells[2]
+    top = initial_layers * hz
+    geo = Geometry(dim=3, n_cells=n_cells, extent=extent, material_height=top, use_powder=True,
+                   powder_layer=powder_layers * hz)
+    bnd = Boundary.from_database({"type": "adiabatic"}, 3)
+    seg = serpentine_segments(rng_for(name + "-scan"), 5e-3, 35e-3, 5e-3, top, n_passes, 0.75e-3, speed)
+    src = Source(type="goldak", depth=50e-6, absorption_efficiency=0.35, diameter=100e-6, max_power=power,
+                 segments=seg)
+    cfg = ThermalConfig(geometry=geo, material=phase_change_material(), boundary=bnd, sources=[src], degree=2,
+                        time_method="rk_fourth_order")
+    boxes = deposition_boxes(cfg, 50e-6, 50e-6, 100e-6, 0.0)
+    return cfg, boxes

@@ -296,6 +296,73 @@ def run_adjoint(args, local_rank):
     }
 
 
+DEPOSITION_WORKLOAD = "deposition_q2_256x256x128_rk4"
+
+
+def run_deposition(args, local_rank, with_cpu):
+    """RK4 steps (dt = 2e-7) of the 67.6 M-node Q2 deposition workload with
+    the driver's per-step activation of the deposition boxes; throughput as
+    operator applications (4 per step) x nodes / time, the fused stages'
+    algorithmic HBM bytes, and (with_cpu) the oracle's time for one RK4 step
+    of the same problem on the host cores (the 20-step window is 20 x that)."""
+    import torch
+
+    from adamantine_b200.deposition import Deposition
+    from adamantine_b200.thermal import ThermalPhysics
+    from adamantine_b200.workloads import deposition_q2, initial_temperature
+
+    cfg, boxes = deposition_q2()
+    g = ThermalPhysics(cfg, device=local_rank)
+    T0 = initial_temperature(cfg, "deposition", melt_pool=False)
+    y = g.from_grid(T0)
+    dep = Deposition(g, boxes)
+    n_nodes = int(np.prod(cfg.geometry.node_shape(2)))
+    dt = 2e-7
+    t = 0.0
+    activated = 0
+    for _ in range(3):  # warm-up (first activation, kernel first launches)
+        activated += dep.step(t, dt, 300.0, y)
+        t = g.evolve_one_time_step(t, dt, y)
+    torch.cuda.synchronize()
+    steps = args.deposition_steps
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    n_act = 0
+    ev0.record(g.stream)
+    for _ in range(steps):
+        n_act += dep.step(t, dt, 300.0, y)
+        t = g.evolve_one_time_step(t, dt, y)
+    ev1.record(g.stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    assert g.device_error() == 0
+    C = g.n_cells
+    # fused RK4 stages: 32 + 48 + 48 + 40 bytes per node (stage input, inverse
+    # mass, y, running sum, next stage vector) and 13 bytes per cell per stage
+    bytes_step = 168 * g.m() + 4 * 13 * C
+    out = {
+        "workload": DEPOSITION_WORKLOAD, "nodes": n_nodes, "cells": C, "steps": steps, "dt": dt,
+        "ms_per_step": ms / steps, "gdofs_per_s": 4 * n_nodes * steps / (ms * 1e-3) / 1e9,
+        "hbm_gbs_algorithmic": bytes_step * steps / (ms * 1e-3) / 1e9, "cells_activated": activated + n_act,
+        "boxes": boxes.n, "activation": "device append list, driver window per step",
+    }
+    if with_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle_py
+
+        st = cfg.to_struct()
+        o = oracle_py.Oracle(st, active=cfg.geometry.active_cells(), initial_state=cfg.geometry.initial_state())
+        yr = np.ascontiguousarray(T0, np.float64).reshape(-1).copy()
+        t0 = time.perf_counter()
+        o.evolve_one_time_step(0.0, dt, yr)
+        cpu_s = time.perf_counter() - t0
+        out["cpu_baseline"] = {"seconds_per_step": cpu_s, "seconds_20_step_window": 20 * cpu_s,
+                               "cores": os.cpu_count() or 1, "kind": "port",
+                               "sample": "one RK4 step of the workload (oracle, OpenMP); the 20-step window is "
+                                         "20 times that"}
+    return out
+
+
 def run_reference(args, rank, world):
     """--impl reference: the oracle's vmult on all host cores (rank 0 only)."""
     if rank != 0:
@@ -431,6 +498,8 @@ def run_ours(args, rank, world, local_rank):
         line["ensemble"] = run_ensemble(args, dist, local_rank)
     if not args.no_adjoint:
         line["adjoint"] = run_adjoint(args, local_rank)
+    if args.deposition_steps > 0:
+        line["deposition"] = run_deposition(args, local_rank, rank == 0 and not args.no_cpu_baseline)
     if rank == 0 and not args.no_cpu_baseline:
         rate, med, n = cpu_vmult_rate(build_workload(args.size)[0], T, os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": rate, "unit": "GDoF/s", "cores": os.cpu_count() or 1, "kind": "port",
@@ -452,6 +521,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--deposition-steps", type=int, default=400,
+                    help="RK4 steps of the deposition workload (0: skip; the configuration runs 2000)")
     ap.add_argument("--size", default="full", choices=sorted(SIZES))
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
