@@ -48,6 +48,8 @@ SIGNATURES = {
     "adm_update_beam": [_VP, ctypes.c_int32, ctypes.POINTER(SourceStruct)],
     "adm_vmult_host_static": [_VP, _D, _D],
     "adm_update_material": [_VP, ctypes.POINTER(ConfigStruct)],
+    "adm_save_checkpoint": [_VP, ctypes.c_char_p, ctypes.c_double, _VP],
+    "adm_load_checkpoint": [_VP, ctypes.c_char_p, ctypes.c_int32, _D, _VP],
     "adm_device_error": [_VP, _I32],
     "adm_synchronize": [_VP],
     # include/adamantine_b200_ensemble.h

@@ -132,6 +132,7 @@ void launch_expand_powder(uint32_t const *cell_info, int NN, uint8_t const *pmod
 
 class Ensemble;
 class Adjoint;
+struct Checkpoint;
 
 // Material-deposition boxes on the device ([n][3] corners) with host copies
 // of the directions (for the host fallback of the activation).
@@ -209,6 +210,7 @@ public:
 private:
   friend class Ensemble;
   friend class Adjoint;
+  friend struct Checkpoint;
   void rebuild();
   void upload_member();
   KernelArgs base_args() const;

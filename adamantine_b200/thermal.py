@@ -227,6 +227,18 @@ class ThermalPhysics:
         st = config.to_struct()
         _lib.check(self._L.adm_update_material(self._h, ctypes.byref(st)))
 
+    def save_checkpoint(self, path: str, time: float, solution: torch.Tensor):
+        """save_checkpoint: cells, state, time and solution to one file."""
+        _lib.check(self._L.adm_save_checkpoint(self._h, str(path).encode(), float(time), _dev(solution)))
+
+    def load_checkpoint(self, path: str, solution: torch.Tensor, exact: bool = False) -> float:
+        """load_checkpoint into solution; returns the saved time. exact
+        restores the per-point phase history (bit-identical continuation)."""
+        t = ctypes.c_double()
+        _lib.check(self._L.adm_load_checkpoint(self._h, str(path).encode(), int(bool(exact)), ctypes.byref(t),
+                                               _dev(solution)))
+        return float(t.value)
+
     def device_error(self) -> int:
         code = ctypes.c_int32()
         _lib.check(self._L.adm_device_error(self._h, ctypes.byref(code)))

@@ -191,6 +191,20 @@ int adm_activate_cells(adm_thermal *h, int64_t const *cells, int64_t n,
  * radius and power for source i (segments are ignored). */
 int adm_update_beam(adm_thermal *h, int32_t i, adm_source const *beam);
 
+/* ThermalPhysicsInterface::save_checkpoint
+ * (source/ThermalPhysics.templates.hh:1062-1185): the cells' activity,
+ * material ids, deposition directions, has_melted flags and state ratios,
+ * the time and the device solution vector, plus the per-point phase history,
+ * written to one file at path. */
+int adm_save_checkpoint(adm_thermal *h, const char *path, double time, double const *solution);
+/* ThermalPhysicsInterface::load_checkpoint (:974-1060) into a handle created
+ * with the same mesh, element and material states: the cells are set up
+ * again, the solution (device) and *time (may be NULL) are restored. exact = 0
+ * broadcasts the saved cell states to the points, as the reference does;
+ * exact = 1 restores the saved per-point history instead (the continued run
+ * is then bit-identical to an uninterrupted one). */
+int adm_load_checkpoint(adm_thermal *h, const char *path, int32_t exact, double *time, double *solution);
+
 /* New material tables of the same shape (number of materials and states,
  * table or polynomial) for the handle: polynomial coefficients, tables and
  * the state-independent properties are taken from cfg, nothing else. No
