@@ -48,6 +48,9 @@ SIGNATURES = {
     "adm_update_beam": [_VP, ctypes.c_int32, ctypes.POINTER(SourceStruct)],
     "adm_vmult_host_static": [_VP, _D, _D],
     "adm_update_material": [_VP, ctypes.POINTER(ConfigStruct)],
+    "adm_set_schedule": [_VP, ctypes.c_int32],
+    "adm_get_schedule": [_VP, _I32],
+    "adm_autotune": [_VP, _VP, _I32, _D],
     "adm_save_checkpoint": [_VP, ctypes.c_char_p, ctypes.c_double, _VP],
     "adm_load_checkpoint": [_VP, ctypes.c_char_p, ctypes.c_int32, _D, _VP],
     "adm_device_error": [_VP, _I32],
@@ -66,6 +69,8 @@ SIGNATURES = {
     "adm_ensemble_update_material": [_VP, ctypes.c_int32, ctypes.POINTER(ConfigStruct)],
     "adm_ensemble_get_cell_state": [_VP, ctypes.c_int32, _D],
     "adm_ensemble_get_inverse_mass_matrix": [_VP, ctypes.c_int32, _VP],
+    "adm_ensemble_set_schedule": [_VP, ctypes.c_int32],
+    "adm_ensemble_autotune": [_VP, _VP, ctypes.c_double, _I32, _D],
     "adm_ensemble_device_error": [_VP, _I32],
     "adm_ensemble_synchronize": [_VP],
     "adm_enkf_create": [ctypes.c_int, _VP, ctypes.POINTER(_VP)],

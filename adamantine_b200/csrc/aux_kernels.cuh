@@ -212,6 +212,47 @@ __global__ void inverse_mass_kernel(GridArgs g, uint32_t const *cell_info,
   inv_mass[idx] = node_inv_mass(g, cell_info, i, j, k);
 }
 
+// ------------------------------------------------------------ atomic schedule
+// Stage update of the atomic schedule: the tile kernel added every node's
+// residual into acc (zeroed before); this pass applies the inverse lumped mass
+// and the explicit Runge-Kutta update exactly as the coloured schedule's last
+// toucher does (blockIdx.y = member).
+__global__ void stage_finalize_kernel(KernelArgs a, size_t n_nodes)
+{
+  size_t const g = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (g >= n_nodes)
+    return;
+  MemberData const &md = a.members[blockIdx.y];
+  double *const y = a.y_override ? a.y_override : md.y;
+  double const dt = md.clock[1];
+  double const f = md.inv_mass[g] * md.acc[g];
+  if (!isfinite(f))
+    atomicCAS(md.error, 0, (int)DERR_NONFINITE);
+  double const yv = y[g];
+  if (a.n_stages == 1)
+  {
+    y[g] = yv + dt * f;
+    return;
+  }
+  double const sv = a.stage > 0 ? md.s[g] : 0.0;
+  if (!a.last)
+  {
+    double zn = yv;
+    if (a.has_f0)
+      zn = zn + (dt * a.a_next_f0) * md.f0[g];
+    zn = zn + (dt * a.a_next) * f;
+    (a.dst_sel == 1 ? md.za : md.zb)[g] = zn;
+    double const sb = (dt * a.b_i) * f;
+    md.s[g] = a.stage == 0 ? sb : sv + sb;
+    if (a.store_f0)
+      md.f0[g] = f;
+  }
+  else
+  {
+    y[g] = yv + (sv + (dt * a.b_i) * f);
+  }
+}
+
 // ------------------------------------------------------------ deposition
 // Boxes of material deposition against the cells of the structured mesh.
 // Cell (i, j, k) spans [origin + i h, origin + (i + 1) h] per direction (the

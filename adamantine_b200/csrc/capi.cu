@@ -250,6 +250,32 @@ int adm_update_material(adm_thermal *h, adm_config const *cfg)
   });
 }
 
+int adm_set_schedule(adm_thermal *h, int32_t schedule)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h, "null handle");
+    as(h)->set_schedule(schedule);
+  });
+}
+
+int adm_get_schedule(adm_thermal const *h, int32_t *schedule)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && schedule, "null argument");
+    *schedule = as(h)->schedule();
+  });
+}
+
+int adm_autotune(adm_thermal *h, double const *field, int32_t *schedule, double *ms)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && field, "null argument");
+    int const c = as(h)->autotune(field, ms);
+    if (schedule)
+      *schedule = c;
+  });
+}
+
 int adm_update_beam(adm_thermal *h, int32_t i, adm_source const *beam)
 {
   return adm::guard([&] {

@@ -176,6 +176,19 @@ void Ensemble::launch_step(double *solutions)
     a.y_override = nullptr;
     double const *src = i == 0 ? solutions : (a.src_sel == 1 ? za_.p : zb_.p);
     CUtensorMap const map = brick_map(members_[0]->mesh_, src, n, stride_);
+    if (schedule_ == Thermal::kScheduleAtomic)
+    {
+      a.atomic = 1;
+      ADM_CK(cudaMemsetAsync(acc_.p, 0, stride_ * (size_t)n * sizeof(double), stream_));
+      if (colour_off_[8] > 0)
+      {
+        a.work = work_d_.p;
+        launch_tile(deg_, ns_, poly_p_, map, a, colour_off_[8], stream_);
+        ADM_CK(cudaGetLastError());
+      }
+      launch_stage_finalize(a, stride_, n, stream_);
+      continue;
+    }
     for (int col = 0; col < 8; ++col)
     {
       int const count = colour_off_[col + 1] - colour_off_[col];
@@ -281,6 +294,69 @@ void Ensemble::update_beam(int i, int beam, adm_source const &src)
   members_.at((size_t)i)->update_beam(beam, src);
   dirty_ = true; // the member table holds a copy of the beam description
   drop_graph();
+}
+
+void Ensemble::set_schedule(int schedule)
+{
+  if (schedule != Thermal::kScheduleColoured && schedule != Thermal::kScheduleAtomic)
+    throw Error(ADM_ERR_INVALID, "unknown schedule");
+  if (schedule != schedule_)
+    drop_graph();
+  schedule_ = schedule;
+  // the looped baseline runs the members with the same schedule
+  for (auto &m : members_)
+    m->set_schedule(schedule);
+}
+
+// Times one batched step with each schedule on a copy of the solutions (the
+// members' phase history and clocks restored afterwards) and keeps the faster.
+int Ensemble::autotune(double const *solutions, double dt, double *ms_out)
+{
+  if (!setup_done_)
+    throw Error(ADM_ERR_INVALID, "setup() has not been called");
+  ADM_CK(cudaSetDevice(device_));
+  size_t const total = stride_ * members_.size();
+  DevBuf<double> scratch;
+  scratch.alloc(total);
+  std::vector<Thermal::PhaseSnapshot> snaps;
+  for (auto &m : members_)
+    snaps.push_back(m->save_phase());
+  cudaEvent_t e0, e1;
+  ADM_CK(cudaEventCreate(&e0));
+  ADM_CK(cudaEventCreate(&e1));
+  int const saved = schedule_;
+  double best = 0.0;
+  int choice = saved;
+  for (int sch : {Thermal::kScheduleColoured, Thermal::kScheduleAtomic})
+  {
+    schedule_ = sch;
+    ADM_CK(cudaMemcpyAsync(scratch.p, solutions, total * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    evolve_one_time_step(0.0, dt, scratch.p);
+    int const reps = 3;
+    ADM_CK(cudaEventRecord(e0, stream_));
+    for (int r = 0; r < reps; ++r)
+      evolve_one_time_step((r + 1) * dt, dt, scratch.p);
+    ADM_CK(cudaEventRecord(e1, stream_));
+    ADM_CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    ADM_CK(cudaEventElapsedTime(&ms, e0, e1));
+    double const per = ms / reps;
+    if (ms_out)
+      ms_out[sch] = per;
+    if (best == 0.0 || per < best)
+    {
+      best = per;
+      choice = sch;
+    }
+    for (size_t k = 0; k < members_.size(); ++k)
+      members_[k]->restore_phase(snaps[k]);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  ADM_CK(cudaStreamSynchronize(stream_));
+  schedule_ = saved;
+  set_schedule(choice);
+  return choice;
 }
 
 int32_t Ensemble::device_error()
@@ -434,6 +510,24 @@ int adm_ensemble_device_error(adm_ensemble *e, int32_t *code)
   return adm::guard([&] {
     ADM_REQUIRE(e && code, "null argument");
     *code = as_ens(e)->device_error();
+  });
+}
+
+int adm_ensemble_set_schedule(adm_ensemble *e, int32_t schedule)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(e, "null handle");
+    as_ens(e)->set_schedule(schedule);
+  });
+}
+
+int adm_ensemble_autotune(adm_ensemble *e, double const *solutions, double dt, int32_t *schedule, double *ms)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(e && solutions, "null argument");
+    int const c = as_ens(e)->autotune(solutions, dt, ms);
+    if (schedule)
+      *schedule = c;
   });
 }
 

@@ -48,6 +48,11 @@ public:
   // a member's material or beam changed (after an analysis step)
   void update_material(int i, adm_config const &cfg);
   void update_beam(int i, int beam, adm_source const &src);
+  // launch schedule of the batched stages (Thermal::kSchedule*) and its
+  // autotuner (one timed batched step per schedule on a copy of solutions)
+  void set_schedule(int schedule);
+  int schedule() const { return schedule_; }
+  int autotune(double const *solutions, double dt, double *ms_out);
   int32_t device_error();
   size_t n_work_items() const { return work_.size(); }
   cudaStream_t stream() const { return stream_; }
@@ -65,6 +70,7 @@ private:
   size_t stride_ = 0;
   int deg_ = 1, ns_ = 1, poly_p_ = 2;
   bool any_source_ = false;
+  int schedule_ = Thermal::kScheduleColoured;
   bool setup_done_ = false;
   Thermal::Tableau tab_;
 

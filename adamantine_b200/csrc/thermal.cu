@@ -808,6 +808,26 @@ CUtensorMap brick_map(Mesh const &m, double const *base, int n_members, size_t m
 void Thermal::launch_pass(KernelArgs a, double const *src)
 {
   CUtensorMap const map = brick_map(mesh_, src, 1, mesh_.n_nodes);
+  if (schedule_ == kScheduleAtomic)
+  {
+    int const count = colour_off_[8];
+    size_t const N = mesh_.n_nodes;
+    a.atomic = 1;
+    if (a.mode == 2)
+      ADM_CK(cudaMemsetAsync(acc_p_, 0, N * sizeof(double), stream_));
+    if (count > 0)
+    {
+      a.work = work_d_.p;
+      launch_tile(mesh_.deg, ns_, poly_p_, map, a, count, stream_);
+      ADM_CK(cudaGetLastError());
+    }
+    if (a.mode == 2)
+    {
+      stage_finalize_kernel<<<dim3((unsigned)((N + 255) / 256), 1), 256, 0, stream_>>>(a, N);
+      ADM_CK(cudaGetLastError());
+    }
+    return;
+  }
   for (int col = 0; col < 8; ++col)
   {
     int const count = colour_off_[col + 1] - colour_off_[col];
@@ -834,6 +854,12 @@ void launch_advance_clock(MemberData *members, int n, cudaStream_t stream)
 void launch_stage_prepare(MemberData *members, int n, double c, cudaStream_t stream)
 {
   stage_prepare_kernel<<<n, 32, 0, stream>>>(members, n, c);
+  ADM_CK(cudaGetLastError());
+}
+
+void launch_stage_finalize(KernelArgs const &a, size_t n_nodes, int n_members, cudaStream_t stream)
+{
+  stage_finalize_kernel<<<dim3((unsigned)((n_nodes + 255) / 256), (unsigned)n_members), 256, 0, stream>>>(a, n_nodes);
   ADM_CK(cudaGetLastError());
 }
 
@@ -870,8 +896,9 @@ void Thermal::vmult(double *dst, double const *src, bool add)
   if (!setup_done_)
     throw Error(ADM_ERR_INVALID, "setup() has not been called");
   ADM_CK(cudaSetDevice(device_));
-  // Nodes that only inactive tiles touch are not written by the tile kernel.
-  if (!add && !topo_.all_tiles_active)
+  // Nodes that only inactive tiles touch are not written by the tile kernel;
+  // the atomic schedule adds into a zeroed vector.
+  if (!add && (!topo_.all_tiles_active || schedule_ == kScheduleAtomic))
     ADM_CK(cudaMemsetAsync(dst, 0, mesh_.n_nodes * sizeof(double), stream_));
   prepare_stage(0.0);
   KernelArgs a = base_args();
@@ -1366,6 +1393,111 @@ int32_t Thermal::device_error()
 }
 
 void Thermal::synchronize() { ADM_CK(cudaStreamSynchronize(stream_)); }
+
+void Thermal::set_schedule(int schedule)
+{
+  if (schedule != kScheduleColoured && schedule != kScheduleAtomic)
+    throw Error(ADM_ERR_INVALID, "unknown schedule");
+  if (schedule != schedule_ && step_graph_)
+  {
+    cudaGraphExecDestroy(step_graph_);
+    step_graph_ = nullptr;
+  }
+  schedule_ = schedule;
+}
+
+Thermal::PhaseSnapshot Thermal::save_phase() const
+{
+  PhaseSnapshot p;
+  size_t const C = mesh_.n_cells;
+  int const NN = (mesh_.deg + 1) * (mesh_.deg + 1) * (mesh_.deg + 1);
+  if (ns_ == 3)
+  {
+    p.mode.alloc(C);
+    p.cell.alloc(C);
+    p.q.alloc(C * NN);
+    ADM_CK(cudaMemcpyAsync(p.mode.p, powder_mode_.p, C, cudaMemcpyDeviceToDevice, stream_));
+    ADM_CK(cudaMemcpyAsync(p.cell.p, powder_cell_.p, C * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    ADM_CK(cudaMemcpyAsync(p.q.p, powder_q_.p, C * NN * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    if (face_powder_.p)
+    {
+      p.face.alloc(face_powder_.n);
+      ADM_CK(cudaMemcpyAsync(p.face.p, face_powder_.p, face_powder_.n * sizeof(double), cudaMemcpyDeviceToDevice,
+                             stream_));
+    }
+  }
+  if (ns_ > 1)
+  {
+    p.liquid.alloc(C);
+    ADM_CK(cudaMemcpyAsync(p.liquid.p, liquid_sum_.p, C * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+  }
+  p.clock.alloc(2);
+  ADM_CK(cudaMemcpyAsync(p.clock.p, clock_.p, 2 * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+  return p;
+}
+
+void Thermal::restore_phase(PhaseSnapshot const &p)
+{
+  if (p.mode.p)
+  {
+    ADM_CK(cudaMemcpyAsync(powder_mode_.p, p.mode.p, p.mode.n, cudaMemcpyDeviceToDevice, stream_));
+    ADM_CK(cudaMemcpyAsync(powder_cell_.p, p.cell.p, p.cell.n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    ADM_CK(cudaMemcpyAsync(powder_q_.p, p.q.p, p.q.n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+  }
+  if (p.face.p)
+    ADM_CK(cudaMemcpyAsync(face_powder_.p, p.face.p, p.face.n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+  if (p.liquid.p)
+    ADM_CK(cudaMemcpyAsync(liquid_sum_.p, p.liquid.p, p.liquid.n * sizeof(double), cudaMemcpyDeviceToDevice,
+                           stream_));
+  ADM_CK(cudaMemcpyAsync(clock_.p, p.clock.p, 2 * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+}
+
+// Times the schedules on the handle's problem (vmults of `field`, the phase
+// history saved before and restored after) and keeps the fastest.
+int Thermal::autotune(double const *field, double *ms_out)
+{
+  if (!setup_done_)
+    throw Error(ADM_ERR_INVALID, "setup() has not been called");
+  ADM_CK(cudaSetDevice(device_));
+  PhaseSnapshot const snap = save_phase();
+  DevBuf<double> dst;
+  dst.alloc(mesh_.n_nodes);
+  cudaEvent_t e0, e1;
+  ADM_CK(cudaEventCreate(&e0));
+  ADM_CK(cudaEventCreate(&e1));
+  int const saved = schedule_;
+  double best = 0.0;
+  int choice = saved;
+  for (int sch : {kScheduleColoured, kScheduleAtomic})
+  {
+    schedule_ = sch;
+    for (int r = 0; r < 2; ++r)
+      vmult(dst.p, field, false);
+    ADM_CK(cudaEventRecord(e0, stream_));
+    int const reps = 5;
+    for (int r = 0; r < reps; ++r)
+      vmult(dst.p, field, false);
+    ADM_CK(cudaEventRecord(e1, stream_));
+    ADM_CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    ADM_CK(cudaEventElapsedTime(&ms, e0, e1));
+    double const per = ms / reps;
+    if (ms_out)
+      ms_out[sch] = per;
+    if (best == 0.0 || per < best)
+    {
+      best = per;
+      choice = sch;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  schedule_ = saved;
+  restore_phase(snap);
+  ADM_CK(cudaStreamSynchronize(stream_));
+  set_schedule(choice);
+  return choice;
+}
 
 void Thermal::bind_stage_vectors(double *za, double *zb, double *s, double *f0, double *acc)
 {

@@ -41,6 +41,23 @@ struct DevBuf
   DevBuf() = default;
   DevBuf(DevBuf const &) = delete;
   DevBuf &operator=(DevBuf const &) = delete;
+  DevBuf(DevBuf &&o) noexcept : p(o.p), n(o.n)
+  {
+    o.p = nullptr;
+    o.n = 0;
+  }
+  DevBuf &operator=(DevBuf &&o) noexcept
+  {
+    if (this != &o)
+    {
+      release();
+      p = o.p;
+      n = o.n;
+      o.p = nullptr;
+      o.n = 0;
+    }
+    return *this;
+  }
   ~DevBuf() { release(); }
   void release()
   {
@@ -127,6 +144,8 @@ void launch_set_clock(MemberData *members, int n, double t, double dt, cudaStrea
 void launch_advance_clock(MemberData *members, int n, cudaStream_t stream);
 void launch_stage_prepare(MemberData *members, int n, double c, cudaStream_t stream);
 // Per-Gauss-point powder ratios [C][NN] from the sparse powder history.
+// Stage update of the atomic schedule for n_members members (a.members).
+void launch_stage_finalize(KernelArgs const &a, size_t n_nodes, int n_members, cudaStream_t stream);
 void launch_expand_powder(uint32_t const *cell_info, int NN, uint8_t const *pmode, double const *pcell,
                           double const *pq, double *out, size_t C, cudaStream_t stream);
 
@@ -199,6 +218,28 @@ public:
   void synchronize();
   void bind_stage_vectors(double *za, double *zb, double *s, double *f0, double *acc);
 
+  // Launch schedules of an operator application / RK stage: coloured (one
+  // launch per tile colour, node sums by colour order, fused update; bit
+  // reproducible) or atomic (one launch over every tile, node sums by
+  // atomics, separate update pass; faster when a colour has fewer tiles than
+  // the GPU holds CTAs, not bit reproducible run to run).
+  static constexpr int kScheduleColoured = 0, kScheduleAtomic = 1;
+  void set_schedule(int schedule);
+  int schedule() const { return schedule_; }
+  // times both schedules on vmults of `field` (phase history restored) and
+  // keeps the faster; ms_out[2] (may be null) receives the per-vmult times
+  int autotune(double const *field, double *ms_out);
+
+  // device copy of the phase history (powder, face powder, liquid sums) and
+  // the clock, to run trial steps without changing the state
+  struct PhaseSnapshot
+  {
+    DevBuf<uint8_t> mode;
+    DevBuf<double> cell, q, face, liquid, clock;
+  };
+  PhaseSnapshot save_phase() const;
+  void restore_phase(PhaseSnapshot const &p);
+
   // stage schedule (Butcher tableau of the configured method)
   struct Tableau
   {
@@ -233,6 +274,7 @@ private:
   bool has_rotation_ = false;
   bool setup_done_ = false;
   double op_time_ = 0.0;
+  int schedule_ = kScheduleColoured;
   Tableau tab_;
 
   std::vector<uint8_t> active_, matid_, init_state_, has_melted_;

@@ -402,7 +402,7 @@ __device__ __forceinline__ void load_member_constants(SmemPhys &sp, MemberData c
 // The persistent tile loop: CTA b processes work items b, b + grid, ... of
 // one colour. The node brick of the next item is fetched by TMA into the
 // other buffer while the current item is computed.
-template <int DEG, int NS, int P>
+template <int DEG, int NS, int P, bool AT>
 __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
     tile_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ KernelArgs args, int n_items)
 {
@@ -475,7 +475,7 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
       if (tid == 0)
         sp.member = w.member;
     }
-    if (tid < 27)
+    if (!AT && tid < 27)
     {
       // first/last toucher role of a node whose per-direction sharing state
       // is (tid % 3, tid / 3 % 3, tid / 9): 0 not shared, 1 shared with the
@@ -1006,10 +1006,20 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
       bool const inside = gx < args.nn[0] && gy < nn1 && gz < args.nn[2];
       int const sx = (X == 0 && tix > 0) ? 1 : ((X == DEG * TX && tix < nt0 - 1) ? 2 : 0);
       int const sy = (Y == 0 && tiy > 0) ? 1 : ((Y == DEG * TY && tiy < nt1 - 1) ? 2 : 0);
-      rl[i] = (own && inside) ? (sp.role[sx + 3 * sy + 9 * sz] | 4) : 0;
+      rl[i] = (own && inside) ? (AT ? 4 : (sp.role[sx + 3 * sy + 9 * sz] | 4)) : 0;
       gidx[i] = gx + (size_t)pitch * (gy + (size_t)nn1 * gz);
     }
-    if (args.mode == 0 || args.mode == 1)
+    if constexpr (AT)
+    {
+      // atomic schedule: every colour in one launch, the node sums are
+      // added into the zeroed target and finalized by a separate pass
+      double *const tgt = args.mode == 2 ? md.acc : args.vdst;
+#pragma unroll
+      for (int i = 0; i < NQS; ++i)
+        if (rl[i] & 4)
+          atomicAdd(&tgt[gidx[i]], res[i]);
+    }
+    else if (args.mode == 0 || args.mode == 1)
     {
       double old[NQS];
 #pragma unroll
@@ -1072,7 +1082,7 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
       }
     }
     // vmult writes zeros into the row padding of the node layout
-    if (args.mode == 0 && tix == nt0 - 1 && pitch > args.nn[0])
+    if (!AT && args.mode == 0 && tix == nt0 - 1 && pitch > args.nn[0])
     {
       int const npad = pitch - args.nn[0];
       for (int i = tid; i < npad * BY * BZ; i += NT)
@@ -1085,6 +1095,27 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
     }
     __syncthreads();
   }
+}
+
+// Launches the persistent tile kernel over n_items work items with at most
+// the number of CTAs that are resident at once on the device.
+template <int DEG, int NS, int P, bool AT>
+void launch_tile_t(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
+{
+  static int grid_cap = 0;
+  if (grid_cap == 0)
+  {
+    cudaFuncSetAttribute(tile_kernel<DEG, NS, P, AT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)TD<DEG>::SMEM);
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_kernel<DEG, NS, P, AT>, TD<DEG>::NT,
+                                                  TD<DEG>::SMEM);
+    grid_cap = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+  }
+  int const grid = n_items < grid_cap ? n_items : grid_cap;
+  tile_kernel<DEG, NS, P, AT><<<grid, TD<DEG>::NT, TD<DEG>::SMEM, stream>>>(map, a, n_items);
 }
 
 } // namespace adm

@@ -174,6 +174,19 @@ class Ensemble:
         _lib.check(self._L.adm_ensemble_get_inverse_mass_matrix(self._h, int(member), _dev(out)))
         return out
 
+    def set_schedule(self, schedule: int):
+        """Launch schedule of the batched stages (0 coloured, 1 atomic)."""
+        _lib.check(self._L.adm_ensemble_set_schedule(self._h, int(schedule)))
+
+    def autotune(self, solutions: torch.Tensor, dt: float):
+        """Times one batched step per schedule on a copy of solutions, keeps
+        the faster; returns (schedule, [ms coloured, ms atomic])."""
+        c = ctypes.c_int32()
+        ms = np.zeros(2)
+        _lib.check(self._L.adm_ensemble_autotune(self._h, self._check(solutions), float(dt), ctypes.byref(c),
+                                                 _ptr(ms, ctypes.c_double)))
+        return int(c.value), ms.tolist()
+
     def device_error(self) -> int:
         code = ctypes.c_int32()
         _lib.check(self._L.adm_ensemble_device_error(self._h, ctypes.byref(code)))

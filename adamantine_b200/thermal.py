@@ -227,6 +227,25 @@ class ThermalPhysics:
         st = config.to_struct()
         _lib.check(self._L.adm_update_material(self._h, ctypes.byref(st)))
 
+    COLOURED, ATOMIC = 0, 1
+
+    def set_schedule(self, schedule: int):
+        """Launch schedule: COLOURED (bit reproducible) or ATOMIC."""
+        _lib.check(self._L.adm_set_schedule(self._h, int(schedule)))
+
+    def schedule(self) -> int:
+        v = ctypes.c_int32()
+        _lib.check(self._L.adm_get_schedule(self._h, ctypes.byref(v)))
+        return int(v.value)
+
+    def autotune(self, field: torch.Tensor):
+        """Times both schedules on vmults of field, keeps the faster; returns
+        (schedule, [ms coloured, ms atomic])."""
+        c = ctypes.c_int32()
+        ms = np.zeros(2)
+        _lib.check(self._L.adm_autotune(self._h, _dev(field), ctypes.byref(c), _ptr(ms, ctypes.c_double)))
+        return int(c.value), ms.tolist()
+
     def save_checkpoint(self, path: str, time: float, solution: torch.Tensor):
         """save_checkpoint: cells, state, time and solution to one file."""
         _lib.check(self._L.adm_save_checkpoint(self._h, str(path).encode(), float(time), _dev(solution)))

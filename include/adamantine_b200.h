@@ -191,6 +191,22 @@ int adm_activate_cells(adm_thermal *h, int64_t const *cells, int64_t n,
  * radius and power for source i (segments are ignored). */
 int adm_update_beam(adm_thermal *h, int32_t i, adm_source const *beam);
 
+/* Launch schedule of operator applications and RK stages (no counterpart in
+ * the reference): ADM_SCHEDULE_COLOURED (default) runs one launch per tile
+ * colour, sums shared nodes in colour order and fuses the stage update --
+ * bit reproducible; ADM_SCHEDULE_ATOMIC runs every tile in one launch, sums
+ * shared nodes with atomics and updates in a separate pass -- faster when a
+ * colour has fewer tiles than the GPU holds CTAs (small meshes), rounding
+ * order not reproducible run to run. */
+#define ADM_SCHEDULE_COLOURED 0
+#define ADM_SCHEDULE_ATOMIC 1
+int adm_set_schedule(adm_thermal *h, int32_t schedule);
+int adm_get_schedule(adm_thermal const *h, int32_t *schedule);
+/* Autotuner: times both schedules on vmults of the device field (the phase
+ * history is restored afterwards), keeps the faster in the handle and
+ * returns it in *schedule; ms[2] (may be NULL) receives the per-vmult times. */
+int adm_autotune(adm_thermal *h, double const *field, int32_t *schedule, double *ms);
+
 /* ThermalPhysicsInterface::save_checkpoint
  * (source/ThermalPhysics.templates.hh:1062-1185): the cells' activity,
  * material ids, deposition directions, has_melted flags and state ratios,

@@ -66,6 +66,12 @@ int adm_ensemble_update_material(adm_ensemble *e, int32_t member, adm_config con
 int adm_ensemble_get_cell_state(adm_ensemble *e, int32_t member, double *state_host);
 /* Inverse lumped mass of member k into a device vector. */
 int adm_ensemble_get_inverse_mass_matrix(adm_ensemble *e, int32_t member, double *dst);
+/* Launch schedule of the batched stages (ADM_SCHEDULE_* of adamantine_b200.h). */
+int adm_ensemble_set_schedule(adm_ensemble *e, int32_t schedule);
+/* Autotuner: times one batched step of size dt with each schedule on a copy
+ * of solutions (phase history and clocks restored), keeps the faster and
+ * returns it; ms[2] (may be NULL) receives the per-step times. */
+int adm_ensemble_autotune(adm_ensemble *e, double const *solutions, double dt, int32_t *schedule, double *ms);
 /* First non-zero sticky device error word over the members (synchronizes). */
 int adm_ensemble_device_error(adm_ensemble *e, int32_t *code);
 int adm_ensemble_synchronize(adm_ensemble *e);
