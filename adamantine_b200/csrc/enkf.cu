@@ -28,6 +28,7 @@ namespace
 constexpr int kNB = 64;        // Cholesky block size
 constexpr int kMaxN = 64;      // members per analysis
 constexpr int kMaxObs = 16384; // observations (the solve keeps one column in shared memory)
+constexpr int kMaxGain = 256;  // members of a sharded analysis (all GPUs)
 
 enum EnkfError
 {
@@ -384,6 +385,110 @@ __global__ void __launch_bounds__(256) update_kernel(double *states, int64_t str
       states[(int64_t)l * stride + i] += s;
   }
 }
+// HX[k][j] = x_k[idx_k[j]] for the local members (sharded analysis).
+__global__ void observe_kernel(double const *states, int64_t stride, int n_members, int64_t n_state,
+                               int64_t const *idx, int m, double *HX, int *err)
+{
+  int64_t const e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= (int64_t)n_members * m)
+    return;
+  int const k = (int)(e / m);
+  int64_t i = idx[e];
+  if (i < 0 || i >= n_state)
+  {
+    atomicCAS(err, 0, (int)EERR_BAD_INDEX);
+    i = 0;
+  }
+  HX[e] = states[(int64_t)k * stride + i];
+}
+
+// HA = HX - mean over members, D = y + e_k - HX (from all members' HX).
+__global__ void center_kernel(double const *HX, int n_members, int m, double const *obs, double const *pert,
+                              double *HA, double *D)
+{
+  int const j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m)
+    return;
+  double sum = 0.0;
+  for (int k = 0; k < n_members; ++k)
+    sum += HX[(int64_t)k * m + j];
+  double const mean = sum / n_members;
+  for (int k = 0; k < n_members; ++k)
+  {
+    double const hx = HX[(int64_t)k * m + j];
+    HA[(int64_t)k * m + j] = hx - mean;
+    D[(int64_t)k * m + j] = obs[j] + pert[(int64_t)k * m + j] - hx;
+  }
+}
+
+// U[k][i] = sum over the local members k' of (x_k'[i] - mean[i]) W[k'][k]
+// for every member k of the ensemble (rows i: the states, then the
+// parameters). W rows of the local members are staged in shared memory.
+__global__ void __launch_bounds__(256) partial_update_kernel(double const *states, int64_t stride, int n_local,
+                                                             int n_members, int64_t n_state, double const *params,
+                                                             int n_params, double const *sum, double const *W,
+                                                             double *U)
+{
+  extern __shared__ double w[]; // [n_local][n_members]
+  for (int e = threadIdx.x; e < n_local * n_members; e += blockDim.x)
+    w[e] = W[e];
+  __syncthreads();
+  int64_t const rows = n_state + n_params;
+  int64_t const i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= rows)
+    return;
+  bool const is_param = i >= n_state;
+  double const mean = sum[i] / n_members;
+  double a[kMaxN];
+#pragma unroll
+  for (int k = 0; k < kMaxN; ++k)
+  {
+    a[k] = 0.0;
+    if (k < n_local)
+      a[k] = (is_param ? params[(int64_t)k * n_params + (i - n_state)] : states[(int64_t)k * stride + i]) - mean;
+  }
+  for (int l = 0; l < n_members; ++l)
+  {
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < kMaxN; ++k)
+      if (k < n_local)
+        s = fma(a[k], w[k * n_members + l], s);
+    U[(int64_t)l * rows + i] = s;
+  }
+}
+
+// sum[i] = sum over the local members of the augmented state (rows: the
+// states, then the parameters).
+__global__ void local_sum_kernel(double const *states, int64_t stride, int n_local, int64_t n_state,
+                                 double const *params, int n_params, double *sum)
+{
+  int64_t const i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n_state + n_params)
+    return;
+  double s = 0.0;
+  for (int k = 0; k < n_local; ++k)
+    s += i < n_state ? states[(int64_t)k * stride + i] : params[(int64_t)k * n_params + (i - n_state)];
+  sum[i] = s;
+}
+
+// x_k[i] += U[k][i] for the local members (mask: 1 = update).
+__global__ void apply_kernel(double *states, int64_t stride, int n_local, int64_t n_state, double *params,
+                             int n_params, double const *U, uint8_t const *mask)
+{
+  int64_t const rows = n_state + n_params;
+  int64_t const e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= (int64_t)n_local * rows)
+    return;
+  int const k = (int)(e / rows);
+  int64_t const i = e % rows;
+  double const u = U[e];
+  if (i >= n_state)
+    params[(int64_t)k * n_params + (i - n_state)] += u;
+  else if (!mask || mask[(int64_t)k * n_state + i])
+    states[(int64_t)k * stride + i] += u;
+}
+
 } // namespace
 
 // Workspace of the analysis, grown on demand.
@@ -452,6 +557,131 @@ struct Enkf
     ADM_CK(cudaGetLastError());
     ADM_CK(cudaStreamSynchronize(stream));
   }
+
+  // ---- building blocks of the sharded analysis (members split over GPUs)
+  void check_err()
+  {
+    int h_err = 0;
+    ADM_CK(cudaMemcpyAsync(&h_err, err.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    ADM_CK(cudaStreamSynchronize(stream));
+    if (h_err == EERR_BAD_INDEX)
+      throw Error(ADM_ERR_INVALID, "an observation index is outside [0, n_state)");
+    if (h_err == EERR_NOT_SPD)
+      throw Error(ADM_ERR_DEVICE, "H P H^T + R is not positive definite (Cholesky pivot <= 0)");
+  }
+
+  void observe(int N, double const *states, int64_t stride, int64_t n_state, int m, int64_t const *idx, double *hx)
+  {
+    if (N < 1 || m < 1 || !states || !idx || !hx || stride < n_state)
+      throw Error(ADM_ERR_INVALID, "invalid observation arguments");
+    ADM_CK(cudaSetDevice(device));
+    err.alloc(1);
+    ADM_CK(cudaMemsetAsync(err.p, 0, sizeof(int), stream));
+    int64_t const total = (int64_t)N * m;
+    observe_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(states, stride, N, n_state, idx, m, hx,
+                                                                        err.p);
+    ADM_CK(cudaGetLastError());
+    check_err();
+  }
+
+  // W = HA^T (HA HA^T / (N-1) + R)^-1 D / (N-1) from every member's HX.
+  void gain(int N, int m, double const *hx, double const *obs, double const *var, double const *cov,
+            double const *pert, double *Wout)
+  {
+    if (N < 2 || N > kMaxGain)
+      throw Error(ADM_ERR_UNSUPPORTED, "the gain takes 2 to 256 members");
+    if (m < 1 || m > kMaxObs)
+      throw Error(ADM_ERR_UNSUPPORTED, "the analysis takes 1 to 16384 observations");
+    if (!hx || !obs || !pert || !Wout || (!var && !cov))
+      throw Error(ADM_ERR_INVALID, "invalid gain arguments");
+    ADM_CK(cudaSetDevice(device));
+    HA.alloc((size_t)N * m);
+    D.alloc((size_t)N * m);
+    Z.alloc((size_t)N * m);
+    C.alloc((size_t)m * m);
+    err.alloc(1);
+    ADM_CK(cudaMemsetAsync(err.p, 0, sizeof(int), stream));
+    center_kernel<<<(m + 127) / 128, 128, 0, stream>>>(hx, N, m, obs, pert, HA.p, D.p);
+    ADM_CK(cudaGetLastError());
+    double const scale = 1.0 / (N - 1.0);
+    factor(N, m, scale, var, cov);
+    check_err();
+    solve_and_w(N, m, scale, Wout);
+    ADM_CK(cudaStreamSynchronize(stream));
+  }
+
+  void local_sum(int n_local, double const *states, int64_t stride, int64_t n_state, double const *params,
+                 int n_params, double *sum)
+  {
+    if (n_local < 1 || !states || !sum || stride < n_state || n_params < 0 || (n_params > 0 && !params))
+      throw Error(ADM_ERR_INVALID, "invalid local-sum arguments");
+    ADM_CK(cudaSetDevice(device));
+    int64_t const rows = n_state + n_params;
+    local_sum_kernel<<<(unsigned)((rows + 255) / 256), 256, 0, stream>>>(states, stride, n_local, n_state, params,
+                                                                        n_params, sum);
+    ADM_CK(cudaGetLastError());
+    ADM_CK(cudaStreamSynchronize(stream));
+  }
+
+  void partial_update(int n_local, int N, double const *states, int64_t stride, int64_t n_state,
+                      double const *params, int n_params, double const *sum, double const *w_rows, double *U)
+  {
+    if (n_local < 1 || n_local > kMaxN || N < n_local || N > kMaxGain || !states || !sum || !w_rows || !U ||
+        stride < n_state || n_params < 0 || (n_params > 0 && !params))
+      throw Error(ADM_ERR_INVALID, "invalid partial-update arguments (at most 64 local members)");
+    ADM_CK(cudaSetDevice(device));
+    int64_t const rows = n_state + n_params;
+    size_t const smem = sizeof(double) * (size_t)n_local * N;
+    ADM_CK(cudaFuncSetAttribute(partial_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    partial_update_kernel<<<(unsigned)((rows + 255) / 256), 256, smem, stream>>>(
+        states, stride, n_local, N, n_state, params, n_params, sum, w_rows, U);
+    ADM_CK(cudaGetLastError());
+    ADM_CK(cudaStreamSynchronize(stream));
+  }
+
+  void apply(int n_local, double *states, int64_t stride, int64_t n_state, double *params, int n_params,
+             double const *U, uint8_t const *mask)
+  {
+    if (n_local < 1 || !states || !U || stride < n_state || n_params < 0 || (n_params > 0 && !params))
+      throw Error(ADM_ERR_INVALID, "invalid apply arguments");
+    ADM_CK(cudaSetDevice(device));
+    int64_t const total = (int64_t)n_local * (n_state + n_params);
+    apply_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(states, stride, n_local, n_state, params,
+                                                                     n_params, U, mask);
+    ADM_CK(cudaGetLastError());
+    ADM_CK(cudaStreamSynchronize(stream));
+  }
+
+  // C = HA HA^T scale + R and its Cholesky factor (lower, in place)
+  void factor(int N, int m, double scale, double const *var, double const *cov)
+  {
+    int const t32 = (m + 31) / 32;
+    cov_kernel<<<dim3(t32, t32), 256, 0, stream>>>(HA.p, N, m, scale, var, cov, C.p);
+    ADM_CK(cudaGetLastError());
+    for (int k0 = 0; k0 < m; k0 += kNB)
+    {
+      potrf_diag_kernel<<<1, 256, 0, stream>>>(C.p, m, k0, err.p);
+      int const below = m - k0 - kNB;
+      if (below > 0)
+      {
+        trsm_panel_kernel<<<(below + 127) / 128, 128, 0, stream>>>(C.p, m, k0);
+        int const t = (below + 63) / 64;
+        syrk_update_kernel<<<dim3(t, t), 256, 0, stream>>>(C.p, m, k0);
+      }
+      ADM_CK(cudaGetLastError());
+    }
+  }
+
+  // Z = C^-1 D, W = HA^T Z scale
+  void solve_and_w(int N, int m, double scale, double *Wout)
+  {
+    size_t const smem = (size_t)m * sizeof(double);
+    ADM_CK(cudaFuncSetAttribute(solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    solve_kernel<<<N, 256, smem, stream>>>(C.p, m, D.p, Z.p);
+    ADM_CK(cudaGetLastError());
+    w_kernel<<<(N * N * 32 + 255) / 256, 256, 0, stream>>>(HA.p, Z.p, N, m, scale, Wout);
+    ADM_CK(cudaGetLastError());
+  }
 };
 
 } // namespace adm
@@ -484,6 +714,53 @@ int adm_enkf_analysis(adm_enkf *e, int32_t n_members, double *states, int64_t st
     ADM_REQUIRE(e, "null handle");
     reinterpret_cast<adm::Enkf *>(e)->analysis(n_members, states, stride, n_state, params, n_params, n_obs,
                                                obs_index, obs, obs_var, obs_cov, perturbations, update_mask);
+  });
+}
+
+int adm_enkf_observe(adm_enkf *e, int32_t n_members, double const *states, int64_t stride, int64_t n_state,
+                     int32_t n_obs, int64_t const *obs_index, double *hx)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(e, "null handle");
+    reinterpret_cast<adm::Enkf *>(e)->observe(n_members, states, stride, n_state, n_obs, obs_index, hx);
+  });
+}
+
+int adm_enkf_gain(adm_enkf *e, int32_t n_members, int32_t n_obs, double const *hx, double const *obs,
+                  double const *obs_var, double const *obs_cov, double const *perturbations, double *w)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(e, "null handle");
+    reinterpret_cast<adm::Enkf *>(e)->gain(n_members, n_obs, hx, obs, obs_var, obs_cov, perturbations, w);
+  });
+}
+
+int adm_enkf_local_sum(adm_enkf *e, int32_t n_local, double const *states, int64_t stride, int64_t n_state,
+                       double const *params, int32_t n_params, double *sum)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(e, "null handle");
+    reinterpret_cast<adm::Enkf *>(e)->local_sum(n_local, states, stride, n_state, params, n_params, sum);
+  });
+}
+
+int adm_enkf_partial_update(adm_enkf *e, int32_t n_local, int32_t n_members, double const *states, int64_t stride,
+                            int64_t n_state, double const *params, int32_t n_params, double const *sum,
+                            double const *w_rows, double *u)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(e, "null handle");
+    reinterpret_cast<adm::Enkf *>(e)->partial_update(n_local, n_members, states, stride, n_state, params, n_params,
+                                                     sum, w_rows, u);
+  });
+}
+
+int adm_enkf_apply(adm_enkf *e, int32_t n_local, double *states, int64_t stride, int64_t n_state, double *params,
+                   int32_t n_params, double const *u, uint8_t const *update_mask)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(e, "null handle");
+    reinterpret_cast<adm::Enkf *>(e)->apply(n_local, states, stride, n_state, params, n_params, u, update_mask);
   });
 }
 

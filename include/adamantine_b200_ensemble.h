@@ -107,6 +107,36 @@ int adm_enkf_analysis(adm_enkf *e, int32_t n_members, double *states, int64_t st
                       double const *obs_cov, double const *perturbations,
                       uint8_t const *update_mask);
 
+/* Building blocks of the analysis of an ensemble whose members are split over
+ * several GPUs (one process per GPU; the caller does the collectives, see
+ * adamantine_b200/sharded.py): each rank observes its members
+ * (adm_enkf_observe), all-gathers HX, computes the N x N weight matrix
+ * redundantly (adm_enkf_gain), all-reduces the per-rank sums of the
+ * augmented state (adm_enkf_local_sum), forms its
+ * members' contribution to every member's update (adm_enkf_partial_update),
+ * reduce-scatters those contributions and applies its share
+ * (adm_enkf_apply). The result equals adm_enkf_analysis on all members.
+ * Device arrays; each call synchronizes.
+ *   hx      [n_members][n_obs]     H_k x_k
+ *   w       [n_members][n_members] W = HA^T (HA HA^T/(N-1) + R)^-1 D / (N-1)
+ *   sum     [n_state + n_params]   sum of the augmented state (local or all members)
+ *   w_rows  [n_local][n_members]   the local members' rows of W
+ *   u       [n_members][n_state + n_params] (partial) or [n_local][...] (apply) */
+int adm_enkf_observe(adm_enkf *e, int32_t n_members, double const *states, int64_t stride, int64_t n_state,
+                     int32_t n_obs, int64_t const *obs_index, double *hx);
+/* 2 <= n_members <= 256. */
+int adm_enkf_gain(adm_enkf *e, int32_t n_members, int32_t n_obs, double const *hx, double const *obs,
+                  double const *obs_var, double const *obs_cov, double const *perturbations, double *w);
+int adm_enkf_local_sum(adm_enkf *e, int32_t n_local, double const *states, int64_t stride, int64_t n_state,
+                       double const *params, int32_t n_params, double *sum);
+/* n_local <= 64 members on this GPU, n_members in the whole ensemble; sum
+ * over all members (the mean is sum / n_members). */
+int adm_enkf_partial_update(adm_enkf *e, int32_t n_local, int32_t n_members, double const *states, int64_t stride,
+                            int64_t n_state, double const *params, int32_t n_params, double const *sum,
+                            double const *w_rows, double *u);
+int adm_enkf_apply(adm_enkf *e, int32_t n_local, double *states, int64_t stride, int64_t n_state, double *params,
+                   int32_t n_params, double const *u, uint8_t const *update_mask);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,45 @@
+"""numpy implementations of the analysis steps of adamantine_b200.sharded --
+test infrastructure: they let the multi-process exchange run on CPU ranks
+(gloo) and be checked against the single-process restatement."""
+import numpy as np
+import torch
+
+
+class NumpySteps:
+    def observe(self, states, n_state, obs_index):
+        X = states.numpy()
+        idx = obs_index.numpy()
+        return torch.from_numpy(np.stack([X[k, idx[k]] for k in range(X.shape[0])]))
+
+    def gain(self, hx, obs, perturbations, obs_var=None, obs_cov=None):
+        HX = hx.numpy()
+        N = HX.shape[0]
+        HA = HX - HX.mean(axis=0)
+        R = np.diag(obs_var.numpy()) if obs_cov is None else obs_cov.numpy()
+        C = HA.T @ HA / (N - 1.0) + R
+        D = obs.numpy()[None, :] + perturbations.numpy() - HX
+        Z = np.linalg.solve(C, D.T)
+        return torch.from_numpy(HA @ Z / (N - 1.0))
+
+    def local_sum(self, states, n_state, params):
+        s = states.numpy()[:, :n_state].sum(axis=0)
+        if params is not None:
+            s = np.concatenate([s, params.numpy().sum(axis=0)])
+        return torch.from_numpy(s)
+
+    def partial_update(self, states, n_state, params, total, w_rows):
+        X = states.numpy()[:, :n_state]
+        if params is not None:
+            X = np.concatenate([X, params.numpy()], axis=1)
+        N = w_rows.shape[1]
+        A = X - total.numpy()[None, :] / N
+        return torch.from_numpy(w_rows.numpy().T @ A)
+
+    def apply(self, states, n_state, params, u, update_mask=None):
+        U = u.numpy()
+        upd = U[:, :n_state]
+        if update_mask is not None:
+            upd = upd * (update_mask.numpy() != 0)
+        states[:, :n_state] += torch.from_numpy(upd)
+        if params is not None:
+            params += torch.from_numpy(U[:, n_state:])

@@ -174,3 +174,32 @@ def test_enkf_rejects_indefinite_covariance():
         EnKF().analysis(X, 4, bad, torch.tensor(obs, device=dev), torch.tensor(pert, device=dev),
                         obs_var=torch.tensor(var, device=dev))
     assert ex.value.code == 1
+
+
+def test_sharded_steps_equal_fused_analysis():
+    """The device building blocks of the sharded analysis, composed on one
+    rank, give the fused analysis."""
+    from adamantine_b200.sharded import LibrarySteps, ShardedAnalysis
+
+    rng = np.random.default_rng(5)
+    N, n_state, stride, m, p = 16, 4000, 4004, 250, 2
+    states = 300.0 + rng.normal(0, 20.0, (N, stride))
+    params = np.stack([np.exp(rng.normal(0, 0.1, N)), 0.35 * np.exp(rng.normal(0, 0.1, N))], axis=1)
+    idx = np.stack([rng.choice(n_state, m, replace=False) for _ in range(N)]).astype(np.int64)
+    obs = 300.0 + rng.normal(0, 20.0, m)
+    var = np.full(m, 25.0)
+    pert = rng.normal(0, 5.0, (N, m))
+    dev = torch.device("cuda")
+    args = dict(obs_var=torch.tensor(var, device=dev))
+    X1, P1 = torch.tensor(states, device=dev), torch.tensor(params, device=dev)
+    X2, P2 = X1.clone(), P1.clone()
+    enkf = EnKF()
+    enkf.analysis(X1, n_state, torch.tensor(idx, device=dev), torch.tensor(obs, device=dev),
+                  torch.tensor(pert, device=dev), params=P1, **args)
+    ShardedAnalysis(LibrarySteps(enkf))(X2, n_state, torch.tensor(idx, device=dev), torch.tensor(obs, device=dev),
+                                        torch.tensor(pert, device=dev), params=P2, **args)
+    assert rel_max((X2 - torch.tensor(states, device=dev)).cpu().numpy(),
+                   (X1 - torch.tensor(states, device=dev)).cpu().numpy()) <= 1e-11
+    assert rel_max(P2.cpu().numpy() - params, P1.cpu().numpy() - params) <= 1e-11
+    ref, ref_p = enkf_analysis(states, n_state, idx, obs, pert, obs_var=var, params=params)
+    assert rel_max(X2.cpu().numpy() - states, ref - states) <= 1e-9
