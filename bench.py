@@ -180,7 +180,10 @@ def run_ensemble(args, dist, local_rank):
     from adamantine_b200.ensemble import EnKF, Ensemble
     from adamantine_b200.workloads import ensemble_q1, initial_temperature, rng_for, surface_observations
 
-    configs, params = ensemble_q1()
+    world = dist.get_world_size() if dist else 1
+    rank = dist.get_rank() if dist else 0
+    # members per GPU fixed; rank r holds its own seeded members
+    configs, params = ensemble_q1(name="ensemble_q1" if rank == 0 else f"ensemble_q1-rank{rank}")
     n = len(configs)
     grids = [initial_temperature(c, f"ensemble-{k}") for k, c in enumerate(configs)]
     e = Ensemble(configs, device=local_rank)
@@ -218,24 +221,36 @@ def run_ensemble(args, dist, local_rank):
     ij, sigma = surface_observations(e.nodes[:2], layers)
     idx = np.stack([e.node_index(ij[:, 0], ij[:, 1], layers[k]) for k in range(n)]).astype(np.int64)
     rng = rng_for("ensemble-analysis")
-    truth = yb[:, :].mean(dim=0).cpu().numpy()[idx[0]]
+    truth = 300.0 + 50.0 * rng.uniform(0.0, 1.0, idx.shape[1])
     obs = truth + rng.normal(0.0, sigma, idx.shape[1])
-    pert = rng.normal(0.0, sigma, (n, idx.shape[1]))
+    pert = rng.normal(0.0, sigma, (n * world, idx.shape[1]))  # all members, same on every rank
     dev = yb.device
     P = torch.tensor([[p[0], p[1]] for p in params], dtype=torch.float64, device=dev)
     enkf = EnKF(device=local_rank)
-    args_a = (torch.tensor(idx, device=dev), torch.tensor(obs, device=dev), torch.tensor(pert, device=dev))
     var = torch.full((idx.shape[1],), sigma * sigma, dtype=torch.float64, device=dev)
+    obs_d, idx_d, pert_d = (torch.tensor(obs, device=dev), torch.tensor(idx, device=dev),
+                            torch.tensor(pert, device=dev))
+    if world > 1:
+        from adamantine_b200.sharded import LibrarySteps, ShardedAnalysis
+
+        sharded = ShardedAnalysis(LibrarySteps(enkf))
+
+        def analysis(Y, Pk):
+            sharded(Y, e.stride, idx_d, obs_d, pert_d, obs_var=var, params=Pk)
+    else:
+
+        def analysis(Y, Pk):
+            enkf.analysis(Y, e.stride, idx_d, obs_d, pert_d, obs_var=var, params=Pk)
+    analysis(yb.clone(), P.clone())  # warm-up
     ya = yb.clone()
-    enkf.analysis(ya, e.stride, *args_a, obs_var=var, params=P.clone())  # warm-up
-    ya = yb.clone()
+    if dist:
+        dist.barrier()
     torch.cuda.synchronize()
     ev[0].record(stream)
-    enkf.analysis(ya, e.stride, *args_a, obs_var=var, params=P)
+    analysis(ya, P)
     ev[1].record(stream)
     ev[1].synchronize()
     ms_a = ev[0].elapsed_time(ev[1])
-    world = dist.get_world_size() if dist else 1
     if dist:
         tt = torch.tensor([ms_b, ms_l, ms_a], device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -251,6 +266,9 @@ def run_ensemble(args, dist, local_rank):
         "batched_path": "one CUDA graph per step (4 stages)",
         "work_items_per_sweep": e.n_work_items(),
         "enkf_analysis_ms": ms_a, "n_obs": int(idx.shape[1]), "augmented_params": 2,
+        "analysis_members": n * world,
+        "analysis_path": "fused (one GPU)" if world == 1 else "sharded: all-gather HX, all-reduce sums, "
+                                                            "reduce-scatter member updates (NCCL)",
     }
 
 
