@@ -467,6 +467,15 @@ Thermal::~Thermal()
   if (step_graph_)
     cudaGraphExecDestroy(step_graph_);
   cudaStreamSynchronize(stream_);
+  if (copy_in_)
+  {
+    cudaStreamSynchronize(copy_in_);
+    cudaStreamSynchronize(copy_out_);
+    cudaStreamDestroy(copy_in_);
+    cudaStreamDestroy(copy_out_);
+    for (auto e : pipe_ev_)
+      cudaEventDestroy(e);
+  }
   if (graph_stream_)
   {
     cudaStreamSynchronize(graph_stream_);
@@ -554,6 +563,7 @@ void Thermal::rebuild()
         }
   }
   colour_off_[8] = (int)work_.size();
+  ++work_version_;
   work_d_.alloc(std::max<size_t>(1, work_.size()));
   if (!work_.empty())
     ADM_CK(cudaMemcpyAsync(work_d_.p, work_.data(), work_.size() * sizeof(TileWork), cudaMemcpyHostToDevice, stream_));
@@ -1327,6 +1337,7 @@ int64_t Thermal::activate_in_boxes(DeviceBoxes const &boxes, int64_t b0, int64_t
         }
   }
   colour_off_[8] = (int)work_.size();
+  ++work_version_;
   work_d_.alloc(std::max<size_t>(1, work_.size()));
   ADM_CK(cudaMemcpyAsync(work_d_.p, work_.data(), work_.size() * sizeof(TileWork), cudaMemcpyHostToDevice, stream_));
   ADM_CK(cudaMemcpyAsync(tile_nbr_d_.p, topo_.tile_nbr.data(), mesh_.n_tiles * sizeof(uint32_t),
@@ -1514,14 +1525,110 @@ void Thermal::bind_stage_vectors(double *za, double *zb, double *s, double *f0, 
   upload_member();
 }
 
+namespace
+{
+bool is_pinned(void const *p)
+{
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess)
+  {
+    (void)cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+} // namespace
+
 void Thermal::vmult_host(double *dst_host, double const *src_host)
 {
+  if (!setup_done_)
+    throw Error(ADM_ERR_INVALID, "setup() has not been called");
+  ADM_CK(cudaSetDevice(device_));
   size_t const n = mesh_.n_nodes;
   stage_in_.alloc(n);
   stage_out_.alloc(n);
-  ADM_CK(cudaMemcpyAsync(stage_in_.p, src_host, n * sizeof(double), cudaMemcpyHostToDevice, stream_));
-  vmult(stage_out_.p, stage_in_.p, false);
-  ADM_CK(cudaMemcpyAsync(dst_host, stage_out_.p, n * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+  int const nt2 = mesh_.nt[2];
+  if (nt2 < 2 || colour_off_[8] == 0 || !is_pinned(src_host) || !is_pinned(dst_host))
+  {
+    ADM_CK(cudaMemcpyAsync(stage_in_.p, src_host, n * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    vmult(stage_out_.p, stage_in_.p, false);
+    ADM_CK(cudaMemcpyAsync(dst_host, stage_out_.p, n * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    ADM_CK(cudaStreamSynchronize(stream_));
+    return;
+  }
+  // Pinned host buffers: the vector moves in z-slabs on two copy streams and
+  // the tiles of each slab run (atomic schedule) as soon as their nodes have
+  // arrived, so the host-to-device copy, the kernel and the device-to-host
+  // copy of earlier slabs overlap.
+  if (zwork_version_ != work_version_ || zwork_.empty())
+  {
+    zwork_.assign(work_.begin(), work_.end());
+    int const per_layer = mesh_.nt[0] * mesh_.nt[1];
+    std::stable_sort(zwork_.begin(), zwork_.end(),
+                     [&](TileWork const &a, TileWork const &b) { return a.tile / per_layer < b.tile / per_layer; });
+    zwork_d_.alloc(zwork_.size());
+    ADM_CK(cudaMemcpyAsync(zwork_d_.p, zwork_.data(), zwork_.size() * sizeof(TileWork), cudaMemcpyHostToDevice,
+                           stream_));
+    zwork_version_ = work_version_;
+  }
+  if (!copy_in_)
+  {
+    ADM_CK(cudaStreamCreateWithFlags(&copy_in_, cudaStreamNonBlocking));
+    ADM_CK(cudaStreamCreateWithFlags(&copy_out_, cudaStreamNonBlocking));
+    for (auto &e : pipe_ev_)
+      ADM_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  int const chunks = std::min(kPipeChunks, nt2);
+  int const per_layer = mesh_.nt[0] * mesh_.nt[1];
+  size_t const row = (size_t)mesh_.pitch * mesh_.nn[1]; // doubles per node z-row
+  int const rows_per_layer = mesh_.deg * mesh_.tz;
+  int const nrows = mesh_.nn[2];
+  cudaEvent_t const start = pipe_ev_[2 * kPipeChunks], done = pipe_ev_[2 * kPipeChunks + 1];
+  ADM_CK(cudaEventRecord(start, stream_));
+  ADM_CK(cudaStreamWaitEvent(copy_in_, start, 0));
+  ADM_CK(cudaStreamWaitEvent(copy_out_, start, 0));
+  ADM_CK(cudaMemsetAsync(stage_out_.p, 0, n * sizeof(double), stream_));
+  prepare_stage(0.0);
+  KernelArgs a = base_args();
+  a.mode = 0;
+  a.atomic = 1;
+  a.vsrc = stage_in_.p;
+  a.vdst = stage_out_.p;
+  CUtensorMap const map = brick_map(mesh_, stage_in_.p, 1, n);
+  int rows_in = 0, rows_out = 0;
+  size_t item = 0;
+  for (int c = 0; c < chunks; ++c)
+  {
+    int const tz1 = (int)((int64_t)(c + 1) * nt2 / chunks);
+    // node rows the tiles of layers < tz1 read, and the rows that are final
+    int const need = std::min(nrows, rows_per_layer * tz1 + 1);
+    int const final_rows = c == chunks - 1 ? nrows : rows_per_layer * tz1;
+    cudaEvent_t const e_in = pipe_ev_[2 * c], e_k = pipe_ev_[2 * c + 1];
+    if (need > rows_in)
+      ADM_CK(cudaMemcpyAsync(stage_in_.p + rows_in * row, src_host + rows_in * row, (need - rows_in) * row * sizeof(double),
+                             cudaMemcpyHostToDevice, copy_in_));
+    rows_in = std::max(rows_in, need);
+    ADM_CK(cudaEventRecord(e_in, copy_in_));
+    ADM_CK(cudaStreamWaitEvent(stream_, e_in, 0));
+    size_t end = item;
+    while (end < zwork_.size() && zwork_[end].tile / per_layer < tz1)
+      ++end;
+    if (end > item)
+    {
+      a.work = zwork_d_.p + item;
+      launch_tile(mesh_.deg, ns_, poly_p_, map, a, (int)(end - item), stream_);
+      ADM_CK(cudaGetLastError());
+    }
+    item = end;
+    ADM_CK(cudaEventRecord(e_k, stream_));
+    ADM_CK(cudaStreamWaitEvent(copy_out_, e_k, 0));
+    if (final_rows > rows_out)
+      ADM_CK(cudaMemcpyAsync(dst_host + rows_out * row, stage_out_.p + rows_out * row,
+                             (final_rows - rows_out) * row * sizeof(double), cudaMemcpyDeviceToHost, copy_out_));
+    rows_out = std::max(rows_out, final_rows);
+  }
+  ADM_CK(cudaEventRecord(done, copy_out_));
+  ADM_CK(cudaStreamWaitEvent(stream_, done, 0));
   ADM_CK(cudaStreamSynchronize(stream_));
 }
 

@@ -304,6 +304,14 @@ private:
   DevBuf<TileWork> work_d_;
   MemberData md_{};
 
+  // z-slab pipeline of vmult_host: tiles sorted by z layer, copy streams
+  static constexpr int kPipeChunks = 8;
+  std::vector<TileWork> zwork_;
+  DevBuf<TileWork> zwork_d_;
+  uint64_t work_version_ = 0, zwork_version_ = ~0ull;
+  cudaStream_t copy_in_ = nullptr, copy_out_ = nullptr;
+  cudaEvent_t pipe_ev_[2 * kPipeChunks + 2] = {};
+
   // captured step graph for evolve_n_steps
   cudaGraphExec_t step_graph_ = nullptr;
   double *graph_solution_ = nullptr;

@@ -524,7 +524,7 @@ def run_ours(args, rank, world, local_rank):
                           "flop_per_vmult": fp64_flop,
                           "peak_kind": "measured FP64 FMA rate (adm_diag_fp64_fma_rate) on this GPU"},
         "e2e": {"value": e2e_val, "unit": "GDoF/s", "h2d_bytes_per_step": 8 * g.m(),
-                "d2h_bytes_per_step": 8 * g.m(), "path": "adm_vmult_host (pinned host buffers)"},
+                "d2h_bytes_per_step": 8 * g.m(), "path": "adm_vmult_host (pinned host buffers: z-slab copies overlapped with the kernel)"},
         # per vmult: the stage-prepare kernel + one tile launch (atomic
         # schedule) or 8 colour launches (coloured schedule)
         "gpu_launches": args.steps * (2 if schedule == 1 else 9),

@@ -130,7 +130,11 @@ int adm_set_time(adm_thermal *h, double t);
 int adm_vmult(adm_thermal *h, double *dst, double const *src);
 /* ThermalOperatorBase::vmult_add (source/ThermalOperator.templates.hh:188-225). */
 int adm_vmult_add(adm_thermal *h, double *dst, double const *src);
-/* vmult on host buffers: copy in, apply, copy out, synchronize. */
+/* vmult on host buffers: copy in, apply, copy out, synchronize. With pinned
+ * (page-locked) buffers the vector moves in z-slabs on two copy streams and
+ * the tiles of each slab run as soon as their nodes have arrived (node sums
+ * by atomics), so both copies and the kernel overlap; pageable buffers take
+ * the plain path. */
 int adm_vmult_host(adm_thermal *h, double *dst_host, double const *src_host);
 
 /* ThermalOperatorBase::compute_inverse_mass_matrix
