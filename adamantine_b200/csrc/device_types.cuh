@@ -145,6 +145,7 @@ struct KernelArgs
   double *y_override; // caller-owned solution vector (member 0), or null
   int mode;     // 0 vmult, 1 vmult_add, 2 stage
   int atomic;   // 1: all colours in one launch, node sums by atomics
+  int blocked;  // 1: each CTA takes one contiguous run of work items
   int stage;
   int last;     // last stage of the step (updates y)
   int n_stages; // 1 forward Euler

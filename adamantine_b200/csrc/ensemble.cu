@@ -130,6 +130,15 @@ void Ensemble::setup()
   if (!work_.empty())
     ADM_CK(cudaMemcpyAsync(work_d_.p, work_.data(), work_.size() * sizeof(TileWork),
                            cudaMemcpyHostToDevice, stream_));
+  // the atomic schedule's list: member-major, each member's tiles in order
+  awork_.clear();
+  for (int i = 0; i < n_members(); ++i)
+    for (TileWork const &tw : members_[i]->work_)
+      awork_.push_back(TileWork{i, tw.tile});
+  awork_d_.alloc(std::max<size_t>(1, awork_.size()));
+  if (!awork_.empty())
+    ADM_CK(cudaMemcpyAsync(awork_d_.p, awork_.data(), awork_.size() * sizeof(TileWork),
+                           cudaMemcpyHostToDevice, stream_));
   ADM_CK(cudaStreamSynchronize(stream_));
   dirty_ = true;
   drop_graph();
@@ -178,17 +187,21 @@ void Ensemble::launch_step(double *solutions)
     CUtensorMap const map = brick_map(members_[0]->mesh_, src, n, stride_);
     if (schedule_ == Thermal::kScheduleAtomic)
     {
+      // member-major list, one contiguous run per CTA: a CTA changes member
+      // (and reloads the material constants) at most once or twice
       a.atomic = 1;
+      a.blocked = 1;
       ADM_CK(cudaMemsetAsync(acc_.p, 0, stride_ * (size_t)n * sizeof(double), stream_));
-      if (colour_off_[8] > 0)
+      if (!awork_.empty())
       {
-        a.work = work_d_.p;
-        launch_tile(deg_, ns_, poly_p_, map, a, colour_off_[8], stream_);
+        a.work = awork_d_.p;
+        launch_tile(deg_, ns_, poly_p_, map, a, (int)awork_.size(), stream_);
         ADM_CK(cudaGetLastError());
       }
       launch_stage_finalize(a, stride_, n, stream_);
       continue;
     }
+    a.blocked = 1; // each colour's list is member-major
     for (int col = 0; col < 8; ++col)
     {
       int const count = colour_off_[col + 1] - colour_off_[col];

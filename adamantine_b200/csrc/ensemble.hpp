@@ -76,8 +76,8 @@ private:
 
   DevBuf<double> za_, zb_, s_, f0_, acc_;
   DevBuf<MemberData> md_d_;
-  DevBuf<TileWork> work_d_;
-  std::vector<TileWork> work_;
+  DevBuf<TileWork> work_d_, awork_d_;
+  std::vector<TileWork> work_, awork_;
   int colour_off_[9] = {0};
   double *bound_ = nullptr; // solutions array the member table points at
   bool dirty_ = true;       // member table must be re-uploaded

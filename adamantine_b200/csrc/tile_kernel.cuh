@@ -443,11 +443,28 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
     sp.member = -1;
   }
   __syncthreads();
-  if (tid == 0 && (int)blockIdx.x < n_items)
-    issue(0, blockIdx.x);
+  // work distribution: strided (CTA b takes items b, b + grid, ...) or, with
+  // args.blocked, one contiguous run of items per CTA (consecutive items of a
+  // member-major list then share the member's constants)
+  int first, last, step;
+  if (args.blocked)
+  {
+    int const per = (n_items + (int)gridDim.x - 1) / (int)gridDim.x;
+    first = (int)blockIdx.x * per;
+    last = min(first + per, n_items);
+    step = 1;
+  }
+  else
+  {
+    first = blockIdx.x;
+    last = n_items;
+    step = gridDim.x;
+  }
+  if (tid == 0 && first < last)
+    issue(0, first);
 
   int it = 0;
-  for (int item = blockIdx.x; item < n_items; item += gridDim.x, ++it)
+  for (int item = first; item < last; item += step, ++it)
   {
     int const buf = it & 1;
     double const *brick = smem + buf * T_::BRICKP;
@@ -463,10 +480,10 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
 
     // prefetch the next item's brick into the other buffer (its previous
     // contents were consumed before the barrier that ended the last item)
-    if (tid == 0 && item + (int)gridDim.x < n_items)
+    if (tid == 0 && item + step < last)
     {
       fence_proxy_async();
-      issue(buf ^ 1, item + gridDim.x);
+      issue(buf ^ 1, item + step);
     }
     if (sp.member != w.member)
     {
@@ -512,7 +529,7 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
       {
         atomicCAS(md.error, 0, (int)DERR_TMA_TIMEOUT);
         // let a prefetch still in flight land before the CTA leaves
-        if (item + (int)gridDim.x < n_items)
+        if (item + step < last)
           mbar_wait(&bars[buf ^ 1], (unsigned)(((it + 1) >> 1) & 1));
       }
       return;
