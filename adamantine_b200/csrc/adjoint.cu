@@ -280,6 +280,7 @@ public:
             A.s_in = Sstore_.p + slot * qn;
             A.lam_s_out = ls_a_.p;
             A.lam_s_in = ls_b_.p;
+            A.powder_start = init_mode_.p;
           }
           A.lam_y = lamYi;
           A.grad = grad_d_.p;

@@ -41,6 +41,7 @@ struct AdjArgs
   double const *s_in;      // [C][NN] powder ratio before the stage (3 states)
   double const *lam_s_out; // [C][NN] adjoint of the powder ratio after the stage
   double *lam_s_in;        // [C][NN] adjoint of the powder ratio before the stage
+  uint8_t const *powder_start; // [C] powder mode of the run's initial state (0: none), or null
   double *lam_y;           // node vector: += the transpose applied to mu
   double *grad;            // [3] += log-derivatives: k scale, c_p scale, source
 };
@@ -392,6 +393,7 @@ __global__ void __launch_bounds__(TD<DEG>::NT, 2)
     if (active)
     {
       size_t const qbase = c * NN + (size_t)NQS * slab;
+      bool const no_powder = NS == 3 && A.powder_start && A.powder_start[c] == 0;
       double const hx2 = args.inv_h[0] * args.inv_h[0], hy2 = args.inv_h[1] * args.inv_h[1],
                    hz2 = args.inv_h[2] * args.inv_h[2];
   #pragma unroll
@@ -418,11 +420,22 @@ __global__ void __launch_bounds__(TD<DEG>::NT, 2)
           Q = beam_sum(sp, px, py, pz);
         }
         double const JxW = args.qw[qa] * args.qw[qb] * args.qw[slab] * args.vol;
-        double const s_in = NS == 3 ? A.s_in[qbase + i] : 0.0;
-        double const lam_out = NS == 3 ? A.lam_s_out[qbase + i] : 0.0;
-        AdjQp const o = adj_qp<NS>(sp, mat, T, mu, gx, gy, gz, mx, my, mz, s_in, lam_out, JxW, Q, hx2, hy2, hz2);
-        if (NS == 3)
-          A.lam_s_in[qbase + i] = o.lsin;
+        AdjQp o;
+        if (NS == 3 && no_powder)
+        {
+          // a cell without powder at the start keeps s = 0 (s' = min(1 - l,
+          // 0) = 0): its points are solid/liquid mixtures and the powder
+          // adjoint there never reaches the temperature or the parameters
+          o = adj_qp<NS == 3 ? 2 : NS>(sp, mat, T, mu, gx, gy, gz, mx, my, mz, 0.0, 0.0, JxW, Q, hx2, hy2, hz2);
+        }
+        else
+        {
+          double const s_in = NS == 3 ? A.s_in[qbase + i] : 0.0;
+          double const lam_out = NS == 3 ? A.lam_s_out[qbase + i] : 0.0;
+          o = adj_qp<NS>(sp, mat, T, mu, gx, gy, gz, mx, my, mz, s_in, lam_out, JxW, Q, hx2, hy2, hz2);
+          if (NS == 3)
+            A.lam_s_in[qbase + i] = o.lsin;
+        }
         g_k += o.gk;
         g_q += o.gq;
         g_c += o.gc;
