@@ -190,6 +190,7 @@ public:
   // Forward run from the captured initial phase state: J and the final field.
   double objective(double t0, double dt, int n_steps, double const *y0, double *y_final)
   {
+    NvtxRange const nvtx_range("adm::adjoint_objective");
     check_run(n_steps, 1);
     forward(t0, dt, n_steps, y0, 0);
     double J = 0.0;
@@ -202,6 +203,7 @@ public:
 
   double gradient(double t0, double dt, int n_steps, int K, double const *y0, double *grad, double *y_final)
   {
+    NvtxRange const nvtx_range("adm::adjoint_gradient");
     check_run(n_steps, K);
     Thermal &t = th_;
     cudaStream_t const st = t.stream_;

@@ -90,3 +90,47 @@ extern "C" int adm_diag_fp64_fma_rate(int device, double *tflops)
     *tflops = 2.0 * 8.0 * iters * (double)blocks * threads / (best * 1e-3) / 1e12;
   return rc;
 }
+
+namespace
+{
+// The bounded mbarrier wait of the tile kernels on a barrier that nothing
+// arrives at: the wait must give up after `limit` polls and report it.
+__global__ void wait_timeout_kernel(long long limit, int *status)
+{
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0)
+  {
+    adm::mbar_init(&bar, 1);
+    adm::fence_mbar_init();
+  }
+  __syncthreads();
+  bool const arrived = adm::mbar_wait(&bar, 0u, limit);
+  if (__syncthreads_or(!arrived) && threadIdx.x == 0)
+    *status = 1;
+}
+} // namespace
+
+extern "C" int adm_diag_wait_timeout(long long limit, int32_t *timed_out)
+{
+  if (!timed_out || limit < 1 || limit > (1ll << 26))
+    return ADM_ERR_INVALID;
+  *timed_out = 0;
+  int *d = nullptr;
+  if (cudaMalloc(&d, sizeof(int)) != cudaSuccess)
+    return ADM_ERR_ALLOC;
+  int rc = ADM_OK;
+  if (cudaMemset(d, 0, sizeof(int)) != cudaSuccess)
+    rc = ADM_ERR_CUDA;
+  if (rc == ADM_OK)
+  {
+    wait_timeout_kernel<<<1, 64>>>(limit, d);
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess)
+      rc = ADM_ERR_CUDA;
+  }
+  int h = 0;
+  if (rc == ADM_OK && cudaMemcpy(&h, d, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = ADM_ERR_CUDA;
+  cudaFree(d);
+  *timed_out = h;
+  return rc;
+}

@@ -503,6 +503,7 @@ struct Enkf
                 int m, int64_t const *idx, double const *obs, double const *var, double const *cov,
                 double const *pert, uint8_t const *mask)
   {
+    NvtxRange const nvtx_range("adm::enkf_analysis");
     if (N < 2 || N > kMaxN)
       throw Error(ADM_ERR_UNSUPPORTED, "the analysis takes 2 to 64 members");
     if (m < 1 || m > kMaxObs)
@@ -588,6 +589,7 @@ struct Enkf
   void gain(int N, int m, double const *hx, double const *obs, double const *var, double const *cov,
             double const *pert, double *Wout)
   {
+    NvtxRange const nvtx_range("adm::enkf_gain");
     if (N < 2 || N > kMaxGain)
       throw Error(ADM_ERR_UNSUPPORTED, "the gain takes 2 to 256 members");
     if (m < 1 || m > kMaxObs)

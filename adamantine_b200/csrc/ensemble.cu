@@ -216,6 +216,7 @@ void Ensemble::launch_step(double *solutions)
 
 double Ensemble::evolve_one_time_step(double t, double dt, double *solutions)
 {
+  NvtxRange const nvtx_range("adm::ensemble_step");
   if (!setup_done_)
     throw Error(ADM_ERR_INVALID, "setup() has not been called");
   ADM_CK(cudaSetDevice(device_));
@@ -228,6 +229,7 @@ double Ensemble::evolve_one_time_step(double t, double dt, double *solutions)
 
 double Ensemble::evolve_looped(double t, double dt, double *solutions)
 {
+  NvtxRange const nvtx_range("adm::ensemble_looped");
   if (!setup_done_)
     throw Error(ADM_ERR_INVALID, "setup() has not been called");
   for (int i = 0; i < n_members(); ++i)
@@ -237,6 +239,7 @@ double Ensemble::evolve_looped(double t, double dt, double *solutions)
 
 double Ensemble::evolve_n_steps(double t, double dt, int n, double *solutions)
 {
+  NvtxRange const nvtx_range("adm::ensemble_n_steps");
   if (!setup_done_)
     throw Error(ADM_ERR_INVALID, "setup() has not been called");
   if (n <= 0)

@@ -903,6 +903,7 @@ void Thermal::set_time(double t)
 
 void Thermal::vmult(double *dst, double const *src, bool add)
 {
+  NvtxRange const nvtx_range("adm::vmult");
   if (!setup_done_)
     throw Error(ADM_ERR_INVALID, "setup() has not been called");
   ADM_CK(cudaSetDevice(device_));
@@ -960,6 +961,7 @@ void Thermal::launch_step(double *solution)
 
 double Thermal::evolve_one_time_step(double t, double dt, double *solution)
 {
+  NvtxRange const nvtx_range("adm::evolve_one_time_step");
   if (!setup_done_)
     throw Error(ADM_ERR_INVALID, "setup() has not been called");
   ADM_CK(cudaSetDevice(device_));
@@ -972,6 +974,7 @@ double Thermal::evolve_one_time_step(double t, double dt, double *solution)
 
 double Thermal::evolve_n_steps(double t, double dt, int n, double *solution)
 {
+  NvtxRange const nvtx_range("adm::evolve_n_steps");
   if (!setup_done_)
     throw Error(ADM_ERR_INVALID, "setup() has not been called");
   if (n <= 0)
@@ -1183,6 +1186,7 @@ void Thermal::activate_cells(int64_t const *cells, int64_t n, double new_tempera
 int64_t Thermal::activate_in_boxes(DeviceBoxes const &boxes, int64_t b0, int64_t b1, double new_temperature,
                                    double *solution)
 {
+  NvtxRange const nvtx_range("adm::activate_in_boxes");
   if (!setup_done_)
     throw Error(ADM_ERR_INVALID, "setup() has not been called");
   if (b0 < 0 || b1 > boxes.n || b0 > b1)
@@ -1467,6 +1471,7 @@ void Thermal::restore_phase(PhaseSnapshot const &p)
 // history saved before and restored after) and keeps the fastest.
 int Thermal::autotune(double const *field, double *ms_out)
 {
+  NvtxRange const nvtx_range("adm::autotune");
   if (!setup_done_)
     throw Error(ADM_ERR_INVALID, "setup() has not been called");
   ADM_CK(cudaSetDevice(device_));
@@ -1541,6 +1546,7 @@ bool is_pinned(void const *p)
 
 void Thermal::vmult_host(double *dst_host, double const *src_host)
 {
+  NvtxRange const nvtx_range("adm::vmult_host");
   if (!setup_done_)
     throw Error(ADM_ERR_INVALID, "setup() has not been called");
   ADM_CK(cudaSetDevice(device_));

@@ -15,6 +15,7 @@
 
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstdint>
 #include <stdexcept>
@@ -31,6 +32,15 @@ struct Error : std::runtime_error
 };
 
 void check_cuda(cudaError_t e, char const *what, char const *file, int line);
+
+// NVTX range for profilers (nsys / ncu timelines); free when no tool listens.
+struct NvtxRange
+{
+  explicit NvtxRange(char const *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(NvtxRange const &) = delete;
+  NvtxRange &operator=(NvtxRange const &) = delete;
+};
 #define ADM_CK(x) ::adm::check_cuda((x), #x, __FILE__, __LINE__)
 
 template <class T>

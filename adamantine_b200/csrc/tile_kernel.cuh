@@ -118,9 +118,9 @@ __device__ __forceinline__ void tma_load_brick(void *dst, CUtensorMap const *map
 // Bounded wait on an mbarrier phase: false after ~kSpinLimit polls (the
 // caller then reports DERR_TMA_TIMEOUT instead of hanging).
 constexpr long long kSpinLimit = 1ll << 26;
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity)
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, long long limit = kSpinLimit)
 {
-  for (long long i = 0; i < kSpinLimit; ++i)
+  for (long long i = 0; i < limit; ++i)
     if (mbar_try_wait(bar, parity))
       return true;
   return false;

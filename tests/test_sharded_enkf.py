@@ -69,3 +69,43 @@ def test_two_rank_exchange_equals_dense_analysis(tmp_path):
     assert np.allclose(X, ref, rtol=1e-12, atol=1e-9)
     assert np.allclose(P, ref_p, rtol=1e-12, atol=1e-12)
     assert not np.allclose(X, states)
+
+
+def worker_lost_rank(rank, port, out):
+    """Rank 1 leaves before the analysis; rank 0's collective must end with an
+    error (short process-group timeout), not wait for ever."""
+    import datetime
+    import sys
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    for pth in (here, os.path.join(os.path.dirname(here), "oracle"), os.path.dirname(here)):
+        sys.path.insert(0, pth)
+    from sharded_steps import NumpySteps
+
+    from adamantine_b200.sharded import ShardedAnalysis
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=WORLD, timeout=datetime.timedelta(seconds=10))
+    if rank == 1:
+        return  # the rank dies between steps, with nothing in flight
+    states, params, idx, obs, var, pert, mask, n_state = problem()
+    nl = states.shape[0] // WORLD
+    outcome = "completed"
+    try:
+        ShardedAnalysis(NumpySteps())(torch.from_numpy(states[:nl].copy()), n_state, torch.from_numpy(idx[:nl]),
+                                      torch.from_numpy(obs), torch.from_numpy(pert), obs_var=torch.from_numpy(var))
+    except Exception as e:  # noqa: BLE001 -- any collective error is the expected outcome
+        outcome = "error: " + type(e).__name__
+    with open(os.path.join(out, "outcome.txt"), "w") as fh:
+        fh.write(outcome)
+
+
+def test_lost_rank_ends_the_analysis_with_an_error(tmp_path):
+    import time
+
+    t0 = time.time()
+    mp.spawn(worker_lost_rank, args=(free_port(), str(tmp_path)), nprocs=WORLD, join=True)
+    outcome = open(os.path.join(tmp_path, "outcome.txt")).read()
+    assert outcome.startswith("error"), outcome
+    assert time.time() - t0 < 120
