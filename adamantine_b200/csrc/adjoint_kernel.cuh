@@ -215,8 +215,8 @@ __global__ void __launch_bounds__(TD<DEG>::NT, 2)
 
   auto issue = [&](int buf, int item) {
     TileWork const wi = args.work[item];
-    int const tl = wi.tile;
-    int const x = DEG * TX * (tl % nt0), y = DEG * TY * ((tl / nt0) % nt1), z = DEG * TZ * (tl / (nt0 * nt1));
+    int const x = DEG * TX * (int)(wi.xyz & 2047u), y = DEG * TY * (int)((wi.xyz >> 11) & 2047u),
+              z = DEG * TZ * (int)(wi.xyz >> 22);
     mbar_arrive_expect_tx(&bars[buf], 2 * kBoxBytes);
     tma_load_brick(smem + (2 * buf) * T_::BRICKP, &ymap, x, y, z, 0, &bars[buf]);
     tma_load_brick(smem + (2 * buf + 1) * T_::BRICKP, &mmap, x, y, z, 0, &bars[buf]);
@@ -241,8 +241,7 @@ __global__ void __launch_bounds__(TD<DEG>::NT, 2)
     double const *const mb = smem + (2 * buf + 1) * T_::BRICKP;
     TileWork const w = args.work[item];
     MemberData const &md = args.members[w.member];
-    int const tile = w.tile;
-    int const tix = tile % nt0, tiy = (tile / nt0) % nt1, tiz = tile / (nt0 * nt1);
+    int const tix = w.xyz & 2047u, tiy = (w.xyz >> 11) & 2047u, tiz = w.xyz >> 22;
     int const ncx0 = TX * tix, ncy0 = TY * tiy, ncz0 = TZ * tiz;
     int const nx0 = DEG * ncx0, ny0 = DEG * ncy0, nz0 = DEG * ncz0;
 

@@ -132,7 +132,14 @@ struct TileWork
 {
   int32_t member;
   int32_t tile;
+  uint32_t xyz; // tile coordinates packed by pack_tile (no division in kernels)
 };
+
+// Tile coordinates in one word: x in bits 0-10, y in 11-21, z in 22-31.
+__host__ __device__ inline uint32_t pack_tile(int tx, int ty, int tz)
+{
+  return (uint32_t)tx | ((uint32_t)ty << 11) | ((uint32_t)tz << 22);
+}
 
 // Mesh and stage description passed by value to the tile kernel.
 struct KernelArgs

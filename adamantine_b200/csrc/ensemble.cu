@@ -122,7 +122,7 @@ void Ensemble::setup()
     {
       Thermal const &m = *members_[i];
       for (int k = m.colour_off_[col]; k < m.colour_off_[col + 1]; ++k)
-        work_.push_back(TileWork{i, m.work_[k].tile});
+        work_.push_back(TileWork{i, m.work_[k].tile, m.work_[k].xyz});
     }
   }
   colour_off_[8] = (int)work_.size();
@@ -134,7 +134,7 @@ void Ensemble::setup()
   awork_.clear();
   for (int i = 0; i < n_members(); ++i)
     for (TileWork const &tw : members_[i]->work_)
-      awork_.push_back(TileWork{i, tw.tile});
+      awork_.push_back(TileWork{i, tw.tile, tw.xyz});
   awork_d_.alloc(std::max<size_t>(1, awork_.size()));
   if (!awork_.empty())
     ADM_CK(cudaMemcpyAsync(awork_d_.p, awork_.data(), awork_.size() * sizeof(TileWork),

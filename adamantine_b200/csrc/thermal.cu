@@ -186,6 +186,8 @@ void Mesh::init(adm_config const &cfg)
     origin[d] = cfg.origin[d];
     nt[d] = (nc[d] + t[d] - 1) / t[d];
   }
+  if (nt[0] > 2047 || nt[1] > 2047 || nt[2] > 1023)
+    throw Error(ADM_ERR_INVALID, "mesh has too many cell tiles along one axis");
   pitch = (nn[0] + 3) / 4 * 4;
   n_nodes = (size_t)pitch * nn[1] * nn[2];
   n_cells = (size_t)nc[0] * nc[1] * nc[2];
@@ -559,7 +561,7 @@ void Thermal::rebuild()
         {
           size_t const tile = tx + (size_t)mesh_.nt[0] * (ty + (size_t)mesh_.nt[1] * tz);
           if (topo_.tile_active[tile])
-            work_.push_back(TileWork{0, (int32_t)tile});
+            work_.push_back(TileWork{0, (int32_t)tile, pack_tile(tx, ty, tz)});
         }
   }
   colour_off_[8] = (int)work_.size();
@@ -1337,7 +1339,7 @@ int64_t Thermal::activate_in_boxes(DeviceBoxes const &boxes, int64_t b0, int64_t
         {
           size_t const tile = tx + (size_t)mesh_.nt[0] * (ty + (size_t)mesh_.nt[1] * tz);
           if (ta[tile])
-            work_.push_back(TileWork{0, (int32_t)tile});
+            work_.push_back(TileWork{0, (int32_t)tile, pack_tile(tx, ty, tz)});
         }
   }
   colour_off_[8] = (int)work_.size();

@@ -428,8 +428,7 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
 
   auto issue = [&](int buf, int item) {
     TileWork const wi = args.work[item];
-    int const tile = wi.tile;
-    int const tix = tile % nt0, tiy = (tile / nt0) % nt1, tiz = tile / (nt0 * nt1);
+    int const tix = wi.xyz & 2047u, tiy = (wi.xyz >> 11) & 2047u, tiz = wi.xyz >> 22;
     mbar_arrive_expect_tx(&bars[buf], kBoxBytes);
     tma_load_brick(smem + buf * T_::BRICKP, &tmap, DEG * TX * tix, DEG * TY * tiy, DEG * TZ * tiz,
                    wi.member, &bars[buf]);
@@ -472,7 +471,7 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
     MemberData const &md = args.members[w.member];
     MaterialDesc const *gm = md.mat;
     int const tile = w.tile;
-    int const tix = tile % nt0, tiy = (tile / nt0) % nt1, tiz = tile / (nt0 * nt1);
+    int const tix = w.xyz & 2047u, tiy = (w.xyz >> 11) & 2047u, tiz = w.xyz >> 22;
     int const colour = (tix & 1) | ((tiy & 1) << 1) | ((tiz & 1) << 2);
     int const ncx0 = TX * tix, ncy0 = TY * tiy, ncz0 = TZ * tiz;      // first cell
     int const nx0 = DEG * ncx0, ny0 = DEG * ncy0, nz0 = DEG * ncz0; // first node
