@@ -96,6 +96,10 @@ SIGNATURES = {
     "adm_enkf_local_sum": [_VP, ctypes.c_int32, _VP, ctypes.c_int64, ctypes.c_int64, _VP, ctypes.c_int32, _VP],
     "adm_enkf_partial_update": [_VP, ctypes.c_int32, ctypes.c_int32, _VP, ctypes.c_int64, ctypes.c_int64, _VP,
                                 ctypes.c_int32, _VP, _VP, _VP],
+    "adm_enkf_partial_update_localized": [_VP, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _VP,
+                                          ctypes.c_int64, ctypes.c_int64, _VP, ctypes.c_int32, _VP, _VP, _VP],
+    "adm_enkf_set_localization": [_VP, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, _VP, _VP, _VP, _VP,
+                                  ctypes.c_int64],
     "adm_enkf_apply": [_VP, ctypes.c_int32, _VP, ctypes.c_int64, ctypes.c_int64, _VP, ctypes.c_int32, _VP, _VP],
     "adm_enkf_analysis": [_VP, ctypes.c_int32, _VP, ctypes.c_int64, ctypes.c_int64, _VP, ctypes.c_int32,
                           ctypes.c_int32, _VP, _VP, _VP, _VP, _VP, _VP],

@@ -15,11 +15,30 @@
 //   W   = HA^T Z / (N - 1)           (N x N)
 //   x_k += A W[:, k]                 (one pass over the states)
 // which is the same matrix product evaluated in a different order.
+//
+// With a diagonal R and no localization the m x m system is not formed at
+// all: by the Sherman-Morrison-Woodbury identity
+//   HA^T (HA HA^T / (N-1) + R)^-1 / (N-1) = ((N-1) I + G)^-1 HA^T R^-1,
+//   G = HA^T R^-1 HA   (N x N),
+// so W = ((N-1) I + G)^-1 E with E = HA^T R^-1 D: two N x N Gram products
+// over the observations and one N x N Cholesky (the ensemble-space form of
+// the same update). A non-positive variance takes the m x m path, which
+// reports the indefinite C as before.
+//
+// With localization (the reference's sparsity pattern of pairs within the
+// cutoff and its cutoff function) P is no longer A A^T / (N - 1): the
+// observation block C is scaled entry by entry, the parameter rows keep
+// x_k += A_p W[:, k], and each state row i takes
+//   x_k[i] += sum_{j near i} rho_ij g_ij Z_k[j],
+//   g_ij = sum_l A_l[i] HA_l[j] / (N - 1),
+// over the observations j within the cutoff of node i, found through a
+// uniform grid of observation buckets (no P, no n x m matrix).
 #include "capi_common.hpp"
 #include "../../include/adamantine_b200_ensemble.h"
 
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 namespace adm
 {
@@ -34,7 +53,8 @@ enum EnkfError
 {
   EERR_NONE = 0,
   EERR_NOT_SPD = 1,   // a Cholesky pivot was not positive and finite
-  EERR_BAD_INDEX = 2  // an observation index outside [0, n_state)
+  EERR_BAD_INDEX = 2, // an observation index outside [0, n_state)
+  EERR_SINGULAR = 3   // an LU pivot was zero or not finite
 };
 
 // HA[k][j] = x_k[idx_k[j]] - mean_k(...), D[k][j] = y_j + e_k[j] - x_k[idx_k[j]].
@@ -64,10 +84,43 @@ __global__ void hx_kernel(double const *states, int64_t stride, int n_members, i
     HA[(int64_t)k * m + j] -= mean;
 }
 
-// Lower triangle of C = HA^T HA * scale + R (R diagonal var, or dense cov).
+// Geometry of a localized analysis: state entry i = a + pitch (b + nn1 c)
+// sits at origin + (a, b, c) spacing; the observations are sorted into
+// nb[0] x nb[1] x nb[2] buckets of size bsize from bmin.
+struct LocGeom
+{
+  int function = ADM_LOC_NONE;
+  double cutoff = 0.0, cutoff2 = 0.0;
+  double origin[3] = {0, 0, 0}, spacing[3] = {0, 0, 0};
+  int64_t nn[3] = {0, 0, 0}, pitch = 0;
+  double bmin[3] = {0, 0, 0}, bsize[3] = {1, 1, 1};
+  int nb[3] = {1, 1, 1};
+};
+
+// Scaling of a covariance entry between support points at squared distance
+// d2: 0 outside the cutoff sphere (the sparsity pattern), else 1 or the
+// Gaspari-Cohn correlation (Gaspari and Cohn 1999, eq. 4.10) of
+// r = 2 d / cutoff, as gaspari_cohn_function (DataAssimilator.cc:672-688).
+__device__ __forceinline__ double loc_weight(LocGeom const &g, double d2)
+{
+  if (!(d2 <= g.cutoff2))
+    return 0.0;
+  if (g.function != ADM_LOC_GASPARI_COHN)
+    return 1.0;
+  double const r = 2.0 * sqrt(d2) / g.cutoff;
+  if (r < 1.0)
+    return 1.0 + r * r * (-5.0 / 3.0 + r * (5.0 / 8.0 + r * (0.5 - 0.25 * r)));
+  if (r < 2.0)
+    return 4.0 - 5.0 * r + r * r * (5.0 / 3.0 + r * (5.0 / 8.0 + r * (-0.5 + r / 12.0))) - 2.0 / (3.0 * r);
+  return 0.0;
+}
+
+// Lower triangle of C = HA^T HA * scale + R (R diagonal var, or dense cov);
+// with oxyz (observation support points) the HA^T HA part is localized.
 // 32 x 32 output tile per block, 256 threads, 4 outputs per thread.
 __global__ void __launch_bounds__(256) cov_kernel(double const *HA, int n_members, int m, double scale,
-                                                  double const *var, double const *cov, double *C)
+                                                  double const *var, double const *cov, double *C,
+                                                  double const *oxyz, LocGeom g, int full)
 {
   int const bi = blockIdx.y, bj = blockIdx.x;
   if (bj > bi)
@@ -107,11 +160,30 @@ __global__ void __launch_bounds__(256) cov_kernel(double const *HA, int n_member
     if (gj > gi || gj >= m)
       continue;
     double v = acc[c] * scale;
+    if (oxyz)
+    {
+      double const dx = oxyz[3 * gi] - oxyz[3 * gj], dy = oxyz[3 * gi + 1] - oxyz[3 * gj + 1],
+                   dz = oxyz[3 * gi + 2] - oxyz[3 * gj + 2];
+      v *= loc_weight(g, dx * dx + dy * dy + dz * dz);
+    }
     if (cov)
       v += cov[(int64_t)gi * m + gj];
     else if (gi == gj)
       v += var[gi];
     C[(int64_t)gi * m + gj] = v;
+    if (full && gj != gi)
+    {
+      double u = acc[c] * scale;
+      if (oxyz)
+      {
+        double const dx = oxyz[3 * gi] - oxyz[3 * gj], dy = oxyz[3 * gi + 1] - oxyz[3 * gj + 1],
+                     dz = oxyz[3 * gi + 2] - oxyz[3 * gj + 2];
+        u *= loc_weight(g, dx * dx + dy * dy + dz * dz);
+      }
+      if (cov)
+        u += cov[(int64_t)gj * m + gi];
+      C[(int64_t)gj * m + gi] = u;
+    }
   }
 }
 
@@ -325,6 +397,410 @@ __global__ void __launch_bounds__(256) solve_kernel(double const *L, int m, doub
     Z[(int64_t)k * m + i] = col[i];
 }
 
+// ---- ensemble-space solve (diagonal R, no localization)
+
+// G[a][b] = sum_j HA[a][j] HA[b][j] / var[j] (which 0) and
+// E[a][b] = sum_j HA[a][j] D[b][j] / var[j] (which 1), one warp per entry;
+// *bad_var is set when a variance is not positive and finite.
+__global__ void ens_gram_kernel(double const *HA, double const *D, double const *var, int n_members, int m,
+                                double *G, double *E, int *bad_var)
+{
+  int const gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  int const nn = n_members * n_members;
+  if (gw >= 2 * nn)
+    return;
+  int const which = gw / nn, a = (gw % nn) / n_members, b = gw % n_members;
+  double const *x = which == 0 ? HA : D;
+  double s = 0.0;
+  bool bad = false;
+  for (int j = lane; j < m; j += 32)
+  {
+    double const v = var[j];
+    bad |= !(v > 0.0) || !isfinite(v);
+    s += HA[(int64_t)a * m + j] * x[(int64_t)b * m + j] / v;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+    s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (__any_sync(0xffffffffu, bad) && lane == 0)
+    atomicExch(bad_var, 1);
+  if (lane == 0)
+    (which == 0 ? G : E)[a * n_members + b] = s;
+}
+
+// W = ((N-1) I + G)^-1 E for N <= kMaxN, one CTA: Cholesky of the N x N
+// matrix in shared memory (the update of a column step forms the scaled
+// entries it needs, so the column is scaled after it), then one right-hand
+// side (column of E) per thread, forward and backward.
+__global__ void __launch_bounds__(256) ens_solve_kernel(double const *G, double const *E, int n, double *W,
+                                                        int *err)
+{
+  extern __shared__ double ens_sm[]; // M [n][n + 1], then X [n][n + 1]
+  int const ld = n + 1;
+  double *const Mp = ens_sm, *const Xp = ens_sm + n * ld;
+#define M(a, b) Mp[(a) * ld + (b)]
+#define X(a, b) Xp[(a) * ld + (b)]
+  int const tid = threadIdx.x;
+  for (int e = tid; e < n * n; e += blockDim.x)
+  {
+    int const a = e / n, b = e % n;
+    M(a, b) = G[e] + (a == b ? (double)(n - 1) : 0.0);
+    X(a, b) = E[e];
+  }
+  __syncthreads();
+  // right-looking Cholesky of the lower triangle
+  for (int j = 0; j < n; ++j)
+  {
+    double const d = M(j, j);
+    bool const ok = d > 0.0 && isfinite(d);
+    if (!ok && tid == 0)
+      atomicCAS(err, 0, (int)EERR_NOT_SPD);
+    double const r = ok ? sqrt(d) : 1.0;
+    int const w = n - j - 1;
+    __syncthreads(); // everyone has read M(j, j) and column j
+    for (int e = tid; e < w * w; e += blockDim.x)
+    {
+      int const i = j + 1 + e / w, l = j + 1 + e % w;
+      if (l <= i)
+        M(i, l) -= (M(i, j) / r) * (M(l, j) / r);
+    }
+    __syncthreads();
+    if (tid == 0)
+      M(j, j) = r;
+    for (int i = j + 1 + tid; i < n; i += blockDim.x)
+      M(i, j) /= r;
+    __syncthreads();
+  }
+  // one column of X per thread: L y = e, L^T x = y
+  if (tid < n)
+  {
+    int const b = tid;
+    for (int i = 0; i < n; ++i)
+    {
+      double s = X(i, b);
+      for (int q = 0; q < i; ++q)
+        s -= M(i, q) * X(q, b);
+      X(i, b) = s / M(i, i);
+    }
+    for (int i = n - 1; i >= 0; --i)
+    {
+      double s = X(i, b);
+      for (int q = i + 1; q < n; ++q)
+        s -= M(q, i) * X(q, b);
+      X(i, b) = s / M(i, i);
+    }
+  }
+  __syncthreads();
+  for (int e = tid; e < n * n; e += blockDim.x)
+    W[e] = X(e / n, e % n);
+#undef M
+#undef X
+}
+
+// ---- LU with partial pivoting (C = P^T L U, row-major, in place), for a
+// localized H P H^T + R that need not be positive definite (a step-function
+// Schur product is not a correlation; the reference solves it with GMRES).
+// Right-looking, blocked by kNB: panel, row swaps, triangular solve of the
+// block row, trailing update.
+
+// Panel k0 .. k0 + nb - 1 over rows k0 .. m - 1, one CTA: per column the
+// pivot (largest magnitude, first on ties), the swap inside the panel, the
+// multipliers (kept in shared memory with the pivot row) and the rank-1
+// update of the rest of the panel, one element per thread, which also finds
+// the next column's pivot candidates. Dynamic shared memory: m - k0 + kNB
+// doubles.
+__global__ void __launch_bounds__(1024) lu_panel_kernel(double *C, int m, int k0, int *piv, int *err)
+{
+  extern __shared__ double lsm[]; // [m - k0] multipliers, then [kNB] pivot row
+  double *const urow = lsm + (m - k0);
+  __shared__ double red_v[32];
+  __shared__ int red_i[32];
+  __shared__ int s_piv;
+  __shared__ double s_d;
+  int const nb = min(kNB, m - k0);
+  int const tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  // candidate of this thread for the first column
+  double best = -1.0;
+  int bidx = m;
+  for (int i = k0 + tid; i < m; i += blockDim.x)
+  {
+    double const v = fabs(C[(int64_t)i * m + k0]);
+    if (v > best)
+    {
+      best = v;
+      bidx = i;
+    }
+  }
+  for (int jj = 0; jj < nb; ++jj)
+  {
+    int const j = k0 + jj;
+    // block argmax (ties: smaller row)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+    {
+      double const ov = __shfl_xor_sync(0xffffffffu, best, o);
+      int const oi = __shfl_xor_sync(0xffffffffu, bidx, o);
+      if (ov > best || (ov == best && oi < bidx))
+      {
+        best = ov;
+        bidx = oi;
+      }
+    }
+    if (lane == 0)
+    {
+      red_v[warp] = best;
+      red_i[warp] = bidx;
+    }
+    __syncthreads();
+    if (tid == 0)
+    {
+      double bv = red_v[0];
+      int bi = red_i[0];
+      for (int w = 1; w < nw; ++w)
+        if (red_v[w] > bv || (red_v[w] == bv && red_i[w] < bi))
+        {
+          bv = red_v[w];
+          bi = red_i[w];
+        }
+      if (bi >= m || !(bv > 0.0) || !isfinite(bv))
+      {
+        atomicCAS(err, 0, (int)EERR_SINGULAR);
+        bi = j;
+      }
+      piv[j] = bi;
+      s_piv = bi;
+    }
+    __syncthreads();
+    int const p = s_piv;
+    int const w = nb - jj - 1;
+    // swap rows j and p inside the panel; the pivot row's tail to shared
+    for (int c = tid; c < nb; c += blockDim.x)
+    {
+      double const a = C[(int64_t)j * m + k0 + c], b = C[(int64_t)p * m + k0 + c];
+      if (p != j)
+      {
+        C[(int64_t)j * m + k0 + c] = b;
+        C[(int64_t)p * m + k0 + c] = a;
+      }
+      double const pj = p != j ? b : a; // the new row j
+      if (c == jj)
+        s_d = (fabs(pj) > 0.0 && isfinite(pj)) ? pj : 1.0; // a bad pivot was flagged above
+      if (c > jj)
+        urow[c - jj - 1] = pj;
+    }
+    __syncthreads();
+    double const d = s_d;
+    // multipliers
+    for (int i = j + 1 + tid; i < m; i += blockDim.x)
+    {
+      double const l = C[(int64_t)i * m + j] / d;
+      C[(int64_t)i * m + j] = l;
+      lsm[i - k0] = l;
+    }
+    __syncthreads();
+    // rank-1 update of the panel's remaining columns, one element per thread
+    best = -1.0;
+    bidx = m;
+    if (w > 0)
+    {
+      int64_t const total = (int64_t)(m - j - 1) * w;
+      for (int64_t e = tid; e < total; e += blockDim.x)
+      {
+        int const i = j + 1 + (int)(e / w), c = 1 + (int)(e % w);
+        double *const a = C + (int64_t)i * m + j + c;
+        double const v = fma(-lsm[i - k0], urow[c - 1], *a);
+        *a = v;
+        if (c == 1 && fabs(v) > best)
+        {
+          best = fabs(v);
+          bidx = i;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// The panel's row swaps applied to the columns outside it, one column per
+// thread.
+__global__ void lu_swap_kernel(double *C, int m, int k0, int const *piv)
+{
+  int const nb = min(kNB, m - k0);
+  int const c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m || (c >= k0 && c < k0 + nb))
+    return;
+  for (int j = k0; j < k0 + nb; ++j)
+  {
+    int const p = piv[j];
+    if (p != j)
+    {
+      double const t = C[(int64_t)j * m + c];
+      C[(int64_t)j * m + c] = C[(int64_t)p * m + c];
+      C[(int64_t)p * m + c] = t;
+    }
+  }
+}
+
+// Block row U12 = L11^-1 A12 (L11 unit lower), one column per thread.
+__global__ void __launch_bounds__(128) lu_trsm_kernel(double *C, int m, int k0)
+{
+  __shared__ double l[kNB][kNB + 1];
+  int const nb = min(kNB, m - k0);
+  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x)
+  {
+    int const r = e / nb, c = e % nb;
+    l[r][c] = c < r ? C[(int64_t)(k0 + r) * m + k0 + c] : 0.0;
+  }
+  __syncthreads();
+  int const c = k0 + nb + blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m)
+    return;
+  double x[kNB];
+#pragma unroll
+  for (int r = 0; r < kNB; ++r)
+  {
+    if (r < nb)
+    {
+      double s = C[(int64_t)(k0 + r) * m + c];
+#pragma unroll
+      for (int q = 0; q < r; ++q)
+        s = fma(-l[r][q], x[q], s);
+      x[r] = s;
+      C[(int64_t)(k0 + r) * m + c] = s;
+    }
+  }
+}
+
+// Trailing update A22 -= L21 U12 on 64 x 64 tiles.
+__global__ void __launch_bounds__(256) lu_update_kernel(double *C, int m, int k0)
+{
+  int const base = k0 + kNB;
+  int const i0 = base + blockIdx.y * 64, j0 = base + blockIdx.x * 64;
+  __shared__ double pa[64][33], pb[32][65];
+  int const tid = threadIdx.x;
+  int const tr = (tid / 16) * 4, tc = (tid % 16) * 4;
+  double acc[4][4] = {};
+  for (int q0 = 0; q0 < kNB; q0 += 32)
+  {
+    for (int e = tid; e < 64 * 32; e += 256)
+    {
+      int const r = e / 32, c = e % 32;
+      pa[r][c] = i0 + r < m ? C[(int64_t)(i0 + r) * m + k0 + q0 + c] : 0.0;
+      int const br = e / 64, bc = e % 64;
+      pb[br][bc] = j0 + bc < m ? C[(int64_t)(k0 + q0 + br) * m + j0 + bc] : 0.0;
+    }
+    __syncthreads();
+    for (int q = 0; q < 32; ++q)
+    {
+      double a[4], b[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+      {
+        a[u] = pa[tr + u][q];
+        b[u] = pb[q][tc + u];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+          acc[u][v] = fma(a[u], b[v], acc[u][v]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+    {
+      int const gi = i0 + tr + u, gj = j0 + tc + v;
+      if (gi < m && gj < m)
+        C[(int64_t)gi * m + gj] -= acc[u][v];
+    }
+}
+
+// Z_k = C^-1 D_k from the LU factors, one member per CTA: the row swaps,
+// forward L y = P d (unit diagonal), backward U z = y; blocked like
+// solve_kernel, the column in shared memory.
+__global__ void __launch_bounds__(256) lu_solve_kernel(double const *LU, int const *piv, int m, double const *D,
+                                                       double *Z)
+{
+  extern __shared__ double col[]; // [m]
+  int const k = blockIdx.x;
+  int const tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int i = tid; i < m; i += blockDim.x)
+    col[i] = D[(int64_t)k * m + i];
+  __syncthreads();
+  if (tid == 0)
+    for (int j = 0; j < m; ++j)
+    {
+      int const p = piv[j];
+      if (p != j)
+      {
+        double const t = col[j];
+        col[j] = col[p];
+        col[p] = t;
+      }
+    }
+  __syncthreads();
+  int const nblk = (m + kNB - 1) / kNB;
+  for (int b = 0; b < nblk; ++b)
+  {
+    int const k0 = b * kNB, nb = min(kNB, m - k0);
+    if (warp == 0)
+      for (int j = 0; j < nb; ++j)
+      {
+        double s = 0.0;
+        for (int q = lane; q < j; q += 32)
+          s += LU[(int64_t)(k0 + j) * m + k0 + q] * col[k0 + q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+          s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0)
+          col[k0 + j] -= s;
+        __syncwarp();
+      }
+    __syncthreads();
+    for (int i = k0 + nb + tid; i < m; i += blockDim.x)
+    {
+      double const *row = LU + (int64_t)i * m + k0;
+      double s = 0.0;
+      for (int q = 0; q < nb; ++q)
+        s += row[q] * col[k0 + q];
+      col[i] -= s;
+    }
+    __syncthreads();
+  }
+  for (int b = nblk - 1; b >= 0; --b)
+  {
+    int const k0 = b * kNB, nb = min(kNB, m - k0);
+    if (warp == 0)
+      for (int j = nb - 1; j >= 0; --j)
+      {
+        double s = 0.0;
+        for (int q = j + 1 + lane; q < nb; q += 32)
+          s += LU[(int64_t)(k0 + j) * m + k0 + q] * col[k0 + q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+          s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0)
+          col[k0 + j] = (col[k0 + j] - s) / LU[(int64_t)(k0 + j) * m + k0 + j];
+        __syncwarp();
+      }
+    __syncthreads();
+    for (int i = tid; i < k0; i += blockDim.x)
+    {
+      double const *row = LU + (int64_t)i * m + k0;
+      double s = 0.0;
+      for (int q = 0; q < nb; ++q)
+        s += row[q] * col[k0 + q];
+      col[i] -= s;
+    }
+    __syncthreads();
+  }
+  for (int i = tid; i < m; i += blockDim.x)
+    Z[(int64_t)k * m + i] = col[i];
+}
+
 // W[a][b] = scale * sum_j HA[a][j] Z[b][j], one warp per entry.
 __global__ void w_kernel(double const *HA, double const *Z, int n_members, int m, double scale, double *W)
 {
@@ -427,14 +903,14 @@ __global__ void center_kernel(double const *HX, int n_members, int m, double con
 __global__ void __launch_bounds__(256) partial_update_kernel(double const *states, int64_t stride, int n_local,
                                                              int n_members, int64_t n_state, double const *params,
                                                              int n_params, double const *sum, double const *W,
-                                                             double *U)
+                                                             double *U, int64_t row0)
 {
   extern __shared__ double w[]; // [n_local][n_members]
   for (int e = threadIdx.x; e < n_local * n_members; e += blockDim.x)
     w[e] = W[e];
   __syncthreads();
   int64_t const rows = n_state + n_params;
-  int64_t const i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int64_t const i = row0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= rows)
     return;
   bool const is_param = i >= n_state;
@@ -489,6 +965,124 @@ __global__ void apply_kernel(double *states, int64_t stride, int n_local, int64_
     states[(int64_t)k * stride + i] += u;
 }
 
+// out[j][k] = in[k][j] (m x N from N x m).
+__global__ void transpose_kernel(double const *in, int n, int m, double *out)
+{
+  int64_t const e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= (int64_t)n * m)
+    return;
+  int const k = (int)(e % n);
+  int64_t const j = e / n;
+  out[e] = in[(int64_t)k * m + j];
+}
+
+// Localized update of the state rows, written as U[l][i] for the n_out
+// members l (the rows of Z). Block: a 32 x 4 x 2 brick of nodes, one per
+// thread; blockIdx.y: 32 output members. The n_k members seen here are
+// members k0 .. k0 + n_k - 1 of HA; their anomalies about sum / n_mean
+// (or, with sum NULL, about their own mean) stay in registers, and the
+// block walks the observation buckets that meet its brick grown by the
+// cutoff (one list for all threads, so HA^T / Z^T rows are broadcast
+// loads).
+template <int KMAX>
+__global__ void __launch_bounds__(256) loc_state_kernel(LocGeom g, double const *states, int64_t stride, int n_k,
+                                                        int k0, double const *sum, int n_mean, double const *HAt,
+                                                        double const *Zt, int N, int n_out, double scale,
+                                                        int const *bstart, int const *perm, double const *sxyz,
+                                                        double *U, int64_t rows)
+{
+  int const tid = threadIdx.x;
+  int64_t const nbx = (g.pitch + 31) / 32, nby = (g.nn[1] + 3) / 4;
+  int64_t const blk = blockIdx.x;
+  int64_t const a0 = (blk % nbx) * 32, b0 = ((blk / nbx) % nby) * 4, c0 = (blk / (nbx * nby)) * 2;
+  int64_t const ia = a0 + (tid & 31), ib = b0 + ((tid >> 5) & 3), ic = c0 + (tid >> 7);
+  // rows of the padded layout get a result (0 in the row padding); nodes
+  // get the update
+  bool const in_rows = ia < g.pitch && ib < g.nn[1] && ic < g.nn[2];
+  bool const valid = in_rows && ia < g.nn[0];
+  int64_t const i = ia + g.pitch * (ib + g.nn[1] * ic);
+  double const px = g.origin[0] + (double)ia * g.spacing[0];
+  double const py = g.origin[1] + (double)ib * g.spacing[1];
+  double const pz = g.origin[2] + (double)ic * g.spacing[2];
+
+  double a[KMAX];
+  double mean = 0.0;
+  if (valid)
+  {
+    if (sum)
+      mean = sum[i] / n_mean;
+    else
+    {
+      double s = 0.0;
+      for (int k = 0; k < n_k; ++k)
+        s += states[(int64_t)k * stride + i];
+      mean = s / n_k;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < KMAX; ++k)
+    a[k] = (valid && k < n_k) ? states[(int64_t)k * stride + i] - mean : 0.0;
+
+  // buckets meeting the brick's box grown by the cutoff
+  int q0[3], q1[3];
+  {
+    int64_t const hi_idx[3] = {min(a0 + 31, g.nn[0] - 1), min(b0 + 3, g.nn[1] - 1), min(c0 + 1, g.nn[2] - 1)};
+    int64_t const lo_idx[3] = {a0, b0, c0};
+    for (int d = 0; d < 3; ++d)
+    {
+      if (g.nb[d] == 1)
+      {
+        q0[d] = 0;
+        q1[d] = 0;
+        continue;
+      }
+      double const lo = g.origin[d] + (double)lo_idx[d] * g.spacing[d] - g.cutoff;
+      double const hi = g.origin[d] + (double)hi_idx[d] * g.spacing[d] + g.cutoff;
+      double const f0 = floor((lo - g.bmin[d]) / g.bsize[d]), f1 = floor((hi - g.bmin[d]) / g.bsize[d]);
+      q0[d] = (int)fmin(fmax(f0, 0.0), (double)g.nb[d]);
+      q1[d] = (int)fmin(fmax(f1, -1.0), (double)(g.nb[d] - 1));
+    }
+  }
+  int const l0 = blockIdx.y * 32;
+  double acc[32];
+#pragma unroll
+  for (int l = 0; l < 32; ++l)
+    acc[l] = 0.0;
+  for (int qz = q0[2]; qz <= q1[2]; ++qz)
+    for (int qy = q0[1]; qy <= q1[1]; ++qy)
+      for (int qx = q0[0]; qx <= q1[0]; ++qx)
+      {
+        int const bucket = qx + g.nb[0] * (qy + g.nb[1] * qz);
+        int const s1 = bstart[bucket + 1];
+        for (int s = bstart[bucket]; s < s1; ++s)
+        {
+          double const dx = sxyz[3 * s] - px, dy = sxyz[3 * s + 1] - py, dz = sxyz[3 * s + 2] - pz;
+          double const w = valid ? loc_weight(g, dx * dx + dy * dy + dz * dz) : 0.0;
+          if (w == 0.0)
+            continue;
+          int64_t const j = perm[s];
+          double const *ha = HAt + j * N + k0;
+          double gk = 0.0;
+#pragma unroll
+          for (int k = 0; k < KMAX; ++k)
+            if (k < n_k)
+              gk = fma(a[k], ha[k], gk);
+          double const f = w * scale * gk;
+          double const *z = Zt + j * N + l0;
+#pragma unroll
+          for (int l = 0; l < 32; ++l)
+            if (l0 + l < n_out)
+              acc[l] = fma(f, z[l], acc[l]);
+        }
+      }
+  if (!in_rows)
+    return;
+#pragma unroll
+  for (int l = 0; l < 32; ++l)
+    if (l0 + l < n_out)
+      U[(int64_t)(l0 + l) * rows + i] = acc[l];
+}
+
 } // namespace
 
 // Workspace of the analysis, grown on demand.
@@ -498,6 +1092,194 @@ struct Enkf
   cudaStream_t stream = nullptr;
   DevBuf<double> HA, D, C, Z, W;
   DevBuf<int> err;
+  // localization: geometry, observation points (input order and bucket
+  // order), bucket offsets, and the transposed HA / Z and the update rows
+  bool loc = false;
+  int loc_m = 0;
+  LocGeom lg;
+  DevBuf<double> oxyz, sxyz, HAt, Zt, U, sumb;
+  DevBuf<int> bstart, perm, piv;
+  int gain_n = 0, gain_m = 0; // shape of the last gain (HA and Z kept)
+
+  // a step-function (or "none") localized H P H^T + R may be indefinite:
+  // LU with pivoting; otherwise (SPD) Cholesky
+  bool use_lu() const { return loc && lg.function != ADM_LOC_GASPARI_COHN; }
+  bool factored_lu = false; // the last factor of C was LU (else Cholesky)
+  DevBuf<double> G, E;
+  DevBuf<int> bad_var;
+
+  // W by the ensemble-space form when R is diagonal, there is no
+  // localization and N <= kMaxN; false (nothing decided) when a variance is
+  // not positive, so that the m x m path runs. Raises on a bad index.
+  bool woodbury_w(int N, int m, double const *var, double const *cov, double *Wout)
+  {
+    if (cov || loc || N > kMaxN)
+      return false;
+    G.alloc((size_t)N * N);
+    E.alloc((size_t)N * N);
+    bad_var.alloc(1);
+    ADM_CK(cudaMemsetAsync(bad_var.p, 0, sizeof(int), stream));
+    int const warps = 2 * N * N;
+    ens_gram_kernel<<<(warps * 32 + 255) / 256, 256, 0, stream>>>(HA.p, D.p, var, N, m, G.p, E.p, bad_var.p);
+    size_t const smem = sizeof(double) * 2 * (size_t)N * (N + 1);
+    ADM_CK(cudaFuncSetAttribute(ens_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ens_solve_kernel<<<1, 256, smem, stream>>>(G.p, E.p, N, Wout, err.p);
+    ADM_CK(cudaGetLastError());
+    int h[2] = {0, 0};
+    ADM_CK(cudaMemcpyAsync(&h[0], err.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    ADM_CK(cudaMemcpyAsync(&h[1], bad_var.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    ADM_CK(cudaStreamSynchronize(stream));
+    if (h[0] == EERR_BAD_INDEX)
+      raise_err(h[0]);
+    if (h[1] || h[0] != 0)
+    {
+      ADM_CK(cudaMemsetAsync(err.p, 0, sizeof(int), stream));
+      return false;
+    }
+    return true;
+  }
+
+  void set_localization(int function, double cutoff, int m, double const *xyz, double const *origin,
+                        double const *spacing, int64_t const *nodes, int64_t pitch)
+  {
+    if (m == 0)
+    {
+      loc = false;
+      loc_m = 0;
+      return;
+    }
+    if (function < ADM_LOC_NONE || function > ADM_LOC_GASPARI_COHN)
+      throw Error(ADM_ERR_INVALID, "unknown localization cutoff function");
+    if (!(cutoff > 0.0))
+      throw Error(ADM_ERR_INVALID, "the localization cutoff distance must be positive");
+    if (m < 0 || m > kMaxObs || !xyz || !origin || !spacing || !nodes)
+      throw Error(ADM_ERR_INVALID, "invalid localization arguments");
+    for (int d = 0; d < 3; ++d)
+      if (nodes[d] < 1 || !std::isfinite(origin[d]) || !std::isfinite(spacing[d]) || spacing[d] < 0.0)
+        throw Error(ADM_ERR_INVALID, "invalid localization grid");
+    if (pitch < nodes[0])
+      throw Error(ADM_ERR_INVALID, "pitch must be at least nodes[0]");
+    LocGeom g;
+    g.function = function;
+    g.cutoff = cutoff;
+    g.cutoff2 = cutoff * cutoff;
+    g.pitch = pitch;
+    double omin[3], omax[3], lo[3], hi[3];
+    for (int d = 0; d < 3; ++d)
+    {
+      g.origin[d] = origin[d];
+      g.spacing[d] = spacing[d];
+      g.nn[d] = nodes[d];
+      omin[d] = omax[d] = xyz[d];
+    }
+    for (int j = 0; j < m; ++j)
+      for (int d = 0; d < 3; ++d)
+      {
+        double const v = xyz[3 * j + d];
+        if (!std::isfinite(v))
+          throw Error(ADM_ERR_INVALID, "observation points must be finite");
+        omin[d] = std::fmin(omin[d], v);
+        omax[d] = std::fmax(omax[d], v);
+      }
+    double diag2 = 0.0;
+    for (int d = 0; d < 3; ++d)
+    {
+      lo[d] = std::fmin(omin[d], origin[d]);
+      hi[d] = std::fmax(omax[d], origin[d] + (double)(nodes[d] - 1) * spacing[d]);
+      diag2 += (hi[d] - lo[d]) * (hi[d] - lo[d]);
+    }
+    bool const covers_all = cutoff * cutoff >= diag2;
+    loc_m = m;
+    if (covers_all && function != ADM_LOC_GASPARI_COHN)
+    {
+      loc = false; // every pair in the pattern, every weight 1
+      return;
+    }
+    // buckets of at least the cutoff (at most 64 per axis over the points)
+    int64_t nbt = 1;
+    for (int d = 0; d < 3; ++d)
+    {
+      double const ext = omax[d] - omin[d];
+      g.bmin[d] = omin[d];
+      if (covers_all || ext <= 0.0)
+      {
+        g.nb[d] = 1;
+        g.bsize[d] = 1.0;
+      }
+      else
+      {
+        g.bsize[d] = std::fmax(cutoff, ext / 64.0);
+        g.nb[d] = (int)std::fmin(65.0, std::floor(ext / g.bsize[d]) + 1.0);
+      }
+      nbt *= g.nb[d];
+    }
+    std::vector<int> bucket(m), start(nbt + 1, 0), order(m);
+    for (int j = 0; j < m; ++j)
+    {
+      int q[3];
+      for (int d = 0; d < 3; ++d)
+      {
+        double const f = g.nb[d] == 1 ? 0.0 : std::floor((xyz[3 * j + d] - g.bmin[d]) / g.bsize[d]);
+        q[d] = (int)std::fmin(std::fmax(f, 0.0), (double)(g.nb[d] - 1));
+      }
+      bucket[j] = q[0] + g.nb[0] * (q[1] + g.nb[1] * q[2]);
+      ++start[bucket[j] + 1];
+    }
+    for (int64_t b = 0; b < nbt; ++b)
+      start[b + 1] += start[b];
+    std::vector<int> fill(start.begin(), start.end() - 1);
+    std::vector<double> sorted(3 * (size_t)m);
+    for (int j = 0; j < m; ++j)
+    {
+      int const s = fill[bucket[j]]++;
+      order[s] = j;
+      for (int d = 0; d < 3; ++d)
+        sorted[3 * (size_t)s + d] = xyz[3 * j + d];
+    }
+    ADM_CK(cudaSetDevice(device));
+    oxyz.alloc(3 * (size_t)m);
+    sxyz.alloc(3 * (size_t)m);
+    perm.alloc(m);
+    bstart.alloc(nbt + 1);
+    ADM_CK(cudaMemcpyAsync(oxyz.p, xyz, 3 * sizeof(double) * m, cudaMemcpyHostToDevice, stream));
+    ADM_CK(cudaMemcpyAsync(sxyz.p, sorted.data(), 3 * sizeof(double) * m, cudaMemcpyHostToDevice, stream));
+    ADM_CK(cudaMemcpyAsync(perm.p, order.data(), sizeof(int) * m, cudaMemcpyHostToDevice, stream));
+    ADM_CK(cudaMemcpyAsync(bstart.p, start.data(), sizeof(int) * (nbt + 1), cudaMemcpyHostToDevice, stream));
+    ADM_CK(cudaStreamSynchronize(stream));
+    lg = g;
+    loc = true;
+  }
+
+  void check_loc(int m, int64_t n_state) const
+  {
+    if (loc_m && m != loc_m)
+      throw Error(ADM_ERR_INVALID, "the number of observations differs from the localization's");
+    if (loc && n_state != lg.pitch * lg.nn[1] * lg.nn[2])
+      throw Error(ADM_ERR_INVALID, "n_state differs from the localization grid (pitch * nodes[1] * nodes[2])");
+  }
+
+  // U[l][i] of the state rows from the localized gain (HA, Z of N members;
+  // the n_k members seen start at k0), then nothing else
+  void launch_loc_state(double const *states, int64_t stride, int n_k, int k0, double const *sum, int N, int m,
+                        double *Uout, int64_t rows)
+  {
+    HAt.alloc((size_t)N * m);
+    Zt.alloc((size_t)N * m);
+    int64_t const nm = (int64_t)N * m;
+    transpose_kernel<<<(unsigned)((nm + 255) / 256), 256, 0, stream>>>(HA.p, N, m, HAt.p);
+    transpose_kernel<<<(unsigned)((nm + 255) / 256), 256, 0, stream>>>(Z.p, N, m, Zt.p);
+    ADM_CK(cudaGetLastError());
+    int64_t const nbx = (lg.pitch + 31) / 32, nby = (lg.nn[1] + 3) / 4, nbz = (lg.nn[2] + 1) / 2;
+    dim3 const grid((unsigned)(nbx * nby * nbz), (unsigned)((N + 31) / 32));
+    double const scale = 1.0 / (N - 1.0);
+    if (n_k <= 32)
+      loc_state_kernel<32><<<grid, 256, 0, stream>>>(lg, states, stride, n_k, k0, sum, N, HAt.p, Zt.p, N, N, scale,
+                                                     bstart.p, perm.p, sxyz.p, Uout, rows);
+    else
+      loc_state_kernel<64><<<grid, 256, 0, stream>>>(lg, states, stride, n_k, k0, sum, N, HAt.p, Zt.p, N, N, scale,
+                                                     bstart.p, perm.p, sxyz.p, Uout, rows);
+    ADM_CK(cudaGetLastError());
+  }
 
   void analysis(int N, double *states, int64_t stride, int64_t n_state, double *params, int n_params,
                 int m, int64_t const *idx, double const *obs, double const *var, double const *cov,
@@ -511,6 +1293,7 @@ struct Enkf
     if (!states || !idx || !obs || !pert || (!var && !cov) || (n_params > 0 && !params) ||
         n_params < 0 || n_state < 1 || stride < n_state)
       throw Error(ADM_ERR_INVALID, "invalid analysis arguments");
+    check_loc(m, n_state);
     ADM_CK(cudaSetDevice(device));
     HA.alloc((size_t)N * m);
     D.alloc((size_t)N * m);
@@ -523,52 +1306,81 @@ struct Enkf
                                                    err.p);
     ADM_CK(cudaGetLastError());
     double const scale = 1.0 / (N - 1.0);
-    int const t32 = (m + 31) / 32;
-    cov_kernel<<<dim3(t32, t32), 256, 0, stream>>>(HA.p, N, m, scale, var, cov, C.p);
-    ADM_CK(cudaGetLastError());
-    for (int k0 = 0; k0 < m; k0 += kNB)
+    // stops before touching the states if an index or a pivot was bad
+    if (!woodbury_w(N, m, var, cov, W.p))
     {
-      potrf_diag_kernel<<<1, 256, 0, stream>>>(C.p, m, k0, err.p);
-      int const below = m - k0 - kNB;
-      if (below > 0)
-      {
-        trsm_panel_kernel<<<(below + 127) / 128, 128, 0, stream>>>(C.p, m, k0);
-        int const t = (below + 63) / 64;
-        syrk_update_kernel<<<dim3(t, t), 256, 0, stream>>>(C.p, m, k0);
-      }
+      factor_checked(N, m, scale, var, cov);
+      solve_and_w(N, m, scale, W.p);
+    }
+    int64_t const rows = n_state + n_params;
+    if (!loc)
+    {
+      update_kernel<<<(unsigned)((rows + 255) / 256), 256, 0, stream>>>(states, stride, N, n_state, params,
+                                                                        n_params, mask, W.p);
       ADM_CK(cudaGetLastError());
     }
-    // stop before touching the states if an index or a pivot was bad
-    int h_err = 0;
-    ADM_CK(cudaMemcpyAsync(&h_err, err.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
-    ADM_CK(cudaStreamSynchronize(stream));
-    if (h_err == EERR_BAD_INDEX)
-      throw Error(ADM_ERR_INVALID, "an observation index is outside [0, n_state)");
-    if (h_err == EERR_NOT_SPD)
-      throw Error(ADM_ERR_DEVICE, "H P H^T + R is not positive definite (Cholesky pivot <= 0)");
-    size_t const smem = (size_t)m * sizeof(double);
-    ADM_CK(cudaFuncSetAttribute(solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    solve_kernel<<<N, 256, smem, stream>>>(C.p, m, D.p, Z.p);
-    ADM_CK(cudaGetLastError());
-    w_kernel<<<(N * N * 32 + 255) / 256, 256, 0, stream>>>(HA.p, Z.p, N, m, scale, W.p);
-    ADM_CK(cudaGetLastError());
-    int64_t const rows = n_state + n_params;
-    update_kernel<<<(unsigned)((rows + 255) / 256), 256, 0, stream>>>(states, stride, N, n_state, params,
-                                                                      n_params, mask, W.p);
-    ADM_CK(cudaGetLastError());
+    else
+    {
+      // U = every member's update (parameter rows through W, state rows
+      // localized), then x += U
+      U.alloc((size_t)N * rows);
+      sumb.alloc(rows);
+      local_sum_kernel<<<(unsigned)((rows + 255) / 256), 256, 0, stream>>>(states, stride, N, n_state, params,
+                                                                          n_params, sumb.p);
+      ADM_CK(cudaGetLastError());
+      if (n_params > 0)
+      {
+        size_t const smem = sizeof(double) * (size_t)N * N;
+        ADM_CK(cudaFuncSetAttribute(partial_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        partial_update_kernel<<<(unsigned)((n_params + 255) / 256), 256, smem, stream>>>(
+            states, stride, N, N, n_state, params, n_params, sumb.p, W.p, U.p, n_state);
+        ADM_CK(cudaGetLastError());
+      }
+      launch_loc_state(states, stride, N, 0, sumb.p, N, m, U.p, rows);
+      int64_t const total = (int64_t)N * rows;
+      apply_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(states, stride, N, n_state, params,
+                                                                       n_params, U.p, mask);
+      ADM_CK(cudaGetLastError());
+    }
     ADM_CK(cudaStreamSynchronize(stream));
   }
 
   // ---- building blocks of the sharded analysis (members split over GPUs)
-  void check_err()
+  int read_err()
   {
     int h_err = 0;
     ADM_CK(cudaMemcpyAsync(&h_err, err.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
     ADM_CK(cudaStreamSynchronize(stream));
+    return h_err;
+  }
+
+  void check_err() { raise_err(read_err()); }
+
+  // Cholesky of C; a localized C that may be indefinite (step function or
+  // "none") and is found not positive definite is factored again by LU
+  void factor_checked(int N, int m, double scale, double const *var, double const *cov)
+  {
+    factored_lu = false;
+    factor(N, m, scale, var, cov);
+    int e = read_err();
+    if (e == EERR_NOT_SPD && use_lu())
+    {
+      ADM_CK(cudaMemsetAsync(err.p, 0, sizeof(int), stream));
+      factor_lu(N, m, scale, var, cov);
+      factored_lu = true;
+      e = read_err();
+    }
+    raise_err(e);
+  }
+
+  static void raise_err(int h_err)
+  {
     if (h_err == EERR_BAD_INDEX)
       throw Error(ADM_ERR_INVALID, "an observation index is outside [0, n_state)");
     if (h_err == EERR_NOT_SPD)
       throw Error(ADM_ERR_DEVICE, "H P H^T + R is not positive definite (Cholesky pivot <= 0)");
+    if (h_err == EERR_SINGULAR)
+      throw Error(ADM_ERR_DEVICE, "the localized H P H^T + R is singular (zero LU pivot)");
   }
 
   void observe(int N, double const *states, int64_t stride, int64_t n_state, int m, int64_t const *idx, double *hx)
@@ -603,13 +1415,20 @@ struct Enkf
     C.alloc((size_t)m * m);
     err.alloc(1);
     ADM_CK(cudaMemsetAsync(err.p, 0, sizeof(int), stream));
+    if (loc_m && m != loc_m)
+      throw Error(ADM_ERR_INVALID, "the number of observations differs from the localization's");
+    gain_n = gain_m = 0;
     center_kernel<<<(m + 127) / 128, 128, 0, stream>>>(hx, N, m, obs, pert, HA.p, D.p);
     ADM_CK(cudaGetLastError());
     double const scale = 1.0 / (N - 1.0);
-    factor(N, m, scale, var, cov);
-    check_err();
-    solve_and_w(N, m, scale, Wout);
+    if (!woodbury_w(N, m, var, cov, Wout))
+    {
+      factor_checked(N, m, scale, var, cov);
+      solve_and_w(N, m, scale, Wout);
+    }
     ADM_CK(cudaStreamSynchronize(stream));
+    gain_n = N;
+    gain_m = m;
   }
 
   void local_sum(int n_local, double const *states, int64_t stride, int64_t n_state, double const *params,
@@ -636,8 +1455,37 @@ struct Enkf
     size_t const smem = sizeof(double) * (size_t)n_local * N;
     ADM_CK(cudaFuncSetAttribute(partial_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     partial_update_kernel<<<(unsigned)((rows + 255) / 256), 256, smem, stream>>>(
-        states, stride, n_local, N, n_state, params, n_params, sum, w_rows, U);
+        states, stride, n_local, N, n_state, params, n_params, sum, w_rows, U, 0);
     ADM_CK(cudaGetLastError());
+    ADM_CK(cudaStreamSynchronize(stream));
+  }
+
+  void partial_update_localized(int n_local, int first, int N, double const *states, int64_t stride,
+                                int64_t n_state, double const *params, int n_params, double const *sum,
+                                double const *w_rows, double *Uout)
+  {
+    if (!loc)
+    {
+      partial_update(n_local, N, states, stride, n_state, params, n_params, sum, w_rows, Uout);
+      return;
+    }
+    if (n_local < 1 || n_local > kMaxN || first < 0 || first + n_local > N || N > kMaxGain || !states || !sum ||
+        !w_rows || !Uout || stride < n_state || n_params < 0 || (n_params > 0 && !params))
+      throw Error(ADM_ERR_INVALID, "invalid partial-update arguments (at most 64 local members)");
+    if (gain_n != N || gain_m != loc_m)
+      throw Error(ADM_ERR_INVALID, "the localized partial update needs adm_enkf_gain of the same ensemble first");
+    check_loc(gain_m, n_state);
+    ADM_CK(cudaSetDevice(device));
+    int64_t const rows = n_state + n_params;
+    if (n_params > 0)
+    {
+      size_t const smem = sizeof(double) * (size_t)n_local * N;
+      ADM_CK(cudaFuncSetAttribute(partial_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      partial_update_kernel<<<(unsigned)((n_params + 255) / 256), 256, smem, stream>>>(
+          states, stride, n_local, N, n_state, params, n_params, sum, w_rows, Uout, n_state);
+      ADM_CK(cudaGetLastError());
+    }
+    launch_loc_state(states, stride, n_local, first, sum, N, gain_m, Uout, rows);
     ADM_CK(cudaStreamSynchronize(stream));
   }
 
@@ -655,10 +1503,35 @@ struct Enkf
   }
 
   // C = HA HA^T scale + R and its Cholesky factor (lower, in place)
+  void factor_lu(int N, int m, double scale, double const *var, double const *cov)
+  {
+    int const t32 = (m + 31) / 32;
+    cov_kernel<<<dim3(t32, t32), 256, 0, stream>>>(HA.p, N, m, scale, var, cov, C.p, loc ? oxyz.p : nullptr, lg, 1);
+    ADM_CK(cudaGetLastError());
+    {
+      piv.alloc(m);
+      size_t const psm = sizeof(double) * ((size_t)m + kNB);
+      ADM_CK(cudaFuncSetAttribute(lu_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
+      for (int k0 = 0; k0 < m; k0 += kNB)
+      {
+        lu_panel_kernel<<<1, 1024, sizeof(double) * ((size_t)(m - k0) + kNB), stream>>>(C.p, m, k0, piv.p, err.p);
+        lu_swap_kernel<<<(m + 255) / 256, 256, 0, stream>>>(C.p, m, k0, piv.p);
+        int const right = m - k0 - kNB;
+        if (right > 0)
+        {
+          lu_trsm_kernel<<<(right + 127) / 128, 128, 0, stream>>>(C.p, m, k0);
+          int const t = (right + 63) / 64;
+          lu_update_kernel<<<dim3(t, t), 256, 0, stream>>>(C.p, m, k0);
+        }
+        ADM_CK(cudaGetLastError());
+      }
+    }
+  }
+
   void factor(int N, int m, double scale, double const *var, double const *cov)
   {
     int const t32 = (m + 31) / 32;
-    cov_kernel<<<dim3(t32, t32), 256, 0, stream>>>(HA.p, N, m, scale, var, cov, C.p);
+    cov_kernel<<<dim3(t32, t32), 256, 0, stream>>>(HA.p, N, m, scale, var, cov, C.p, loc ? oxyz.p : nullptr, lg, 0);
     ADM_CK(cudaGetLastError());
     for (int k0 = 0; k0 < m; k0 += kNB)
     {
@@ -678,8 +1551,16 @@ struct Enkf
   void solve_and_w(int N, int m, double scale, double *Wout)
   {
     size_t const smem = (size_t)m * sizeof(double);
-    ADM_CK(cudaFuncSetAttribute(solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    solve_kernel<<<N, 256, smem, stream>>>(C.p, m, D.p, Z.p);
+    if (factored_lu)
+    {
+      ADM_CK(cudaFuncSetAttribute(lu_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      lu_solve_kernel<<<N, 256, smem, stream>>>(C.p, piv.p, m, D.p, Z.p);
+    }
+    else
+    {
+      ADM_CK(cudaFuncSetAttribute(solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      solve_kernel<<<N, 256, smem, stream>>>(C.p, m, D.p, Z.p);
+    }
     ADM_CK(cudaGetLastError());
     w_kernel<<<(N * N * 32 + 255) / 256, 256, 0, stream>>>(HA.p, Z.p, N, m, scale, Wout);
     ADM_CK(cudaGetLastError());
@@ -754,6 +1635,27 @@ int adm_enkf_partial_update(adm_enkf *e, int32_t n_local, int32_t n_members, dou
     ADM_REQUIRE(e, "null handle");
     reinterpret_cast<adm::Enkf *>(e)->partial_update(n_local, n_members, states, stride, n_state, params, n_params,
                                                      sum, w_rows, u);
+  });
+}
+
+int adm_enkf_set_localization(adm_enkf *e, int32_t function, double cutoff, int32_t n_obs, double const *obs_xyz,
+                              double const *origin, double const *spacing, int64_t const *nodes, int64_t pitch)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(e, "null handle");
+    reinterpret_cast<adm::Enkf *>(e)->set_localization(function, cutoff, n_obs, obs_xyz, origin, spacing, nodes,
+                                                       pitch);
+  });
+}
+
+int adm_enkf_partial_update_localized(adm_enkf *e, int32_t n_local, int32_t first_member, int32_t n_members,
+                                      double const *states, int64_t stride, int64_t n_state, double const *params,
+                                      int32_t n_params, double const *sum, double const *w_rows, double *u)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(e, "null handle");
+    reinterpret_cast<adm::Enkf *>(e)->partial_update_localized(n_local, first_member, n_members, states, stride,
+                                                               n_state, params, n_params, sum, w_rows, u);
   });
 }
 

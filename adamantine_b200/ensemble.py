@@ -126,6 +126,24 @@ class Ensemble:
         """Offset of node (i, j, k) inside one member's vector."""
         return np.asarray(i) + self.pitch * (np.asarray(j) + self.nodes[1] * np.asarray(k))
 
+    def grid(self):
+        """(origin, node spacing, nodes per axis, pitch) of the member vectors:
+        entry a + pitch (b + nodes[1] c) is the support point origin +
+        (a, b, c) spacing (FE_Q(1) and FE_Q(2) support points are uniform)."""
+        geo = self.configs[0].geometry
+        deg = self.configs[0].degree
+        spacing = tuple(float(geo.extent[d]) / (deg * geo.n_cells[d]) for d in range(3))
+        return tuple(float(o) for o in geo.origin[:3]), spacing, self.nodes, self.pitch
+
+    def node_points(self, index) -> np.ndarray:
+        """Support points (n, 3) of the entries ``index`` of a member vector."""
+        origin, spacing, nodes, pitch = self.grid()
+        index = np.asarray(index, np.int64)
+        a = index % pitch
+        b = (index // pitch) % nodes[1]
+        c = index // (pitch * nodes[1])
+        return np.stack([origin[0] + a * spacing[0], origin[1] + b * spacing[1], origin[2] + c * spacing[2]], axis=1)
+
     # ------------------------------------------------------------ stepping
     def _check(self, sol: torch.Tensor):
         if tuple(sol.shape) != (self.n_members, self.stride):
@@ -196,9 +214,13 @@ class Ensemble:
         _lib.check(self._L.adm_ensemble_synchronize(self._h))
 
 
+LOC_NONE, LOC_STEP, LOC_GASPARI_COHN = 0, 1, 2
+_LOC_NAMES = {"none": LOC_NONE, "step_function": LOC_STEP, "gaspari_cohn": LOC_GASPARI_COHN}
+
+
 class EnKF:
     """FP64 ensemble Kalman analysis on the device (perturbed observations,
-    localization "none", Cholesky of H P H^T + R)."""
+    Cholesky of H P H^T + R; localization off until set_localization)."""
 
     def __init__(self, device: int = 0, stream: Optional[torch.cuda.Stream] = None):
         self._L = _lib.load()
@@ -219,6 +241,26 @@ class EnKF:
             self.close()
         except Exception:
             pass
+
+    def set_localization(self, function, cutoff: float, obs_points, grid):
+        """Covariance localization of the following analyses
+        (data_assimilation.localization_cutoff_function / _distance of the
+        reference): function "none", "step_function" or "gaspari_cohn" (or
+        LOC_*), obs_points (m, 3) the support points of the observed entries,
+        grid = (origin, spacing, nodes, pitch) of the state vectors
+        (Ensemble.grid()). obs_points=None removes the localization."""
+        if obs_points is None:
+            _lib.check(self._L.adm_enkf_set_localization(self._h, 0, 1.0, 0, None, None, None, None, 0))
+            return
+        fn = _LOC_NAMES[function.lower()] if isinstance(function, str) else int(function)
+        pts = np.ascontiguousarray(obs_points, np.float64).reshape(-1, 3)
+        origin, spacing, nodes, pitch = grid
+        o = np.ascontiguousarray(origin, np.float64)
+        sp = np.ascontiguousarray(spacing, np.float64)
+        nn = np.ascontiguousarray(nodes, np.int64)
+        _lib.check(self._L.adm_enkf_set_localization(
+            self._h, fn, float(cutoff), len(pts), _ptr(pts, ctypes.c_double), _ptr(o, ctypes.c_double),
+            _ptr(sp, ctypes.c_double), _ptr(nn, ctypes.c_int64), int(pitch)))
 
     def analysis(self, states: torch.Tensor, n_state: int, obs_index: torch.Tensor, obs: torch.Tensor,
                  perturbations: torch.Tensor, obs_var: Optional[torch.Tensor] = None,

@@ -60,13 +60,17 @@ class LibrarySteps:
                                               _dev(out)))
         return out
 
-    def partial_update(self, states, n_state, params, total, w_rows):
+    def partial_update(self, states, n_state, params, total, w_rows, first=0):
+        """The local members' contribution to every member's update; first
+        is the ensemble index of the first local member (used by the
+        localized update, which reads the anomalies kept by gain)."""
         n_local, stride = states.shape
         N = w_rows.shape[1]
         n_params = 0 if params is None else params.shape[1]
         u = torch.empty((N, n_state + n_params), dtype=torch.float64, device=states.device)
-        _lib.check(self._L.adm_enkf_partial_update(self._h, n_local, N, _dev(states), stride, n_state, _p(params),
-                                                   n_params, _dev(total), _dev(w_rows.contiguous()), _dev(u)))
+        _lib.check(self._L.adm_enkf_partial_update_localized(
+            self._h, n_local, int(first), N, _dev(states), stride, n_state, _p(params), n_params, _dev(total),
+            _dev(w_rows.contiguous()), _dev(u)))
         return u
 
     def apply(self, states, n_state, params, u, update_mask=None):
@@ -105,7 +109,8 @@ class ShardedAnalysis:
         total = self.steps.local_sum(states, n_state, params)
         if world > 1:
             dist.all_reduce(total, group=self.group)
-        u = self.steps.partial_update(states, n_state, params, total, w[rank * n_local:(rank + 1) * n_local])
+        u = self.steps.partial_update(states, n_state, params, total, w[rank * n_local:(rank + 1) * n_local],
+                                      first=rank * n_local)
         if world > 1:
             mine = torch.empty((n_local, u.shape[1]), dtype=u.dtype, device=u.device)
             dist.reduce_scatter_tensor(mine, u.contiguous(), group=self.group)

@@ -242,32 +242,59 @@ def run_ensemble(args, dist, local_rank):
     var = torch.full((idx.shape[1],), sigma * sigma, dtype=torch.float64, device=dev)
     obs_d, idx_d, pert_d = (torch.tensor(obs, device=dev), torch.tensor(idx, device=dev),
                             torch.tensor(pert, device=dev))
+    # the same analysis with Gaspari-Cohn localization (cutoff 1 mm, about
+    # three cells), observation points at member 0's observed nodes
+    enkf_loc = EnKF(device=local_rank)
+    enkf_loc.set_localization("gaspari_cohn", LOC_CUTOFF, e.node_points(idx[0]), e.grid())
+    # step function: H P H^T + R may be indefinite, solved by pivoted LU
+    enkf_step = EnKF(device=local_rank)
+    enkf_step.set_localization("step_function", LOC_CUTOFF, e.node_points(idx[0]), e.grid())
     if world > 1:
         from adamantine_b200.sharded import LibrarySteps, ShardedAnalysis
 
         sharded = ShardedAnalysis(LibrarySteps(enkf))
+        sharded_loc = ShardedAnalysis(LibrarySteps(enkf_loc))
+        sharded_step = ShardedAnalysis(LibrarySteps(enkf_step))
 
         def analysis(Y, Pk):
             sharded(Y, e.stride, idx_d, obs_d, pert_d, obs_var=var, params=Pk)
+
+        def analysis_loc(Y, Pk):
+            sharded_loc(Y, e.stride, idx_d, obs_d, pert_d, obs_var=var, params=Pk)
+
+        def analysis_step(Y, Pk):
+            sharded_step(Y, e.stride, idx_d, obs_d, pert_d, obs_var=var, params=Pk)
     else:
 
         def analysis(Y, Pk):
             enkf.analysis(Y, e.stride, idx_d, obs_d, pert_d, obs_var=var, params=Pk)
-    analysis(yb.clone(), P.clone())  # warm-up
-    ya = yb.clone()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    ev[0].record(stream)
-    analysis(ya, P)
-    ev[1].record(stream)
-    ev[1].synchronize()
-    ms_a = ev[0].elapsed_time(ev[1])
+
+        def analysis_loc(Y, Pk):
+            enkf_loc.analysis(Y, e.stride, idx_d, obs_d, pert_d, obs_var=var, params=Pk)
+
+        def analysis_step(Y, Pk):
+            enkf_step.analysis(Y, e.stride, idx_d, obs_d, pert_d, obs_var=var, params=Pk)
+
+    def timed(fn):
+        fn(yb.clone(), P.clone())  # warm-up
+        ya, pa = yb.clone(), P.clone()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        fn(ya, pa)
+        ev[1].record(stream)
+        ev[1].synchronize()
+        return ev[0].elapsed_time(ev[1])
+
+    ms_a = timed(analysis)
+    ms_al = timed(analysis_loc)
+    ms_as = timed(analysis_step)
     ms_la = looped["atomic"][0]
     if dist:
-        tt = torch.tensor([ms_b, ms_l, ms_la, ms_a], device="cuda")
+        tt = torch.tensor([ms_b, ms_l, ms_la, ms_a, ms_al, ms_as], device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms_b, ms_l, ms_la, ms_a = (float(x) for x in tt.tolist())
+        ms_b, ms_l, ms_la, ms_a, ms_al, ms_as = (float(x) for x in tt.tolist())
     return {
         "workload": ENSEMBLE_WORKLOAD, "members_per_gpu": n, "steps": steps, "dt": dt,
         "active_layers": [min(layers), max(layers)],
@@ -282,6 +309,8 @@ def run_ensemble(args, dist, local_rank):
         "batched_path": "one CUDA graph per step (4 stages)",
         "work_items_per_sweep": e.n_work_items(),
         "enkf_analysis_ms": ms_a, "n_obs": int(idx.shape[1]), "augmented_params": 2,
+        "enkf_localized_analysis_ms": ms_al, "enkf_step_localized_analysis_ms": ms_as,
+        "localization": f"gaspari_cohn (Cholesky) and step_function (pivoted LU), cutoff {LOC_CUTOFF * 1e3:g} mm",
         "analysis_members": n * world,
         "analysis_path": "fused (one GPU)" if world == 1 else "sharded: all-gather HX, all-reduce sums, "
                                                             "reduce-scatter member updates (NCCL)",
@@ -289,6 +318,7 @@ def run_ensemble(args, dist, local_rank):
 
 
 ADJOINT_WORKLOAD = "adjoint_q2_64x64x32_rk2_200steps"
+LOC_CUTOFF = 1.0e-3
 
 
 def run_adjoint(args, local_rank):

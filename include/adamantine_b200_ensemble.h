@@ -79,9 +79,14 @@ int adm_ensemble_synchronize(adm_ensemble *e);
 /* Analysis workspace on a device and stream (NULL: default stream). */
 int adm_enkf_create(int device, void *stream, adm_enkf **out);
 int adm_enkf_destroy(adm_enkf *e);
-/* DataAssimilator::update_ensemble (source/DataAssimilator.cc:95-189) with
- * localization "none" (every state entry correlates with every observation),
- * in FP64 on the device, dense Cholesky of H P H^T + R instead of GMRES:
+/* Covariance localization functions (data_assimilation.
+ * localization_cutoff_function, source/DataAssimilator.cc:71-91). */
+#define ADM_LOC_NONE 0
+#define ADM_LOC_STEP 1
+#define ADM_LOC_GASPARI_COHN 2
+
+/* DataAssimilator::update_ensemble (source/DataAssimilator.cc:95-189) in
+ * FP64 on the device, dense Cholesky of H P H^T + R instead of GMRES:
  *   x_k += P H^T (H P H^T + R)^-1 (obs + perturbations_k - H_k x_k)
  * for the augmented states [x_k; p_k], P their sample covariance (divided
  * by N - 1). All arrays are device memory:
@@ -101,6 +106,24 @@ int adm_enkf_destroy(adm_enkf *e);
  * 2 <= N <= 64, 1 <= n_obs <= 16384. Synchronizes. Nothing is updated
  * when H P H^T + R is not positive definite (ADM_ERR_DEVICE) or an index is
  * outside [0, n_state) (ADM_ERR_INVALID). */
+/* Localization of the analyses of this handle
+ * (update_covariance_sparsity_pattern and calc_sample_covariance_sparse,
+ * source/DataAssimilator.cc:512-611,690-752): a covariance entry between two
+ * state entries whose support points are farther apart than cutoff is zero
+ * (the reference's sparsity pattern, whatever the function); within the
+ * cutoff it is scaled by 1 (ADM_LOC_NONE, ADM_LOC_STEP) or by the
+ * Gaspari-Cohn function of 2 d / cutoff (ADM_LOC_GASPARI_COHN). Parameter
+ * rows are not localized. The support point of state entry
+ *   i = a + pitch * (b + nodes[1] * c)   (0 <= a < nodes[0], ...)
+ * is origin + (a, b, c) * spacing; entries with a >= nodes[0] (row padding)
+ * are left unchanged. obs_xyz [n_obs][3] (host) are the support points of
+ * the observed entries. The analyses then need n_state == pitch * nodes[1] *
+ * nodes[2] and n_obs observations. cutoff covering every pair with
+ * ADM_LOC_NONE or ADM_LOC_STEP is the plain analysis; n_obs == 0 removes the
+ * localization. */
+int adm_enkf_set_localization(adm_enkf *e, int32_t function, double cutoff, int32_t n_obs, double const *obs_xyz,
+                              double const *origin, double const *spacing, int64_t const *nodes, int64_t pitch);
+
 int adm_enkf_analysis(adm_enkf *e, int32_t n_members, double *states, int64_t stride,
                       int64_t n_state, double *params, int32_t n_params, int32_t n_obs,
                       int64_t const *obs_index, double const *obs, double const *obs_var,
@@ -134,6 +157,14 @@ int adm_enkf_local_sum(adm_enkf *e, int32_t n_local, double const *states, int64
 int adm_enkf_partial_update(adm_enkf *e, int32_t n_local, int32_t n_members, double const *states, int64_t stride,
                             int64_t n_state, double const *params, int32_t n_params, double const *sum,
                             double const *w_rows, double *u);
+/* adm_enkf_partial_update with the handle's localization: the local members
+ * are members first_member .. first_member + n_local - 1 of the ensemble,
+ * and the observation-space anomalies and weights come from the last
+ * adm_enkf_gain on this handle (same members and observations). Without
+ * localization it is adm_enkf_partial_update. */
+int adm_enkf_partial_update_localized(adm_enkf *e, int32_t n_local, int32_t first_member, int32_t n_members,
+                                      double const *states, int64_t stride, int64_t n_state, double const *params,
+                                      int32_t n_params, double const *sum, double const *w_rows, double *u);
 int adm_enkf_apply(adm_enkf *e, int32_t n_local, double *states, int64_t stride, int64_t n_state, double *params,
                    int32_t n_params, double const *u, uint8_t const *update_mask);
 
