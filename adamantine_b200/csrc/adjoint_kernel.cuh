@@ -137,7 +137,7 @@ __device__ __noinline__ AdjQp adj_qp(SmemPhys const &sp, int mat, double T, doub
   double cp_eff = cp;
   if (NS > 1 && r[1] * r[0] > 0.0)
     cp_eff += sp.latent_term[mat];
-  double const inv = 1.0 / (rho * cp_eff);
+  double const inv = recip(rho * cp_eff);
   double const inv_T = -inv * inv * (rho_T * cp_eff + rho * cp_T);
   double const inv_s = -inv * inv * (rho_s * cp_eff + rho * cp_s);
   double kd[3], kd_T[3], kd_s[3];
@@ -180,6 +180,53 @@ __device__ __noinline__ AdjQp adj_qp(SmemPhys const &sp, int mat, double T, doub
   o.gq = JxW * b * mu;
   o.gc = -(cp / cp_eff) * (o.gk + o.gq);
   // fluxes of the transposed diffusion term in reference coordinates
+  double const cf = -inv * JxW;
+  o.fx = cf * kd[0] * mx * hx2;
+  o.fy = cf * kd[1] * my * hy2;
+  o.fz = cf * kd[2] * mz * hz2;
+  return o;
+}
+
+// adj_qp at a point in one pure state st below the solidus: ratios 1 for st
+// and 0 elsewhere, no liquid-ratio derivative, no latent heat, and a
+// powder adjoint that does not propagate (the point is solid without powder
+// history, or untouched powder, whose s' = 1 - l follows T with
+// dl/dT = 0). One polynomial per property, inline.
+__device__ __forceinline__ AdjQp adj_qp_pure(SmemPhys const &sp, int mat, int st, double T, double mu, double gx,
+                                             double gy, double gz, double mx, double my, double mz, double JxW,
+                                             double Q, double hx2, double hy2, double hz2)
+{
+  double rho, rho_T, cp, cp_T;
+  poly_vd(&sp.poly[mat][P_DENSITY][st][0], sp.prop_deg[P_DENSITY], T, rho, rho_T);
+  poly_vd(&sp.poly[mat][P_SPECIFIC_HEAT][st][0], sp.prop_deg[P_SPECIFIC_HEAT], T, cp, cp_T);
+  double const inv = recip(rho * cp);
+  double const inv_T = -inv * inv * (rho_T * cp + rho * cp_T);
+  double kd[3], kd_T[3];
+  poly_vd(&sp.poly[mat][P_KX][st][0], sp.prop_deg[P_KX], T, kd[0], kd_T[0]);
+  if (sp.isotropic)
+  {
+    kd[1] = kd[2] = kd[0];
+    kd_T[1] = kd_T[2] = kd_T[0];
+  }
+  else
+  {
+    poly_vd(&sp.poly[mat][P_KY][st][0], sp.prop_deg[P_KY], T, kd[1], kd_T[1]);
+    poly_vd(&sp.poly[mat][P_KZ][st][0], sp.prop_deg[P_KZ], T, kd[2], kd_T[2]);
+  }
+  double const uv[3] = {gx * mx * hx2, gy * my * hy2, gz * mz * hz2};
+  double dot_a = 0.0, dot_aT = 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+  {
+    dot_a = fma(kd[d] * inv, uv[d], dot_a);
+    dot_aT = fma(fma(kd_T[d], inv, kd[d] * inv_T), uv[d], dot_aT);
+  }
+  AdjQp o;
+  o.val = JxW * (-dot_aT + Q * inv_T * mu);
+  o.lsin = 0.0;
+  o.gk = JxW * (-dot_a);
+  o.gq = JxW * (Q * inv) * mu;
+  o.gc = -(o.gk + o.gq);
   double const cf = -inv * JxW;
   o.fx = cf * kd[0] * mx * hx2;
   o.fy = cf * kd[1] * my * hy2;
@@ -420,7 +467,17 @@ __global__ void __launch_bounds__(TD<DEG>::NT, 2)
         }
         double const JxW = args.qw[qa] * args.qw[qb] * args.qw[slab] * args.vol;
         AdjQp o;
-        if (NS == 3 && no_powder)
+        bool const with_powder = NS == 3 && !no_powder;
+        double const s_in = with_powder ? A.s_in[qbase + i] : 0.0;
+        // one pure state below the solidus (see adj_qp_pure)
+        int pure = -1;
+        if (NS == 1)
+          pure = 0;
+        else if (T < sp.props[mat][Q_SOLIDUS])
+          pure = !with_powder ? 0 : (s_in == 1.0 ? 2 : -1);
+        if (pure >= 0)
+          o = adj_qp_pure(sp, mat, pure, T, mu, gx, gy, gz, mx, my, mz, JxW, Q, hx2, hy2, hz2);
+        else if (NS == 3 && no_powder)
         {
           // a cell without powder at the start keeps s = 0 (s' = min(1 - l,
           // 0) = 0): its points are solid/liquid mixtures and the powder
@@ -429,12 +486,11 @@ __global__ void __launch_bounds__(TD<DEG>::NT, 2)
         }
         else
         {
-          double const s_in = NS == 3 ? A.s_in[qbase + i] : 0.0;
           double const lam_out = NS == 3 ? A.lam_s_out[qbase + i] : 0.0;
           o = adj_qp<NS>(sp, mat, T, mu, gx, gy, gz, mx, my, mz, s_in, lam_out, JxW, Q, hx2, hy2, hz2);
-          if (NS == 3)
-            A.lam_s_in[qbase + i] = o.lsin;
         }
+        if (with_powder)
+          A.lam_s_in[qbase + i] = o.lsin;
         g_k += o.gk;
         g_q += o.gq;
         g_c += o.gc;
