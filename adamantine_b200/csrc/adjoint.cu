@@ -444,7 +444,7 @@ private:
       ADM_CK(cudaMemcpyAsync(Ystore_.p + slot * n_, src, n_ * sizeof(double), cudaMemcpyDeviceToDevice, st));
       if (t.ns_ == 3)
         launch_expand_powder(t.cell_info_d_.p, NN_, t.powder_mode_.p, t.powder_cell_.p, t.powder_q_.p,
-                             Sstore_.p + slot * qn, C_, st);
+                             Sstore_.p + slot * qn, C_, st, init_mode_.p);
       t.launch_pass(a, src);
     }
   }

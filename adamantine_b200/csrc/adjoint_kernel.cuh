@@ -90,16 +90,14 @@ struct AdjQp
   double fx, fy, fz, val, lsin, gk, gq, gc;
 };
 
-// The transposed coefficients at one Gauss point (out of line: the kernel
-// calls it for the 9 or 4 points of a thread's level, and one copy of the
-// code keeps the instruction footprint small). Inputs: the field T and mu
+// The transposed coefficients at one Gauss point. Inputs: the field T and mu
 // with their reference gradients, the powder ratio before the stage, the
 // adjoint of the powder ratio after it, JxW, the source value Q and the
 // squared inverse cell sizes. Outputs: the reference-space fluxes and the
 // value term of the transposed operator, the adjoint of the powder ratio
 // before the stage and the three log-derivative contributions.
 template <int NS>
-__device__ __noinline__ AdjQp adj_qp(SmemPhys const &sp, int mat, double T, double mu, double gx, double gy,
+__device__ __forceinline__ AdjQp adj_qp(SmemPhys const &sp, int mat, double T, double mu, double gx, double gy,
                                      double gz, double mx, double my, double mz, double s_in, double lam_out,
                                      double JxW, double Q, double hx2, double hy2, double hz2)
 {
@@ -232,6 +230,25 @@ __device__ __forceinline__ AdjQp adj_qp_pure(SmemPhys const &sp, int mat, int st
   o.fy = cf * kd[1] * my * hy2;
   o.fz = cf * kd[2] * mz * hz2;
   return o;
+}
+
+// One Gauss point of the adjoint kernel: the pure-state path, the cells
+// without powder at the start (solid/liquid mixtures: the powder adjoint
+// never reaches the temperature or the parameters there) or the full
+// mixture. Out of line: the kernel calls it for the 9 or 4 points of a
+// thread's level, and one copy of the code keeps the instruction footprint
+// small.
+template <int NS>
+__device__ __noinline__ AdjQp adj_point(SmemPhys const &sp, int mat, int pure, bool no_powder, double T,
+                                        double mu, double gx, double gy, double gz, double mx, double my,
+                                        double mz, double s_in, double lam_out, double JxW, double Q, double hx2,
+                                        double hy2, double hz2)
+{
+  if (pure >= 0)
+    return adj_qp_pure(sp, mat, pure, T, mu, gx, gy, gz, mx, my, mz, JxW, Q, hx2, hy2, hz2);
+  if (NS == 3 && no_powder)
+    return adj_qp<NS == 3 ? 2 : NS>(sp, mat, T, mu, gx, gy, gz, mx, my, mz, 0.0, 0.0, JxW, Q, hx2, hy2, hz2);
+  return adj_qp<NS>(sp, mat, T, mu, gx, gy, gz, mx, my, mz, s_in, lam_out, JxW, Q, hx2, hy2, hz2);
 }
 
 template <int DEG, int NS>
@@ -475,20 +492,9 @@ __global__ void __launch_bounds__(TD<DEG>::NT, 2)
           pure = 0;
         else if (T < sp.props[mat][Q_SOLIDUS])
           pure = !with_powder ? 0 : (s_in == 1.0 ? 2 : -1);
-        if (pure >= 0)
-          o = adj_qp_pure(sp, mat, pure, T, mu, gx, gy, gz, mx, my, mz, JxW, Q, hx2, hy2, hz2);
-        else if (NS == 3 && no_powder)
-        {
-          // a cell without powder at the start keeps s = 0 (s' = min(1 - l,
-          // 0) = 0): its points are solid/liquid mixtures and the powder
-          // adjoint there never reaches the temperature or the parameters
-          o = adj_qp<NS == 3 ? 2 : NS>(sp, mat, T, mu, gx, gy, gz, mx, my, mz, 0.0, 0.0, JxW, Q, hx2, hy2, hz2);
-        }
-        else
-        {
-          double const lam_out = NS == 3 ? A.lam_s_out[qbase + i] : 0.0;
-          o = adj_qp<NS>(sp, mat, T, mu, gx, gy, gz, mx, my, mz, s_in, lam_out, JxW, Q, hx2, hy2, hz2);
-        }
+        double const lam_out = (with_powder && pure < 0) ? A.lam_s_out[qbase + i] : 0.0;
+        o = adj_point<NS>(sp, mat, pure, no_powder, T, mu, gx, gy, gz, mx, my, mz, s_in, lam_out, JxW, Q, hx2,
+                          hy2, hz2);
         if (with_powder)
           A.lam_s_in[qbase + i] = o.lsin;
         g_k += o.gk;

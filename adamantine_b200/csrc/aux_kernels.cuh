@@ -657,12 +657,17 @@ __global__ void get_state_kernel(uint32_t const *cell_info, int ns, int NN, int 
 // Expand the powder representation to [C][NN] values (diagnostics).
 __global__ void expand_powder_kernel(uint32_t const *cell_info, int NN,
                                      uint8_t const *pmode, double const *pcell,
-                                     double const *pq, double *out, size_t C)
+                                     double const *pq, double *out, size_t C,
+                                     uint8_t const *skip)
 {
   size_t const idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (idx >= C * NN)
     return;
   size_t const c = idx / NN;
+  // cells whose skip entry is 0 are left unwritten (no powder at the start
+  // of an adjoint run: their readers never look)
+  if (skip && skip[c] == 0)
+    return;
   int const mode = pmode[c];
   out[idx] = mode == 2 ? pq[idx] : (mode == 1 ? pcell[c] : 0.0);
 }

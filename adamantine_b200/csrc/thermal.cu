@@ -876,10 +876,10 @@ void launch_stage_finalize(KernelArgs const &a, size_t n_nodes, int n_members, c
 }
 
 void launch_expand_powder(uint32_t const *cell_info, int NN, uint8_t const *pmode, double const *pcell,
-                          double const *pq, double *out, size_t C, cudaStream_t stream)
+                          double const *pq, double *out, size_t C, cudaStream_t stream, uint8_t const *skip)
 {
   expand_powder_kernel<<<(unsigned)((C * NN + 255) / 256), 256, 0, stream>>>(cell_info, NN, pmode, pcell, pq,
-                                                                            out, C);
+                                                                            out, C, skip);
   ADM_CK(cudaGetLastError());
 }
 
@@ -1123,7 +1123,7 @@ void Thermal::get_qp_powder(double *host)
   DevBuf<double> tmp;
   tmp.alloc(C * NN);
   expand_powder_kernel<<<(unsigned)((C * NN + 255) / 256), 256, 0, stream_>>>(
-      cell_info_d_.p, NN, powder_mode_.p, powder_cell_.p, powder_q_.p, tmp.p, C);
+      cell_info_d_.p, NN, powder_mode_.p, powder_cell_.p, powder_q_.p, tmp.p, C, nullptr);
   ADM_CK(cudaGetLastError());
   ADM_CK(cudaMemcpyAsync(host, tmp.p, C * NN * sizeof(double), cudaMemcpyDeviceToHost, stream_));
   ADM_CK(cudaStreamSynchronize(stream_));

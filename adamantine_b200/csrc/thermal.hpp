@@ -156,8 +156,11 @@ void launch_stage_prepare(MemberData *members, int n, double c, cudaStream_t str
 // Per-Gauss-point powder ratios [C][NN] from the sparse powder history.
 // Stage update of the atomic schedule for n_members members (a.members).
 void launch_stage_finalize(KernelArgs const &a, size_t n_nodes, int n_members, cudaStream_t stream);
+// The per-point powder ratio [C][NN] from the sparse modes; cells with
+// skip[c] == 0 are not written (skip may be null).
 void launch_expand_powder(uint32_t const *cell_info, int NN, uint8_t const *pmode, double const *pcell,
-                          double const *pq, double *out, size_t C, cudaStream_t stream);
+                          double const *pq, double *out, size_t C, cudaStream_t stream,
+                          uint8_t const *skip = nullptr);
 
 class Ensemble;
 class Adjoint;
