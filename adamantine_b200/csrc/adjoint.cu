@@ -117,17 +117,28 @@ struct LamTerms
   int n;
 };
 
-// mu = inv_mass * (cb * lam_new + sum_l c_l lam_Y_l)
-__global__ void lamk_kernel(double *mu, double const *inv_mass, double const *lam_new, double cb, LamTerms t,
-                            size_t n)
+// lam += sum of the pending stage adjoints of the step after (pend, at the
+// first stage of a step), mu = inv_mass * (cb * lam + sum_l c_l lam_Y_l),
+// and the stage adjoint the next launch accumulates into is cleared
+// (zero, which may be one of the pending vectors: read before written).
+__global__ void lamk_kernel(double *mu, double const *inv_mass, double *lam, LamTerms pend, double cb, LamTerms t,
+                            double *zero, size_t n)
 {
   size_t const i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (i >= n)
     return;
-  double s = cb * lam_new[i];
+  double L = lam[i];
+  if (pend.n > 0)
+  {
+    for (int l = 0; l < pend.n; ++l)
+      L += pend.v[l][i];
+    lam[i] = L;
+  }
+  double s = cb * L;
   for (int l = 0; l < t.n; ++l)
     s = fma(t.c[l], t.v[l][i], s);
   mu[i] = inv_mass[i] * s;
+  zero[i] = 0.0;
 }
 
 // lam += sum_l lam_Y_l
@@ -236,6 +247,13 @@ public:
     grad_d_.alloc(3);
     ADM_CK(cudaMemsetAsync(grad_d_.p, 0, 3 * sizeof(double), st));
     int const n_seg = (n_steps + K - 1) / K;
+    // the stage adjoints of a step are added into lam by the first stage
+    // launch of the step before (and once at the end)
+    LamTerms all{};
+    all.n = S;
+    for (int i = 0; i < S; ++i)
+      all.v[i] = lamY_.p + (size_t)i * n_;
+    bool pending = false;
     for (int seg = n_seg - 1; seg >= 0; --seg)
     {
       int const n0 = seg * K, n1 = std::min(n_steps, n0 + K);
@@ -266,10 +284,14 @@ public:
               lt.c[lt.n] = dt * t.tab_.a[l][i];
               ++lt.n;
             }
-          lamk_kernel<<<blocks(n_), 256, 0, st>>>(mu_.p, t.inv_mass_.p, lam_.p, dt * t.tab_.b[i], lt, n_);
-          ADM_CK(cudaGetLastError());
           double *lamYi = lamY_.p + (size_t)i * n_;
-          ADM_CK(cudaMemsetAsync(lamYi, 0, n_ * sizeof(double), st));
+          LamTerms pend{};
+          pend.n = 0;
+          if (i == S - 1 && pending)
+            pend = all;
+          lamk_kernel<<<blocks(n_), 256, 0, st>>>(mu_.p, t.inv_mass_.p, lam_.p, pend, dt * t.tab_.b[i], lt, lamYi,
+                                                  n_);
+          ADM_CK(cudaGetLastError());
           t.prepare_stage(t.tab_.c[i]);
           size_t const slot = (size_t)(n - n0) * S + i;
           AdjArgs A;
@@ -290,13 +312,13 @@ public:
           if (ns3)
             std::swap(ls_a_.p, ls_b_.p);
         }
-        LamTerms all{};
-        all.n = S;
-        for (int i = 0; i < S; ++i)
-          all.v[i] = lamY_.p + (size_t)i * n_;
-        sum_kernel<<<blocks(n_), 256, 0, st>>>(lam_.p, all, n_);
-        ADM_CK(cudaGetLastError());
+        pending = true;
       }
+    }
+    if (pending)
+    {
+      sum_kernel<<<blocks(n_), 256, 0, st>>>(lam_.p, all, n_);
+      ADM_CK(cudaGetLastError());
     }
     double g[3] = {0, 0, 0};
     ADM_CK(cudaMemcpyAsync(g, grad_d_.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
