@@ -101,6 +101,11 @@ SIGNATURES = {
     "adm_enkf_set_localization": [_VP, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, _VP, _VP, _VP, _VP,
                                   ctypes.c_int64],
     "adm_enkf_apply": [_VP, ctypes.c_int32, _VP, ctypes.c_int64, ctypes.c_int64, _VP, ctypes.c_int32, _VP, _VP],
+    "adm_microstructure_create": [_VP, ctypes.POINTER(_VP)],
+    "adm_microstructure_destroy": [_VP],
+    "adm_microstructure_set_old_temperature": [_VP, _VP],
+    "adm_microstructure_compute_G_and_R": [_VP, _VP, ctypes.c_double, ctypes.c_int64, _VP,
+                                           ctypes.POINTER(ctypes.c_int64)],
     "adm_enkf_analysis": [_VP, ctypes.c_int32, _VP, ctypes.c_int64, ctypes.c_int64, _VP, ctypes.c_int32,
                           ctypes.c_int32, _VP, _VP, _VP, _VP, _VP, _VP],
 }

@@ -265,6 +265,7 @@ private:
   friend class Ensemble;
   friend class Adjoint;
   friend struct Checkpoint;
+  friend class Microstructure;
   void rebuild();
   void upload_member();
   KernelArgs base_args() const;

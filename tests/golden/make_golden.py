@@ -13,6 +13,10 @@ Run in a container where the reference is mounted at /root/reference:
   seconds, mode 0 = line at `param` m/s), and the box file
   material_path_test_material_deposition.txt as rows (center[3], size[3],
   time, angle).
+* microstructure_G_R_gold_1.txt, microstructure_G_R_gold_2.txt -- the gold
+  files of test_microstructure.cc (one 10 mm x 10 mm Q2 cell, liquidus 100,
+  old field 1000 (+ (x - 1)^2 + y^2 in the second), new field 50 (+ the
+  same), delta_t 1.1), copied line by line.
 """
 import os
 import sys
@@ -41,6 +45,13 @@ def main():
     out["material_path"] = np.array([[float(v) for v in ln.split()] for ln in lines[1:] if ln.strip()])
     np.savez(os.path.join(HERE, "deposition_inputs.npz"), **out)
     print("wrote deposition_inputs.npz", {k: v.shape for k, v in out.items()})
+
+    for k in (1, 2):
+        name = f"microstructure_G_R_gold_{k}.txt"
+        lines = [ln for ln in open(os.path.join(data, name)).read().split("\n") if ln.strip()]
+        with open(os.path.join(HERE, name), "w") as fh:
+            fh.write("\n".join(lines) + "\n")
+        print("wrote", name, len(lines))
 
 
 def segments(text):

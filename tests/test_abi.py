@@ -15,7 +15,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def header_functions(header="adamantine_b200.h"):
     text = open(os.path.join(ROOT, "include", header)).read()
-    return sorted(set(re.findall(r"\b(adm_[a-z0-9_]+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(adm_[A-Za-z0-9_]+)\s*\(", text)))
 
 
 def all_headers():
@@ -32,7 +32,8 @@ def test_library_exports_every_declared_symbol():
 
 def test_python_binding_covers_header():
     names = set(header_functions()) | set(header_functions("adamantine_b200_ensemble.h")) | \
-        set(header_functions("adamantine_b200_adjoint.h")) | set(header_functions("adamantine_b200_deposition.h"))
+        set(header_functions("adamantine_b200_adjoint.h")) | set(header_functions("adamantine_b200_deposition.h")) | \
+        set(header_functions("adamantine_b200_microstructure.h"))
     assert names - {"adm_last_error"} == set(_lib.SIGNATURES)
 
 
