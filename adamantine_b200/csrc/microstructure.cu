@@ -2,10 +2,11 @@
 // set_old_temperature and compute_G_and_R, source/Microstructure.hh:41-207,
 // Microstructure.cc:57-63).
 //
-// One thread per (active cell, support point): the point's node went from
-// above the cell material's liquidus (old field) to at or below it (new
-// field) during the step; the thread evaluates the gradient of the cell's
-// interpolant of the new field at that node with the nodal derivative
+// A node scan lists the nodes that crossed some material's liquidus
+// downward during the step; then one thread per (listed node, cell around
+// it) checks the cell (active, its material's liquidus) and evaluates the
+// gradient of the cell's interpolant of the new field at that node with the
+// nodal derivative
 // matrix of the 1D Lagrange basis (the Gauss-Lobatto points of
 // QGaussLobatto(p + 1) are the support points), G = |grad T|, the cooling
 // rate as the reference computes it (old - new / delta_t, the division
@@ -37,36 +38,79 @@ struct GrGeom
   double D[3][3];    // D[a][i] = phi_i'(pt[a])
 };
 
+// Pass 1, one thread per node (coalesced): the nodes whose old value is
+// above and new value at or below the liquidus of some material go to a
+// compact list (the few nodes the step solidified).
+__global__ void gr_scan_kernel(GrGeom g, int nn0, size_t n_nodes, int n_mat, MaterialDesc const *mat,
+                               double const *t_old, double const *t_new, int64_t *list, unsigned long long *count,
+                               unsigned long long cap)
+{
+  size_t const i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= n_nodes || (int)(i % g.pitch) >= nn0)
+    return;
+  double const to = t_old[i], tn = t_new[i];
+  bool hit = false;
+  for (int m = 0; m < n_mat; ++m)
+  {
+    double const liq = mat->props[m][Q_LIQUIDUS];
+    hit |= to > liq && tn <= liq;
+  }
+  if (!hit)
+    return;
+  unsigned long long const slot = atomicAdd(count, 1ull);
+  if (slot < cap)
+    list[slot] = (int64_t)i;
+}
+
+// Pass 2, one thread per (listed node, cell that may hold it): the up to
+// eight cells around the node (one per axis where the node is inside a
+// cell), each with its own material's liquidus; the crossing records of the
+// reference with the key (cell, point).
 __global__ void gr_kernel(GrGeom g, uint32_t const *cell_info, MaterialDesc const *mat, double const *t_old,
-                          double const *t_new, double dt, size_t n_cells, double *rec, int64_t *key,
-                          unsigned long long *count, unsigned long long cap)
+                          double const *t_new, double dt, int64_t const *list, size_t n_list, double *rec,
+                          int64_t *key, unsigned long long *count, unsigned long long cap)
 {
   int const n = g.deg + 1, nq = n * n * n;
   size_t const idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (idx >= n_cells * nq)
+  if (idx >= n_list * 8)
     return;
-  size_t const c = idx / nq;
-  int const q = (int)(idx % nq);
+  size_t const node = (size_t)list[idx / 8];
+  int const combo = (int)(idx % 8);
+  int const nidx[3] = {(int)(node % g.pitch), (int)((node / g.pitch) % g.nn1),
+                       (int)(node / ((size_t)g.pitch * g.nn1))};
+  int cell[3], loc[3];
+  for (int d = 0; d < 3; ++d)
+  {
+    int const lower = (combo >> d) & 1; // 1: the cell below the node along d
+    int cd = nidx[d] / g.deg;
+    if (lower)
+    {
+      if (nidx[d] % g.deg != 0)
+        return; // inside a cell along d: only one cell holds the node
+      cd -= 1;
+    }
+    if (cd < 0 || cd >= g.nc[d])
+      return;
+    cell[d] = cd;
+    loc[d] = nidx[d] - g.deg * cd;
+  }
+  size_t const c = cell[0] + (size_t)g.nc[0] * (cell[1] + (size_t)g.nc[1] * cell[2]);
   uint32_t const info = cell_info[c];
   if (!(info & CI_ACTIVE))
     return;
-  int const loc[3] = {q % n, (q / n) % n, q / (n * n)};
-  int const cell[3] = {(int)(c % g.nc[0]), (int)((c / g.nc[0]) % g.nc[1]), (int)(c / ((size_t)g.nc[0] * g.nc[1]))};
-  int const ix = g.deg * cell[0] + loc[0], iy = g.deg * cell[1] + loc[1], iz = g.deg * cell[2] + loc[2];
-  size_t const node = ix + (size_t)g.pitch * (iy + (size_t)g.nn1 * iz);
   double const liq = mat->props[(info >> CI_MAT_SHIFT) & 15][Q_LIQUIDUS];
   double const to = t_old[node], tn = t_new[node];
   if (!(to > liq && tn <= liq))
     return;
+  int const q = loc[0] + n * (loc[1] + n * loc[2]);
   size_t const stride[3] = {1, (size_t)g.pitch, (size_t)g.pitch * g.nn1};
-  size_t const first[3] = {node - (size_t)loc[0] * stride[0], node - (size_t)loc[1] * stride[1],
-                           node - (size_t)loc[2] * stride[2]};
   double G2 = 0.0;
   for (int d = 0; d < 3; ++d)
   {
+    size_t const first = node - (size_t)loc[d] * stride[d];
     double s = 0.0;
     for (int i = 0; i < n; ++i)
-      s = __dadd_rn(s, __dmul_rn(g.D[loc[d]][i], t_new[first[d] + i * stride[d]]));
+      s = __dadd_rn(s, __dmul_rn(g.D[loc[d]][i], t_new[first + i * stride[d]]));
     double const gd = s / g.h[d];
     G2 = __dadd_rn(G2, __dmul_rn(gd, gd));
   }
@@ -81,7 +125,7 @@ __global__ void gr_kernel(GrGeom g, uint32_t const *cell_info, MaterialDesc cons
   r[3] = G;
   r[4] = rate;
   r[5] = rate / G;
-  key[slot] = (int64_t)idx;
+  key[slot] = (int64_t)(c * nq + q);
 }
 } // namespace
 
@@ -143,16 +187,34 @@ public:
           g.D[a][i] = D[a][i];
       }
     }
-    size_t const nq = (size_t)(m.deg + 1) * (m.deg + 1) * (m.deg + 1);
-    size_t const total = m.n_cells * nq;
     count_.alloc(1);
-    unsigned long long n_rec = 0;
+    // pass 1: the crossing nodes (the list grows and the scan reruns when
+    // it overflows)
+    unsigned long long n_nodes_hit = 0;
+    int const n_mat = t.cfg_.n_materials;
     for (int pass = 0; pass < 2; ++pass)
     {
       ADM_CK(cudaMemsetAsync(count_.p, 0, sizeof(unsigned long long), st));
-      if (total > 0)
-        gr_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(g, t.cell_info_d_.p, t.mat_d_.p, old_.p, t_new,
-                                                                    dt, m.n_cells, rec_.p, key_.p, count_.p, cap_);
+      gr_scan_kernel<<<(unsigned)((m.n_nodes + 255) / 256), 256, 0, st>>>(g, m.nn[0], m.n_nodes, n_mat, t.mat_d_.p,
+                                                                          old_.p, t_new, list_.p, count_.p,
+                                                                          list_cap_);
+      ADM_CK(cudaGetLastError());
+      ADM_CK(cudaMemcpyAsync(&n_nodes_hit, count_.p, sizeof(n_nodes_hit), cudaMemcpyDeviceToHost, st));
+      ADM_CK(cudaStreamSynchronize(st));
+      if (n_nodes_hit <= list_cap_)
+        break;
+      list_cap_ = std::max<unsigned long long>(n_nodes_hit, 2 * list_cap_);
+      list_.alloc(list_cap_);
+    }
+    // pass 2: the records of the cells around those nodes
+    unsigned long long n_rec = 0;
+    for (int pass = 0; pass < 2 && n_nodes_hit > 0; ++pass)
+    {
+      ADM_CK(cudaMemsetAsync(count_.p, 0, sizeof(unsigned long long), st));
+      size_t const threads = 8 * (size_t)n_nodes_hit;
+      gr_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(g, t.cell_info_d_.p, t.mat_d_.p, old_.p, t_new,
+                                                                   dt, list_.p, n_nodes_hit, rec_.p, key_.p,
+                                                                   count_.p, cap_);
       ADM_CK(cudaGetLastError());
       ADM_CK(cudaMemcpyAsync(&n_rec, count_.p, sizeof(n_rec), cudaMemcpyDeviceToHost, st));
       ADM_CK(cudaStreamSynchronize(st));
@@ -182,9 +244,9 @@ public:
 private:
   Thermal &th_;
   DevBuf<double> old_, rec_;
-  DevBuf<int64_t> key_;
+  DevBuf<int64_t> key_, list_;
   DevBuf<unsigned long long> count_;
-  unsigned long long cap_ = 0;
+  unsigned long long cap_ = 0, list_cap_ = 0;
   bool has_old_ = false;
 };
 

@@ -423,6 +423,25 @@ def run_deposition(args, local_rank, with_cpu):
     ev1.synchronize()
     ms = ev0.elapsed_time(ev1)
     assert g.device_error() == 0
+    # microstructure records around 5 more steps (save the field, step,
+    # collect the liquidus crossings): host time of the two calls
+    from adamantine_b200.microstructure import Microstructure
+
+    micro = Microstructure(g)
+    ms_micro, n_records = 0.0, 0
+    for _ in range(5):
+        dep.step(t, dt, 300.0, y)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        micro.set_old_temperature(y)
+        torch.cuda.synchronize()
+        ms_micro += 1e3 * (time.perf_counter() - t0)
+        t = g.evolve_one_time_step(t, dt, y)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        n_records += len(micro.compute_G_and_R(y, dt))
+        ms_micro += 1e3 * (time.perf_counter() - t0)
+    micro.close()
     C = g.n_cells
     # fused RK4 stages: 32 + 48 + 48 + 40 bytes per node (stage input, inverse
     # mass, y, running sum, next stage vector) and 13 bytes per cell per stage
@@ -433,6 +452,7 @@ def run_deposition(args, local_rank, with_cpu):
         "hbm_gbs_algorithmic": bytes_step * steps / (ms * 1e-3) / 1e9, "cells_activated": activated + n_act,
         "boxes": boxes.n, "activation": "device append list, driver window per step",
         "schedule": ["coloured", "atomic"][schedule],
+        "microstructure_ms_per_step": ms_micro / 5, "microstructure_records_per_step": n_records / 5,
     }
     if with_cpu:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
