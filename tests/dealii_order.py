@@ -21,7 +21,10 @@ def _vcoord(v, dim):
     return [(v >> d) & 1 for d in range(dim)]
 
 
-def dof_to_node(dim, n_cells, degree):
+def dof_to_node(dim, n_cells, degree, active=None):
+    """active: per cell (lexicographic), or None for all. Cells without
+    degrees of freedom (FE_Nothing, inactive) are skipped by the walk, so the
+    DoFs of an hp mesh are those of its active cells in the same order."""
     nc = list(n_cells[:dim])
     nn = [degree * n + 1 for n in nc]
 
@@ -48,7 +51,9 @@ def dof_to_node(dim, n_cells, degree):
                 objects.append(loc)
         objects.append([1] * dim)
     order, seen = [], set()
-    for cell_rev in itertools.product(*[range(n) for n in reversed(nc)]):
+    for ci, cell_rev in enumerate(itertools.product(*[range(n) for n in reversed(nc)])):
+        if active is not None and not active[ci]:
+            continue
         cc = list(reversed(cell_rev))
         for loc in objects:
             g = node(cc, loc)

@@ -17,6 +17,12 @@ Run in a container where the reference is mounted at /root/reference:
   files of test_microstructure.cc (one 10 mm x 10 mm Q2 cell, liquidus 100,
   old field 1000 (+ (x - 1)^2 + y^2 in the second), new field 50 (+ the
   same), delta_t 1.1), copied line by line.
+* integration_3d_gold.txt -- tests/data/integration_3d_gold.txt of the
+  reference: the 26177 temperatures (4 significant digits, deal.II DoF
+  order) after 100 forward Euler steps of demo_316_short_anisotropic.info
+  (test_integration_3d.cc:112-115), copied as is; and
+  integration_3d_scan_path.npy, the segments of demo_316_short_scan_path.txt
+  as (end_time, power_modifier, x, y, z) rows.
 """
 import os
 import sys
@@ -45,6 +51,15 @@ def main():
     out["material_path"] = np.array([[float(v) for v in ln.split()] for ln in lines[1:] if ln.strip()])
     np.savez(os.path.join(HERE, "deposition_inputs.npz"), **out)
     print("wrote deposition_inputs.npz", {k: v.shape for k, v in out.items()})
+
+    src = os.path.join(data, "integration_3d_gold.txt")
+    vals = open(src).read().split()
+    assert len(vals) == 26177, len(vals)
+    with open(os.path.join(HERE, "integration_3d_gold.txt"), "w") as fh:
+        fh.write(" ".join(vals) + "\n")
+    np.save(os.path.join(HERE, "integration_3d_scan_path.npy"),
+            np.array(segments(open(os.path.join(data, "demo_316_short_scan_path.txt")).read())))
+    print("wrote integration_3d_gold.txt", len(vals), "and integration_3d_scan_path.npy")
 
     for k in (1, 2):
         name = f"microstructure_G_R_gold_{k}.txt"

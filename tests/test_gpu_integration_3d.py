@@ -1,0 +1,42 @@
+"""The reference's 3-D integration case on the GPU through the C ABI: the
+anisotropic demo (deposition along the scan path with the driver's window,
+conductivity rotated by the deposition angle, solid / powder / liquid,
+Goldak source, forward Euler) for its 100 steps, against the CPU oracle run
+the same way (every active node to 1e-9), and against the reference's gold
+file (test_integration_3d.cc:112-115) in its own 4-significant-digit format
+and deal.II DoF order."""
+import numpy as np
+import pytest
+
+from dealii_order import dof_to_node
+from integration_demo import BOX, DT, DURATION, NEW_T, demo_config, gold_text, run_oracle
+from pairs import rel_max
+
+from adamantine_b200.deposition import Deposition, deposition_boxes
+from adamantine_b200.thermal import ThermalPhysics
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_integration_3d_on_the_gpu(schedule):
+    cfg = demo_config()
+    boxes = deposition_boxes(cfg, *BOX)
+    g = ThermalPhysics(cfg)
+    g.set_schedule(schedule)
+    dep = Deposition(g, boxes, deposition_time=0.0, duration=DURATION)
+    y = g.initialize_dof_vector(300.0)
+    t, n = 0.0, 0
+    while t < DURATION:
+        dep.step(t, DT, NEW_T, y)
+        t = g.evolve_one_time_step(t, DT, y)
+        n += 1
+    assert n == 100 and g.device_error() == 0
+    y_ref, active, _ = run_oracle(cfg, boxes)
+    order = dof_to_node(3, cfg.geometry.n_cells, 2, active=active)
+    got = g.to_grid(y).reshape(-1)[order]
+    assert rel_max(got, y_ref[order]) <= 1e-9
+    gold = np.array([float(v) for v in gold_text()])
+    assert len(got) == len(gold) == 26177
+    # within the gold's printed precision (half a unit of the 4th digit)
+    assert np.all(np.abs(got - gold) <= 0.5e-3 * 10.0 ** np.floor(np.log10(np.abs(gold))) * (1 + 1e-9))
