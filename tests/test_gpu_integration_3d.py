@@ -40,3 +40,38 @@ def test_integration_3d_on_the_gpu(schedule):
     assert len(got) == len(gold) == 26177
     # within the gold's printed precision (half a unit of the 4th digit)
     assert np.all(np.abs(got - gold) <= 0.5e-3 * 10.0 ** np.floor(np.log10(np.abs(gold))) * (1 + 1e-9))
+
+
+@pytest.mark.parametrize("exact", [False, True])
+def test_integration_3d_checkpoint_restart(tmp_path, exact):
+    """test_integration_3d.cc:117-165: a checkpoint after 80 of the 100 steps,
+    then a restart (fresh handle, fresh deposition window, as the driver
+    restarts) ends at the uninterrupted run's temperatures to 1e-10. With the
+    reference's restart (cell states broadcast to the points) this holds
+    because no point of the demo reaches the solidus."""
+    cfg = demo_config()
+    boxes = deposition_boxes(cfg, *BOX)
+
+    def run(g, dep, y, t, n_stop):
+        n = 0
+        while t < DURATION and n < n_stop:
+            dep.step(t, DT, NEW_T, y)
+            t = g.evolve_one_time_step(t, DT, y)
+            n += 1
+        return t
+
+    g1 = ThermalPhysics(cfg)
+    y1 = g1.initialize_dof_vector(300.0)
+    run(g1, Deposition(g1, boxes, deposition_time=0.0, duration=DURATION), y1, 0.0, 1000)
+
+    g2 = ThermalPhysics(cfg)
+    y2 = g2.initialize_dof_vector(300.0)
+    t = run(g2, Deposition(g2, boxes, deposition_time=0.0, duration=DURATION), y2, 0.0, 80)
+    path = str(tmp_path / "test_checkpoint")
+    g2.save_checkpoint(path, t, y2)
+    g3 = ThermalPhysics(cfg)
+    y3 = g3.initialize_dof_vector(0.0)
+    t3 = g3.load_checkpoint(path, y3, exact=exact)
+    assert t3 == t
+    run(g3, Deposition(g3, boxes, deposition_time=0.0, duration=DURATION), y3, t3, 1000)
+    assert rel_max(g3.to_grid(y3), g1.to_grid(y1)) <= 1e-10
