@@ -91,6 +91,7 @@ SIGNATURES = {
     "adm_adjoint_gradient": [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_int32, _VP, _D, _D,
                              _VP],
     "adm_adjoint_vmult_transpose": [_VP, _VP, _VP, _VP, _D],
+    "adm_adjoint_set_flush": [_VP, ctypes.c_double],
     "adm_enkf_observe": [_VP, ctypes.c_int32, _VP, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, _VP, _VP],
     "adm_enkf_gain": [_VP, ctypes.c_int32, ctypes.c_int32, _VP, _VP, _VP, _VP, _VP, _VP],
     "adm_enkf_local_sum": [_VP, ctypes.c_int32, _VP, ctypes.c_int64, ctypes.c_int64, _VP, ctypes.c_int32, _VP],

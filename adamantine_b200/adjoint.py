@@ -142,6 +142,12 @@ class AdjointProblem:
                                                 _dev(self.y0), ctypes.byref(J), _ptr(g, ctypes.c_double), None))
         return float(J.value), g / np.asarray(self._theta, np.float64)
 
+    def set_flush(self, flush: float):
+        """Adjoint values at or below flush x the stage's largest count as
+        zero in the gradient (tiles of them are skipped); 0: exact zeros
+        only. Default 1e-30."""
+        _lib.check(self._L.adm_adjoint_set_flush(self._h, float(flush)))
+
     def vmult_transpose(self, y: torch.Tensor, mu: torch.Tensor):
         """((dr/dT)^T mu, log-derivatives of mu . r) at y."""
         out = torch.empty_like(y)

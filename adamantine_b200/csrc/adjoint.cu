@@ -117,16 +117,9 @@ struct LamTerms
   int n;
 };
 
-// lam += sum of the pending stage adjoints of the step after (pend, at the
-// first stage of a step), mu = inv_mass * (cb * lam + sum_l c_l lam_Y_l),
-// and the stage adjoint the next launch accumulates into is cleared
-// (zero, which may be one of the pending vectors: read before written).
-__global__ void lamk_kernel(double *mu, double const *inv_mass, double *lam, LamTerms pend, double cb, LamTerms t,
-                            double *zero, size_t n)
+__device__ __forceinline__ double lamk_point(double *mu, double const *inv_mass, double *lam, LamTerms const &pend,
+                                             double cb, LamTerms const &t, double *zero, size_t i)
 {
-  size_t const i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (i >= n)
-    return;
   double L = lam[i];
   if (pend.n > 0)
   {
@@ -137,8 +130,30 @@ __global__ void lamk_kernel(double *mu, double const *inv_mass, double *lam, Lam
   double s = cb * L;
   for (int l = 0; l < t.n; ++l)
     s = fma(t.c[l], t.v[l][i], s);
-  mu[i] = inv_mass[i] * s;
+  double const m = inv_mass[i] * s;
+  mu[i] = m;
   zero[i] = 0.0;
+  return fabs(m);
+}
+
+// lam += sum of the pending stage adjoints of the step after (pend, at the
+// first stage of a step), mu = inv_mass * (cb * lam + sum_l c_l lam_Y_l),
+// and the stage adjoint the next launch accumulates into is cleared
+// (zero, which may be one of the pending vectors: read before written).
+__global__ void lamk_kernel(double *mu, double const *inv_mass, double *lam, LamTerms pend, double cb, LamTerms t,
+                            double *zero, size_t n, unsigned long long *mu_max)
+{
+  size_t const i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  double m = 0.0;
+  if (i < n)
+    m = lamk_point(mu, inv_mass, lam, pend, cb, t, zero, i);
+  // max |mu| of the stage (bit patterns of non-negative doubles order as
+  // integers)
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m > 0.0)
+    atomicMax(mu_max, (unsigned long long)__double_as_longlong(m));
 }
 
 // lam += sum_l lam_Y_l
@@ -236,6 +251,7 @@ public:
     lam_.alloc(n_);
     mu_.alloc(n_);
     lamY_.alloc(n_ * S);
+    mumax_.alloc(1);
     ADM_CK(cudaMemsetAsync(lam_.p, 0, n_ * sizeof(double), st));
     if (ns3)
     {
@@ -289,8 +305,9 @@ public:
           pend.n = 0;
           if (i == S - 1 && pending)
             pend = all;
+          ADM_CK(cudaMemsetAsync(mumax_.p, 0, sizeof(unsigned long long), st));
           lamk_kernel<<<blocks(n_), 256, 0, st>>>(mu_.p, t.inv_mass_.p, lam_.p, pend, dt * t.tab_.b[i], lt, lamYi,
-                                                  n_);
+                                                  n_, mumax_.p);
           ADM_CK(cudaGetLastError());
           t.prepare_stage(t.tab_.c[i]);
           size_t const slot = (size_t)(n - n0) * S + i;
@@ -308,6 +325,8 @@ public:
           }
           A.lam_y = lamYi;
           A.grad = grad_d_.p;
+          A.mu_max = reinterpret_cast<double const *>(mumax_.p);
+          A.flush = flush_;
           run_kernel(A);
           if (ns3)
             std::swap(ls_a_.p, ls_b_.p);
@@ -542,8 +561,15 @@ private:
     times_[n_steps] = tt;
   }
 
+public:
+  // adjoint values at or below flush * (the stage's max |mu|) count as zero
+  // (whole tiles of them are skipped)
+  double flush_ = 1e-30;
+
+private:
   Thermal &th_;
   size_t C_ = 0, n_ = 0;
+  DevBuf<unsigned long long> mumax_;
   int NN_ = 0;
   std::vector<int32_t> obs_steps_;
   int n_points_ = 0;
@@ -597,6 +623,15 @@ int adm_adjoint_gradient(adm_adjoint *a, double t0, double dt, int32_t n_steps, 
   return adm::guard([&] {
     ADM_REQUIRE(a && y0 && J && grad, "null argument");
     *J = reinterpret_cast<adm::Adjoint *>(a)->gradient(t0, dt, n_steps, checkpoint_every, y0, grad, y_final);
+  });
+}
+
+int adm_adjoint_set_flush(adm_adjoint *a, double flush)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(a, "null handle");
+    ADM_REQUIRE(flush >= 0.0 && flush < 1e-3, "flush must be in [0, 1e-3)");
+    reinterpret_cast<adm::Adjoint *>(a)->flush_ = flush;
   });
 }
 

@@ -48,6 +48,15 @@ int adm_adjoint_objective(adm_adjoint *a, double t0, double dt, int32_t n_steps,
  * phase state ends as after the forward run. */
 int adm_adjoint_gradient(adm_adjoint *a, double t0, double dt, int32_t n_steps, int32_t checkpoint_every,
                          double const *y0, double *J, double *grad, double *y_final);
+/* Adjoint values at or below flush times the stage's largest |M^-1 lambda|
+ * count as zero in adm_adjoint_gradient, and tiles holding only such values
+ * (and no powder adjoint) are skipped. The explicit stencil spreads the
+ * adjoint of a misfit at a few points by about one cell per stage with
+ * values falling by orders of magnitude per cell, so most tiles hold only
+ * negligible values. Default 1e-30 (the dropped terms lie some 14 orders of
+ * magnitude below double rounding); 0 skips exact zeros only. 0 <= flush <
+ * 1e-3. No counterpart in the reference. */
+int adm_adjoint_set_flush(adm_adjoint *a, double flush);
 /* The transpose operator: dst = (d r / d T)^T mu at the field y (device
  * vectors), r the vmult residual at the handle's time, with the handle's
  * current phase state as the history input; grad[3] (may be NULL) receives

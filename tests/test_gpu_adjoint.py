@@ -146,6 +146,23 @@ def test_checkpoint_interval_does_not_change_the_gradient():
     assert rel(g1, g2) <= 1e-12
 
 
+def test_flushed_adjoint_gives_the_same_gradient():
+    """Skipping tiles whose adjoint is at most 1e-30 of the stage's largest
+    (the default) against skipping exact zeros only: the same gradient to
+    rounding, on a mesh large enough for most tiles to be skipped."""
+    cfg = adjoint_q2(n_cells=(48, 48, 16), extent=(15e-3, 15e-3, 5e-3), powder_layers=4)
+    T0 = initial_temperature(cfg, "adjoint-flush")
+    pts = interior_points(cfg, n_points=80, radius=0.6e-3, depth=0.6e-3, name="adjoint-flush-points")
+    prob = AdjointProblem(cfg, T0, 0.0, 1e-6, 60, [30, 60], pts, checkpoint_every=20)
+    prob.set_targets(prob.observe(THETA_TRUE))
+    J1, g1 = prob.gradient(THETA)
+    prob.set_flush(0.0)
+    J0, g0 = prob.gradient(THETA)
+    assert J1 == J0
+    assert rel(g1, g0) <= 1e-13
+    assert np.all(np.abs(g0) > 0)
+
+
 def test_autograd_binding():
     cfg, T0, pts, obs, prob = small_problem(n_steps=20, K=5)
     theta = torch.tensor(THETA, dtype=torch.float64, requires_grad=True)
