@@ -147,13 +147,22 @@ __global__ void lamk_kernel(double *mu, double const *inv_mass, double *lam, Lam
   double m = 0.0;
   if (i < n)
     m = lamk_point(mu, inv_mass, lam, pend, cb, t, zero, i);
-  // max |mu| of the stage (bit patterns of non-negative doubles order as
-  // integers)
+  // max |mu| of the stage: warp, block, then one atomic per block (bit
+  // patterns of non-negative doubles order as integers)
+  __shared__ double wmax[8];
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1)
     m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0 && m > 0.0)
-    atomicMax(mu_max, (unsigned long long)__double_as_longlong(m));
+  if ((threadIdx.x & 31) == 0)
+    wmax[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0)
+  {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+      m = fmax(m, wmax[w]);
+    if (m > 0.0)
+      atomicMax(mu_max, (unsigned long long)__double_as_longlong(m));
+  }
 }
 
 // lam += sum_l lam_Y_l
