@@ -102,12 +102,57 @@ __global__ void misfit_kernel(double const *y, int64_t const *idx, double const 
     *J += part[0];
 }
 
-// lambda[idx[p]] += 2 resid[p] (points may repeat a node)
-__global__ void inject_kernel(double *lam, int64_t const *idx, double const *resid, int n)
+// Tile geometry for the activity flags of the backward sweep.
+struct TileGrid
+{
+  int pitch, nn1, deg, t[3], nt[3];
+};
+
+// lambda[idx[p]] += 2 resid[p] (points may repeat a node); the tiles that
+// hold the node (up to eight) are marked for the next stage.
+__global__ void inject_kernel(double *lam, int64_t const *idx, double const *resid, int n, TileGrid g,
+                              uint8_t *act)
 {
   int const p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p < n)
-    atomicAdd(&lam[idx[p]], 2.0 * resid[p]);
+  if (p >= n)
+    return;
+  int64_t const node = idx[p];
+  atomicAdd(&lam[node], 2.0 * resid[p]);
+  if (!act)
+    return;
+  int const ni[3] = {(int)(node % g.pitch), (int)((node / g.pitch) % g.nn1), (int)(node / ((int64_t)g.pitch * g.nn1))};
+  for (int m = 0; m < 8; ++m)
+  {
+    int tc[3];
+    bool ok = true;
+    for (int d = 0; d < 3; ++d)
+    {
+      int const span = g.deg * g.t[d];
+      int c = ni[d] / span;
+      if ((m >> d) & 1)
+      {
+        if (ni[d] % span != 0)
+          ok = false;
+        c -= 1;
+      }
+      if (c < 0 || c >= g.nt[d])
+        ok = false;
+      tc[d] = c;
+    }
+    if (ok)
+      act[tc[0] + (size_t)g.nt[0] * (tc[1] + (size_t)g.nt[1] * tc[2])] = 1;
+  }
+}
+
+// The work items whose tile is marked, compacted (order of arrival).
+__global__ void adj_select_kernel(TileWork const *work, int n_items, uint8_t const *act, TileWork *out, int *n_out)
+{
+  int const i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_items)
+    return;
+  TileWork const w = work[i];
+  if (act[w.tile])
+    out[atomicAdd(n_out, 1)] = w;
 }
 
 struct LamTerms
@@ -140,10 +185,20 @@ __device__ __forceinline__ double lamk_point(double *mu, double const *inv_mass,
 // first stage of a step), mu = inv_mass * (cb * lam + sum_l c_l lam_Y_l),
 // and the stage adjoint the next launch accumulates into is cleared
 // (zero, which may be one of the pending vectors: read before written).
+// Also clears what the next launches accumulate into: the other max slot
+// (the next stage's), the selection counter and the next stage's tile flags.
 __global__ void lamk_kernel(double *mu, double const *inv_mass, double *lam, LamTerms pend, double cb, LamTerms t,
-                            double *zero, size_t n, unsigned long long *mu_max)
+                            double *zero, size_t n, unsigned long long *mu_max, unsigned long long *mu_max_other,
+                            int *n_sel, uint8_t *act_next, size_t n_tiles)
 {
   size_t const i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i == 0)
+  {
+    *mu_max_other = 0ull;
+    *n_sel = 0;
+  }
+  if (i < n_tiles)
+    act_next[i] = 0;
   double m = 0.0;
   if (i < n)
     m = lamk_point(mu, inv_mass, lam, pend, cb, t, zero, i);
@@ -260,7 +315,16 @@ public:
     lam_.alloc(n_);
     mu_.alloc(n_);
     lamY_.alloc(n_ * S);
-    mumax_.alloc(1);
+    mumax_.alloc(2);
+    ADM_CK(cudaMemsetAsync(mumax_.p, 0, 2 * sizeof(unsigned long long), st));
+    stage_count_ = 0;
+    act_a_.alloc(t.mesh_.n_tiles);
+    act_b_.alloc(t.mesh_.n_tiles);
+    act_cur_ = act_a_.p;
+    act_next_ = act_b_.p;
+    ADM_CK(cudaMemsetAsync(act_cur_, 0, t.mesh_.n_tiles, st));
+    sel_.alloc(std::max(1, t.colour_off_[8]));
+    nsel_.alloc(1);
     ADM_CK(cudaMemsetAsync(lam_.p, 0, n_ * sizeof(double), st));
     if (ns3)
     {
@@ -314,9 +378,12 @@ public:
           pend.n = 0;
           if (i == S - 1 && pending)
             pend = all;
-          ADM_CK(cudaMemsetAsync(mumax_.p, 0, sizeof(unsigned long long), st));
-          lamk_kernel<<<blocks(n_), 256, 0, st>>>(mu_.p, t.inv_mass_.p, lam_.p, pend, dt * t.tab_.b[i], lt, lamYi,
-                                                  n_, mumax_.p);
+          unsigned long long *const mmax = mumax_.p + (stage_count_ & 1), *const mmax_next = mumax_.p + ((stage_count_ + 1) & 1);
+          ++stage_count_;
+          size_t const n_tiles = t.mesh_.n_tiles;
+          lamk_kernel<<<blocks(std::max(n_, n_tiles)), 256, 0, st>>>(mu_.p, t.inv_mass_.p, lam_.p, pend,
+                                                                     dt * t.tab_.b[i], lt, lamYi, n_, mmax, mmax_next,
+                                                                     nsel_.p, act_next_, n_tiles);
           ADM_CK(cudaGetLastError());
           t.prepare_stage(t.tab_.c[i]);
           size_t const slot = (size_t)(n - n0) * S + i;
@@ -334,9 +401,18 @@ public:
           }
           A.lam_y = lamYi;
           A.grad = grad_d_.p;
-          A.mu_max = reinterpret_cast<double const *>(mumax_.p);
+          A.mu_max = reinterpret_cast<double const *>(mmax);
           A.flush = flush_;
-          run_kernel(A);
+          // visit the marked tiles only; they mark the next stage's
+          int const count = t.colour_off_[8];
+          if (count > 0)
+            adj_select_kernel<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(t.work_d_.p, count, act_cur_, sel_.p,
+                                                                            nsel_.p);
+          ADM_CK(cudaGetLastError());
+          A.n_items_dev = nsel_.p;
+          A.act_next = act_next_;
+          run_kernel(A, sel_.p);
+          std::swap(act_cur_, act_next_);
           if (ns3)
             std::swap(ls_a_.p, ls_b_.p);
         }
@@ -409,13 +485,29 @@ public:
 private:
   // one launch over the work items of every colour (atomics merge the nodes
   // that tiles share)
-  void run_kernel(AdjArgs &A)
+  TileGrid tile_grid() const
+  {
+    Mesh const &m = th_.mesh_;
+    TileGrid g{};
+    g.pitch = m.pitch;
+    g.nn1 = m.nn[1];
+    g.deg = m.deg;
+    g.t[0] = m.tx;
+    g.t[1] = m.ty;
+    g.t[2] = m.tz;
+    for (int d = 0; d < 3; ++d)
+      g.nt[d] = m.nt[d];
+    return g;
+  }
+
+  // work: the items to visit (default: every tile of the handle)
+  void run_kernel(AdjArgs &A, TileWork const *work = nullptr)
   {
     Thermal &t = th_;
     int const count = t.colour_off_[8];
     if (count == 0)
       return;
-    A.k.work = t.work_d_.p;
+    A.k.work = work ? work : t.work_d_.p;
     CUtensorMap const ym = brick_map(t.mesh_, A.yv, 1, n_);
     CUtensorMap const mm = brick_map(t.mesh_, A.mu, 1, n_);
     launch_adjoint(t.mesh_.deg, t.ns_, ym, mm, A, count, t.stream_);
@@ -516,7 +608,7 @@ private:
       if (obs_steps_[k] == n && n_points_ > 0)
       {
         inject_kernel<<<blocks(n_points_), 256, 0, th_.stream_>>>(lam_.p, idx_.p, resid_.p + k * n_points_,
-                                                                  n_points_);
+                                                                  n_points_, tile_grid(), act_cur_);
         ADM_CK(cudaGetLastError());
       }
   }
@@ -578,7 +670,12 @@ public:
 private:
   Thermal &th_;
   size_t C_ = 0, n_ = 0;
-  DevBuf<unsigned long long> mumax_;
+  DevBuf<unsigned long long> mumax_; // two slots: this stage's and the next one's
+  unsigned stage_count_ = 0;
+  DevBuf<uint8_t> act_a_, act_b_; // per tile: visit in this / the next stage
+  uint8_t *act_cur_ = nullptr, *act_next_ = nullptr;
+  DevBuf<TileWork> sel_;
+  DevBuf<int> nsel_;
   int NN_ = 0;
   std::vector<int32_t> obs_steps_;
   int n_points_ = 0;

@@ -39,13 +39,15 @@ struct AdjArgs
   double const *yv;        // stage input (node vector)
   double const *mu;        // M^-1 lambda_k (node vector)
   double const *s_in;      // [C][NN] powder ratio before the stage (3 states)
-  double const *lam_s_out; // [C][NN] adjoint of the powder ratio after the stage
+  double *lam_s_out;       // [C][NN] adjoint of the powder ratio after the stage (cleared where a tile drops out)
   double *lam_s_in;        // [C][NN] adjoint of the powder ratio before the stage
   uint8_t const *powder_start; // [C] powder mode of the run's initial state (0: none), or null
   double *lam_y;           // node vector: += the transpose applied to mu
   double *grad;            // [3] += log-derivatives: k scale, c_p scale, source
   double const *mu_max;    // max |mu| of the stage, or null (no flush)
   double flush;            // tiles with |mu| <= flush * *mu_max and no powder adjoint are skipped
+  int const *n_items_dev;  // number of work items (a selected list) in device memory, or null
+  uint8_t *act_next;       // per tile: may hold a non-negligible adjoint next stage (set here), or null
 };
 
 // Horner value and derivative of sum_i c[i] T^i up to degree deg.
@@ -256,8 +258,9 @@ __device__ __noinline__ AdjQp adj_point(SmemPhys const &sp, int mat, int pure, b
 template <int DEG, int NS>
 __global__ void __launch_bounds__(TD<DEG>::NT, 2)
     adjoint_kernel(const __grid_constant__ CUtensorMap ymap, const __grid_constant__ CUtensorMap mmap,
-                   const __grid_constant__ AdjArgs A, int n_items)
+                   const __grid_constant__ AdjArgs A, int n_items_max)
 {
+  int const n_items = A.n_items_dev ? min(n_items_max, *A.n_items_dev) : n_items_max;
   using T_ = TD<DEG>;
   constexpr int N = T_::N, NN = T_::NN, NT = T_::NT, NCELL = T_::NCELL, NQS = T_::NQS;
   constexpr int TX = T_::TX, TY = T_::TY, TZ = T_::TZ;
@@ -363,10 +366,24 @@ __global__ void __launch_bounds__(TD<DEG>::NT, 2)
           nz |= A.lam_s_out[sbase + i] != 0.0;
       if (!__syncthreads_or(nz))
       {
+        // the tile drops out of the list: both powder-adjoint buffers of
+        // its cells are left clean for when it comes back (only this
+        // tile's threads read them)
         if (powder_cell)
           for (int i = 0; i < NQS; ++i)
+          {
             A.lam_s_in[sbase + i] = 0.0;
+            A.lam_s_out[sbase + i] = 0.0;
+          }
         continue;
+      }
+      // the adjoint spreads by at most one cell per stage: this tile and its
+      // neighbours are visited next stage
+      if (A.act_next && tid < 27)
+      {
+        int const ox = tix + tid % 3 - 1, oy = tiy + (tid / 3) % 3 - 1, oz = tiz + tid / 9 - 1;
+        if (ox >= 0 && ox < args.nt[0] && oy >= 0 && oy < args.nt[1] && oz >= 0 && oz < args.nt[2])
+          A.act_next[ox + (size_t)args.nt[0] * (oy + (size_t)args.nt[1] * oz)] = 1;
       }
     }
 
