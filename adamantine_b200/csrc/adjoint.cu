@@ -18,6 +18,7 @@
 // sparse powder history) and each K-step segment is recomputed, stage by
 // stage, right before its backward sweep.
 #include "adjoint_kernel.cuh"
+#include "beam_state.cuh"
 #include "capi_common.hpp"
 #include "../../include/adamantine_b200_adjoint.h"
 
@@ -144,16 +145,6 @@ __global__ void inject_kernel(double *lam, int64_t const *idx, double const *res
   }
 }
 
-// The work items whose tile is marked, compacted (order of arrival).
-__global__ void adj_select_kernel(TileWork const *work, int n_items, uint8_t const *act, TileWork *out, int *n_out)
-{
-  int const i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n_items)
-    return;
-  TileWork const w = work[i];
-  if (act[w.tile])
-    out[atomicAdd(n_out, 1)] = w;
-}
 
 struct LamTerms
 {
@@ -185,20 +176,44 @@ __device__ __forceinline__ double lamk_point(double *mu, double const *inv_mass,
 // first stage of a step), mu = inv_mass * (cb * lam + sum_l c_l lam_Y_l),
 // and the stage adjoint the next launch accumulates into is cleared
 // (zero, which may be one of the pending vectors: read before written).
-// Also clears what the next launches accumulate into: the other max slot
-// (the next stage's), the selection counter and the next stage's tile flags.
+// Also, for the stage's transpose launch: the work items of the marked
+// tiles (sel, counter n_sel), and the heat-source state at the stage time
+// (md, when given); and it clears what the next stage accumulates into: the
+// other max and counter slots and the next stage's tile flags.
+struct LamkAux
+{
+  unsigned long long *mu_max, *mu_max_next;
+  int *n_sel, *n_sel_next;
+  TileWork const *work;
+  int n_items;
+  uint8_t const *act_cur;
+  uint8_t *act_next;
+  size_t n_tiles;
+  TileWork *sel;
+  MemberData *md;
+  double c;
+};
+
 __global__ void lamk_kernel(double *mu, double const *inv_mass, double *lam, LamTerms pend, double cb, LamTerms t,
-                            double *zero, size_t n, unsigned long long *mu_max, unsigned long long *mu_max_other,
-                            int *n_sel, uint8_t *act_next, size_t n_tiles)
+                            double *zero, size_t n, LamkAux x)
 {
   size_t const i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (i == 0)
   {
-    *mu_max_other = 0ull;
-    *n_sel = 0;
+    *x.mu_max_next = 0ull;
+    *x.n_sel_next = 0;
   }
-  if (i < n_tiles)
-    act_next[i] = 0;
+  if (i < x.n_tiles)
+    x.act_next[i] = 0;
+  if (i < (size_t)x.n_items)
+  {
+    TileWork const w = x.work[i];
+    if (x.act_cur[w.tile])
+      x.sel[atomicAdd(x.n_sel, 1)] = w;
+  }
+  if (x.md && blockIdx.x == 0 && (int)threadIdx.x < x.md->n_beams)
+    prepare_beam(*x.md, threadIdx.x, x.c);
+  unsigned long long *const mu_max = x.mu_max;
   double m = 0.0;
   if (i < n)
     m = lamk_point(mu, inv_mass, lam, pend, cb, t, zero, i);
@@ -324,7 +339,8 @@ public:
     act_next_ = act_b_.p;
     ADM_CK(cudaMemsetAsync(act_cur_, 0, t.mesh_.n_tiles, st));
     sel_.alloc(std::max(1, t.colour_off_[8]));
-    nsel_.alloc(1);
+    nsel_.alloc(2);
+    ADM_CK(cudaMemsetAsync(nsel_.p, 0, 2 * sizeof(int), st));
     ADM_CK(cudaMemsetAsync(lam_.p, 0, n_ * sizeof(double), st));
     if (ns3)
     {
@@ -378,38 +394,45 @@ public:
           pend.n = 0;
           if (i == S - 1 && pending)
             pend = all;
-          unsigned long long *const mmax = mumax_.p + (stage_count_ & 1), *const mmax_next = mumax_.p + ((stage_count_ + 1) & 1);
+          int const slot = stage_count_ & 1;
           ++stage_count_;
-          size_t const n_tiles = t.mesh_.n_tiles;
-          lamk_kernel<<<blocks(std::max(n_, n_tiles)), 256, 0, st>>>(mu_.p, t.inv_mass_.p, lam_.p, pend,
-                                                                     dt * t.tab_.b[i], lt, lamYi, n_, mmax, mmax_next,
-                                                                     nsel_.p, act_next_, n_tiles);
+          int const count = t.colour_off_[8];
+          LamkAux x{};
+          x.mu_max = mumax_.p + slot;
+          x.mu_max_next = mumax_.p + (slot ^ 1);
+          x.n_sel = nsel_.p + slot;
+          x.n_sel_next = nsel_.p + (slot ^ 1);
+          x.work = t.work_d_.p;
+          x.n_items = count;
+          x.act_cur = act_cur_;
+          x.act_next = act_next_;
+          x.n_tiles = t.mesh_.n_tiles;
+          x.sel = sel_.p;
+          x.md = t.cfg_.n_sources > 0 ? t.member_d_.p : nullptr;
+          x.c = t.tab_.c[i];
+          size_t const threads = std::max({n_, x.n_tiles, (size_t)count});
+          lamk_kernel<<<blocks(threads), 256, 0, st>>>(mu_.p, t.inv_mass_.p, lam_.p, pend, dt * t.tab_.b[i], lt,
+                                                       lamYi, n_, x);
           ADM_CK(cudaGetLastError());
-          t.prepare_stage(t.tab_.c[i]);
-          size_t const slot = (size_t)(n - n0) * S + i;
+          size_t const rslot = (size_t)(n - n0) * S + i;
           AdjArgs A;
           std::memset(&A, 0, sizeof(A));
           A.k = t.base_args();
-          A.yv = Ystore_.p + slot * n_;
+          A.yv = Ystore_.p + rslot * n_;
           A.mu = mu_.p;
           if (ns3)
           {
-            A.s_in = Sstore_.p + slot * qn;
+            A.s_in = Sstore_.p + rslot * qn;
             A.lam_s_out = ls_a_.p;
             A.lam_s_in = ls_b_.p;
             A.powder_start = init_mode_.p;
           }
           A.lam_y = lamYi;
           A.grad = grad_d_.p;
-          A.mu_max = reinterpret_cast<double const *>(mmax);
+          A.mu_max = reinterpret_cast<double const *>(x.mu_max);
           A.flush = flush_;
           // visit the marked tiles only; they mark the next stage's
-          int const count = t.colour_off_[8];
-          if (count > 0)
-            adj_select_kernel<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(t.work_d_.p, count, act_cur_, sel_.p,
-                                                                            nsel_.p);
-          ADM_CK(cudaGetLastError());
-          A.n_items_dev = nsel_.p;
+          A.n_items_dev = x.n_sel;
           A.act_next = act_next_;
           run_kernel(A, sel_.p);
           std::swap(act_cur_, act_next_);
