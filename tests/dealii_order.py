@@ -5,7 +5,8 @@ subdivided_hyper_rectangle without refinement, DoFHandler::distribute_dofs
 walks the cells in creation (lexicographic) order and, on each cell, numbers
 the not-yet-numbered DoFs of its vertices, then its lines, then its quads, then
 its interior, using deal.II's GeometryInfo numbering of those objects.  This
-module restates that walk for FE_Q(1) and FE_Q(2) and returns, for every
+module restates that walk for FE_Q(1), FE_Q(2) and (3-D) FE_Q(3) and
+returns, for every
 deal.II DoF, the node index of the full-grid lexicographic numbering.
 """
 import itertools
@@ -35,9 +36,35 @@ def dof_to_node(dim, n_cells, degree, active=None):
             mul *= nn[d]
         return idx
 
-    objects = []  # local coordinates (in units of 1/2 cell for Q2) per object
+    objects = []  # local node offsets (0..degree per axis) of each DoF, in order
     for v in range(2 ** dim):
         objects.append([degree * c for c in _vcoord(v, dim)])
+    if degree == 3 and dim == 3:
+        # two DoFs per line, from its first vertex to its second; four per
+        # face, lexicographic in the face's own coordinates (faces 0/1:
+        # (y, z), 2/3: (z, x), 4/5: (x, y)); eight inside, lexicographic
+        for a, b in _LINES_3D:
+            ca, cb = _vcoord(a, dim), _vcoord(b, dim)
+            d = [k for k in range(3) if ca[k] != cb[k]][0]
+            for j in (1, 2):
+                loc = [3 * c for c in ca]
+                loc[d] = j
+                objects.append(loc)
+        face_axes = {0: (1, 2), 1: (2, 0), 2: (0, 1)}
+        for f in range(6):
+            d, side = divmod(f, 2)
+            u, w = face_axes[d]
+            for jw in (1, 2):
+                for ju in (1, 2):
+                    loc = [0, 0, 0]
+                    loc[d] = 3 * side
+                    loc[u] = ju
+                    loc[w] = jw
+                    objects.append(loc)
+        for k in (1, 2):
+            for j in (1, 2):
+                for i in (1, 2):
+                    objects.append([i, j, k])
     if degree == 2:
         lines = _LINES_3D if dim == 3 else _LINES_2D
         for a, b in lines:

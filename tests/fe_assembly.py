@@ -15,8 +15,12 @@ import numpy as np
 
 
 def gl_nodes(degree):
-    """FE_Q support points (Gauss-Lobatto) on [0,1] for degree 1..2."""
-    return {1: np.array([0.0, 1.0]), 2: np.array([0.0, 0.5, 1.0])}[degree]
+    """FE_Q support points (Gauss-Lobatto) on [0,1] for degree 1..4: the end
+    points and the roots of P'_degree."""
+    if degree == 1:
+        return np.array([0.0, 1.0])
+    inner = np.polynomial.legendre.Legendre.basis(degree).deriv().roots()
+    return np.concatenate([[0.0], np.sort((inner + 1.0) / 2.0), [1.0]])
 
 
 def gauss(n):

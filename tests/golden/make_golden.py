@@ -23,6 +23,11 @@ Run in a container where the reference is mounted at /root/reference:
   (test_integration_3d.cc:112-115), copied as is; and
   integration_3d_scan_path.npy, the segments of demo_316_short_scan_path.txt
   as (end_time, power_modifier, x, y, z) rows.
+* integration_3d_gold_short.npz -- tests/data/integration_3d_gold_short.txt
+  (229570 temperatures, 6 significant digits, stored as float32, exact to
+  the printed digits) of demo_316_short.info (test_integration_3d.cc:117-120:
+  50 x 50 x 8 FE_Q(3), convective and radiative faces, 67 forward Euler
+  steps of 6e-5 s).
 """
 import os
 import sys
@@ -60,6 +65,10 @@ def main():
     np.save(os.path.join(HERE, "integration_3d_scan_path.npy"),
             np.array(segments(open(os.path.join(data, "demo_316_short_scan_path.txt")).read())))
     print("wrote integration_3d_gold.txt", len(vals), "and integration_3d_scan_path.npy")
+    short = np.array([float(v) for v in open(os.path.join(data, "integration_3d_gold_short.txt")).read().split()])
+    assert short.size == 229570, short.size
+    np.savez_compressed(os.path.join(HERE, "integration_3d_gold_short.npz"), values=short.astype(np.float32))
+    print("wrote integration_3d_gold_short.npz", short.size)
 
     for k in (1, 2):
         name = f"microstructure_G_R_gold_{k}.txt"

@@ -32,7 +32,7 @@ def test_integration_3d_on_the_gpu(schedule):
         t = g.evolve_one_time_step(t, DT, y)
         n += 1
     assert n == 100 and g.device_error() == 0
-    y_ref, active, _ = run_oracle(cfg, boxes)
+    y_ref, active, _, _ = run_oracle(cfg, boxes)
     order = dof_to_node(3, cfg.geometry.n_cells, 2, active=active)
     got = g.to_grid(y).reshape(-1)[order]
     assert rel_max(got, y_ref[order]) <= 1e-9
