@@ -27,6 +27,7 @@ SIGNATURES = {
     "adm_setup": [_VP],
     "adm_n_nodes": [_VP, _I64],
     "adm_n_cells": [_VP, _I64],
+    "adm_get_active_cells": [_VP, _VP],
     "adm_node_layout": [_VP, _I64, _I64],
     "adm_set_time": [_VP, ctypes.c_double],
     "adm_vmult": [_VP, _VP, _VP],

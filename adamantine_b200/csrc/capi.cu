@@ -3,6 +3,8 @@
 // the message for adm_last_error().
 #include "capi_common.hpp"
 
+#include <algorithm>
+
 #include <string>
 
 namespace
@@ -73,6 +75,15 @@ int adm_n_cells(adm_thermal const *h, int64_t *n)
   return adm::guard([&] {
     ADM_REQUIRE(h && n, "null argument");
     *n = (int64_t)as(h)->n_cells();
+  });
+}
+
+int adm_get_active_cells(adm_thermal const *h, uint8_t *active)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && active, "null argument");
+    auto const &a = as(h)->active_cells();
+    std::copy(a.begin(), a.end(), active);
   });
 }
 

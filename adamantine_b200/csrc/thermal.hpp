@@ -195,6 +195,7 @@ public:
   // ---- ThermalOperatorBase
   size_t m() const { return mesh_.n_nodes; }
   size_t n_cells() const { return mesh_.n_cells; }
+  std::vector<uint8_t> const &active_cells() const { return active_; }
   Mesh const &mesh() const { return mesh_; }
   void set_time(double t);
   void vmult(double *dst, double const *src, bool add);

@@ -111,6 +111,12 @@ class ThermalPhysics:
     def n(self) -> int:
         return self._m
 
+    def active_cells(self) -> np.ndarray:
+        """The cells that carry material now (initial set and activations)."""
+        out = np.zeros(self.n_cells, np.uint8)
+        _lib.check(self._L.adm_get_active_cells(self._h, _ptr(out, ctypes.c_uint8)))
+        return out
+
     def initialize_dof_vector(self, value: float = 0.0) -> torch.Tensor:
         return torch.full((self._m,), float(value), dtype=torch.float64, device=self.device)
 

@@ -119,6 +119,10 @@ int adm_setup(adm_thermal *h);
 /* ThermalOperatorBase::m() / n(): length of a node vector (with padding). */
 int adm_n_nodes(adm_thermal const *h, int64_t *n);
 int adm_n_cells(adm_thermal const *h, int64_t *n);
+/* The cells that currently carry material (FE_Q rather than FE_Nothing:
+ * the initial set plus every activation), 1 byte per cell, lexicographic
+ * (x fastest); host array of adm_n_cells bytes. */
+int adm_get_active_cells(adm_thermal const *h, uint8_t *active);
 /* Node grid extents (x, y, z) and the row pitch of the vector layout. */
 int adm_node_layout(adm_thermal const *h, int64_t nodes[3], int64_t *pitch);
 

@@ -75,3 +75,46 @@ def test_integration_3d_checkpoint_restart(tmp_path, exact):
     assert t3 == t
     run(g3, Deposition(g3, boxes, deposition_time=0.0, duration=DURATION), y3, t3, 1000)
     assert rel_max(g3.to_grid(y3), g1.to_grid(y1)) <= 1e-10
+
+
+def test_vtk_output_of_the_demo(tmp_path):
+    """PostProcessor.write_thermal_output after the demo's deposition run:
+    one hexahedron per cell that carries material (deposited cells
+    included), the corner temperatures of the device field, and the .pvd
+    record."""
+    import base64
+    import xml.etree.ElementTree as ET
+
+    from adamantine_b200.postprocessor import PostProcessor
+
+    cfg = demo_config()
+    boxes = deposition_boxes(cfg, *BOX)
+    g = ThermalPhysics(cfg)
+    dep = Deposition(g, boxes, deposition_time=0.0, duration=DURATION)
+    y = g.initialize_dof_vector(300.0)
+    pp = PostProcessor(g, "demo", str(tmp_path))
+    t, n = 0.0, 0
+    pp.write_thermal_output(0, t, y)
+    while t < DURATION:
+        dep.step(t, DT, NEW_T, y)
+        t = g.evolve_one_time_step(t, DT, y)
+        n += 1
+    pp.write_thermal_output(n, t, y)
+    pp.write_pvd()
+    active = g.active_cells()
+    assert active.sum() == cfg.geometry.active_cells().sum() + 12
+    root = ET.parse(str(tmp_path / f"demo.{n}.0.vtu")).getroot()
+    assert int(root.find(".//Piece").get("NumberOfCells")) == active.sum()
+    arr = {el.get("Name"): el for el in root.iter("DataArray")}
+    raw = base64.b64decode(arr["temperature"].text)
+    T = np.frombuffer(raw[4:], np.float64)
+    raw = base64.b64decode(arr["Points"].text)
+    P = np.frombuffer(raw[4:], np.float64).reshape(-1, 3)
+    geo = cfg.geometry
+    step = np.array(geo.extent) / (2 * np.array(geo.n_cells))
+    ijk = np.rint((P - np.array(geo.origin)) / step).astype(int)
+    grid = g.to_grid(y)
+    assert (T == grid[ijk[:, 2], ijk[:, 1], ijk[:, 0]]).all()  # the cells' corner values
+    assert T.min() >= 285.0 and T.max() > 400.0
+    ds = list(ET.parse(str(tmp_path / "demo.pvd")).getroot().iter("DataSet"))
+    assert len(ds) == 2 and float(ds[1].get("timestep")) == t
