@@ -187,8 +187,10 @@ __global__ void __launch_bounds__(256) cov_kernel(double const *HA, int n_member
   }
 }
 
-// Unblocked Cholesky of the diagonal block at (k0, k0), one CTA.
-__global__ void __launch_bounds__(256) potrf_diag_kernel(double *C, int m, int k0, int *err)
+// Unblocked Cholesky of the diagonal block at (k0, k0), one CTA; the
+// inverse of the factor goes to Linv (kNB x kNB, row-major), for the panel
+// solve and the triangular solves (products instead of substitutions).
+__global__ void __launch_bounds__(256) potrf_diag_kernel(double *C, int m, int k0, int *err, double *Linv)
 {
   __shared__ double a[kNB][kNB + 1];
   int const nb = min(kNB, m - k0);
@@ -232,41 +234,58 @@ __global__ void __launch_bounds__(256) potrf_diag_kernel(double *C, int m, int k
     if (c <= r)
       C[(int64_t)(k0 + r) * m + k0 + c] = a[r][c];
   }
+  // inverse of the lower-triangular factor, one column per thread:
+  // L x = e_j by forward substitution
+  if (tid < kNB)
+  {
+    int const j = tid;
+    double x[kNB];
+#pragma unroll
+    for (int i = 0; i < kNB; ++i)
+    {
+      double v = 0.0;
+      if (i >= j && i < nb)
+      {
+        double s = i == j ? 1.0 : 0.0;
+        for (int q = j; q < i; ++q)
+          s -= a[i][q] * x[q];
+        v = s / a[i][i];
+      }
+      x[i] = v;
+    }
+#pragma unroll
+    for (int i = 0; i < kNB; ++i)
+      Linv[i * kNB + j] = x[i];
+  }
 }
 
-// Panel below the diagonal block: L[r, k0:k0+nb] = C[r, k0:k0+nb] L_kk^-T,
-// one row per thread.
-__global__ void __launch_bounds__(128) trsm_panel_kernel(double *C, int m, int k0)
+// Panel below the diagonal block: L[r, k0:k0+nb] = C[r, k0:k0+nb] L_kk^-T
+// = row * Linv^T, one row per thread (independent sums, no substitution
+// chain).
+__global__ void __launch_bounds__(128) trsm_panel_kernel(double *C, int m, int k0, double const *Linv)
 {
-  __shared__ double l[kNB][kNB + 1];
-  __shared__ double inv_d[kNB];
+  __shared__ double li[kNB][kNB + 1];
   int const nb = min(kNB, m - k0);
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x)
-  {
-    int const r = e / nb, c = e % nb;
-    l[r][c] = c <= r ? C[(int64_t)(k0 + r) * m + k0 + c] : 0.0;
-  }
-  __syncthreads();
-  if (threadIdx.x < nb)
-    inv_d[threadIdx.x] = 1.0 / l[threadIdx.x][threadIdx.x];
+  for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x)
+    li[e / kNB][e % kNB] = Linv[e];
   __syncthreads();
   int const r = k0 + nb + blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= m)
     return;
   double *row = C + (int64_t)r * m + k0;
-  double x[kNB];
+  double v[kNB];
 #pragma unroll
-  for (int j = 0; j < kNB; ++j)
+  for (int q = 0; q < kNB; ++q)
+    v[q] = q < nb ? row[q] : 0.0;
+#pragma unroll 4
+  for (int j = 0; j < nb; ++j)
   {
-    if (j < nb)
-    {
-      double s = row[j];
+    double s = 0.0;
 #pragma unroll
-      for (int q = 0; q < j; ++q)
-        s -= x[q] * l[j][q];
-      x[j] = s * inv_d[j];
-      row[j] = x[j];
-    }
+    for (int q = 0; q < kNB; ++q)
+      if (q <= j)
+        s = fma(v[q], li[j][q], s);
+    row[j] = s;
   }
 }
 
@@ -322,14 +341,15 @@ __global__ void __launch_bounds__(256) syrk_update_kernel(double *C, int m, int 
 }
 
 // Z_k = C^-1 D_k for one member k per CTA: forward L y = d, backward
-// L^T z = y, blocked by kNB; the diagonal block is solved by warp 0 with
-// shuffles, the off-diagonal updates by all threads. The column lives in
-// shared memory.
-__global__ void __launch_bounds__(256) solve_kernel(double const *L, int m, double const *D, double *Z)
+// L^T z = y, blocked by kNB; a diagonal block is a product with the inverse
+// of the factor's block (one output per thread), the off-diagonal updates
+// use all threads. The column lives in shared memory.
+__global__ void __launch_bounds__(256) solve_kernel(double const *L, int m, double const *D, double *Z,
+                                                    double const *Linv)
 {
   extern __shared__ double col[]; // [m]
   int const k = blockIdx.x;
-  int const tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  int const tid = threadIdx.x;
   for (int i = tid; i < m; i += blockDim.x)
     col[i] = D[(int64_t)k * m + i];
   __syncthreads();
@@ -338,20 +358,16 @@ __global__ void __launch_bounds__(256) solve_kernel(double const *L, int m, doub
   for (int b = 0; b < nblk; ++b)
   {
     int const k0 = b * kNB, nb = min(kNB, m - k0);
-    if (warp == 0)
     {
-      for (int j = 0; j < nb; ++j)
-      {
-        double s = 0.0;
-        for (int q = lane; q < j; q += 32)
-          s += L[(int64_t)(k0 + j) * m + k0 + q] * col[k0 + q];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1)
-          s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0)
-          col[k0 + j] = (col[k0 + j] - s) / L[(int64_t)(k0 + j) * m + k0 + j];
-        __syncwarp();
-      }
+      // y = Linv t on the block (t: the block's entries, already updated)
+      double const *li = Linv + (size_t)b * kNB * kNB;
+      double y = 0.0;
+      if (tid < nb)
+        for (int q = 0; q <= tid; ++q)
+          y = fma(li[tid * kNB + q], col[k0 + q], y);
+      __syncthreads();
+      if (tid < nb)
+        col[k0 + tid] = y;
     }
     __syncthreads();
     for (int i = k0 + nb + tid; i < m; i += blockDim.x)
@@ -368,20 +384,16 @@ __global__ void __launch_bounds__(256) solve_kernel(double const *L, int m, doub
   for (int b = nblk - 1; b >= 0; --b)
   {
     int const k0 = b * kNB, nb = min(kNB, m - k0);
-    if (warp == 0)
     {
-      for (int j = nb - 1; j >= 0; --j)
-      {
-        double s = 0.0;
-        for (int q = j + 1 + lane; q < nb; q += 32)
-          s += L[(int64_t)(k0 + q) * m + k0 + j] * col[k0 + q];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1)
-          s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0)
-          col[k0 + j] = (col[k0 + j] - s) / L[(int64_t)(k0 + j) * m + k0 + j];
-        __syncwarp();
-      }
+      // z = Linv^T t on the block
+      double const *li = Linv + (size_t)b * kNB * kNB;
+      double z = 0.0;
+      if (tid < nb)
+        for (int q = tid; q < nb; ++q)
+          z = fma(li[q * kNB + tid], col[k0 + q], z);
+      __syncthreads();
+      if (tid < nb)
+        col[k0 + tid] = z;
     }
     __syncthreads();
     for (int i = tid; i < k0; i += blockDim.x)
@@ -1091,6 +1103,7 @@ struct Enkf
   int device = 0;
   cudaStream_t stream = nullptr;
   DevBuf<double> HA, D, C, Z, W;
+  DevBuf<double> Linv; // inverses of the Cholesky factor's diagonal blocks
   DevBuf<int> err;
   // localization: geometry, observation points (input order and bucket
   // order), bucket offsets, and the transposed HA / Z and the update rows
@@ -1533,13 +1546,15 @@ struct Enkf
     int const t32 = (m + 31) / 32;
     cov_kernel<<<dim3(t32, t32), 256, 0, stream>>>(HA.p, N, m, scale, var, cov, C.p, loc ? oxyz.p : nullptr, lg, 0);
     ADM_CK(cudaGetLastError());
+    Linv.alloc((size_t)((m + kNB - 1) / kNB) * kNB * kNB);
     for (int k0 = 0; k0 < m; k0 += kNB)
     {
-      potrf_diag_kernel<<<1, 256, 0, stream>>>(C.p, m, k0, err.p);
+      double *const li = Linv.p + (size_t)(k0 / kNB) * kNB * kNB;
+      potrf_diag_kernel<<<1, 256, 0, stream>>>(C.p, m, k0, err.p, li);
       int const below = m - k0 - kNB;
       if (below > 0)
       {
-        trsm_panel_kernel<<<(below + 127) / 128, 128, 0, stream>>>(C.p, m, k0);
+        trsm_panel_kernel<<<(below + 127) / 128, 128, 0, stream>>>(C.p, m, k0, li);
         int const t = (below + 63) / 64;
         syrk_update_kernel<<<dim3(t, t), 256, 0, stream>>>(C.p, m, k0);
       }
@@ -1559,7 +1574,7 @@ struct Enkf
     else
     {
       ADM_CK(cudaFuncSetAttribute(solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      solve_kernel<<<N, 256, smem, stream>>>(C.p, m, D.p, Z.p);
+      solve_kernel<<<N, 256, smem, stream>>>(C.p, m, D.p, Z.p, Linv.p);
     }
     ADM_CK(cudaGetLastError());
     w_kernel<<<(N * N * 32 + 255) / 256, 256, 0, stream>>>(HA.p, Z.p, N, m, scale, Wout);
