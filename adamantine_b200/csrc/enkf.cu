@@ -36,6 +36,7 @@
 #include "capi_common.hpp"
 #include "../../include/adamantine_b200_ensemble.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -45,6 +46,8 @@ namespace adm
 namespace
 {
 constexpr int kNB = 64;        // Cholesky block size
+constexpr size_t kPotrfSmem = sizeof(double) * 2 * kNB * (kNB + 1); // potrf_diag_kernel
+constexpr size_t kPanelSmem = sizeof(double) * 2 * kNB * (kNB + 1); // trsm_panel_kernel
 constexpr int kMaxN = 64;      // members per analysis
 constexpr int kMaxObs = 16384; // observations (the solve keeps one column in shared memory)
 constexpr int kMaxGain = 256;  // members of a sharded analysis (all GPUs)
@@ -187,121 +190,230 @@ __global__ void __launch_bounds__(256) cov_kernel(double const *HA, int n_member
   }
 }
 
+// acc[u][v] = sum_q A[r + u][q] B[q][c + 16 v] over the kNB columns of A,
+// with r = 4 (tid / 16), c = tid % 16: a 64 x 64 product, 4 x 4 outputs per
+// thread of 256 (B row-major with leading dimension ldb >= 64; consecutive
+// threads read consecutive entries of B, two rows of A per warp). With
+// upper = true, A is upper triangular and the sum starts at q = r.
+template <bool upper = false>
+__device__ __forceinline__ void mm64(double const (*A)[kNB + 1], double const *B, int ldb, double acc[4][4])
+{
+  int const r = 4 * (threadIdx.x >> 4), c = threadIdx.x & 15;
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+      acc[u][v] = 0.0;
+#pragma unroll 4
+  for (int q = upper ? r : 0; q < kNB; ++q)
+  {
+    double x[4], y[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      x[u] = A[r + u][q];
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+      y[v] = B[q * ldb + c + 16 * v];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v)
+        acc[u][v] = fma(x[u], y[v], acc[u][v]);
+  }
+}
+
 // Unblocked Cholesky of the diagonal block at (k0, k0), one CTA; the
-// inverse of the factor goes to Linv (kNB x kNB, row-major), for the panel
-// solve and the triangular solves (products instead of substitutions).
+// inverse of the factor goes to Linv (kNB x kNB, row-major, zero above the
+// diagonal and beyond the block), for the panel solve and the triangular
+// solves (products instead of substitutions). Each thread keeps a 4 x 4
+// set of the block's entries in registers, (ty + 16 u, tx + 16 v); one
+// barrier per column: step j reads column j (published by its owners into
+// col[j & 1]), writes column j of the factor into l and updates the
+// trailing triangle with a[i][c] -= (a[i][j] / sqrt(a[j][j]))
+// (a[c][j] / sqrt(a[j][j])), after which the owners of column j + 1 publish
+// it; the same step forms row j - 1 of the inverse, whose inputs (rows < j
+// of l and of the inverse) are complete after the previous barrier:
+// xi[i][c] = (delta_ic - sum_{q=c}^{i-1} l[i][q] xi[q][c]) / l[i][i]
+// (four threads per column, a fixed 16-term predicated sum each).
+// Dynamic shared memory kPotrfSmem: l and xi, kNB x (kNB + 1) each.
 __global__ void __launch_bounds__(256) potrf_diag_kernel(double *C, int m, int k0, int *err, double *Linv)
 {
-  __shared__ double a[kNB][kNB + 1];
+  extern __shared__ double pd_sm[];
+  double(*l)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(pd_sm);
+  double(*xi)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(pd_sm + kNB * (kNB + 1));
+  __shared__ double col[2][kNB];
+  __shared__ double rdiag[kNB];
   int const nb = min(kNB, m - k0);
-  int const tid = threadIdx.x;
-  for (int e = tid; e < nb * nb; e += blockDim.x)
-  {
-    int const r = e / nb, c = e % nb;
-    a[r][c] = c <= r ? C[(int64_t)(k0 + r) * m + k0 + c] : 0.0;
-  }
-  __syncthreads();
-  for (int j = 0; j < nb; ++j)
-  {
-    if (tid == 0)
+  int const tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+  double a[4][4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
     {
-      double const d = a[j][j];
+      int const r = ty + 16 * u, c = tx + 16 * v;
+      a[u][v] = (r < nb && c <= r) ? C[(int64_t)(k0 + r) * m + k0 + c] : 0.0;
+    }
+  for (int e = tid; e < kNB * kNB; e += blockDim.x)
+  {
+    l[e / kNB][e % kNB] = 0.0;
+    xi[e / kNB][e % kNB] = 0.0;
+  }
+  if (tx == 0)
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      col[0][ty + 16 * u] = a[u][0];
+  __syncthreads();
+  int const icol = tid >> 2, part = tid & 3; // inverse: four threads per column
+  for (int j = 0; j <= nb; ++j)
+  {
+    if (j < nb)
+    {
+      double const *cb = col[j & 1];
+      double d = cb[j];
       if (!(d > 0.0) || !isfinite(d))
       {
-        atomicCAS(err, 0, (int)EERR_NOT_SPD);
-        a[j][j] = 1.0;
+        if (tid == 0)
+          atomicCAS(err, 0, (int)EERR_NOT_SPD);
+        d = 1.0;
       }
-      else
-        a[j][j] = sqrt(d);
-    }
-    __syncthreads();
-    double const piv = a[j][j];
-    for (int i = j + 1 + tid; i < nb; i += blockDim.x)
-      a[i][j] /= piv;
-    __syncthreads();
-    int const w = nb - j - 1;
-    for (int e = tid; e < w * w; e += blockDim.x)
-    {
-      int const i = j + 1 + e / w, l = j + 1 + e % w;
-      if (l <= i)
-        a[i][l] -= a[i][j] * a[l][j];
-    }
-    __syncthreads();
-  }
-  for (int e = tid; e < nb * nb; e += blockDim.x)
-  {
-    int const r = e / nb, c = e % nb;
-    if (c <= r)
-      C[(int64_t)(k0 + r) * m + k0 + c] = a[r][c];
-  }
-  // inverse of the lower-triangular factor, one column per thread:
-  // L x = e_j by forward substitution
-  if (tid < kNB)
-  {
-    int const j = tid;
-    double x[kNB];
+      double const sd = sqrt(d), rs = 1.0 / sd;
+      if (tid < nb - j)
+        l[j + tid][j] = tid == 0 ? sd : cb[j + tid] * rs;
+      if (tid == 0)
+        rdiag[j] = rs;
+      double li[4], lc[4];
 #pragma unroll
-    for (int i = 0; i < kNB; ++i)
-    {
-      double v = 0.0;
-      if (i >= j && i < nb)
+      for (int u = 0; u < 4; ++u)
       {
-        double s = i == j ? 1.0 : 0.0;
-        for (int q = j; q < i; ++q)
-          s -= a[i][q] * x[q];
-        v = s / a[i][i];
+        li[u] = cb[ty + 16 * u] * rs;
+        lc[u] = cb[tx + 16 * u] * rs;
       }
-      x[i] = v;
-    }
 #pragma unroll
-    for (int i = 0; i < kNB; ++i)
-      Linv[i * kNB + j] = x[i];
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+        {
+          int const i = ty + 16 * u, c = tx + 16 * v;
+          if (c > j && c <= i)
+            a[u][v] -= li[u] * lc[v];
+        }
+      int const jn = j + 1;
+#pragma unroll
+      for (int v = 0; v < 4; ++v)
+        if (jn < nb && tx + 16 * v == jn)
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+            col[jn & 1][ty + 16 * u] = a[u][v];
+    }
+    if (j >= 1)
+    {
+      int const i = j - 1;
+      double s = 0.0;
+#pragma unroll
+      for (int k = 0; k < kNB / 4; ++k)
+      {
+        int const q = part + 4 * k;
+        if (q >= icol && q < i)
+          s = fma(l[i][q], xi[q][icol], s);
+      }
+      s += __shfl_xor_sync(0xffffffffu, s, 1);
+      s += __shfl_xor_sync(0xffffffffu, s, 2);
+      if (part == 0 && icol <= i)
+        xi[i][icol] = ((i == icol ? 1.0 : 0.0) - s) * rdiag[i];
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < kNB * kNB; e += blockDim.x)
+  {
+    int const r = e / kNB, c = e % kNB;
+    if (r < nb && c <= r)
+      C[(int64_t)(k0 + r) * m + k0 + c] = l[r][c];
+    Linv[e] = xi[r][c];
   }
 }
 
 // Panel below the diagonal block: L[r, k0:k0+nb] = C[r, k0:k0+nb] L_kk^-T
-// = row * Linv^T, one row per thread (independent sums, no substitution
-// chain).
-__global__ void __launch_bounds__(128) trsm_panel_kernel(double *C, int m, int k0, double const *Linv)
+// = rows * Linv^T, 64 rows per CTA as one 64 x 64 x 64 product (no
+// substitution chain). With right-hand sides R (m x N, row-major), the
+// CTAs after the row CTAs also take the forward solve's block step, 64
+// columns each: R[k0 .. k0+nb] = Linv R[k0 .. k0+nb] in place (those rows
+// are final once the earlier steps' trailing updates have run). Dynamic
+// shared memory kPanelSmem: two kNB x (kNB + 1) tiles.
+__global__ void __launch_bounds__(256) trsm_panel_kernel(double *C, int m, int k0, double const *Linv, double *R,
+                                                         int N)
 {
-  __shared__ double li[kNB][kNB + 1];
+  extern __shared__ double tp_sm[];
+  double(*v)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(tp_sm);
+  double(*lb)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(tp_sm + kNB * (kNB + 1));
   int const nb = min(kNB, m - k0);
-  for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x)
-    li[e / kNB][e % kNB] = Linv[e];
-  __syncthreads();
-  int const r = k0 + nb + blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= m)
-    return;
-  double *row = C + (int64_t)r * m + k0;
-  double v[kNB];
-#pragma unroll
-  for (int q = 0; q < kNB; ++q)
-    v[q] = q < nb ? row[q] : 0.0;
-#pragma unroll 4
-  for (int j = 0; j < nb; ++j)
+  int const n_row = (m - k0 - nb + kNB - 1) / kNB;
+  int const tid = threadIdx.x;
+  int const rr = 4 * (tid >> 4), cc = tid & 15;
+  double acc[4][4];
+  if ((int)blockIdx.x >= n_row)
   {
-    double s = 0.0;
+    int const n0 = 64 * ((int)blockIdx.x - n_row), nc = min(64, N - n0);
+    for (int e = tid; e < kNB * kNB; e += blockDim.x)
+    {
+      int const q = e / kNB, n = e % kNB;
+      v[q][n] = Linv[e];
+      lb[q][n] = (q < nb && n < nc) ? R[(int64_t)(k0 + q) * N + n0 + n] : 0.0;
+    }
+    __syncthreads();
+    mm64(v, &lb[0][0], kNB + 1, acc);
 #pragma unroll
-    for (int q = 0; q < kNB; ++q)
-      if (q <= j)
-        s = fma(v[q], li[j][q], s);
-    row[j] = s;
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int w = 0; w < 4; ++w)
+      {
+        int const q = rr + u, n = cc + 16 * w;
+        if (q < nb && n < nc)
+          R[(int64_t)(k0 + q) * N + n0 + n] = acc[u][w];
+      }
+    return;
   }
+  int const r0 = k0 + nb + kNB * (int)blockIdx.x, nr = min(kNB, m - r0);
+  for (int e = tid; e < kNB * kNB; e += blockDim.x)
+  {
+    int const r = e / kNB, q = e % kNB;
+    v[r][q] = (r < nr && q < nb) ? C[(int64_t)(r0 + r) * m + k0 + q] : 0.0;
+    lb[q][r] = Linv[e]; // lb[q][j] = Linv[j][q]
+  }
+  __syncthreads();
+  mm64(v, &lb[0][0], kNB + 1, acc);
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int w = 0; w < 4; ++w)
+    {
+      int const r = rr + u, c = cc + 16 * w;
+      if (r < nr && c < nb)
+        C[(int64_t)(r0 + r) * m + k0 + c] = acc[u][w];
+    }
 }
 
 // Trailing update of the lower triangle: C[i][j] -= L[i, panel] L[j, panel]^T
-// for 64 x 64 tiles right of / below the panel.
-__global__ void __launch_bounds__(256) syrk_update_kernel(double *C, int m, int k0)
+// for 64 x 64 tiles right of / below the panel (blockIdx.x < t, the tile
+// columns). With right-hand sides R (m x N), the CTAs with blockIdx.x >= t
+// take the forward solve's update of the rows below the block, 64 columns
+// each: R[i][n] -= L[i, panel] Y[panel][n], Y being R's block rows after
+// the panel kernel.
+__global__ void __launch_bounds__(256) syrk_update_kernel(double *C, int m, int k0, double *R, int N)
 {
   int const base = k0 + kNB;
+  int const t = (m - base + 63) / 64;
   int const bi = blockIdx.y, bj = blockIdx.x;
-  if (bj > bi)
+  bool const aug = bj >= t;
+  if (!aug && bj > bi)
     return;
-  int const i0 = base + bi * 64, j0 = base + bj * 64;
+  int const i0 = base + bi * 64, j0 = aug ? 64 * (bj - t) : base + bj * 64;
   // the panel's 64 columns in two chunks of 32 (static shared memory)
   __shared__ double pi[64][33], pj[64][33];
   int const tid = threadIdx.x;
-  int const tr = (tid / 16) * 4, tc = (tid % 16) * 4;
+  // rows tr + u, columns tc + 16 v (consecutive threads read consecutive
+  // rows of pj: no bank conflicts at the 33-double pitch)
+  int const tr = (tid / 16) * 4, tc = tid % 16;
   double acc[4][4] = {};
   for (int q0 = 0; q0 < kNB; q0 += 32)
   {
@@ -309,7 +421,13 @@ __global__ void __launch_bounds__(256) syrk_update_kernel(double *C, int m, int 
     {
       int const r = e / 32, c = e % 32;
       pi[r][c] = i0 + r < m ? C[(int64_t)(i0 + r) * m + k0 + q0 + c] : 0.0;
-      pj[r][c] = j0 + r < m ? C[(int64_t)(j0 + r) * m + k0 + q0 + c] : 0.0;
+      if (aug)
+      {
+        int const n = e % 64, q = e / 64; // consecutive threads: consecutive columns of R
+        pj[n][q] = j0 + n < N ? R[(int64_t)(k0 + q0 + q) * N + j0 + n] : 0.0;
+      }
+      else
+        pj[r][c] = j0 + r < m ? C[(int64_t)(j0 + r) * m + k0 + q0 + c] : 0.0;
     }
     __syncthreads();
     for (int q = 0; q < 32; ++q)
@@ -319,7 +437,7 @@ __global__ void __launch_bounds__(256) syrk_update_kernel(double *C, int m, int 
       for (int u = 0; u < 4; ++u)
       {
         a[u] = pi[tr + u][q];
-        b[u] = pj[tc + u][q];
+        b[u] = pj[tc + 16 * u][q];
       }
 #pragma unroll
       for (int u = 0; u < 4; ++u)
@@ -334,79 +452,79 @@ __global__ void __launch_bounds__(256) syrk_update_kernel(double *C, int m, int 
 #pragma unroll
     for (int v = 0; v < 4; ++v)
     {
-      int const gi = i0 + tr + u, gj = j0 + tc + v;
-      if (gi < m && gj <= gi)
+      int const gi = i0 + tr + u, gj = j0 + tc + 16 * v;
+      if (aug)
+      {
+        if (gi < m && gj < N)
+          R[(int64_t)gi * N + gj] -= acc[u][v];
+      }
+      else if (gi < m && gj <= gi)
         C[(int64_t)gi * m + gj] -= acc[u][v];
     }
 }
 
-// Z_k = C^-1 D_k for one member k per CTA: forward L y = d, backward
-// L^T z = y, blocked by kNB; a diagonal block is a product with the inverse
-// of the factor's block (one output per thread), the off-diagonal updates
-// use all threads. The column lives in shared memory.
-__global__ void __launch_bounds__(256) solve_kernel(double const *L, int m, double const *D, double *Z,
-                                                    double const *Linv)
+// One block step of the backward solve L^T Z = Y for N right-hand sides
+// (R and Z are m x N, row-major; R holds the forward solution Y, which the
+// factorization carried along), 64 of them per blockIdx.y. Every CTA forms
+// the block's solution z = Linv^T r_b from the inverse of the factor's
+// diagonal block (r_b: rows k0 .. k0 + nb of R, final for this step); CTA
+// 0 stores it in Z; then each CTA updates its 64-row chunk of the rows
+// above, R[r] -= L[b, r]^T z. Both are 64 x 64 x 64 products (mm64; zero
+// padding beyond nb, N and the chunk). Dynamic shared memory kTrsmSmem:
+// r_b and z (kNB x 64 each) and one kNB x (kNB + 1) tile, first Linv^T,
+// then the tile of L.
+constexpr size_t kTrsmSmem = sizeof(double) * (2 * (size_t)kNB * 64 + (size_t)kNB * (kNB + 1));
+
+__global__ void __launch_bounds__(256) trsm_back_kernel(double const *L, double const *Linv_b, int m, int N, int k0,
+                                                        double *R, double *Z)
 {
-  extern __shared__ double col[]; // [m]
-  int const k = blockIdx.x;
+  extern __shared__ double ts_sm[];
+  double *const rb = ts_sm;            // [kNB][64]
+  double *const zb = ts_sm + kNB * 64; // [kNB][64]
+  double(*lt)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(ts_sm + 2 * kNB * 64);
+  int const nb = min(kNB, m - k0);
+  int const n0 = 64 * (int)blockIdx.y, nc = min(64, N - n0); // the CTA's columns
   int const tid = threadIdx.x;
-  for (int i = tid; i < m; i += blockDim.x)
-    col[i] = D[(int64_t)k * m + i];
+  int const rr = 4 * (tid >> 4), cc = tid & 15;
+  for (int e = tid; e < kNB * 64; e += blockDim.x)
+  {
+    int const q = e / 64, n = e % 64;
+    rb[e] = (q < nb && n < nc) ? R[(int64_t)(k0 + q) * N + n0 + n] : 0.0;
+    lt[e % kNB][e / kNB] = Linv_b[e];
+  }
   __syncthreads();
-  int const nblk = (m + kNB - 1) / kNB;
-  // forward
-  for (int b = 0; b < nblk; ++b)
+  double acc[4][4];
+  mm64<true>(lt, rb, 64, acc); // Linv^T is upper triangular
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int w = 0; w < 4; ++w)
+      zb[(rr + u) * 64 + cc + 16 * w] = acc[u][w];
+  __syncthreads();
+  if (blockIdx.x == 0)
+    for (int e = tid; e < nb * nc; e += blockDim.x)
+      Z[(int64_t)(k0 + e / nc) * N + n0 + e % nc] = zb[(e / nc) * 64 + e % nc];
+  // the CTA's rows, above the block
+  int const r0 = kNB * (int)blockIdx.x, nr = min(k0, r0 + kNB) - r0;
+  if (nr <= 0)
+    return;
+  // the tile: lt[r][q] = L[k0 + q][r0 + r]
+  for (int e = tid; e < kNB * kNB; e += blockDim.x)
   {
-    int const k0 = b * kNB, nb = min(kNB, m - k0);
-    {
-      // y = Linv t on the block (t: the block's entries, already updated)
-      double const *li = Linv + (size_t)b * kNB * kNB;
-      double y = 0.0;
-      if (tid < nb)
-        for (int q = 0; q <= tid; ++q)
-          y = fma(li[tid * kNB + q], col[k0 + q], y);
-      __syncthreads();
-      if (tid < nb)
-        col[k0 + tid] = y;
-    }
-    __syncthreads();
-    for (int i = k0 + nb + tid; i < m; i += blockDim.x)
-    {
-      double const *row = L + (int64_t)i * m + k0;
-      double s = 0.0;
-      for (int q = 0; q < nb; ++q)
-        s += row[q] * col[k0 + q];
-      col[i] -= s;
-    }
-    __syncthreads();
+    int const q = e / kNB, r = e % kNB;
+    lt[r][q] = (r < nr && q < nb) ? L[(int64_t)(k0 + q) * m + r0 + r] : 0.0;
   }
-  // backward
-  for (int b = nblk - 1; b >= 0; --b)
-  {
-    int const k0 = b * kNB, nb = min(kNB, m - k0);
+  __syncthreads();
+  mm64(lt, zb, 64, acc);
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int w = 0; w < 4; ++w)
     {
-      // z = Linv^T t on the block
-      double const *li = Linv + (size_t)b * kNB * kNB;
-      double z = 0.0;
-      if (tid < nb)
-        for (int q = tid; q < nb; ++q)
-          z = fma(li[q * kNB + tid], col[k0 + q], z);
-      __syncthreads();
-      if (tid < nb)
-        col[k0 + tid] = z;
+      int const r = rr + u, n = cc + 16 * w;
+      if (r < nr && n < nc)
+        R[(int64_t)(r0 + r) * N + n0 + n] -= acc[u][w];
     }
-    __syncthreads();
-    for (int i = tid; i < k0; i += blockDim.x)
-    {
-      double s = 0.0;
-      for (int q = 0; q < nb; ++q)
-        s += L[(int64_t)(k0 + q) * m + i] * col[k0 + q];
-      col[i] -= s;
-    }
-    __syncthreads();
-  }
-  for (int i = tid; i < m; i += blockDim.x)
-    Z[(int64_t)k * m + i] = col[i];
 }
 
 // ---- ensemble-space solve (diagonal R, no localization)
@@ -731,8 +849,8 @@ __global__ void __launch_bounds__(256) lu_update_kernel(double *C, int m, int k0
 }
 
 // Z_k = C^-1 D_k from the LU factors, one member per CTA: the row swaps,
-// forward L y = P d (unit diagonal), backward U z = y; blocked like
-// solve_kernel, the column in shared memory.
+// forward L y = P d (unit diagonal), backward U z = y; blocked by kNB,
+// the column in shared memory.
 __global__ void __launch_bounds__(256) lu_solve_kernel(double const *LU, int const *piv, int m, double const *D,
                                                        double *Z)
 {
@@ -1103,7 +1221,8 @@ struct Enkf
   int device = 0;
   cudaStream_t stream = nullptr;
   DevBuf<double> HA, D, C, Z, W;
-  DevBuf<double> Linv; // inverses of the Cholesky factor's diagonal blocks
+  DevBuf<double> Linv;   // inverses of the Cholesky factor's diagonal blocks
+  DevBuf<double> Rt, Yt; // m x N: the right-hand sides (then the forward solution), Z
   DevBuf<int> err;
   // localization: geometry, observation points (input order and bucket
   // order), bucket offsets, and the transposed HA / Z and the update rows
@@ -1541,23 +1660,32 @@ struct Enkf
     }
   }
 
+  // Cholesky of C = HA^T HA scale (localized) + R by blocks of kNB, carrying
+  // the forward solve L Y = D^T of the right-hand sides along (Rt, m x N):
+  // the panel kernel takes each block's solve, the trailing update the
+  // rows below.
   void factor(int N, int m, double scale, double const *var, double const *cov)
   {
     int const t32 = (m + 31) / 32;
     cov_kernel<<<dim3(t32, t32), 256, 0, stream>>>(HA.p, N, m, scale, var, cov, C.p, loc ? oxyz.p : nullptr, lg, 0);
     ADM_CK(cudaGetLastError());
+    Rt.alloc((size_t)m * N);
+    int64_t const nm = (int64_t)N * m;
+    transpose_kernel<<<(unsigned)((nm + 255) / 256), 256, 0, stream>>>(D.p, N, m, Rt.p);
+    ADM_CK(cudaGetLastError());
     Linv.alloc((size_t)((m + kNB - 1) / kNB) * kNB * kNB);
+    ADM_CK(cudaFuncSetAttribute(potrf_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPotrfSmem));
+    ADM_CK(cudaFuncSetAttribute(trsm_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmem));
+    int const nchunk = (N + 63) / 64;
     for (int k0 = 0; k0 < m; k0 += kNB)
     {
       double *const li = Linv.p + (size_t)(k0 / kNB) * kNB * kNB;
-      potrf_diag_kernel<<<1, 256, 0, stream>>>(C.p, m, k0, err.p, li);
-      int const below = m - k0 - kNB;
+      potrf_diag_kernel<<<1, 256, kPotrfSmem, stream>>>(C.p, m, k0, err.p, li);
+      int const below = std::max(0, m - k0 - kNB);
+      int const t = (below + 63) / 64;
+      trsm_panel_kernel<<<t + nchunk, 256, kPanelSmem, stream>>>(C.p, m, k0, li, Rt.p, N);
       if (below > 0)
-      {
-        trsm_panel_kernel<<<(below + 127) / 128, 128, 0, stream>>>(C.p, m, k0, li);
-        int const t = (below + 63) / 64;
-        syrk_update_kernel<<<dim3(t, t), 256, 0, stream>>>(C.p, m, k0);
-      }
+        syrk_update_kernel<<<dim3(t + nchunk, t), 256, 0, stream>>>(C.p, m, k0, Rt.p, N);
       ADM_CK(cudaGetLastError());
     }
   }
@@ -1565,16 +1693,30 @@ struct Enkf
   // Z = C^-1 D, W = HA^T Z scale
   void solve_and_w(int N, int m, double scale, double *Wout)
   {
-    size_t const smem = (size_t)m * sizeof(double);
     if (factored_lu)
     {
+      size_t const smem = (size_t)m * sizeof(double);
       ADM_CK(cudaFuncSetAttribute(lu_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       lu_solve_kernel<<<N, 256, smem, stream>>>(C.p, piv.p, m, D.p, Z.p);
     }
     else
     {
-      ADM_CK(cudaFuncSetAttribute(solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      solve_kernel<<<N, 256, smem, stream>>>(C.p, m, D.p, Z.p, Linv.p);
+      // blocked backward solve of all N columns (m x N layout, 64 columns
+      // per CTA) from the forward solution that the factorization left in Rt
+      Yt.alloc((size_t)m * N);
+      int64_t const nm = (int64_t)N * m;
+      ADM_CK(cudaFuncSetAttribute(trsm_back_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmSmem));
+      int const nblk = (m + kNB - 1) / kNB;
+      unsigned const nchunk = (unsigned)((N + 63) / 64);
+      for (int b = nblk - 1; b >= 0; --b)
+      {
+        int const k0 = b * kNB;
+        trsm_back_kernel<<<dim3(std::max(1, (k0 + kNB - 1) / kNB), nchunk), 256, kTrsmSmem, stream>>>(
+            C.p, Linv.p + (size_t)b * kNB * kNB, m, N, k0, Rt.p, Yt.p);
+      }
+      ADM_CK(cudaGetLastError());
+      // Yt holds Z (m x N)
+      transpose_kernel<<<(unsigned)((nm + 255) / 256), 256, 0, stream>>>(Yt.p, m, N, Z.p);
     }
     ADM_CK(cudaGetLastError());
     w_kernel<<<(N * N * 32 + 255) / 256, 256, 0, stream>>>(HA.p, Z.p, N, m, scale, Wout);

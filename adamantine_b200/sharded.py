@@ -36,6 +36,7 @@ class LibrarySteps:
 
     def __init__(self, enkf):
         self._L = _lib.load()
+        self._enkf = enkf  # keeps the handle alive while the steps use it
         self._h = enkf._h
 
     def observe(self, states, n_state, obs_index):

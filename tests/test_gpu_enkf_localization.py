@@ -176,3 +176,25 @@ def test_localization_rejects_bad_arguments():
     enkf.set_localization("step_function", 1e-3, pts[idx[0]][:10], grid)
     with pytest.raises(AdmError):  # 60 observations against a localization of 10
         run_gpu(enkf, states, params, idx, obs, var, pert, n_state)
+
+
+def test_gain_of_many_members_through_the_blocked_solve():
+    """The gain of 100 members (more than one 64-column chunk of the blocked
+    triangular solves) with a full observation covariance (the m x m
+    Cholesky path; m = 150, a partial last block) against the numpy gain."""
+    from adamantine_b200.sharded import LibrarySteps
+
+    from sharded_steps import NumpySteps
+
+    rng = np.random.default_rng(41)
+    N, m = 100, 150
+    hx = 300.0 + rng.normal(0.0, 20.0, (N, m))
+    obs = 300.0 + rng.normal(0.0, 20.0, m)
+    pert = rng.normal(0.0, 5.0, (N, m))
+    a = rng.normal(size=(m, m))
+    cov = a @ a.T / m + 25.0 * np.eye(m)
+    dev = torch.device("cuda")
+    w = LibrarySteps(EnKF()).gain(torch.tensor(hx, device=dev), torch.tensor(obs, device=dev),
+                                  torch.tensor(pert, device=dev), obs_cov=torch.tensor(cov, device=dev))
+    ref = NumpySteps().gain(torch.tensor(hx), torch.tensor(obs), torch.tensor(pert), obs_cov=torch.tensor(cov))
+    assert rel_max(w.cpu().numpy(), ref.numpy()) <= 1e-10
