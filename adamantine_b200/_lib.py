@@ -108,6 +108,40 @@ SIGNATURES = {
     "adm_microstructure_set_old_temperature": [_VP, _VP],
     "adm_microstructure_compute_G_and_R": [_VP, _VP, ctypes.c_double, ctypes.c_int64, _VP,
                                            ctypes.POINTER(ctypes.c_int64)],
+    "adm_amr_mesh_create": [_VP, ctypes.c_int32, ctypes.POINTER(_VP)],
+    "adm_amr_mesh_destroy": [_VP],
+    "adm_amr_mesh_set_cells": [_VP, _VP, _VP, _VP],
+    "adm_amr_mesh_refine_mesh": [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_int32,
+                                 ctypes.c_int32],
+    "adm_amr_mesh_execute": [_VP, _VP, _VP],
+    "adm_amr_mesh_build": [_VP],
+    "adm_amr_mesh_n_leaves": [_VP, ctypes.POINTER(ctypes.c_int64)],
+    "adm_amr_mesh_leaves": [_VP, _VP],
+    "adm_amr_mesh_n_dofs": [_VP, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)],
+    "adm_amr_mesh_dof_lattice": [_VP, _VP],
+    "adm_amr_mesh_constraints": [_VP, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64), _VP, _VP,
+                                 _VP, _VP],
+    "adm_amr_create": [_VP, ctypes.c_int32, ctypes.c_int32, _VP, ctypes.POINTER(_VP)],
+    "adm_amr_destroy": [_VP],
+    "adm_amr_set_cells": [_VP, _VP, _VP, _VP],
+    "adm_amr_setup": [_VP, ctypes.c_double],
+    "adm_amr_refine_mesh": [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32],
+    "adm_amr_execute": [_VP, _VP, _VP],
+    "adm_amr_n_dofs": [_VP, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)],
+    "adm_amr_n_leaves": [_VP, ctypes.POINTER(ctypes.c_int64)],
+    "adm_amr_leaves": [_VP, _VP],
+    "adm_amr_dof_lattice": [_VP, _VP],
+    "adm_amr_solution": [_VP, ctypes.POINTER(_VP)],
+    "adm_amr_get_solution": [_VP, _VP],
+    "adm_amr_set_solution": [_VP, _VP],
+    "adm_amr_set_time": [_VP, ctypes.c_double],
+    "adm_amr_vmult": [_VP, _VP, _VP],
+    "adm_amr_inverse_mass": [_VP, _VP],
+    "adm_amr_evolve_one_time_step": [_VP, ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_double)],
+    "adm_amr_level_values": [_VP, ctypes.c_int32, _VP],
+    "adm_amr_level_layout": [_VP, ctypes.c_int32, _VP, ctypes.POINTER(ctypes.c_int64)],
+    "adm_amr_level_cell_state": [_VP, ctypes.c_int32, _VP],
+    "adm_amr_synchronize": [_VP],
     "adm_enkf_analysis": [_VP, ctypes.c_int32, _VP, ctypes.c_int64, ctypes.c_int64, _VP, ctypes.c_int32,
                           ctypes.c_int32, _VP, _VP, _VP, _VP, _VP, _VP],
 }

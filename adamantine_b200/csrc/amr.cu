@@ -1,0 +1,1549 @@
+/* Refined meshes for the thermal path: a forest of octrees over the coarse
+ * box mesh, refined along the beams' paths and balanced 2:1 across faces and
+ * edges, with hanging-node constraints.
+ *
+ * Reference behaviour followed:
+ *  - compute_cells_to_refine (application/adamantine.hh:540-606): the active
+ *    cells whose bounding box meets a beam's box (scaled by 2) at any of
+ *    n_time_steps sample times in [time, next_refinement_time);
+ *    HeatSource::get_bounding_box (GoldakHeatSource.cc:152-190,
+ *    ElectronBeamHeatSource.cc:162-200, CubeHeatSource.cc:111-123);
+ *  - refine_mesh (application/adamantine.hh:608-681): n_refinements rounds of
+ *    {coarsen flags on every cell above level 0 when coarsen_after_beam,
+ *    cleared on the cells to refine; refine flags on the cells to refine
+ *    below level n_refinements; execute};
+ *  - make_hanging_node_constraints (application/adamantine.hh:514-523): the
+ *    value at a node of a fine cell lying inside a face or edge of a coarser
+ *    active neighbour, and not one of its nodes, is the coarse cell's
+ *    interpolant there;
+ *  - ThermalOperator::vmult_add with constraints (ThermalOperator.templates.hh
+ *    :205-224: read through the constraints, distribute the result back) and
+ *    compute_inverse_mass_matrix (:140-160);
+ *  - refine_and_transfer (application/adamantine.hh:312-539): the solution is
+ *    interpolated onto the new mesh (SolutionTransfer: the old finite-element
+ *    field evaluated at the new nodes) and the cell data carried over
+ *    (CellDataTransfer: children copy their parent; a coarsened parent takes
+ *    its first child's data).
+ *
+ * B200 layout: one structured level grid per refinement level (the coarse box
+ * refined 2^l times), with the tile kernel of the uniform path run on the
+ * tiles that hold leaves of that level (its active cells); faces towards
+ * cells of the material region are interior on every level. The composite
+ * vector holds the non-hanging nodes; one gather kernel prolongs it to the
+ * level grids (constraints resolved, C y) and one gather kernel restricts the
+ * level results back (C^T), both from host-built CSR tables, deterministic
+ * (no atomics).
+ *
+ * Lattice: every node of a level-l cell lies on the vertex lattice of level
+ * max_level + 1 (degree 1 and 2 nodes are vertices and midpoints), so a node
+ * is keyed by its integer lattice coordinates and coincident nodes of
+ * different levels share a key.
+ */
+#include "capi_common.hpp"
+#include "thermal.hpp"
+#include "../../include/adamantine_b200_amr.h"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <unordered_map>
+#include <vector>
+
+namespace adm
+{
+namespace
+{
+
+// face (6) and edge (12) neighbour offsets
+struct Offsets
+{
+  int o[18][3];
+  int n = 0;
+  Offsets()
+  {
+    for (int z = -1; z <= 1; ++z)
+      for (int y = -1; y <= 1; ++y)
+        for (int x = -1; x <= 1; ++x)
+        {
+          int const nz = (x != 0) + (y != 0) + (z != 0);
+          if (nz == 1 || nz == 2)
+          {
+            o[n][0] = x;
+            o[n][1] = y;
+            o[n][2] = z;
+            ++n;
+          }
+        }
+  }
+};
+Offsets const kFaceEdge;
+
+// 1-D Lagrange basis of degree p on the equidistant (= Gauss-Lobatto for
+// p <= 2) nodes a / p, at u in [0, 1].
+double lagrange(int p, int a, double u)
+{
+  double v = 1.0;
+  for (int b = 0; b <= p; ++b)
+    if (b != a)
+      v *= (u * p - b) / (double)(a - b);
+  return v;
+}
+
+} // namespace
+
+// ---------------------------------------------------------------- forest
+struct Forest
+{
+  int nc[3] = {0, 0, 0};
+  int max_level = 0;
+  std::vector<std::vector<uint8_t>> leaf, exists;
+
+  int64_t n(int l, int d) const { return (int64_t)nc[d] << l; }
+  int64_t cells(int l) const { return n(l, 0) * n(l, 1) * n(l, 2); }
+  int64_t index(int l, int64_t i, int64_t j, int64_t k) const { return i + n(l, 0) * (j + n(l, 1) * k); }
+  bool inside(int l, int64_t i, int64_t j, int64_t k) const
+  {
+    return i >= 0 && j >= 0 && k >= 0 && i < n(l, 0) && j < n(l, 1) && k < n(l, 2);
+  }
+
+  void init(int const c[3], int L)
+  {
+    std::copy(c, c + 3, nc);
+    max_level = L;
+    leaf.assign(L + 1, {});
+    exists.assign(L + 1, {});
+    for (int l = 0; l <= L; ++l)
+    {
+      leaf[l].assign(cells(l), 0);
+      exists[l].assign(cells(l), 0);
+    }
+    std::fill(leaf[0].begin(), leaf[0].end(), 1);
+    std::fill(exists[0].begin(), exists[0].end(), 1);
+  }
+
+  // m <= l: the region of cell (l, i, j, k) lies in the leaf of level m;
+  // l + 1: that cell exists and is refined.
+  int status(int l, int64_t i, int64_t j, int64_t k) const
+  {
+    for (int m = l; m >= 0; --m)
+    {
+      int const s = l - m;
+      int64_t const c = index(m, i >> s, j >> s, k >> s);
+      if (exists[m][c])
+        return leaf[m][c] ? m : m + 1;
+    }
+    return 0;
+  }
+
+  void refine(int l, int64_t i, int64_t j, int64_t k)
+  {
+    int64_t const c = index(l, i, j, k);
+    leaf[l][c] = 0;
+    for (int q = 0; q < 8; ++q)
+    {
+      int64_t const cc = index(l + 1, 2 * i + (q & 1), 2 * j + ((q >> 1) & 1), 2 * k + (q >> 2));
+      exists[l + 1][cc] = 1;
+      leaf[l + 1][cc] = 1;
+    }
+  }
+
+  void coarsen(int l, int64_t i, int64_t j, int64_t k)
+  {
+    for (int q = 0; q < 8; ++q)
+    {
+      int64_t const cc = index(l + 1, 2 * i + (q & 1), 2 * j + ((q >> 1) & 1), 2 * k + (q >> 2));
+      exists[l + 1][cc] = 0;
+      leaf[l + 1][cc] = 0;
+    }
+    leaf[l][index(l, i, j, k)] = 1;
+  }
+
+  // Leaves no more than one level apart across every face and edge: a leaf
+  // of level l whose face/edge neighbour region lies in a leaf of level
+  // m < l - 1 refines that leaf (repeated until nothing changes).
+  void balance()
+  {
+    bool changed = true;
+    while (changed)
+    {
+      changed = false;
+      for (int l = max_level; l >= 2; --l)
+        for (int64_t k = 0; k < n(l, 2); ++k)
+          for (int64_t j = 0; j < n(l, 1); ++j)
+            for (int64_t i = 0; i < n(l, 0); ++i)
+            {
+              if (!leaf[l][index(l, i, j, k)])
+                continue;
+              for (int o = 0; o < kFaceEdge.n; ++o)
+              {
+                int64_t const a = i + kFaceEdge.o[o][0], b = j + kFaceEdge.o[o][1], c = k + kFaceEdge.o[o][2];
+                if (!inside(l, a, b, c))
+                  continue;
+                int const m = status(l, a, b, c);
+                if (m < l - 1)
+                {
+                  int const s = l - m;
+                  refine(m, a >> s, b >> s, c >> s);
+                  changed = true;
+                }
+              }
+            }
+    }
+  }
+
+  // Coarsening the family of parent (l, i, j, k) keeps the balance: no
+  // face/edge neighbour of its children is refined below level l + 1.
+  bool coarsening_keeps_balance(int l, int64_t i, int64_t j, int64_t k) const
+  {
+    for (int q = 0; q < 8; ++q)
+    {
+      int64_t const ci = 2 * i + (q & 1), cj = 2 * j + ((q >> 1) & 1), ck = 2 * k + (q >> 2);
+      for (int o = 0; o < kFaceEdge.n; ++o)
+      {
+        int64_t const a = ci + kFaceEdge.o[o][0], b = cj + kFaceEdge.o[o][1], c = ck + kFaceEdge.o[o][2];
+        if (!inside(l + 1, a, b, c) || ((a >> 1) == i && (b >> 1) == j && (c >> 1) == k))
+          continue;
+        if (status(l + 1, a, b, c) > l + 1)
+          return false;
+      }
+    }
+    return true;
+  }
+};
+
+// ------------------------------------------------------------------ mesh
+// DoFs, hanging-node constraints and the level-grid maps of a forest.
+struct AmrMesh
+{
+  adm_config cfg{};
+  std::vector<std::vector<double>> segments; // per source, 5 doubles per segment
+  int p = 1;
+  Forest forest;
+  std::vector<uint8_t> coarse_active, coarse_mat, coarse_init;
+  // lattice (vertex lattice of level max_level + 1)
+  int64_t NX[3] = {0, 0, 0};
+  // composite DoFs (sorted lattice keys) and hanging constraints
+  std::vector<int64_t> dof_key;
+  std::unordered_map<int64_t, int32_t> dof_of;
+  std::unordered_map<int64_t, std::vector<std::pair<int32_t, double>>> hanging;
+  int64_t n_nodes_all = 0; // distinct node positions of the active leaves
+
+  int64_t key(int64_t X, int64_t Y, int64_t Z) const { return X + (NX[0] + 1) * (Y + (NX[1] + 1) * Z); }
+  void unkey(int64_t k, int64_t x[3]) const
+  {
+    x[0] = k % (NX[0] + 1);
+    k /= NX[0] + 1;
+    x[1] = k % (NX[1] + 1);
+    x[2] = k / (NX[1] + 1);
+  }
+  // lattice coordinate of local node a of cell i of level l
+  int64_t lat(int l, int64_t i, int a) const { return (p * i + a) * ((int64_t)2 << (forest.max_level - l)) / p; }
+  int64_t cell_size(int l) const { return (int64_t)2 << (forest.max_level - l); }
+
+  bool in_domain(int l, int64_t i, int64_t j, int64_t k) const
+  {
+    return coarse_active[forest.index(0, i >> l, j >> l, k >> l)] != 0;
+  }
+  bool active_leaf(int l, int64_t i, int64_t j, int64_t k) const
+  {
+    return forest.leaf[l][forest.index(l, i, j, k)] && in_domain(l, i, j, k);
+  }
+
+  void init(adm_config const &c, int max_level)
+  {
+    cfg = c;
+    if (cfg.degree != 1 && cfg.degree != 2)
+      throw Error(ADM_ERR_UNSUPPORTED, "refined meshes take FE degree 1 or 2");
+    if (max_level < 0 || max_level > 6)
+      throw Error(ADM_ERR_UNSUPPORTED, "refinement levels: 0 to 6");
+    for (int d = 0; d < 3; ++d)
+      if (cfg.n_cells[d] < 1)
+        throw Error(ADM_ERR_INVALID, "n_cells must be positive");
+    p = cfg.degree;
+    segments.assign(cfg.n_sources, {});
+    for (int b = 0; b < cfg.n_sources; ++b)
+    {
+      adm_source const &s = cfg.sources[b];
+      if (s.type != 2 && s.n_segments > 0)
+      {
+        if (!s.segments)
+          throw Error(ADM_ERR_INVALID, "scan path segments missing");
+        segments[b].assign(s.segments, s.segments + 5 * s.n_segments);
+      }
+      cfg.sources[b].segments = nullptr;
+    }
+    forest.init(cfg.n_cells, max_level);
+    for (int d = 0; d < 3; ++d)
+      NX[d] = (int64_t)cfg.n_cells[d] << (max_level + 1);
+    size_t const C = forest.cells(0);
+    coarse_active.assign(C, 1);
+    coarse_mat.assign(C, 0);
+    coarse_init.assign(C, 0);
+  }
+
+  void set_cells(uint8_t const *active, uint8_t const *mat, uint8_t const *init)
+  {
+    size_t const C = forest.cells(0);
+    for (size_t c = 0; c < C; ++c)
+    {
+      coarse_active[c] = active ? (active[c] ? 1 : 0) : 1;
+      if (mat && mat[c] >= cfg.n_materials)
+        throw Error(ADM_ERR_INVALID, "material id out of range");
+      coarse_mat[c] = mat ? mat[c] : 0;
+      if (init && init[c] >= cfg.n_states)
+        throw Error(ADM_ERR_INVALID, "initial state index out of range for the material states");
+      coarse_init[c] = init ? init[c] : 0;
+    }
+  }
+
+  // ScanPath::value (source/ScanPath.cc:228-257): the beam centre at t;
+  // after the last segment a point far outside the domain.
+  void beam_center(int b, double t, double out[3]) const
+  {
+    std::vector<double> const &sg = segments[b];
+    int const n = (int)(sg.size() / 5);
+    if (n == 0 || t > sg[(n - 1) * 5])
+    {
+      out[0] = out[1] = out[2] = std::numeric_limits<double>::lowest();
+      return;
+    }
+    int lo = 0, hi = n - 1;
+    while (lo < hi)
+    {
+      int const mid = (lo + hi) / 2;
+      if (t > sg[mid * 5])
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    double st_t = 0.0, sp[3];
+    for (int d = 0; d < 3; ++d)
+      sp[d] = lo > 0 ? sg[(lo - 1) * 5 + 2 + d] : sg[lo * 5 + 2 + d];
+    if (lo > 0)
+      st_t = sg[(lo - 1) * 5];
+    double const et = sg[lo * 5];
+    for (int d = 0; d < 3; ++d)
+      out[d] = sp[d] + (sg[lo * 5 + 2 + d] - sp[d]) / (et - st_t) * (t - st_t);
+  }
+
+  // compute_cells_to_refine: every leaf (material or not) whose bounding box
+  // meets a beam box at one of the sample times (closed boxes).
+  std::vector<uint8_t> cells_to_refine(int l, double time, double next_time, int n_steps) const
+  {
+    std::vector<std::array<double, 6>> boxes;
+    double const scaling = 2.0;
+    for (int s = 0; s < n_steps; ++s)
+    {
+      double const t = time + (double)s / (double)n_steps * (next_time - time);
+      for (int b = 0; b < cfg.n_sources; ++b)
+      {
+        adm_source const &src = cfg.sources[b];
+        if (src.type == 2)
+        {
+          boxes.push_back({src.cube_min[0], src.cube_min[1], src.cube_min[2], src.cube_max[0], src.cube_max[1],
+                           src.cube_max[2]});
+          continue;
+        }
+        double c[3];
+        beam_center(b, t, c);
+        double const r = std::sqrt(src.radius_squared);
+        boxes.push_back({c[0] - scaling * r, c[1] - scaling * r, c[2] - scaling * src.depth, c[0] + scaling * r,
+                         c[1] + scaling * r, c[2]});
+      }
+    }
+    std::vector<uint8_t> flag(forest.cells(l), 0);
+    double h[3];
+    for (int d = 0; d < 3; ++d)
+      h[d] = cfg.extent[d] / (double)forest.n(l, d);
+    for (int64_t k = 0; k < forest.n(l, 2); ++k)
+      for (int64_t j = 0; j < forest.n(l, 1); ++j)
+        for (int64_t i = 0; i < forest.n(l, 0); ++i)
+        {
+          int64_t const c = forest.index(l, i, j, k);
+          if (!forest.leaf[l][c])
+            continue;
+          double const lo[3] = {cfg.origin[0] + i * h[0], cfg.origin[1] + j * h[1], cfg.origin[2] + k * h[2]};
+          double const hi[3] = {cfg.origin[0] + (i + 1) * h[0], cfg.origin[1] + (j + 1) * h[1],
+                                cfg.origin[2] + (k + 1) * h[2]};
+          for (auto const &bx : boxes)
+            if (lo[0] <= bx[3] && bx[0] <= hi[0] && lo[1] <= bx[4] && bx[1] <= hi[1] && lo[2] <= bx[5] &&
+                bx[2] <= hi[2])
+            {
+              flag[c] = 1;
+              break;
+            }
+        }
+    return flag;
+  }
+
+  // Execute per-leaf refine / coarsen flags (level-indexed arrays of the
+  // current leaves): refine, coarsen the families whose 8 children are all
+  // flagged leaves (unless that breaks the balance), then balance.
+  void execute(std::vector<std::vector<uint8_t>> const &refine, std::vector<std::vector<uint8_t>> const &coarsen)
+  {
+    Forest const old = forest;
+    int const L = forest.max_level;
+    for (int l = 0; l < L; ++l)
+      for (int64_t k = 0; k < forest.n(l, 2); ++k)
+        for (int64_t j = 0; j < forest.n(l, 1); ++j)
+          for (int64_t i = 0; i < forest.n(l, 0); ++i)
+          {
+            int64_t const c = forest.index(l, i, j, k);
+            if (old.leaf[l][c] && !refine[l].empty() && refine[l][c])
+              forest.refine(l, i, j, k);
+          }
+    for (int l = L - 1; l >= 0; --l)
+    {
+      if (coarsen[l + 1].empty())
+        continue;
+      for (int64_t k = 0; k < forest.n(l, 2); ++k)
+        for (int64_t j = 0; j < forest.n(l, 1); ++j)
+          for (int64_t i = 0; i < forest.n(l, 0); ++i)
+          {
+            int64_t const c = forest.index(l, i, j, k);
+            if (!forest.exists[l][c] || forest.leaf[l][c])
+              continue;
+            bool all = true;
+            for (int q = 0; q < 8 && all; ++q)
+            {
+              int64_t const cc = forest.index(l + 1, 2 * i + (q & 1), 2 * j + ((q >> 1) & 1), 2 * k + (q >> 2));
+              all = forest.leaf[l + 1][cc] && old.leaf[l + 1][cc] && coarsen[l + 1][cc];
+            }
+            if (all && forest.coarsening_keeps_balance(l, i, j, k))
+              forest.coarsen(l, i, j, k);
+          }
+    }
+    forest.balance();
+  }
+
+  // refine_mesh: n_refinements rounds of beam-box flags.
+  void refine_mesh(double time, double next_time, int n_steps, int n_refinements, bool coarsen_after_beam)
+  {
+    int const L = forest.max_level;
+    if (n_refinements > L)
+      throw Error(ADM_ERR_INVALID, "n_refinements exceeds the mesh's maximum level");
+    if (n_steps < 1)
+      throw Error(ADM_ERR_INVALID, "n_time_steps must be positive");
+    for (int r = 0; r < n_refinements; ++r)
+    {
+      std::vector<std::vector<uint8_t>> ref(L + 1), crs(L + 1);
+      for (int l = 0; l <= L; ++l)
+      {
+        std::vector<uint8_t> const hit = cells_to_refine(l, time, next_time, n_steps);
+        ref[l].assign(forest.cells(l), 0);
+        crs[l].assign(forest.cells(l), 0);
+        for (int64_t c = 0; c < forest.cells(l); ++c)
+        {
+          if (!forest.leaf[l][c])
+            continue;
+          if (coarsen_after_beam && l > 0 && !hit[c])
+            crs[l][c] = 1;
+          if (hit[c] && l < n_refinements)
+            ref[l][c] = 1;
+        }
+      }
+      execute(ref, crs);
+    }
+  }
+
+  // DoFs and constraints of the current forest.
+  void build()
+  {
+    int const L = forest.max_level;
+    std::unordered_map<int64_t, uint8_t> nodes; // key -> 1
+    for (int l = 0; l <= L; ++l)
+      for (int64_t k = 0; k < forest.n(l, 2); ++k)
+        for (int64_t j = 0; j < forest.n(l, 1); ++j)
+          for (int64_t i = 0; i < forest.n(l, 0); ++i)
+          {
+            if (!active_leaf(l, i, j, k))
+              continue;
+            for (int c = 0; c <= p; ++c)
+              for (int b = 0; b <= p; ++b)
+                for (int a = 0; a <= p; ++a)
+                  nodes[key(lat(l, i, a), lat(l, j, b), lat(l, k, c))] = 1;
+          }
+    n_nodes_all = (int64_t)nodes.size();
+    // hanging nodes: fine nodes on a face / edge of an active leaf whose
+    // neighbour region across it is refined material, off the leaf's nodes
+    std::unordered_map<int64_t, std::vector<std::pair<int64_t, double>>> hk;
+    for (int l = 0; l < L; ++l)
+      for (int64_t k = 0; k < forest.n(l, 2); ++k)
+        for (int64_t j = 0; j < forest.n(l, 1); ++j)
+          for (int64_t i = 0; i < forest.n(l, 0); ++i)
+          {
+            if (!active_leaf(l, i, j, k))
+              continue;
+            int64_t const cc[3] = {i, j, k};
+            for (int o = 0; o < kFaceEdge.n; ++o)
+            {
+              int64_t nb[3];
+              for (int d = 0; d < 3; ++d)
+                nb[d] = cc[d] + kFaceEdge.o[o][d];
+              if (!forest.inside(l, nb[0], nb[1], nb[2]) || !in_domain(l, nb[0], nb[1], nb[2]) ||
+                  forest.status(l, nb[0], nb[1], nb[2]) != l + 1)
+                continue;
+              // the shared entity: fixed coordinate (0 or p) along the
+              // offset's nonzero directions, free along the others
+              int fixed[3];
+              for (int d = 0; d < 3; ++d)
+                fixed[d] = kFaceEdge.o[o][d] == 0 ? -1 : (kFaceEdge.o[o][d] > 0 ? 2 * p : 0);
+              int const lim[3] = {fixed[0] < 0 ? 2 * p : 0, fixed[1] < 0 ? 2 * p : 0, fixed[2] < 0 ? 2 * p : 0};
+              for (int sz = 0; sz <= lim[2]; ++sz)
+                for (int sy = 0; sy <= lim[1]; ++sy)
+                  for (int sx = 0; sx <= lim[0]; ++sx)
+                  {
+                    int s[3] = {sx, sy, sz};
+                    for (int d = 0; d < 3; ++d)
+                      if (fixed[d] >= 0)
+                        s[d] = fixed[d];
+                    // s: level-(l+1) node offsets within the leaf (0..2p)
+                    if (s[0] % 2 == 0 && s[1] % 2 == 0 && s[2] % 2 == 0)
+                      continue; // a node of the leaf itself
+                    int64_t X[3];
+                    for (int d = 0; d < 3; ++d)
+                      X[d] = lat(l, cc[d], 0) + (int64_t)s[d] * cell_size(l) / (2 * p);
+                    int64_t const hkey = key(X[0], X[1], X[2]);
+                    if (hk.count(hkey))
+                      continue;
+                    std::vector<std::pair<int64_t, double>> ent;
+                    double wsum = 0.0;
+                    for (int c = 0; c <= p; ++c)
+                      for (int b = 0; b <= p; ++b)
+                        for (int a = 0; a <= p; ++a)
+                        {
+                          int const abc[3] = {a, b, c};
+                          double w = 1.0;
+                          for (int d = 0; d < 3; ++d)
+                            w *= lagrange(p, abc[d], s[d] / (2.0 * p));
+                          if (w == 0.0)
+                            continue;
+                          ent.push_back({key(lat(l, i, a), lat(l, j, b), lat(l, k, c)), w});
+                          wsum += w;
+                        }
+                    (void)wsum;
+                    hk[hkey] = std::move(ent);
+                  }
+            }
+          }
+    // masters: sorted keys of the non-hanging nodes
+    dof_key.clear();
+    for (auto const &kv : nodes)
+      if (!hk.count(kv.first))
+        dof_key.push_back(kv.first);
+    std::sort(dof_key.begin(), dof_key.end());
+    dof_of.clear();
+    dof_of.reserve(dof_key.size() * 2);
+    for (size_t d = 0; d < dof_key.size(); ++d)
+      dof_of[dof_key[d]] = (int32_t)d;
+    // resolve chains (a master that is itself hanging)
+    hanging.clear();
+    for (auto const &kv : hk)
+    {
+      std::vector<std::pair<int64_t, double>> cur = kv.second;
+      for (int depth = 0; depth < 8; ++depth)
+      {
+        bool again = false;
+        std::vector<std::pair<int64_t, double>> nxt;
+        for (auto const &e : cur)
+        {
+          auto it = hk.find(e.first);
+          if (it == hk.end())
+            nxt.push_back(e);
+          else
+          {
+            again = true;
+            for (auto const &f : it->second)
+              nxt.push_back({f.first, e.second * f.second});
+          }
+        }
+        cur.swap(nxt);
+        if (!again)
+          break;
+        if (depth == 7)
+          throw Error(ADM_ERR_INVALID, "internal: hanging-node constraints do not resolve");
+      }
+      std::vector<std::pair<int32_t, double>> res;
+      for (auto const &e : cur)
+      {
+        auto it = dof_of.find(e.first);
+        if (it == dof_of.end())
+          throw Error(ADM_ERR_INVALID, "internal: constraint master is not a node of the mesh");
+        bool merged = false;
+        for (auto &r : res)
+          if (r.first == it->second)
+          {
+            r.second += e.second;
+            merged = true;
+          }
+        if (!merged)
+          res.push_back({it->second, e.second});
+      }
+      std::sort(res.begin(), res.end());
+      hanging[kv.first] = std::move(res);
+    }
+  }
+
+  // entries (dof, weight) of the value at a node key
+  void entries(int64_t k, std::vector<std::pair<int32_t, double>> &out) const
+  {
+    out.clear();
+    auto it = dof_of.find(k);
+    if (it != dof_of.end())
+    {
+      out.push_back({it->second, 1.0});
+      return;
+    }
+    auto h = hanging.find(k);
+    if (h == hanging.end())
+      throw Error(ADM_ERR_INVALID, "internal: node without DoF or constraint");
+    out = h->second;
+  }
+
+  int64_t n_active_leaves(int l) const
+  {
+    int64_t n = 0;
+    for (int64_t k = 0; k < forest.n(l, 2); ++k)
+      for (int64_t j = 0; j < forest.n(l, 1); ++j)
+        for (int64_t i = 0; i < forest.n(l, 0); ++i)
+          n += active_leaf(l, i, j, k) ? 1 : 0;
+    return n;
+  }
+};
+
+// ------------------------------------------------------------ GPU kernels
+namespace
+{
+// y_lev[row_pos[r]] = sum_e w[e] y[dof[e]] over the row's entries
+__global__ void prolong_kernel(int64_t n_rows, int64_t const *row_pos, int64_t const *row_ptr, int32_t const *dof,
+                               double const *w, double const *y, double *lev)
+{
+  int64_t const r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= n_rows)
+    return;
+  double s = 0.0;
+  for (int64_t e = row_ptr[r]; e < row_ptr[r + 1]; ++e)
+    s += w[e] * y[dof[e]];
+  lev[row_pos[r]] = s;
+}
+
+// out[d] = sum_e w[e] lev[pos[e]] (add: out[d] += ...)
+__global__ void restrict_kernel(int64_t n_dofs, int64_t const *ptr, int64_t const *pos, double const *w,
+                                double const *lev, double *out, int add)
+{
+  int64_t const d = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (d >= n_dofs)
+    return;
+  double s = 0.0;
+  for (int64_t e = ptr[d]; e < ptr[d + 1]; ++e)
+    s += w[e] * lev[pos[e]];
+  out[d] = add ? out[d] + s : s;
+}
+
+__global__ void invert_kernel(int64_t n, double *m)
+{
+  int64_t const i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n)
+    m[i] = m[i] > 0.0 ? 1.0 / m[i] : 0.0;
+}
+
+// mass_lev = 1 / inv_mass_lev on the rows' nodes
+__global__ void mass_from_inverse_kernel(int64_t n_rows, int64_t const *row_pos, int64_t off,
+                                         double const *inv_mass, double *lev)
+{
+  int64_t const r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= n_rows)
+    return;
+  int64_t const p = row_pos[r];
+  double const v = inv_mass[p - off];
+  lev[p] = v > 0.0 ? 1.0 / v : 0.0;
+}
+
+// z = y + dt sum_j a_j k_j (up to 3 stage vectors)
+__global__ void stage_input_kernel(int64_t n, double const *y, double dt, int nk, double a0, double const *k0,
+                                   double a1, double const *k1, double a2, double const *k2, double *z)
+{
+  int64_t const i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  double s = 0.0;
+  if (nk > 0)
+    s += a0 * k0[i];
+  if (nk > 1)
+    s += a1 * k1[i];
+  if (nk > 2)
+    s += a2 * k2[i];
+  z[i] = y[i] + dt * s;
+}
+
+__global__ void scale_kernel(int64_t n, double const *inv_m, double *k)
+{
+  int64_t const i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n)
+    k[i] *= inv_m[i];
+}
+
+__global__ void fill_kernel(int64_t n, double v, double *y)
+{
+  int64_t const i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n)
+    y[i] = v;
+}
+
+unsigned blocks(int64_t n) { return (unsigned)std::max<int64_t>(1, (n + 255) / 256); }
+} // namespace
+
+// -------------------------------------------------------------- GPU driver
+class Amr
+{
+public:
+  Amr(adm_config const &cfg, int max_level, int device, cudaStream_t stream) : device_(device), stream_(stream)
+  {
+    mesh_.init(cfg, max_level);
+    if (cfg.dim != 3)
+      throw Error(ADM_ERR_UNSUPPORTED, "refined meshes are 3-D");
+  }
+
+  AmrMesh &mesh() { return mesh_; }
+  AmrMesh const &mesh() const { return mesh_; }
+  int64_t n_dofs() const { return (int64_t)mesh_.dof_key.size(); }
+  double *solution() { return y_.p; }
+
+  void setup(double initial_temperature)
+  {
+    ADM_CK(cudaSetDevice(device_));
+    mesh_.build();
+    build_levels(nullptr);
+    y_.alloc(n_dofs());
+    fill_kernel<<<blocks(n_dofs()), 256, 0, stream_>>>(n_dofs(), initial_temperature, y_.p);
+    ADM_CK(cudaGetLastError());
+    compute_inverse_mass();
+    ready_ = true;
+  }
+
+  void require_ready() const
+  {
+    if (!ready_)
+      throw Error(ADM_ERR_INVALID, "setup() has not been called");
+  }
+
+  // refine_and_transfer around an AmrMesh change (done by `change`)
+  template <class F> void remesh(F &&change)
+  {
+    require_ready();
+    ADM_CK(cudaSetDevice(device_));
+    // the old field on the level grids (constraints resolved) and the old
+    // cell states (ThermalPhysics::set_state_to_material_properties)
+    prolong(y_.p);
+    std::vector<double> old_lev(lev_n_);
+    ADM_CK(cudaMemcpyAsync(old_lev.data(), src_lev_.p, lev_n_ * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    ADM_CK(cudaStreamSynchronize(stream_));
+    Snapshot old;
+    old.forest = mesh_.forest;
+    old.off = lev_off_;
+    old.lev = std::move(old_lev);
+    int const ns = mesh_.cfg.n_states;
+    old.states.resize(levels_.size());
+    for (size_t l = 0; l < levels_.size(); ++l)
+    {
+      if (!levels_[l])
+        continue;
+      levels_[l]->set_state_to_material_properties();
+      old.states[l].resize(levels_[l]->n_cells() * ns);
+      levels_[l]->get_cell_state(old.states[l].data());
+    }
+    old.pitch.assign(levels_.size(), 0);
+    old.nn1.assign(levels_.size(), 0);
+    for (size_t l = 0; l < levels_.size(); ++l)
+      if (levels_[l])
+      {
+        old.pitch[l] = levels_[l]->mesh().pitch;
+        old.nn1[l] = levels_[l]->mesh().nn[1];
+      }
+    change();
+    mesh_.build();
+    build_levels(&old);
+    // SolutionTransfer: the old field at the new nodes
+    std::vector<double> y(n_dofs());
+    for (int64_t d = 0; d < n_dofs(); ++d)
+      y[d] = old.evaluate(mesh_, mesh_.dof_key[d]);
+    y_.alloc(n_dofs());
+    ADM_CK(cudaMemcpyAsync(y_.p, y.data(), y.size() * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    ADM_CK(cudaStreamSynchronize(stream_));
+    compute_inverse_mass();
+  }
+
+  void set_time(double t)
+  {
+    for (auto &th : levels_)
+      if (th)
+        th->set_time(t);
+  }
+
+  // dst = C^T (sum_l A_l) C src (composite vectors on the device)
+  void vmult(double *dst, double const *src)
+  {
+    require_ready();
+    ADM_CK(cudaSetDevice(device_));
+    prolong(src);
+    for (size_t l = 0; l < levels_.size(); ++l)
+      if (levels_[l])
+        levels_[l]->vmult(dst_lev_.p + lev_off_[l], src_lev_.p + lev_off_[l], false);
+    restrict_to(dst, 0);
+  }
+
+  double const *inverse_mass() const { return inv_m_.p; }
+
+  void copy_inverse_mass(double *dst)
+  {
+    require_ready();
+    ADM_CK(cudaSetDevice(device_));
+    ADM_CK(cudaMemcpyAsync(dst, inv_m_.p, n_dofs() * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    ADM_CK(cudaStreamSynchronize(stream_));
+  }
+
+  // device copies of the solution, ordered on the handle's stream
+  void copy_solution(double *other, bool out)
+  {
+    require_ready();
+    ADM_CK(cudaSetDevice(device_));
+    size_t const bytes = n_dofs() * sizeof(double);
+    if (out)
+      ADM_CK(cudaMemcpyAsync(other, y_.p, bytes, cudaMemcpyDeviceToDevice, stream_));
+    else
+      ADM_CK(cudaMemcpyAsync(y_.p, other, bytes, cudaMemcpyDeviceToDevice, stream_));
+    ADM_CK(cudaStreamSynchronize(stream_));
+  }
+
+  double evolve_one_time_step(double t, double dt)
+  {
+    require_ready();
+    ADM_CK(cudaSetDevice(device_));
+    Thermal::Tableau const tab = Thermal::tableau(mesh_.cfg.time_method);
+    int64_t const n = n_dofs();
+    for (int i = 0; i < tab.s; ++i)
+      k_[i].alloc(n);
+    z_.alloc(n);
+    for (int i = 0; i < tab.s; ++i)
+    {
+      double const *in = y_.p;
+      if (i > 0)
+      {
+        // z = y + dt sum_{j<i} a_ij k_j
+        double a[3] = {0, 0, 0};
+        double const *kk[3] = {k_[0].p, k_[0].p, k_[0].p};
+        int nk = 0;
+        for (int j = 0; j < i; ++j)
+          if (tab.a[i][j] != 0.0)
+          {
+            a[nk] = tab.a[i][j];
+            kk[nk] = k_[j].p;
+            ++nk;
+          }
+        stage_input_kernel<<<blocks(n), 256, 0, stream_>>>(n, y_.p, dt, nk, a[0], kk[0], a[1], kk[1], a[2], kk[2],
+                                                            z_.p);
+        ADM_CK(cudaGetLastError());
+        in = z_.p;
+      }
+      set_time(t + tab.c[i] * dt);
+      vmult(k_[i].p, in);
+      scale_kernel<<<blocks(n), 256, 0, stream_>>>(n, inv_m_.p, k_[i].p);
+      ADM_CK(cudaGetLastError());
+    }
+    // y += dt sum_i b_i k_i
+    double a[3] = {0, 0, 0};
+    double const *kk[3] = {k_[0].p, k_[0].p, k_[0].p};
+    int nk = 0;
+    for (int i = 0; i < tab.s; ++i)
+      if (tab.b[i] != 0.0)
+      {
+        if (nk == 3)
+        {
+          stage_input_kernel<<<blocks(n), 256, 0, stream_>>>(n, y_.p, dt, nk, a[0], kk[0], a[1], kk[1], a[2],
+                                                              kk[2], y_.p);
+          nk = 0;
+        }
+        a[nk] = tab.b[i];
+        kk[nk] = k_[i].p;
+        ++nk;
+      }
+    stage_input_kernel<<<blocks(n), 256, 0, stream_>>>(n, y_.p, dt, nk, a[0], kk[0], a[1], kk[1], a[2], kk[2],
+                                                        y_.p);
+    ADM_CK(cudaGetLastError());
+    return t + dt;
+  }
+
+  // the composite field on the level grid of level l (constraints resolved)
+  void level_values(int l, double *host)
+  {
+    require_ready();
+    if (l < 0 || l >= (int)levels_.size() || !levels_[l])
+      throw Error(ADM_ERR_INVALID, "no leaves on this level");
+    prolong(y_.p);
+    ADM_CK(cudaMemcpyAsync(host, src_lev_.p + lev_off_[l], levels_[l]->m() * sizeof(double),
+                           cudaMemcpyDeviceToHost, stream_));
+    ADM_CK(cudaStreamSynchronize(stream_));
+  }
+
+  Thermal *level(int l) { return (l >= 0 && l < (int)levels_.size()) ? levels_[l].get() : nullptr; }
+
+  void synchronize() { ADM_CK(cudaStreamSynchronize(stream_)); }
+
+private:
+  struct Snapshot
+  {
+    Forest forest;
+    std::vector<int64_t> off;
+    std::vector<double> lev;
+    std::vector<std::vector<double>> states;
+    std::vector<int> pitch, nn1;
+
+    // the old field at lattice node k: an old active leaf containing it
+    double evaluate(AmrMesh const &m, int64_t k) const
+    {
+      int64_t X[3];
+      m.unkey(k, X);
+      int const p = m.p;
+      for (int l = 0; l <= forest.max_level; ++l)
+      {
+        int64_t const S = m.cell_size(l);
+        int64_t lo[3], hi[3];
+        for (int d = 0; d < 3; ++d)
+        {
+          hi[d] = X[d] / S;
+          lo[d] = (X[d] % S == 0) ? hi[d] - 1 : hi[d];
+        }
+        for (int64_t c = lo[2]; c <= hi[2]; ++c)
+          for (int64_t b = lo[1]; b <= hi[1]; ++b)
+            for (int64_t a = lo[0]; a <= hi[0]; ++a)
+            {
+              if (!forest.inside(l, a, b, c) || !forest.leaf[l][forest.index(l, a, b, c)] ||
+                  !m.in_domain(l, a, b, c))
+                continue;
+              int64_t const cell[3] = {a, b, c};
+              double u[3];
+              for (int d = 0; d < 3; ++d)
+                u[d] = (double)(X[d] - cell[d] * S) / (double)S;
+              double v = 0.0;
+              for (int q2 = 0; q2 <= p; ++q2)
+                for (int q1 = 0; q1 <= p; ++q1)
+                  for (int q0 = 0; q0 <= p; ++q0)
+                  {
+                    double const w = lagrange(p, q0, u[0]) * lagrange(p, q1, u[1]) * lagrange(p, q2, u[2]);
+                    if (w == 0.0)
+                      continue;
+                    int64_t const nidx = (p * a + q0) + (int64_t)pitch[l] * ((p * b + q1) + (int64_t)nn1[l] * (p * c + q2));
+                    v += w * lev[off[l] + nidx];
+                  }
+              return v;
+            }
+      }
+      throw Error(ADM_ERR_INVALID, "internal: a new node lies in no old active leaf");
+    }
+
+    // CellDataTransfer: the state of the new leaf (l, i, j, k)
+    void state_of(int l, int64_t i, int64_t j, int64_t k, int ns, double *out) const
+    {
+      int m = forest.status(l, i, j, k);
+      int64_t a = i, b = j, c = k;
+      if (m <= l)
+      {
+        int const s = l - m;
+        a >>= s;
+        b >>= s;
+        c >>= s;
+      }
+      else
+      {
+        // coarsened: the first child, down to a leaf
+        m = l;
+        while (!forest.leaf[m][forest.index(m, a, b, c)])
+        {
+          a *= 2;
+          b *= 2;
+          c *= 2;
+          ++m;
+        }
+      }
+      int64_t const C = forest.cells(m);
+      int64_t const cell = forest.index(m, a, b, c);
+      for (int q = 0; q < ns; ++q)
+        out[q] = states[m][q * C + cell];
+    }
+  };
+
+  void build_levels(Snapshot const *old)
+  {
+    int const L = mesh_.forest.max_level;
+    int const ns = mesh_.cfg.n_states;
+    levels_.clear();
+    levels_.resize(L + 1);
+    lev_off_.assign(L + 1, 0);
+    int64_t off = 0;
+    for (int l = 0; l <= L; ++l)
+    {
+      if (mesh_.n_active_leaves(l) == 0)
+        continue;
+      adm_config c = mesh_.cfg;
+      for (int d = 0; d < 3; ++d)
+        c.n_cells[d] = (int32_t)mesh_.forest.n(l, d);
+      for (int b = 0; b < c.n_sources; ++b)
+        c.sources[b].segments = mesh_.segments[b].empty() ? nullptr : mesh_.segments[b].data();
+      auto th = std::make_unique<Thermal>(c, device_, stream_);
+      int64_t const C = mesh_.forest.cells(l);
+      std::vector<uint8_t> act(C), dom(C), mat(C), init(C);
+      for (int64_t k = 0; k < mesh_.forest.n(l, 2); ++k)
+        for (int64_t j = 0; j < mesh_.forest.n(l, 1); ++j)
+          for (int64_t i = 0; i < mesh_.forest.n(l, 0); ++i)
+          {
+            int64_t const cell = mesh_.forest.index(l, i, j, k);
+            int64_t const coarse = mesh_.forest.index(0, i >> l, j >> l, k >> l);
+            dom[cell] = mesh_.coarse_active[coarse];
+            act[cell] = mesh_.active_leaf(l, i, j, k) ? 1 : 0;
+            mat[cell] = mesh_.coarse_mat[coarse];
+            init[cell] = mesh_.coarse_init[coarse];
+          }
+      th->set_cells(act.data(), mat.data(), init.data(), nullptr, nullptr);
+      th->set_domain(dom.data());
+      th->setup();
+      if (old)
+      {
+        std::vector<double> st((size_t)C * ns, 0.0);
+        for (int64_t k = 0; k < mesh_.forest.n(l, 2); ++k)
+          for (int64_t j = 0; j < mesh_.forest.n(l, 1); ++j)
+            for (int64_t i = 0; i < mesh_.forest.n(l, 0); ++i)
+            {
+              int64_t const cell = mesh_.forest.index(l, i, j, k);
+              if (!act[cell])
+                continue;
+              double v[3] = {0, 0, 0};
+              old->state_of(l, i, j, k, ns, v);
+              for (int q = 0; q < ns; ++q)
+                st[(size_t)q * C + cell] = v[q];
+            }
+        th->set_cell_state(st.data());
+        th->get_state_from_material_properties();
+      }
+      lev_off_[l] = off;
+      off += (int64_t)((th->m() + 31) / 32 * 32);
+      levels_[l] = std::move(th);
+    }
+    lev_n_ = off;
+    src_lev_.alloc(std::max<int64_t>(1, lev_n_));
+    dst_lev_.alloc(std::max<int64_t>(1, lev_n_));
+    ADM_CK(cudaMemsetAsync(src_lev_.p, 0, lev_n_ * sizeof(double), stream_));
+    // prolongation rows (level nodes of active leaves) and their transpose
+    std::vector<int64_t> row_pos, row_ptr{0};
+    std::vector<int32_t> ent_dof;
+    std::vector<double> ent_w;
+    row_lev_.assign(L + 2, 0);
+    std::vector<std::pair<int32_t, double>> ent;
+    for (int l = 0; l <= L; ++l)
+    {
+      row_lev_[l] = (int64_t)row_pos.size();
+      if (!levels_[l])
+        continue;
+      Mesh const &lm = levels_[l]->mesh();
+      std::vector<int64_t> nodes;
+      for (int64_t k = 0; k < mesh_.forest.n(l, 2); ++k)
+        for (int64_t j = 0; j < mesh_.forest.n(l, 1); ++j)
+          for (int64_t i = 0; i < mesh_.forest.n(l, 0); ++i)
+          {
+            if (!mesh_.active_leaf(l, i, j, k))
+              continue;
+            int const p = mesh_.p;
+            for (int c = 0; c <= p; ++c)
+              for (int b = 0; b <= p; ++b)
+                for (int a = 0; a <= p; ++a)
+                  nodes.push_back((p * i + a) + (int64_t)lm.pitch * ((p * j + b) + (int64_t)lm.nn[1] * (p * k + c)));
+          }
+      std::sort(nodes.begin(), nodes.end());
+      nodes.erase(std::unique(nodes.begin(), nodes.end()), nodes.end());
+      for (int64_t nidx : nodes)
+      {
+        int64_t const x = nidx % lm.pitch, y = (nidx / lm.pitch) % lm.nn[1], z = nidx / ((int64_t)lm.pitch * lm.nn[1]);
+        int const s = mesh_.forest.max_level - l;
+        int64_t const f = ((int64_t)2 << s) / mesh_.p;
+        mesh_.entries(mesh_.key(x * f, y * f, z * f), ent);
+        row_pos.push_back(lev_off_[l] + nidx);
+        for (auto const &e : ent)
+        {
+          ent_dof.push_back(e.first);
+          ent_w.push_back(e.second);
+        }
+        row_ptr.push_back((int64_t)ent_dof.size());
+      }
+    }
+    row_lev_[L + 1] = (int64_t)row_pos.size();
+    n_rows_ = (int64_t)row_pos.size();
+    // transpose
+    int64_t const nd = n_dofs();
+    std::vector<int64_t> tptr(nd + 1, 0);
+    for (int32_t d : ent_dof)
+      ++tptr[d + 1];
+    for (int64_t d = 0; d < nd; ++d)
+      tptr[d + 1] += tptr[d];
+    std::vector<int64_t> tpos(ent_dof.size()), fill(tptr.begin(), tptr.end() - 1);
+    std::vector<double> tw(ent_dof.size());
+    for (int64_t r = 0; r < n_rows_; ++r)
+      for (int64_t e = row_ptr[r]; e < row_ptr[r + 1]; ++e)
+      {
+        int64_t const at = fill[ent_dof[e]]++;
+        tpos[at] = row_pos[r];
+        tw[at] = ent_w[e];
+      }
+    upload(row_pos_, row_pos);
+    upload(row_ptr_, row_ptr);
+    upload(ent_dof_, ent_dof);
+    upload(ent_w_, ent_w);
+    upload(tptr_, tptr);
+    upload(tpos_, tpos);
+    upload(tw_, tw);
+    ADM_CK(cudaStreamSynchronize(stream_));
+  }
+
+  template <class T> void upload(DevBuf<T> &buf, std::vector<T> const &v)
+  {
+    buf.alloc(std::max<size_t>(1, v.size()));
+    if (!v.empty())
+      ADM_CK(cudaMemcpyAsync(buf.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream_));
+    // the host vectors die with the caller: finish the copies first
+    ADM_CK(cudaStreamSynchronize(stream_));
+  }
+
+  void prolong(double const *y)
+  {
+    if (n_rows_ == 0)
+      return;
+    prolong_kernel<<<blocks(n_rows_), 256, 0, stream_>>>(n_rows_, row_pos_.p, row_ptr_.p, ent_dof_.p, ent_w_.p, y,
+                                                          src_lev_.p);
+    ADM_CK(cudaGetLastError());
+  }
+
+  void restrict_to(double *dst, int add)
+  {
+    restrict_kernel<<<blocks(n_dofs()), 256, 0, stream_>>>(n_dofs(), tptr_.p, tpos_.p, tw_.p, dst_lev_.p, dst, add);
+    ADM_CK(cudaGetLastError());
+  }
+
+  // compute_inverse_mass_matrix: 1 / (C^T sum_l M_l) with the lumped level
+  // masses of the leaves (the composite vector has no constrained entries)
+  void compute_inverse_mass()
+  {
+    inv_m_.alloc(std::max<int64_t>(1, n_dofs()));
+    for (size_t l = 0; l < levels_.size(); ++l)
+    {
+      if (!levels_[l])
+        continue;
+      levels_[l]->compute_inverse_mass_matrix();
+      int64_t const r0 = row_lev_[l], r1 = row_lev_[l + 1];
+      if (r1 > r0)
+        mass_from_inverse_kernel<<<blocks(r1 - r0), 256, 0, stream_>>>(r1 - r0, row_pos_.p + r0, lev_off_[l],
+                                                                       levels_[l]->inverse_mass_matrix(),
+                                                                       dst_lev_.p);
+      ADM_CK(cudaGetLastError());
+    }
+    restrict_to(inv_m_.p, 0);
+    invert_kernel<<<blocks(n_dofs()), 256, 0, stream_>>>(n_dofs(), inv_m_.p);
+    ADM_CK(cudaGetLastError());
+    ADM_CK(cudaStreamSynchronize(stream_));
+  }
+
+  int device_ = 0;
+  cudaStream_t stream_ = nullptr;
+  bool ready_ = false;
+  AmrMesh mesh_;
+  std::vector<std::unique_ptr<Thermal>> levels_;
+  std::vector<int64_t> lev_off_, row_lev_;
+  int64_t lev_n_ = 0, n_rows_ = 0;
+  DevBuf<double> src_lev_, dst_lev_;
+  DevBuf<int64_t> row_pos_, row_ptr_, tptr_, tpos_;
+  DevBuf<int32_t> ent_dof_;
+  DevBuf<double> ent_w_, tw_;
+  DevBuf<double> y_, inv_m_, z_, k_[4];
+};
+
+} // namespace adm
+
+struct adm_amr_mesh
+{
+  adm::AmrMesh m;
+};
+struct adm_amr
+{
+  std::unique_ptr<adm::Amr> a;
+};
+
+namespace
+{
+std::vector<std::vector<uint8_t>> level_flags(adm::AmrMesh const &m, uint8_t const *flags)
+{
+  // flags: one byte per active leaf ... of every leaf, in leaf order
+  std::vector<std::vector<uint8_t>> out(m.forest.max_level + 1);
+  int64_t q = 0;
+  for (int l = 0; l <= m.forest.max_level; ++l)
+  {
+    out[l].assign(m.forest.cells(l), 0);
+    for (int64_t c = 0; c < m.forest.cells(l); ++c)
+      if (m.forest.leaf[l][c])
+        out[l][c] = flags ? flags[q++] : 0;
+  }
+  return out;
+}
+
+int64_t n_leaves(adm::AmrMesh const &m)
+{
+  int64_t n = 0;
+  for (int l = 0; l <= m.forest.max_level; ++l)
+    for (int64_t c = 0; c < m.forest.cells(l); ++c)
+      n += m.forest.leaf[l][c];
+  return n;
+}
+
+void leaves(adm::AmrMesh const &m, int32_t *out)
+{
+  int64_t q = 0;
+  for (int l = 0; l <= m.forest.max_level; ++l)
+    for (int64_t k = 0; k < m.forest.n(l, 2); ++k)
+      for (int64_t j = 0; j < m.forest.n(l, 1); ++j)
+        for (int64_t i = 0; i < m.forest.n(l, 0); ++i)
+          if (m.forest.leaf[l][m.forest.index(l, i, j, k)])
+          {
+            out[4 * q + 0] = l;
+            out[4 * q + 1] = (int32_t)i;
+            out[4 * q + 2] = (int32_t)j;
+            out[4 * q + 3] = (int32_t)k;
+            ++q;
+          }
+}
+
+void dof_lattice(adm::AmrMesh const &m, int64_t *xyz)
+{
+  for (size_t d = 0; d < m.dof_key.size(); ++d)
+    m.unkey(m.dof_key[d], xyz + 3 * d);
+}
+
+void constraints(adm::AmrMesh const &m, int64_t *n_hanging, int64_t *n_entries, int64_t *xyz, int64_t *ptr,
+                 int32_t *dof, double *w)
+{
+  std::vector<int64_t> keys;
+  for (auto const &kv : m.hanging)
+    keys.push_back(kv.first);
+  std::sort(keys.begin(), keys.end());
+  int64_t ne = 0;
+  for (int64_t k : keys)
+    ne += (int64_t)m.hanging.at(k).size();
+  if (n_hanging)
+    *n_hanging = (int64_t)keys.size();
+  if (n_entries)
+    *n_entries = ne;
+  if (!xyz || !ptr || !dof || !w)
+    return;
+  int64_t e = 0;
+  ptr[0] = 0;
+  for (size_t h = 0; h < keys.size(); ++h)
+  {
+    m.unkey(keys[h], xyz + 3 * h);
+    for (auto const &pe : m.hanging.at(keys[h]))
+    {
+      dof[e] = pe.first;
+      w[e] = pe.second;
+      ++e;
+    }
+    ptr[h + 1] = e;
+  }
+}
+} // namespace
+
+extern "C" {
+
+// ------------------------------------------------------ host mesh entries
+int adm_amr_mesh_create(adm_config const *cfg, int max_level, adm_amr_mesh **out)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(cfg && out, "null argument");
+    auto h = std::make_unique<adm_amr_mesh>();
+    h->m.init(*cfg, max_level);
+    *out = h.release();
+  });
+}
+
+int adm_amr_mesh_destroy(adm_amr_mesh *h)
+{
+  delete h;
+  return ADM_OK;
+}
+
+int adm_amr_mesh_set_cells(adm_amr_mesh *h, uint8_t const *active, uint8_t const *material_id,
+                           uint8_t const *initial_state)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h, "null handle");
+    h->m.set_cells(active, material_id, initial_state);
+  });
+}
+
+int adm_amr_mesh_refine_mesh(adm_amr_mesh *h, double time, double next_refinement_time, int n_time_steps,
+                             int n_refinements, int coarsen_after_beam)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h, "null handle");
+    h->m.refine_mesh(time, next_refinement_time, n_time_steps, n_refinements, coarsen_after_beam != 0);
+    h->m.build();
+  });
+}
+
+int adm_amr_mesh_execute(adm_amr_mesh *h, uint8_t const *refine, uint8_t const *coarsen)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h, "null handle");
+    h->m.execute(level_flags(h->m, refine), level_flags(h->m, coarsen));
+    h->m.build();
+  });
+}
+
+int adm_amr_mesh_build(adm_amr_mesh *h)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h, "null handle");
+    h->m.build();
+  });
+}
+
+int adm_amr_mesh_n_leaves(adm_amr_mesh const *h, int64_t *n)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && n, "null argument");
+    *n = n_leaves(h->m);
+  });
+}
+
+int adm_amr_mesh_leaves(adm_amr_mesh const *h, int32_t *lijk)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && lijk, "null argument");
+    leaves(h->m, lijk);
+  });
+}
+
+int adm_amr_mesh_n_dofs(adm_amr_mesh const *h, int64_t *n_dofs, int64_t *n_nodes)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h, "null handle");
+    if (n_dofs)
+      *n_dofs = (int64_t)h->m.dof_key.size();
+    if (n_nodes)
+      *n_nodes = h->m.n_nodes_all;
+  });
+}
+
+int adm_amr_mesh_dof_lattice(adm_amr_mesh const *h, int64_t *xyz)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && xyz, "null argument");
+    dof_lattice(h->m, xyz);
+  });
+}
+
+int adm_amr_mesh_constraints(adm_amr_mesh const *h, int64_t *n_hanging, int64_t *n_entries, int64_t *xyz,
+                             int64_t *ptr, int32_t *dof, double *w)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h, "null handle");
+    constraints(h->m, n_hanging, n_entries, xyz, ptr, dof, w);
+  });
+}
+
+// ------------------------------------------------------------ GPU entries
+int adm_amr_create(adm_config const *cfg, int max_level, int device, void *stream, adm_amr **out)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(cfg && out, "null argument");
+    auto h = std::make_unique<adm_amr>();
+    h->a = std::make_unique<adm::Amr>(*cfg, max_level, device, (cudaStream_t)stream);
+    *out = h.release();
+  });
+}
+
+int adm_amr_destroy(adm_amr *h)
+{
+  delete h;
+  return ADM_OK;
+}
+
+int adm_amr_set_cells(adm_amr *h, uint8_t const *active, uint8_t const *material_id, uint8_t const *initial_state)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h, "null handle");
+    h->a->mesh().set_cells(active, material_id, initial_state);
+  });
+}
+
+int adm_amr_setup(adm_amr *h, double initial_temperature)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h, "null handle");
+    h->a->setup(initial_temperature);
+  });
+}
+
+int adm_amr_refine_mesh(adm_amr *h, double time, double next_refinement_time, int n_time_steps, int n_refinements,
+                        int coarsen_after_beam)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h, "null handle");
+    h->a->remesh([&] {
+      h->a->mesh().refine_mesh(time, next_refinement_time, n_time_steps, n_refinements, coarsen_after_beam != 0);
+    });
+  });
+}
+
+int adm_amr_execute(adm_amr *h, uint8_t const *refine, uint8_t const *coarsen)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h, "null handle");
+    auto r = level_flags(h->a->mesh(), refine);
+    auto c = level_flags(h->a->mesh(), coarsen);
+    h->a->remesh([&] { h->a->mesh().execute(r, c); });
+  });
+}
+
+int adm_amr_n_dofs(adm_amr const *h, int64_t *n_dofs, int64_t *n_nodes)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h, "null handle");
+    if (n_dofs)
+      *n_dofs = (int64_t)h->a->mesh().dof_key.size();
+    if (n_nodes)
+      *n_nodes = h->a->mesh().n_nodes_all;
+  });
+}
+
+int adm_amr_n_leaves(adm_amr const *h, int64_t *n)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && n, "null argument");
+    *n = n_leaves(h->a->mesh());
+  });
+}
+
+int adm_amr_leaves(adm_amr const *h, int32_t *lijk)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && lijk, "null argument");
+    leaves(h->a->mesh(), lijk);
+  });
+}
+
+int adm_amr_dof_lattice(adm_amr const *h, int64_t *xyz)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && xyz, "null argument");
+    dof_lattice(h->a->mesh(), xyz);
+  });
+}
+
+int adm_amr_solution(adm_amr *h, double **y)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && y, "null argument");
+    h->a->require_ready();
+    *y = h->a->solution();
+  });
+}
+
+int adm_amr_get_solution(adm_amr *h, double *dst)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && dst, "null argument");
+    h->a->copy_solution(dst, true);
+  });
+}
+
+int adm_amr_set_solution(adm_amr *h, double const *src)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && src, "null argument");
+    h->a->copy_solution(const_cast<double *>(src), false);
+  });
+}
+
+int adm_amr_set_time(adm_amr *h, double t)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h, "null handle");
+    h->a->require_ready();
+    h->a->set_time(t);
+  });
+}
+
+int adm_amr_vmult(adm_amr *h, double *dst, double const *src)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && dst && src, "null argument");
+    h->a->vmult(dst, src);
+  });
+}
+
+int adm_amr_inverse_mass(adm_amr *h, double *dst)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && dst, "null argument");
+    h->a->require_ready();
+    h->a->copy_inverse_mass(dst);
+  });
+}
+
+int adm_amr_evolve_one_time_step(adm_amr *h, double t, double dt, double *t_out)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h, "null handle");
+    double const tn = h->a->evolve_one_time_step(t, dt);
+    if (t_out)
+      *t_out = tn;
+  });
+}
+
+int adm_amr_level_values(adm_amr *h, int level, double *host)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && host, "null argument");
+    h->a->level_values(level, host);
+  });
+}
+
+int adm_amr_level_cell_state(adm_amr *h, int level, double *host)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && host, "null argument");
+    adm::Thermal *th = h->a->level(level);
+    ADM_REQUIRE(th, "no leaves on this level");
+    th->set_state_to_material_properties();
+    th->get_cell_state(host);
+  });
+}
+
+int adm_amr_level_layout(adm_amr *h, int level, int64_t nodes[3], int64_t *pitch)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && nodes && pitch, "null argument");
+    adm::Thermal *th = h->a->level(level);
+    ADM_REQUIRE(th, "no leaves on this level");
+    for (int d = 0; d < 3; ++d)
+      nodes[d] = th->mesh().nn[d];
+    *pitch = th->mesh().pitch;
+  });
+}
+
+int adm_amr_synchronize(adm_amr *h)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h, "null handle");
+    h->a->synchronize();
+  });
+}
+
+} // extern "C"

@@ -251,8 +251,10 @@ MaterialDesc make_material(adm_config const &cfg)
 }
 
 CellTopology build_topology(Mesh const &mesh, std::vector<uint8_t> const &active,
-                            std::vector<uint8_t> const &matid, bool need_slots)
+                            std::vector<uint8_t> const &matid, bool need_slots,
+                            std::vector<uint8_t> const *domain)
 {
+  std::vector<uint8_t> const &inside = domain ? *domain : active;
   CellTopology t;
   size_t const C = mesh.n_cells;
   t.cell_info.assign(C, 0u);
@@ -273,7 +275,7 @@ CellTopology build_topology(Mesh const &mesh, std::vector<uint8_t> const &active
           nb[d] += (f % 2) ? 1 : -1;
           if (nb[d] < 0 || nb[d] >= mesh.nc[d])
             info |= 1u << (CI_FACE_SHIFT + f);
-          else if (!active[mesh.cell_index(nb[0], nb[1], nb[2])])
+          else if (!inside[mesh.cell_index(nb[0], nb[1], nb[2])])
             info |= (1u << (CI_FACE_SHIFT + f)) | (1u << (CI_INTERFACE_SHIFT + f));
         }
         t.cell_info[c] = info;
@@ -522,6 +524,14 @@ void Thermal::set_cells(uint8_t const *active, uint8_t const *material_id,
   setup_done_ = false;
 }
 
+void Thermal::set_domain(uint8_t const *domain)
+{
+  domain_.clear();
+  if (domain)
+    domain_.assign(domain, domain + mesh_.n_cells);
+  setup_done_ = false;
+}
+
 void Thermal::rebuild()
 {
   size_t const C = mesh_.n_cells;
@@ -533,7 +543,7 @@ void Thermal::rebuild()
       break;
     }
   bool const need_slots = (ns_ == 3) && !adiabatic_only_;
-  topo_ = build_topology(mesh_, active_, matid_, need_slots);
+  topo_ = build_topology(mesh_, active_, matid_, need_slots, domain_.empty() ? nullptr : &domain_);
   ADM_CK(cudaMemcpyAsync(cell_info_d_.p, topo_.cell_info.data(), C * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_));
   ADM_CK(cudaMemcpyAsync(tile_nbr_d_.p, topo_.tile_nbr.data(), mesh_.n_tiles * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_));
   if (has_rotation_)

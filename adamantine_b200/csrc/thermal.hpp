@@ -138,8 +138,14 @@ struct CellTopology
   int n_slots = 0;
   bool all_tiles_active = true;
 };
+// domain (optional, one byte per cell): the cells whose region carries
+// material; a face of an active cell is a boundary face where the neighbour
+// is outside the domain. Without it the domain is the active set. A level
+// grid of a refined mesh passes the region of the whole material (its
+// active cells are only the leaves of that level).
 CellTopology build_topology(Mesh const &mesh, std::vector<uint8_t> const &active,
-                            std::vector<uint8_t> const &matid, bool need_slots);
+                            std::vector<uint8_t> const &matid, bool need_slots,
+                            std::vector<uint8_t> const *domain = nullptr);
 
 // Tensor map of n_members node vectors laid out member after member,
 // member_stride doubles apart (1 member: one vector), for the 4D TMA brick
@@ -191,6 +197,9 @@ public:
                  uint8_t const *initial_state, double const *cosv,
                  double const *sinv);
   void setup();
+  // Level grid of a refined mesh: the cells whose region carries material
+  // (faces towards them are interior); before setup().
+  void set_domain(uint8_t const *domain);
 
   // ---- ThermalOperatorBase
   size_t m() const { return mesh_.n_nodes; }
@@ -293,6 +302,7 @@ private:
   Tableau tab_;
 
   std::vector<uint8_t> active_, matid_, init_state_, has_melted_;
+  std::vector<uint8_t> domain_; // empty: the active cells
   std::vector<double> cos_, sin_;
   CellTopology topo_;
   std::vector<TileWork> work_;

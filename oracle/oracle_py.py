@@ -46,6 +46,7 @@ def lib():
         L.orc_n_qp.argtypes = [ctypes.c_void_p]
         L.orc_set_cells.argtypes = [ctypes.c_void_p, _U8, _U8, _U8, _D, _D]
         L.orc_setup.argtypes = [ctypes.c_void_p]
+        L.orc_set_domain.argtypes = [ctypes.c_void_p, _U8]
         L.orc_set_time.argtypes = [ctypes.c_void_p, ctypes.c_double]
         L.orc_vmult.argtypes = [ctypes.c_void_p, _D, _D]
         L.orc_vmult_add.argtypes = [ctypes.c_void_p, _D, _D]
@@ -84,7 +85,7 @@ class Oracle:
     """
 
     def __init__(self, config_struct, active=None, material_id=None, initial_state=None,
-                 deposition_cos=None, deposition_sin=None, n_states=None):
+                 deposition_cos=None, deposition_sin=None, n_states=None, domain=None):
         self._L = lib()
         self._cfg = config_struct
         self._h = self._L.orc_create(ctypes.addressof(config_struct))
@@ -101,6 +102,9 @@ class Oracle:
             None if deposition_sin is None else np.ascontiguousarray(deposition_sin, np.float64).reshape(C),
         ]
         self._L.orc_set_cells(self._h, _u8(arrs[0]), _u8(arrs[1]), _u8(arrs[2]), _dp(arrs[3]), _dp(arrs[4]))
+        if domain is not None:
+            self._keep_domain = np.ascontiguousarray(domain, np.uint8).reshape(C)
+            self._L.orc_set_domain(self._h, _u8(self._keep_domain))
         self._L.orc_setup(self._h)
 
     def __del__(self):

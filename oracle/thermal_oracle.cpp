@@ -197,6 +197,9 @@ struct orc_oracle
   std::vector<double> hq;                     // QGauss(deg+1) for averages
   std::vector<double> hqw, Sh;                // weights, values [nh][np]
   std::vector<uint8_t> active, matid, node_active, has_melted;
+  // cells whose region carries material (level grid of a refined mesh:
+  // the active cells are that level's leaves); empty: the active cells
+  std::vector<uint8_t> domain;
   std::vector<double> cosv, sinv;
   std::vector<double> state;                  // [n_states][C]
   // mutable like the reference's tables (ThermalOperator.hh:210-226):
@@ -514,7 +517,7 @@ struct orc_oracle
       return true;
     }
     *outer = false;
-    return !active[cell_index(nb)];
+    return domain.empty() ? !active[cell_index(nb)] : !domain[cell_index(nb)];
   }
 
   // cell_local_apply (ThermalOperator.templates.hh:479-617) plus
@@ -981,6 +984,13 @@ void orc_set_cells(orc_oracle *o, uint8_t const *active,
     for (int k = 0; k < ns; ++k)
       o->state[(size_t)k * o->ncells + c] = (k == s) ? 1.0 : 0.0;
   }
+}
+
+void orc_set_domain(orc_oracle *o, uint8_t const *domain)
+{
+  o->domain.clear();
+  if (domain)
+    o->domain.assign(domain, domain + o->ncells);
 }
 
 void orc_setup(orc_oracle *o)

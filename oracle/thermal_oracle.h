@@ -87,6 +87,11 @@ int32_t orc_n_qp(orc_oracle const *o);
 void orc_set_cells(orc_oracle *o, uint8_t const *active,
                    uint8_t const *material_id, uint8_t const *initial_state,
                    double const *deposition_cos, double const *deposition_sin);
+/* Cells whose region carries material (NULL: the active cells). A face of an
+ * active cell is a boundary face where the neighbour is outside it: a level
+ * grid of a refined mesh passes the whole material region, its active cells
+ * being only that level's leaves. Before orc_setup. */
+void orc_set_domain(orc_oracle *o, uint8_t const *domain);
 /* ThermalPhysics::setup(): inverse mass + get_state_from_material_properties */
 void orc_setup(orc_oracle *o);
 

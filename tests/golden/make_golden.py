@@ -23,6 +23,11 @@ Run in a container where the reference is mounted at /root/reference:
   (test_integration_3d.cc:112-115), copied as is; and
   integration_3d_scan_path.npy, the segments of demo_316_short_scan_path.txt
   as (end_time, power_modifier, x, y, z) rows.
+* amr_test_scan_path.npy -- the segments of bare_plate_L_scan_path_fast.txt,
+  the scan path of amr_test.info (test_integration_3d_amr.cc:19-58: 4 x 4 x 1
+  FE_Q(3) cells of 5 x 5 x 0.5 mm, one refinement along the beam every 200
+  steps, 250 forward Euler steps of 1 us; expected max 329.5 K, min 296.1 K),
+  as (end_time, power_modifier, x, y, z) rows.
 * integration_3d_gold_short.npz -- tests/data/integration_3d_gold_short.txt
   (229570 temperatures, 6 significant digits, stored as float32, exact to
   the printed digits) of demo_316_short.info (test_integration_3d.cc:117-120:
@@ -69,6 +74,10 @@ def main():
     assert short.size == 229570, short.size
     np.savez_compressed(os.path.join(HERE, "integration_3d_gold_short.npz"), values=short.astype(np.float32))
     print("wrote integration_3d_gold_short.npz", short.size)
+
+    np.save(os.path.join(HERE, "amr_test_scan_path.npy"),
+            segments(open(os.path.join(data, "bare_plate_L_scan_path_fast.txt")).read()))
+    print("wrote amr_test_scan_path.npy")
 
     for k in (1, 2):
         name = f"microstructure_G_R_gold_{k}.txt"

@@ -1,0 +1,125 @@
+"""Refined meshes on the GPU (through the C ABI) against the CPU
+restatement (oracle/amr_oracle.py) on the same meshes: the constrained
+operator and inverse mass, whole runs of the reference's amr_test.info
+driver loop at FE degree 2 (refinement before step 1 and every 200 steps),
+runs with coarsening after the beam (the solution and the cell states
+carried through refine_and_transfer), and the uniformly refined mesh, whose
+operator must be the uniform fine grid's bit for bit."""
+import numpy as np
+import pytest
+import torch
+
+import amr_oracle
+from amr_cases import AMR_MAX, AMR_MIN, amr_test_config, run_amr
+
+from adamantine_b200.amr import AmrThermalPhysics
+from adamantine_b200.thermal import ThermalPhysics
+
+pytestmark = pytest.mark.gpu
+
+
+def both(cfg, max_level, **kw):
+    g = AmrThermalPhysics(cfg, max_level, initial_state=cfg.geometry.initial_state(), **kw)
+    o = amr_oracle.AmrProblem(cfg, max_level, initial_state=cfg.geometry.initial_state(), **kw)
+    o.setup(300.0)
+    return g, o
+
+
+def field(pts, rng):
+    r2 = (pts[:, 0] - 2.0) ** 2 + (pts[:, 1] - 2.5) ** 2
+    return 320.0 + 1600.0 * np.exp(-r2 / 0.3) + rng.uniform(0.0, 3.0, len(pts))
+
+
+@pytest.mark.parametrize("degree", [1, 2])
+@pytest.mark.parametrize("boundary", ["adiabatic", "convective,radiative"])
+def test_constrained_operator_and_mass_match_oracle(degree, boundary):
+    cfg = amr_test_config(degree=degree, n_cells=(4, 4, 2), boundary=boundary)
+    g, o = both(cfg, 2)
+    g.refine_mesh(0.0, 200e-6, 200, 2)
+    o.refine_mesh(0.0, 200e-6, 200, 2)
+    assert g.n_dofs == o.n_dofs and len(o.hanging) > 0
+    assert (g.leaves() == np.array(o.forest.sorted_leaves())).all()
+    im = g.inverse_mass().cpu().numpy()
+    assert np.abs(im - o.inv_mass).max() <= 1e-13 * np.abs(o.inv_mass).max()
+    rng = np.random.default_rng(5)
+    y = field(o.dof_points(), rng)
+    dev = torch.device("cuda")
+    src = torch.tensor(y, device=dev)
+    dst = torch.zeros_like(src)
+    for t in (20e-6, 90e-6):
+        g.set_time(t)
+        o.set_time(t)
+        g.vmult(dst, src)
+        ref = o.vmult(y)
+        assert np.abs(dst.cpu().numpy() - ref).max() <= 1e-10 * np.abs(ref).max()
+
+
+def test_amr_test_run_matches_oracle_at_degree_2():
+    """amr_test.info's loop at FE degree 2 (the GPU path's degrees are 1-2;
+    the reference's FE_Q(3) pin is checked on the restatement)."""
+    cfg = amr_test_config(degree=2)
+    g, o = both(cfg, 1)
+    run_amr(g)
+    run_amr(o)
+    y = g.get_solution().cpu().numpy()
+    assert g.n_dofs == o.n_dofs
+    assert np.abs(y - o.y).max() <= 1e-9 * np.abs(o.y).max()
+    # the reference's bounds for FE_Q(3), with its 10 % tolerance
+    assert abs(y.max() - AMR_MAX) <= 0.1 * AMR_MAX and abs(y.min() - AMR_MIN) <= 0.1 * AMR_MIN
+
+
+@pytest.mark.parametrize("method", ["forward_euler", "rk_fourth_order"])
+def test_coarsening_after_the_beam_matches_oracle(method):
+    # a 40 kW beam melts the plate within the 120 us (the cell states then
+    # carry liquid fractions through every remeshing)
+    cfg = amr_test_config(degree=2, n_cells=(6, 6, 2), boundary="convective,radiative", method=method,
+                          max_power=40000.0)
+    g, o = both(cfg, 2)
+    run = lambda p: run_amr(p, dt=2e-6, duration=120e-6, every=20, n_refinements=2, coarsen=True)
+    run(g)
+    run(o)
+    assert (g.leaves() == np.array(o.forest.sorted_leaves())).all()
+    y = g.get_solution().cpu().numpy()
+    assert np.abs(y - o.y).max() <= 1e-9 * np.abs(o.y).max()
+    assert y.max() > 1708.0  # above the liquidus
+    liquid = 0.0
+    for l, lev in o.levels.items():
+        lev["oracle"].set_state_to_material_properties()
+        ns = g.config.material.n_states
+        ref = np.asarray(lev["oracle"].cell_state()).reshape(ns, -1)
+        act = np.zeros(ref.shape[1], bool)
+        n = lev["n"]
+        for c in lev["cells"]:
+            act[c[1] + n[0] * (c[2] + n[1] * c[3])] = True
+        mine = g.level_cell_state(l)
+        assert np.abs(mine[:, act] - ref[:, act]).max() <= 1e-9
+        liquid += ref[1, act].sum()
+    assert liquid > 0.0  # cells carried their molten state through the remeshing
+
+
+@pytest.mark.parametrize("degree", [1, 2])
+def test_uniform_refinement_is_the_fine_grid(degree):
+    cfg = amr_test_config(degree=degree, n_cells=(3, 2, 2))
+    g = AmrThermalPhysics(cfg, 1)
+    g.execute({tuple(c) for c in g.leaves()}, None)
+    assert (g.leaves()[:, 0] == 1).all()
+    fine_cfg = amr_test_config(degree=degree, n_cells=(6, 4, 4))
+    fine = ThermalPhysics(fine_cfg)
+    rng = np.random.default_rng(9)
+    lat = g.dof_lattice()  # the level-1 node grid: lattice / (2 / degree)
+    idx = lat * degree // 2
+    y = field(g.dof_points() / np.array([5e-3 / 3, 5e-3 / 2, 0.5e-3 / 2]), rng)
+    grid = np.zeros((fine.nodes[2], fine.nodes[1], fine.pitch))
+    grid[idx[:, 2], idx[:, 1], idx[:, 0]] = y
+    dev = torch.device("cuda")
+    src_f = torch.tensor(grid.reshape(-1), device=dev)
+    dst_f = torch.zeros_like(src_f)
+    src = torch.tensor(y, device=dev)
+    dst = torch.zeros_like(src)
+    for t in (10e-6, 80e-6):
+        g.set_time(t)
+        fine.set_time(t)
+        g.vmult(dst, src)
+        fine.vmult(dst_f, src_f)
+        ref = dst_f.cpu().numpy().reshape(grid.shape)[idx[:, 2], idx[:, 1], idx[:, 0]]
+        assert (dst.cpu().numpy() == ref).all()
