@@ -141,6 +141,7 @@ SIGNATURES = {
     "adm_amr_level_values": [_VP, ctypes.c_int32, _VP],
     "adm_amr_level_layout": [_VP, ctypes.c_int32, _VP, ctypes.POINTER(ctypes.c_int64)],
     "adm_amr_level_cell_state": [_VP, ctypes.c_int32, _VP],
+    "adm_amr_set_schedule": [_VP, ctypes.c_int32],
     "adm_amr_synchronize": [_VP],
     "adm_enkf_analysis": [_VP, ctypes.c_int32, _VP, ctypes.c_int64, ctypes.c_int64, _VP, ctypes.c_int32,
                           ctypes.c_int32, _VP, _VP, _VP, _VP, _VP, _VP],

@@ -237,5 +237,10 @@ class AmrThermalPhysics(_Common):
         self._call("level_cell_state", int(level), _p(out))
         return out.reshape(ns, -1)
 
+    def set_schedule(self, schedule: str):
+        """'atomic' (default: one launch per level and application) or
+        'coloured' (eight launches, a fixed order of additions)."""
+        self._call("set_schedule", {"coloured": 0, "atomic": 1}[schedule])
+
     def synchronize(self):
         self._call("synchronize")

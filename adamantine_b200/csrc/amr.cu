@@ -643,6 +643,14 @@ __global__ void restrict_kernel(int64_t n_dofs, int64_t const *ptr, int64_t cons
   out[d] = add ? out[d] + s : s;
 }
 
+// out[r] = lev[pos[r]]
+__global__ void gather_kernel(int64_t n, int64_t const *pos, double const *lev, double *out)
+{
+  int64_t const r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r < n)
+    out[r] = lev[pos[r]];
+}
+
 __global__ void invert_kernel(int64_t n, double *m)
 {
   int64_t const i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -700,12 +708,53 @@ unsigned blocks(int64_t n) { return (unsigned)std::max<int64_t>(1, (n + 255) / 2
 class Amr
 {
 public:
-  Amr(adm_config const &cfg, int max_level, int device, cudaStream_t stream) : device_(device), stream_(stream)
+  // All work runs on the handle's own stream, ordered after the caller's
+  // stream at every entry and before it at every exit (events), so a time
+  // step can be captured in a graph whatever stream the caller uses.
+  Amr(adm_config const &cfg, int max_level, int device, cudaStream_t stream) : device_(device), user_(stream)
   {
     mesh_.init(cfg, max_level);
     if (cfg.dim != 3)
       throw Error(ADM_ERR_UNSUPPORTED, "refined meshes are 3-D");
+    ADM_CK(cudaSetDevice(device_));
+    ADM_CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    ADM_CK(cudaEventCreateWithFlags(&ev_in_, cudaEventDisableTiming));
+    ADM_CK(cudaEventCreateWithFlags(&ev_out_, cudaEventDisableTiming));
   }
+
+  ~Amr()
+  {
+    cudaSetDevice(device_);
+    if (stream_)
+      cudaStreamSynchronize(stream_);
+    drop_graph();
+    levels_.clear();
+    if (ev_in_)
+      cudaEventDestroy(ev_in_);
+    if (ev_out_)
+      cudaEventDestroy(ev_out_);
+    if (stream_)
+      cudaStreamDestroy(stream_);
+  }
+
+  Amr(Amr const &) = delete;
+  Amr &operator=(Amr const &) = delete;
+
+  struct Ordered
+  {
+    Amr &a;
+    explicit Ordered(Amr &x) : a(x)
+    {
+      ADM_CK(cudaSetDevice(a.device_));
+      ADM_CK(cudaEventRecord(a.ev_in_, a.user_));
+      ADM_CK(cudaStreamWaitEvent(a.stream_, a.ev_in_, 0));
+    }
+    ~Ordered()
+    {
+      cudaEventRecord(a.ev_out_, a.stream_);
+      cudaStreamWaitEvent(a.user_, a.ev_out_, 0);
+    }
+  };
 
   AmrMesh &mesh() { return mesh_; }
   AmrMesh const &mesh() const { return mesh_; }
@@ -714,7 +763,7 @@ public:
 
   void setup(double initial_temperature)
   {
-    ADM_CK(cudaSetDevice(device_));
+    Ordered ord(*this);
     mesh_.build();
     build_levels(nullptr);
     y_.alloc(n_dofs());
@@ -734,35 +783,41 @@ public:
   template <class F> void remesh(F &&change)
   {
     require_ready();
-    ADM_CK(cudaSetDevice(device_));
-    // the old field on the level grids (constraints resolved) and the old
-    // cell states (ThermalPhysics::set_state_to_material_properties)
+    Ordered ord(*this);
+    // the old field at the level nodes of the old leaves (constraints
+    // resolved; only those nodes come back to the host) and the old cell
+    // states (ThermalPhysics::set_state_to_material_properties)
     prolong(y_.p);
-    std::vector<double> old_lev(lev_n_);
-    ADM_CK(cudaMemcpyAsync(old_lev.data(), src_lev_.p, lev_n_ * sizeof(double), cudaMemcpyDeviceToHost, stream_));
-    ADM_CK(cudaStreamSynchronize(stream_));
     Snapshot old;
     old.forest = mesh_.forest;
     old.off = lev_off_;
-    old.lev = std::move(old_lev);
+    if (n_rows_ > 0)
+    {
+      DevBuf<double> rv;
+      rv.alloc(n_rows_);
+      gather_kernel<<<blocks(n_rows_), 256, 0, stream_>>>(n_rows_, row_pos_.p, src_lev_.p, rv.p);
+      ADM_CK(cudaGetLastError());
+      std::vector<double> vals(n_rows_);
+      ADM_CK(cudaMemcpyAsync(vals.data(), rv.p, n_rows_ * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+      ADM_CK(cudaStreamSynchronize(stream_));
+      old.value.reserve(2 * n_rows_);
+      for (int64_t r = 0; r < n_rows_; ++r)
+        old.value[row_pos_h_[r]] = vals[r];
+    }
     int const ns = mesh_.cfg.n_states;
     old.states.resize(levels_.size());
+    old.pitch.assign(levels_.size(), 0);
+    old.nn1.assign(levels_.size(), 0);
     for (size_t l = 0; l < levels_.size(); ++l)
     {
-      if (!levels_[l])
+      if (!alive(l))
         continue;
       levels_[l]->set_state_to_material_properties();
       old.states[l].resize(levels_[l]->n_cells() * ns);
       levels_[l]->get_cell_state(old.states[l].data());
+      old.pitch[l] = levels_[l]->mesh().pitch;
+      old.nn1[l] = levels_[l]->mesh().nn[1];
     }
-    old.pitch.assign(levels_.size(), 0);
-    old.nn1.assign(levels_.size(), 0);
-    for (size_t l = 0; l < levels_.size(); ++l)
-      if (levels_[l])
-      {
-        old.pitch[l] = levels_[l]->mesh().pitch;
-        old.nn1[l] = levels_[l]->mesh().nn[1];
-      }
     change();
     mesh_.build();
     build_levels(&old);
@@ -776,21 +831,36 @@ public:
     compute_inverse_mass();
   }
 
-  void set_time(double t)
+  // Level-grid schedule (coloured: 8 launches per level and application,
+  // deterministic; atomic: 1 launch, additions in any order).
+  void set_schedule(int schedule)
   {
+    if (schedule != Thermal::kScheduleColoured && schedule != Thermal::kScheduleAtomic)
+      throw Error(ADM_ERR_INVALID, "unknown schedule");
+    schedule_ = schedule;
+    drop_graph();
     for (auto &th : levels_)
       if (th)
-        th->set_time(t);
+        th->set_schedule(schedule);
+  }
+
+  void set_time(double t)
+  {
+    require_ready();
+    Ordered ord(*this);
+    for (size_t l = 0; l < levels_.size(); ++l)
+      if (alive(l))
+        levels_[l]->set_time(t);
   }
 
   // dst = C^T (sum_l A_l) C src (composite vectors on the device)
   void vmult(double *dst, double const *src)
   {
     require_ready();
-    ADM_CK(cudaSetDevice(device_));
+    Ordered ord(*this);
     prolong(src);
     for (size_t l = 0; l < levels_.size(); ++l)
-      if (levels_[l])
+      if (alive(l))
         levels_[l]->vmult(dst_lev_.p + lev_off_[l], src_lev_.p + lev_off_[l], false);
     restrict_to(dst, 0);
   }
@@ -800,7 +870,7 @@ public:
   void copy_inverse_mass(double *dst)
   {
     require_ready();
-    ADM_CK(cudaSetDevice(device_));
+    Ordered ord(*this);
     ADM_CK(cudaMemcpyAsync(dst, inv_m_.p, n_dofs() * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
     ADM_CK(cudaStreamSynchronize(stream_));
   }
@@ -809,7 +879,7 @@ public:
   void copy_solution(double *other, bool out)
   {
     require_ready();
-    ADM_CK(cudaSetDevice(device_));
+    Ordered ord(*this);
     size_t const bytes = n_dofs() * sizeof(double);
     if (out)
       ADM_CK(cudaMemcpyAsync(other, y_.p, bytes, cudaMemcpyDeviceToDevice, stream_));
@@ -818,15 +888,93 @@ public:
     ADM_CK(cudaStreamSynchronize(stream_));
   }
 
+  // One explicit Runge-Kutta step of the solution: the level clocks are set
+  // to (t, dt), then the step's launches (stage inputs, prolongation, the
+  // levels' operators with the sources at t + c_i dt, restriction, inverse
+  // mass, update) replay as one graph, captured on the first step after a
+  // mesh change or with a new dt.
   double evolve_one_time_step(double t, double dt)
   {
     require_ready();
-    ADM_CK(cudaSetDevice(device_));
+    Ordered ord(*this);
     Thermal::Tableau const tab = Thermal::tableau(mesh_.cfg.time_method);
     int64_t const n = n_dofs();
+    double *const before = z_.p;
     for (int i = 0; i < tab.s; ++i)
       k_[i].alloc(n);
     z_.alloc(n);
+    if (z_.p != before)
+      drop_graph();
+    for (size_t l = 0; l < levels_.size(); ++l)
+      if (alive(l))
+        levels_[l]->set_step_clock(t, dt);
+    if (!step_exec_ || step_dt_ != dt)
+    {
+      drop_graph();
+      cudaGraph_t g = nullptr;
+      ADM_CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+      try
+      {
+        step_body(dt, tab);
+      }
+      catch (...)
+      {
+        cudaStreamEndCapture(stream_, &g);
+        if (g)
+          cudaGraphDestroy(g);
+        throw;
+      }
+      ADM_CK(cudaStreamEndCapture(stream_, &g));
+      cudaError_t const e = cudaGraphInstantiate(&step_exec_, g, 0);
+      cudaGraphDestroy(g);
+      ADM_CK(e);
+      step_dt_ = dt;
+    }
+    ADM_CK(cudaGraphLaunch(step_exec_, stream_));
+    return t + dt;
+  }
+
+  // the composite field on the level grid of level l (constraints resolved)
+  void level_values(int l, double *host)
+  {
+    require_ready();
+    Ordered ord(*this);
+    if (l < 0 || l >= (int)levels_.size() || !alive(l))
+      throw Error(ADM_ERR_INVALID, "no leaves on this level");
+    prolong(y_.p);
+    ADM_CK(cudaMemcpyAsync(host, src_lev_.p + lev_off_[l], levels_[l]->m() * sizeof(double),
+                           cudaMemcpyDeviceToHost, stream_));
+    ADM_CK(cudaStreamSynchronize(stream_));
+  }
+
+  Thermal *level(int l) { return (l >= 0 && l < (int)levels_.size() && alive(l)) ? levels_[l].get() : nullptr; }
+  bool alive(size_t l) const { return l < alive_.size() && alive_[l] && levels_[l]; }
+
+  void synchronize() { ADM_CK(cudaStreamSynchronize(stream_)); }
+
+private:
+  void drop_graph()
+  {
+    if (step_exec_)
+    {
+      cudaGraphExecDestroy(step_exec_);
+      step_exec_ = nullptr;
+    }
+  }
+
+  // k = C^T (sum_l A_l) C src with the sources at stage c of the clocked step
+  void vmult_stage(double *dst, double const *src, double c)
+  {
+    prolong(src);
+    for (size_t l = 0; l < levels_.size(); ++l)
+      if (alive(l))
+        levels_[l]->vmult_stage(dst_lev_.p + lev_off_[l], src_lev_.p + lev_off_[l], c);
+    restrict_to(dst, 0);
+  }
+
+  void step_body(double dt, Thermal::Tableau const &tab)
+  {
+    int64_t const n = n_dofs();
     for (int i = 0; i < tab.s; ++i)
     {
       double const *in = y_.p;
@@ -848,8 +996,7 @@ public:
         ADM_CK(cudaGetLastError());
         in = z_.p;
       }
-      set_time(t + tab.c[i] * dt);
-      vmult(k_[i].p, in);
+      vmult_stage(k_[i].p, in, tab.c[i]);
       scale_kernel<<<blocks(n), 256, 0, stream_>>>(n, inv_m_.p, k_[i].p);
       ADM_CK(cudaGetLastError());
     }
@@ -873,31 +1020,13 @@ public:
     stage_input_kernel<<<blocks(n), 256, 0, stream_>>>(n, y_.p, dt, nk, a[0], kk[0], a[1], kk[1], a[2], kk[2],
                                                         y_.p);
     ADM_CK(cudaGetLastError());
-    return t + dt;
   }
 
-  // the composite field on the level grid of level l (constraints resolved)
-  void level_values(int l, double *host)
-  {
-    require_ready();
-    if (l < 0 || l >= (int)levels_.size() || !levels_[l])
-      throw Error(ADM_ERR_INVALID, "no leaves on this level");
-    prolong(y_.p);
-    ADM_CK(cudaMemcpyAsync(host, src_lev_.p + lev_off_[l], levels_[l]->m() * sizeof(double),
-                           cudaMemcpyDeviceToHost, stream_));
-    ADM_CK(cudaStreamSynchronize(stream_));
-  }
-
-  Thermal *level(int l) { return (l >= 0 && l < (int)levels_.size()) ? levels_[l].get() : nullptr; }
-
-  void synchronize() { ADM_CK(cudaStreamSynchronize(stream_)); }
-
-private:
   struct Snapshot
   {
     Forest forest;
     std::vector<int64_t> off;
-    std::vector<double> lev;
+    std::unordered_map<int64_t, double> value; // level-buffer position -> old field
     std::vector<std::vector<double>> states;
     std::vector<int> pitch, nn1;
 
@@ -936,7 +1065,10 @@ private:
                     if (w == 0.0)
                       continue;
                     int64_t const nidx = (p * a + q0) + (int64_t)pitch[l] * ((p * b + q1) + (int64_t)nn1[l] * (p * c + q2));
-                    v += w * lev[off[l] + nidx];
+                    auto it = value.find(off[l] + nidx);
+                    if (it == value.end())
+                      throw Error(ADM_ERR_INVALID, "internal: old leaf node without a value");
+                    v += w * it->second;
                   }
               return v;
             }
@@ -977,22 +1109,29 @@ private:
 
   void build_levels(Snapshot const *old)
   {
+    drop_graph();
     int const L = mesh_.forest.max_level;
     int const ns = mesh_.cfg.n_states;
-    levels_.clear();
+    // level Thermals persist across remeshing (set up again on the new
+    // leaves); a level without leaves keeps its grid and is skipped
     levels_.resize(L + 1);
-    lev_off_.assign(L + 1, 0);
-    int64_t off = 0;
+    alive_.assign(L + 1, 0);
     for (int l = 0; l <= L; ++l)
     {
       if (mesh_.n_active_leaves(l) == 0)
         continue;
-      adm_config c = mesh_.cfg;
-      for (int d = 0; d < 3; ++d)
-        c.n_cells[d] = (int32_t)mesh_.forest.n(l, d);
-      for (int b = 0; b < c.n_sources; ++b)
-        c.sources[b].segments = mesh_.segments[b].empty() ? nullptr : mesh_.segments[b].data();
-      auto th = std::make_unique<Thermal>(c, device_, stream_);
+      alive_[l] = 1;
+      if (!levels_[l])
+      {
+        adm_config c = mesh_.cfg;
+        for (int d = 0; d < 3; ++d)
+          c.n_cells[d] = (int32_t)mesh_.forest.n(l, d);
+        for (int b = 0; b < c.n_sources; ++b)
+          c.sources[b].segments = mesh_.segments[b].empty() ? nullptr : mesh_.segments[b].data();
+        levels_[l] = std::make_unique<Thermal>(c, device_, stream_);
+        levels_[l]->set_schedule(schedule_);
+      }
+      Thermal *th = levels_[l].get();
       int64_t const C = mesh_.forest.cells(l);
       std::vector<uint8_t> act(C), dom(C), mat(C), init(C);
       for (int64_t k = 0; k < mesh_.forest.n(l, 2); ++k)
@@ -1027,10 +1166,15 @@ private:
         th->set_cell_state(st.data());
         th->get_state_from_material_properties();
       }
-      lev_off_[l] = off;
-      off += (int64_t)((th->m() + 31) / 32 * 32);
-      levels_[l] = std::move(th);
     }
+    lev_off_.assign(L + 1, 0);
+    int64_t off = 0;
+    for (int l = 0; l <= L; ++l)
+      if (levels_[l])
+      {
+        lev_off_[l] = off;
+        off += (int64_t)((levels_[l]->m() + 31) / 32 * 32);
+      }
     lev_n_ = off;
     src_lev_.alloc(std::max<int64_t>(1, lev_n_));
     dst_lev_.alloc(std::max<int64_t>(1, lev_n_));
@@ -1044,7 +1188,7 @@ private:
     for (int l = 0; l <= L; ++l)
     {
       row_lev_[l] = (int64_t)row_pos.size();
-      if (!levels_[l])
+      if (!alive(l))
         continue;
       Mesh const &lm = levels_[l]->mesh();
       std::vector<int64_t> nodes;
@@ -1096,6 +1240,7 @@ private:
         tw[at] = ent_w[e];
       }
     upload(row_pos_, row_pos);
+    row_pos_h_ = row_pos;
     upload(row_ptr_, row_ptr);
     upload(ent_dof_, ent_dof);
     upload(ent_w_, ent_w);
@@ -1136,7 +1281,7 @@ private:
     inv_m_.alloc(std::max<int64_t>(1, n_dofs()));
     for (size_t l = 0; l < levels_.size(); ++l)
     {
-      if (!levels_[l])
+      if (!alive(l))
         continue;
       levels_[l]->compute_inverse_mass_matrix();
       int64_t const r0 = row_lev_[l], r1 = row_lev_[l + 1];
@@ -1153,10 +1298,16 @@ private:
   }
 
   int device_ = 0;
-  cudaStream_t stream_ = nullptr;
+  cudaStream_t user_ = nullptr, stream_ = nullptr;
+  cudaEvent_t ev_in_ = nullptr, ev_out_ = nullptr;
+  cudaGraphExec_t step_exec_ = nullptr;
+  double step_dt_ = 0.0;
   bool ready_ = false;
   AmrMesh mesh_;
   std::vector<std::unique_ptr<Thermal>> levels_;
+  std::vector<uint8_t> alive_;
+  std::vector<int64_t> row_pos_h_;
+  int schedule_ = Thermal::kScheduleAtomic;
   std::vector<int64_t> lev_off_, row_lev_;
   int64_t lev_n_ = 0, n_rows_ = 0;
   DevBuf<double> src_lev_, dst_lev_;
@@ -1535,6 +1686,14 @@ int adm_amr_level_layout(adm_amr *h, int level, int64_t nodes[3], int64_t *pitch
     for (int d = 0; d < 3; ++d)
       nodes[d] = th->mesh().nn[d];
     *pitch = th->mesh().pitch;
+  });
+}
+
+int adm_amr_set_schedule(adm_amr *h, int schedule)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h, "null handle");
+    h->a->set_schedule(schedule);
   });
 }
 

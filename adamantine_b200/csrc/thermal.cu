@@ -931,6 +931,27 @@ void Thermal::vmult(double *dst, double const *src, bool add)
   launch_pass(a, src);
 }
 
+void Thermal::set_step_clock(double t, double dt)
+{
+  ADM_CK(cudaSetDevice(device_));
+  op_time_ = t;
+  set_clock(t, dt);
+}
+
+void Thermal::vmult_stage(double *dst, double const *src, double c)
+{
+  if (!setup_done_)
+    throw Error(ADM_ERR_INVALID, "setup() has not been called");
+  if (!topo_.all_tiles_active || schedule_ == kScheduleAtomic)
+    ADM_CK(cudaMemsetAsync(dst, 0, mesh_.n_nodes * sizeof(double), stream_));
+  prepare_stage(c);
+  KernelArgs a = base_args();
+  a.mode = 0;
+  a.vsrc = src;
+  a.vdst = dst;
+  launch_pass(a, src);
+}
+
 // Kernel arguments of RK stage i: stage input y (i == 0) or the stage vector
 // the previous stage wrote; za/zb alternate as stage outputs.
 KernelArgs Thermal::stage_args(int i) const

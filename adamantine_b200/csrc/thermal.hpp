@@ -208,6 +208,12 @@ public:
   Mesh const &mesh() const { return mesh_; }
   void set_time(double t);
   void vmult(double *dst, double const *src, bool add);
+  // A time step driven from outside (refined meshes): set_step_clock(t, dt)
+  // once, then vmult_stage(dst, src, c) evaluates dst = A src with the heat
+  // sources at t + c dt (computed on the device, so the launches can be
+  // captured in a graph and replayed with another clock).
+  void set_step_clock(double t, double dt);
+  void vmult_stage(double *dst, double const *src, double c);
   void compute_inverse_mass_matrix();
   double const *inverse_mass_matrix() const { return inv_mass_.p; }
   void get_state_from_material_properties();

@@ -252,3 +252,23 @@ def deposition_q2(n_cells=(256, 256, 128), extent=(40e-3, 40e-3, 20e-3), initial
                         time_method="rk_fourth_order")
     boxes = deposition_boxes(cfg, 50e-6, 50e-6, 100e-6, 0.0)
     return cfg, boxes
+
+
+def amr_q2(n_cells=(64, 64, 8), extent=(16e-3, 16e-3, 2e-3), max_level=2, speed=1.0, power=400.0,
+           name="amr_q2"):
+    """Refined-mesh workload: 64x64x8 coarse Q2 cells (Gauss 3) over
+    16x16x2 mm (0.25 mm cells), the phase-change material (solid),
+    adiabatic, Goldak 400 W / 0.3 (diameter
+    0.25 mm, depth 0.2 mm) along a line across the top surface at 1 m/s; the
+    beam's surroundings refined max_level = 2 times (62.5 um cells, the
+    resolution of the uniform 256x256x32 grid); RK4. Returns the
+    configuration and max_level."""
+    geo = Geometry(dim=3, n_cells=n_cells, extent=extent)
+    bnd = Boundary.from_database({"type": "adiabatic"}, 3)
+    seg = line_segments(2e-3, 14e-3, 8e-3 + rng_for(name).uniform(-0.1e-3, 0.1e-3), extent[2], speed)
+    src = Source(type="goldak", depth=0.2e-3, absorption_efficiency=0.3, diameter=0.25e-3, max_power=power,
+                 segments=seg)
+    mat = phase_change_material()
+    cfg = ThermalConfig(geometry=geo, material=mat, boundary=bnd, sources=[src], degree=2,
+                        time_method="rk_fourth_order")
+    return cfg, max_level

@@ -471,6 +471,79 @@ def run_deposition(args, local_rank, with_cpu):
     return out
 
 
+AMR_WORKLOAD = "amr_q2_64x64x8_2levels_rk4"
+
+
+def run_amr(args, local_rank):
+    """RK4 steps (dt = 1 us) of the refined-mesh workload after refine_mesh
+    over a 100-step window (2 levels along the beam), against the same steps
+    on the uniform grid of the finest resolution (256x256x32 Q2, CUDA-graph
+    steps); also one moving-window refine_mesh with coarsening after the
+    beam (refine_and_transfer: host mesh rebuild, level grids, transfer)."""
+    import copy
+
+    import torch
+
+    from adamantine_b200.amr import AmrThermalPhysics
+    from adamantine_b200.thermal import ThermalPhysics
+    from adamantine_b200.workloads import amr_q2
+
+    cfg, L = amr_q2()
+    dt, K = 1e-6, 100
+    g = AmrThermalPhysics(cfg, L, device=local_rank)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g.refine_mesh(0.0, K * dt, K, L)
+    torch.cuda.synchronize()
+    first_remesh_ms = 1e3 * (time.perf_counter() - t0)
+    leaves = g.leaves()
+    per_level = [int((leaves[:, 0] == l).sum()) for l in range(L + 1)]
+    t = 0.0
+    for _ in range(3):
+        t = g.evolve_one_time_step(t, dt)
+    torch.cuda.synchronize()
+    steps = args.amr_steps
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(g.stream)
+    for _ in range(steps):
+        t = g.evolve_one_time_step(t, dt)
+    ev1.record(g.stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    y = g.get_solution().cpu().numpy()
+    n_dofs, n_nodes = g.n_dofs, g.n_nodes
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g.refine_mesh(t, t + K * dt, K, L, True)
+    torch.cuda.synchronize()
+    remesh_ms = 1e3 * (time.perf_counter() - t0)
+    g.close()
+    # the uniform grid of the finest cells
+    fine_cfg = copy.deepcopy(cfg)
+    fine_cfg.geometry.n_cells = tuple(n << L for n in cfg.geometry.n_cells)
+    f = ThermalPhysics(fine_cfg, device=local_rank)
+    yf = f.from_grid(np.full(tuple(reversed(fine_cfg.geometry.node_shape(2))), 300.0))
+    tf = f.evolve_n_steps(0.0, dt, 3, yf)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(f.stream)
+    f.evolve_n_steps(tf, dt, steps, yf)
+    e1.record(f.stream)
+    e1.synchronize()
+    ms_fine = e0.elapsed_time(e1)
+    fine_nodes = int(np.prod(fine_cfg.geometry.node_shape(2)))
+    return {
+        "workload": AMR_WORKLOAD, "max_level": L, "leaves_per_level": per_level, "dofs": n_dofs,
+        "hanging_nodes": n_nodes - n_dofs, "steps": steps, "dt": dt, "ms_per_step": ms / steps,
+        "mdofs_per_s": 4 * n_dofs * steps / (ms * 1e-3) / 1e6, "peak_temperature": float(y.max()),
+        "first_refine_mesh_ms": first_remesh_ms, "refine_mesh_ms": remesh_ms,
+        "uniform_fine": {"nodes": fine_nodes, "ms_per_step": ms_fine / steps, "path": "evolve_n_steps (graphs)"},
+        "speedup_vs_uniform_fine": ms_fine / ms,
+    }
+
+
 def run_reference(args, rank, world):
     """--impl reference: the oracle's vmult on all host cores (rank 0 only)."""
     if rank != 0:
@@ -617,6 +690,8 @@ def run_ours(args, rank, world, local_rank):
         line["adjoint"] = run_adjoint(args, local_rank)
     if args.deposition_steps > 0:
         line["deposition"] = run_deposition(args, local_rank, rank == 0 and not args.no_cpu_baseline)
+    if args.amr_steps > 0:
+        line["amr"] = run_amr(args, local_rank)
     if rank == 0 and not args.no_cpu_baseline:
         rate, med, n = cpu_vmult_rate(build_workload(args.size)[0], T, os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": rate, "unit": "GDoF/s", "cores": os.cpu_count() or 1, "kind": "port",
@@ -641,6 +716,8 @@ def main():
     ap.add_argument("--deposition-steps", type=int, default=400,
                     help="RK4 steps of the deposition workload (0: skip; the configuration runs 2000)")
     ap.add_argument("--size", default="full", choices=sorted(SIZES))
+    ap.add_argument("--amr-steps", type=int, default=50,
+                    help="RK4 steps of the refined-mesh workload (0: skip it)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

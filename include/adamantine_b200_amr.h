@@ -118,6 +118,10 @@ int adm_amr_level_layout(adm_amr *h, int level, int64_t nodes[3], int64_t *pitch
  * set_state_to_material_properties, then the n_states x n_cells ratios,
  * state-major; cells that are not leaves of the level hold 0). */
 int adm_amr_level_cell_state(adm_amr *h, int level, double *host);
+/* Launch schedule of the level grids (adm_set_schedule's values): the
+ * atomic schedule (default) launches once per level and application, the
+ * coloured one eight times and adds in a fixed order (bit-reproducible). */
+int adm_amr_set_schedule(adm_amr *h, int schedule);
 int adm_amr_synchronize(adm_amr *h);
 
 #ifdef __cplusplus

@@ -52,6 +52,11 @@ def test_constrained_operator_and_mass_match_oracle(degree, boundary):
         g.vmult(dst, src)
         ref = o.vmult(y)
         assert np.abs(dst.cpu().numpy() - ref).max() <= 1e-10 * np.abs(ref).max()
+        g.set_schedule("coloured")
+        dst_c = torch.zeros_like(src)
+        g.vmult(dst_c, src)
+        g.set_schedule("atomic")
+        assert torch.abs(dst_c - dst).max().item() <= 1e-12 * np.abs(ref).max()
 
 
 def test_amr_test_run_matches_oracle_at_degree_2():
@@ -101,6 +106,7 @@ def test_coarsening_after_the_beam_matches_oracle(method):
 def test_uniform_refinement_is_the_fine_grid(degree):
     cfg = amr_test_config(degree=degree, n_cells=(3, 2, 2))
     g = AmrThermalPhysics(cfg, 1)
+    g.set_schedule("coloured")  # the uniform grid's default: the same additions in the same order
     g.execute({tuple(c) for c in g.leaves()}, None)
     assert (g.leaves()[:, 0] == 1).all()
     fine_cfg = amr_test_config(degree=degree, n_cells=(6, 4, 4))
