@@ -244,3 +244,30 @@ class AmrThermalPhysics(_Common):
 
     def synchronize(self):
         self._call("synchronize")
+
+
+def _main(argv=None):
+    """python -m adamantine_b200.amr [--steps N]: the refined-mesh workload
+    (workloads.amr_q2: refine_mesh over a 100-step window, then N RK4
+    steps); prints the mesh and the peak temperature."""
+    import argparse
+
+    from .workloads import amr_q2
+
+    ap = argparse.ArgumentParser(description=_main.__doc__)
+    ap.add_argument("--steps", type=int, default=8)
+    args = ap.parse_args(argv)
+    cfg, L = amr_q2()
+    g = AmrThermalPhysics(cfg, L)
+    dt, K = 1e-6, 100
+    g.refine_mesh(0.0, K * dt, K, L)
+    t = 0.0
+    for _ in range(args.steps):
+        t = g.evolve_one_time_step(t, dt)
+    lv = g.leaves()
+    print({"leaves_per_level": [int((lv[:, 0] == l).sum()) for l in range(L + 1)], "dofs": g.n_dofs,
+           "t": t, "peak_temperature": float(g.get_solution().max().item())})
+
+
+if __name__ == "__main__":
+    _main()
