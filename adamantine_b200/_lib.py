@@ -143,6 +143,14 @@ SIGNATURES = {
     "adm_amr_level_cell_state": [_VP, ctypes.c_int32, _VP],
     "adm_amr_set_schedule": [_VP, ctypes.c_int32],
     "adm_amr_synchronize": [_VP],
+    "adm_mechanics_create": [_VP, _VP, ctypes.POINTER(_VP)],
+    "adm_mechanics_destroy": [_VP],
+    "adm_mechanics_setup": [_VP, _VP],
+    "adm_mechanics_vmult": [_VP, _VP, _VP],
+    "adm_mechanics_rhs": [_VP, _VP],
+    "adm_mechanics_solve": [_VP, _VP, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double)],
+    "adm_mechanics_n_dofs": [_VP, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)],
+    "adm_mechanics_node_mask": [_VP, _VP],
     "adm_enkf_analysis": [_VP, ctypes.c_int32, _VP, ctypes.c_int64, ctypes.c_int64, _VP, ctypes.c_int32,
                           ctypes.c_int32, _VP, _VP, _VP, _VP, _VP, _VP],
 }

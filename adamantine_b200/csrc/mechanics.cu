@@ -1,0 +1,672 @@
+/* Thermoelastic displacement on the thermal mesh: the isotropic elasticity
+ * operator of MechanicalOperator::assemble_matrix
+ * (source/MechanicalOperator.cc:183-280), its right-hand side
+ * (assemble_rhs, :283-486: thermal expansion and gravity), the cell
+ * selection of MechanicalPhysics::setup_dofs (source/MechanicalPhysics.cc
+ * :280-440: thermally active cells with a solid ratio above 0.99) and the
+ * CG solve of MechanicalPhysics::solve (:488-520), matrix-free on the GPU.
+ *
+ * Layout: the thermal handle's node layout (pitch, z-slabs); a displacement
+ * vector is three node vectors (x, y, z components). Work: one warp per
+ * cell that carries displacement; the reference-element tables (values and
+ * gradients of the (p+1)^3 nodal functions at the (p+1)^3 Gauss points)
+ * sit in constant memory; each lane gathers one node's three components,
+ * then evaluates one quadrature point's stress, then integrates one node's
+ * three test functions and adds them into the result (FP64 atomics: a node
+ * is shared by up to 8 cells). Clamped displacements are eliminated: their
+ * columns are dropped and their rows are the identity.
+ */
+#include "capi_common.hpp"
+#include "thermal.hpp"
+#include "../../include/adamantine_b200_mechanics.h"
+
+#include <algorithm>
+#include <cmath>
+#include <memory>
+#include <vector>
+
+namespace adm
+{
+namespace
+{
+constexpr int kMaxN = 27; // nodes (and quadrature points) of a Q2 cell
+constexpr double kGravity = 9.80665; // GravityForce::g (source/BodyForce.hh:53)
+
+__constant__ double c_val[kMaxN * kMaxN];     // [q][n] phi_n(x_q)
+__constant__ double c_grad[kMaxN * kMaxN * 3]; // [q][n][d] d phi_n / d xi_d (x_q)
+__constant__ double c_wq[kMaxN];              // reference weights of the Gauss points
+
+struct MechArgs
+{
+  int p, N; // degree, nodes (= quadrature points) per cell
+  int nc[3], nn[3], pitch;
+  int64_t m; // node vector length (component stride)
+  double inv_h[3], jxw; // 1 / h and the cell volume (x the reference weight)
+  int32_t const *cells; // cells that carry displacement
+  int n_cells;
+  uint8_t const *node_mask; // 0 none, 1 free, 2 clamped
+  uint8_t const *matid;
+  double lambda[4], mu[4], alpha[4], rho[4], tref[4];
+  double tinit;
+  int thermoelastic, gravity;
+  uint8_t const *melted;
+};
+
+__device__ __forceinline__ int64_t node_of(MechArgs const &a, int cx, int cy, int cz, int n)
+{
+  int const np = a.p + 1;
+  int const i = n % np, j = (n / np) % np, k = n / (np * np);
+  return (int64_t)(a.p * cx + i) + (int64_t)a.pitch * ((a.p * cy + j) + (int64_t)a.nn[1] * (a.p * cz + k));
+}
+
+// dst += A src on the free rows; 4 warps per block, one cell per warp.
+__global__ void __launch_bounds__(128) elastic_apply_kernel(MechArgs a, double const *src, double *dst)
+{
+  __shared__ double u[4][3][kMaxN];
+  __shared__ double S[4][kMaxN][9];
+  int const w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int const gw = blockIdx.x * 4 + w, nw = gridDim.x * 4;
+  for (int ci = gw; ci < a.n_cells; ci += nw)
+  {
+    int const c = a.cells[ci];
+    int const cx = c % a.nc[0], cy = (c / a.nc[0]) % a.nc[1], cz = c / (a.nc[0] * a.nc[1]);
+    int const mat = a.matid[c];
+    double const lam = a.lambda[mat], mu = a.mu[mat];
+    int64_t g = 0;
+    bool freen = false;
+    if (lane < a.N)
+    {
+      g = node_of(a, cx, cy, cz, lane);
+      freen = a.node_mask[g] == 1;
+      for (int comp = 0; comp < 3; ++comp)
+        u[w][comp][lane] = freen ? src[comp * a.m + g] : 0.0;
+    }
+    __syncwarp();
+    if (lane < a.N)
+    {
+      int const q = lane;
+      double G[3][3];
+#pragma unroll
+      for (int comp = 0; comp < 3; ++comp)
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+        {
+          double s = 0.0;
+          for (int n = 0; n < a.N; ++n)
+            s = fma(u[w][comp][n], c_grad[(q * kMaxN + n) * 3 + d], s);
+          G[comp][d] = s * a.inv_h[d];
+        }
+      double const div = G[0][0] + G[1][1] + G[2][2];
+      double const jw = a.jxw * c_wq[q];
+#pragma unroll
+      for (int comp = 0; comp < 3; ++comp)
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+          S[w][q][comp * 3 + d] = jw * ((comp == d ? lam * div : 0.0) + mu * (G[comp][d] + G[d][comp]));
+    }
+    __syncwarp();
+    if (lane < a.N && freen)
+    {
+      int const n = lane;
+      for (int comp = 0; comp < 3; ++comp)
+      {
+        double r = 0.0;
+        for (int q = 0; q < a.N; ++q)
+          for (int d = 0; d < 3; ++d)
+            r = fma(S[w][q][comp * 3 + d], c_grad[(q * kMaxN + n) * 3 + d] * a.inv_h[d], r);
+        atomicAdd(dst + comp * a.m + g, r);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// rhs += sum_q JxW ((3 lambda + 2 mu) alpha (T - T_ref) div v + f . v)
+__global__ void __launch_bounds__(128) elastic_rhs_kernel(MechArgs a, double const *T, double *rhs)
+{
+  __shared__ double Tn[4][kMaxN];
+  __shared__ double B[4][kMaxN], F[4][kMaxN];
+  int const w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int const gw = blockIdx.x * 4 + w, nw = gridDim.x * 4;
+  for (int ci = gw; ci < a.n_cells; ci += nw)
+  {
+    int const c = a.cells[ci];
+    int const cx = c % a.nc[0], cy = (c / a.nc[0]) % a.nc[1], cz = c / (a.nc[0] * a.nc[1]);
+    int const mat = a.matid[c];
+    double const lam = a.lambda[mat], mu = a.mu[mat];
+    double const tref = (a.melted && a.melted[c]) ? a.tref[mat] : a.tinit;
+    int64_t g = 0;
+    if (lane < a.N)
+    {
+      g = node_of(a, cx, cy, cz, lane);
+      Tn[w][lane] = T ? T[g] : 0.0;
+    }
+    __syncwarp();
+    if (lane < a.N)
+    {
+      int const q = lane;
+      double const jw = a.jxw * c_wq[q];
+      double b = 0.0;
+      if (a.thermoelastic)
+      {
+        double dT = -tref;
+        for (int n = 0; n < a.N; ++n)
+          dT = fma(c_val[q * kMaxN + n], Tn[w][n], dT);
+        b = (3.0 * lam + 2.0 * mu) * a.alpha[mat] * dT;
+      }
+      B[w][q] = jw * b;
+      F[w][q] = a.gravity ? jw * (-a.rho[mat] * kGravity) : 0.0;
+    }
+    __syncwarp();
+    if (lane < a.N && a.node_mask[g] == 1)
+    {
+      int const n = lane;
+      for (int comp = 0; comp < 3; ++comp)
+      {
+        double r = 0.0;
+        for (int q = 0; q < a.N; ++q)
+        {
+          r = fma(B[w][q], c_grad[(q * kMaxN + n) * 3 + comp] * a.inv_h[comp], r);
+          if (comp == 2)
+            r = fma(F[w][q], c_val[q * kMaxN + n], r);
+        }
+        atomicAdd(rhs + comp * a.m + g, r);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// diag += the operator's diagonal on the free rows
+__global__ void __launch_bounds__(128) elastic_diag_kernel(MechArgs a, double *diag)
+{
+  int const w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int const gw = blockIdx.x * 4 + w, nw = gridDim.x * 4;
+  for (int ci = gw; ci < a.n_cells; ci += nw)
+  {
+    int const c = a.cells[ci];
+    int const cx = c % a.nc[0], cy = (c / a.nc[0]) % a.nc[1], cz = c / (a.nc[0] * a.nc[1]);
+    int const mat = a.matid[c];
+    double const lam = a.lambda[mat], mu = a.mu[mat];
+    if (lane >= a.N)
+      continue;
+    int64_t const g = node_of(a, cx, cy, cz, lane);
+    if (a.node_mask[g] != 1)
+      continue;
+    int const n = lane;
+    for (int comp = 0; comp < 3; ++comp)
+    {
+      double r = 0.0;
+      for (int q = 0; q < a.N; ++q)
+      {
+        double gg = 0.0, gc = 0.0;
+        for (int d = 0; d < 3; ++d)
+        {
+          double const gd = c_grad[(q * kMaxN + n) * 3 + d] * a.inv_h[d];
+          gg += gd * gd;
+          if (d == comp)
+            gc = gd;
+        }
+        r += a.jxw * c_wq[q] * ((lam + mu) * gc * gc + mu * gg);
+      }
+      atomicAdd(diag + comp * a.m + g, r);
+    }
+  }
+}
+
+// constrained rows: dst = src; rows without displacement: 0
+__global__ void identity_rows_kernel(int64_t m, uint8_t const *mask, double const *src, double *dst)
+{
+  int64_t const i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= 3 * m)
+    return;
+  uint8_t const k = mask[i % m];
+  if (k == 2)
+    dst[i] = src[i];
+  else if (k == 0)
+    dst[i] = 0.0;
+}
+
+// ---- CG vector kernels (3 m entries)
+__global__ void dot_kernel(int64_t n, double const *x, double const *y, double *out)
+{
+  __shared__ double red[256];
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    s = fma(x[i], y[i], s);
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1)
+  {
+    if (threadIdx.x < o)
+      red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    atomicAdd(out, red[0]);
+}
+
+// z = r / diag (diag 0: z = r)
+__global__ void jacobi_kernel(int64_t n, double const *r, double const *diag, double *z)
+{
+  int64_t const i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n)
+    z[i] = diag[i] != 0.0 ? r[i] / diag[i] : r[i];
+}
+
+// x += alpha p, r -= alpha q  (alpha = s[0] / s[1])
+__global__ void cg_update_kernel(int64_t n, double const *s, double const *p, double const *q, double *x, double *r)
+{
+  int64_t const i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  double const alpha = s[0] / s[1];
+  x[i] = fma(alpha, p[i], x[i]);
+  r[i] = fma(-alpha, q[i], r[i]);
+}
+
+// p = z + beta p (beta = s_new / s_old)
+__global__ void cg_direction_kernel(int64_t n, double const *s_new, double const *s_old, double const *z, double *p)
+{
+  int64_t const i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  p[i] = fma(s_new[0] / s_old[0], p[i], z[i]);
+}
+
+unsigned blocks_for(int64_t n) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16)); }
+
+// 1-D Gauss points / weights on [0, 1] and the Lagrange basis on the
+// equidistant (Gauss-Lobatto for p <= 2) nodes
+void gauss_1d(int n, double *x, double *w)
+{
+  if (n == 2)
+  {
+    double const s = 0.5 / std::sqrt(3.0);
+    x[0] = 0.5 - s;
+    x[1] = 0.5 + s;
+    w[0] = w[1] = 0.5;
+  }
+  else
+  {
+    double const s = 0.5 * std::sqrt(0.6);
+    x[0] = 0.5 - s;
+    x[1] = 0.5;
+    x[2] = 0.5 + s;
+    w[0] = w[2] = 5.0 / 18.0;
+    w[1] = 8.0 / 18.0;
+  }
+}
+
+double lag(int p, int a, double u)
+{
+  double v = 1.0;
+  for (int b = 0; b <= p; ++b)
+    if (b != a)
+      v *= (u * p - b) / (double)(a - b);
+  return v;
+}
+
+double lag_d(int p, int a, double u)
+{
+  double s = 0.0;
+  for (int k = 0; k <= p; ++k)
+  {
+    if (k == a)
+      continue;
+    double v = p / (double)(a - k);
+    for (int b = 0; b <= p; ++b)
+      if (b != a && b != k)
+        v *= (u * p - b) / (double)(a - b);
+    s += v;
+  }
+  return s;
+}
+} // namespace
+
+class Mechanics
+{
+public:
+  Mechanics(Thermal &th, adm_mech_config const &cfg) : th_(th), cfg_(cfg)
+  {
+    Mesh const &M = th_.mesh_;
+    if (M.deg != 1 && M.deg != 2)
+      throw Error(ADM_ERR_UNSUPPORTED, "mechanics takes FE degree 1 or 2");
+    if (cfg_.clamped_faces < 0 || cfg_.clamped_faces > 63)
+      throw Error(ADM_ERR_INVALID, "clamped_faces is a 6-bit mask");
+    for (int k = 0; k < th_.cfg_.n_materials; ++k)
+      if (!(cfg_.lame_second[k] > 0.0) || !(cfg_.lame_first[k] > -2.0 / 3.0 * cfg_.lame_second[k]))
+        throw Error(ADM_ERR_INVALID, "Lame parameters must give a positive definite elasticity tensor");
+    p_ = M.deg;
+    N_ = (p_ + 1) * (p_ + 1) * (p_ + 1);
+    // reference-element tables
+    int const np = p_ + 1;
+    double x[3], w[3];
+    gauss_1d(np, x, w);
+    std::vector<double> val(kMaxN * kMaxN, 0.0), grad(kMaxN * kMaxN * 3, 0.0), wq(kMaxN, 0.0);
+    for (int q = 0; q < N_; ++q)
+    {
+      int const qi = q % np, qj = (q / np) % np, qk = q / (np * np);
+      wq[q] = w[qi] * w[qj] * w[qk];
+      for (int n = 0; n < N_; ++n)
+      {
+        int const ni = n % np, nj = (n / np) % np, nk = n / (np * np);
+        double const vx = lag(p_, ni, x[qi]), vy = lag(p_, nj, x[qj]), vz = lag(p_, nk, x[qk]);
+        val[q * kMaxN + n] = vx * vy * vz;
+        grad[(q * kMaxN + n) * 3 + 0] = lag_d(p_, ni, x[qi]) * vy * vz;
+        grad[(q * kMaxN + n) * 3 + 1] = vx * lag_d(p_, nj, x[qj]) * vz;
+        grad[(q * kMaxN + n) * 3 + 2] = vx * vy * lag_d(p_, nk, x[qk]);
+      }
+    }
+    ADM_CK(cudaSetDevice(th_.device_));
+    ADM_CK(cudaMemcpyToSymbol(c_val, val.data(), val.size() * sizeof(double)));
+    ADM_CK(cudaMemcpyToSymbol(c_grad, grad.data(), grad.size() * sizeof(double)));
+    ADM_CK(cudaMemcpyToSymbol(c_wq, wq.data(), wq.size() * sizeof(double)));
+  }
+
+  void setup(double const *temperature)
+  {
+    Thermal &t = th_;
+    Mesh const &M = t.mesh_;
+    if (!t.setup_done_)
+      throw Error(ADM_ERR_INVALID, "the thermal handle is not set up");
+    ADM_CK(cudaSetDevice(t.device_));
+    size_t const C = M.n_cells;
+    int const ns = t.ns_;
+    // cell states (MaterialProperty state after set_state_to_material_properties)
+    t.set_state_to_material_properties();
+    std::vector<double> st((size_t)ns * C);
+    t.get_cell_state(st.data());
+    std::vector<int32_t> cells;
+    for (size_t c = 0; c < C; ++c)
+      if (t.active_[c] && st[c] > 0.99) // state 0: solid
+        cells.push_back((int32_t)c);
+    n_cells_ = (int64_t)cells.size();
+    // nodes of those cells; clamped: on a clamped box face
+    m_ = (int64_t)M.n_nodes;
+    std::vector<uint8_t> mask(m_, 0);
+    int const np = p_ + 1;
+    for (int32_t c : cells)
+    {
+      int const cx = c % M.nc[0], cy = (c / M.nc[0]) % M.nc[1], cz = c / (M.nc[0] * M.nc[1]);
+      for (int n = 0; n < N_; ++n)
+      {
+        int const i = p_ * cx + n % np, j = p_ * cy + (n / np) % np, k = p_ * cz + n / (np * np);
+        int const ijk[3] = {i, j, k};
+        bool clamped = false;
+        for (int f = 0; f < 6; ++f)
+          if ((cfg_.clamped_faces >> f) & 1)
+          {
+            int const d = f / 2;
+            if (ijk[d] == ((f & 1) ? M.nn[d] - 1 : 0))
+              clamped = true;
+          }
+        uint8_t &mk = mask[i + (int64_t)M.pitch * (j + (int64_t)M.nn[1] * k)];
+        mk = clamped ? 2 : std::max<uint8_t>(mk, 1);
+      }
+    }
+    n_dofs_ = 0;
+    for (uint8_t v : mask)
+      n_dofs_ += v ? 3 : 0;
+    mask_h_ = mask;
+    cells_.alloc(std::max<size_t>(1, cells.size()));
+    mask_.alloc(m_);
+    matid_.alloc(C);
+    melted_.alloc(C);
+    cudaStream_t const s = t.stream_;
+    if (!cells.empty())
+      ADM_CK(cudaMemcpyAsync(cells_.p, cells.data(), cells.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    ADM_CK(cudaMemcpyAsync(mask_.p, mask.data(), m_, cudaMemcpyHostToDevice, s));
+    ADM_CK(cudaMemcpyAsync(matid_.p, t.matid_.data(), C, cudaMemcpyHostToDevice, s));
+    ADM_CK(cudaMemcpyAsync(melted_.p, t.has_melted_.data(), C, cudaMemcpyHostToDevice, s));
+    // right-hand side and Jacobi diagonal
+    rhs_.alloc(3 * m_);
+    diag_.alloc(3 * m_);
+    ADM_CK(cudaMemsetAsync(rhs_.p, 0, 3 * m_ * sizeof(double), s));
+    ADM_CK(cudaMemsetAsync(diag_.p, 0, 3 * m_ * sizeof(double), s));
+    MechArgs const a = args();
+    unsigned const nb = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n_cells_ + 3) / 4, 148 * 16));
+    if (n_cells_ > 0)
+    {
+      if (cfg_.thermoelastic && !temperature)
+        throw Error(ADM_ERR_INVALID, "a thermoelastic setup needs the temperature");
+      elastic_rhs_kernel<<<nb, 128, 0, s>>>(a, cfg_.thermoelastic ? temperature : nullptr, rhs_.p);
+      elastic_diag_kernel<<<nb, 128, 0, s>>>(a, diag_.p);
+      ADM_CK(cudaGetLastError());
+    }
+    ADM_CK(cudaStreamSynchronize(s));
+    ready_ = true;
+  }
+
+  void vmult(double *dst, double const *src)
+  {
+    require();
+    cudaStream_t const s = th_.stream_;
+    ADM_CK(cudaSetDevice(th_.device_));
+    ADM_CK(cudaMemsetAsync(dst, 0, 3 * m_ * sizeof(double), s));
+    apply_free(dst, src);
+    identity_rows_kernel<<<(unsigned)((3 * m_ + 255) / 256), 256, 0, s>>>(m_, mask_.p, src, dst);
+    ADM_CK(cudaGetLastError());
+  }
+
+  void copy_rhs(double *dst)
+  {
+    require();
+    ADM_CK(cudaMemcpyAsync(dst, rhs_.p, 3 * m_ * sizeof(double), cudaMemcpyDeviceToDevice, th_.stream_));
+    ADM_CK(cudaStreamSynchronize(th_.stream_));
+  }
+
+  // Jacobi-preconditioned CG from x = 0 (the constrained and absent entries
+  // stay 0): stops at |r| <= rel_tol |rhs| (SolverControl of
+  // MechanicalPhysics::solve) or after max_iter iterations (an error).
+  void solve(double *x, int32_t *iterations, double *residual)
+  {
+    require();
+    cudaStream_t const s = th_.stream_;
+    ADM_CK(cudaSetDevice(th_.device_));
+    int64_t const n = 3 * m_;
+    r_.alloc(n);
+    z_.alloc(n);
+    pv_.alloc(n);
+    qv_.alloc(n);
+    sc_.alloc(8);
+    ADM_CK(cudaMemsetAsync(x, 0, n * sizeof(double), s));
+    ADM_CK(cudaMemcpyAsync(r_.p, rhs_.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    double const rhs_norm = std::sqrt(dot(rhs_.p, rhs_.p, 0));
+    double const tol = (cfg_.rel_tol > 0.0 ? cfg_.rel_tol : 1e-12) * rhs_norm;
+    int const max_iter = cfg_.max_iter > 0 ? cfg_.max_iter : (int)std::max<int64_t>(1, n_dofs_);
+    double res = rhs_norm;
+    int it = 0;
+    if (res > tol)
+    {
+      precondition(r_.p, z_.p);
+      ADM_CK(cudaMemcpyAsync(pv_.p, z_.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      dot(r_.p, z_.p, 0); // sc[0] = r.z
+      for (it = 1; it <= max_iter; ++it)
+      {
+        vmult(qv_.p, pv_.p);
+        dot(pv_.p, qv_.p, 1); // sc[1] = p.q
+        cg_update_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, sc_.p, pv_.p, qv_.p, x, r_.p);
+        ADM_CK(cudaGetLastError());
+        res = std::sqrt(dot(r_.p, r_.p, 2));
+        if (res <= tol)
+          break;
+        precondition(r_.p, z_.p);
+        dot(r_.p, z_.p, 3); // sc[3] = new r.z
+        cg_direction_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, sc_.p + 3, sc_.p, z_.p, pv_.p);
+        ADM_CK(cudaGetLastError());
+        ADM_CK(cudaMemcpyAsync(sc_.p, sc_.p + 3, sizeof(double), cudaMemcpyDeviceToDevice, s));
+      }
+      if (it > max_iter)
+        throw Error(ADM_ERR_DEVICE, "the mechanical CG did not converge within max_iter iterations");
+    }
+    if (iterations)
+      *iterations = it;
+    if (residual)
+      *residual = res;
+  }
+
+  int64_t n_dofs() const { return n_dofs_; }
+  int64_t n_cells() const { return n_cells_; }
+  std::vector<uint8_t> const &mask() const { return mask_h_; }
+
+private:
+  void require() const
+  {
+    if (!ready_)
+      throw Error(ADM_ERR_INVALID, "adm_mechanics_setup has not been called");
+  }
+
+  MechArgs args() const
+  {
+    Thermal const &t = th_;
+    Mesh const &M = t.mesh_;
+    MechArgs a{};
+    a.p = p_;
+    a.N = N_;
+    for (int d = 0; d < 3; ++d)
+    {
+      a.nc[d] = M.nc[d];
+      a.nn[d] = M.nn[d];
+      a.inv_h[d] = 1.0 / M.h[d];
+    }
+    a.pitch = M.pitch;
+    a.m = m_;
+    a.jxw = M.h[0] * M.h[1] * M.h[2];
+    a.cells = cells_.p;
+    a.n_cells = (int)n_cells_;
+    a.node_mask = mask_.p;
+    a.matid = matid_.p;
+    for (int k = 0; k < 4; ++k)
+    {
+      a.lambda[k] = cfg_.lame_first[k];
+      a.mu[k] = cfg_.lame_second[k];
+      a.alpha[k] = cfg_.thermal_expansion[k];
+      a.rho[k] = cfg_.density[k];
+      a.tref[k] = cfg_.reference_temperature[k];
+    }
+    a.tinit = cfg_.initial_temperature;
+    a.thermoelastic = cfg_.thermoelastic;
+    a.gravity = cfg_.gravity;
+    a.melted = melted_.p;
+    return a;
+  }
+
+  void apply_free(double *dst, double const *src)
+  {
+    if (n_cells_ == 0)
+      return;
+    unsigned const nb = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n_cells_ + 3) / 4, 148 * 16));
+    elastic_apply_kernel<<<nb, 128, 0, th_.stream_>>>(args(), src, dst);
+    ADM_CK(cudaGetLastError());
+  }
+
+  void precondition(double const *r, double *z)
+  {
+    int64_t const n = 3 * m_;
+    jacobi_kernel<<<(unsigned)((n + 255) / 256), 256, 0, th_.stream_>>>(n, r, diag_.p, z);
+    ADM_CK(cudaGetLastError());
+  }
+
+  // sc[slot] = x . y (device), also returned to the host
+  double dot(double const *x, double const *y, int slot)
+  {
+    cudaStream_t const s = th_.stream_;
+    int64_t const n = 3 * m_;
+    ADM_CK(cudaMemsetAsync(sc_.p + slot, 0, sizeof(double), s));
+    dot_kernel<<<blocks_for(n), 256, 0, s>>>(n, x, y, sc_.p + slot);
+    ADM_CK(cudaGetLastError());
+    double v = 0.0;
+    ADM_CK(cudaMemcpyAsync(&v, sc_.p + slot, sizeof(double), cudaMemcpyDeviceToHost, s));
+    ADM_CK(cudaStreamSynchronize(s));
+    return v;
+  }
+
+  Thermal &th_;
+  adm_mech_config cfg_;
+  int p_ = 1, N_ = 8;
+  bool ready_ = false;
+  int64_t m_ = 0, n_cells_ = 0, n_dofs_ = 0;
+  std::vector<uint8_t> mask_h_;
+  DevBuf<int32_t> cells_;
+  DevBuf<uint8_t> mask_, matid_, melted_;
+  DevBuf<double> rhs_, diag_, r_, z_, pv_, qv_, sc_;
+};
+
+} // namespace adm
+
+struct adm_mechanics
+{
+  std::unique_ptr<adm::Mechanics> m;
+};
+
+extern "C" {
+
+int adm_mechanics_create(adm_thermal *thermal, adm_mech_config const *cfg, adm_mechanics **out)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(thermal && cfg && out, "null argument");
+    auto h = std::make_unique<adm_mechanics>();
+    h->m = std::make_unique<adm::Mechanics>(*reinterpret_cast<adm::Thermal *>(thermal), *cfg);
+    *out = h.release();
+  });
+}
+
+int adm_mechanics_destroy(adm_mechanics *h)
+{
+  delete h;
+  return ADM_OK;
+}
+
+int adm_mechanics_setup(adm_mechanics *h, double const *temperature)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h, "null handle");
+    h->m->setup(temperature);
+  });
+}
+
+int adm_mechanics_vmult(adm_mechanics *h, double *dst, double const *src)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && dst && src, "null argument");
+    h->m->vmult(dst, src);
+  });
+}
+
+int adm_mechanics_rhs(adm_mechanics *h, double *dst)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && dst, "null argument");
+    h->m->copy_rhs(dst);
+  });
+}
+
+int adm_mechanics_solve(adm_mechanics *h, double *displacement, int32_t *iterations, double *residual)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && displacement, "null argument");
+    h->m->solve(displacement, iterations, residual);
+  });
+}
+
+int adm_mechanics_n_dofs(adm_mechanics const *h, int64_t *n_dofs, int64_t *n_cells)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h, "null handle");
+    if (n_dofs)
+      *n_dofs = h->m->n_dofs();
+    if (n_cells)
+      *n_cells = h->m->n_cells();
+  });
+}
+
+int adm_mechanics_node_mask(adm_mechanics const *h, uint8_t *mask)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && mask, "null argument");
+    std::copy(h->m->mask().begin(), h->m->mask().end(), mask);
+  });
+}
+
+} // extern "C"

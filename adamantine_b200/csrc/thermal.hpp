@@ -282,6 +282,7 @@ private:
   friend class Adjoint;
   friend struct Checkpoint;
   friend class Microstructure;
+  friend class Mechanics;
   void rebuild();
   void upload_member();
   KernelArgs base_args() const;

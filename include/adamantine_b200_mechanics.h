@@ -1,0 +1,92 @@
+/*
+ * adamantine_b200 -- thermoelastic displacement on the thermal mesh (C ABI).
+ *
+ * The mechanical solve the driver runs after the thermal step
+ * (application/adamantine.hh:1289-1345): MechanicalPhysics::setup_dofs
+ * (source/MechanicalPhysics.cc:280-440) picks the cells that carry
+ * displacement (thermally active, solid ratio above 0.99), MechanicalOperator
+ * (source/MechanicalOperator.cc:183-486) forms the isotropic elasticity
+ * operator
+ *   a(u, v) = sum_q JxW (lambda div u div v + mu grad u : grad v^T
+ *                        + mu grad u : grad v)
+ * (FE_Q(p)^3, QGauss(p + 1)) and the right-hand side
+ *   sum_q JxW ((3 lambda + 2 mu) alpha (T - T_ref) div v + f . v),
+ * T the thermal field interpolated at the quadrature points, T_ref the
+ * material's reference temperature where the cell has melted and the
+ * initial temperature elsewhere, f = (0, 0, -rho_s g) with g = 9.80665
+ * (GravityForce, source/BodyForce.cc:18-31); MechanicalPhysics::solve
+ * (:488-520) runs CG to 1e-12 |rhs|. Displacements on clamped boundary
+ * faces are zero (Dirichlet, eliminated: the constrained rows of the
+ * operator are the identity).
+ *
+ * The handle is bound to a thermal handle (same mesh, degree and node
+ * layout): displacement vectors are 3 node vectors (x, y, z components)
+ * of adm_n_nodes doubles each, consecutive; entries of nodes that carry no
+ * displacement are 0. The elastic solve only: the reference's J2
+ * plasticity after the solve (:520-634) is not built.
+ */
+#ifndef ADAMANTINE_B200_MECHANICS_H
+#define ADAMANTINE_B200_MECHANICS_H
+
+#include "adamantine_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct adm_mech_config
+{
+  /* per material (the thermal configuration's materials), the solid
+   * state's mechanical properties (MaterialProperty mechanical_properties):
+   * lame_first_parameter, lame_second_parameter, thermal_expansion_coef,
+   * density (solid) */
+  double lame_first[4];
+  double lame_second[4];
+  double thermal_expansion[4];
+  double density[4];
+  /* reference temperature per material (cells that have melted) and the
+   * initial temperature (the others); thermoelastic: 1, elastostatic: 0
+   * (no thermal term) */
+  double reference_temperature[4];
+  double initial_temperature;
+  int32_t thermoelastic;
+  /* 1: gravity (GravityForce) in the right-hand side */
+  int32_t gravity;
+  /* bit f: box face f (x-, x+, y-, y+, z-, z+) is clamped */
+  int32_t clamped_faces;
+  /* CG: relative tolerance (0: 1e-12) and iteration limit (0: the number
+   * of displacement DoFs) */
+  double rel_tol;
+  int32_t max_iter;
+  int32_t pad0;
+} adm_mech_config;
+
+typedef struct adm_mechanics adm_mechanics;
+
+/* Bound to a set-up thermal handle, which must outlive it. */
+int adm_mechanics_create(adm_thermal *thermal, adm_mech_config const *cfg, adm_mechanics **out);
+int adm_mechanics_destroy(adm_mechanics *h);
+/* MechanicalPhysics::setup_dofs + update_rhs: the cells that carry
+ * displacement from the thermal handle's activity and cell states
+ * (ThermalPhysics::set_state_to_material_properties is called) and the
+ * right-hand side from the temperature (device node vector of the thermal
+ * handle) and the thermal handle's has_melted flags. */
+int adm_mechanics_setup(adm_mechanics *h, double const *temperature);
+/* dst = A src (device displacement vectors, 3 x adm_n_nodes doubles). */
+int adm_mechanics_vmult(adm_mechanics *h, double *dst, double const *src);
+/* The right-hand side of the last setup (device, 3 x adm_n_nodes). */
+int adm_mechanics_rhs(adm_mechanics *h, double *dst);
+/* MechanicalPhysics::solve (elastic): displacement (device, 3 x
+ * adm_n_nodes), CG iterations and final residual norm. */
+int adm_mechanics_solve(adm_mechanics *h, double *displacement, int32_t *iterations, double *residual);
+/* Counts: displacement DoFs (3 per node of a cell that carries
+ * displacement, clamped ones included) and cells that carry displacement. */
+int adm_mechanics_n_dofs(adm_mechanics const *h, int64_t *n_dofs, int64_t *n_cells);
+/* Per node (adm_n_nodes bytes): 0 no displacement, 1 free, 2 clamped. */
+int adm_mechanics_node_mask(adm_mechanics const *h, uint8_t *mask);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

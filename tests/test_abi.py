@@ -33,7 +33,8 @@ def test_library_exports_every_declared_symbol():
 def test_python_binding_covers_header():
     names = set(header_functions()) | set(header_functions("adamantine_b200_ensemble.h")) | \
         set(header_functions("adamantine_b200_adjoint.h")) | set(header_functions("adamantine_b200_deposition.h")) | \
-        set(header_functions("adamantine_b200_microstructure.h")) | set(header_functions("adamantine_b200_amr.h"))
+        set(header_functions("adamantine_b200_microstructure.h")) | set(header_functions("adamantine_b200_amr.h")) | \
+        set(header_functions("adamantine_b200_mechanics.h"))
     assert names - {"adm_last_error"} == set(_lib.SIGNATURES)
 
 

@@ -1,0 +1,113 @@
+"""Thermoelastic displacement on the GPU (through the C ABI) against the dense
+restatement (oracle/mechanics_oracle.py): the elasticity operator of the
+reference's own operator test (3 x 3 x 3 FE_Q(2)^3 cells of a 6 m cube,
+lambda = 2, mu = 3, boundary id 0 clamped: tests/test_mechanical_operator.cc
+:49-256) on free rows and the identity on clamped rows; the thermoelastic
+right-hand side from a GPU temperature field with melted and liquid cells
+(the liquid ones carry no displacement, melted ones expand from the
+material's reference temperature); and the CG displacement against the
+dense solve."""
+import numpy as np
+import pytest
+import torch
+
+from amr_cases import amr_test_config
+from mechanics_oracle import Elasticity, cells_with_displacement
+
+from adamantine_b200.config import Boundary, Geometry, ThermalConfig
+from adamantine_b200.mechanics import MechanicalPhysics
+from adamantine_b200.thermal import ThermalPhysics
+
+pytestmark = pytest.mark.gpu
+
+
+def plain(phys, v):
+    """(3 m) device displacement -> (3 n_nodes) plain-grid numpy vector."""
+    nx, ny, nz = phys.nodes
+    a = v.detach().cpu().numpy().reshape(3, nz, ny, phys.pitch)[:, :, :, :nx]
+    return np.ascontiguousarray(a).reshape(-1)
+
+
+def padded(phys, u):
+    nx, ny, nz = phys.nodes
+    full = np.zeros((3, nz, ny, phys.pitch))
+    full[:, :, :, :nx] = np.asarray(u).reshape(3, nz, ny, nx)
+    return torch.tensor(full.reshape(-1), device=phys.device)
+
+
+def reference_cube(degree):
+    cfg = amr_test_config(degree=degree, n_cells=(3, 3, 3), n_states=1)
+    cfg.geometry = Geometry(dim=3, n_cells=(3, 3, 3), extent=(6.0, 6.0, 6.0))
+    cfg.sources = []
+    return cfg
+
+
+@pytest.mark.parametrize("degree", [1, 2])
+def test_elastostatic_operator_matches_textbook_assembly(degree):
+    cfg = reference_cube(degree)
+    phys = ThermalPhysics(cfg)
+    mech = MechanicalPhysics(phys, 2.0, 3.0, density=1.0, thermoelastic=False, gravity=True, clamped=("x-",))
+    mech.setup_dofs()
+    C = 27
+    e = Elasticity((3, 3, 3), (6.0, 6.0, 6.0), degree, range(C), np.zeros(C, int), [2.0] * 4, [3.0] * 4,
+                   density=[1.0] * 4, clamped_faces=1)
+    assert (mech.node_mask() .reshape(phys.nodes[2], phys.nodes[1], phys.pitch)[:, :, :phys.nodes[0]]
+            .reshape(-1) == e.mask).all()
+    assert mech.n_dofs == 3 * e.n_nodes and mech.n_cells == C
+    K = e.matrix()
+    fr = e.free()
+    cl = np.concatenate([c * e.n_nodes + np.nonzero(e.mask == 2)[0] for c in range(3)])
+    rng = np.random.default_rng(4)
+    for _ in range(3):
+        x = rng.normal(size=3 * e.n_nodes)
+        dst = mech.new_vector()
+        mech.vmult(dst, padded(phys, x))
+        y = plain(phys, dst)
+        xf = np.zeros_like(x)
+        xf[fr] = x[fr]
+        ref = K @ xf
+        assert np.abs(y[fr] - ref[fr]).max() <= 1e-12 * np.abs(ref[fr]).max()
+        assert (y[cl] == x[cl]).all()
+    f = plain(phys, mech.rhs())
+    fo = e.rhs(thermoelastic=False, gravity=True)
+    fo[cl] = 0.0
+    assert np.abs(f - fo).max() <= 1e-12 * np.abs(fo).max()
+    u = mech.solve()
+    uo = e.solve(K, e.rhs(thermoelastic=False, gravity=True))
+    assert np.abs(plain(phys, u) - uo).max() <= 1e-8 * np.abs(uo).max()
+    assert mech.residual <= 1e-12 * np.linalg.norm(fo) * 1.0001
+
+
+def test_thermoelastic_after_a_melting_beam():
+    cfg = amr_test_config(degree=2, n_cells=(6, 6, 2), boundary="adiabatic", max_power=40000.0)
+    phys = ThermalPhysics(cfg)
+    T = phys.from_grid(np.full(tuple(reversed(cfg.geometry.node_shape(2))), 300.0))
+    t = 0.0
+    for _ in range(40):
+        t = phys.evolve_one_time_step(t, 2e-6, T)
+    # flag the cells heated along the path (the flag compares the cell
+    # average, far below the peak on these 0.8 mm cells), so that solid
+    # cells expand from the material's reference temperature
+    melted = phys.mark_has_melted(320.0, T)
+    phys.set_state_to_material_properties()
+    st = phys.get_cell_state()
+    active = cfg.geometry.active_cells()
+    cells = cells_with_displacement(active, st[0])
+    assert 0 < len(cells) < phys.n_cells  # liquid cells are left out
+    assert melted[cells].any() and not melted[cells].all()
+    lam, mu, alpha, rho = 1.1e11, 7.9e10, 1.6e-5, 7904.0
+    mech = MechanicalPhysics(phys, lam, mu, alpha, rho, reference_temperatures=[1673.0], initial_temperature=300.0,
+                             clamped=("z-",))
+    mech.setup_dofs(T)
+    e = Elasticity(cfg.geometry.n_cells, cfg.geometry.extent, 2, cells, np.zeros(phys.n_cells, int), [lam] * 4,
+                   [mu] * 4, [alpha] * 4, [rho] * 4, clamped_faces=1 << 4)
+    Tg = phys.to_grid(T).reshape(-1)
+    f = e.rhs(T=Tg, melted=melted, reference_temperatures=[1673.0] * 4, initial_temperature=300.0)
+    fr = e.free()
+    fg = plain(phys, mech.rhs())
+    assert np.abs(fg[fr] - f[fr]).max() <= 1e-11 * np.abs(f[fr]).max()
+    K = e.matrix()
+    u = mech.solve()
+    uo = e.solve(K, f)
+    assert np.abs(plain(phys, u) - uo).max() <= 1e-7 * np.abs(uo).max()
+    assert mech.iterations > 0 and np.abs(uo).max() > 0.0

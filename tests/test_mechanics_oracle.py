@@ -1,0 +1,90 @@
+"""The thermoelastic restatement (oracle/mechanics_oracle.py) checked for
+what the elasticity operator must satisfy: symmetry, rigid-body modes in the
+kernel of the unconstrained matrix, the patch test (a uniform strain field
+leaves only boundary rows nonzero), and the exact thermal-expansion solution:
+for a uniform temperature rise the field u = alpha dT (x - x0) satisfies
+K u = rhs in every row (sigma = (3 lambda + 2 mu) alpha dT I), which ties the
+operator and the right-hand side together; gravity's total force is
+-rho g V."""
+import numpy as np
+import pytest
+
+from mechanics_oracle import Elasticity, cells_with_displacement
+
+
+def box(degree, nc=(3, 2, 2), extent=(6.0, 4.0, 3.0), clamped=0, lam=2.0, mu=3.0, alpha=1e-5, rho=7.9e3):
+    C = int(np.prod(nc))
+    return Elasticity(nc, extent, degree, range(C), np.zeros(C, int), [lam] * 4, [mu] * 4, [alpha] * 4,
+                      [rho] * 4, clamped)
+
+
+def coords(e):
+    g = np.arange(e.n_nodes)
+    i, j, k = e.node_ijk(g)
+    return np.stack([i * e.h[0] / e.p, j * e.h[1] / e.p, k * e.h[2] / e.p], axis=1)
+
+
+@pytest.mark.parametrize("degree", [1, 2])
+def test_symmetric_with_rigid_body_kernel(degree):
+    e = box(degree)
+    K = e.matrix()
+    assert np.abs(K - K.T).max() <= 1e-12 * np.abs(K).max()
+    x = coords(e)
+    n = e.n_nodes
+    modes = []
+    for c in range(3):
+        t = np.zeros(3 * n)
+        t[c * n:(c + 1) * n] = 1.0
+        modes.append(t)
+    for a, b in ((0, 1), (1, 2), (0, 2)):  # rotation in the (a, b) plane
+        r = np.zeros(3 * n)
+        r[a * n:(a + 1) * n] = -x[:, b]
+        r[b * n:(b + 1) * n] = x[:, a]
+        modes.append(r)
+    for m in modes:
+        assert np.abs(K @ m).max() <= 1e-11 * np.abs(K).max() * np.abs(m).max()
+
+
+@pytest.mark.parametrize("degree", [1, 2])
+def test_patch_test_interior_rows_vanish(degree):
+    e = box(degree, nc=(3, 3, 3), extent=(3.0, 3.0, 3.0))
+    x = coords(e)
+    n = e.n_nodes
+    E = np.array([[1.0, 0.3, -0.2], [0.1, -0.5, 0.4], [0.2, 0.0, 0.7]])
+    u = (x @ E.T).T.reshape(-1)  # u_c = sum_d E[c, d] x_d
+    r = e.matrix() @ u
+    i, j, k = e.node_ijk(np.arange(n))
+    interior = (i > 0) & (j > 0) & (k > 0) & (i < e.nn[0] - 1) & (j < e.nn[1] - 1) & (k < e.nn[2] - 1)
+    for c in range(3):
+        assert np.abs(r[c * n:(c + 1) * n][interior]).max() <= 1e-11 * np.abs(r).max()
+
+
+@pytest.mark.parametrize("degree", [1, 2])
+def test_uniform_heating_gives_free_thermal_expansion(degree):
+    e = box(degree, alpha=1.2e-5)
+    x = coords(e)
+    dT, T0 = 150.0, 300.0
+    u = (1.2e-5 * dT * x).T.reshape(-1)
+    K = e.matrix()
+    f = e.rhs(T=np.full(e.n_nodes, T0 + dT), initial_temperature=T0, gravity=False)
+    assert np.abs(K @ u - f).max() <= 1e-10 * np.abs(f).max()
+
+
+def test_gravity_total_force_and_melted_reference():
+    e = box(2, rho=8000.0)
+    f = e.rhs(T=None, thermoelastic=False, gravity=True)
+    n = e.n_nodes
+    assert abs(f[2 * n:].sum() + 8000.0 * 9.80665 * 6.0 * 4.0 * 3.0) <= 1e-9 * 8000 * 9.81 * 72
+    assert np.abs(f[:2 * n]).max() == 0.0
+    # melted cells expand from the material's reference temperature
+    melted = np.zeros(12, np.uint8)
+    melted[:6] = 1
+    T = np.full(n, 500.0)
+    a = e.rhs(T=T, melted=melted, reference_temperatures=[500.0] * 4, initial_temperature=300.0, gravity=False)
+    b = Elasticity(e.nc, (6.0, 4.0, 3.0), 2, range(6, 12), np.zeros(12, int), [2.0] * 4, [3.0] * 4,
+                   [1e-5] * 4).rhs(T=T, initial_temperature=300.0, gravity=False)
+    assert np.allclose(a, b, rtol=0, atol=1e-12 * np.abs(b).max())
+
+
+def test_cell_selection():
+    assert cells_with_displacement([1, 1, 0, 1], [1.0, 0.5, 1.0, 0.995]) == [0, 3]
