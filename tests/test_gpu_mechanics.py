@@ -157,3 +157,23 @@ def test_eshelby_inclusion_matches_reference_values():
                 assert abs(v[i]) <= 0.16 * abs(ref[0] if ref[0] else 1e-9)
             else:
                 assert abs(v[i] - ref[i]) <= 0.16 * abs(ref[i]), (p, i, v[i], ref[i])
+
+
+def test_elastostatic_physics_case():
+    """The reference's MechanicalPhysics elastostatic case
+    (test_mechanical_physics.cc:196-264): 6 x 3 x 3 FE_Q(1)^3 cells over
+    12 x 6 x 6 m, density 1, lambda = 2, mu = 3, boundary 4 (z-) clamped,
+    gravity; its check is against a textbook CG solve with 2e-9 absolute
+    tolerance, here against the dense solve of the restatement."""
+    cfg = amr_test_config(degree=1, n_cells=(6, 3, 3), n_states=1)
+    cfg.geometry = Geometry(dim=3, n_cells=(6, 3, 3), extent=(12.0, 6.0, 6.0))
+    cfg.sources = []
+    phys = ThermalPhysics(cfg)
+    mech = MechanicalPhysics(phys, 2.0, 3.0, density=1.0, thermoelastic=False, gravity=True, clamped=("z-",))
+    mech.setup_dofs()
+    e = Elasticity((6, 3, 3), (12.0, 6.0, 6.0), 1, range(54), np.zeros(54, int), [2.0] * 4, [3.0] * 4,
+                   density=[1.0] * 4, clamped_faces=1 << 4)
+    uo = e.solve(e.matrix(), e.rhs(thermoelastic=False, gravity=True))
+    u = plain(phys, mech.solve())
+    assert np.abs(u - uo).max() <= 2e-9
+    assert np.abs(uo).max() > 1.0  # O(1) and larger displacements, as the reference notes
