@@ -92,6 +92,7 @@ SIGNATURES = {
     "adm_adjoint_gradient": [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_int32, _VP, _D, _D,
                              _VP],
     "adm_adjoint_vmult_transpose": [_VP, _VP, _VP, _VP, _D],
+    "adm_adjoint_checkpoint_interval": [_VP, ctypes.POINTER(ctypes.c_int32)],
     "adm_adjoint_set_flush": [_VP, ctypes.c_double],
     "adm_enkf_observe": [_VP, ctypes.c_int32, _VP, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, _VP, _VP],
     "adm_enkf_gain": [_VP, ctypes.c_int32, ctypes.c_int32, _VP, _VP, _VP, _VP, _VP, _VP],

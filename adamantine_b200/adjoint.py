@@ -61,7 +61,7 @@ class AdjointProblem:
 
     def __init__(self, base: ThermalConfig, y0_grid: np.ndarray, t0: float, dt: float, n_steps: int,
                  obs_steps: Sequence[int], points: np.ndarray, targets: Optional[np.ndarray] = None,
-                 device: int = 0, checkpoint_every: int = 20):
+                 device: int = 0, checkpoint_every: int = 0):
         self.base = base
         self.t0, self.dt, self.n_steps = float(t0), float(dt), int(n_steps)
         self.checkpoint_every = int(checkpoint_every)
@@ -141,6 +141,14 @@ class AdjointProblem:
         _lib.check(self._L.adm_adjoint_gradient(self._h, self.t0, self.dt, self.n_steps, self.checkpoint_every,
                                                 _dev(self.y0), ctypes.byref(J), _ptr(g, ctypes.c_double), None))
         return float(J.value), g / np.asarray(self._theta, np.float64)
+
+    def last_checkpoint_interval(self) -> int:
+        """The checkpoint interval the last gradient used (checkpoint_every
+        0, the default: the longest segment whose stores fit in half of the
+        free device memory, the whole run when it fits)."""
+        k = ctypes.c_int32()
+        _lib.check(self._L.adm_adjoint_checkpoint_interval(self._h, ctypes.byref(k)))
+        return int(k.value)
 
     def set_flush(self, flush: float):
         """Adjoint values at or below flush x the stage's largest count as

@@ -23,6 +23,7 @@
 #include "../../include/adamantine_b200_adjoint.h"
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <vector>
 
@@ -306,10 +307,34 @@ public:
     return J;
   }
 
+  // K <= 0: the longest segment whose stage stores fit in half of the free
+  // device memory (every step of the run when it fits: no recompute)
+  int auto_interval(int n_steps)
+  {
+    Thermal &t = th_;
+    ADM_CK(cudaSetDevice(t.device_));
+    int const S = t.tab_.s;
+    double const per_step = 8.0 * S * ((double)n_ + (t.ns_ == 3 ? (double)C_ * NN_ : 0.0));
+    size_t free_b = 0, total_b = 0;
+    ADM_CK(cudaMemGetInfo(&free_b, &total_b));
+    // the stores already held are released before the new ones are made
+    double const held = 8.0 * ((double)Ystore_.n + (double)Sstore_.n);
+    double const budget = 0.5 * ((double)free_b + held);
+    double const fit = std::floor(budget / per_step);
+    if (fit < 1.0)
+      throw Error(ADM_ERR_ALLOC, "not enough device memory for one step of adjoint stores");
+    return (int)std::min<double>(n_steps, fit);
+  }
+
+  int last_interval() const { return last_K_; }
+
   double gradient(double t0, double dt, int n_steps, int K, double const *y0, double *grad, double *y_final)
   {
     NvtxRange const nvtx_range("adm::adjoint_gradient");
+    if (K <= 0 && n_steps >= 1)
+      K = auto_interval(n_steps);
     check_run(n_steps, K);
+    last_K_ = K;
     Thermal &t = th_;
     cudaStream_t const st = t.stream_;
     int const S = t.tab_.s;
@@ -689,6 +714,7 @@ public:
   // adjoint values at or below flush * (the stage's max |mu|) count as zero
   // (whole tiles of them are skipped)
   double flush_ = 1e-30;
+  int last_K_ = 0;
 
 private:
   Thermal &th_;
@@ -752,6 +778,14 @@ int adm_adjoint_gradient(adm_adjoint *a, double t0, double dt, int32_t n_steps, 
   return adm::guard([&] {
     ADM_REQUIRE(a && y0 && J && grad, "null argument");
     *J = reinterpret_cast<adm::Adjoint *>(a)->gradient(t0, dt, n_steps, checkpoint_every, y0, grad, y_final);
+  });
+}
+
+int adm_adjoint_checkpoint_interval(adm_adjoint const *a, int32_t *checkpoint_every)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(a && checkpoint_every, "null argument");
+    *checkpoint_every = reinterpret_cast<adm::Adjoint const *>(a)->last_interval();
   });
 }
 

@@ -45,9 +45,15 @@ int adm_adjoint_objective(adm_adjoint *a, double t0, double dt, int32_t n_steps,
 /* Forward run with a checkpoint every checkpoint_every steps, then the
  * backward sweep (each segment recomputed from its checkpoint): *J and
  * grad[4] = dJ/dlog(k scale, c_p scale, absorptivity, power). The handle's
- * phase state ends as after the forward run. */
+ * phase state ends as after the forward run. checkpoint_every <= 0 picks
+ * the longest segment whose stage stores (the stage inputs, and the phase
+ * states with three material states) fit in half of the free device
+ * memory: the whole run when it fits, so that nothing is recomputed. */
 int adm_adjoint_gradient(adm_adjoint *a, double t0, double dt, int32_t n_steps, int32_t checkpoint_every,
                          double const *y0, double *J, double *grad, double *y_final);
+/* The checkpoint interval the last adm_adjoint_gradient used. No
+ * counterpart in the reference. */
+int adm_adjoint_checkpoint_interval(adm_adjoint const *a, int32_t *checkpoint_every);
 /* Adjoint values at or below flush times the stage's largest |M^-1 lambda|
  * count as zero in adm_adjoint_gradient, and tiles holding only such values
  * (and no powder adjoint) are skipped. The explicit stencil spreads the

@@ -144,6 +144,11 @@ def test_checkpoint_interval_does_not_change_the_gradient():
     J2, g2 = prob.gradient(THETA)
     assert J1 == J2
     assert rel(g1, g2) <= 1e-12
+    # the automatic interval keeps the whole (small) run: no recompute
+    prob.checkpoint_every = 0
+    J3, g3 = prob.gradient(THETA)
+    assert prob.last_checkpoint_interval() == prob.n_steps
+    assert J3 == J1 and rel(g1, g3) <= 1e-12
 
 
 def test_flushed_adjoint_gives_the_same_gradient():
