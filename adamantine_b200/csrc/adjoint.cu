@@ -51,6 +51,16 @@ void launch_adj(CUtensorMap const &ymap, CUtensorMap const &mmap, AdjArgs const 
   adjoint_kernel<DEG, NS><<<grid, T_::NT, smem, stream>>>(ymap, mmap, a, n_items);
 }
 
+// the backward member data's stage clock
+__global__ void bclock_kernel(double *clock, double t, double dt)
+{
+  if (threadIdx.x == 0)
+  {
+    clock[0] = t;
+    clock[1] = dt;
+  }
+}
+
 void launch_adjoint(int deg, int ns, CUtensorMap const &ym, CUtensorMap const &mm, AdjArgs const &a, int n_items,
                     cudaStream_t stream)
 {
@@ -318,12 +328,16 @@ public:
     size_t free_b = 0, total_b = 0;
     ADM_CK(cudaMemGetInfo(&free_b, &total_b));
     // the stores already held are released before the new ones are made
-    double const held = 8.0 * ((double)Ystore_.n + (double)Sstore_.n);
+    double const held = 8.0 * ((double)Ystore_.n + (double)Sstore_.n + (double)Ystore2_.n + (double)Sstore2_.n);
     double const budget = 0.5 * ((double)free_b + held);
     double const fit = std::floor(budget / per_step);
-    if (fit < 1.0)
+    if (fit >= (double)n_steps)
+      return n_steps;
+    // segments recomputed while the previous one runs backward: two stores
+    double const fit2 = std::floor(fit / 2.0);
+    if (fit2 < 1.0)
       throw Error(ADM_ERR_ALLOC, "not enough device memory for one step of adjoint stores");
-    return (int)std::min<double>(n_steps, fit);
+    return (int)fit2;
   }
 
   int last_interval() const { return last_K_; }
@@ -338,10 +352,24 @@ public:
     Thermal &t = th_;
     cudaStream_t const st = t.stream_;
     int const S = t.tab_.s;
-    // per step of a segment: the S stage inputs and (3 states) S phase states
+    // per step of a segment: the S stage inputs and (3 states) S phase
+    // states; with more than one segment two stores alternate, so that the
+    // recompute of a segment runs while the one after it goes backward
+    int const n_seg = (n_steps + K - 1) / K;
     Ystore_.alloc((size_t)K * S * n_);
     if (t.ns_ == 3)
       Sstore_.alloc((size_t)K * S * C_ * NN_);
+    if (n_seg > 1)
+    {
+      Ystore2_.alloc((size_t)K * S * n_);
+      if (t.ns_ == 3)
+        Sstore2_.alloc((size_t)K * S * C_ * NN_);
+    }
+    ystore_[0] = Ystore_.p;
+    ystore_[1] = n_seg > 1 ? Ystore2_.p : Ystore_.p;
+    sstore_[0] = Sstore_.p;
+    sstore_[1] = n_seg > 1 ? Sstore2_.p : Sstore_.p;
+    rec_buf_ = (n_seg - 1) & 1;
     forward(t0, dt, n_steps, y0, K);
     double J = 0.0;
     ADM_CK(cudaMemcpyAsync(&J, Jd_.p, sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -376,7 +404,14 @@ public:
     }
     grad_d_.alloc(3);
     ADM_CK(cudaMemsetAsync(grad_d_.p, 0, 3 * sizeof(double), st));
-    int const n_seg = (n_steps + K - 1) / K;
+    // the backward sweep runs on its own stream with its own member data
+    // (stage clock and beam state: the recompute on the handle's stream
+    // writes the handle's); everything else it reads is read-only here
+    backward_setup();
+    cudaStream_t const bs = bst_;
+    ADM_CK(cudaEventRecord(ev_start_, st));
+    ADM_CK(cudaStreamWaitEvent(bs, ev_start_, 0));
+    ADM_CK(cudaEventRecord(ev_rec_[(n_seg - 1) & 1], st));
     // the stage adjoints of a step are added into lam by the first stage
     // launch of the step before (and once at the end)
     LamTerms all{};
@@ -387,22 +422,16 @@ public:
     for (int seg = n_seg - 1; seg >= 0; --seg)
     {
       int const n0 = seg * K, n1 = std::min(n_steps, n0 + K);
-      // recompute the segment from its checkpoint, recording the stages (the
-      // forward run recorded the last segment already)
-      if (seg != n_seg - 1)
-      {
-        ADM_CK(cudaMemcpyAsync(y_.p, ck_y_.p + (size_t)seg * n_, n_ * sizeof(double), cudaMemcpyDeviceToDevice,
-                               st));
-        if (ns3)
-          restore_phase(seg);
-        for (int n = n0; n < n1; ++n)
-          record_step(n, n0, dt);
-      }
+      int const b = seg & 1;
+      // the segment's stages are recorded (the forward run recorded the last)
+      ADM_CK(cudaStreamWaitEvent(bs, ev_rec_[b], 0));
+      double const *ys = ystore_[b];
+      double *ss = sstore_[b];
       // backward sweep over the segment
       for (int n = n1 - 1; n >= n0; --n)
       {
-        inject(n + 1);
-        t.set_clock(times_[n], dt);
+        inject(n + 1, bs);
+        bclock_kernel<<<1, 32, 0, bs>>>(bclock_.p, times_[n], dt);
         for (int i = S - 1; i >= 0; --i)
         {
           LamTerms lt{};
@@ -433,21 +462,22 @@ public:
           x.act_next = act_next_;
           x.n_tiles = t.mesh_.n_tiles;
           x.sel = sel_.p;
-          x.md = t.cfg_.n_sources > 0 ? t.member_d_.p : nullptr;
+          x.md = t.cfg_.n_sources > 0 ? bmd_.p : nullptr;
           x.c = t.tab_.c[i];
           size_t const threads = std::max({n_, x.n_tiles, (size_t)count});
-          lamk_kernel<<<blocks(threads), 256, 0, st>>>(mu_.p, t.inv_mass_.p, lam_.p, pend, dt * t.tab_.b[i], lt,
+          lamk_kernel<<<blocks(threads), 256, 0, bs>>>(mu_.p, t.inv_mass_.p, lam_.p, pend, dt * t.tab_.b[i], lt,
                                                        lamYi, n_, x);
           ADM_CK(cudaGetLastError());
           size_t const rslot = (size_t)(n - n0) * S + i;
           AdjArgs A;
           std::memset(&A, 0, sizeof(A));
           A.k = t.base_args();
-          A.yv = Ystore_.p + rslot * n_;
+          A.k.members = bmd_.p;
+          A.yv = ys + rslot * n_;
           A.mu = mu_.p;
           if (ns3)
           {
-            A.s_in = Sstore_.p + rslot * qn;
+            A.s_in = ss + rslot * qn;
             A.lam_s_out = ls_a_.p;
             A.lam_s_in = ls_b_.p;
             A.powder_start = init_mode_.p;
@@ -459,19 +489,39 @@ public:
           // visit the marked tiles only; they mark the next stage's
           A.n_items_dev = x.n_sel;
           A.act_next = act_next_;
-          run_kernel(A, sel_.p);
+          run_kernel(A, sel_.p, bs);
           std::swap(act_cur_, act_next_);
           if (ns3)
             std::swap(ls_a_.p, ls_b_.p);
         }
         pending = true;
       }
+      ADM_CK(cudaEventRecord(ev_bwd_[b], bs));
+      // meanwhile: recompute the segment before from its checkpoint into the
+      // other store, once the backward sweep that last read it has ended
+      if (seg >= 1)
+      {
+        int const nb = b ^ 1, s0 = (seg - 1) * K, s1 = seg * K;
+        if (seg + 1 <= n_seg - 1)
+          ADM_CK(cudaStreamWaitEvent(st, ev_bwd_[nb], 0));
+        ADM_CK(cudaMemcpyAsync(y_.p, ck_y_.p + (size_t)(seg - 1) * n_, n_ * sizeof(double),
+                               cudaMemcpyDeviceToDevice, st));
+        if (ns3)
+          restore_phase(seg - 1);
+        rec_buf_ = nb;
+        for (int n = s0; n < s1; ++n)
+          record_step(n, s0, dt);
+        ADM_CK(cudaEventRecord(ev_rec_[nb], st));
+      }
     }
     if (pending)
     {
-      sum_kernel<<<blocks(n_), 256, 0, st>>>(lam_.p, all, n_);
+      sum_kernel<<<blocks(n_), 256, 0, bs>>>(lam_.p, all, n_);
       ADM_CK(cudaGetLastError());
     }
+    // join the backward stream
+    ADM_CK(cudaEventRecord(ev_start_, bs));
+    ADM_CK(cudaStreamWaitEvent(st, ev_start_, 0));
     double g[3] = {0, 0, 0};
     ADM_CK(cudaMemcpyAsync(g, grad_d_.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
     // the handle ends with the phase state of the forward run
@@ -549,7 +599,7 @@ private:
   }
 
   // work: the items to visit (default: every tile of the handle)
-  void run_kernel(AdjArgs &A, TileWork const *work = nullptr)
+  void run_kernel(AdjArgs &A, TileWork const *work = nullptr, cudaStream_t stream = nullptr)
   {
     Thermal &t = th_;
     int const count = t.colour_off_[8];
@@ -558,7 +608,7 @@ private:
     A.k.work = work ? work : t.work_d_.p;
     CUtensorMap const ym = brick_map(t.mesh_, A.yv, 1, n_);
     CUtensorMap const mm = brick_map(t.mesh_, A.mu, 1, n_);
-    launch_adjoint(t.mesh_.deg, t.ns_, ym, mm, A, count, t.stream_);
+    launch_adjoint(t.mesh_.deg, t.ns_, ym, mm, A, count, stream ? stream : t.stream_);
     ADM_CK(cudaGetLastError());
   }
 
@@ -631,10 +681,11 @@ private:
       a.y_override = y_.p;
       double const *src = i == 0 ? y_.p : (a.src_sel == 1 ? t.za_p_ : t.zb_p_);
       size_t const slot = (size_t)(n - n0) * S + i;
-      ADM_CK(cudaMemcpyAsync(Ystore_.p + slot * n_, src, n_ * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      ADM_CK(cudaMemcpyAsync(ystore_[rec_buf_] + slot * n_, src, n_ * sizeof(double), cudaMemcpyDeviceToDevice,
+                             st));
       if (t.ns_ == 3)
         launch_expand_powder(t.cell_info_d_.p, NN_, t.powder_mode_.p, t.powder_cell_.p, t.powder_q_.p,
-                             Sstore_.p + slot * qn, C_, st, init_mode_.p);
+                             sstore_[rec_buf_] + slot * qn, C_, st, init_mode_.p);
       t.launch_pass(a, src);
     }
   }
@@ -650,12 +701,12 @@ private:
       }
   }
 
-  void inject(int n)
+  void inject(int n, cudaStream_t stream)
   {
     for (size_t k = 0; k < obs_steps_.size(); ++k)
       if (obs_steps_[k] == n && n_points_ > 0)
       {
-        inject_kernel<<<blocks(n_points_), 256, 0, th_.stream_>>>(lam_.p, idx_.p, resid_.p + k * n_points_,
+        inject_kernel<<<blocks(n_points_), 256, 0, stream>>>(lam_.p, idx_.p, resid_.p + k * n_points_,
                                                                   n_points_, tile_grid(), act_cur_);
         ADM_CK(cudaGetLastError());
       }
@@ -710,7 +761,51 @@ private:
     times_[n_steps] = tt;
   }
 
+  // the backward stream, its events and member data: a copy of the handle's
+  // with its own stage clock and beam state
+  void backward_setup()
+  {
+    Thermal &t = th_;
+    if (!bst_)
+    {
+      ADM_CK(cudaStreamCreateWithFlags(&bst_, cudaStreamNonBlocking));
+      ADM_CK(cudaEventCreateWithFlags(&ev_start_, cudaEventDisableTiming));
+      for (int i = 0; i < 2; ++i)
+      {
+        ADM_CK(cudaEventCreateWithFlags(&ev_rec_[i], cudaEventDisableTiming));
+        ADM_CK(cudaEventCreateWithFlags(&ev_bwd_[i], cudaEventDisableTiming));
+      }
+    }
+    MemberData md;
+    ADM_CK(cudaMemcpyAsync(&md, t.member_d_.p, sizeof(MemberData), cudaMemcpyDeviceToHost, t.stream_));
+    ADM_CK(cudaStreamSynchronize(t.stream_));
+    bbeam_.alloc(kMaxBeams);
+    bclock_.alloc(2);
+    md.beam_state = bbeam_.p;
+    md.clock = bclock_.p;
+    bmd_.alloc(1);
+    ADM_CK(cudaMemcpyAsync(bmd_.p, &md, sizeof(MemberData), cudaMemcpyHostToDevice, t.stream_));
+    ADM_CK(cudaStreamSynchronize(t.stream_));
+  }
+
 public:
+  ~Adjoint()
+  {
+    if (bst_)
+    {
+      cudaStreamSynchronize(bst_);
+      cudaEventDestroy(ev_start_);
+      for (int i = 0; i < 2; ++i)
+      {
+        cudaEventDestroy(ev_rec_[i]);
+        cudaEventDestroy(ev_bwd_[i]);
+      }
+      cudaStreamDestroy(bst_);
+    }
+  }
+  Adjoint(Adjoint const &) = delete;
+  Adjoint &operator=(Adjoint const &) = delete;
+
   // adjoint values at or below flush * (the stage's max |mu|) count as zero
   // (whole tiles of them are skipped)
   double flush_ = 1e-30;
@@ -731,6 +826,14 @@ private:
   std::vector<double> times_;
   DevBuf<int64_t> idx_;
   DevBuf<double> tgt_, resid_, Jd_, y_, lam_, mu_, lamY_, ls_a_, ls_b_, grad_d_, Ystore_, Sstore_;
+  DevBuf<double> Ystore2_, Sstore2_, bclock_;
+  double *ystore_[2] = {nullptr, nullptr};
+  double *sstore_[2] = {nullptr, nullptr};
+  int rec_buf_ = 0;
+  DevBuf<MemberData> bmd_;
+  DevBuf<BeamState> bbeam_;
+  cudaStream_t bst_ = nullptr;
+  cudaEvent_t ev_start_ = nullptr, ev_rec_[2] = {nullptr, nullptr}, ev_bwd_[2] = {nullptr, nullptr};
   DevBuf<double> ck_y_, ck_cell_, ck_q_, init_cell_, init_q_, fin_cell_, fin_q_;
   DevBuf<uint8_t> ck_mode_, init_mode_, fin_mode_;
 };
