@@ -59,33 +59,44 @@ __device__ __forceinline__ int64_t node_of(MechArgs const &a, int cx, int cy, in
   return (int64_t)(a.p * cx + i) + (int64_t)a.pitch * ((a.p * cy + j) + (int64_t)a.nn[1] * (a.p * cz + k));
 }
 
-// dst += A src on the free rows; 4 warps per block, one cell per warp.
+// dst += A src on the free rows; 4 warps per block, 32 / N cells per warp
+// (4 for FE_Q(1), 1 for FE_Q(2)), N lanes per cell.
 __global__ void __launch_bounds__(128) elastic_apply_kernel(MechArgs a, double const *src, double *dst)
 {
-  __shared__ double u[4][3][kMaxN];
-  __shared__ double S[4][kMaxN][9];
+  __shared__ double u[4][3][32];
+  __shared__ double S[4][32][9];
   int const w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int const G = 32 / a.N; // cells per warp
+  int const g = lane / a.N, l = lane - g * a.N;
+  bool const on = g < G;
   int const gw = blockIdx.x * 4 + w, nw = gridDim.x * 4;
-  for (int ci = gw; ci < a.n_cells; ci += nw)
+  // every lane runs the same number of rounds (the warp syncs inside)
+  int const rounds = (a.n_cells + nw * G - 1) / (nw * G);
+  for (int rd = 0; rd < rounds; ++rd)
   {
-    int const c = a.cells[ci];
-    int const cx = c % a.nc[0], cy = (c / a.nc[0]) % a.nc[1], cz = c / (a.nc[0] * a.nc[1]);
-    int const mat = a.matid[c];
-    double const lam = a.lambda[mat], mu = a.mu[mat];
-    int64_t g = 0;
+    int const ci = (rd * nw + gw) * G + g;
+    bool const act = on && ci < a.n_cells;
+    int64_t gidx = 0;
     bool freen = false;
-    if (lane < a.N)
+    double lam = 0.0, mu = 0.0;
+    if (act)
     {
-      g = node_of(a, cx, cy, cz, lane);
-      freen = a.node_mask[g] == 1;
+      int const c = a.cells[ci];
+      int const cx = c % a.nc[0], cy = (c / a.nc[0]) % a.nc[1], cz = c / (a.nc[0] * a.nc[1]);
+      int const mat = a.matid[c];
+      lam = a.lambda[mat];
+      mu = a.mu[mat];
+      gidx = node_of(a, cx, cy, cz, l);
+      freen = a.node_mask[gidx] == 1;
       for (int comp = 0; comp < 3; ++comp)
-        u[w][comp][lane] = freen ? src[comp * a.m + g] : 0.0;
+        u[w][comp][g * a.N + l] = freen ? src[comp * a.m + gidx] : 0.0;
     }
     __syncwarp();
-    if (lane < a.N)
+    if (act)
     {
-      int const q = lane;
-      double G[3][3];
+      int const q = l;
+      double const *uc = &u[w][0][g * a.N];
+      double G3[3][3];
 #pragma unroll
       for (int comp = 0; comp < 3; ++comp)
 #pragma unroll
@@ -93,28 +104,28 @@ __global__ void __launch_bounds__(128) elastic_apply_kernel(MechArgs a, double c
         {
           double s = 0.0;
           for (int n = 0; n < a.N; ++n)
-            s = fma(u[w][comp][n], c_grad[(q * kMaxN + n) * 3 + d], s);
-          G[comp][d] = s * a.inv_h[d];
+            s = fma(uc[comp * 32 + n], c_grad[(q * kMaxN + n) * 3 + d], s);
+          G3[comp][d] = s * a.inv_h[d];
         }
-      double const div = G[0][0] + G[1][1] + G[2][2];
+      double const div = G3[0][0] + G3[1][1] + G3[2][2];
       double const jw = a.jxw * c_wq[q];
 #pragma unroll
       for (int comp = 0; comp < 3; ++comp)
 #pragma unroll
         for (int d = 0; d < 3; ++d)
-          S[w][q][comp * 3 + d] = jw * ((comp == d ? lam * div : 0.0) + mu * (G[comp][d] + G[d][comp]));
+          S[w][g * a.N + q][comp * 3 + d] = jw * ((comp == d ? lam * div : 0.0) + mu * (G3[comp][d] + G3[d][comp]));
     }
     __syncwarp();
-    if (lane < a.N && freen)
+    if (act && freen)
     {
-      int const n = lane;
+      int const n = l;
       for (int comp = 0; comp < 3; ++comp)
       {
         double r = 0.0;
         for (int q = 0; q < a.N; ++q)
           for (int d = 0; d < 3; ++d)
-            r = fma(S[w][q][comp * 3 + d], c_grad[(q * kMaxN + n) * 3 + d] * a.inv_h[d], r);
-        atomicAdd(dst + comp * a.m + g, r);
+            r = fma(S[w][g * a.N + q][comp * 3 + d], c_grad[(q * kMaxN + n) * 3 + d] * a.inv_h[d], r);
+        atomicAdd(dst + comp * a.m + gidx, r);
       }
     }
     __syncwarp();
@@ -556,7 +567,9 @@ private:
   {
     if (n_cells_ == 0)
       return;
-    unsigned const nb = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n_cells_ + 3) / 4, 148 * 16));
+    int64_t const per_warp = 32 / N_;
+    unsigned const nb =
+        (unsigned)std::max<int64_t>(1, std::min<int64_t>((n_cells_ + 4 * per_warp - 1) / (4 * per_warp), 148 * 16));
     elastic_apply_kernel<<<nb, 128, 0, th_.stream_>>>(args(), src, dst);
     ADM_CK(cudaGetLastError());
   }

@@ -549,6 +549,63 @@ def run_amr(args, local_rank):
     }
 
 
+MECHANICS_WORKLOAD = "eshelby_inclusion_64x64x64_q1"
+
+
+def run_mechanics(args, local_rank):
+    """The thermoelastic solve of the reference's Eshelby case (a 1 um
+    inclusion 1 K warmer, alpha = 0.01, K = 160 GPa, G = 79 GPa, in a 40 um
+    cube clamped on z-) on 64^3 FE_Q(1) cells: setup (cells, right-hand side,
+    Jacobi diagonal), one operator application and the CG solve to 1e-12
+    |rhs| (host wall clock, synchronized)."""
+    import torch
+
+    from adamantine_b200.config import Boundary, Geometry, ThermalConfig
+    from adamantine_b200.mechanics import MechanicalPhysics
+    from adamantine_b200.thermal import ThermalPhysics
+    from adamantine_b200.workloads import steel_solid_material
+
+    n, L, a = 64, 4.0e-5, 1.0e-6
+    cfg = ThermalConfig(geometry=Geometry(dim=3, n_cells=(n, n, n), extent=(L, L, L)),
+                        material=steel_solid_material(), boundary=Boundary.from_database({"type": "adiabatic"}, 3),
+                        sources=[], degree=1, time_method="forward_euler")
+    phys = ThermalPhysics(cfg, device=local_rank)
+    x = np.linspace(0.0, L, n + 1)
+    Z, Y, X = np.meshgrid(x, x, x, indexing="ij")
+    dist = np.sqrt((X - 2e-5) ** 2 + (Y - 2e-5) ** 2 + (Z - 2e-5) ** 2)
+    T = phys.from_grid(np.where(dist < a, 3.0, 2.0))
+    mech = MechanicalPhysics(phys, 160.0e9 - 2.0 / 3.0 * 79.0e9, 79.0e9, 0.01, reference_temperatures=[2.0],
+                             initial_temperature=2.0, gravity=False, clamped=("z-",))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    mech.setup_dofs(T)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    src = torch.rand(3 * phys.m(), dtype=torch.float64, device=phys.device)
+    dst = torch.zeros_like(src)
+    mech.vmult(dst, src)  # warm-up
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(phys.stream)
+    for _ in range(10):
+        mech.vmult(dst, src)
+    e1.record(phys.stream)
+    e1.synchronize()
+    apply_ms = e0.elapsed_time(e1) / 10
+    t2 = time.perf_counter()
+    u = mech.solve()
+    torch.cuda.synchronize()
+    t3 = time.perf_counter()
+    return {
+        "workload": MECHANICS_WORKLOAD, "dofs": mech.n_dofs, "cells": mech.n_cells,
+        "setup_ms": 1e3 * (t1 - t0), "apply_ms": apply_ms, "apply_mdofs_per_s": mech.n_dofs / apply_ms / 1e3,
+        "cg_iterations": mech.iterations, "solve_ms": 1e3 * (t3 - t2),
+        "ms_per_iteration": 1e3 * (t3 - t2) / max(1, mech.iterations), "residual": mech.residual,
+        "max_displacement": float(u.abs().max().item()),
+        "solver": "Jacobi-preconditioned CG to 1e-12 |rhs| (the reference: AMG-preconditioned CG)",
+    }
+
+
 def run_reference(args, rank, world):
     """--impl reference: the oracle's vmult on all host cores (rank 0 only)."""
     if rank != 0:
@@ -697,6 +754,8 @@ def run_ours(args, rank, world, local_rank):
         line["deposition"] = run_deposition(args, local_rank, rank == 0 and not args.no_cpu_baseline)
     if args.amr_steps > 0:
         line["amr"] = run_amr(args, local_rank)
+    if not args.no_mechanics:
+        line["mechanics"] = run_mechanics(args, local_rank)
     if rank == 0 and not args.no_cpu_baseline:
         rate, med, n = cpu_vmult_rate(build_workload(args.size)[0], T, os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": rate, "unit": "GDoF/s", "cores": os.cpu_count() or 1, "kind": "port",
@@ -721,6 +780,7 @@ def main():
     ap.add_argument("--deposition-steps", type=int, default=400,
                     help="RK4 steps of the deposition workload (0: skip; the configuration runs 2000)")
     ap.add_argument("--size", default="full", choices=sorted(SIZES))
+    ap.add_argument("--no-mechanics", action="store_true")
     ap.add_argument("--amr-steps", type=int, default=50,
                     help="RK4 steps of the refined-mesh workload (0: skip it)")
     args = ap.parse_args()
