@@ -720,6 +720,16 @@ public:
     ADM_CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     ADM_CK(cudaEventCreateWithFlags(&ev_in_, cudaEventDisableTiming));
     ADM_CK(cudaEventCreateWithFlags(&ev_out_, cudaEventDisableTiming));
+    ADM_CK(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
+    // one stream per level grid: the levels' operators run concurrently,
+    // forked from the handle's stream and joined back (events)
+    lstream_.assign(max_level + 1, nullptr);
+    ev_lev_.assign(max_level + 1, nullptr);
+    for (int l = 0; l <= max_level; ++l)
+    {
+      ADM_CK(cudaStreamCreateWithFlags(&lstream_[l], cudaStreamNonBlocking));
+      ADM_CK(cudaEventCreateWithFlags(&ev_lev_[l], cudaEventDisableTiming));
+    }
   }
 
   ~Amr()
@@ -728,7 +738,18 @@ public:
     if (stream_)
       cudaStreamSynchronize(stream_);
     drop_graph();
+    for (cudaStream_t ls : lstream_)
+      if (ls)
+        cudaStreamSynchronize(ls);
     levels_.clear();
+    for (cudaStream_t ls : lstream_)
+      if (ls)
+        cudaStreamDestroy(ls);
+    for (cudaEvent_t e : ev_lev_)
+      if (e)
+        cudaEventDestroy(e);
+    if (ev_fork_)
+      cudaEventDestroy(ev_fork_);
     if (ev_in_)
       cudaEventDestroy(ev_in_);
     if (ev_out_)
@@ -805,6 +826,7 @@ public:
         old.value[row_pos_h_[r]] = vals[r];
     }
     int const ns = mesh_.cfg.n_states;
+    fork();
     old.states.resize(levels_.size());
     old.pitch.assign(levels_.size(), 0);
     old.nn1.assign(levels_.size(), 0);
@@ -848,9 +870,11 @@ public:
   {
     require_ready();
     Ordered ord(*this);
+    fork();
     for (size_t l = 0; l < levels_.size(); ++l)
       if (alive(l))
         levels_[l]->set_time(t);
+    join();
   }
 
   // dst = C^T (sum_l A_l) C src (composite vectors on the device)
@@ -859,9 +883,11 @@ public:
     require_ready();
     Ordered ord(*this);
     prolong(src);
+    fork();
     for (size_t l = 0; l < levels_.size(); ++l)
       if (alive(l))
         levels_[l]->vmult(dst_lev_.p + lev_off_[l], src_lev_.p + lev_off_[l], false);
+    join();
     restrict_to(dst, 0);
   }
 
@@ -905,9 +931,12 @@ public:
     z_.alloc(n);
     if (z_.p != before)
       drop_graph();
+    // the level clocks, after the last replay and before this one
+    fork();
     for (size_t l = 0; l < levels_.size(); ++l)
       if (alive(l))
         levels_[l]->set_step_clock(t, dt);
+    join();
     if (!step_exec_ || step_dt_ != dt)
     {
       drop_graph();
@@ -952,6 +981,39 @@ public:
 
   void synchronize() { ADM_CK(cudaStreamSynchronize(stream_)); }
 
+  // the level streams wait for the handle's stream / the handle's stream
+  // waits for the level streams
+  void fork()
+  {
+    ADM_CK(cudaEventRecord(ev_fork_, stream_));
+    for (size_t l = 0; l < lstream_.size(); ++l)
+      if (levels_.size() > l && levels_[l])
+        ADM_CK(cudaStreamWaitEvent(lstream_[l], ev_fork_, 0));
+  }
+
+  void join()
+  {
+    for (size_t l = 0; l < lstream_.size(); ++l)
+      if (levels_.size() > l && levels_[l])
+      {
+        ADM_CK(cudaEventRecord(ev_lev_[l], lstream_[l]));
+        ADM_CK(cudaStreamWaitEvent(stream_, ev_lev_[l], 0));
+      }
+  }
+
+  // the cell states of a level grid (host, n_states x cells of the grid)
+  void level_cell_state(int l, double *host)
+  {
+    require_ready();
+    Ordered ord(*this);
+    Thermal *th = level(l);
+    if (!th)
+      throw Error(ADM_ERR_INVALID, "no leaves on this level");
+    fork();
+    th->set_state_to_material_properties();
+    th->get_cell_state(host);
+  }
+
 private:
   void drop_graph()
   {
@@ -966,9 +1028,11 @@ private:
   void vmult_stage(double *dst, double const *src, double c)
   {
     prolong(src);
+    fork();
     for (size_t l = 0; l < levels_.size(); ++l)
       if (alive(l))
         levels_[l]->vmult_stage(dst_lev_.p + lev_off_[l], src_lev_.p + lev_off_[l], c);
+    join();
     restrict_to(dst, 0);
   }
 
@@ -1110,6 +1174,7 @@ private:
   void build_levels(Snapshot const *old)
   {
     drop_graph();
+    fork();
     int const L = mesh_.forest.max_level;
     int const ns = mesh_.cfg.n_states;
     // level Thermals persist across remeshing (set up again on the new
@@ -1128,7 +1193,7 @@ private:
           c.n_cells[d] = (int32_t)mesh_.forest.n(l, d);
         for (int b = 0; b < c.n_sources; ++b)
           c.sources[b].segments = mesh_.segments[b].empty() ? nullptr : mesh_.segments[b].data();
-        levels_[l] = std::make_unique<Thermal>(c, device_, stream_);
+        levels_[l] = std::make_unique<Thermal>(c, device_, lstream_[l]);
         levels_[l]->set_schedule(schedule_);
       }
       Thermal *th = levels_[l].get();
@@ -1279,11 +1344,15 @@ private:
   void compute_inverse_mass()
   {
     inv_m_.alloc(std::max<int64_t>(1, n_dofs()));
+    fork();
+    for (size_t l = 0; l < levels_.size(); ++l)
+      if (alive(l))
+        levels_[l]->compute_inverse_mass_matrix();
+    join();
     for (size_t l = 0; l < levels_.size(); ++l)
     {
       if (!alive(l))
         continue;
-      levels_[l]->compute_inverse_mass_matrix();
       int64_t const r0 = row_lev_[l], r1 = row_lev_[l + 1];
       if (r1 > r0)
         mass_from_inverse_kernel<<<blocks(r1 - r0), 256, 0, stream_>>>(r1 - r0, row_pos_.p + r0, lev_off_[l],
@@ -1301,6 +1370,9 @@ private:
   cudaStream_t user_ = nullptr, stream_ = nullptr;
   cudaEvent_t ev_in_ = nullptr, ev_out_ = nullptr;
   cudaGraphExec_t step_exec_ = nullptr;
+  cudaEvent_t ev_fork_ = nullptr;
+  std::vector<cudaStream_t> lstream_;
+  std::vector<cudaEvent_t> ev_lev_;
   double step_dt_ = 0.0;
   bool ready_ = false;
   AmrMesh mesh_;
@@ -1670,10 +1742,7 @@ int adm_amr_level_cell_state(adm_amr *h, int level, double *host)
 {
   return adm::guard([&] {
     ADM_REQUIRE(h && host, "null argument");
-    adm::Thermal *th = h->a->level(level);
-    ADM_REQUIRE(th, "no leaves on this level");
-    th->set_state_to_material_properties();
-    th->get_cell_state(host);
+    h->a->level_cell_state(level, host);
   });
 }
 

@@ -492,18 +492,18 @@ public:
     {
       precondition(r_.p, z_.p);
       ADM_CK(cudaMemcpyAsync(pv_.p, z_.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-      dot(r_.p, z_.p, 0); // sc[0] = r.z
+      dot_device(r_.p, z_.p, 0); // sc[0] = r.z
       for (it = 1; it <= max_iter; ++it)
       {
         vmult(qv_.p, pv_.p);
-        dot(pv_.p, qv_.p, 1); // sc[1] = p.q
+        dot_device(pv_.p, qv_.p, 1); // sc[1] = p.q (alpha = sc[0] / sc[1] on the device)
         cg_update_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, sc_.p, pv_.p, qv_.p, x, r_.p);
         ADM_CK(cudaGetLastError());
         res = std::sqrt(dot(r_.p, r_.p, 2));
         if (res <= tol)
           break;
         precondition(r_.p, z_.p);
-        dot(r_.p, z_.p, 3); // sc[3] = new r.z
+        dot_device(r_.p, z_.p, 3); // sc[3] = new r.z
         cg_direction_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, sc_.p + 3, sc_.p, z_.p, pv_.p);
         ADM_CK(cudaGetLastError());
         ADM_CK(cudaMemcpyAsync(sc_.p, sc_.p + 3, sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -581,14 +581,22 @@ private:
     ADM_CK(cudaGetLastError());
   }
 
-  // sc[slot] = x . y (device), also returned to the host
-  double dot(double const *x, double const *y, int slot)
+  // sc[slot] = x . y on the device (no read-back: the CG's scalars stay
+  // there; only the residual norm comes back, once per iteration)
+  void dot_device(double const *x, double const *y, int slot)
   {
     cudaStream_t const s = th_.stream_;
     int64_t const n = 3 * m_;
     ADM_CK(cudaMemsetAsync(sc_.p + slot, 0, sizeof(double), s));
     dot_kernel<<<blocks_for(n), 256, 0, s>>>(n, x, y, sc_.p + slot);
     ADM_CK(cudaGetLastError());
+  }
+
+  // sc[slot] = x . y (device), also returned to the host
+  double dot(double const *x, double const *y, int slot)
+  {
+    cudaStream_t const s = th_.stream_;
+    dot_device(x, y, slot);
     double v = 0.0;
     ADM_CK(cudaMemcpyAsync(&v, sc_.p + slot, sizeof(double), cudaMemcpyDeviceToHost, s));
     ADM_CK(cudaStreamSynchronize(s));
