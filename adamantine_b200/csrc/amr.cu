@@ -454,6 +454,12 @@ struct AmrMesh
   {
     int const L = forest.max_level;
     std::unordered_map<int64_t, uint8_t> nodes; // key -> 1
+    {
+      int64_t n_leaf = 0;
+      for (int l = 0; l <= L; ++l)
+        n_leaf += n_active_leaves(l);
+      nodes.reserve((size_t)(n_leaf * (p + 1) * (p + 1) * 2));
+    }
     for (int l = 0; l <= L; ++l)
       for (int64_t k = 0; k < forest.n(l, 2); ++k)
         for (int64_t j = 0; j < forest.n(l, 1); ++j)
@@ -812,18 +818,22 @@ public:
     Snapshot old;
     old.forest = mesh_.forest;
     old.off = lev_off_;
+    // the old composite values with their (sorted) lattice keys: a new DoF
+    // on an old DoF's position takes its value as it is
+    old.dof_key = mesh_.dof_key;
+    old.dof_val.resize(n_dofs());
+    ADM_CK(cudaMemcpyAsync(old.dof_val.data(), y_.p, n_dofs() * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    ADM_CK(cudaStreamSynchronize(stream_));
     if (n_rows_ > 0)
     {
       DevBuf<double> rv;
       rv.alloc(n_rows_);
       gather_kernel<<<blocks(n_rows_), 256, 0, stream_>>>(n_rows_, row_pos_.p, src_lev_.p, rv.p);
       ADM_CK(cudaGetLastError());
-      std::vector<double> vals(n_rows_);
-      ADM_CK(cudaMemcpyAsync(vals.data(), rv.p, n_rows_ * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+      old.row_val.resize(n_rows_);
+      ADM_CK(cudaMemcpyAsync(old.row_val.data(), rv.p, n_rows_ * sizeof(double), cudaMemcpyDeviceToHost, stream_));
       ADM_CK(cudaStreamSynchronize(stream_));
-      old.value.reserve(2 * n_rows_);
-      for (int64_t r = 0; r < n_rows_; ++r)
-        old.value[row_pos_h_[r]] = vals[r];
+      old.row_pos = row_pos_h_; // ascending: levels in order, nodes sorted
     }
     int const ns = mesh_.cfg.n_states;
     fork();
@@ -846,7 +856,10 @@ public:
     // SolutionTransfer: the old field at the new nodes
     std::vector<double> y(n_dofs());
     for (int64_t d = 0; d < n_dofs(); ++d)
-      y[d] = old.evaluate(mesh_, mesh_.dof_key[d]);
+    {
+      double v;
+      y[d] = old.dof_lookup(mesh_.dof_key[d], v) ? v : old.evaluate(mesh_, mesh_.dof_key[d]);
+    }
     y_.alloc(n_dofs());
     ADM_CK(cudaMemcpyAsync(y_.p, y.data(), y.size() * sizeof(double), cudaMemcpyHostToDevice, stream_));
     ADM_CK(cudaStreamSynchronize(stream_));
@@ -1090,7 +1103,19 @@ private:
   {
     Forest forest;
     std::vector<int64_t> off;
-    std::unordered_map<int64_t, double> value; // level-buffer position -> old field
+    // the old field at the old leaves' level nodes (ascending level-buffer
+    // positions) and the old composite DoFs (ascending lattice keys)
+    std::vector<int64_t> row_pos, dof_key;
+    std::vector<double> row_val, dof_val;
+
+    bool dof_lookup(int64_t key, double &v) const
+    {
+      auto it = std::lower_bound(dof_key.begin(), dof_key.end(), key);
+      if (it == dof_key.end() || *it != key)
+        return false;
+      v = dof_val[it - dof_key.begin()];
+      return true;
+    }
     std::vector<std::vector<double>> states;
     std::vector<int> pitch, nn1;
 
@@ -1129,10 +1154,10 @@ private:
                     if (w == 0.0)
                       continue;
                     int64_t const nidx = (p * a + q0) + (int64_t)pitch[l] * ((p * b + q1) + (int64_t)nn1[l] * (p * c + q2));
-                    auto it = value.find(off[l] + nidx);
-                    if (it == value.end())
+                    auto it = std::lower_bound(row_pos.begin(), row_pos.end(), off[l] + nidx);
+                    if (it == row_pos.end() || *it != off[l] + nidx)
                       throw Error(ADM_ERR_INVALID, "internal: old leaf node without a value");
-                    v += w * it->second;
+                    v += w * row_val[it - row_pos.begin()];
                   }
               return v;
             }
