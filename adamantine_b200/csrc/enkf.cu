@@ -97,6 +97,7 @@ struct LocGeom
   double origin[3] = {0, 0, 0}, spacing[3] = {0, 0, 0};
   int64_t nn[3] = {0, 0, 0}, pitch = 0;
   double bmin[3] = {0, 0, 0}, bsize[3] = {1, 1, 1};
+  double bmax[3] = {0, 0, 0}; // the observation points' extent (with bmin)
   int nb[3] = {1, 1, 1};
 };
 
@@ -1160,14 +1161,18 @@ __global__ void __launch_bounds__(256) loc_state_kernel(LocGeom g, double const 
     int64_t const lo_idx[3] = {a0, b0, c0};
     for (int d = 0; d < 3; ++d)
     {
-      if (g.nb[d] == 1)
-      {
-        q0[d] = 0;
-        q1[d] = 0;
-        continue;
-      }
       double const lo = g.origin[d] + (double)lo_idx[d] * g.spacing[d] - g.cutoff;
       double const hi = g.origin[d] + (double)hi_idx[d] * g.spacing[d] + g.cutoff;
+      if (g.nb[d] == 1)
+      {
+        // one bucket along d: none of its points is within the cutoff of
+        // the brick when the grown brick misses their extent (the margin
+        // keeps the test on the safe side of rounding)
+        double const margin = 1e-9 * g.cutoff;
+        q0[d] = 0;
+        q1[d] = (hi + margin < g.bmin[d] || lo - margin > g.bmax[d]) ? -1 : 0;
+        continue;
+      }
       double const f0 = floor((lo - g.bmin[d]) / g.bsize[d]), f1 = floor((hi - g.bmin[d]) / g.bsize[d]);
       q0[d] = (int)fmin(fmax(f0, 0.0), (double)g.nb[d]);
       q1[d] = (int)fmin(fmax(f1, -1.0), (double)(g.nb[d] - 1));
@@ -1333,6 +1338,7 @@ struct Enkf
     {
       double const ext = omax[d] - omin[d];
       g.bmin[d] = omin[d];
+      g.bmax[d] = omax[d];
       if (covers_all || ext <= 0.0)
       {
         g.nb[d] = 1;
