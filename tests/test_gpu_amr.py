@@ -59,10 +59,12 @@ def test_constrained_operator_and_mass_match_oracle(degree, boundary):
         assert torch.abs(dst_c - dst).max().item() <= 1e-12 * np.abs(ref).max()
 
 
-def test_amr_test_run_matches_oracle_at_degree_2():
-    """amr_test.info's loop at FE degree 2 (the GPU path's degrees are 1-2;
-    the reference's FE_Q(3) pin is checked on the restatement)."""
-    cfg = amr_test_config(degree=2)
+@pytest.mark.parametrize("degree,method", [(2, "forward_euler"), (1, "forward_euler"), (2, "rk_third_order")])
+def test_amr_test_run_matches_oracle(degree, method):
+    """amr_test.info's loop at FE degree 1 and 2 (the GPU path's degrees;
+    the reference's FE_Q(3) pin is checked on the restatement), also with
+    the RK3 tableau (a stage input from two earlier stages)."""
+    cfg = amr_test_config(degree=degree, method=method)
     g, o = both(cfg, 1)
     run_amr(g)
     run_amr(o)
