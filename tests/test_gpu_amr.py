@@ -131,3 +131,31 @@ def test_uniform_refinement_is_the_fine_grid(degree):
         fine.vmult(dst_f, src_f)
         ref = dst_f.cpu().numpy().reshape(grid.shape)[idx[:, 2], idx[:, 1], idx[:, 0]]
         assert (dst.cpu().numpy() == ref).all()
+
+
+@pytest.mark.parametrize("degree", [1, 2])
+def test_operator_with_inactive_coarse_cells(degree):
+    """Part of the upper layer carries no material: faces towards missing
+    material take the convective / radiative terms on every level, faces
+    between levels inside the material do not; refined along the beam
+    across the edge of the material, against the restatement."""
+    cfg = amr_test_config(degree=degree, n_cells=(4, 4, 2), boundary="convective,radiative")
+    active = np.ones(32, np.uint8)
+    active[16 + 8:] = 0  # the upper layer's back half is missing
+    active[16 + 1] = 0
+    g, o = both(cfg, 2, active=active)
+    g.refine_mesh(0.0, 200e-6, 200, 2)
+    o.refine_mesh(0.0, 200e-6, 200, 2)
+    assert g.n_dofs == o.n_dofs and len(o.hanging) > 0
+    im = g.inverse_mass().cpu().numpy()
+    assert np.abs(im - o.inv_mass).max() <= 1e-13 * np.abs(o.inv_mass).max()
+    rng = np.random.default_rng(13)
+    y = field(o.dof_points(), rng)
+    src = torch.tensor(y, device=torch.device("cuda"))
+    dst = torch.zeros_like(src)
+    for t in (30e-6, 120e-6):
+        g.set_time(t)
+        o.set_time(t)
+        g.vmult(dst, src)
+        ref = o.vmult(y)
+        assert np.abs(dst.cpu().numpy() - ref).max() <= 1e-10 * np.abs(ref).max()
