@@ -143,6 +143,8 @@ SIGNATURES = {
     "adm_amr_level_layout": [_VP, ctypes.c_int32, _VP, ctypes.POINTER(ctypes.c_int64)],
     "adm_amr_level_cell_state": [_VP, ctypes.c_int32, _VP],
     "adm_amr_set_schedule": [_VP, ctypes.c_int32],
+    "adm_amr_mark_has_melted": [_VP, ctypes.c_double],
+    "adm_amr_level_has_melted": [_VP, ctypes.c_int32, _VP],
     "adm_amr_synchronize": [_VP],
     "adm_mechanics_create": [_VP, _VP, ctypes.POINTER(_VP)],
     "adm_mechanics_destroy": [_VP],

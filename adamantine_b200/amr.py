@@ -237,6 +237,17 @@ class AmrThermalPhysics(_Common):
         self._call("level_cell_state", int(level), _p(out))
         return out.reshape(ns, -1)
 
+    def mark_has_melted(self, threshold: float):
+        """Flag the leaves whose cell-average temperature exceeds threshold
+        (ThermalPhysics::mark_has_melted); the flags follow refinement."""
+        self._call("mark_has_melted", float(threshold))
+
+    def level_has_melted(self, level: int) -> np.ndarray:
+        n = [self.config.geometry.n_cells[d] << level for d in range(3)]
+        out = np.zeros(n[0] * n[1] * n[2], np.uint8)
+        self._call("level_has_melted", int(level), _p(out))
+        return out
+
     def set_schedule(self, schedule: str):
         """'atomic' (default: one launch per level and application) or
         'coloured' (eight launches, a fixed order of additions)."""

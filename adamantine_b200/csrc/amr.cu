@@ -838,6 +838,7 @@ public:
     int const ns = mesh_.cfg.n_states;
     fork();
     old.states.resize(levels_.size());
+    old.melted.resize(levels_.size());
     old.pitch.assign(levels_.size(), 0);
     old.nn1.assign(levels_.size(), 0);
     for (size_t l = 0; l < levels_.size(); ++l)
@@ -847,6 +848,7 @@ public:
       levels_[l]->set_state_to_material_properties();
       old.states[l].resize(levels_[l]->n_cells() * ns);
       levels_[l]->get_cell_state(old.states[l].data());
+      old.melted[l] = levels_[l]->has_melted_cells();
       old.pitch[l] = levels_[l]->mesh().pitch;
       old.nn1[l] = levels_[l]->mesh().nn[1];
     }
@@ -1014,6 +1016,30 @@ public:
       }
   }
 
+  // ThermalPhysics::mark_has_melted on the refined mesh: the leaves whose
+  // cell average of the field exceeds threshold (flags stay set)
+  void mark_has_melted(double threshold)
+  {
+    require_ready();
+    Ordered ord(*this);
+    prolong(y_.p);
+    fork();
+    for (size_t l = 0; l < levels_.size(); ++l)
+      if (alive(l))
+        levels_[l]->mark_has_melted(threshold, src_lev_.p + lev_off_[l], nullptr);
+    join();
+  }
+
+  // the has_melted flags of a level grid's cells (host, cells of the grid)
+  void level_has_melted(int l, uint8_t *host)
+  {
+    require_ready();
+    Thermal *th = level(l);
+    if (!th)
+      throw Error(ADM_ERR_INVALID, "no leaves on this level");
+    std::copy(th->has_melted_cells().begin(), th->has_melted_cells().end(), host);
+  }
+
   // the cell states of a level grid (host, n_states x cells of the grid)
   void level_cell_state(int l, double *host)
   {
@@ -1117,6 +1143,7 @@ private:
       return true;
     }
     std::vector<std::vector<double>> states;
+    std::vector<std::vector<uint8_t>> melted;
     std::vector<int> pitch, nn1;
 
     // the old field at lattice node k: an old active leaf containing it
@@ -1165,8 +1192,9 @@ private:
       throw Error(ADM_ERR_INVALID, "internal: a new node lies in no old active leaf");
     }
 
-    // CellDataTransfer: the state of the new leaf (l, i, j, k)
-    void state_of(int l, int64_t i, int64_t j, int64_t k, int ns, double *out) const
+    // CellDataTransfer: the state and has_melted flag of the new leaf
+    // (l, i, j, k)
+    void state_of(int l, int64_t i, int64_t j, int64_t k, int ns, double *out, uint8_t *melt = nullptr) const
     {
       int m = forest.status(l, i, j, k);
       int64_t a = i, b = j, c = k;
@@ -1193,6 +1221,8 @@ private:
       int64_t const cell = forest.index(m, a, b, c);
       for (int q = 0; q < ns; ++q)
         out[q] = states[m][q * C + cell];
+      if (melt)
+        *melt = melted[m].empty() ? 0 : melted[m][cell];
     }
   };
 
@@ -1241,6 +1271,7 @@ private:
       if (old)
       {
         std::vector<double> st((size_t)C * ns, 0.0);
+        std::vector<uint8_t> melt(C, 0);
         for (int64_t k = 0; k < mesh_.forest.n(l, 2); ++k)
           for (int64_t j = 0; j < mesh_.forest.n(l, 1); ++j)
             for (int64_t i = 0; i < mesh_.forest.n(l, 0); ++i)
@@ -1249,12 +1280,13 @@ private:
               if (!act[cell])
                 continue;
               double v[3] = {0, 0, 0};
-              old->state_of(l, i, j, k, ns, v);
+              old->state_of(l, i, j, k, ns, v, &melt[cell]);
               for (int q = 0; q < ns; ++q)
                 st[(size_t)q * C + cell] = v[q];
             }
         th->set_cell_state(st.data());
         th->get_state_from_material_properties();
+        th->set_has_melted(melt.data());
       }
     }
     lev_off_.assign(L + 1, 0);
@@ -1768,6 +1800,22 @@ int adm_amr_level_cell_state(adm_amr *h, int level, double *host)
   return adm::guard([&] {
     ADM_REQUIRE(h && host, "null argument");
     h->a->level_cell_state(level, host);
+  });
+}
+
+int adm_amr_mark_has_melted(adm_amr *h, double threshold)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h, "null handle");
+    h->a->mark_has_melted(threshold);
+  });
+}
+
+int adm_amr_level_has_melted(adm_amr *h, int level, uint8_t *host)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && host, "null argument");
+    h->a->level_has_melted(level, host);
   });
 }
 

@@ -1173,6 +1173,15 @@ void Thermal::mark_has_melted(double threshold, double const *temperature, uint8
     std::memcpy(host, has_melted_.data(), C);
 }
 
+void Thermal::set_has_melted(uint8_t const *host)
+{
+  size_t const C = mesh_.n_cells;
+  for (size_t c = 0; c < C; ++c)
+    has_melted_[c] = host[c] ? 1 : 0;
+  ADM_CK(cudaMemcpyAsync(has_melted_d_.p, has_melted_.data(), C, cudaMemcpyHostToDevice, stream_));
+  ADM_CK(cudaStreamSynchronize(stream_));
+}
+
 void Thermal::activate_cells(int64_t const *cells, int64_t n, double new_temperature,
                              double const *cos_new, double const *sin_new, double *solution)
 {

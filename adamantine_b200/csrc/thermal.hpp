@@ -227,6 +227,10 @@ public:
   void set_cell_state(double const *host);
   void get_qp_powder(double *host);
   void mark_has_melted(double threshold, double const *temperature, uint8_t *host);
+  // the has_melted flags per cell (host copy) and their replacement (a
+  // refined mesh carries them through refinement)
+  std::vector<uint8_t> const &has_melted_cells() const { return has_melted_; }
+  void set_has_melted(uint8_t const *host);
   void activate_cells(int64_t const *cells, int64_t n, double new_temperature,
                       double const *cos_new, double const *sin_new, double *solution);
   void update_beam(int i, adm_source const &beam);

@@ -122,6 +122,13 @@ int adm_amr_level_cell_state(adm_amr *h, int level, double *host);
  * atomic schedule (default) launches once per level and application, the
  * coloured one eight times and adds in a fixed order (bit-reproducible). */
 int adm_amr_set_schedule(adm_amr *h, int schedule);
+/* ThermalPhysics::mark_has_melted on the refined mesh: every leaf whose
+ * cell average of the solution exceeds threshold is flagged (flags stay
+ * set); refine_and_transfer carries the flags like the cell states. */
+int adm_amr_mark_has_melted(adm_amr *h, double threshold);
+/* The has_melted flags of a level grid's cells (host array of the grid's
+ * cells; cells that are not leaves of the level are 0). */
+int adm_amr_level_has_melted(adm_amr *h, int level, uint8_t *host);
 int adm_amr_synchronize(adm_amr *h);
 
 #ifdef __cplusplus

@@ -159,3 +159,44 @@ def test_operator_with_inactive_coarse_cells(degree):
         g.vmult(dst, src)
         ref = o.vmult(y)
         assert np.abs(dst.cpu().numpy() - ref).max() <= 1e-10 * np.abs(ref).max()
+
+
+def test_has_melted_follows_refinement():
+    """refine_and_transfer carries the has_melted flags like the cell data
+    (application/adamantine.hh:339-376, 463-495): a refined leaf's children
+    take its flag, a coarsened family takes its first child's."""
+    cfg = amr_test_config(degree=2, n_cells=(6, 6, 2), boundary="adiabatic", max_power=40000.0)
+    g = AmrThermalPhysics(cfg, 2, initial_state=cfg.geometry.initial_state())
+    g.refine_mesh(0.0, 40e-6, 20, 2)
+    t = 0.0
+    for _ in range(20):
+        t = g.evolve_one_time_step(t, 2e-6)
+    g.mark_has_melted(600.0)
+
+    def flags():
+        out = {}
+        lv = g.leaves()
+        for l in sorted(set(lv[:, 0].tolist())):
+            f = g.level_has_melted(int(l))
+            n0, n1 = 6 << l, 6 << l
+            for c in lv[lv[:, 0] == l]:
+                out[tuple(int(v) for v in c)] = int(f[c[1] + n0 * (c[2] + n1 * c[3])])
+        return out
+
+    old = flags()
+    assert any(old.values()) and not all(old.values())
+    g.refine_mesh(t, t + 40e-6, 20, 2, True)
+    new = flags()
+    assert set(new) != set(old)
+    for (l, i, j, k), f in new.items():
+        src = None
+        for m in range(l, -1, -1):
+            s = l - m
+            if (m, i >> s, j >> s, k >> s) in old:
+                src = (m, i >> s, j >> s, k >> s)
+                break
+        if src is None:  # coarsened: the first child, down to an old leaf
+            src = (l, i, j, k)
+            while src not in old:
+                src = (src[0] + 1, 2 * src[1], 2 * src[2], 2 * src[3])
+        assert f == old[src], ((l, i, j, k), src)
