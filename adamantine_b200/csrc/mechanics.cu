@@ -65,6 +65,12 @@ __global__ void __launch_bounds__(128) elastic_apply_kernel(MechArgs a, double c
 {
   __shared__ double u[4][3][32];
   __shared__ double S[4][32][9];
+  // the gradient table in shared memory: the lanes of a warp read
+  // different quadrature points' rows, which constant memory serializes
+  __shared__ double grad_s[kMaxN * kMaxN * 3];
+  for (int e = threadIdx.x; e < kMaxN * kMaxN * 3; e += blockDim.x)
+    grad_s[e] = c_grad[e];
+  __syncthreads();
   int const w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int const G = 32 / a.N; // cells per warp
   int const g = lane / a.N, l = lane - g * a.N;
@@ -104,7 +110,7 @@ __global__ void __launch_bounds__(128) elastic_apply_kernel(MechArgs a, double c
         {
           double s = 0.0;
           for (int n = 0; n < a.N; ++n)
-            s = fma(uc[comp * 32 + n], c_grad[(q * kMaxN + n) * 3 + d], s);
+            s = fma(uc[comp * 32 + n], grad_s[(q * kMaxN + n) * 3 + d], s);
           G3[comp][d] = s * a.inv_h[d];
         }
       double const div = G3[0][0] + G3[1][1] + G3[2][2];
@@ -124,7 +130,7 @@ __global__ void __launch_bounds__(128) elastic_apply_kernel(MechArgs a, double c
         double r = 0.0;
         for (int q = 0; q < a.N; ++q)
           for (int d = 0; d < 3; ++d)
-            r = fma(S[w][g * a.N + q][comp * 3 + d], c_grad[(q * kMaxN + n) * 3 + d] * a.inv_h[d], r);
+            r = fma(S[w][g * a.N + q][comp * 3 + d], grad_s[(q * kMaxN + n) * 3 + d] * a.inv_h[d], r);
         atomicAdd(dst + comp * a.m + gidx, r);
       }
     }
