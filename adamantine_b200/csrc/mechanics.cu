@@ -143,6 +143,15 @@ __global__ void __launch_bounds__(128) elastic_rhs_kernel(MechArgs a, double con
 {
   __shared__ double Tn[4][kMaxN];
   __shared__ double B[4][kMaxN], F[4][kMaxN];
+  // the tables in shared memory (lane-divergent rows; see the operator)
+  __shared__ double val_s[kMaxN * kMaxN], grad_s[kMaxN * kMaxN * 3];
+  for (int e = threadIdx.x; e < kMaxN * kMaxN * 3; e += blockDim.x)
+  {
+    grad_s[e] = c_grad[e];
+    if (e < kMaxN * kMaxN)
+      val_s[e] = c_val[e];
+  }
+  __syncthreads();
   int const w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int const gw = blockIdx.x * 4 + w, nw = gridDim.x * 4;
   for (int ci = gw; ci < a.n_cells; ci += nw)
@@ -168,7 +177,7 @@ __global__ void __launch_bounds__(128) elastic_rhs_kernel(MechArgs a, double con
       {
         double dT = -tref;
         for (int n = 0; n < a.N; ++n)
-          dT = fma(c_val[q * kMaxN + n], Tn[w][n], dT);
+          dT = fma(val_s[q * kMaxN + n], Tn[w][n], dT);
         b = (3.0 * lam + 2.0 * mu) * a.alpha[mat] * dT;
       }
       B[w][q] = jw * b;
@@ -183,9 +192,9 @@ __global__ void __launch_bounds__(128) elastic_rhs_kernel(MechArgs a, double con
         double r = 0.0;
         for (int q = 0; q < a.N; ++q)
         {
-          r = fma(B[w][q], c_grad[(q * kMaxN + n) * 3 + comp] * a.inv_h[comp], r);
+          r = fma(B[w][q], grad_s[(q * kMaxN + n) * 3 + comp] * a.inv_h[comp], r);
           if (comp == 2)
-            r = fma(F[w][q], c_val[q * kMaxN + n], r);
+            r = fma(F[w][q], val_s[q * kMaxN + n], r);
         }
         atomicAdd(rhs + comp * a.m + g, r);
       }
@@ -197,6 +206,10 @@ __global__ void __launch_bounds__(128) elastic_rhs_kernel(MechArgs a, double con
 // diag += the operator's diagonal on the free rows
 __global__ void __launch_bounds__(128) elastic_diag_kernel(MechArgs a, double *diag)
 {
+  __shared__ double grad_s[kMaxN * kMaxN * 3];
+  for (int e = threadIdx.x; e < kMaxN * kMaxN * 3; e += blockDim.x)
+    grad_s[e] = c_grad[e];
+  __syncthreads();
   int const w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int const gw = blockIdx.x * 4 + w, nw = gridDim.x * 4;
   for (int ci = gw; ci < a.n_cells; ci += nw)
@@ -219,7 +232,7 @@ __global__ void __launch_bounds__(128) elastic_diag_kernel(MechArgs a, double *d
         double gg = 0.0, gc = 0.0;
         for (int d = 0; d < 3; ++d)
         {
-          double const gd = c_grad[(q * kMaxN + n) * 3 + d] * a.inv_h[d];
+          double const gd = grad_s[(q * kMaxN + n) * 3 + d] * a.inv_h[d];
           gg += gd * gd;
           if (d == comp)
             gc = gd;
