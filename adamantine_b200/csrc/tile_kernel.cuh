@@ -126,6 +126,90 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, long l
   return false;
 }
 
+// ------------------------------------------------------------ 1D contractions
+// Known entries of the FE_Q(2) one-dimensional matrices. The middle Gauss
+// point 1/2 is also the middle support point, so S[1] = (0, 1, 0) and
+// G[1] = (-1, 0, 1) (nodal-basis derivative at 1/2 on [0, 1]), and the
+// symmetric points give D[1][1] = 0 (collocation derivative); the host checks
+// these entries when it builds the rule (check_q2_structure). Contractions
+// skip zero entries and add or subtract for unit ones. That is exact: an FMA
+// with a zero coefficient returns its addend, and one with a unit coefficient
+// rounds the same sum as the addition.
+enum CoefKind
+{
+  K_GEN = 0,
+  K_ZERO,
+  K_ONE,
+  K_MONE
+};
+enum OneDMatrix
+{
+  M_S = 0, // S[q][i] = phi_i(x_q)
+  M_G,     // G[q][i] = phi_i'(x_q)
+  M_D      // D[q][j] = l_j'(x_q), Lagrange basis through the Gauss points
+};
+template <int DEG, int MAT>
+__device__ __forceinline__ constexpr int coef_kind(int q, int k)
+{
+  if (DEG != 2 || q != 1)
+    return K_GEN;
+  if (MAT == M_S)
+    return k == 1 ? K_ONE : K_ZERO;
+  if (MAT == M_G)
+    return k == 1 ? K_ZERO : (k == 0 ? K_MONE : K_ONE);
+  return k == 1 ? K_ZERO : K_GEN;
+}
+// sum_k M[q][k] u[k * st] (row contraction); q and the loop index are
+// compile-time constants after unrolling, so the kinds fold away
+template <int DEG, int MAT>
+__device__ __forceinline__ double row_dot(double const (&M)[3][3], int q, double const *u, int st)
+{
+  double acc = 0.0;
+  bool started = false;
+#pragma unroll
+  for (int k = 0; k < DEG + 1; ++k)
+  {
+    int const kd = coef_kind<DEG, MAT>(q, k);
+    double const v = u[k * st];
+    if (kd == K_ZERO)
+      continue;
+    if (!started)
+      acc = kd == K_ONE ? v : (kd == K_MONE ? -v : M[q][k] * v);
+    else
+      acc = kd == K_ONE ? acc + v : (kd == K_MONE ? acc - v : fma(M[q][k], v, acc));
+    started = true;
+  }
+  return acc;
+}
+// sum_q M[q][n] u[q * st] (column contraction, the transpose)
+template <int DEG, int MAT>
+__device__ __forceinline__ double col_dot(double const (&M)[3][3], int n, double const *u, int st)
+{
+  double acc = 0.0;
+  bool started = false;
+#pragma unroll
+  for (int q = 0; q < DEG + 1; ++q)
+  {
+    int const kd = coef_kind<DEG, MAT>(q, n);
+    double const v = u[q * st];
+    if (kd == K_ZERO)
+      continue;
+    if (!started)
+      acc = kd == K_ONE ? v : (kd == K_MONE ? -v : M[q][n] * v);
+    else
+      acc = kd == K_ONE ? acc + v : (kd == K_MONE ? acc - v : fma(M[q][n], v, acc));
+    started = true;
+  }
+  return acc;
+}
+// acc + M[q][k] * v for one entry of known kind
+template <int DEG, int MAT>
+__device__ __forceinline__ double entry_mac(double const (&M)[3][3], int q, int k, double v, double acc)
+{
+  int const kd = coef_kind<DEG, MAT>(q, k);
+  return kd == K_ZERO ? acc : (kd == K_ONE ? acc + v : (kd == K_MONE ? acc - v : fma(M[q][k], v, acc)));
+}
+
 struct SmemPhys
 {
   double poly[kMaxMaterials][kNStateProps][kMaxStates][kMaxPoly];
@@ -586,13 +670,7 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
         double t[N];
 #pragma unroll
         for (int q = 0; q < N; ++q)
-        {
-          double acc = args.S[q][0] * wv[N * j];
-#pragma unroll
-          for (int k = 1; k < N; ++k)
-            acc = fma(args.S[q][k], wv[k + N * j], acc);
-          t[q] = acc;
-        }
+          t[q] = row_dot<DEG, M_S>(args.S, q, &wv[N * j], 1);
 #pragma unroll
         for (int q = 0; q < N; ++q)
           wv[q + N * j] = t[q];
@@ -603,13 +681,7 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
         double t[N];
 #pragma unroll
         for (int q = 0; q < N; ++q)
-        {
-          double acc = args.S[q][0] * wv[i];
-#pragma unroll
-          for (int k = 1; k < N; ++k)
-            acc = fma(args.S[q][k], wv[i + N * k], acc);
-          t[q] = acc;
-        }
+          t[q] = row_dot<DEG, M_S>(args.S, q, &wv[i], N);
 #pragma unroll
         for (int q = 0; q < N; ++q)
           wv[i + N * q] = t[q];
@@ -682,18 +754,68 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
       constexpr int PS = kMaxStates * kMaxPoly; // stride between properties
       double const *cold_c = &sp.poly[mat][0][cold < 0 ? 0 : cold][0];
       double const *cw = &args.cw[NQS * slab][0];
+      // every point of this level cold: one straight-line pass (no branch
+      // per point, so the points' dependency chains interleave)
+      bool all_cold = cold >= 0;
+      if (NS > 1)
+      {
+#pragma unroll
+        for (int i = 0; i < NQS; ++i)
+          all_cold &= Tq[i] < solidus;
+      }
+      if (all_cold)
+      {
+        double crho[P + 1], ccp[P + 1], ck[P + 1];
+#pragma unroll
+        for (int k = 0; k <= P; ++k)
+        {
+          crho[k] = cold_c[P_DENSITY * PS + k];
+          ccp[k] = cold_c[P_SPECIFIC_HEAT * PS + k];
+          ck[k] = cold_c[P_KX * PS + k];
+        }
+#pragma unroll
+        for (int i = 0; i < NQS; ++i)
+        {
+          int const qa = i % N, qb = i / N;
+          double const T = Tq[i];
+          double const gx = row_dot<DEG, M_D>(args.D, qa, &Tq[N * qb], 1);
+          double const gy = row_dot<DEG, M_D>(args.D, qb, &Tq[qa], N);
+          double const inv = recip(horner_fixed<P>(crho, T) * horner_fixed<P>(ccp, T));
+          double const cf = -inv * horner_fixed<P>(ck, T);
+          double const fx = (cf * cw[4 * i + 0]) * gx;
+          double const fy = (cf * cw[4 * i + 1]) * gy;
+          az[i] = (cf * cw[4 * i + 2]) * az[i];
+#pragma unroll
+          for (int m = 0; m < N; ++m)
+          {
+            axy[m + N * qb] = entry_mac<DEG, M_D>(args.D, qa, m, fx, axy[m + N * qb]);
+            axy[qa + N * m] = entry_mac<DEG, M_D>(args.D, qb, m, fy, axy[qa + N * m]);
+          }
+        }
+        if (do_src)
+        {
+#pragma unroll
+          for (int i = 0; i < NQS; ++i)
+          {
+            int const qa = i % N, qb = i / N;
+            double const T = Tq[i];
+            double const inv = recip(horner_fixed<P>(crho, T) * horner_fixed<P>(ccp, T));
+            double const px = (args.origin[0] + cx * args.h[0]) + args.qx[qa] * args.h[0];
+            double const py = (args.origin[1] + cy * args.h[1]) + args.qx[qb] * args.h[1];
+            double const pz = (args.origin[2] + cz * args.h[2]) + args.qx[slab] * args.h[2];
+            axy[i] += beam_sum(sp, px, py, pz) * inv * cw[4 * i + 3];
+          }
+        }
+      }
+      else
+      {
 #pragma unroll
       for (int i = 0; i < NQS; ++i)
       {
         int const qa = i % N, qb = i / N;
         double const T = Tq[i];
-        double gx = 0.0, gy = 0.0;
-#pragma unroll
-        for (int k = 0; k < N; ++k)
-        {
-          gx = fma(args.D[qa][k], Tq[k + N * qb], gx);
-          gy = fma(args.D[qb][k], Tq[qa + N * k], gy);
-        }
+        double const gx = row_dot<DEG, M_D>(args.D, qa, &Tq[N * qb], 1);
+        double const gy = row_dot<DEG, M_D>(args.D, qb, &Tq[qa], N);
         double const gz = az[i];
         double inv, fx, fy, fz;
         if (cold >= 0 && (NS == 1 || T < solidus))
@@ -765,8 +887,8 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
 #pragma unroll
         for (int m = 0; m < N; ++m)
         {
-          axy[m + N * qb] = fma(args.D[qa][m], fx, axy[m + N * qb]);
-          axy[qa + N * m] = fma(args.D[qb][m], fy, axy[qa + N * m]);
+          axy[m + N * qb] = entry_mac<DEG, M_D>(args.D, qa, m, fx, axy[m + N * qb]);
+          axy[qa + N * m] = entry_mac<DEG, M_D>(args.D, qb, m, fy, axy[qa + N * m]);
         }
         if (do_src)
         {
@@ -775,6 +897,7 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
           double const pz = (args.origin[2] + cz * args.h[2]) + args.qx[slab] * args.h[2];
           axy[i] += beam_sum(sp, px, py, pz) * inv * cw[4 * i + 3];
         }
+      }
       }
       if (NS == 3 && pmode != 2 && changed_mask)
         changed[cl] = 1;
@@ -790,13 +913,7 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
         double t[N];
 #pragma unroll
         for (int n = 0; n < N; ++n)
-        {
-          double acc = args.S[0][n] * a[N * j];
-#pragma unroll
-          for (int q = 1; q < N; ++q)
-            acc = fma(args.S[q][n], a[q + N * j], acc);
-          t[n] = acc;
-        }
+          t[n] = col_dot<DEG, M_S>(args.S, n, &a[N * j], 1);
 #pragma unroll
         for (int n = 0; n < N; ++n)
           a[n + N * j] = t[n];
@@ -807,13 +924,7 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
         double t[N];
 #pragma unroll
         for (int n = 0; n < N; ++n)
-        {
-          double acc = args.S[0][n] * a[i];
-#pragma unroll
-          for (int q = 1; q < N; ++q)
-            acc = fma(args.S[q][n], a[i + N * q], acc);
-          t[n] = acc;
-        }
+          t[n] = col_dot<DEG, M_S>(args.S, n, &a[i], N);
 #pragma unroll
         for (int n = 0; n < N; ++n)
           a[i + N * n] = t[n];
