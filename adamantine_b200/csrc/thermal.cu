@@ -47,6 +47,17 @@ void lagrange(int n, long double const *nodes, long double x, long double *v,
   }
 }
 
+// The tile kernel's FE_Q(2) contractions skip the entries of the middle Gauss
+// point's rows that are exactly 0 or +-1 (S[1] = (0, 1, 0), G[1] = (-1, 0, 1),
+// D[1][1] = 0); this checks that the computed rule has them.
+void check_q2_structure(Rule1D const &r)
+{
+  bool const ok = r.S[1][0] == 0.0 && r.S[1][1] == 1.0 && r.S[1][2] == 0.0 && r.G[1][0] == -1.0 &&
+                  r.G[1][1] == 0.0 && r.G[1][2] == 1.0 && r.D[1][1] == 0.0;
+  if (!ok)
+    throw Error(ADM_ERR_UNSUPPORTED, "FE_Q(2) Gauss rule lacks the exact middle-point entries the kernels assume");
+}
+
 Rule1D make_rule(int deg, bool lobatto)
 {
   Rule1D r;
@@ -110,6 +121,8 @@ Rule1D make_rule(int deg, bool lobatto)
     for (int j = 0; j < n; ++j)
       r.D[q][j] = (double)dv[j];
   }
+  if (deg == 2 && !lobatto)
+    check_q2_structure(r);
   return r;
 }
 } // namespace

@@ -66,11 +66,12 @@ struct TD
   static constexpr int NF = N * N;
   // nodes each thread writes back
   static constexpr int WIT = (BRICK + NT - 1) / NT;
-  // dynamic shared memory: two staged bricks, the level exchange / per-cell
-  // result buffer [NN][NCELL], the flux exchange [2][NN][NCELL], per-cell
-  // liquid partial sums [N][NCELL] and powder-change flags [NCELL]
+  // dynamic shared memory: two staged bricks, the level exchange
+  // [NN][NCELL], the flux exchange [2][NN][NCELL], the z-shared node sums
+  // [NQS][NCELL], per-cell liquid partial sums [N][NCELL] and powder-change
+  // flags [2][NCELL] (one set per item parity)
   static constexpr size_t SMEM =
-      sizeof(double) * (2 * BRICKP + 3 * NN * NCELL + N * NCELL) + sizeof(int) * NCELL;
+      sizeof(double) * (2 * BRICKP + 3 * NN * NCELL + NQS * NCELL + N * NCELL) + sizeof(int) * 2 * NCELL;
 };
 
 // ------------------------------------------------------------ TMA + mbarrier
@@ -220,7 +221,7 @@ struct SmemPhys
   int n_materials, use_table, isotropic, n_beams;
   int has_rotation, sources_here;
   int member;
-  int role[27];
+  int role[2][27]; // per item parity
 };
 
 // ------------------------------------------------------------ properties
@@ -497,10 +498,11 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
   constexpr int WIT = T_::WIT;
   constexpr unsigned kBoxBytes = sizeof(double) * BXP * BY * BZ;
   extern __shared__ __align__(128) double smem[];
-  double *const xbuf = smem + 2 * T_::BRICKP;  // [NN][NCELL]: levels, then results
+  double *const xbuf = smem + 2 * T_::BRICKP;  // [NN][NCELL]: level exchange
   double *const pzbuf = xbuf + NN * NCELL;     // [2][NN][NCELL]: flux exchange
-  double *const lsum = pzbuf + 2 * NN * NCELL; // [N][NCELL]
-  int *const changed = reinterpret_cast<int *>(lsum + N * NCELL); // [NCELL]
+  double *const mbuf = pzbuf + 2 * NN * NCELL; // [NQS][NCELL]: z-shared node sums
+  double *const lsum = mbuf + NQS * NCELL;     // [N][NCELL]
+  int *const changed_p = reinterpret_cast<int *>(lsum + N * NCELL); // [2][NCELL]
   __shared__ SmemPhys sp;
   __shared__ __align__(8) uint64_t bars[2];
 
@@ -546,12 +548,46 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
   if (tid == 0 && first < last)
     issue(0, first);
 
+  // The work item and this thread's cell data (info word, powder mode and
+  // uniform powder value) are loaded one item ahead, so that their
+  // dependent global loads overlap the previous item's arithmetic.
+  TileWork nx_w{0, 0, 0u};
+  uint32_t nx_info = 0u;
+  int nx_pmode = 0;
+  double nx_pu = 0.0;
+  auto load_item = [&](int item2) {
+    nx_w = args.work[item2];
+    MemberData const &mk = args.members[nx_w.member];
+    int const kx = TX * (int)(nx_w.xyz & 2047u) + lx, ky = TY * (int)((nx_w.xyz >> 11) & 2047u) + ly,
+              kz = TZ * (int)(nx_w.xyz >> 22) + lz;
+    nx_info = 0u;
+    nx_pmode = 0;
+    nx_pu = 0.0;
+    if (kx < args.nc[0] && ky < args.nc[1] && kz < args.nc[2])
+    {
+      size_t const kc = kx + (size_t)args.nc[0] * (ky + (size_t)args.nc[1] * kz);
+      nx_info = mk.cell_info[kc];
+      if (NS == 3)
+      {
+        nx_pmode = mk.powder_mode[kc];
+        nx_pu = mk.powder_cell[kc];
+      }
+    }
+  };
+  if (first < last)
+    load_item(first);
+
   int it = 0;
   for (int item = first; item < last; item += step, ++it)
   {
     int const buf = it & 1;
     double const *brick = smem + buf * T_::BRICKP;
-    TileWork const w = args.work[item];
+    TileWork const w = nx_w;
+    uint32_t const cur_info = nx_info;
+    int const cur_pmode = nx_pmode;
+    double const cur_pu = nx_pu;
+    if (item + step < last)
+      load_item(item + step);
     MemberData const &md = args.members[w.member];
     MaterialDesc const *gm = md.mat;
     int const tile = w.tile;
@@ -560,14 +596,14 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
     int const ncx0 = TX * tix, ncy0 = TY * tiy, ncz0 = TZ * tiz;      // first cell
     int const nx0 = DEG * ncx0, ny0 = DEG * ncy0, nz0 = DEG * ncz0; // first node
     double *const y = args.y_override ? args.y_override : md.y;
-
-    // prefetch the next item's brick into the other buffer (its previous
-    // contents were consumed before the barrier that ended the last item)
-    if (tid == 0 && item + step < last)
-    {
-      fence_proxy_async();
-      issue(buf ^ 1, item + step);
-    }
+    // Three CTA barriers per item: the level exchange (which also publishes
+    // this item's roles and cleared flags and carries the brick-timeout
+    // vote), the flux exchange and the z-shared node sums. Per-item shared
+    // state that a thread still finishing the previous item may read (roles,
+    // powder-change flags) alternates between two copies by item parity;
+    // the next brick is requested after the first barrier, when every
+    // thread has finished the previous item and no longer reads its buffer.
+    int *const changed = changed_p + buf * NCELL;
     if (sp.member != w.member)
     {
       load_member_constants<NT>(sp, md, tid);
@@ -599,24 +635,14 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
         cmin = c < cmin ? c : cmin;
         cmax = c > cmax ? c : cmax;
       }
-      sp.role[tid] = (colour == cmin ? 1 : 0) | (colour == cmax ? 2 : 0);
+      sp.role[buf][tid] = (colour == cmin ? 1 : 0) | (colour == cmax ? 2 : 0);
     }
     if (slab == 0)
       changed[cl] = 0;
-    // wait for this item's brick (bounded; every thread polls); the barrier
-    // also publishes the role table and the cleared flags
+    // wait for this item's brick (bounded; every thread polls); a thread
+    // whose wait gave up computes on whatever the buffer holds and the vote
+    // at the level-exchange barrier ends the CTA before anything is written
     bool const arrived = mbar_wait(&bars[buf], (unsigned)((it >> 1) & 1));
-    if (__syncthreads_or(!arrived))
-    {
-      if (tid == 0)
-      {
-        atomicCAS(md.error, 0, (int)DERR_TMA_TIMEOUT);
-        // let a prefetch still in flight land before the CTA leaves
-        if (item + step < last)
-          mbar_wait(&bars[buf ^ 1], (unsigned)(((it + 1) >> 1) & 1));
-      }
-      return;
-    }
 
     // Tile-level source culling, evaluated by every thread (exact: it skips
     // only points where every source is zero by its own cutoff rules).
@@ -653,7 +679,7 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
     int const cx = ncx0 + lx, cy = ncy0 + ly, cz = ncz0 + lz;
     bool const in_domain = cx < args.nc[0] && cy < args.nc[1] && cz < args.nc[2];
     size_t const c = in_domain ? cx + (size_t)args.nc[0] * (cy + (size_t)args.nc[1] * cz) : 0;
-    uint32_t const info = in_domain ? md.cell_info[c] : 0u;
+    uint32_t const info = cur_info;
     bool const active = (info & CI_ACTIVE) != 0;
     int const mat = (info >> CI_MAT_SHIFT) & 15;
     // 1. x/y interpolation of the nodes of z-level `slab` (in registers)
@@ -692,7 +718,22 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
 #pragma unroll
     for (int i = 0; i < NQS; ++i)
       xbuf[(i + NQS * slab) * NCELL + cl] = wv[i];
-    __syncthreads();
+    if (__syncthreads_or(!arrived))
+    {
+      if (tid == 0)
+      {
+        atomicCAS(md.error, 0, (int)DERR_TMA_TIMEOUT);
+        // let the late copy land before the CTA leaves (bounded as well)
+        mbar_wait(&bars[buf], (unsigned)((it >> 1) & 1));
+      }
+      return;
+    }
+    // prefetch the next item's brick into the other buffer
+    if (tid == 0 && item + step < last)
+    {
+      fence_proxy_async();
+      issue(buf ^ 1, item + step);
+    }
     double Tq[NQS], az[NQS];
 #pragma unroll
     for (int i = 0; i < NQS; ++i)
@@ -724,9 +765,9 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
       size_t const pbase = c * NN + (size_t)NQS * slab;
       if (NS == 3)
       {
-        pmode = md.powder_mode[c];
+        pmode = cur_pmode;
         if (pmode == 1)
-          pu = md.powder_cell[c];
+          pu = cur_pu;
       }
       double cs = 1.0, sn = 0.0;
       if (sp.has_rotation)
@@ -1079,14 +1120,14 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
     {
 #pragma unroll
       for (int i = 0; i < NQS; ++i)
-        xbuf[i * NCELL + cl] = res[i];
+        mbuf[i * NCELL + cl] = res[i];
     }
     __syncthreads();
     if (slab == DEG && lz < TZ - 1)
     {
 #pragma unroll
       for (int i = 0; i < NQS; ++i)
-        res[i] += xbuf[i * NCELL + cl + TX * TY];
+        res[i] += mbuf[i * NCELL + cl + TX * TY];
     }
 
     // ---- state write-back
@@ -1133,7 +1174,7 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
       bool const inside = gx < args.nn[0] && gy < nn1 && gz < args.nn[2];
       int const sx = (X == 0 && tix > 0) ? 1 : ((X == DEG * TX && tix < nt0 - 1) ? 2 : 0);
       int const sy = (Y == 0 && tiy > 0) ? 1 : ((Y == DEG * TY && tiy < nt1 - 1) ? 2 : 0);
-      rl[i] = (own && inside) ? (AT ? 4 : (sp.role[sx + 3 * sy + 9 * sz] | 4)) : 0;
+      rl[i] = (own && inside) ? (AT ? 4 : (sp.role[buf][sx + 3 * sy + 9 * sz] | 4)) : 0;
       gidx[i] = gx + (size_t)pitch * (gy + (size_t)nn1 * gz);
     }
     if constexpr (AT)
@@ -1220,7 +1261,6 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
           args.vdst[args.nn[0] + X + (size_t)pitch * (gy + (size_t)nn1 * gz)] = 0.0;
       }
     }
-    __syncthreads();
   }
 }
 
