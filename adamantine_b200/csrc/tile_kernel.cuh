@@ -451,6 +451,205 @@ static __device__ __noinline__ double beam_sum(SmemPhys const &sp, double px, do
   return qs;
 }
 
+// The quadrature points of one node level of a cell on the general path
+// (update_state_ratios, get_inv_rho_cp and the conductivity of
+// source/ThermalOperator.templates.hh:227-617): per point the phase-state
+// update with its history write, the material evaluation (pure-state
+// polynomials inline, everything else in qp_general), the fluxes and their
+// collocation D^T in x/y, and the source. Tq holds the level's temperatures,
+// az its z-gradients on entry and the z fluxes on return; axy accumulates.
+template <int DEG, int NS, int P>
+__device__ __noinline__ void general_level(SmemPhys const &sp, MaterialDesc const *gm, MemberData const &md,
+                                           KernelArgs const &args, int mat, int slab, int cold, int pmode,
+                                           double pu, size_t pbase, double cs, double sn, bool fast_ok,
+                                           bool do_src, int cx, int cy, int cz, double const *__restrict__ Tq,
+                                           double *__restrict__ az, double *__restrict__ axy,
+                                           double *__restrict__ liquid_out, uint32_t *__restrict__ changed_out)
+{
+  constexpr int N = DEG + 1, NQS = N * N;
+  constexpr int PS = kMaxStates * kMaxPoly; // stride between properties
+  double const solidus = sp.props[mat][Q_SOLIDUS];
+  double const *cold_c = &sp.poly[mat][0][cold < 0 ? 0 : cold][0];
+  double const *cw = &args.cw[NQS * slab][0];
+  double liquid_acc = 0.0;
+  uint32_t changed_mask = 0;
+#pragma unroll
+  for (int i = 0; i < NQS; ++i)
+  {
+    int const qa = i % N, qb = i / N;
+    double const T = Tq[i];
+    double const gx = row_dot<DEG, M_D>(args.D, qa, &Tq[N * qb], 1);
+    double const gy = row_dot<DEG, M_D>(args.D, qb, &Tq[qa], N);
+    double const gz = az[i];
+    double inv, fx, fy, fz;
+    if (cold >= 0 && (NS == 1 || T < solidus))
+    {
+      // one state, polynomial, isotropic: Horner in that state only; cw
+      // holds W_q * vol / h_d^2 and W_q * vol for this point
+      double const rho = horner_fixed<P>(cold_c + P_DENSITY * PS, T);
+      double const cp = horner_fixed<P>(cold_c + P_SPECIFIC_HEAT * PS, T);
+      inv = recip(rho * cp);
+      double const cf = -inv * horner_fixed<P>(cold_c + P_KX * PS, T);
+      fx = (cf * cw[4 * i + 0]) * gx;
+      fy = (cf * cw[4 * i + 1]) * gy;
+      fz = (cf * cw[4 * i + 2]) * gz;
+    }
+    else
+    {
+      double p_old = 0.0;
+      if (NS == 3)
+        p_old = (pmode == 2) ? md.powder_q[pbase + i] : pu;
+      double r0, r1 = 0.0, r2 = 0.0;
+      double liquid = 0.0, p_new = p_old;
+      int pure;
+      {
+        double rat[NS > 1 ? NS : 1];
+        pure = state_ratios<NS>(sp, mat, T, p_old, rat, liquid, p_new);
+        r0 = rat[0];
+        if (NS > 1)
+          r1 = rat[1];
+        if (NS > 2)
+          r2 = rat[NS > 2 ? 2 : 0];
+      }
+      if (NS > 1)
+        liquid_acc += liquid;
+      if (NS == 3 && p_new != p_old)
+      {
+        md.powder_q[pbase + i] = p_new;
+        changed_mask |= 1u << i;
+      }
+      double kxx, kxy, kyy, kzz;
+      if (fast_ok && pure >= 0)
+      {
+        double const *cc = &sp.poly[mat][0][NS == 1 ? 0 : pure][0];
+        double const rho = horner_fixed<P>(cc + P_DENSITY * PS, T);
+        double const cp = horner_fixed<P>(cc + P_SPECIFIC_HEAT * PS, T);
+        inv = recip(rho * cp);
+        kxx = horner_fixed<P>(cc + P_KX * PS, T);
+        kyy = kxx;
+        kzz = kxx;
+        kxy = 0.0;
+      }
+      else
+      {
+        QpCoef kk;
+        qp_general<NS>(sp, gm, mat, r0, r1, r2, pure, T, cs, sn, kk);
+        inv = kk.inv;
+        kxx = kk.kxx;
+        kxy = kk.kxy;
+        kyy = kk.kyy;
+        kzz = kk.kzz;
+      }
+      double const W = args.qw[qa] * args.qw[qb] * args.qw[slab];
+      double const grx = gx * args.inv_h[0], gry = gy * args.inv_h[1];
+      double const cf = -inv * W;
+      fx = cf * (kxx * grx + kxy * gry) * args.vol_over_h[0];
+      fy = cf * (kxy * grx + kyy * gry) * args.vol_over_h[1];
+      fz = cf * kzz * gz * args.vol_over_h2[2];
+    }
+    az[i] = fz;
+#pragma unroll
+    for (int m = 0; m < N; ++m)
+    {
+      axy[m + N * qb] = entry_mac<DEG, M_D>(args.D, qa, m, fx, axy[m + N * qb]);
+      axy[qa + N * m] = entry_mac<DEG, M_D>(args.D, qb, m, fy, axy[qa + N * m]);
+    }
+    if (do_src)
+    {
+      double const px = (args.origin[0] + cx * args.h[0]) + args.qx[qa] * args.h[0];
+      double const py = (args.origin[1] + cy * args.h[1]) + args.qx[qb] * args.h[1];
+      double const pz = (args.origin[2] + cz * args.h[2]) + args.qx[slab] * args.h[2];
+      axy[i] += beam_sum(sp, px, py, pz) * inv * cw[4 * i + 3];
+    }
+  }
+  *liquid_out = liquid_acc;
+  *changed_out = changed_mask;
+}
+
+// Convective / radiative face terms of one cell (face_local_apply,
+// source/ThermalOperator.templates.hh:619-751) for the node level `slab`:
+// every level thread of a cell evaluates the face quadrature and keeps the
+// test functions of its own level; out[e] receives the contribution to the
+// level's node e.
+template <int DEG, int NS>
+__device__ __noinline__ void face_terms(SmemPhys const &sp, MaterialDesc const *gm, MemberData const &md,
+                                        KernelArgs const &args, double const *brick, int lx, int ly, int lz,
+                                        int slab, uint32_t info, int mat, size_t c, double *out)
+{
+  constexpr int N = DEG + 1, NQS = N * N;
+  constexpr int BXP = TD<DEG>::BXP, BY = TD<DEG>::BY;
+  for (int e = 0; e < NQS; ++e)
+    out[e] = 0.0;
+  int const slot = (NS == 3) ? md.face_slot[c] : -1;
+  for (int f = 0; f < 6; ++f)
+  {
+    if (!((info >> (CI_FACE_SHIFT + f)) & 1u))
+      continue;
+    int const d = f / 2, side = f % 2;
+    if (d == 2 && slab != (side ? N - 1 : 0))
+      continue; // a z face only touches one node level
+    int const t0 = d == 0 ? 1 : 0, t1 = d == 2 ? 1 : 2;
+    int const btype =
+        ((info >> (CI_INTERFACE_SHIFT + f)) & 1u) ? args.interface_type : args.boundary_type[f];
+    double const ht0 = args.h[t0], ht1 = args.h[t1];
+    for (int fq = 0; fq < N * N; ++fq)
+    {
+      int const qa = fq % N, qb = fq / N;
+      double T = 0.0;
+      for (int j = 0; j < N; ++j)
+        for (int i = 0; i < N; ++i)
+        {
+          int loc[3];
+          loc[d] = side ? N - 1 : 0;
+          loc[t0] = i;
+          loc[t1] = j;
+          double const u = brick[(DEG * lx + loc[0]) + BXP * ((DEG * ly + loc[1]) + BY * (DEG * lz + loc[2]))];
+          T += args.S[qa][i] * args.S[qb][j] * u;
+        }
+      double rat[NS > 1 ? NS : 1];
+      double liquid = 0.0, p_old = 0.0, p_new = 0.0;
+      double *ph = nullptr;
+      if (NS == 3 && slot >= 0)
+      {
+        ph = &md.face_powder[((size_t)slot * 6 + f) * (N * N) + fq];
+        p_old = *ph;
+      }
+      int const pure = state_ratios<NS>(sp, mat, T, p_old, rat, liquid, p_new);
+      // p_new = min(1 - l, p_old) is idempotent, so the other level threads
+      // of this cell compute the same value whether they read the history
+      // before or after this store
+      if (ph && (d == 2 || slab == 0) && p_new != p_old)
+        *ph = p_new;
+      double const inv = inv_rho_cp<NS>(sp, gm, mat, rat, pure, T);
+      double conv_tinf = 0.0, conv_h = 0.0, rad_tinf = 0.0, rad_h = 0.0;
+      if (btype & B_CONVECTIVE)
+      {
+        conv_tinf = sp.props[mat][Q_CONV_TINF];
+        conv_h = property<NS>(sp, gm, P_CONV_COEF, mat, rat, pure, T);
+      }
+      if (btype & B_RADIATIVE)
+      {
+        rad_tinf = sp.props[mat][Q_RAD_TINF];
+        rad_h = property<NS>(sp, gm, P_EMISSIVITY, mat, rat, pure, T) * 5.670374419e-8 * (T + rad_tinf) *
+                (T * T + rad_tinf * rad_tinf);
+      }
+      double const bval = -inv * (conv_h * (T - conv_tinf) + rad_h * (T - rad_tinf));
+      double const JxW = args.qw[qa] * ht0 * args.qw[qb] * ht1;
+      for (int j = 0; j < N; ++j)
+        for (int i = 0; i < N; ++i)
+        {
+          // node (la, lb, lc) of this face; kept if it is on level `slab`
+          int const la = d == 0 ? (side ? N - 1 : 0) : i;
+          int const lb = d == 0 ? i : (d == 1 ? (side ? N - 1 : 0) : j);
+          int const lc = d == 2 ? (side ? N - 1 : 0) : j;
+          if (lc != slab)
+            continue;
+          out[la + N * lb] += bval * (args.S[qa][i] * args.S[qb][j]) * JxW;
+        }
+    }
+  }
+}
+
 // ------------------------------------------------------------ the kernel
 // Loads the physics constants of a member into shared memory.
 template <int NT>
@@ -487,7 +686,9 @@ __device__ __forceinline__ void load_member_constants(SmemPhys &sp, MemberData c
 // The persistent tile loop: CTA b processes work items b, b + grid, ... of
 // one colour. The node brick of the next item is fetched by TMA into the
 // other buffer while the current item is computed.
-template <int DEG, int NS, int P, bool AT>
+// FC: the problem has convective / radiative faces (instantiated apart so
+// that adiabatic problems carry no face code).
+template <int DEG, int NS, int P, bool AT, bool FC>
 __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
     tile_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ KernelArgs args, int n_items)
 {
@@ -850,95 +1051,29 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
       }
       else
       {
+        // mixed states, the mushy range, tables, anisotropy or rotation: an
+        // out-of-line pass over the level's points on copies of the arrays
+        // (only threads near the melt or in partly melted powder take it)
+        double tq_l[NQS], az_l[NQS], axy_l[NQS];
 #pragma unroll
-      for (int i = 0; i < NQS; ++i)
-      {
-        int const qa = i % N, qb = i / N;
-        double const T = Tq[i];
-        double const gx = row_dot<DEG, M_D>(args.D, qa, &Tq[N * qb], 1);
-        double const gy = row_dot<DEG, M_D>(args.D, qb, &Tq[qa], N);
-        double const gz = az[i];
-        double inv, fx, fy, fz;
-        if (cold >= 0 && (NS == 1 || T < solidus))
+        for (int i = 0; i < NQS; ++i)
         {
-          // one state, polynomial, isotropic: Horner in that state only;
-          // cw holds W_q * vol / h_d^2 and W_q * vol for this point
-          double const rho = horner_fixed<P>(cold_c + P_DENSITY * PS, T);
-          double const cp = horner_fixed<P>(cold_c + P_SPECIFIC_HEAT * PS, T);
-          inv = recip(rho * cp);
-          double const cf = -inv * horner_fixed<P>(cold_c + P_KX * PS, T);
-          fx = (cf * cw[4 * i + 0]) * gx;
-          fy = (cf * cw[4 * i + 1]) * gy;
-          fz = (cf * cw[4 * i + 2]) * gz;
+          tq_l[i] = Tq[i];
+          az_l[i] = az[i];
+          axy_l[i] = axy[i];
         }
-        else
-        {
-          double p_old = 0.0;
-          if (NS == 3)
-            p_old = (pmode == 2) ? md.powder_q[pbase + i] : pu;
-          double r0, r1 = 0.0, r2 = 0.0;
-          double liquid = 0.0, p_new = p_old;
-          int pure;
-          {
-            double rat[NS > 1 ? NS : 1];
-            pure = state_ratios<NS>(sp, mat, T, p_old, rat, liquid, p_new);
-            r0 = rat[0];
-            if (NS > 1)
-              r1 = rat[1];
-            if (NS > 2)
-              r2 = rat[NS > 2 ? 2 : 0];
-          }
-          if (NS > 1)
-            liquid_acc += liquid;
-          if (NS == 3 && p_new != p_old)
-          {
-            md.powder_q[pbase + i] = p_new;
-            changed_mask |= 1u << i;
-          }
-          double kxx, kxy, kyy, kzz;
-          if (fast_ok && pure >= 0)
-          {
-            double const *cc = &sp.poly[mat][0][NS == 1 ? 0 : pure][0];
-            double const rho = horner_fixed<P>(cc + P_DENSITY * PS, T);
-            double const cp = horner_fixed<P>(cc + P_SPECIFIC_HEAT * PS, T);
-            inv = recip(rho * cp);
-            kxx = horner_fixed<P>(cc + P_KX * PS, T);
-            kyy = kxx;
-            kzz = kxx;
-            kxy = 0.0;
-          }
-          else
-          {
-            QpCoef kk;
-            qp_general<NS>(sp, gm, mat, r0, r1, r2, pure, T, cs, sn, kk);
-            inv = kk.inv;
-            kxx = kk.kxx;
-            kxy = kk.kxy;
-            kyy = kk.kyy;
-            kzz = kk.kzz;
-          }
-          double const W = args.qw[qa] * args.qw[qb] * args.qw[slab];
-          double const grx = gx * args.inv_h[0], gry = gy * args.inv_h[1];
-          double const cf = -inv * W;
-          fx = cf * (kxx * grx + kxy * gry) * args.vol_over_h[0];
-          fy = cf * (kxy * grx + kyy * gry) * args.vol_over_h[1];
-          fz = cf * kzz * gz * args.vol_over_h2[2];
-        }
-        az[i] = fz;
+        double lacc = 0.0;
+        uint32_t cmask = 0;
+        general_level<DEG, NS, P>(sp, gm, md, args, mat, slab, cold, pmode, pu, c * NN + (size_t)NQS * slab, cs, sn,
+                                  fast_ok, do_src, cx, cy, cz, tq_l, az_l, axy_l, &lacc, &cmask);
 #pragma unroll
-        for (int m = 0; m < N; ++m)
+        for (int i = 0; i < NQS; ++i)
         {
-          axy[m + N * qb] = entry_mac<DEG, M_D>(args.D, qa, m, fx, axy[m + N * qb]);
-          axy[qa + N * m] = entry_mac<DEG, M_D>(args.D, qb, m, fy, axy[qa + N * m]);
+          az[i] = az_l[i];
+          axy[i] = axy_l[i];
         }
-        if (do_src)
-        {
-          double const px = (args.origin[0] + cx * args.h[0]) + args.qx[qa] * args.h[0];
-          double const py = (args.origin[1] + cy * args.h[1]) + args.qx[qb] * args.h[1];
-          double const pz = (args.origin[2] + cz * args.h[2]) + args.qx[slab] * args.h[2];
-          axy[i] += beam_sum(sp, px, py, pz) * inv * cw[4 * i + 3];
-        }
-      }
+        liquid_acc = lacc;
+        changed_mask = cmask;
       }
       if (NS == 3 && pmode != 2 && changed_mask)
         changed[cl] = 1;
@@ -999,102 +1134,15 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
     }
 
     // ---- face terms of this node level (face_local_apply,
-    // source/ThermalOperator.templates.hh:619-751); every slab thread of a
-    // cell evaluates the face quadrature and keeps the test functions of its
-    // own node level
-    if (args.faces && active && ((info >> CI_FACE_SHIFT) & 63u))
+    // source/ThermalOperator.templates.hh:619-751), out of line: only cells
+    // with active-boundary faces take them
+    if (FC && active && ((info >> CI_FACE_SHIFT) & 63u))
     {
-      int const slot = (NS == 3) ? md.face_slot[c] : -1;
-      for (int f = 0; f < 6; ++f)
-      {
-        if (!((info >> (CI_FACE_SHIFT + f)) & 1u))
-          continue;
-        int const d = f / 2, side = f % 2;
-        if (d == 2 && slab != (side ? N - 1 : 0))
-          continue; // a z face only touches one node level
-        int const t0 = d == 0 ? 1 : 0, t1 = d == 2 ? 1 : 2;
-        int const btype =
-            ((info >> (CI_INTERFACE_SHIFT + f)) & 1u) ? args.interface_type : args.boundary_type[f];
-        double const ht0 = args.h[t0], ht1 = args.h[t1];
-        for (int fq = 0; fq < N * N; ++fq)
-        {
-          int const qa = fq % N, qb = fq / N;
-          double T = 0.0;
-          for (int j = 0; j < N; ++j)
-            for (int i = 0; i < N; ++i)
-            {
-              int loc[3];
-              loc[d] = side ? N - 1 : 0;
-              loc[t0] = i;
-              loc[t1] = j;
-              double const u =
-                  brick[(DEG * lx + loc[0]) + BXP * ((DEG * ly + loc[1]) + BY * (DEG * lz + loc[2]))];
-              T += args.S[qa][i] * args.S[qb][j] * u;
-            }
-          double rat[NS > 1 ? NS : 1];
-          double liquid = 0.0, p_old = 0.0, p_new = 0.0;
-          double *ph = nullptr;
-          if (NS == 3 && slot >= 0)
-          {
-            ph = &md.face_powder[((size_t)slot * 6 + f) * (N * N) + fq];
-            p_old = *ph;
-          }
-          int const pure = state_ratios<NS>(sp, mat, T, p_old, rat, liquid, p_new);
-          // p_new = min(1 - l, p_old) is idempotent, so the other level
-          // threads of this cell compute the same value whether they read
-          // the history before or after this store
-          if (ph && (d == 2 || slab == 0) && p_new != p_old)
-            *ph = p_new;
-          double const inv = inv_rho_cp<NS>(sp, gm, mat, rat, pure, T);
-          double conv_tinf = 0.0, conv_h = 0.0, rad_tinf = 0.0, rad_h = 0.0;
-          if (btype & B_CONVECTIVE)
-          {
-            conv_tinf = sp.props[mat][Q_CONV_TINF];
-            conv_h = property<NS>(sp, gm, P_CONV_COEF, mat, rat, pure, T);
-          }
-          if (btype & B_RADIATIVE)
-          {
-            rad_tinf = sp.props[mat][Q_RAD_TINF];
-            rad_h = property<NS>(sp, gm, P_EMISSIVITY, mat, rat, pure, T) * 5.670374419e-8 *
-                    (T + rad_tinf) * (T * T + rad_tinf * rad_tinf);
-          }
-          double const bval = -inv * (conv_h * (T - conv_tinf) + rad_h * (T - rad_tinf));
-          double const JxW = args.qw[qa] * ht0 * args.qw[qb] * ht1;
+      double fres[NQS];
+      face_terms<DEG, NS>(sp, gm, md, args, brick, lx, ly, lz, slab, info, mat, c, fres);
 #pragma unroll
-          for (int j = 0; j < N; ++j)
-#pragma unroll
-            for (int i = 0; i < N; ++i)
-            {
-              // node (loc) of this face; keep it if it is on level `slab`
-              int la, lb, lc;
-              if (d == 0)
-              {
-                la = side ? N - 1 : 0;
-                lb = i;
-                lc = j;
-              }
-              else if (d == 1)
-              {
-                la = i;
-                lb = side ? N - 1 : 0;
-                lc = j;
-              }
-              else
-              {
-                la = i;
-                lb = j;
-                lc = side ? N - 1 : 0;
-              }
-              if (lc != slab)
-                continue;
-              double const add = bval * (args.S[qa][i] * args.S[qb][j]) * JxW;
-#pragma unroll
-              for (int e = 0; e < NQS; ++e)
-                if (e == la + N * lb)
-                  res[e] += add;
-            }
-        }
-      }
+      for (int e = 0; e < NQS; ++e)
+        res[e] += fres[e];
     }
     // ---- per-node sums: a warp holds one 8 x 4 layer of cells (lane =
     // lx + 8 ly), so the nodes shared in x and y are summed with shuffles
@@ -1266,23 +1314,32 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
 
 // Launches the persistent tile kernel over n_items work items with at most
 // the number of CTAs that are resident at once on the device.
-template <int DEG, int NS, int P, bool AT>
-void launch_tile_t(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
+template <int DEG, int NS, int P, bool AT, bool FC>
+void launch_tile_f(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
 {
   static int grid_cap = 0;
   if (grid_cap == 0)
   {
-    cudaFuncSetAttribute(tile_kernel<DEG, NS, P, AT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(tile_kernel<DEG, NS, P, AT, FC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)TD<DEG>::SMEM);
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_kernel<DEG, NS, P, AT>, TD<DEG>::NT,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_kernel<DEG, NS, P, AT, FC>, TD<DEG>::NT,
                                                   TD<DEG>::SMEM);
     grid_cap = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
   }
   int const grid = n_items < grid_cap ? n_items : grid_cap;
-  tile_kernel<DEG, NS, P, AT><<<grid, TD<DEG>::NT, TD<DEG>::SMEM, stream>>>(map, a, n_items);
+  tile_kernel<DEG, NS, P, AT, FC><<<grid, TD<DEG>::NT, TD<DEG>::SMEM, stream>>>(map, a, n_items);
+}
+
+template <int DEG, int NS, int P, bool AT>
+void launch_tile_t(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
+{
+  if (a.faces)
+    launch_tile_f<DEG, NS, P, AT, true>(map, a, n_items, stream);
+  else
+    launch_tile_f<DEG, NS, P, AT, false>(map, a, n_items, stream);
 }
 
 } // namespace adm
