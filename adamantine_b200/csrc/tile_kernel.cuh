@@ -211,6 +211,61 @@ __device__ __forceinline__ double entry_mac(double const (&M)[3][3], int q, int 
   return kd == K_ZERO ? acc : (kd == K_ONE ? acc + v : (kd == K_MONE ? acc - v : fma(M[q][k], v, acc)));
 }
 
+// z direction at Gauss-point level SL: the values (S) and z-gradients (G)
+// from the x/y-interpolated node levels (this thread's own level in wv, the
+// others in the level exchange buffer)
+template <int DEG, int SL, int NCELL>
+__device__ __forceinline__ void z_interp(KernelArgs const &args, double const *wv, double const *xbuf, int cl,
+                                         double *Tq, double *az)
+{
+  constexpr int N = DEG + 1, NQS = N * N;
+#pragma unroll
+  for (int i = 0; i < NQS; ++i)
+  {
+    double w[N];
+#pragma unroll
+    for (int m = 0; m < N; ++m)
+      w[m] = (m == SL) ? wv[i] : xbuf[(i + NQS * m) * NCELL + cl];
+    Tq[i] = row_dot<DEG, M_S>(args.S, SL, w, 1);
+    az[i] = row_dot<DEG, M_G>(args.G, SL, w, 1);
+  }
+}
+// z direction into node level SL: S^T of the values / x-y fluxes and G^T of
+// the z fluxes of every Gauss-point level (this thread's own in axy / az,
+// the others in the flux exchange buffer)
+template <int DEG, int SL, int NCELL>
+__device__ __forceinline__ void z_integrate(KernelArgs const &args, double const *axy, double const *az,
+                                            double const *pzbuf, int cl, double *res)
+{
+  constexpr int N = DEG + 1, NQS = N * N, NN = N * NQS;
+#pragma unroll
+  for (int i = 0; i < NQS; ++i)
+  {
+    double acc = 0.0;
+    bool started = false;
+#pragma unroll
+    for (int q = 0; q < N; ++q)
+    {
+      double const vp = (q == SL) ? axy[i] : pzbuf[(i + NQS * q) * NCELL + cl];
+      double const vz = (q == SL) ? az[i] : pzbuf[(NN + i + NQS * q) * NCELL + cl];
+      int const ks = coef_kind<DEG, M_S>(q, SL), kg = coef_kind<DEG, M_G>(q, SL);
+      if (ks != K_ZERO)
+      {
+        acc = started ? entry_mac<DEG, M_S>(args.S, q, SL, vp, acc)
+                      : (ks == K_ONE ? vp : (ks == K_MONE ? -vp : args.S[q][SL] * vp));
+        started = true;
+      }
+      if (kg != K_ZERO)
+      {
+        acc = started ? entry_mac<DEG, M_G>(args.G, q, SL, vz, acc)
+                      : (kg == K_ONE ? vz : (kg == K_MONE ? -vz : args.G[q][SL] * vz));
+        started = true;
+      }
+    }
+    res[i] = acc;
+  }
+}
+
 struct SmemPhys
 {
   double poly[kMaxMaterials][kNStateProps][kMaxStates][kMaxPoly];
@@ -221,6 +276,7 @@ struct SmemPhys
   int n_materials, use_table, isotropic, n_beams;
   int has_rotation, sources_here;
   int member;
+  int src_on;      // the current item's tile meets a source
   int role[2][27]; // per item parity
 };
 
@@ -845,10 +901,14 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
     // at the level-exchange barrier ends the CTA before anything is written
     bool const arrived = mbar_wait(&bars[buf], (unsigned)((it >> 1) & 1));
 
-    // Tile-level source culling, evaluated by every thread (exact: it skips
-    // only points where every source is zero by its own cutoff rules).
-    bool do_src = false;
+    // Tile-level source culling (exact: it skips only points where every
+    // source is zero by its own cutoff rules), evaluated by the first warp
+    // and published through the level-exchange barrier. A thread that
+    // writes the flag for the next item has passed the flux barrier of this
+    // one, after which nobody reads it.
+    if (tid < 32)
     {
+      bool do_src = false;
       double const x0 = args.origin[0] + ncx0 * args.h[0];
       double const y0 = args.origin[1] + ncy0 * args.h[1];
       double const z0 = args.origin[2] + ncz0 * args.h[2];
@@ -874,6 +934,8 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
           continue;
         do_src = true;
       }
+      if (tid == 0)
+        sp.src_on = do_src;
     }
 
     // ---- the cell: thread (slab, cl) handles Gauss-point level qc = slab
@@ -935,21 +997,15 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
       fence_proxy_async();
       issue(buf ^ 1, item + step);
     }
+    bool const do_src = sp.src_on != 0;
     double Tq[NQS], az[NQS];
-#pragma unroll
-    for (int i = 0; i < NQS; ++i)
-    {
-      double tv = 0.0, gz = 0.0;
-#pragma unroll
-      for (int m = 0; m < N; ++m)
-      {
-        double const wm = (m == slab) ? wv[i] : xbuf[(i + NQS * m) * NCELL + cl];
-        tv = fma(args.S[slab][m], wm, tv);
-        gz = fma(args.G[slab][m], wm, gz);
-      }
-      Tq[i] = tv;
-      az[i] = gz;
-    }
+    // (a warp-uniform branch: a warp's threads share the level)
+    if (slab == 0)
+      z_interp<DEG, 0, NCELL>(args, wv, xbuf, cl, Tq, az);
+    else if (DEG == 1 || slab == 1)
+      z_interp<DEG, 1, NCELL>(args, wv, xbuf, cl, Tq, az);
+    else
+      z_interp<DEG, DEG, NCELL>(args, wv, xbuf, cl, Tq, az);
     // 3. physics at the NQS Gauss points of this level; axy accumulates the
     //    x/y flux contributions (collocation D^T) and the source, az ends
     //    up holding the z fluxes
@@ -1118,19 +1174,17 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
     }
     __syncthreads();
     double res[NQS];
-#pragma unroll
-    for (int i = 0; i < NQS; ++i)
+    if (slab == 0)
+      z_integrate<DEG, 0, NCELL>(args, axy, az, pzbuf, cl, res);
+    else if (DEG == 1 || slab == 1)
+      z_integrate<DEG, 1, NCELL>(args, axy, az, pzbuf, cl, res);
+    else
+      z_integrate<DEG, DEG, NCELL>(args, axy, az, pzbuf, cl, res);
+    if (!active)
     {
-      double acc = 0.0;
 #pragma unroll
-      for (int q = 0; q < N; ++q)
-      {
-        double const vp = (q == slab) ? axy[i] : pzbuf[(i + NQS * q) * NCELL + cl];
-        double const vz = (q == slab) ? az[i] : pzbuf[(NN + i + NQS * q) * NCELL + cl];
-        acc = fma(args.S[q][slab], vp, acc);
-        acc = fma(args.G[q][slab], vz, acc);
-      }
-      res[i] = active ? acc : 0.0;
+      for (int i = 0; i < NQS; ++i)
+        res[i] = 0.0;
     }
 
     // ---- face terms of this node level (face_local_apply,
