@@ -139,8 +139,10 @@ def build_workload(size="full"):
     return cfg, T
 
 
-def cpu_vmult_rate(cfg, T, n_threads, budget_s=20.0, max_steps=3):
-    """Times the oracle's vmult (reference CPU algorithm) on the host."""
+def cpu_vmult_rate(cfg, T, n_threads, budget_s=20.0, max_steps=5, keep_result=False):
+    """Times the oracle's vmult (reference CPU algorithm) on the host: median
+    of max_steps applications after one warm-up (fewer if budget_s runs
+    out). With keep_result, also returns the first application's output."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py
 
@@ -152,6 +154,7 @@ def cpu_vmult_rate(cfg, T, n_threads, budget_s=20.0, max_steps=3):
     src = np.ascontiguousarray(T.reshape(-1))
     dst = np.zeros_like(src)
     o.vmult_add(dst, src)  # warm-up
+    first = dst.copy() if keep_result else None
     times = []
     t_start = time.perf_counter()
     for _ in range(max_steps):
@@ -163,7 +166,18 @@ def cpu_vmult_rate(cfg, T, n_threads, budget_s=20.0, max_steps=3):
             break
     n_dofs = int(np.prod(geo.node_shape(cfg.degree)))
     med = statistics.median(times)
+    if keep_result:
+        return n_dofs / med / 1e9, med, len(times), first
     return n_dofs / med / 1e9, med, len(times)
+
+
+def workload_config(size, world):
+    """The workload description both --impl arms print (identical dicts)."""
+    cfg_size = SIZES[size][0]
+    n_dofs = (2 * cfg_size[0] + 1) * (2 * cfg_size[1] + 1) * (2 * cfg_size[2] + 1)
+    return {"workload": WORKLOAD if size == "full" else WORKLOAD + "_" + size,
+            "mesh": "x".join(map(str, cfg_size)) + " Q2", "dofs": n_dofs, "states": "solid/liquid/powder",
+            "source": "Goldak 400 W", "parallelism": f"replicas x{world}"}
 
 
 ENSEMBLE_WORKLOAD = "ensemble_q1_64x64x32_32members_rk4_100steps"
@@ -228,6 +242,28 @@ def run_ensemble(args, dist, local_rank):
     identical = looped["coloured"][1] == 0.0 and looped["atomic"][1] == 0.0
     max_rel_diff = max(v[1] for v in looped.values())
     assert e.device_error() == 0
+    # the fair member loop: every member through its own single-member
+    # handle and adm_evolve_n_steps (one CUDA graph per step), with the
+    # launch schedule the single-member autotuner picks on member 0
+    from adamantine_b200.thermal import ThermalPhysics
+
+    singles = [ThermalPhysics(c, device=local_rank, stream=stream) for c in configs]
+    ys = [singles[k].from_grid(grids[k]) for k in range(n)]
+    single_schedule, _ = singles[0].autotune(ys[0])
+    for k, g in enumerate(singles):  # warm-up: graph capture of every handle
+        g.set_schedule(single_schedule)
+        g.evolve_n_steps(0.0, dt, 2, ys[k].clone())
+    ys = [singles[k].from_grid(grids[k]) for k in range(n)]
+    torch.cuda.synchronize()
+    ev[2].record(stream)
+    for k in range(n):
+        singles[k].evolve_n_steps(0.0, dt, steps, ys[k])
+    ev[3].record(stream)
+    ev[3].synchronize()
+    ms_g = ev[2].elapsed_time(ev[3])
+    graph_loop_diff = max(float(((yb[k] - ys[k]).abs().max() / ys[k].abs().max()).item()) for k in range(n))
+    assert all(g.device_error() == 0 for g in singles)
+    del singles, ys
     # EnKF analysis on the forecast (member-specific top-surface node maps)
     layers = [p[2] for p in params]
     ij, sigma = surface_observations(e.nodes[:2], layers)
@@ -292,20 +328,26 @@ def run_ensemble(args, dist, local_rank):
     ms_as = timed(analysis_step)
     ms_la = looped["atomic"][0]
     if dist:
-        tt = torch.tensor([ms_b, ms_l, ms_la, ms_a, ms_al, ms_as], device="cuda")
+        tt = torch.tensor([ms_b, ms_l, ms_la, ms_a, ms_al, ms_as, ms_g], device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms_b, ms_l, ms_la, ms_a, ms_al, ms_as = (float(x) for x in tt.tolist())
+        ms_b, ms_l, ms_la, ms_a, ms_al, ms_as, ms_g = (float(x) for x in tt.tolist())
     return {
         "workload": ENSEMBLE_WORKLOAD, "members_per_gpu": n, "steps": steps, "dt": dt,
         "active_layers": [min(layers), max(layers)],
         "batched_member_steps_per_s": world * n * steps / (ms_b * 1e-3),
-        "looped_member_steps_per_s": world * n * steps / (ms_l * 1e-3),
-        "speedup": ms_l / ms_b, "batched_ms_per_step": ms_b / steps, "looped_ms_per_step": ms_l / steps,
-        "looped_atomic_member_steps_per_s": world * n * steps / (ms_la * 1e-3),
-        "speedup_vs_looped_atomic": ms_la / ms_b,
+        # headline: against each member through its own graph-captured
+        # single-member path with the single-member autotuner's schedule
+        "looped_member_steps_per_s": world * n * steps / (ms_g * 1e-3),
+        "speedup": ms_g / ms_b, "batched_ms_per_step": ms_b / steps, "looped_ms_per_step": ms_g / steps,
+        "looped_path": "32 single-member handles, adm_evolve_n_steps (one CUDA graph per step), "
+                       f"{['coloured', 'atomic'][single_schedule]} schedule (single-member autotuner)",
+        "max_rel_diff_batched_vs_graph_loop": graph_loop_diff,
+        "per_step_loop": {"coloured_member_steps_per_s": world * n * steps / (ms_l * 1e-3),
+                          "atomic_member_steps_per_s": world * n * steps / (ms_la * 1e-3),
+                          "speedup_vs_coloured": ms_l / ms_b, "speedup_vs_atomic": ms_la / ms_b,
+                          "path": "adm_ensemble_evolve_looped: each member's stages launched one by one"},
         "identical_results": identical, "max_rel_diff_batched_vs_looped": max_rel_diff,
         "batched_schedule": ["coloured", "atomic"][schedule],
-        "looped_schedule": "coloured (the single-member default); looped_atomic_*: atomic",
         "batched_path": "one CUDA graph per step (4 stages)",
         "work_items_per_sweep": e.n_work_items(),
         "enkf_analysis_ms": ms_a, "n_obs": int(idx.shape[1]), "augmented_params": 2,
@@ -393,6 +435,53 @@ def run_adjoint(args, local_rank):
 DEPOSITION_WORKLOAD = "deposition_q2_256x256x128_rk4"
 
 
+RK4_WORKLOAD = "phase_change_q2_128x128x64_rk4_step"
+
+
+def run_rk4_steps(args, local_rank):
+    """The time step the operator serves: RK4 steps of dt = 5e-7 on the
+    128x128x64 Q2 phase-change problem through adm_evolve_n_steps (one CUDA
+    graph per step: per stage the heat-source state, the tile sweep with the
+    fused inverse mass and stage update). GDoF/s counts four operator
+    applications per step."""
+    import torch
+
+    from adamantine_b200.thermal import ThermalPhysics
+
+    cfg, T = build_workload(args.size)
+    g = ThermalPhysics(cfg, device=local_rank)
+    n = g.m()
+    n_dofs = int(np.prod(cfg.geometry.node_shape(cfg.degree)))
+    y = g.from_grid(T)
+    schedule, sched_ms = g.autotune(y)
+    dt = 5e-7
+    t = g.evolve_n_steps(0.0, dt, 3, y)  # warm-up: graph capture
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(g.stream)
+    t = g.evolve_n_steps(t, dt, args.rk4_steps, y)
+    e1.record(g.stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.rk4_steps
+    assert g.device_error() == 0
+    # node-vector bytes a fused RK4 step must move (8 B per node per read or
+    # write): stage 1 reads y (its input) and the inverse mass and writes the
+    # next stage input and the running sum (32 B); stages 2-3 read their
+    # input, the inverse mass and y, read and write the running sum and write
+    # the next input (48 B each); stage 4 reads its input, the inverse mass,
+    # y and the running sum and writes y (40 B); plus 13 B of cell data per
+    # cell and stage
+    alg = 168 * n + 4 * 13 * g.n_cells
+    peak, kind = measured_peaks()
+    return {"workload": RK4_WORKLOAD, "steps": args.rk4_steps, "dt": dt, "ms_per_step": ms,
+            "gdof_per_s": 4 * n_dofs / (ms * 1e-3) / 1e9, "steps_per_s": 1e3 / ms,
+            "schedule": ["coloured", "atomic"][schedule],
+            "autotune_ms_per_vmult": {"coloured": sched_ms[0], "atomic": sched_ms[1]},
+            "algorithmic_bytes_per_step": alg, "achieved_gbs": alg / (ms * 1e-3) / 1e9,
+            "hbm_frac": alg / (ms * 1e-3) / 1e9 / peak, "peak_kind": f"{kind} hbm_gbs",
+            "path": "adm_evolve_n_steps (CUDA graph per step)"}
+
+
 def run_deposition(args, local_rank, with_cpu):
     """RK4 steps (dt = 2e-7) of the 67.6 M-node Q2 deposition workload with
     the driver's per-step activation of the deposition boxes; throughput as
@@ -455,7 +544,8 @@ def run_deposition(args, local_rank, with_cpu):
     # mass, y, running sum, next stage vector) and 13 bytes per cell per stage
     bytes_step = 168 * g.m() + 4 * 13 * C
     out = {
-        "workload": DEPOSITION_WORKLOAD, "nodes": n_nodes, "cells": C, "steps": steps, "dt": dt,
+        "workload": DEPOSITION_WORKLOAD, "nodes": n_nodes, "cells": C, "steps": steps, "steps_run": steps,
+        "steps_config": 2000, "dt": dt,
         "ms_per_step": ms / steps, "gdofs_per_s": 4 * n_nodes * steps / (ms * 1e-3) / 1e9,
         "hbm_gbs_algorithmic": bytes_step * steps / (ms * 1e-3) / 1e9, "cells_activated": activated + n_act,
         "boxes": boxes.n, "activation": "device append list, driver window per step",
@@ -469,13 +559,19 @@ def run_deposition(args, local_rank, with_cpu):
         st = cfg.to_struct()
         o = oracle_py.Oracle(st, active=cfg.geometry.active_cells(), initial_state=cfg.geometry.initial_state())
         yr = np.ascontiguousarray(T0, np.float64).reshape(-1).copy()
+        k_cpu = max(1, args.deposition_cpu_steps)
+        tr = 0.0
         t0 = time.perf_counter()
-        o.evolve_one_time_step(0.0, dt, yr)
-        cpu_s = time.perf_counter() - t0
-        out["cpu_baseline"] = {"seconds_per_step": cpu_s, "seconds_20_step_window": 20 * cpu_s,
+        for _ in range(k_cpu):
+            tr = o.evolve_one_time_step(tr, dt, yr)
+        cpu_s = (time.perf_counter() - t0) / k_cpu
+        out["cpu_baseline"] = {"seconds_per_step": cpu_s, "steps_timed": k_cpu,
+                               "seconds_20_step_window": 20 * cpu_s,
+                               "window_measured": k_cpu >= 20,
                                "cores": os.cpu_count() or 1, "kind": "port",
-                               "sample": "one RK4 step of the workload (oracle, OpenMP); the 20-step window is "
-                                         "20 times that"}
+                               "sample": f"{k_cpu} RK4 step(s) of the workload (oracle, OpenMP); the 20-step "
+                                         f"window is 20 x the mean step"
+                                         + ("" if k_cpu >= 20 else " (extrapolated)")}
     return out
 
 
@@ -628,8 +724,8 @@ def run_reference(args, rank, world):
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * n_dofs / value / 1e9,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "mesh": "128x128x64 Q2", "dofs": n_dofs},
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded; no public dataset)", "config": workload_config("full", world),
         "cpu_baseline": {"value": value, "unit": "GDoF/s", "cores": n_threads, "kind": "port",
                          "sample": f"{args.steps} full vmults of the workload (C++/OpenMP restatement of the "
                                    f"reference CPU ThermalOperator::vmult), {elapsed:.1f} s"},
@@ -722,12 +818,11 @@ def run_ours(args, rank, world, local_rank):
         "metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded; no public dataset)",
-        "config": {"workload": WORKLOAD if args.size == "full" else WORKLOAD + "_" + args.size,
-                   "mesh": "x".join(map(str, SIZES[args.size][0])) + " Q2", "dofs": n_dofs,
-                   "states": "solid/liquid/powder", "source": "Goldak 400 W", "parallelism": f"replicas x{world}",
-                   "l2": "two src/dst pairs alternate (272 MB working set > 126 MB L2)",
-                   "schedule": sched_name,
-                   "autotune_ms_per_vmult": {"coloured": schedule_ms[0], "atomic": schedule_ms[1]}},
+        "config": workload_config(args.size, world),
+        "timing": {"l2": "two src/dst pairs alternate (272 MB working set > 126 MB L2)",
+                   "events": "CUDA events on the handle's stream around the K vmults"},
+        "schedule": sched_name,
+        "autotune_ms_per_vmult": {"coloured": schedule_ms[0], "atomic": schedule_ms[1]},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,
                      "traffic": DRAM_BYTES_PER_VMULT_FULL[sched_name] if args.size == "full" else None,
@@ -749,6 +844,8 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": args.steps * (2 if schedule == 1 else 9),
         "clocks": clk.summary(),
     }
+    if args.rk4_steps > 0:
+        line["rk4_step"] = run_rk4_steps(args, local_rank)
     if not args.no_ensemble:
         line["ensemble"] = run_ensemble(args, dist, local_rank)
     if not args.no_adjoint:
@@ -760,10 +857,24 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_mechanics:
         line["mechanics"] = run_mechanics(args, local_rank)
     if rank == 0 and not args.no_cpu_baseline:
-        rate, med, n = cpu_vmult_rate(build_workload(args.size)[0], T, os.cpu_count() or 1)
+        rate, med, n, ref_out = cpu_vmult_rate(build_workload(args.size)[0], T, os.cpu_count() or 1,
+                                               keep_result=True)
         line["cpu_baseline"] = {"value": rate, "unit": "GDoF/s", "cores": os.cpu_count() or 1, "kind": "port",
                                 "sample": f"{n} full vmults of the workload on the host (oracle, OpenMP), "
                                           f"median {med:.2f} s"}
+        # parity of the timed path: the same vmult (autotuned schedule, a
+        # fresh handle so the phase history starts as the oracle's) against
+        # the oracle's first application on the same field
+        gp = ThermalPhysics(cfg, device=local_rank)
+        gp.set_schedule(schedule)
+        gp.set_time(t_op)
+        dp = gp.initialize_dof_vector()
+        gp.vmult(dp, gp.from_grid(T))
+        got = gp.to_grid(dp).reshape(-1)
+        line["parity"] = {"max_rel": float(np.max(np.abs(got - ref_out)) / np.max(np.abs(ref_out))),
+                          "tol": 1e-12, "against": "oracle vmult (C++ restatement of the reference CPU path)",
+                          "schedule": sched_name}
+        del gp
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
@@ -780,8 +891,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
-    ap.add_argument("--deposition-steps", type=int, default=400,
+    ap.add_argument("--rk4-steps", type=int, default=100,
+                    help="graph-captured RK4 steps of the headline problem (0: skip)")
+    ap.add_argument("--deposition-steps", type=int, default=2000,
                     help="RK4 steps of the deposition workload (0: skip; the configuration runs 2000)")
+    ap.add_argument("--deposition-cpu-steps", type=int, default=2,
+                    help="oracle RK4 steps timed for the deposition workload's CPU window (20: the full window)")
     ap.add_argument("--size", default="full", choices=sorted(SIZES))
     ap.add_argument("--no-mechanics", action="store_true")
     ap.add_argument("--amr-steps", type=int, default=50,
