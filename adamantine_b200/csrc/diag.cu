@@ -94,8 +94,9 @@ extern "C" int adm_diag_fp64_fma_rate(int device, double *tflops)
 namespace
 {
 // The bounded mbarrier wait of the tile kernels on a barrier that nothing
-// arrives at: the wait must give up after `limit` polls and report it.
-__global__ void wait_timeout_kernel(long long limit, int *status)
+// arrives at: the wait must give up after `limit_ns` nanoseconds and report
+// it.
+__global__ void wait_timeout_kernel(long long limit_ns, int *status)
 {
   __shared__ __align__(8) uint64_t bar;
   if (threadIdx.x == 0)
@@ -104,15 +105,15 @@ __global__ void wait_timeout_kernel(long long limit, int *status)
     adm::fence_mbar_init();
   }
   __syncthreads();
-  bool const arrived = adm::mbar_wait(&bar, 0u, limit);
+  bool const arrived = adm::mbar_wait(&bar, 0u, limit_ns);
   if (__syncthreads_or(!arrived) && threadIdx.x == 0)
     *status = 1;
 }
 } // namespace
 
-extern "C" int adm_diag_wait_timeout(long long limit, int32_t *timed_out)
+extern "C" int adm_diag_wait_timeout(long long limit_us, int32_t *timed_out)
 {
-  if (!timed_out || limit < 1 || limit > (1ll << 26))
+  if (!timed_out || limit_us < 1 || limit_us > 1000000)
     return ADM_ERR_INVALID;
   *timed_out = 0;
   int *d = nullptr;
@@ -123,7 +124,7 @@ extern "C" int adm_diag_wait_timeout(long long limit, int32_t *timed_out)
     rc = ADM_ERR_CUDA;
   if (rc == ADM_OK)
   {
-    wait_timeout_kernel<<<1, 64>>>(limit, d);
+    wait_timeout_kernel<<<1, 64>>>(limit_us * 1000, d);
     if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess)
       rc = ADM_ERR_CUDA;
   }

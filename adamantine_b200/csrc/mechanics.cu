@@ -32,9 +32,14 @@ namespace
 constexpr int kMaxN = 27; // nodes (and quadrature points) of a Q2 cell
 constexpr double kGravity = 9.80665; // GravityForce::g (source/BodyForce.hh:53)
 
-__constant__ double c_val[kMaxN * kMaxN];     // [q][n] phi_n(x_q)
-__constant__ double c_grad[kMaxN * kMaxN * 3]; // [q][n][d] d phi_n / d xi_d (x_q)
-__constant__ double c_wq[kMaxN];              // reference weights of the Gauss points
+// Reference-element tables of one handle, in that handle's device buffer
+// (handles of different FE degrees coexist on a device): values
+// [q][n] phi_n(x_q), gradients [q][n][d] d phi_n / d xi_d (x_q) and the
+// reference weights of the Gauss points, at these offsets.
+constexpr int kTabVal = 0;
+constexpr int kTabGrad = kMaxN * kMaxN;
+constexpr int kTabWq = kTabGrad + kMaxN * kMaxN * 3;
+constexpr int kTabSize = kTabWq + kMaxN;
 
 struct MechArgs
 {
@@ -50,6 +55,7 @@ struct MechArgs
   double tinit;
   int thermoelastic, gravity;
   uint8_t const *melted;
+  double const *tab; // the handle's reference-element tables (kTab* offsets)
 };
 
 __device__ __forceinline__ int64_t node_of(MechArgs const &a, int cx, int cy, int cz, int n)
@@ -69,7 +75,7 @@ __global__ void __launch_bounds__(128) elastic_apply_kernel(MechArgs a, double c
   // different quadrature points' rows, which constant memory serializes
   __shared__ double grad_s[kMaxN * kMaxN * 3];
   for (int e = threadIdx.x; e < kMaxN * kMaxN * 3; e += blockDim.x)
-    grad_s[e] = c_grad[e];
+    grad_s[e] = a.tab[kTabGrad + e];
   __syncthreads();
   int const w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int const G = 32 / a.N; // cells per warp
@@ -114,7 +120,7 @@ __global__ void __launch_bounds__(128) elastic_apply_kernel(MechArgs a, double c
           G3[comp][d] = s * a.inv_h[d];
         }
       double const div = G3[0][0] + G3[1][1] + G3[2][2];
-      double const jw = a.jxw * c_wq[q];
+      double const jw = a.jxw * a.tab[kTabWq + q];
 #pragma unroll
       for (int comp = 0; comp < 3; ++comp)
 #pragma unroll
@@ -147,9 +153,9 @@ __global__ void __launch_bounds__(128) elastic_rhs_kernel(MechArgs a, double con
   __shared__ double val_s[kMaxN * kMaxN], grad_s[kMaxN * kMaxN * 3];
   for (int e = threadIdx.x; e < kMaxN * kMaxN * 3; e += blockDim.x)
   {
-    grad_s[e] = c_grad[e];
+    grad_s[e] = a.tab[kTabGrad + e];
     if (e < kMaxN * kMaxN)
-      val_s[e] = c_val[e];
+      val_s[e] = a.tab[kTabVal + e];
   }
   __syncthreads();
   int const w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -171,7 +177,7 @@ __global__ void __launch_bounds__(128) elastic_rhs_kernel(MechArgs a, double con
     if (lane < a.N)
     {
       int const q = lane;
-      double const jw = a.jxw * c_wq[q];
+      double const jw = a.jxw * a.tab[kTabWq + q];
       double b = 0.0;
       if (a.thermoelastic)
       {
@@ -208,7 +214,7 @@ __global__ void __launch_bounds__(128) elastic_diag_kernel(MechArgs a, double *d
 {
   __shared__ double grad_s[kMaxN * kMaxN * 3];
   for (int e = threadIdx.x; e < kMaxN * kMaxN * 3; e += blockDim.x)
-    grad_s[e] = c_grad[e];
+    grad_s[e] = a.tab[kTabGrad + e];
   __syncthreads();
   int const w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int const gw = blockIdx.x * 4 + w, nw = gridDim.x * 4;
@@ -237,7 +243,7 @@ __global__ void __launch_bounds__(128) elastic_diag_kernel(MechArgs a, double *d
           if (d == comp)
             gc = gd;
         }
-        r += a.jxw * c_wq[q] * ((lam + mu) * gc * gc + mu * gg);
+        r += a.jxw * a.tab[kTabWq + q] * ((lam + mu) * gc * gc + mu * gg);
       }
       atomicAdd(diag + comp * a.m + g, r);
     }
@@ -389,9 +395,13 @@ public:
       }
     }
     ADM_CK(cudaSetDevice(th_.device_));
-    ADM_CK(cudaMemcpyToSymbol(c_val, val.data(), val.size() * sizeof(double)));
-    ADM_CK(cudaMemcpyToSymbol(c_grad, grad.data(), grad.size() * sizeof(double)));
-    ADM_CK(cudaMemcpyToSymbol(c_wq, wq.data(), wq.size() * sizeof(double)));
+    std::vector<double> tab(kTabSize, 0.0);
+    std::copy(val.begin(), val.end(), tab.begin() + kTabVal);
+    std::copy(grad.begin(), grad.end(), tab.begin() + kTabGrad);
+    std::copy(wq.begin(), wq.end(), tab.begin() + kTabWq);
+    tab_.alloc(kTabSize);
+    ADM_CK(cudaMemcpyAsync(tab_.p, tab.data(), kTabSize * sizeof(double), cudaMemcpyHostToDevice, th_.stream_));
+    ADM_CK(cudaStreamSynchronize(th_.stream_));
   }
 
   void setup(double const *temperature)
@@ -579,6 +589,7 @@ private:
     a.thermoelastic = cfg_.thermoelastic;
     a.gravity = cfg_.gravity;
     a.melted = melted_.p;
+    a.tab = tab_.p;
     return a;
   }
 
@@ -630,6 +641,7 @@ private:
   std::vector<uint8_t> mask_h_;
   DevBuf<int32_t> cells_;
   DevBuf<uint8_t> mask_, matid_, melted_;
+  DevBuf<double> tab_; // reference-element tables of this handle's degree
   DevBuf<double> rhs_, diag_, r_, z_, pv_, qv_, sc_;
 };
 

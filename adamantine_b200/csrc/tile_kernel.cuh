@@ -116,14 +116,30 @@ __device__ __forceinline__ void tma_load_brick(void *dst, CUtensorMap const *map
                "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(m), "r"(smem_addr(bar))
                : "memory");
 }
-// Bounded wait on an mbarrier phase: false after ~kSpinLimit polls (the
-// caller then reports DERR_TMA_TIMEOUT instead of hanging).
-constexpr long long kSpinLimit = 1ll << 26;
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, long long limit = kSpinLimit)
+// Bounded wait on an mbarrier phase: false once limit_ns nanoseconds of the
+// global timer have passed without the phase completing (or, as a backstop
+// should the timer stall, after kPollCap polls); the caller then reports
+// DERR_TMA_TIMEOUT instead of hanging. A brick copy lands in microseconds.
+constexpr long long kWaitLimitNs = 2000000000ll; // 2 s
+constexpr long long kPollCap = 1ll << 32;
+__device__ __forceinline__ unsigned long long globaltimer_ns()
 {
-  for (long long i = 0; i < limit; ++i)
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, long long limit_ns = kWaitLimitNs)
+{
+  if (mbar_try_wait(bar, parity))
+    return true;
+  unsigned long long const t0 = globaltimer_ns();
+  for (long long i = 0; i < kPollCap; ++i)
+  {
     if (mbar_try_wait(bar, parity))
       return true;
+    if ((long long)(globaltimer_ns() - t0) > limit_ns)
+      return false;
+  }
   return false;
 }
 

@@ -98,6 +98,14 @@ class ShardedAnalysis:
         world = dist.get_world_size(self.group) if dist.is_initialized() else 1
         rank = dist.get_rank(self.group) if dist.is_initialized() else 0
         n_local = states.shape[0]
+        if world > 1:
+            # every rank must hold the same number of members: the gathers
+            # and the reduce-scatter below are sized by it
+            counts = torch.tensor([n_local, -n_local], dtype=torch.int64, device=states.device)
+            dist.all_reduce(counts, op=dist.ReduceOp.MAX, group=self.group)
+            if int(counts[0]) != n_local or int(-counts[1]) != n_local:
+                raise ValueError(f"ShardedAnalysis needs the same member count on every rank: this rank holds "
+                                 f"{n_local}, the counts range from {int(-counts[1])} to {int(counts[0])}")
         N = n_local * world
         hx_local = self.steps.observe(states, n_state, obs_index)
         if world > 1:

@@ -22,10 +22,12 @@ int adm_diag_reciprocal(double const *x, double *y, double *y_ref, int64_t n);
  * Best of five timed launches after one warm-up; synchronizes. */
 int adm_diag_fp64_fma_rate(int device, double *tflops);
 
-/* Runs the kernels' bounded mbarrier wait (limit polls, 1..2^26) on a barrier
- * that nothing arrives at; *timed_out = 1 when the wait gave up and reported
- * it (the path a TMA copy that never lands takes). The GPU keeps running. */
-int adm_diag_wait_timeout(long long limit, int32_t *timed_out);
+/* Runs the kernels' bounded mbarrier wait (a wall-time limit of limit_us
+ * microseconds on the GPU's global timer, 1..10^6; the kernels use 2 s) on a
+ * barrier that nothing arrives at; *timed_out = 1 when the wait gave up and
+ * reported it (the path a TMA copy that never lands takes). The GPU keeps
+ * running. */
+int adm_diag_wait_timeout(long long limit_us, int32_t *timed_out);
 
 #ifdef __cplusplus
 }

@@ -1,8 +1,9 @@
 """Regenerates the golden fixtures in this folder from the reference's test data.
 
-Run in a container where the reference is mounted at /root/reference:
+Give the reference's source tree as the argument (or in the environment
+variable ADAMANTINE_REFERENCE):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py <adamantine source tree>
 
 * convective_bc_gold.npy -- tests/data/convective_bc_gold.txt of the reference
   (the 1809 nodal temperatures of test_thermal_physics.hh:513-625, deal.II DoF
@@ -39,11 +40,15 @@ import sys
 
 import numpy as np
 
-REF = os.environ.get("ADAMANTINE_REFERENCE", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
+REF = None
 
 
 def main():
+    global REF
+    REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("ADAMANTINE_REFERENCE")
+    if not REF:
+        sys.exit("usage: make_golden.py <adamantine source tree> (or set ADAMANTINE_REFERENCE)")
     src = os.path.join(REF, "tests", "data", "convective_bc_gold.txt")
     if not os.path.exists(src):
         sys.exit(f"reference test data not found: {src}")

@@ -22,8 +22,13 @@ def test_bounded_wait_times_out_and_reports():
     fn.argtypes = [ctypes.c_longlong, ctypes.POINTER(ctypes.c_int32)]
     fn.restype = ctypes.c_int
     out = ctypes.c_int32(-1)
-    assert fn(2000, ctypes.byref(out)) == 0
+    import time
+
+    t0 = time.perf_counter()
+    assert fn(2000, ctypes.byref(out)) == 0  # 2 ms of wall time
     assert out.value == 1
+    assert time.perf_counter() - t0 < 5.0
+    assert fn(0, ctypes.byref(out)) != 0 and fn(2000000, ctypes.byref(out)) != 0
     # the device keeps working afterwards
     x = torch.ones(8, device="cuda") * 2
     assert float(x.sum().item()) == 16.0

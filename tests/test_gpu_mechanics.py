@@ -177,3 +177,43 @@ def test_elastostatic_physics_case():
     u = plain(phys, mech.solve())
     assert np.abs(u - uo).max() <= 2e-9
     assert np.abs(uo).max() > 1.0  # O(1) and larger displacements, as the reference notes
+
+
+def test_handles_of_different_degrees_coexist():
+    """A FE_Q(1) and a FE_Q(2) handle alive on one device, their operator
+    applications and solves interleaved, give the results each gives alone
+    (the reference-element tables belong to the handle)."""
+    def make(degree):
+        phys = ThermalPhysics(reference_cube(degree))
+        mech = MechanicalPhysics(phys, 2.0, 3.0, density=1.0, thermoelastic=False, gravity=True,
+                                 clamped=("x-",))
+        mech.setup_dofs()
+        return phys, mech
+
+    rng = np.random.default_rng(11)
+    alone = {}
+    for degree in (1, 2):
+        phys, mech = make(degree)
+        x = torch.tensor(rng.uniform(-1, 1, 3 * phys.m()), device=phys.device)
+        dst = mech.new_vector()
+        mech.vmult(dst, x)
+        alone[degree] = (x, dst.clone(), mech.solve().clone())
+        del mech, phys
+    p1, m1 = make(1)
+    p2, m2 = make(2)
+    d1, d2 = m1.new_vector(), m2.new_vector()
+
+    def close(a, b, tol):
+        return float((a - b).abs().max() / b.abs().max()) <= tol
+
+    # the operator adds with atomics (rounding order varies): 1e-13; the
+    # CG solve: 1e-10 (a swapped table would be off by O(1))
+    for _ in range(2):
+        d1.zero_()
+        d2.zero_()
+        m1.vmult(d1, alone[1][0])
+        m2.vmult(d2, alone[2][0])
+        assert close(d1, alone[1][1], 1e-13) and close(d2, alone[2][1], 1e-13)
+        u2 = m2.solve()
+        u1 = m1.solve()
+        assert close(u1, alone[1][2], 1e-10) and close(u2, alone[2][2], 1e-10)

@@ -174,3 +174,37 @@ def test_lost_rank_ends_the_analysis_with_an_error(tmp_path):
     outcome = open(os.path.join(tmp_path, "outcome.txt")).read()
     assert outcome.startswith("error"), outcome
     assert time.time() - t0 < 120
+
+
+def worker_uneven(rank, port, out):
+    import sys
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    for pth in (here, os.path.join(os.path.dirname(here), "oracle"), os.path.dirname(here)):
+        sys.path.insert(0, pth)
+    from sharded_steps import NumpySteps
+
+    from adamantine_b200.sharded import ShardedAnalysis
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=WORLD)
+    states, params, idx, obs, var, pert, mask, n_state = problem()
+    sl = slice(0, 3) if rank == 0 else slice(3, 8)  # 3 and 5 members
+    outcome = "ok"
+    try:
+        ShardedAnalysis(NumpySteps())(torch.from_numpy(states[sl].copy()), n_state, torch.from_numpy(idx[sl]),
+                                      torch.from_numpy(obs), torch.from_numpy(pert), obs_var=torch.from_numpy(var))
+    except ValueError as e:
+        outcome = "ValueError: " + str(e)
+    with open(os.path.join(out, f"uneven{rank}.txt"), "w") as fh:
+        fh.write(outcome)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_uneven_member_counts_are_rejected_on_every_rank(tmp_path):
+    mp.spawn(worker_uneven, args=(free_port(), str(tmp_path)), nprocs=WORLD, join=True)
+    for r in range(WORLD):
+        outcome = open(os.path.join(tmp_path, f"uneven{r}.txt")).read()
+        assert outcome.startswith("ValueError") and "from 3 to 5" in outcome, outcome
