@@ -1,16 +1,16 @@
-// Instantiations of the fused tile kernel for FE degree 1, 2 material
+// Instantiations of the FE_Q(1) cell kernel (one thread per cell), 2 material
 // state(s) and polynomial properties up to degree 2, in both launch
 // schedules; one translation unit per (degree, states, degree) so the build
 // runs in parallel.
-#include "tile_kernel.cuh"
+#include "cell_kernel_q1.cuh"
 
 namespace adm
 {
 void launch_tile_d1_s2_p2(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
 {
   if (a.atomic)
-    launch_tile_t<1, 2, 2, true>(map, a, n_items, stream);
+    launch_cell_q1<2, 2, true>(map, a, n_items, stream);
   else
-    launch_tile_t<1, 2, 2, false>(map, a, n_items, stream);
+    launch_cell_q1<2, 2, false>(map, a, n_items, stream);
 }
 } // namespace adm

@@ -722,6 +722,90 @@ __device__ __noinline__ void face_terms(SmemPhys const &sp, MaterialDesc const *
   }
 }
 
+// Write-out of the node sums res[i] of one thread (rl[i]: bit 4 the thread
+// owns the node, bit 1 / 2 first / last toucher in colour order; gidx[i]:
+// its index in the node vector). Atomic schedule: added into the zeroed
+// target. Coloured schedule: the first toucher writes, later ones add (acc),
+// the last one finalizes -- vmult writes dst, a stage applies the inverse
+// lumped mass and the explicit Runge-Kutta update. All loads, then stores.
+template <bool AT, int NV>
+__device__ __forceinline__ void write_nodes(KernelArgs const &args, MemberData const &md, double *y,
+                                            double const *res, int const *rl, size_t const *gidx)
+{
+  if constexpr (AT)
+  {
+    double *const tgt = args.mode == 2 ? md.acc : args.vdst;
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+      if (rl[i] & 4)
+        atomicAdd(&tgt[gidx[i]], res[i]);
+  }
+  else if (args.mode == 0 || args.mode == 1)
+  {
+    double old[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+      old[i] = ((rl[i] & 4) && (args.mode == 1 || !(rl[i] & 1))) ? args.vdst[gidx[i]] : 0.0;
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+      if (rl[i] & 4)
+        args.vdst[gidx[i]] = old[i] + res[i];
+  }
+  else
+  {
+    double const dt = md.clock[1];
+    double *const znext = args.dst_sel == 1 ? md.za : md.zb;
+    double pa[NV], im[NV], yv[NV], sv[NV], fv[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+    {
+      bool const valid = rl[i] & 4, first = rl[i] & 1, last = rl[i] & 2;
+      size_t const g = gidx[i];
+      pa[i] = (valid && !first) ? md.acc[g] : 0.0;
+      im[i] = (valid && last) ? md.inv_mass[g] : 0.0;
+      yv[i] = (valid && last) ? y[g] : 0.0;
+      sv[i] = (valid && last && args.n_stages > 1 && (args.stage > 0)) ? md.s[g] : 0.0;
+      fv[i] = (valid && last && args.has_f0) ? md.f0[g] : 0.0;
+    }
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+    {
+      if (!(rl[i] & 4))
+        continue;
+      size_t const g = gidx[i];
+      double const total = pa[i] + res[i];
+      if (!(rl[i] & 2))
+      {
+        md.acc[g] = total;
+        continue;
+      }
+      double const f = im[i] * total;
+      if (!isfinite(f))
+        atomicCAS(md.error, 0, (int)DERR_NONFINITE);
+      if (args.n_stages == 1)
+      {
+        y[g] = yv[i] + dt * f;
+      }
+      else if (!args.last)
+      {
+        double zn = yv[i];
+        if (args.has_f0)
+          zn = zn + (dt * args.a_next_f0) * fv[i];
+        zn = zn + (dt * args.a_next) * f;
+        znext[g] = zn;
+        double const sb = (dt * args.b_i) * f;
+        md.s[g] = args.stage == 0 ? sb : sv[i] + sb;
+        if (args.store_f0)
+          md.f0[g] = f;
+      }
+      else
+      {
+        y[g] = yv[i] + (sv[i] + (dt * args.b_i) * f);
+      }
+    }
+  }
+}
+
 // ------------------------------------------------------------ the kernel
 // Loads the physics constants of a member into shared memory.
 template <int NT>
@@ -1274,8 +1358,6 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
     // ---- colour-ordered write-out of the nodes this thread owns: the
     // first tile (in colour order) that touches a node writes it, later
     // ones add, the last one finalizes it. All loads first, then stores.
-    double const dt = (args.mode == 2) ? md.clock[1] : 0.0;
-    double *const znext = args.dst_sel == 1 ? md.za : md.zb;
     bool const own_k = slab > 0 || lz == 0;
     int const Z = DEG * lz + slab;
     int const gz = nz0 + Z;
@@ -1295,78 +1377,7 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
       rl[i] = (own && inside) ? (AT ? 4 : (sp.role[buf][sx + 3 * sy + 9 * sz] | 4)) : 0;
       gidx[i] = gx + (size_t)pitch * (gy + (size_t)nn1 * gz);
     }
-    if constexpr (AT)
-    {
-      // atomic schedule: every colour in one launch, the node sums are
-      // added into the zeroed target and finalized by a separate pass
-      double *const tgt = args.mode == 2 ? md.acc : args.vdst;
-#pragma unroll
-      for (int i = 0; i < NQS; ++i)
-        if (rl[i] & 4)
-          atomicAdd(&tgt[gidx[i]], res[i]);
-    }
-    else if (args.mode == 0 || args.mode == 1)
-    {
-      double old[NQS];
-#pragma unroll
-      for (int i = 0; i < NQS; ++i)
-        old[i] = ((rl[i] & 4) && (args.mode == 1 || !(rl[i] & 1))) ? args.vdst[gidx[i]] : 0.0;
-#pragma unroll
-      for (int i = 0; i < NQS; ++i)
-        if (rl[i] & 4)
-          args.vdst[gidx[i]] = old[i] + res[i];
-    }
-    else
-    {
-      double pa[NQS], im[NQS], yv[NQS], sv[NQS], fv[NQS];
-#pragma unroll
-      for (int i = 0; i < NQS; ++i)
-      {
-        bool const valid = rl[i] & 4, first = rl[i] & 1, last = rl[i] & 2;
-        size_t const g = gidx[i];
-        pa[i] = (valid && !first) ? md.acc[g] : 0.0;
-        im[i] = (valid && last) ? md.inv_mass[g] : 0.0;
-        yv[i] = (valid && last) ? y[g] : 0.0;
-        sv[i] = (valid && last && args.n_stages > 1 && (args.stage > 0)) ? md.s[g] : 0.0;
-        fv[i] = (valid && last && args.has_f0) ? md.f0[g] : 0.0;
-      }
-#pragma unroll
-      for (int i = 0; i < NQS; ++i)
-      {
-        if (!(rl[i] & 4))
-          continue;
-        size_t const g = gidx[i];
-        double const total = pa[i] + res[i];
-        if (!(rl[i] & 2))
-        {
-          md.acc[g] = total;
-          continue;
-        }
-        double const f = im[i] * total;
-        if (!isfinite(f))
-          atomicCAS(md.error, 0, (int)DERR_NONFINITE);
-        if (args.n_stages == 1)
-        {
-          y[g] = yv[i] + dt * f;
-        }
-        else if (!args.last)
-        {
-          double zn = yv[i];
-          if (args.has_f0)
-            zn = zn + (dt * args.a_next_f0) * fv[i];
-          zn = zn + (dt * args.a_next) * f;
-          znext[g] = zn;
-          double const sb = (dt * args.b_i) * f;
-          md.s[g] = args.stage == 0 ? sb : sv[i] + sb;
-          if (args.store_f0)
-            md.f0[g] = f;
-        }
-        else
-        {
-          y[g] = yv[i] + (sv[i] + (dt * args.b_i) * f);
-        }
-      }
-    }
+    write_nodes<AT, NQS>(args, md, y, res, rl, gidx);
     // vmult writes zeros into the row padding of the node layout
     if (!AT && args.mode == 0 && tix == nt0 - 1 && pitch > args.nn[0])
     {
