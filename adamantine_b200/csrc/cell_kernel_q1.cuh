@@ -113,20 +113,25 @@ __global__ void __launch_bounds__(Q1Cell::NT, Q1Cell::MINB)
                                          (int)((wk.xyz >> 11) & 2047u), (int)(wk.xyz >> 22));
   };
 
+  // work distribution as in tile_kernel: dynamic with args.claim (each
+  // further item claimed two items ahead), else strided or blocked
+  bool const dyn = args.claim != nullptr;
+  __shared__ int claimed[2]; // dynamic: the item after the current one, by item parity
   int first, last, step;
-  if (args.blocked)
+  if (dyn || !args.blocked)
+  {
+    first = blockIdx.x;
+    last = n_items;
+    step = gridDim.x;
+  }
+  else
   {
     int const per = (n_items + (int)gridDim.x - 1) / (int)gridDim.x;
     first = (int)blockIdx.x * per;
     last = min(first + per, n_items);
     step = 1;
   }
-  else
-  {
-    first = blockIdx.x;
-    last = n_items;
-    step = gridDim.x;
-  }
+  int second = first + step; // the item after the first
   if (tid == 0)
   {
 #pragma unroll
@@ -134,6 +139,11 @@ __global__ void __launch_bounds__(Q1Cell::NT, Q1Cell::MINB)
       mbar_init(&bars[b], 1);
     fence_mbar_init();
     sp.member = -1;
+    if (dyn)
+    {
+      second = first < last ? atomicAdd(args.claim, 1) + (int)gridDim.x : last;
+      claimed[1] = second;
+    }
   }
   if (tid < 32 && first < last)
   {
@@ -146,8 +156,8 @@ __global__ void __launch_bounds__(Q1Cell::NT, Q1Cell::MINB)
   {
     if (first < last)
       issue(0, first);
-    if (first + step < last)
-      issue(1, first + step);
+    if (second < last)
+      issue(1, second);
   }
 
   // the work item and this thread's cell data, loaded one item ahead
@@ -179,17 +189,28 @@ __global__ void __launch_bounds__(Q1Cell::NT, Q1Cell::MINB)
 
   int it = 0, buf = 0;
   unsigned phase = 0; // completion parity of the current buffer's barrier
-  for (int item = first; item < last; item += step, ++it)
+  for (int item = first; item < last; ++it)
   {
     double const *brick = smem + buf * Q::BRICKP;
     double *const mbuf = mbuf0 + (it & 1) * 4 * NCELL; // [4][NCELL] of this item's parity
+    // the next item (claimed during the previous item, published by its
+    // barrier) and, on thread 0, the one after it: claimed here into the
+    // slot last read at the start of the previous item, its brick requested
+    // after this item's barrier
+    int const next = dyn ? claimed[(it + 1) & 1] : item + step;
+    int next2 = next + step;
+    if (dyn && tid == 0)
+    {
+      next2 = next < last ? atomicAdd(args.claim, 1) + (int)gridDim.x : last;
+      claimed[it & 1] = next2;
+    }
     TileWork const w = nx_w;
     uint32_t const info = nx_info;
     int const cur_pmode = nx_pmode;
     double const cur_pu = nx_pu;
-    if (item + step < last)
+    if (next < last)
     {
-      load_item(item + step);
+      load_item(next);
       if (tid < 32)
       {
         bool const f = source_flag(nx_w);
@@ -486,16 +507,16 @@ __global__ void __launch_bounds__(Q1Cell::NT, Q1Cell::MINB)
         // let the late copy, and the one requested for the next item, land
         // before the CTA leaves (bounded as well)
         mbar_wait(&bars[buf], phase);
-        if (item + step < last)
+        if (next < last)
           mbar_wait(&bars[buf == NBUF - 1 ? 0 : buf + 1], buf == NBUF - 1 ? phase ^ 1u : phase);
       }
       return;
     }
     // request the next-but-one brick into the buffer the previous item used
-    if (tid == 0 && item + 2 * step < last)
+    if (tid == 0 && next2 < last)
     {
       fence_proxy_async();
-      issue(buf == 0 ? NBUF - 1 : buf - 1, item + 2 * step);
+      issue(buf == 0 ? NBUF - 1 : buf - 1, next2);
     }
     if (lz < TZ - 1)
     {
@@ -541,6 +562,7 @@ __global__ void __launch_bounds__(Q1Cell::NT, Q1Cell::MINB)
       buf = 0;
       phase ^= 1u;
     }
+    item = next;
   }
 }
 

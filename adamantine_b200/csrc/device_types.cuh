@@ -153,6 +153,8 @@ struct KernelArgs
   int mode;     // 0 vmult, 1 vmult_add, 2 stage
   int atomic;   // 1: all colours in one launch, node sums by atomics
   int blocked;  // 1: each CTA takes one contiguous run of work items
+  int *claim;   // non-null: items after each CTA's first are claimed from this
+                // counter (zero at the launch), dynamic load balance
   int stage;
   int last;     // last stage of the step (updates y)
   int n_stages; // 1 forward Euler

@@ -136,6 +136,7 @@ void Ensemble::setup()
     for (TileWork const &tw : members_[i]->work_)
       awork_.push_back(TileWork{i, tw.tile, tw.xyz});
   awork_d_.alloc(std::max<size_t>(1, awork_.size()));
+  claim_d_.alloc(8);
   if (!awork_.empty())
     ADM_CK(cudaMemcpyAsync(awork_d_.p, awork_.data(), awork_.size() * sizeof(TileWork),
                            cudaMemcpyHostToDevice, stream_));
@@ -185,6 +186,8 @@ void Ensemble::launch_step(double *solutions)
     a.y_override = nullptr;
     double const *src = i == 0 ? solutions : (a.src_sel == 1 ? za_.p : zb_.p);
     CUtensorMap const map = brick_map(members_[0]->mesh_, src, n, stride_);
+    // the launches claim their work items from zeroed counters
+    ADM_CK(cudaMemsetAsync(claim_d_.p, 0, 8 * sizeof(int32_t), stream_));
     if (schedule_ == Thermal::kScheduleAtomic)
     {
       // member-major list, one contiguous run per CTA: a CTA changes member
@@ -195,6 +198,7 @@ void Ensemble::launch_step(double *solutions)
       if (!awork_.empty())
       {
         a.work = awork_d_.p;
+        a.claim = claim_d_.p;
         launch_tile(deg_, ns_, poly_p_, map, a, (int)awork_.size(), stream_);
         ADM_CK(cudaGetLastError());
       }
@@ -208,6 +212,7 @@ void Ensemble::launch_step(double *solutions)
       if (count == 0)
         continue;
       a.work = work_d_.p + colour_off_[col];
+      a.claim = claim_d_.p + col;
       launch_tile(deg_, ns_, poly_p_, map, a, count, stream_);
       ADM_CK(cudaGetLastError());
     }

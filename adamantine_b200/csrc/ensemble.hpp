@@ -77,6 +77,7 @@ private:
   DevBuf<double> za_, zb_, s_, f0_, acc_;
   DevBuf<MemberData> md_d_;
   DevBuf<TileWork> work_d_, awork_d_;
+  DevBuf<int32_t> claim_d_; // per-colour work counters of the tile launches
   std::vector<TileWork> work_, awork_;
   int colour_off_[9] = {0};
   double *bound_ = nullptr; // solutions array the member table points at

@@ -448,6 +448,7 @@ Thermal::Thermal(adm_config const &cfg, int device, cudaStream_t stream, bool ow
   tile_nbr_d_.alloc(mesh_.n_tiles);
   clock_.alloc(2);
   error_d_.alloc(1);
+  claim_d_.alloc(8);
   mat_d_.alloc(1);
   beam_state_d_.alloc(kMaxBeams);
   member_d_.alloc(1);
@@ -843,11 +844,14 @@ CUtensorMap brick_map(Mesh const &m, double const *base, int n_members, size_t m
 void Thermal::launch_pass(KernelArgs a, double const *src)
 {
   CUtensorMap const map = brick_map(mesh_, src, 1, mesh_.n_nodes);
+  // the launches claim their work items from zeroed counters
+  ADM_CK(cudaMemsetAsync(claim_d_.p, 0, 8 * sizeof(int32_t), stream_));
   if (schedule_ == kScheduleAtomic)
   {
     int const count = colour_off_[8];
     size_t const N = mesh_.n_nodes;
     a.atomic = 1;
+    a.claim = claim_d_.p;
     if (a.mode == 2)
       ADM_CK(cudaMemsetAsync(acc_p_, 0, N * sizeof(double), stream_));
     if (count > 0)
@@ -869,6 +873,7 @@ void Thermal::launch_pass(KernelArgs a, double const *src)
     if (count == 0)
       continue;
     a.work = work_d_.p + colour_off_[col];
+    a.claim = claim_d_.p + col;
     launch_tile(mesh_.deg, ns_, poly_p_, map, a, count, stream_);
     ADM_CK(cudaGetLastError());
   }

@@ -328,6 +328,7 @@ private:
   DevBuf<uint32_t> cell_info_d_, tile_nbr_d_;
   DevBuf<uint8_t> powder_mode_, has_melted_d_;
   DevBuf<int32_t> face_slot_d_, error_d_;
+  DevBuf<int32_t> claim_d_; // per-colour work counters of the tile launches (dynamic claiming)
   DevBuf<int64_t> cells_d_;
   // deposition: per-cell mark, append list, material ids
   DevBuf<int32_t> last_box_d_, list_box_d_;

@@ -877,31 +877,38 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
                    wi.member, &bars[buf]);
   };
 
-  if (tid == 0)
-  {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
-    fence_mbar_init();
-    sp.member = -1;
-  }
-  __syncthreads();
-  // work distribution: strided (CTA b takes items b, b + grid, ...) or, with
-  // args.blocked, one contiguous run of items per CTA (consecutive items of a
-  // member-major list then share the member's constants)
+  // work distribution: with args.claim, dynamic -- CTA b starts with item
+  // b and claims each further item from the launch's counter, one item ahead
+  // (a CTA held up by a slow tile, near the melt pool, takes fewer); else
+  // strided (CTA b takes items b, b + grid, ...) or, with args.blocked, one
+  // contiguous run of items per CTA (consecutive items of a member-major
+  // list then share the member's constants)
+  bool const dyn = args.claim != nullptr;
+  __shared__ int claimed[2]; // dynamic: the item after the current one, by item parity
   int first, last, step;
-  if (args.blocked)
+  if (dyn || !args.blocked)
+  {
+    first = blockIdx.x;
+    last = n_items;
+    step = gridDim.x;
+  }
+  else
   {
     int const per = (n_items + (int)gridDim.x - 1) / (int)gridDim.x;
     first = (int)blockIdx.x * per;
     last = min(first + per, n_items);
     step = 1;
   }
-  else
+  if (tid == 0)
   {
-    first = blockIdx.x;
-    last = n_items;
-    step = gridDim.x;
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    fence_mbar_init();
+    sp.member = -1;
+    if (dyn)
+      claimed[1] = first < last ? atomicAdd(args.claim, 1) + (int)gridDim.x : last;
   }
+  __syncthreads();
   if (tid == 0 && first < last)
     issue(0, first);
 
@@ -935,16 +942,19 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
     load_item(first);
 
   int it = 0;
-  for (int item = first; item < last; item += step, ++it)
+  for (int item = first; item < last; ++it)
   {
     int const buf = it & 1;
+    // the next item: claimed during the previous one (published by its
+    // barriers), or the next of the static distribution
+    int const next = dyn ? claimed[(it + 1) & 1] : item + step;
     double const *brick = smem + buf * T_::BRICKP;
     TileWork const w = nx_w;
     uint32_t const cur_info = nx_info;
     int const cur_pmode = nx_pmode;
     double const cur_pu = nx_pu;
-    if (item + step < last)
-      load_item(item + step);
+    if (next < last)
+      load_item(next);
     MemberData const &md = args.members[w.member];
     MaterialDesc const *gm = md.mat;
     int const tile = w.tile;
@@ -1091,11 +1101,19 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
       }
       return;
     }
-    // prefetch the next item's brick into the other buffer
-    if (tid == 0 && item + step < last)
+    // prefetch the next item's brick into the other buffer, and claim the
+    // item after it (read at the start of the next item, after this item's
+    // flux and node barriers; the slot's previous value was read at the
+    // start of the previous item)
+    if (tid == 0)
     {
-      fence_proxy_async();
-      issue(buf ^ 1, item + step);
+      if (next < last)
+      {
+        fence_proxy_async();
+        issue(buf ^ 1, next);
+      }
+      if (dyn)
+        claimed[it & 1] = next < last ? atomicAdd(args.claim, 1) + (int)gridDim.x : last;
     }
     bool const do_src = sp.src_on != 0;
     double Tq[NQS], az[NQS];
@@ -1390,6 +1408,7 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
           args.vdst[args.nn[0] + X + (size_t)pitch * (gy + (size_t)nn1 * gz)] = 0.0;
       }
     }
+    item = next;
   }
 }
 

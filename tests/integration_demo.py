@@ -77,10 +77,17 @@ def gold_short():
     return np.load(os.path.join(HERE, "golden", "integration_3d_gold_short.npz"))["values"].astype(np.float64)
 
 
+def driver_dt(t, dt, duration):
+    """The driver's step at time t: dt, cut so that the run ends at the
+    duration (application/adamantine.hh:1110-1111)."""
+    return duration - t if t + dt > duration else dt
+
+
 def run_oracle(cfg, boxes, dt=DT, duration=DURATION):
-    """The driver loop on the oracle: the deposition window, then one step,
-    while t < duration. Returns (field, active cells, number of steps,
-    oracle)."""
+    """The driver loop on the oracle (application/adamantine.hh:1063-1285):
+    while t < duration, the step is cut to end at the duration
+    (:1110-1111), then the deposition window, then one step. Returns (field,
+    active cells, number of steps, oracle)."""
     import oracle_py
     from deposition_oracle import activate
 
@@ -93,6 +100,7 @@ def run_oracle(cfg, boxes, dt=DT, duration=DURATION):
     h = [geo.extent[d] / geo.n_cells[d] for d in range(3)]
     t, window_end, n = 0.0, -1.0, 0
     while t < duration:
+        dt = driver_dt(t, dt, duration)
         tol = dt * 1e-6
         if t - window_end > -tol:
             s = int(np.searchsorted(boxes.time, t - tol, side="left"))

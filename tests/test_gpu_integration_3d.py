@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from dealii_order import dof_to_node
-from integration_demo import BOX, DT, DURATION, NEW_T, demo_config, gold_text, run_oracle
+from integration_demo import BOX, DT, DURATION, NEW_T, demo_config, driver_dt, gold_text, run_oracle
 from pairs import rel_max
 
 from adamantine_b200.deposition import Deposition, deposition_boxes
@@ -28,8 +28,9 @@ def test_integration_3d_on_the_gpu(schedule):
     y = g.initialize_dof_vector(300.0)
     t, n = 0.0, 0
     while t < DURATION:
-        dep.step(t, DT, NEW_T, y)
-        t = g.evolve_one_time_step(t, DT, y)
+        dt = driver_dt(t, DT, DURATION)
+        dep.step(t, dt, NEW_T, y)
+        t = g.evolve_one_time_step(t, dt, y)
         n += 1
     assert n == 100 and g.device_error() == 0
     y_ref, active, _, _ = run_oracle(cfg, boxes)
@@ -55,8 +56,9 @@ def test_integration_3d_checkpoint_restart(tmp_path, exact):
     def run(g, dep, y, t, n_stop):
         n = 0
         while t < DURATION and n < n_stop:
-            dep.step(t, DT, NEW_T, y)
-            t = g.evolve_one_time_step(t, DT, y)
+            dt = driver_dt(t, DT, DURATION)
+            dep.step(t, dt, NEW_T, y)
+            t = g.evolve_one_time_step(t, dt, y)
             n += 1
         return t
 
@@ -96,8 +98,9 @@ def test_vtk_output_of_the_demo(tmp_path):
     t, n = 0.0, 0
     pp.write_thermal_output(0, t, y)
     while t < DURATION:
-        dep.step(t, DT, NEW_T, y)
-        t = g.evolve_one_time_step(t, DT, y)
+        dt = driver_dt(t, DT, DURATION)
+        dep.step(t, dt, NEW_T, y)
+        t = g.evolve_one_time_step(t, dt, y)
         n += 1
     pp.write_thermal_output(n, t, y)
     pp.write_pvd()
