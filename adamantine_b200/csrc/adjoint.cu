@@ -456,7 +456,7 @@ public:
           x.mu_max_next = mumax_.p + (slot ^ 1);
           x.n_sel = nsel_.p + slot;
           x.n_sel_next = nsel_.p + (slot ^ 1);
-          x.work = t.work_d_.p;
+          x.work = t.awork_d_.p;
           x.n_items = count;
           x.act_cur = act_cur_;
           x.act_next = act_next_;
@@ -605,7 +605,7 @@ private:
     int const count = t.colour_off_[8];
     if (count == 0)
       return;
-    A.k.work = work ? work : t.work_d_.p;
+    A.k.work = work ? work : t.awork_d_.p;
     CUtensorMap const ym = brick_map(t.mesh_, A.yv, 1, n_);
     CUtensorMap const mm = brick_map(t.mesh_, A.mu, 1, n_);
     launch_adjoint(t.mesh_.deg, t.ns_, ym, mm, A, count, stream ? stream : t.stream_);

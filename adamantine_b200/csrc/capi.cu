@@ -277,6 +277,22 @@ int adm_get_schedule(adm_thermal const *h, int32_t *schedule)
   });
 }
 
+int adm_set_cells_per_thread(adm_thermal *h, int32_t n)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h, "null handle");
+    as(h)->set_cells_per_thread(n);
+  });
+}
+
+int adm_get_cells_per_thread(adm_thermal const *h, int32_t *n)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && n, "null argument");
+    *n = as(h)->cells_per_thread();
+  });
+}
+
 int adm_autotune(adm_thermal *h, double const *field, int32_t *schedule, double *ms)
 {
   return adm::guard([&] {

@@ -1,4 +1,5 @@
-// FE_Q(1) variant of the fused tile kernel: one thread per hex cell.
+// FE_Q(1) variant of the fused tile kernel: one thread per hex cell (or per
+// column of two).
 //
 // Same tiles (8 x 4 x 4 cells), node bricks, work lists, tensor maps, launch
 // schedules and arithmetic as tile_kernel<1, ...> in tile_kernel.cuh, but a
@@ -20,21 +21,27 @@
 namespace adm
 {
 
+// CZ cells per thread, stacked in z (1 or 2): with 2, a thread merges the
+// node level its two cells share in registers and pays the per-item work
+// (prefetch, waits, the barrier, the write-out bookkeeping) once for both.
+template <int CZ>
 struct Q1Cell
 {
   static constexpr int TX = 8, TY = 4, TZ = 4;
   static constexpr int NCELL = TX * TY * TZ;
-  static constexpr int NT = NCELL; // one thread per cell
-  static constexpr int MINB = 3;   // resident CTAs per SM the register budget targets
+  static constexpr int NT = NCELL / CZ; // threads: one per column of CZ cells
+  static constexpr int NPZ = TZ / CZ;   // thread layers (warps) in z
+  static constexpr int MINB = CZ == 1 ? 3 : 4; // resident CTAs per SM the register budget targets (12 or 8 warps)
   static constexpr int BXP = TD<1>::BXP, BY = TD<1>::BY, BZ = TD<1>::BZ;
   static constexpr int BRICKP = (BXP * BY * BZ + 15) / 16 * 16;
   static constexpr int NBUF = 3;
   // dynamic shared memory: NBUF staged bricks and the z-shared node sums
-  // [2][4][NCELL] (one set per item parity)
-  static constexpr size_t SMEM = sizeof(double) * (NBUF * BRICKP + 2 * 4 * NCELL);
+  // [2][4][NT] (one set per item parity)
+  static constexpr size_t SMEM = sizeof(double) * (NBUF * BRICKP + 2 * 4 * NT);
+  static_assert(TX == TD<1>::TX && TY == TD<1>::TY && TZ == TD<1>::TZ,
+                "the Q1 cell kernel uses the tiles of the Q1 tile kernel");
+  static_assert(TZ % CZ == 0, "whole cell columns per thread");
 };
-static_assert(Q1Cell::TX == TD<1>::TX && Q1Cell::TY == TD<1>::TY && Q1Cell::TZ == TD<1>::TZ,
-              "the Q1 cell kernel uses the tiles of the Q1 tile kernel");
 
 // Does the tile (tix, tiy, tiz) meet the support of any source of a member
 // whose current beam states are `beams` (exact: it skips only points where
@@ -72,32 +79,270 @@ __device__ __forceinline__ bool tile_meets_source(KernelArgs const &args, BeamSt
   return hit;
 }
 
+// One FE_Q(1) cell of a tile (cell lx, ly, lz of the tile whose first cell
+// is ncx0, ncy0, ncz0; info / cur_pmode / cur_pu its prefetched cell data):
+// gather the 8 nodes from the staged brick, interpolate to the 8 Gauss
+// points, evaluate the physics (straight-line when every point is cold, the
+// out-of-line pass otherwise), integrate back, add the face terms, write the
+// cell's liquid sum and powder-storage switch. res[e] (e = i + 2 j + 4 k)
+// receives the cell's node results, zero when it is inactive or its brick
+// did not arrive.
+template <int NS, int P, bool FC>
+__device__ __forceinline__ void q1_cell(SmemPhys const &sp, MemberData const &md, KernelArgs const &args,
+                                        double const *brick, int lx, int ly, int lz, int ncx0, int ncy0,
+                                        int ncz0, uint32_t info, int cur_pmode, double cur_pu, bool arrived,
+                                        bool do_src, double *res)
+{
+  constexpr int BXP = TD<1>::BXP, BY = TD<1>::BY;
+  MaterialDesc const *gm = md.mat;
+  int const cx = ncx0 + lx, cy = ncy0 + ly, cz = ncz0 + lz;
+  bool const in_domain = cx < args.nc[0] && cy < args.nc[1] && cz < args.nc[2];
+  size_t const c = in_domain ? cx + (size_t)args.nc[0] * (cy + (size_t)args.nc[1] * cz) : 0;
+  bool const active = arrived && (info & CI_ACTIVE) != 0;
+  int const mat = (info >> CI_MAT_SHIFT) & 15;
+#pragma unroll
+  for (int e = 0; e < 8; ++e)
+    res[e] = 0.0;
+  double liq = 0.0;
+  uint32_t cmask = 0;
+  int pmode = 0;
+  double pu = 0.0;
+  if (active)
+  {
+    // nodes (i, j, k) of the cell, e = i + 2 j + 4 k; Gauss points
+    // q = qa + 2 qb + 4 qc
+    double T[8];
+    {
+      double u[8], w1[8], w2[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e)
+        u[e] = brick[(lx + (e & 1)) + BXP * ((ly + ((e >> 1) & 1)) + BY * (lz + (e >> 2)))];
+#pragma unroll
+      for (int jk = 0; jk < 4; ++jk)
+#pragma unroll
+        for (int qa = 0; qa < 2; ++qa)
+          w1[qa + 2 * jk] = row_dot<1, M_S>(args.S, qa, &u[2 * jk], 1);
+#pragma unroll
+      for (int qa = 0; qa < 2; ++qa)
+#pragma unroll
+        for (int k = 0; k < 2; ++k)
+#pragma unroll
+          for (int qb = 0; qb < 2; ++qb)
+            w2[qa + 2 * qb + 4 * k] = row_dot<1, M_S>(args.S, qb, &w1[qa + 4 * k], 2);
+#pragma unroll
+      for (int ab = 0; ab < 4; ++ab)
+#pragma unroll
+        for (int qc = 0; qc < 2; ++qc)
+          T[ab + 4 * qc] = row_dot<1, M_S>(args.S, qc, &w2[ab], 4);
+    }
+
+    if (NS == 3)
+    {
+      pmode = cur_pmode;
+      if (pmode == 1)
+        pu = cur_pu;
+    }
+    double cs = 1.0, sn = 0.0;
+    if (sp.has_rotation)
+    {
+      cs = md.cosv[c];
+      sn = md.sinv[c];
+    }
+    bool const fast_ok = !sp.use_table && sp.isotropic && !sp.has_rotation;
+    // below the solidus a cell whose powder ratio is uniformly 0 or 1 is in
+    // one pure state: `cold` names it (or -1)
+    double const solidus = sp.props[mat][Q_SOLIDUS];
+    int cold = -1;
+    if (fast_ok)
+    {
+      if (NS < 3 || pmode == 0)
+        cold = 0;
+      else if (pmode == 1 && pu == 1.0)
+        cold = 2;
+    }
+    constexpr int PS = kMaxStates * kMaxPoly; // stride between properties
+    bool all_cold = cold >= 0;
+    if (NS > 1)
+    {
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        all_cold &= T[q] < solidus;
+    }
+    // r: the test-function values at the Gauss points -- the fluxes after
+    // the collocation D^T in x, y and z, and the source term -- before
+    // the S^T back to the nodes
+    double r[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      r[q] = 0.0;
+    if (all_cold)
+    {
+      double const *cold_c = &sp.poly[mat][0][cold][0];
+      double crho[P + 1], ccp[P + 1], ck[P + 1];
+#pragma unroll
+      for (int k = 0; k <= P; ++k)
+      {
+        crho[k] = cold_c[P_DENSITY * PS + k];
+        ccp[k] = cold_c[P_SPECIFIC_HEAT * PS + k];
+        ck[k] = cold_c[P_KX * PS + k];
+      }
+      // cf = -k / (rho c_p) at the points
+      double cf[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+      {
+        double const Tq = T[q];
+        double const inv = recip(horner_fixed<P>(crho, Tq) * horner_fixed<P>(ccp, Tq));
+        cf[q] = -inv * horner_fixed<P>(ck, Tq);
+      }
+      // Q1 structure (checked on the host): the collocation derivative of
+      // the two Gauss points is one row repeated, D[q] = (-d, d), and all
+      // eight points weigh 1/8 (cw[q] the same for every q). So along a
+      // direction both points of a pair (i0, i1) see the gradient
+      // d (T1 - T0), and the D^T of their fluxes adds t to the test value
+      // of i1 and -t to that of i0, with
+      // t = d^2 cw_d (T1 - T0) (cf_0 + cf_1).
+      double const d = args.D[0][1];
+      double const K[3] = {d * d * args.cw[0][0], d * d * args.cw[0][1], d * d * args.cw[0][2]};
+#pragma unroll
+      for (int dir = 0; dir < 3; ++dir)
+      {
+        int const stride = 1 << dir; // point index step along the direction
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+        {
+          // the pair's first point: p's two bits fill the other directions
+          int const lo = p & ((1 << dir) - 1), hi = p >> dir;
+          int const i0 = lo + (hi << (dir + 1)), i1 = i0 + stride;
+          double const t = (K[dir] * (T[i1] - T[i0])) * (cf[i0] + cf[i1]);
+          r[i1] += t;
+          r[i0] -= t;
+        }
+      }
+      if (do_src)
+      {
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+        {
+          int const qa = q & 1, qb = (q >> 1) & 1, qc = q >> 2;
+          double const Tq = T[q];
+          double const inv = recip(horner_fixed<P>(crho, Tq) * horner_fixed<P>(ccp, Tq));
+          double const px = (args.origin[0] + cx * args.h[0]) + args.qx[qa] * args.h[0];
+          double const py = (args.origin[1] + cy * args.h[1]) + args.qx[qb] * args.h[1];
+          double const pz = (args.origin[2] + cz * args.h[2]) + args.qx[qc] * args.h[2];
+          r[q] += beam_sum(sp, px, py, pz) * inv * args.cw[q][3];
+        }
+      }
+    }
+    else
+    {
+      // mixed states, the mushy range, tables, anisotropy or rotation: the
+      // out-of-line pass of the Q1 tile kernel, one Gauss-point level at a
+      // time, on copies of the level's arrays
+#pragma unroll
+      for (int qc = 0; qc < 2; ++qc)
+      {
+        double tq_l[4], az_l[4], axy_l[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+        {
+          tq_l[i] = T[i + 4 * qc];
+          az_l[i] = row_dot<1, M_D>(args.D, qc, &T[i], 4);
+          axy_l[i] = 0.0;
+        }
+        double lacc = 0.0;
+        uint32_t cm = 0;
+        general_level<1, NS, P>(sp, gm, md, args, mat, qc, cold, pmode, pu, c * 8 + (size_t)4 * qc, cs, sn,
+                                fast_ok, do_src, cx, cy, cz, tq_l, az_l, axy_l, &lacc, &cm);
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+        {
+          r[i + 4 * qc] += axy_l[i];
+#pragma unroll
+          for (int m = 0; m < 2; ++m)
+            r[i + 4 * m] = entry_mac<1, M_D>(args.D, qc, m, az_l[i], r[i + 4 * m]);
+        }
+        liq += lacc;
+        cmask |= cm << (4 * qc);
+      }
+    }
+    // S^T in z, y and x back to the nodes
+    double r1[8], r2[8];
+#pragma unroll
+    for (int ab = 0; ab < 4; ++ab)
+#pragma unroll
+      for (int k = 0; k < 2; ++k)
+        r1[ab + 4 * k] = col_dot<1, M_S>(args.S, k, &r[ab], 4);
+#pragma unroll
+    for (int qa = 0; qa < 2; ++qa)
+#pragma unroll
+      for (int k = 0; k < 2; ++k)
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+          r2[qa + 2 * j + 4 * k] = col_dot<1, M_S>(args.S, j, &r1[qa + 4 * k], 2);
+#pragma unroll
+    for (int jk = 0; jk < 4; ++jk)
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+        res[i + 2 * jk] = col_dot<1, M_S>(args.S, i, &r2[2 * jk], 1);
+
+    // convective / radiative faces (face_local_apply,
+    // source/ThermalOperator.templates.hh:619-751), per node level
+    if (FC && ((info >> CI_FACE_SHIFT) & 63u))
+    {
+#pragma unroll
+      for (int lev = 0; lev < 2; ++lev)
+      {
+        double fo[4];
+        face_terms<1, NS>(sp, gm, md, args, brick, lx, ly, lz, lev, info, mat, c, fo);
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          res[e + 4 * lev] += fo[e];
+      }
+    }
+    // state write-back: the liquid sum and, when a point of a uniform
+    // powder cell changed, the switch to per-point storage
+    if (NS > 1)
+      md.liquid_sum[c] = liq;
+    if (NS == 3 && pmode != 2 && cmask)
+    {
+      md.powder_mode[c] = 2;
+#pragma unroll
+      for (int e = 0; e < 8; ++e)
+        if (!((cmask >> e) & 1u))
+          md.powder_q[c * 8 + e] = pu;
+    }
+  }
+
+}
+
 // The persistent loop over work items (as in tile_kernel): CTA b processes
 // items b, b + grid, ... (or one contiguous run with args.blocked).
-// Per item and thread (cell lx, ly, lz of the tile): gather the 8 nodes,
-// interpolate to the 8 Gauss points, evaluate the physics, integrate back,
-// add the face terms, merge the shared nodes, write out. One CTA barrier per
+// Per item and thread (the column of CZ cells lx, ly, CZ pz .. CZ pz + CZ - 1
+// of the tile): each cell's 8 nodes to its 8 Gauss points, the physics and
+// back (q1_cell), then the shared nodes merged and written out. One CTA barrier per
 // item (before the z-shared node sums are read); per-item shared state that
 // a thread still finishing the previous item may read (roles, the source
 // flag, the z sums) alternates between two copies by item parity, and the
 // brick of item k + 2 is requested after the barrier of item k into the
 // buffer that item k - 1 used.
-template <int NS, int P, bool AT, bool FC>
-__global__ void __launch_bounds__(Q1Cell::NT, Q1Cell::MINB)
+template <int NS, int P, bool AT, bool FC, int CZ>
+__global__ void __launch_bounds__(Q1Cell<CZ>::NT, Q1Cell<CZ>::MINB)
     cell_kernel_q1(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ KernelArgs args, int n_items)
 {
-  using Q = Q1Cell;
-  constexpr int TX = Q::TX, TY = Q::TY, TZ = Q::TZ, NCELL = Q::NCELL, NT = Q::NT;
+  using Q = Q1Cell<CZ>;
+  constexpr int TX = Q::TX, TY = Q::TY, TZ = Q::TZ, NT = Q::NT, NPZ = Q::NPZ;
+  constexpr int NV = 4 * (CZ + 1); // node results of a thread: CZ + 1 levels of 4
   constexpr int BXP = Q::BXP, BY = Q::BY, BZ = Q::BZ, NBUF = Q::NBUF;
   constexpr unsigned kBoxBytes = sizeof(double) * BXP * BY * BZ;
   extern __shared__ __align__(128) double smem[];
-  double *const mbuf0 = smem + NBUF * Q::BRICKP; // [2][4][NCELL]: z-shared node sums per item parity
+  double *const mbuf0 = smem + NBUF * Q::BRICKP; // [2][4][NT]: z-shared node sums per item parity
   __shared__ SmemPhys sp;
   __shared__ __align__(8) uint64_t bars[NBUF];
   __shared__ int src_flag[2];
 
   int const tid = threadIdx.x;
-  int const lx = tid % TX, ly = (tid / TX) % TY, lz = tid / (TX * TY);
+  int const lx = tid % TX, ly = (tid / TX) % TY, pz = tid / (TX * TY); // cells CZ pz .. CZ pz + CZ - 1
   int const nt0 = args.nt[0], nt1 = args.nt[1];
   int const pitch = args.pitch, nn1 = args.nn[1];
 
@@ -115,7 +360,7 @@ __global__ void __launch_bounds__(Q1Cell::NT, Q1Cell::MINB)
 
   // work distribution as in tile_kernel: dynamic with args.claim (each
   // further item claimed two items ahead), else strided or blocked
-  bool const dyn = args.claim != nullptr;
+  bool const dyn = args.claim != nullptr && !args.blocked;
   __shared__ int claimed[2]; // dynamic: the item after the current one, by item parity
   int first, last, step;
   if (dyn || !args.blocked)
@@ -160,27 +405,31 @@ __global__ void __launch_bounds__(Q1Cell::NT, Q1Cell::MINB)
       issue(1, second);
   }
 
-  // the work item and this thread's cell data, loaded one item ahead
+  // the work item and this thread's cells' data, loaded one item ahead
   TileWork nx_w{0, 0, 0u};
-  uint32_t nx_info = 0u;
-  int nx_pmode = 0;
-  double nx_pu = 0.0;
+  uint32_t nx_info[CZ];
+  int nx_pmode[CZ];
+  double nx_pu[CZ];
   auto load_item = [&](int item2) {
     nx_w = args.work[item2];
     MemberData const &mk = args.members[nx_w.member];
-    int const kx = TX * (int)(nx_w.xyz & 2047u) + lx, ky = TY * (int)((nx_w.xyz >> 11) & 2047u) + ly,
-              kz = TZ * (int)(nx_w.xyz >> 22) + lz;
-    nx_info = 0u;
-    nx_pmode = 0;
-    nx_pu = 0.0;
-    if (kx < args.nc[0] && ky < args.nc[1] && kz < args.nc[2])
+    int const kx = TX * (int)(nx_w.xyz & 2047u) + lx, ky = TY * (int)((nx_w.xyz >> 11) & 2047u) + ly;
+#pragma unroll
+    for (int j = 0; j < CZ; ++j)
     {
-      size_t const kc = kx + (size_t)args.nc[0] * (ky + (size_t)args.nc[1] * kz);
-      nx_info = mk.cell_info[kc];
-      if (NS == 3)
+      int const kz = TZ * (int)(nx_w.xyz >> 22) + CZ * pz + j;
+      nx_info[j] = 0u;
+      nx_pmode[j] = 0;
+      nx_pu[j] = 0.0;
+      if (kx < args.nc[0] && ky < args.nc[1] && kz < args.nc[2])
       {
-        nx_pmode = mk.powder_mode[kc];
-        nx_pu = mk.powder_cell[kc];
+        size_t const kc = kx + (size_t)args.nc[0] * (ky + (size_t)args.nc[1] * kz);
+        nx_info[j] = mk.cell_info[kc];
+        if (NS == 3)
+        {
+          nx_pmode[j] = mk.powder_mode[kc];
+          nx_pu[j] = mk.powder_cell[kc];
+        }
       }
     }
   };
@@ -192,7 +441,7 @@ __global__ void __launch_bounds__(Q1Cell::NT, Q1Cell::MINB)
   for (int item = first; item < last; ++it)
   {
     double const *brick = smem + buf * Q::BRICKP;
-    double *const mbuf = mbuf0 + (it & 1) * 4 * NCELL; // [4][NCELL] of this item's parity
+    double *const mbuf = mbuf0 + (it & 1) * 4 * NT; // [4][NT] of this item's parity
     // the next item (claimed during the previous item, published by its
     // barrier) and, on thread 0, the one after it: claimed here into the
     // slot last read at the start of the previous item, its brick requested
@@ -205,9 +454,16 @@ __global__ void __launch_bounds__(Q1Cell::NT, Q1Cell::MINB)
       claimed[it & 1] = next2;
     }
     TileWork const w = nx_w;
-    uint32_t const info = nx_info;
-    int const cur_pmode = nx_pmode;
-    double const cur_pu = nx_pu;
+    uint32_t info[CZ];
+    int cur_pmode[CZ];
+    double cur_pu[CZ];
+#pragma unroll
+    for (int j = 0; j < CZ; ++j)
+    {
+      info[j] = nx_info[j];
+      cur_pmode[j] = nx_pmode[j];
+      cur_pu[j] = nx_pu[j];
+    }
     if (next < last)
     {
       load_item(next);
@@ -219,7 +475,6 @@ __global__ void __launch_bounds__(Q1Cell::NT, Q1Cell::MINB)
       }
     }
     MemberData const &md = args.members[w.member];
-    MaterialDesc const *gm = md.mat;
     int const tile = w.tile;
     int const tix = w.xyz & 2047u, tiy = (w.xyz >> 11) & 2047u, tiz = w.xyz >> 22;
     int const colour = (tix & 1) | ((tiy & 1) << 1) | ((tiz & 1) << 2);
@@ -264,221 +519,32 @@ __global__ void __launch_bounds__(Q1Cell::NT, Q1Cell::MINB)
     bool const arrived = mbar_wait(&bars[buf], phase);
     bool const do_src = src_flag[it & 1] != 0;
 
-    int const cx = ncx0 + lx, cy = ncy0 + ly, cz = ncz0 + lz;
-    bool const in_domain = cx < args.nc[0] && cy < args.nc[1] && cz < args.nc[2];
-    size_t const c = in_domain ? cx + (size_t)args.nc[0] * (cy + (size_t)args.nc[1] * cz) : 0;
-    bool const active = arrived && (info & CI_ACTIVE) != 0;
-    int const mat = (info >> CI_MAT_SHIFT) & 15;
-    double res[8];
+    // the thread's CZ cells, their node results summed per node level
+    double res[NV];
 #pragma unroll
-    for (int e = 0; e < 8; ++e)
+    for (int e = 0; e < NV; ++e)
       res[e] = 0.0;
-    double liq = 0.0;
-    uint32_t cmask = 0;
-    int pmode = 0;
-    double pu = 0.0;
-    if (active)
+#pragma unroll
+    for (int j = 0; j < CZ; ++j)
     {
-      // nodes (i, j, k) of the cell, e = i + 2 j + 4 k; Gauss points
-      // q = qa + 2 qb + 4 qc
-      double T[8];
+      double cres[8];
+      q1_cell<NS, P, FC>(sp, md, args, brick, lx, ly, CZ * pz + j, ncx0, ncy0, ncz0, info[j], cur_pmode[j],
+                         cur_pu[j], arrived, do_src, cres);
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
       {
-        double u[8], w1[8], w2[8];
-#pragma unroll
-        for (int e = 0; e < 8; ++e)
-          u[e] = brick[(lx + (e & 1)) + BXP * ((ly + ((e >> 1) & 1)) + BY * (lz + (e >> 2)))];
-#pragma unroll
-        for (int jk = 0; jk < 4; ++jk)
-#pragma unroll
-          for (int qa = 0; qa < 2; ++qa)
-            w1[qa + 2 * jk] = row_dot<1, M_S>(args.S, qa, &u[2 * jk], 1);
-#pragma unroll
-        for (int qa = 0; qa < 2; ++qa)
-#pragma unroll
-          for (int k = 0; k < 2; ++k)
-#pragma unroll
-            for (int qb = 0; qb < 2; ++qb)
-              w2[qa + 2 * qb + 4 * k] = row_dot<1, M_S>(args.S, qb, &w1[qa + 4 * k], 2);
-#pragma unroll
-        for (int ab = 0; ab < 4; ++ab)
-#pragma unroll
-          for (int qc = 0; qc < 2; ++qc)
-            T[ab + 4 * qc] = row_dot<1, M_S>(args.S, qc, &w2[ab], 4);
-      }
-
-      if (NS == 3)
-      {
-        pmode = cur_pmode;
-        if (pmode == 1)
-          pu = cur_pu;
-      }
-      double cs = 1.0, sn = 0.0;
-      if (sp.has_rotation)
-      {
-        cs = md.cosv[c];
-        sn = md.sinv[c];
-      }
-      bool const fast_ok = !sp.use_table && sp.isotropic && !sp.has_rotation;
-      // below the solidus a cell whose powder ratio is uniformly 0 or 1 is in
-      // one pure state: `cold` names it (or -1)
-      double const solidus = sp.props[mat][Q_SOLIDUS];
-      int cold = -1;
-      if (fast_ok)
-      {
-        if (NS < 3 || pmode == 0)
-          cold = 0;
-        else if (pmode == 1 && pu == 1.0)
-          cold = 2;
-      }
-      constexpr int PS = kMaxStates * kMaxPoly; // stride between properties
-      bool all_cold = cold >= 0;
-      if (NS > 1)
-      {
-#pragma unroll
-        for (int q = 0; q < 8; ++q)
-          all_cold &= T[q] < solidus;
-      }
-      // r: the test-function values at the Gauss points -- the fluxes after
-      // the collocation D^T in x, y and z, and the source term -- before
-      // the S^T back to the nodes
-      double r[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q)
-        r[q] = 0.0;
-      if (all_cold)
-      {
-        double const *cold_c = &sp.poly[mat][0][cold][0];
-        double crho[P + 1], ccp[P + 1], ck[P + 1];
-#pragma unroll
-        for (int k = 0; k <= P; ++k)
-        {
-          crho[k] = cold_c[P_DENSITY * PS + k];
-          ccp[k] = cold_c[P_SPECIFIC_HEAT * PS + k];
-          ck[k] = cold_c[P_KX * PS + k];
-        }
-#pragma unroll
-        for (int q = 0; q < 8; ++q)
-        {
-          int const qa = q & 1, qb = (q >> 1) & 1, qc = q >> 2;
-          double const Tq = T[q];
-          double const gx = row_dot<1, M_D>(args.D, qa, &T[2 * qb + 4 * qc], 1);
-          double const gy = row_dot<1, M_D>(args.D, qb, &T[qa + 4 * qc], 2);
-          double const gz = row_dot<1, M_D>(args.D, qc, &T[qa + 2 * qb], 4);
-          double const inv = recip(horner_fixed<P>(crho, Tq) * horner_fixed<P>(ccp, Tq));
-          double const cf = -inv * horner_fixed<P>(ck, Tq);
-          double const fx = (cf * args.cw[q][0]) * gx;
-          double const fy = (cf * args.cw[q][1]) * gy;
-          double const fz = (cf * args.cw[q][2]) * gz;
-#pragma unroll
-          for (int m = 0; m < 2; ++m)
-          {
-            r[m + 2 * qb + 4 * qc] = entry_mac<1, M_D>(args.D, qa, m, fx, r[m + 2 * qb + 4 * qc]);
-            r[qa + 2 * m + 4 * qc] = entry_mac<1, M_D>(args.D, qb, m, fy, r[qa + 2 * m + 4 * qc]);
-            r[qa + 2 * qb + 4 * m] = entry_mac<1, M_D>(args.D, qc, m, fz, r[qa + 2 * qb + 4 * m]);
-          }
-        }
-        if (do_src)
-        {
-#pragma unroll
-          for (int q = 0; q < 8; ++q)
-          {
-            int const qa = q & 1, qb = (q >> 1) & 1, qc = q >> 2;
-            double const Tq = T[q];
-            double const inv = recip(horner_fixed<P>(crho, Tq) * horner_fixed<P>(ccp, Tq));
-            double const px = (args.origin[0] + cx * args.h[0]) + args.qx[qa] * args.h[0];
-            double const py = (args.origin[1] + cy * args.h[1]) + args.qx[qb] * args.h[1];
-            double const pz = (args.origin[2] + cz * args.h[2]) + args.qx[qc] * args.h[2];
-            r[q] += beam_sum(sp, px, py, pz) * inv * args.cw[q][3];
-          }
-        }
-      }
-      else
-      {
-        // mixed states, the mushy range, tables, anisotropy or rotation: the
-        // out-of-line pass of the Q1 tile kernel, one Gauss-point level at a
-        // time, on copies of the level's arrays
-#pragma unroll
-        for (int qc = 0; qc < 2; ++qc)
-        {
-          double tq_l[4], az_l[4], axy_l[4];
-#pragma unroll
-          for (int i = 0; i < 4; ++i)
-          {
-            tq_l[i] = T[i + 4 * qc];
-            az_l[i] = row_dot<1, M_D>(args.D, qc, &T[i], 4);
-            axy_l[i] = 0.0;
-          }
-          double lacc = 0.0;
-          uint32_t cm = 0;
-          general_level<1, NS, P>(sp, gm, md, args, mat, qc, cold, pmode, pu, c * 8 + (size_t)4 * qc, cs, sn,
-                                  fast_ok, do_src, cx, cy, cz, tq_l, az_l, axy_l, &lacc, &cm);
-#pragma unroll
-          for (int i = 0; i < 4; ++i)
-          {
-            r[i + 4 * qc] += axy_l[i];
-#pragma unroll
-            for (int m = 0; m < 2; ++m)
-              r[i + 4 * m] = entry_mac<1, M_D>(args.D, qc, m, az_l[i], r[i + 4 * m]);
-          }
-          liq += lacc;
-          cmask |= cm << (4 * qc);
-        }
-      }
-      // S^T in z, y and x back to the nodes
-      double r1[8], r2[8];
-#pragma unroll
-      for (int ab = 0; ab < 4; ++ab)
-#pragma unroll
-        for (int k = 0; k < 2; ++k)
-          r1[ab + 4 * k] = col_dot<1, M_S>(args.S, k, &r[ab], 4);
-#pragma unroll
-      for (int qa = 0; qa < 2; ++qa)
-#pragma unroll
-        for (int k = 0; k < 2; ++k)
-#pragma unroll
-          for (int j = 0; j < 2; ++j)
-            r2[qa + 2 * j + 4 * k] = col_dot<1, M_S>(args.S, j, &r1[qa + 4 * k], 2);
-#pragma unroll
-      for (int jk = 0; jk < 4; ++jk)
-#pragma unroll
-        for (int i = 0; i < 2; ++i)
-          res[i + 2 * jk] = col_dot<1, M_S>(args.S, i, &r2[2 * jk], 1);
-
-      // convective / radiative faces (face_local_apply,
-      // source/ThermalOperator.templates.hh:619-751), per node level
-      if (FC && ((info >> CI_FACE_SHIFT) & 63u))
-      {
-#pragma unroll
-        for (int lev = 0; lev < 2; ++lev)
-        {
-          double fo[4];
-          face_terms<1, NS>(sp, gm, md, args, brick, lx, ly, lz, lev, info, mat, c, fo);
-#pragma unroll
-          for (int e = 0; e < 4; ++e)
-            res[e + 4 * lev] += fo[e];
-        }
-      }
-      // state write-back: the liquid sum and, when a point of a uniform
-      // powder cell changed, the switch to per-point storage
-      if (NS > 1)
-        md.liquid_sum[c] = liq;
-      if (NS == 3 && pmode != 2 && cmask)
-      {
-        md.powder_mode[c] = 2;
-#pragma unroll
-        for (int e = 0; e < 8; ++e)
-          if (!((cmask >> e) & 1u))
-            md.powder_q[c * 8 + e] = pu;
+        res[e + 4 * j] += cres[e];
+        res[e + 4 * (j + 1)] += cres[e + 4];
       }
     }
 
-    // ---- per-node sums: a warp is one 8 x 4 layer of cells (lane =
+    // ---- per-node sums: a warp is one 8 x 4 layer of cell columns (lane =
     // lx + 8 ly); nodes shared in x and y go to the lower cell by shuffles,
-    // the level-0 nodes of layer lz > 0 to the layer below through shared
-    // memory
+    // the lowest node level of thread layer pz > 0 to the layer below
+    // through shared memory
     unsigned const full = 0xffffffffu;
 #pragma unroll
-    for (int jk = 0; jk < 4; ++jk)
+    for (int jk = 0; jk < 2 * (CZ + 1); ++jk)
     {
       double const v = __shfl_down_sync(full, res[2 * jk], 1);
       if (lx < TX - 1)
@@ -487,17 +553,17 @@ __global__ void __launch_bounds__(Q1Cell::NT, Q1Cell::MINB)
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
-      for (int k = 0; k < 2; ++k)
+      for (int k = 0; k <= CZ; ++k)
       {
         double const v = __shfl_down_sync(full, res[i + 4 * k], TX);
         if (ly < TY - 1)
           res[i + 2 + 4 * k] += v;
       }
-    if (lz > 0)
+    if (pz > 0)
     {
 #pragma unroll
       for (int e = 0; e < 4; ++e)
-        mbuf[e * NCELL + tid] = res[e];
+        mbuf[e * NT + tid] = res[e];
     }
     if (__syncthreads_or(!arrived))
     {
@@ -518,24 +584,24 @@ __global__ void __launch_bounds__(Q1Cell::NT, Q1Cell::MINB)
       fence_proxy_async();
       issue(buf == 0 ? NBUF - 1 : buf - 1, next2);
     }
-    if (lz < TZ - 1)
+    if (pz < NPZ - 1)
     {
 #pragma unroll
       for (int e = 0; e < 4; ++e)
-        res[e + 4] += mbuf[e * NCELL + tid + TX * TY];
+        res[e + 4 * CZ] += mbuf[e * NT + tid + TX * TY];
     }
 
     // ---- write-out of the nodes this thread owns (the lower cell of a
     // shared node owns it)
-    int rl[8];
-    size_t gidx[8];
+    int rl[NV];
+    size_t gidx[NV];
 #pragma unroll
-    for (int e = 0; e < 8; ++e)
+    for (int e = 0; e < NV; ++e)
     {
       int const a = e & 1, b = (e >> 1) & 1, k = e >> 2;
-      int const X = lx + a, Y = ly + b, Z = lz + k;
+      int const X = lx + a, Y = ly + b, Z = CZ * pz + k;
       int const gx = ncx0 + X, gy = ncy0 + Y, gzn = ncz0 + Z;
-      bool const own = (a > 0 || lx == 0) && (b > 0 || ly == 0) && (k > 0 || lz == 0);
+      bool const own = (a > 0 || lx == 0) && (b > 0 || ly == 0) && (k > 0 || pz == 0);
       bool const inside = gx < args.nn[0] && gy < nn1 && gzn < args.nn[2];
       int const sx = (X == 0 && tix > 0) ? 1 : ((X == TX && tix < nt0 - 1) ? 2 : 0);
       int const sy = (Y == 0 && tiy > 0) ? 1 : ((Y == TY && tiy < nt1 - 1) ? 2 : 0);
@@ -543,7 +609,7 @@ __global__ void __launch_bounds__(Q1Cell::NT, Q1Cell::MINB)
       rl[e] = (own && inside) ? (AT ? 4 : (sp.role[it & 1][sx + 3 * sy + 9 * sz] | 4)) : 0;
       gidx[e] = gx + (size_t)pitch * (gy + (size_t)nn1 * gzn);
     }
-    write_nodes<AT, 8>(args, md, y, res, rl, gidx);
+    write_nodes<AT, NV>(args, md, y, res, rl, gidx);
     // vmult writes zeros into the row padding of the node layout
     if (!AT && args.mode == 0 && tix == nt0 - 1 && pitch > args.nn[0])
     {
@@ -568,32 +634,42 @@ __global__ void __launch_bounds__(Q1Cell::NT, Q1Cell::MINB)
 
 // Launches the persistent Q1 cell kernel over n_items work items with at
 // most the number of CTAs that are resident at once on the device.
-template <int NS, int P, bool AT, bool FC>
+template <int NS, int P, bool AT, bool FC, int CZ>
 void launch_cell_q1_f(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
 {
+  using Q = Q1Cell<CZ>;
   static int grid_cap = 0;
   if (grid_cap == 0)
   {
-    cudaFuncSetAttribute(cell_kernel_q1<NS, P, AT, FC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)Q1Cell::SMEM);
+    cudaFuncSetAttribute(cell_kernel_q1<NS, P, AT, FC, CZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)Q::SMEM);
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cell_kernel_q1<NS, P, AT, FC>, Q1Cell::NT,
-                                                  Q1Cell::SMEM);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cell_kernel_q1<NS, P, AT, FC, CZ>, Q::NT, Q::SMEM);
     grid_cap = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
   }
   int const grid = n_items < grid_cap ? n_items : grid_cap;
-  cell_kernel_q1<NS, P, AT, FC><<<grid, Q1Cell::NT, Q1Cell::SMEM, stream>>>(map, a, n_items);
+  cell_kernel_q1<NS, P, AT, FC, CZ><<<grid, Q::NT, Q::SMEM, stream>>>(map, a, n_items);
 }
 
+template <int NS, int P, bool AT, int CZ>
+void launch_cell_q1_z(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
+{
+  if (a.faces)
+    launch_cell_q1_f<NS, P, AT, true, CZ>(map, a, n_items, stream);
+  else
+    launch_cell_q1_f<NS, P, AT, false, CZ>(map, a, n_items, stream);
+}
+
+// a.cells_per_thread 2: two cells per thread (z), else one
 template <int NS, int P, bool AT>
 void launch_cell_q1(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
 {
-  if (a.faces)
-    launch_cell_q1_f<NS, P, AT, true>(map, a, n_items, stream);
+  if (a.cells_per_thread == 2)
+    launch_cell_q1_z<NS, P, AT, 2>(map, a, n_items, stream);
   else
-    launch_cell_q1_f<NS, P, AT, false>(map, a, n_items, stream);
+    launch_cell_q1_z<NS, P, AT, 1>(map, a, n_items, stream);
 }
 
 } // namespace adm

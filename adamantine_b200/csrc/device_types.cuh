@@ -155,6 +155,7 @@ struct KernelArgs
   int blocked;  // 1: each CTA takes one contiguous run of work items
   int *claim;   // non-null: items after each CTA's first are claimed from this
                 // counter (zero at the launch), dynamic load balance
+  int cells_per_thread; // FE_Q(1) cell kernel: 1 or 2 cells (stacked in z) per thread
   int stage;
   int last;     // last stage of the step (updates y)
   int n_stages; // 1 forward Euler

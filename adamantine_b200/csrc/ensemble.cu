@@ -133,10 +133,9 @@ void Ensemble::setup()
   // the atomic schedule's list: member-major, each member's tiles in order
   awork_.clear();
   for (int i = 0; i < n_members(); ++i)
-    for (TileWork const &tw : members_[i]->work_)
+    for (TileWork const &tw : members_[i]->awork_)
       awork_.push_back(TileWork{i, tw.tile, tw.xyz});
   awork_d_.alloc(std::max<size_t>(1, awork_.size()));
-  claim_d_.alloc(8);
   if (!awork_.empty())
     ADM_CK(cudaMemcpyAsync(awork_d_.p, awork_.data(), awork_.size() * sizeof(TileWork),
                            cudaMemcpyHostToDevice, stream_));
@@ -186,8 +185,6 @@ void Ensemble::launch_step(double *solutions)
     a.y_override = nullptr;
     double const *src = i == 0 ? solutions : (a.src_sel == 1 ? za_.p : zb_.p);
     CUtensorMap const map = brick_map(members_[0]->mesh_, src, n, stride_);
-    // the launches claim their work items from zeroed counters
-    ADM_CK(cudaMemsetAsync(claim_d_.p, 0, 8 * sizeof(int32_t), stream_));
     if (schedule_ == Thermal::kScheduleAtomic)
     {
       // member-major list, one contiguous run per CTA: a CTA changes member
@@ -198,7 +195,6 @@ void Ensemble::launch_step(double *solutions)
       if (!awork_.empty())
       {
         a.work = awork_d_.p;
-        a.claim = claim_d_.p;
         launch_tile(deg_, ns_, poly_p_, map, a, (int)awork_.size(), stream_);
         ADM_CK(cudaGetLastError());
       }
@@ -212,7 +208,6 @@ void Ensemble::launch_step(double *solutions)
       if (count == 0)
         continue;
       a.work = work_d_.p + colour_off_[col];
-      a.claim = claim_d_.p + col;
       launch_tile(deg_, ns_, poly_p_, map, a, count, stream_);
       ADM_CK(cudaGetLastError());
     }
@@ -317,6 +312,16 @@ void Ensemble::update_beam(int i, int beam, adm_source const &src)
   drop_graph();
 }
 
+void Ensemble::set_cells_per_thread(int n)
+{
+  // the members validate n; the looped baseline runs the same kernel variant
+  for (auto &m : members_)
+    m->set_cells_per_thread(n);
+  if (n != cells_per_thread_)
+    drop_graph();
+  cells_per_thread_ = n;
+}
+
 void Ensemble::set_schedule(int schedule)
 {
   if (schedule != Thermal::kScheduleColoured && schedule != Thermal::kScheduleAtomic)
@@ -345,12 +350,15 @@ int Ensemble::autotune(double const *solutions, double dt, double *ms_out)
   cudaEvent_t e0, e1;
   ADM_CK(cudaEventCreate(&e0));
   ADM_CK(cudaEventCreate(&e1));
-  int const saved = schedule_;
+  int const saved = schedule_, saved_cz = cells_per_thread_;
   double best = 0.0;
-  int choice = saved;
+  int choice = saved, choice_cz = saved_cz;
+  int const deg = members_.empty() ? 2 : members_[0]->mesh_.deg;
   for (int sch : {Thermal::kScheduleColoured, Thermal::kScheduleAtomic})
+    for (int cz = 1; cz <= (deg == 1 ? 2 : 1); ++cz)
   {
     schedule_ = sch;
+    set_cells_per_thread(cz);
     ADM_CK(cudaMemcpyAsync(scratch.p, solutions, total * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
     evolve_one_time_step(0.0, dt, scratch.p);
     int const reps = 3;
@@ -362,12 +370,13 @@ int Ensemble::autotune(double const *solutions, double dt, double *ms_out)
     float ms = 0.f;
     ADM_CK(cudaEventElapsedTime(&ms, e0, e1));
     double const per = ms / reps;
-    if (ms_out)
+    if (ms_out && (cz == 1 || per < ms_out[sch]))
       ms_out[sch] = per;
     if (best == 0.0 || per < best)
     {
       best = per;
       choice = sch;
+      choice_cz = cz;
     }
     for (size_t k = 0; k < members_.size(); ++k)
       members_[k]->restore_phase(snaps[k]);
@@ -377,6 +386,7 @@ int Ensemble::autotune(double const *solutions, double dt, double *ms_out)
   ADM_CK(cudaStreamSynchronize(stream_));
   schedule_ = saved;
   set_schedule(choice);
+  set_cells_per_thread(choice_cz);
   return choice;
 }
 
@@ -539,6 +549,22 @@ int adm_ensemble_set_schedule(adm_ensemble *e, int32_t schedule)
   return adm::guard([&] {
     ADM_REQUIRE(e, "null handle");
     as_ens(e)->set_schedule(schedule);
+  });
+}
+
+int adm_ensemble_set_cells_per_thread(adm_ensemble *e, int32_t n)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(e, "null handle");
+    as_ens(e)->set_cells_per_thread(n);
+  });
+}
+
+int adm_ensemble_get_cells_per_thread(adm_ensemble const *e, int32_t *n)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(e && n, "null argument");
+    *n = reinterpret_cast<adm::Ensemble const *>(e)->cells_per_thread();
   });
 }
 

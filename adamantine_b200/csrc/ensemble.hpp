@@ -52,6 +52,9 @@ public:
   // autotuner (one timed batched step per schedule on a copy of solutions)
   void set_schedule(int schedule);
   int schedule() const { return schedule_; }
+  // FE_Q(1) operator kernel: 1 or 2 cells per thread (members follow)
+  void set_cells_per_thread(int n);
+  int cells_per_thread() const { return cells_per_thread_; }
   int autotune(double const *solutions, double dt, double *ms_out);
   int32_t device_error();
   size_t n_work_items() const { return work_.size(); }
@@ -71,13 +74,13 @@ private:
   int deg_ = 1, ns_ = 1, poly_p_ = 2;
   bool any_source_ = false;
   int schedule_ = Thermal::kScheduleColoured;
+  int cells_per_thread_ = 1;
   bool setup_done_ = false;
   Thermal::Tableau tab_;
 
   DevBuf<double> za_, zb_, s_, f0_, acc_;
   DevBuf<MemberData> md_d_;
   DevBuf<TileWork> work_d_, awork_d_;
-  DevBuf<int32_t> claim_d_; // per-colour work counters of the tile launches
   std::vector<TileWork> work_, awork_;
   int colour_off_[9] = {0};
   double *bound_ = nullptr; // solutions array the member table points at

@@ -58,6 +58,17 @@ void check_q2_structure(Rule1D const &r)
     throw Error(ADM_ERR_UNSUPPORTED, "FE_Q(2) Gauss rule lacks the exact middle-point entries the kernels assume");
 }
 
+// The FE_Q(1) cell kernel takes the collocation derivative of the two
+// points as one row repeated, D[q] = (-d, d), and equal weights; this checks
+// that the computed rule has them exactly.
+void check_q1_structure(Rule1D const &r)
+{
+  bool const ok = r.D[0][0] == r.D[1][0] && r.D[0][1] == r.D[1][1] && r.D[0][0] == -r.D[0][1] &&
+                  r.w[0] == r.w[1];
+  if (!ok)
+    throw Error(ADM_ERR_UNSUPPORTED, "FE_Q(1) rule lacks the exact structure the kernels assume");
+}
+
 Rule1D make_rule(int deg, bool lobatto)
 {
   Rule1D r;
@@ -123,6 +134,8 @@ Rule1D make_rule(int deg, bool lobatto)
   }
   if (deg == 2 && !lobatto)
     check_q2_structure(r);
+  if (deg == 1)
+    check_q1_structure(r);
   return r;
 }
 } // namespace
@@ -579,7 +592,10 @@ void Thermal::rebuild()
   for (int col = 0; col < 8; ++col)
   {
     colour_off_[col] = (int)work_.size();
-    for (int tz = (col >> 2) & 1; tz < mesh_.nt[2]; tz += 2)
+    // top layers first: the beam works the top surface, so the slow tiles
+    // (melt pool, source) are claimed early and the others balance them
+    int const tz_top = mesh_.nt[2] - 1 - (((mesh_.nt[2] - 1) ^ (col >> 2)) & 1);
+    for (int tz = tz_top; tz >= 0; tz -= 2)
       for (int ty = (col >> 1) & 1; ty < mesh_.nt[1]; ty += 2)
         for (int tx = col & 1; tx < mesh_.nt[0]; tx += 2)
         {
@@ -589,6 +605,7 @@ void Thermal::rebuild()
         }
   }
   colour_off_[8] = (int)work_.size();
+  build_atomic_list(topo_.tile_active);
   ++work_version_;
   work_d_.alloc(std::max<size_t>(1, work_.size()));
   if (!work_.empty())
@@ -695,6 +712,7 @@ KernelArgs Thermal::base_args() const
     a.origin[d] = mesh_.origin[d];
   }
   a.pitch = mesh_.pitch;
+  a.cells_per_thread = cells_per_thread_;
   a.faces = adiabatic_only_ ? 0 : 1;
   int const nb = cfg_.n_boundary_types;
   for (int f = 0; f < 6; ++f)
@@ -844,19 +862,18 @@ CUtensorMap brick_map(Mesh const &m, double const *base, int n_members, size_t m
 void Thermal::launch_pass(KernelArgs a, double const *src)
 {
   CUtensorMap const map = brick_map(mesh_, src, 1, mesh_.n_nodes);
-  // the launches claim their work items from zeroed counters
-  ADM_CK(cudaMemsetAsync(claim_d_.p, 0, 8 * sizeof(int32_t), stream_));
   if (schedule_ == kScheduleAtomic)
   {
+    // one launch over every tile (the ascending list), items strided over
+    // the CTAs (measured faster here than claiming them from a counter)
     int const count = colour_off_[8];
     size_t const N = mesh_.n_nodes;
     a.atomic = 1;
-    a.claim = claim_d_.p;
     if (a.mode == 2)
       ADM_CK(cudaMemsetAsync(acc_p_, 0, N * sizeof(double), stream_));
     if (count > 0)
     {
-      a.work = work_d_.p;
+      a.work = awork_d_.p;
       launch_tile(mesh_.deg, ns_, poly_p_, map, a, count, stream_);
       ADM_CK(cudaGetLastError());
     }
@@ -867,6 +884,10 @@ void Thermal::launch_pass(KernelArgs a, double const *src)
     }
     return;
   }
+  // colour launches claim their items from zeroed counters: a colour ends
+  // with its slowest CTA, and a CTA held up by a tile under the beam takes
+  // fewer of the others
+  ADM_CK(cudaMemsetAsync(claim_d_.p, 0, 8 * sizeof(int32_t), stream_));
   for (int col = 0; col < 8; ++col)
   {
     int const count = colour_off_[col + 1] - colour_off_[col];
@@ -1391,7 +1412,10 @@ int64_t Thermal::activate_in_boxes(DeviceBoxes const &boxes, int64_t b0, int64_t
   for (int col = 0; col < 8; ++col)
   {
     colour_off_[col] = (int)work_.size();
-    for (int tz = (col >> 2) & 1; tz < mesh_.nt[2]; tz += 2)
+    // top layers first: the beam works the top surface, so the slow tiles
+    // (melt pool, source) are claimed early and the others balance them
+    int const tz_top = mesh_.nt[2] - 1 - (((mesh_.nt[2] - 1) ^ (col >> 2)) & 1);
+    for (int tz = tz_top; tz >= 0; tz -= 2)
       for (int ty = (col >> 1) & 1; ty < mesh_.nt[1]; ty += 2)
         for (int tx = col & 1; tx < mesh_.nt[0]; tx += 2)
         {
@@ -1401,6 +1425,7 @@ int64_t Thermal::activate_in_boxes(DeviceBoxes const &boxes, int64_t b0, int64_t
         }
   }
   colour_off_[8] = (int)work_.size();
+  build_atomic_list(ta);
   ++work_version_;
   work_d_.alloc(std::max<size_t>(1, work_.size()));
   ADM_CK(cudaMemcpyAsync(work_d_.p, work_.data(), work_.size() * sizeof(TileWork), cudaMemcpyHostToDevice, stream_));
@@ -1468,6 +1493,41 @@ int32_t Thermal::device_error()
 }
 
 void Thermal::synchronize() { ADM_CK(cudaStreamSynchronize(stream_)); }
+
+// The atomic schedule's list: every active tile, colour by colour, bottom
+// layers first (measured faster for the one strided launch than the top-down
+// order of the colour lists, which suits the claimed colour launches).
+void Thermal::build_atomic_list(std::vector<uint8_t> const &tile_active)
+{
+  awork_.clear();
+  for (int col = 0; col < 8; ++col)
+    for (int tz = (col >> 2) & 1; tz < mesh_.nt[2]; tz += 2)
+      for (int ty = (col >> 1) & 1; ty < mesh_.nt[1]; ty += 2)
+        for (int tx = col & 1; tx < mesh_.nt[0]; tx += 2)
+        {
+          size_t const tile = tx + (size_t)mesh_.nt[0] * (ty + (size_t)mesh_.nt[1] * tz);
+          if (tile_active[tile])
+            awork_.push_back(TileWork{0, (int32_t)tile, pack_tile(tx, ty, tz)});
+        }
+  awork_d_.alloc(std::max<size_t>(1, awork_.size()));
+  if (!awork_.empty())
+    ADM_CK(cudaMemcpyAsync(awork_d_.p, awork_.data(), awork_.size() * sizeof(TileWork), cudaMemcpyHostToDevice,
+                           stream_));
+}
+
+void Thermal::set_cells_per_thread(int n)
+{
+  if (n != 1 && n != 2)
+    throw Error(ADM_ERR_INVALID, "cells per thread must be 1 or 2");
+  if (n == 2 && mesh_.deg != 1)
+    throw Error(ADM_ERR_UNSUPPORTED, "two cells per thread is a variant of the FE_Q(1) kernel");
+  if (n != cells_per_thread_ && step_graph_)
+  {
+    cudaGraphExecDestroy(step_graph_);
+    step_graph_ = nullptr;
+  }
+  cells_per_thread_ = n;
+}
 
 void Thermal::set_schedule(int schedule)
 {
@@ -1541,37 +1601,44 @@ int Thermal::autotune(double const *field, double *ms_out)
   cudaEvent_t e0, e1;
   ADM_CK(cudaEventCreate(&e0));
   ADM_CK(cudaEventCreate(&e1));
-  int const saved = schedule_;
+  int const saved = schedule_, saved_cz = cells_per_thread_;
   double best = 0.0;
-  int choice = saved;
+  int choice = saved, choice_cz = saved_cz;
+  // launch schedules x (FE_Q(1)) cells per thread; ms_out[schedule] is the
+  // schedule's best time
   for (int sch : {kScheduleColoured, kScheduleAtomic})
-  {
-    schedule_ = sch;
-    for (int r = 0; r < 2; ++r)
-      vmult(dst.p, field, false);
-    ADM_CK(cudaEventRecord(e0, stream_));
-    int const reps = 5;
-    for (int r = 0; r < reps; ++r)
-      vmult(dst.p, field, false);
-    ADM_CK(cudaEventRecord(e1, stream_));
-    ADM_CK(cudaEventSynchronize(e1));
-    float ms = 0.f;
-    ADM_CK(cudaEventElapsedTime(&ms, e0, e1));
-    double const per = ms / reps;
-    if (ms_out)
-      ms_out[sch] = per;
-    if (best == 0.0 || per < best)
+    for (int cz = 1; cz <= (mesh_.deg == 1 ? 2 : 1); ++cz)
     {
-      best = per;
-      choice = sch;
+      schedule_ = sch;
+      cells_per_thread_ = cz;
+      for (int r = 0; r < 2; ++r)
+        vmult(dst.p, field, false);
+      ADM_CK(cudaEventRecord(e0, stream_));
+      int const reps = 5;
+      for (int r = 0; r < reps; ++r)
+        vmult(dst.p, field, false);
+      ADM_CK(cudaEventRecord(e1, stream_));
+      ADM_CK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      ADM_CK(cudaEventElapsedTime(&ms, e0, e1));
+      double const per = ms / reps;
+      if (ms_out && (cz == 1 || per < ms_out[sch]))
+        ms_out[sch] = per;
+      if (best == 0.0 || per < best)
+      {
+        best = per;
+        choice = sch;
+        choice_cz = cz;
+      }
     }
-  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   schedule_ = saved;
+  cells_per_thread_ = saved_cz;
   restore_phase(snap);
   ADM_CK(cudaStreamSynchronize(stream_));
   set_schedule(choice);
+  set_cells_per_thread(choice_cz);
   return choice;
 }
 

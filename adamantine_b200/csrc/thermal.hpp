@@ -259,6 +259,10 @@ public:
   static constexpr int kScheduleColoured = 0, kScheduleAtomic = 1;
   void set_schedule(int schedule);
   int schedule() const { return schedule_; }
+  // FE_Q(1) operator kernel: 1 or 2 cells (stacked in z) per thread
+  void set_cells_per_thread(int n);
+  void build_atomic_list(std::vector<uint8_t> const &tile_active);
+  int cells_per_thread() const { return cells_per_thread_; }
   // times both schedules on vmults of `field` (phase history restored) and
   // keeps the faster; ms_out[2] (may be null) receives the per-vmult times
   int autotune(double const *field, double *ms_out);
@@ -310,6 +314,7 @@ private:
   bool setup_done_ = false;
   double op_time_ = 0.0;
   int schedule_ = kScheduleColoured;
+  int cells_per_thread_ = 1;
   Tableau tab_;
 
   std::vector<uint8_t> active_, matid_, init_state_, has_melted_;
@@ -339,6 +344,8 @@ private:
   DevBuf<BeamState> beam_state_d_;
   DevBuf<MemberData> member_d_;
   DevBuf<TileWork> work_d_;
+  std::vector<TileWork> awork_;  // atomic schedule: every active tile, bottom layers first
+  DevBuf<TileWork> awork_d_;
   MemberData md_{};
 
   // z-slab pipeline of vmult_host: tiles sorted by z layer, copy streams

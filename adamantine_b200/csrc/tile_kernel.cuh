@@ -877,13 +877,14 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
                    wi.member, &bars[buf]);
   };
 
-  // work distribution: with args.claim, dynamic -- CTA b starts with item
-  // b and claims each further item from the launch's counter, one item ahead
-  // (a CTA held up by a slow tile, near the melt pool, takes fewer); else
+  // work distribution: with args.claim (and a list that is not blocked),
+  // dynamic -- CTA b starts with item b and claims each further item from
+  // the launch's counter, one item ahead (a CTA held up by a slow tile, near
+  // the melt pool, takes fewer; the lists put the top tile layers first); else
   // strided (CTA b takes items b, b + grid, ...) or, with args.blocked, one
   // contiguous run of items per CTA (consecutive items of a member-major
   // list then share the member's constants)
-  bool const dyn = args.claim != nullptr;
+  bool const dyn = args.claim != nullptr && !args.blocked;
   __shared__ int claimed[2]; // dynamic: the item after the current one, by item parity
   int first, last, step;
   if (dyn || !args.blocked)

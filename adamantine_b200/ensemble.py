@@ -196,9 +196,20 @@ class Ensemble:
         """Launch schedule of the batched stages (0 coloured, 1 atomic)."""
         _lib.check(self._L.adm_ensemble_set_schedule(self._h, int(schedule)))
 
+    def set_cells_per_thread(self, n: int):
+        """FE_Q(1) kernel variant (1 or 2 cells per thread) of the batched
+        stages and the members' own launches."""
+        _lib.check(self._L.adm_ensemble_set_cells_per_thread(self._h, int(n)))
+
+    def cells_per_thread(self) -> int:
+        v = ctypes.c_int32()
+        _lib.check(self._L.adm_ensemble_get_cells_per_thread(self._h, ctypes.byref(v)))
+        return int(v.value)
+
     def autotune(self, solutions: torch.Tensor, dt: float):
-        """Times one batched step per schedule on a copy of solutions, keeps
-        the faster; returns (schedule, [ms coloured, ms atomic])."""
+        """Times one batched step per schedule (and, for FE degree 1, per
+        cells-per-thread variant) on a copy of solutions, keeps the fastest;
+        returns (schedule, [best ms coloured, best ms atomic])."""
         c = ctypes.c_int32()
         ms = np.zeros(2)
         _lib.check(self._L.adm_ensemble_autotune(self._h, self._check(solutions), float(dt), ctypes.byref(c),

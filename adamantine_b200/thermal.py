@@ -244,9 +244,20 @@ class ThermalPhysics:
         _lib.check(self._L.adm_get_schedule(self._h, ctypes.byref(v)))
         return int(v.value)
 
+    def set_cells_per_thread(self, n: int):
+        """FE_Q(1) operator kernel variant: 1 or 2 cells (stacked in z) per
+        thread."""
+        _lib.check(self._L.adm_set_cells_per_thread(self._h, int(n)))
+
+    def cells_per_thread(self) -> int:
+        v = ctypes.c_int32()
+        _lib.check(self._L.adm_get_cells_per_thread(self._h, ctypes.byref(v)))
+        return int(v.value)
+
     def autotune(self, field: torch.Tensor):
-        """Times both schedules on vmults of field, keeps the faster; returns
-        (schedule, [ms coloured, ms atomic])."""
+        """Times both schedules (and, for FE degree 1, both cells-per-thread
+        variants) on vmults of field, keeps the fastest; returns (schedule,
+        [best ms coloured, best ms atomic])."""
         c = ctypes.c_int32()
         ms = np.zeros(2)
         _lib.check(self._L.adm_autotune(self._h, _dev(field), ctypes.byref(c), _ptr(ms, ctypes.c_double)))

@@ -210,9 +210,18 @@ int adm_update_beam(adm_thermal *h, int32_t i, adm_source const *beam);
 #define ADM_SCHEDULE_ATOMIC 1
 int adm_set_schedule(adm_thermal *h, int32_t schedule);
 int adm_get_schedule(adm_thermal const *h, int32_t *schedule);
-/* Autotuner: times both schedules on vmults of the device field (the phase
- * history is restored afterwards), keeps the faster in the handle and
- * returns it in *schedule; ms[2] (may be NULL) receives the per-vmult times. */
+/* Cells per thread of the FE_Q(1) operator kernel (no counterpart in the
+ * reference): 1 (default) or 2 cells stacked in z per thread, the second
+ * sharing the per-tile bookkeeping and one node level in registers. FE
+ * degree 2 takes 1 only. Results agree to rounding; each variant is
+ * bit-reproducible in the coloured schedule. */
+int adm_set_cells_per_thread(adm_thermal *h, int32_t n);
+int adm_get_cells_per_thread(adm_thermal const *h, int32_t *n);
+/* Autotuner: times both schedules (and, for FE degree 1, both cells-per-
+ * thread variants) on vmults of the device field (the phase history is
+ * restored afterwards), keeps the fastest in the handle and returns its
+ * schedule in *schedule; ms[2] (may be NULL) receives each schedule's best
+ * per-vmult time. */
 int adm_autotune(adm_thermal *h, double const *field, int32_t *schedule, double *ms);
 
 /* ThermalPhysicsInterface::save_checkpoint

@@ -68,9 +68,14 @@ int adm_ensemble_get_cell_state(adm_ensemble *e, int32_t member, double *state_h
 int adm_ensemble_get_inverse_mass_matrix(adm_ensemble *e, int32_t member, double *dst);
 /* Launch schedule of the batched stages (ADM_SCHEDULE_* of adamantine_b200.h). */
 int adm_ensemble_set_schedule(adm_ensemble *e, int32_t schedule);
-/* Autotuner: times one batched step of size dt with each schedule on a copy
- * of solutions (phase history and clocks restored), keeps the faster and
- * returns it; ms[2] (may be NULL) receives the per-step times. */
+/* Cells per thread of the FE_Q(1) kernel for the batched stages and the
+ * members' own (looped) launches (adm_set_cells_per_thread). */
+int adm_ensemble_set_cells_per_thread(adm_ensemble *e, int32_t n);
+int adm_ensemble_get_cells_per_thread(adm_ensemble const *e, int32_t *n);
+/* Autotuner: times one batched step of size dt with each schedule (and, for
+ * FE degree 1, each cells-per-thread variant) on a copy of solutions (phase
+ * history and clocks restored), keeps the fastest and returns its schedule;
+ * ms[2] (may be NULL) receives each schedule's best per-step time. */
 int adm_ensemble_autotune(adm_ensemble *e, double const *solutions, double dt, int32_t *schedule, double *ms);
 /* First non-zero sticky device error word over the members (synchronizes). */
 int adm_ensemble_device_error(adm_ensemble *e, int32_t *code);

@@ -45,11 +45,15 @@ def test_ragged_members_have_distinct_work():
     assert e.stride % 2 == 0
 
 
-@pytest.mark.parametrize("method", ["rk_fourth_order", "rk_third_order", "forward_euler"])
-def test_batched_equals_looped_and_oracle(method):
+@pytest.mark.parametrize("method,cells_per_thread", [("rk_fourth_order", 1), ("rk_third_order", 1),
+                                                     ("forward_euler", 1), ("rk_fourth_order", 2)])
+def test_batched_equals_looped_and_oracle(method, cells_per_thread):
     configs, params, grids = small_ensemble(method=method)
     e1 = Ensemble(configs)
     e2 = Ensemble(configs)
+    e1.set_cells_per_thread(cells_per_thread)
+    e2.set_cells_per_thread(cells_per_thread)
+    assert e1.cells_per_thread() == cells_per_thread
     y1 = e1.from_grids(grids)
     y2 = y1.clone()
     dt = 1e-6

@@ -135,3 +135,50 @@ def test_activation_parity():
         t = g.evolve_one_time_step(t, dt, y)
     assert rel_max(grid(g.to_grid(y)), y_ref) <= STEP_TOL
     assert g.device_error() == 0
+
+
+Q1_CASES = [c for c in CASES if c.startswith("q1_")]
+
+
+@pytest.mark.parametrize("schedule", [0, 1])
+@pytest.mark.parametrize("name", Q1_CASES)
+def test_q1_two_cells_per_thread(name, schedule):
+    """The FE_Q(1) kernel variant with two cells (stacked in z) per thread:
+    the same bars against the oracle in both launch schedules (vmult with
+    its phase history over three applications, 12 time steps)."""
+    cfg, cells, T = make_case(name)
+    o = make_oracle(cfg, cells)
+    g = make_gpu(cfg, cells)
+    g.set_cells_per_thread(2)
+    g.set_schedule(schedule)
+    assert g.cells_per_thread() == 2
+    o.set_time(2e-4)
+    g.set_time(2e-4)
+    dst = g.initialize_dof_vector()
+    for k in range(3):
+        Tk = T * (1.0 + 0.05 * k)
+        g.vmult(dst, g.from_grid(Tk))
+        assert rel_max(grid(g.to_grid(dst)), o.vmult(grid(Tk))) <= VMULT_TOL, k
+    if cfg.material.n_states == 3:
+        assert np.max(np.abs(g.get_qp_powder() - o.qp_powder())) < 1e-12
+    o2 = make_oracle(cfg, cells)
+    g2 = make_gpu(cfg, cells)
+    g2.set_cells_per_thread(2)
+    g2.set_schedule(schedule)
+    y_ref = grid(T).copy()
+    y = g2.from_grid(T)
+    t_ref = t = 1e-5
+    for _ in range(12):
+        t_ref = o2.evolve_one_time_step(t_ref, 5e-6, y_ref)
+        t = g2.evolve_one_time_step(t, 5e-6, y)
+    assert rel_max(grid(g2.to_grid(y)), y_ref) <= STEP_TOL
+    assert g.device_error() == 0 and g2.device_error() == 0
+
+
+def test_two_cells_per_thread_is_a_q1_variant():
+    cfg, cells, T = make_case("q2_slp_goldak")
+    g = make_gpu(cfg, cells)
+    with pytest.raises(Exception):
+        g.set_cells_per_thread(2)
+    with pytest.raises(Exception):
+        g.set_cells_per_thread(3)
