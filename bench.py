@@ -35,10 +35,10 @@ METRIC = "heat vmult GDoF/s (FP64 Q2) & %HBM peak; batched-ensemble vs looped st
 WORKLOAD = "phase_change_q2_128x128x64_vmult"
 
 
-# FP64 work of one Q2 cell of this workload: 1257 DFMA + 379 DMUL + 41 DADD
-# thread instructions per cell (ncu sm__sass_thread_inst_executed_op_d*
-# counts of tile_kernel<2,3,2> on the 128x128x32 case) = 2934 FLOP.
-FP64_FLOP_PER_Q2_CELL = 2934
+# FP64 work of one Q2 cell of this workload: 876 DFMA + 432 DMUL + 63 DADD
+# thread instructions per cell (ncu smsp__sass_thread_inst_executed_op_d*
+# counts of tile_kernel<2,3,2,1,0> on the 128x128x32 case) = 2247 FLOP.
+FP64_FLOP_PER_Q2_CELL = 2247
 
 # DRAM bytes (read + write) of one vmult of the 128x128x64 workload from ncu
 # captures (dram__bytes_read.sum + dram__bytes_write.sum): the atomic
