@@ -52,6 +52,7 @@ SIGNATURES = {
     "adm_set_schedule": [_VP, ctypes.c_int32],
     "adm_get_schedule": [_VP, _I32],
     "adm_autotune": [_VP, _VP, _I32, _D],
+    "adm_autotune_schedules": [_VP, _VP, _I32, _D, ctypes.c_int32],
     "adm_set_cells_per_thread": [_VP, ctypes.c_int32],
     "adm_get_cells_per_thread": [_VP, _I32],
     "adm_save_checkpoint": [_VP, ctypes.c_char_p, ctypes.c_double, _VP],
@@ -74,6 +75,7 @@ SIGNATURES = {
     "adm_ensemble_get_inverse_mass_matrix": [_VP, ctypes.c_int32, _VP],
     "adm_ensemble_set_schedule": [_VP, ctypes.c_int32],
     "adm_ensemble_autotune": [_VP, _VP, ctypes.c_double, _I32, _D],
+    "adm_ensemble_autotune_schedules": [_VP, _VP, ctypes.c_double, _I32, _D, ctypes.c_int32],
     "adm_ensemble_set_cells_per_thread": [_VP, ctypes.c_int32],
     "adm_ensemble_get_cells_per_thread": [_VP, _I32],
     "adm_ensemble_device_error": [_VP, _I32],

@@ -293,14 +293,23 @@ int adm_get_cells_per_thread(adm_thermal const *h, int32_t *n)
   });
 }
 
-int adm_autotune(adm_thermal *h, double const *field, int32_t *schedule, double *ms)
+int adm_autotune_schedules(adm_thermal *h, double const *field, int32_t *schedule, double *ms, int32_t n_ms)
 {
   return adm::guard([&] {
     ADM_REQUIRE(h && field, "null argument");
-    int const c = as(h)->autotune(field, ms);
+    ADM_REQUIRE(n_ms >= 0, "n_ms must not be negative");
+    double t[ADM_N_SCHEDULES] = {0.0, 0.0, 0.0};
+    int const c = as(h)->autotune(field, t);
     if (schedule)
       *schedule = c;
+    for (int k = 0; ms && k < n_ms && k < ADM_N_SCHEDULES; ++k)
+      ms[k] = t[k];
   });
+}
+
+int adm_autotune(adm_thermal *h, double const *field, int32_t *schedule, double *ms)
+{
+  return adm_autotune_schedules(h, field, schedule, ms, 2);
 }
 
 int adm_update_beam(adm_thermal *h, int32_t i, adm_source const *beam)

@@ -488,31 +488,7 @@ __global__ void __launch_bounds__(Q1Cell<CZ>::NT, Q1Cell<CZ>::MINB)
         sp.member = w.member;
     }
     if (!AT && tid < 27)
-    {
-      // first/last toucher role of a node whose per-direction sharing state
-      // is (tid % 3, tid / 3 % 3, tid / 9): 0 not shared, 1 shared with the
-      // lower neighbour tile, 2 with the upper one
-      uint32_t const nbr = md.tile_nbr[tile];
-      int const s0 = tid % 3, s1 = (tid / 3) % 3, s2 = tid / 9;
-      int cmin = 8, cmax = -1;
-#pragma unroll
-      for (int m = 0; m < 8; ++m)
-      {
-        int const b0 = m & 1, b1 = (m >> 1) & 1, b2 = (m >> 2) & 1;
-        if ((b0 && s0 == 0) || (b1 && s1 == 0) || (b2 && s2 == 0))
-          continue;
-        int const o0 = b0 ? (s0 == 1 ? -1 : 1) : 0;
-        int const o1 = b1 ? (s1 == 1 ? -1 : 1) : 0;
-        int const o2 = b2 ? (s2 == 1 ? -1 : 1) : 0;
-        int const bit = (o0 + 1) + 3 * (o1 + 1) + 9 * (o2 + 1);
-        if (!((nbr >> bit) & 1u))
-          continue;
-        int const cc = colour ^ (b0 | (b1 << 1) | (b2 << 2));
-        cmin = cc < cmin ? cc : cmin;
-        cmax = cc > cmax ? cc : cmax;
-      }
-      sp.role[it & 1][tid] = (colour == cmin ? 1 : 0) | (colour == cmax ? 2 : 0);
-    }
+      sp.role[it & 1][tid] = node_role(md.tile_nbr[tile], colour, tid % 3, (tid / 3) % 3, tid / 9, args.two_pass != 0);
     // wait for this item's brick (bounded); a thread whose wait gave up
     // computes nothing and the vote at the barrier ends the CTA before
     // anything is written
@@ -593,7 +569,7 @@ __global__ void __launch_bounds__(Q1Cell<CZ>::NT, Q1Cell<CZ>::MINB)
 
     // ---- write-out of the nodes this thread owns (the lower cell of a
     // shared node owns it)
-    int rl[NV];
+    int rl[NV], xyz[NV];
     size_t gidx[NV];
 #pragma unroll
     for (int e = 0; e < NV; ++e)
@@ -608,10 +584,14 @@ __global__ void __launch_bounds__(Q1Cell<CZ>::NT, Q1Cell<CZ>::MINB)
       int const sz = (Z == 0 && tiz > 0) ? 1 : ((Z == TZ && tiz < args.nt[2] - 1) ? 2 : 0);
       rl[e] = (own && inside) ? (AT ? 4 : (sp.role[it & 1][sx + 3 * sy + 9 * sz] | 4)) : 0;
       gidx[e] = gx + (size_t)pitch * (gy + (size_t)nn1 * gzn);
+      xyz[e] = X | (Y << 8) | (Z << 16);
     }
+    if (!AT && args.two_pass)
+      send_halo<1, NV>(md, tile, res, rl, xyz);
     write_nodes<AT, NV>(args, md, y, res, rl, gidx);
-    // vmult writes zeros into the row padding of the node layout
-    if (!AT && args.mode == 0 && tix == nt0 - 1 && pitch > args.nn[0])
+    // vmult writes zeros into the row padding of the node layout (the
+    // two-pass gather does that itself)
+    if (!AT && !args.two_pass && args.mode == 0 && tix == nt0 - 1 && pitch > args.nn[0])
     {
       int const npad = pitch - args.nn[0];
       for (int i = tid; i < npad * BY * BZ; i += NT)

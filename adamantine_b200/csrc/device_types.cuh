@@ -116,7 +116,9 @@ struct MemberData
   int32_t const *face_slot;
   double *face_powder;  // [slot][6][NF]
   double const *cosv, *sinv;
-  uint32_t const *tile_nbr; // 27-bit neighbour-activity mask per tile
+  uint32_t const *tile_nbr; // 27-bit neighbour-activity mask per tile (bit 13: the tile itself)
+  double *halo;             // two-pass schedule: [n_tiles][halo size] partial sums of the
+                            // nodes on each tile's upper brick faces
   MaterialDesc const *mat;
   BeamState *beam_state; // [kMaxBeams], current stage
   double *clock;        // [0] stage base time, [1] dt
@@ -156,6 +158,7 @@ struct KernelArgs
   int *claim;   // non-null: items after each CTA's first are claimed from this
                 // counter (zero at the launch), dynamic load balance
   int cells_per_thread; // FE_Q(1) cell kernel: 1 or 2 cells (stacked in z) per thread
+  int two_pass;         // two-pass schedule: owners write, upper-face partial sums to md.halo
   int stage;
   int last;     // last stage of the step (updates y)
   int n_stages; // 1 forward Euler

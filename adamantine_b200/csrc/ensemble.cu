@@ -185,6 +185,21 @@ void Ensemble::launch_step(double *solutions)
     a.y_override = nullptr;
     double const *src = i == 0 ? solutions : (a.src_sel == 1 ? za_.p : zb_.p);
     CUtensorMap const map = brick_map(members_[0]->mesh_, src, n, stride_);
+    if (schedule_ == Thermal::kScheduleTwoPass)
+    {
+      // every member's tiles in one launch (member-major runs per CTA), then
+      // the gather pass over every member's nodes
+      a.two_pass = 1;
+      a.blocked = 1;
+      if (!awork_.empty())
+      {
+        a.work = awork_d_.p;
+        launch_tile(deg_, ns_, poly_p_, map, a, (int)awork_.size(), stream_);
+        ADM_CK(cudaGetLastError());
+      }
+      launch_two_pass_gather(deg_, a, n, stream_);
+      continue;
+    }
     if (schedule_ == Thermal::kScheduleAtomic)
     {
       // member-major list, one contiguous run per CTA: a CTA changes member
@@ -324,7 +339,8 @@ void Ensemble::set_cells_per_thread(int n)
 
 void Ensemble::set_schedule(int schedule)
 {
-  if (schedule != Thermal::kScheduleColoured && schedule != Thermal::kScheduleAtomic)
+  if (schedule != Thermal::kScheduleColoured && schedule != Thermal::kScheduleAtomic &&
+      schedule != Thermal::kScheduleTwoPass)
     throw Error(ADM_ERR_INVALID, "unknown schedule");
   if (schedule != schedule_)
     drop_graph();
@@ -354,7 +370,7 @@ int Ensemble::autotune(double const *solutions, double dt, double *ms_out)
   double best = 0.0;
   int choice = saved, choice_cz = saved_cz;
   int const deg = members_.empty() ? 2 : members_[0]->mesh_.deg;
-  for (int sch : {Thermal::kScheduleColoured, Thermal::kScheduleAtomic})
+  for (int sch : {Thermal::kScheduleColoured, Thermal::kScheduleAtomic, Thermal::kScheduleTwoPass})
     for (int cz = 1; cz <= (deg == 1 ? 2 : 1); ++cz)
   {
     schedule_ = sch;
@@ -568,14 +584,24 @@ int adm_ensemble_get_cells_per_thread(adm_ensemble const *e, int32_t *n)
   });
 }
 
-int adm_ensemble_autotune(adm_ensemble *e, double const *solutions, double dt, int32_t *schedule, double *ms)
+int adm_ensemble_autotune_schedules(adm_ensemble *e, double const *solutions, double dt, int32_t *schedule,
+                                    double *ms, int32_t n_ms)
 {
   return adm::guard([&] {
     ADM_REQUIRE(e && solutions, "null argument");
-    int const c = as_ens(e)->autotune(solutions, dt, ms);
+    ADM_REQUIRE(n_ms >= 0, "n_ms must not be negative");
+    double t[ADM_N_SCHEDULES] = {0.0, 0.0, 0.0};
+    int const c = as_ens(e)->autotune(solutions, dt, t);
     if (schedule)
       *schedule = c;
+    for (int k = 0; ms && k < n_ms && k < ADM_N_SCHEDULES; ++k)
+      ms[k] = t[k];
   });
+}
+
+int adm_ensemble_autotune(adm_ensemble *e, double const *solutions, double dt, int32_t *schedule, double *ms)
+{
+  return adm_ensemble_autotune_schedules(e, solutions, dt, schedule, ms, 2);
 }
 
 int adm_ensemble_synchronize(adm_ensemble *e)

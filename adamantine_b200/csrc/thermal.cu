@@ -459,6 +459,7 @@ Thermal::Thermal(adm_config const &cfg, int device, cudaStream_t stream, bool ow
   cell_info_d_.alloc(C);
   has_melted_d_.alloc(C);
   tile_nbr_d_.alloc(mesh_.n_tiles);
+  halo_d_.alloc(mesh_.n_tiles * two_pass_halo_size(mesh_.deg));
   clock_.alloc(2);
   error_d_.alloc(1);
   claim_d_.alloc(8);
@@ -641,6 +642,7 @@ void Thermal::upload_member()
   md.cosv = cos_d_.p;
   md.sinv = sin_d_.p;
   md.tile_nbr = tile_nbr_d_.p;
+  md.halo = halo_d_.p;
   md.mat = mat_d_.p;
   md.beam_state = beam_state_d_.p;
   md.clock = clock_.p;
@@ -862,6 +864,22 @@ CUtensorMap brick_map(Mesh const &m, double const *base, int n_members, size_t m
 void Thermal::launch_pass(KernelArgs a, double const *src)
 {
   CUtensorMap const map = brick_map(mesh_, src, 1, mesh_.n_nodes);
+  if (schedule_ == kScheduleTwoPass)
+  {
+    // one launch over every tile (no atomics): each node's owner writes it,
+    // the partial sums of nodes on a tile's upper faces go to its halo
+    // array, and the gather pass completes the shared nodes in a fixed order
+    int const count = colour_off_[8];
+    a.two_pass = 1;
+    if (count > 0)
+    {
+      a.work = awork_d_.p;
+      launch_tile(mesh_.deg, ns_, poly_p_, map, a, count, stream_);
+      ADM_CK(cudaGetLastError());
+    }
+    launch_two_pass_gather(mesh_.deg, a, 1, stream_);
+    return;
+  }
   if (schedule_ == kScheduleAtomic)
   {
     // one launch over every tile (the ascending list), items strided over
@@ -960,7 +978,8 @@ void Thermal::vmult(double *dst, double const *src, bool add)
   ADM_CK(cudaSetDevice(device_));
   // Nodes that only inactive tiles touch are not written by the tile kernel;
   // the atomic schedule adds into a zeroed vector.
-  if (!add && (!topo_.all_tiles_active || schedule_ == kScheduleAtomic))
+  // (the two-pass gather writes every node itself)
+  if (!add && schedule_ != kScheduleTwoPass && (!topo_.all_tiles_active || schedule_ == kScheduleAtomic))
     ADM_CK(cudaMemsetAsync(dst, 0, mesh_.n_nodes * sizeof(double), stream_));
   prepare_stage(0.0);
   KernelArgs a = base_args();
@@ -981,7 +1000,7 @@ void Thermal::vmult_stage(double *dst, double const *src, double c)
 {
   if (!setup_done_)
     throw Error(ADM_ERR_INVALID, "setup() has not been called");
-  if (!topo_.all_tiles_active || schedule_ == kScheduleAtomic)
+  if (schedule_ != kScheduleTwoPass && (!topo_.all_tiles_active || schedule_ == kScheduleAtomic))
     ADM_CK(cudaMemsetAsync(dst, 0, mesh_.n_nodes * sizeof(double), stream_));
   prepare_stage(c);
   KernelArgs a = base_args();
@@ -1531,7 +1550,7 @@ void Thermal::set_cells_per_thread(int n)
 
 void Thermal::set_schedule(int schedule)
 {
-  if (schedule != kScheduleColoured && schedule != kScheduleAtomic)
+  if (schedule != kScheduleColoured && schedule != kScheduleAtomic && schedule != kScheduleTwoPass)
     throw Error(ADM_ERR_INVALID, "unknown schedule");
   if (schedule != schedule_ && step_graph_)
   {
@@ -1606,7 +1625,7 @@ int Thermal::autotune(double const *field, double *ms_out)
   int choice = saved, choice_cz = saved_cz;
   // launch schedules x (FE_Q(1)) cells per thread; ms_out[schedule] is the
   // schedule's best time
-  for (int sch : {kScheduleColoured, kScheduleAtomic})
+  for (int sch : {kScheduleColoured, kScheduleAtomic, kScheduleTwoPass})
     for (int cz = 1; cz <= (mesh_.deg == 1 ? 2 : 1); ++cz)
     {
       schedule_ = sch;

@@ -162,6 +162,9 @@ void launch_stage_prepare(MemberData *members, int n, double c, cudaStream_t str
 // Per-Gauss-point powder ratios [C][NN] from the sparse powder history.
 // Stage update of the atomic schedule for n_members members (a.members).
 void launch_stage_finalize(KernelArgs const &a, size_t n_nodes, int n_members, cudaStream_t stream);
+// two-pass schedule: the gather pass, and a tile's halo array length
+void launch_two_pass_gather(int deg, KernelArgs const &a, int n_members, cudaStream_t stream);
+size_t two_pass_halo_size(int deg);
 // The per-point powder ratio [C][NN] from the sparse modes; cells with
 // skip[c] == 0 are not written (skip may be null).
 void launch_expand_powder(uint32_t const *cell_info, int NN, uint8_t const *pmode, double const *pcell,
@@ -256,7 +259,7 @@ public:
   // reproducible) or atomic (one launch over every tile, node sums by
   // atomics, separate update pass; faster when a colour has fewer tiles than
   // the GPU holds CTAs, not bit reproducible run to run).
-  static constexpr int kScheduleColoured = 0, kScheduleAtomic = 1;
+  static constexpr int kScheduleColoured = 0, kScheduleAtomic = 1, kScheduleTwoPass = 2;
   void set_schedule(int schedule);
   int schedule() const { return schedule_; }
   // FE_Q(1) operator kernel: 1 or 2 cells (stacked in z) per thread
@@ -334,6 +337,7 @@ private:
   DevBuf<uint8_t> powder_mode_, has_melted_d_;
   DevBuf<int32_t> face_slot_d_, error_d_;
   DevBuf<int32_t> claim_d_; // per-colour work counters of the tile launches (dynamic claiming)
+  DevBuf<double> halo_d_;   // two-pass schedule: per-tile upper-face partial sums
   DevBuf<int64_t> cells_d_;
   // deposition: per-cell mark, append list, material ids
   DevBuf<int32_t> last_box_d_, list_box_d_;

@@ -722,6 +722,76 @@ __device__ __noinline__ void face_terms(SmemPhys const &sp, MaterialDesc const *
   }
 }
 
+// Role of a node class of a tile whose sharing state per direction is
+// (s0, s1, s2) (0 not shared, 1 shared with the lower neighbour tile, 2 with
+// the upper one), from the tile's neighbour-activity mask nbr and colour.
+// Coloured schedule: bit 1 first and bit 2 last toucher in colour order.
+// Two-pass schedule: 8 -- the node belongs to an upper neighbour tile (the
+// partial sum goes to this tile's halo array); 1 -- the node is this tile's:
+// its partial sum is stored here, and the gather pass adds the neighbours'
+// halo sums and applies the stage update (so the tile's write-out stores
+// only, with no loads to wait for).
+__device__ __forceinline__ int node_role(uint32_t nbr, int colour, int s0, int s1, int s2, bool two_pass)
+{
+  if (two_pass)
+    return (s0 == 2 || s1 == 2 || s2 == 2) ? 8 : 1;
+  int cmin = 8, cmax = -1;
+#pragma unroll
+  for (int m = 0; m < 8; ++m)
+  {
+    int const b0 = m & 1, b1 = (m >> 1) & 1, b2 = (m >> 2) & 1;
+    if ((b0 && s0 == 0) || (b1 && s1 == 0) || (b2 && s2 == 0))
+      continue;
+    int const o0 = b0 ? (s0 == 1 ? -1 : 1) : 0;
+    int const o1 = b1 ? (s1 == 1 ? -1 : 1) : 0;
+    int const o2 = b2 ? (s2 == 1 ? -1 : 1) : 0;
+    int const bit = (o0 + 1) + 3 * (o1 + 1) + 9 * (o2 + 1);
+    if (!((nbr >> bit) & 1u))
+      continue;
+    int const c = colour ^ (b0 | (b1 << 1) | (b2 << 2));
+    cmin = c < cmin ? c : cmin;
+    cmax = c > cmax ? c : cmax;
+  }
+  return (colour == cmin ? 1 : 0) | (colour == cmax ? 2 : 0);
+}
+
+// Two-pass schedule: the halo array of a tile holds one partial sum per node
+// on its upper brick faces (x = BX - 1, y = BY - 1 or z = BZ - 1, brick-local);
+// these nodes belong to the upper neighbours.
+template <int BX, int BY, int BZ>
+struct HaloLayout
+{
+  static constexpr int SIZE = BX * BY + BX * (BZ - 1) + (BY - 1) * (BZ - 1);
+  __host__ __device__ static int index(int X, int Y, int Z)
+  {
+    if (Z == BZ - 1)
+      return X + BX * Y;
+    if (Y == BY - 1)
+      return BX * BY + X + BX * Z;
+    return BX * BY + BX * (BZ - 1) + Y + (BY - 1) * Z; // X == BX - 1
+  }
+};
+template <int DEG>
+using HaloOf = HaloLayout<TD<DEG>::BX, TD<DEG>::BY, TD<DEG>::BZ>;
+
+// Two-pass write-out of the nodes of a thread marked 8 (owned by an upper
+// neighbour): their partial sums into the tile's halo array; the mark is
+// cleared so write_nodes leaves them alone. XYZ[i] packs the node's
+// brick-local coordinates (X | Y << 8 | Z << 16).
+template <int DEG, int NV>
+__device__ __forceinline__ void send_halo(MemberData const &md, int tile, double const *res, int *rl,
+                                          int const *xyz)
+{
+  using HL = HaloOf<DEG>;
+#pragma unroll
+  for (int i = 0; i < NV; ++i)
+    if ((rl[i] & 12) == 12)
+    {
+      md.halo[(size_t)tile * HL::SIZE + HL::index(xyz[i] & 255, (xyz[i] >> 8) & 255, xyz[i] >> 16)] = res[i];
+      rl[i] = 0;
+    }
+}
+
 // Write-out of the node sums res[i] of one thread (rl[i]: bit 4 the thread
 // owns the node, bit 1 / 2 first / last toucher in colour order; gidx[i]:
 // its index in the node vector). Atomic schedule: added into the zeroed
@@ -981,29 +1051,10 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
     }
     if (!AT && tid < 27)
     {
-      // first/last toucher role of a node whose per-direction sharing state
-      // is (tid % 3, tid / 3 % 3, tid / 9): 0 not shared, 1 shared with the
-      // lower neighbour tile, 2 with the upper one.
-      uint32_t const nbr = md.tile_nbr[tile];
-      int const s0 = tid % 3, s1 = (tid / 3) % 3, s2 = tid / 9;
-      int cmin = 8, cmax = -1;
-#pragma unroll
-      for (int m = 0; m < 8; ++m)
-      {
-        int const b0 = m & 1, b1 = (m >> 1) & 1, b2 = (m >> 2) & 1;
-        if ((b0 && s0 == 0) || (b1 && s1 == 0) || (b2 && s2 == 0))
-          continue;
-        int const o0 = b0 ? (s0 == 1 ? -1 : 1) : 0;
-        int const o1 = b1 ? (s1 == 1 ? -1 : 1) : 0;
-        int const o2 = b2 ? (s2 == 1 ? -1 : 1) : 0;
-        int const bit = (o0 + 1) + 3 * (o1 + 1) + 9 * (o2 + 1);
-        if (!((nbr >> bit) & 1u))
-          continue;
-        int const c = colour ^ (b0 | (b1 << 1) | (b2 << 2));
-        cmin = c < cmin ? c : cmin;
-        cmax = c > cmax ? c : cmax;
-      }
-      sp.role[buf][tid] = (colour == cmin ? 1 : 0) | (colour == cmax ? 2 : 0);
+      // the role of the node class (tid % 3, tid / 3 % 3, tid / 9): sharing
+      // state per direction, 0 not shared, 1 with the lower neighbour tile,
+      // 2 with the upper one
+      sp.role[buf][tid] = node_role(md.tile_nbr[tile], colour, tid % 3, (tid / 3) % 3, tid / 9, args.two_pass != 0);
     }
     if (slab == 0)
       changed[cl] = 0;
@@ -1381,7 +1432,7 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
     int const Z = DEG * lz + slab;
     int const gz = nz0 + Z;
     int const sz = (Z == 0 && tiz > 0) ? 1 : ((Z == DEG * TZ && tiz < args.nt[2] - 1) ? 2 : 0);
-    int rl[NQS];
+    int rl[NQS], xyz[NQS];
     size_t gidx[NQS];
 #pragma unroll
     for (int i = 0; i < NQS; ++i)
@@ -1395,10 +1446,14 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
       int const sy = (Y == 0 && tiy > 0) ? 1 : ((Y == DEG * TY && tiy < nt1 - 1) ? 2 : 0);
       rl[i] = (own && inside) ? (AT ? 4 : (sp.role[buf][sx + 3 * sy + 9 * sz] | 4)) : 0;
       gidx[i] = gx + (size_t)pitch * (gy + (size_t)nn1 * gz);
+      xyz[i] = X | (Y << 8) | (Z << 16);
     }
+    if (!AT && args.two_pass)
+      send_halo<DEG, NQS>(md, tile, res, rl, xyz);
     write_nodes<AT, NQS>(args, md, y, res, rl, gidx);
-    // vmult writes zeros into the row padding of the node layout
-    if (!AT && args.mode == 0 && tix == nt0 - 1 && pitch > args.nn[0])
+    // vmult writes zeros into the row padding of the node layout (the
+    // two-pass gather does that itself)
+    if (!AT && !args.two_pass && args.mode == 0 && tix == nt0 - 1 && pitch > args.nn[0])
     {
       int const npad = pitch - args.nn[0];
       for (int i = tid; i < npad * BY * BZ; i += NT)
@@ -1443,4 +1498,116 @@ void launch_tile_t(CUtensorMap const &map, KernelArgs const &a, int n_items, cud
     launch_tile_f<DEG, NS, P, AT, false>(map, a, n_items, stream);
 }
 
+} // namespace adm
+
+namespace adm
+{
+// Two-pass schedule, second pass, over every node of the padded layout of
+// every member (blockIdx.y). A node belongs to the tile whose half-open node
+// range holds it (the last tile per direction takes the upper end too). Its
+// sum is the owner's partial sum (when the owner is active) plus, in a fixed
+// order, the halo partial sums of the active lower neighbour tiles that
+// touch it -- no atomics, bit-reproducible. vmult: the owner's sum is in dst
+// already, the halo sums are added (nodes no active tile touches and the
+// row padding get zero); a stage: the inverse lumped mass and the
+// Runge-Kutta update for every node an active tile touches.
+template <int DEG>
+__device__ __forceinline__ void two_pass_gather_node(KernelArgs const &a, MemberData const &md, int gx, int gy,
+                                                     int gz, size_t g)
+{
+  using T_ = TD<DEG>;
+  using HL = HaloOf<DEG>;
+  constexpr int SX = DEG * T_::TX, SY = DEG * T_::TY, SZ = DEG * T_::TZ;
+  bool const vm = a.mode != 2;
+  if (gx >= a.nn[0])
+  {
+    if (a.mode == 0)
+      a.vdst[g] = 0.0;
+    return;
+  }
+  int const tx = min(gx / SX, a.nt[0] - 1), ty = min(gy / SY, a.nt[1] - 1), tz = min(gz / SZ, a.nt[2] - 1);
+  int const X = gx - SX * tx, Y = gy - SY * ty, Z = gz - SZ * tz;
+  bool const fx = X == 0 && tx > 0, fy = Y == 0 && ty > 0, fz = Z == 0 && tz > 0;
+  size_t const owner = tx + (size_t)a.nt[0] * (ty + (size_t)a.nt[1] * tz);
+  bool const owner_active = (md.tile_nbr[owner] >> 13) & 1u;
+  double h = 0.0;
+  bool any = false;
+#pragma unroll
+  for (int m = 1; m < 8; ++m)
+  {
+    int const dx = m & 1, dy = (m >> 1) & 1, dz = m >> 2;
+    if ((dx && !fx) || (dy && !fy) || (dz && !fz))
+      continue;
+    size_t const c = owner - (size_t)dx - (size_t)a.nt[0] * ((size_t)dy + (size_t)a.nt[1] * (size_t)dz);
+    if (!((md.tile_nbr[c] >> 13) & 1u))
+      continue;
+    h += md.halo[c * HL::SIZE + HL::index(X + dx * SX, Y + dy * SY, Z + dz * SZ)];
+    any = true;
+  }
+  if (vm && !any)
+  {
+    // complete in its owner's tile, or touched by no active tile
+    if (!owner_active && a.mode == 0)
+      a.vdst[g] = 0.0;
+    return;
+  }
+  if (!any && !owner_active)
+    return; // no active tile touches it: not a degree of freedom
+  if (vm)
+  {
+    // the owner's partial sum (or, mode 1, the caller's value plus it) is in
+    // dst already
+    if (owner_active || a.mode == 1)
+      a.vdst[g] += h;
+    else
+      a.vdst[g] = h;
+    return;
+  }
+  double *const y = a.y_override ? a.y_override : md.y;
+  double const total = (owner_active ? md.acc[g] : 0.0) + h;
+  double const dt = md.clock[1];
+  double const f = md.inv_mass[g] * total;
+  if (!isfinite(f))
+    atomicCAS(md.error, 0, (int)DERR_NONFINITE);
+  double const yv = y[g];
+  if (a.n_stages == 1)
+  {
+    y[g] = yv + dt * f;
+    return;
+  }
+  double const sv = a.stage > 0 ? md.s[g] : 0.0;
+  if (!a.last)
+  {
+    double zn = yv;
+    if (a.has_f0)
+      zn = zn + (dt * a.a_next_f0) * md.f0[g];
+    zn = zn + (dt * a.a_next) * f;
+    (a.dst_sel == 1 ? md.za : md.zb)[g] = zn;
+    double const sb = (dt * a.b_i) * f;
+    md.s[g] = a.stage == 0 ? sb : sv + sb;
+    if (a.store_f0)
+      md.f0[g] = f;
+  }
+  else
+  {
+    y[g] = yv + (sv + (dt * a.b_i) * f);
+  }
+}
+
+// Grid: x over the padded row (pitch), y strided over the node rows
+// (nn[1] * nn[2] of them), z over the members; no 64-bit divisions.
+template <int DEG>
+__global__ void two_pass_gather_kernel(KernelArgs a)
+{
+  int const gx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gx >= a.pitch)
+    return;
+  MemberData const &md = a.members[blockIdx.z];
+  int const nn1 = a.nn[1], rows = nn1 * a.nn[2];
+  for (int r = blockIdx.y; r < rows; r += gridDim.y)
+  {
+    int const gz = r / nn1, gy = r - gz * nn1;
+    two_pass_gather_node<DEG>(a, md, gx, gy, gz, gx + (size_t)a.pitch * (size_t)r);
+  }
+}
 } // namespace adm

@@ -193,7 +193,8 @@ class Ensemble:
         return out
 
     def set_schedule(self, schedule: int):
-        """Launch schedule of the batched stages (0 coloured, 1 atomic)."""
+        """Launch schedule of the batched stages (0 coloured, 1 atomic, 2
+        two-pass)."""
         _lib.check(self._L.adm_ensemble_set_schedule(self._h, int(schedule)))
 
     def set_cells_per_thread(self, n: int):
@@ -209,11 +210,11 @@ class Ensemble:
     def autotune(self, solutions: torch.Tensor, dt: float):
         """Times one batched step per schedule (and, for FE degree 1, per
         cells-per-thread variant) on a copy of solutions, keeps the fastest;
-        returns (schedule, [best ms coloured, best ms atomic])."""
+        returns (schedule, [best ms coloured, atomic, two-pass])."""
         c = ctypes.c_int32()
-        ms = np.zeros(2)
-        _lib.check(self._L.adm_ensemble_autotune(self._h, self._check(solutions), float(dt), ctypes.byref(c),
-                                                 _ptr(ms, ctypes.c_double)))
+        ms = np.zeros(3)
+        _lib.check(self._L.adm_ensemble_autotune_schedules(self._h, self._check(solutions), float(dt),
+                                                           ctypes.byref(c), _ptr(ms, ctypes.c_double), 3))
         return int(c.value), ms.tolist()
 
     def device_error(self) -> int:

@@ -233,10 +233,12 @@ class ThermalPhysics:
         st = config.to_struct()
         _lib.check(self._L.adm_update_material(self._h, ctypes.byref(st)))
 
-    COLOURED, ATOMIC = 0, 1
+    COLOURED, ATOMIC, TWO_PASS = 0, 1, 2
+    SCHEDULES = ("coloured", "atomic", "two_pass")
 
     def set_schedule(self, schedule: int):
-        """Launch schedule: COLOURED (bit reproducible) or ATOMIC."""
+        """Launch schedule: COLOURED or TWO_PASS (no atomics, bit
+        reproducible) or ATOMIC."""
         _lib.check(self._L.adm_set_schedule(self._h, int(schedule)))
 
     def schedule(self) -> int:
@@ -255,12 +257,13 @@ class ThermalPhysics:
         return int(v.value)
 
     def autotune(self, field: torch.Tensor):
-        """Times both schedules (and, for FE degree 1, both cells-per-thread
+        """Times every schedule (and, for FE degree 1, both cells-per-thread
         variants) on vmults of field, keeps the fastest; returns (schedule,
-        [best ms coloured, best ms atomic])."""
+        [best ms coloured, atomic, two-pass])."""
         c = ctypes.c_int32()
-        ms = np.zeros(2)
-        _lib.check(self._L.adm_autotune(self._h, _dev(field), ctypes.byref(c), _ptr(ms, ctypes.c_double)))
+        ms = np.zeros(3)
+        _lib.check(self._L.adm_autotune_schedules(self._h, _dev(field), ctypes.byref(c), _ptr(ms, ctypes.c_double),
+                                                  3))
         return int(c.value), ms.tolist()
 
     def save_checkpoint(self, path: str, time: float, solution: torch.Tensor):

@@ -32,6 +32,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "heat vmult GDoF/s (FP64 Q2) & %HBM peak; batched-ensemble vs looped steps/s"
+SCHEDULE_NAMES = ("coloured", "atomic", "two_pass")
 WORKLOAD = "phase_change_q2_128x128x64_vmult"
 
 
@@ -46,6 +47,13 @@ FP64_FLOP_PER_Q2_CELL = 2247
 # colour launches of the coloured schedule (L2 flushed before every launch,
 # so re-reads that stay in L2 in the timed loop are counted).
 DRAM_BYTES_PER_VMULT_FULL = {"atomic": 211.8e6, "coloured": 327.0e6}
+TRAFFIC_NOTE = {"atomic": "ncu, one launch per vmult",
+                "coloured": "ncu, L2 flushed before each of the 8 colour launches"}
+# per schedule: the kernels of one vmult, their launch pattern and count
+KERNELS = {"coloured": ("adm::tile_kernel<2,3,2,0,0>", "8 colour launches", 8),
+           "atomic": ("adm::tile_kernel<2,3,2,1,0>", "1 launch", 1),
+           "two_pass": ("adm::tile_kernel<2,3,2,0,0> (two-pass write-out) + adm::two_pass_gather_kernel<2>",
+                        "1 tile launch + 1 gather launch", 2)}
 
 
 def fp64_fma_peak(device):
@@ -347,7 +355,7 @@ def run_ensemble(args, dist, local_rank):
                           "speedup_vs_coloured": ms_l / ms_b, "speedup_vs_atomic": ms_la / ms_b,
                           "path": "adm_ensemble_evolve_looped: each member's stages launched one by one"},
         "identical_results": identical, "max_rel_diff_batched_vs_looped": max_rel_diff,
-        "batched_schedule": ["coloured", "atomic"][schedule],
+        "batched_schedule": SCHEDULE_NAMES[schedule],
         "batched_path": "one CUDA graph per step (4 stages)",
         "work_items_per_sweep": e.n_work_items(),
         "enkf_analysis_ms": ms_a, "n_obs": int(idx.shape[1]), "augmented_params": 2,
@@ -425,7 +433,7 @@ def run_adjoint(args, local_rank):
         "cost_ratio": grad_s / fwd_s, "checkpoint_every": k_auto,
         "checkpoint_policy": "auto: the longest segment whose stores fit in half of the free HBM "
                              "(3.5 GB of stage inputs and 11 GB of powder states for the whole run here)",
-        "timing": "host wall clock, synchronized, median of 3", "forward_schedule": ["coloured", "atomic"][schedule],
+        "timing": "host wall clock, synchronized, median of 3", "forward_schedule": SCHEDULE_NAMES[schedule],
         "checkpoint_every_20": {"forward_ms": 1e3 * fwd20_s, "gradient_ms": 1e3 * grad20_s,
                                 "cost_ratio": grad20_s / fwd20_s, "checkpoint_every": 20,
                                 "max_rel_diff_vs_auto": same},
@@ -475,8 +483,8 @@ def run_rk4_steps(args, local_rank):
     peak, kind = measured_peaks()
     return {"workload": RK4_WORKLOAD, "steps": args.rk4_steps, "dt": dt, "ms_per_step": ms,
             "gdof_per_s": 4 * n_dofs / (ms * 1e-3) / 1e9, "steps_per_s": 1e3 / ms,
-            "schedule": ["coloured", "atomic"][schedule],
-            "autotune_ms_per_vmult": {"coloured": sched_ms[0], "atomic": sched_ms[1]},
+            "schedule": SCHEDULE_NAMES[schedule],
+            "autotune_ms_per_vmult": dict(zip(SCHEDULE_NAMES, sched_ms)),
             "algorithmic_bytes_per_step": alg, "achieved_gbs": alg / (ms * 1e-3) / 1e9,
             "hbm_frac": alg / (ms * 1e-3) / 1e9 / peak, "peak_kind": f"{kind} hbm_gbs",
             "path": "adm_evolve_n_steps (CUDA graph per step)"}
@@ -549,7 +557,7 @@ def run_deposition(args, local_rank, with_cpu):
         "ms_per_step": ms / steps, "gdofs_per_s": 4 * n_nodes * steps / (ms * 1e-3) / 1e9,
         "hbm_gbs_algorithmic": bytes_step * steps / (ms * 1e-3) / 1e9, "cells_activated": activated + n_act,
         "boxes": boxes.n, "activation": "device append list, driver window per step",
-        "schedule": ["coloured", "atomic"][schedule],
+        "schedule": SCHEDULE_NAMES[schedule],
         "microstructure_ms_per_step": ms_micro / 5, "microstructure_records_per_step": n_records / 5,
     }
     if with_cpu:
@@ -799,7 +807,7 @@ def run_ours(args, rank, world, local_rank):
     e2e_val = world * n_dofs / e2e_s / 1e9
     del src_h
 
-    sched_name = ["coloured", "atomic"][schedule]
+    sched_name = SCHEDULE_NAMES[schedule]
     peak, peak_kind = measured_peaks()
     fp64_peak = fp64_fma_peak(local_rank)
     # algorithmic bytes of one vmult: read src, write dst (8 B per node each),
@@ -822,14 +830,12 @@ def run_ours(args, rank, world, local_rank):
         "timing": {"l2": "two src/dst pairs alternate (272 MB working set > 126 MB L2)",
                    "events": "CUDA events on the handle's stream around the K vmults"},
         "schedule": sched_name,
-        "autotune_ms_per_vmult": {"coloured": schedule_ms[0], "atomic": schedule_ms[1]},
+        "autotune_ms_per_vmult": dict(zip(SCHEDULE_NAMES, schedule_ms)),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,
-                     "traffic": DRAM_BYTES_PER_VMULT_FULL[sched_name] if args.size == "full" else None,
-                     "traffic_note": ("ncu, one launch per vmult" if schedule == 1 else
-                                      "ncu, L2 flushed before each of the 8 colour launches"), "peak_kind": f"{peak_kind} hbm_gbs",
-                     "kernel": (f"adm::tile_kernel<2,3,2,{'true' if schedule == 1 else 'false'}> "
-                                f"({'1 launch' if schedule == 1 else '8 colour launches'} per vmult)"),
+                     "traffic": DRAM_BYTES_PER_VMULT_FULL.get(sched_name) if args.size == "full" else None,
+                     "traffic_note": TRAFFIC_NOTE.get(sched_name), "peak_kind": f"{peak_kind} hbm_gbs",
+                     "kernel": KERNELS[sched_name][0] + f" ({KERNELS[sched_name][1]} per vmult)",
                      "algorithmic_bytes_per_vmult": alg_bytes},
         # the operator is FP64-issue bound (per-qp physics plus sum
         # factorization), so the FP64 roofline is the binding one
@@ -839,9 +845,8 @@ def run_ours(args, rank, world, local_rank):
                           "peak_kind": "measured FP64 FMA rate (adm_diag_fp64_fma_rate) on this GPU"},
         "e2e": {"value": e2e_val, "unit": "GDoF/s", "h2d_bytes_per_step": 8 * g.m(),
                 "d2h_bytes_per_step": 8 * g.m(), "path": "adm_vmult_host (pinned host buffers: z-slab copies overlapped with the kernel)"},
-        # per vmult: the stage-prepare kernel + one tile launch (atomic
-        # schedule) or 8 colour launches (coloured schedule)
-        "gpu_launches": args.steps * (2 if schedule == 1 else 9),
+        # per vmult: the stage-prepare kernel + the schedule's launches
+        "gpu_launches": args.steps * (1 + KERNELS[sched_name][2]),
         "clocks": clk.summary(),
     }
     if args.rk4_steps > 0:

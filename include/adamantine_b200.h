@@ -203,11 +203,16 @@ int adm_update_beam(adm_thermal *h, int32_t i, adm_source const *beam);
  * the reference): ADM_SCHEDULE_COLOURED (default) runs one launch per tile
  * colour, sums shared nodes in colour order and fuses the stage update --
  * bit reproducible; ADM_SCHEDULE_ATOMIC runs every tile in one launch, sums
- * shared nodes with atomics and updates in a separate pass -- faster when a
- * colour has fewer tiles than the GPU holds CTAs (small meshes), rounding
- * order not reproducible run to run. */
+ * shared nodes with FP64 atomics and updates in a separate pass -- rounding
+ * order not reproducible run to run; ADM_SCHEDULE_TWO_PASS runs every tile
+ * in one launch without atomics: each node's owner tile writes it (and
+ * applies the stage update where no other tile touches it), partial sums of
+ * nodes on a tile's upper faces go to a per-tile halo array, and a streaming
+ * pass completes the shared nodes in a fixed order -- bit reproducible. */
 #define ADM_SCHEDULE_COLOURED 0
 #define ADM_SCHEDULE_ATOMIC 1
+#define ADM_SCHEDULE_TWO_PASS 2
+#define ADM_N_SCHEDULES 3
 int adm_set_schedule(adm_thermal *h, int32_t schedule);
 int adm_get_schedule(adm_thermal const *h, int32_t *schedule);
 /* Cells per thread of the FE_Q(1) operator kernel (no counterpart in the
@@ -217,12 +222,15 @@ int adm_get_schedule(adm_thermal const *h, int32_t *schedule);
  * bit-reproducible in the coloured schedule. */
 int adm_set_cells_per_thread(adm_thermal *h, int32_t n);
 int adm_get_cells_per_thread(adm_thermal const *h, int32_t *n);
-/* Autotuner: times both schedules (and, for FE degree 1, both cells-per-
+/* Autotuner: times every schedule (and, for FE degree 1, both cells-per-
  * thread variants) on vmults of the device field (the phase history is
  * restored afterwards), keeps the fastest in the handle and returns its
- * schedule in *schedule; ms[2] (may be NULL) receives each schedule's best
- * per-vmult time. */
+ * schedule in *schedule; ms[2] (may be NULL) receives the best per-vmult
+ * times of the coloured and atomic schedules. */
 int adm_autotune(adm_thermal *h, double const *field, int32_t *schedule, double *ms);
+/* The same autotuner over every schedule; ms (may be NULL) receives up to
+ * n_ms of the ADM_N_SCHEDULES best per-vmult times, indexed by schedule. */
+int adm_autotune_schedules(adm_thermal *h, double const *field, int32_t *schedule, double *ms, int32_t n_ms);
 
 /* ThermalPhysicsInterface::save_checkpoint
  * (source/ThermalPhysics.templates.hh:1062-1185): the cells' activity,

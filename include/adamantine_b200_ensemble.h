@@ -75,8 +75,13 @@ int adm_ensemble_get_cells_per_thread(adm_ensemble const *e, int32_t *n);
 /* Autotuner: times one batched step of size dt with each schedule (and, for
  * FE degree 1, each cells-per-thread variant) on a copy of solutions (phase
  * history and clocks restored), keeps the fastest and returns its schedule;
- * ms[2] (may be NULL) receives each schedule's best per-step time. */
+ * ms[2] (may be NULL) receives the best per-step times of the coloured and
+ * atomic schedules. */
 int adm_ensemble_autotune(adm_ensemble *e, double const *solutions, double dt, int32_t *schedule, double *ms);
+/* The same over every schedule; ms (may be NULL) receives up to n_ms of the
+ * ADM_N_SCHEDULES best per-step times, indexed by schedule. */
+int adm_ensemble_autotune_schedules(adm_ensemble *e, double const *solutions, double dt, int32_t *schedule,
+                                    double *ms, int32_t n_ms);
 /* First non-zero sticky device error word over the members (synchronizes). */
 int adm_ensemble_device_error(adm_ensemble *e, int32_t *code);
 int adm_ensemble_synchronize(adm_ensemble *e);

@@ -2,11 +2,11 @@
 configurations at their stated sizes (through the C ABI).
 
 - 32x32x16 Q1 solid with a convective top: 200 forward-Euler steps of 1e-6,
-  every step's vmult <= 1e-12 and the final field <= 1e-9, in both launch
-  schedules.
+  every step's vmult <= 1e-12 and the final field <= 1e-9, in all three
+  launch schedules.
 - 128x128x64 Q2 solid/liquid/powder (8,520,321 DoFs): one vmult <= 1e-12 and
-  the per-point powder history, then 20 RK4 steps <= 1e-9, in both launch
-  schedules.
+  the per-point powder history, then 20 RK4 steps <= 1e-9, in all three
+  launch schedules.
 - The 32-member 64x64x32 Q1 ensemble with ragged deposited heights: 100 RK4
   steps of the batched launch, every member <= 1e-9 against its own oracle
   run.
@@ -35,7 +35,7 @@ pytestmark = pytest.mark.gpu
 VMULT_TOL = 1e-12
 STEP_TOL = 1e-9
 FD_TOL = 1e-6
-COLOURED, ATOMIC = 0, 1
+COLOURED, ATOMIC, TWO_PASS = 0, 1, 2
 
 
 def oracle_for(cfg):
@@ -66,7 +66,7 @@ def solid_q1_reference():
     return cfg, T0, vm, y, t
 
 
-@pytest.mark.parametrize("schedule", [COLOURED, ATOMIC])
+@pytest.mark.parametrize("schedule", [COLOURED, ATOMIC, TWO_PASS])
 def test_solid_q1_200_forward_euler_steps(solid_q1_reference, schedule):
     cfg, T0, vm_ref, y_ref, t_ref = solid_q1_reference
     g = ThermalPhysics(cfg)
@@ -107,7 +107,7 @@ def phase_change_reference():
     return cfg, T0, vm, powder, y, t
 
 
-@pytest.mark.parametrize("schedule", [COLOURED, ATOMIC])
+@pytest.mark.parametrize("schedule", [COLOURED, ATOMIC, TWO_PASS])
 def test_phase_change_q2_full_size(phase_change_reference, schedule):
     cfg, T0, vm_ref, powder_ref, y_ref, t_ref = phase_change_reference
     g = ThermalPhysics(cfg)
