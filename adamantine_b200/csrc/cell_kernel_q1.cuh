@@ -326,7 +326,7 @@ __device__ __forceinline__ void q1_cell(SmemPhys const &sp, MemberData const &md
 // flag, the z sums) alternates between two copies by item parity, and the
 // brick of item k + 2 is requested after the barrier of item k into the
 // buffer that item k - 1 used.
-template <int NS, int P, bool AT, bool FC, int CZ>
+template <int NS, int P, int SC, bool FC, int CZ>
 __global__ void __launch_bounds__(Q1Cell<CZ>::NT, Q1Cell<CZ>::MINB)
     cell_kernel_q1(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ KernelArgs args, int n_items)
 {
@@ -487,8 +487,8 @@ __global__ void __launch_bounds__(Q1Cell<CZ>::NT, Q1Cell<CZ>::MINB)
       if (tid == 0)
         sp.member = w.member;
     }
-    if (!AT && tid < 27)
-      sp.role[it & 1][tid] = node_role(md.tile_nbr[tile], colour, tid % 3, (tid / 3) % 3, tid / 9, args.two_pass != 0);
+    if (SC == SC_COLOURED && tid < 27)
+      sp.role[it & 1][tid] = node_role(md.tile_nbr[tile], colour, tid % 3, (tid / 3) % 3, tid / 9);
     // wait for this item's brick (bounded); a thread whose wait gave up
     // computes nothing and the vote at the barrier ends the CTA before
     // anything is written
@@ -569,7 +569,7 @@ __global__ void __launch_bounds__(Q1Cell<CZ>::NT, Q1Cell<CZ>::MINB)
 
     // ---- write-out of the nodes this thread owns (the lower cell of a
     // shared node owns it)
-    int rl[NV], xyz[NV];
+    int rl[NV], slot[NV];
     size_t gidx[NV];
 #pragma unroll
     for (int e = 0; e < NV; ++e)
@@ -582,16 +582,20 @@ __global__ void __launch_bounds__(Q1Cell<CZ>::NT, Q1Cell<CZ>::MINB)
       int const sx = (X == 0 && tix > 0) ? 1 : ((X == TX && tix < nt0 - 1) ? 2 : 0);
       int const sy = (Y == 0 && tiy > 0) ? 1 : ((Y == TY && tiy < nt1 - 1) ? 2 : 0);
       int const sz = (Z == 0 && tiz > 0) ? 1 : ((Z == TZ && tiz < args.nt[2] - 1) ? 2 : 0);
-      rl[e] = (own && inside) ? (AT ? 4 : (sp.role[it & 1][sx + 3 * sy + 9 * sz] | 4)) : 0;
+      slot[e] = 0;
+      if constexpr (SC == SC_TWO_PASS)
+        rl[e] = (own && inside) ? two_pass_slot<HaloOf<1>>(X, Y, Z, sx, sy, sz, &slot[e]) : 0;
+      else
+        rl[e] = (own && inside) ? (SC == SC_ATOMIC ? 4 : (sp.role[it & 1][sx + 3 * sy + 9 * sz] | 4)) : 0;
       gidx[e] = gx + (size_t)pitch * (gy + (size_t)nn1 * gzn);
-      xyz[e] = X | (Y << 8) | (Z << 16);
     }
-    if (!AT && args.two_pass)
-      send_halo<1, NV>(md, tile, res, rl, xyz);
-    write_nodes<AT, NV>(args, md, y, res, rl, gidx);
+    if constexpr (SC == SC_TWO_PASS)
+      write_nodes_two_pass<HaloOf<1>, NV>(args, md, tile, res, rl, gidx, slot);
+    else
+      write_nodes<SC == SC_ATOMIC, NV>(args, md, y, res, rl, gidx);
     // vmult writes zeros into the row padding of the node layout (the
     // two-pass gather does that itself)
-    if (!AT && !args.two_pass && args.mode == 0 && tix == nt0 - 1 && pitch > args.nn[0])
+    if (SC == SC_COLOURED && args.mode == 0 && tix == nt0 - 1 && pitch > args.nn[0])
     {
       int const npad = pitch - args.nn[0];
       for (int i = tid; i < npad * BY * BZ; i += NT)
@@ -614,42 +618,54 @@ __global__ void __launch_bounds__(Q1Cell<CZ>::NT, Q1Cell<CZ>::MINB)
 
 // Launches the persistent Q1 cell kernel over n_items work items with at
 // most the number of CTAs that are resident at once on the device.
-template <int NS, int P, bool AT, bool FC, int CZ>
+template <int NS, int P, int SC, bool FC, int CZ>
 void launch_cell_q1_f(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
 {
   using Q = Q1Cell<CZ>;
   static int grid_cap = 0;
   if (grid_cap == 0)
   {
-    cudaFuncSetAttribute(cell_kernel_q1<NS, P, AT, FC, CZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(cell_kernel_q1<NS, P, SC, FC, CZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)Q::SMEM);
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cell_kernel_q1<NS, P, AT, FC, CZ>, Q::NT, Q::SMEM);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cell_kernel_q1<NS, P, SC, FC, CZ>, Q::NT, Q::SMEM);
     grid_cap = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
   }
   int const grid = n_items < grid_cap ? n_items : grid_cap;
-  cell_kernel_q1<NS, P, AT, FC, CZ><<<grid, Q::NT, Q::SMEM, stream>>>(map, a, n_items);
+  cell_kernel_q1<NS, P, SC, FC, CZ><<<grid, Q::NT, Q::SMEM, stream>>>(map, a, n_items);
 }
 
-template <int NS, int P, bool AT, int CZ>
+template <int NS, int P, int SC, int CZ>
 void launch_cell_q1_z(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
 {
   if (a.faces)
-    launch_cell_q1_f<NS, P, AT, true, CZ>(map, a, n_items, stream);
+    launch_cell_q1_f<NS, P, SC, true, CZ>(map, a, n_items, stream);
   else
-    launch_cell_q1_f<NS, P, AT, false, CZ>(map, a, n_items, stream);
+    launch_cell_q1_f<NS, P, SC, false, CZ>(map, a, n_items, stream);
 }
 
 // a.cells_per_thread 2: two cells per thread (z), else one
-template <int NS, int P, bool AT>
-void launch_cell_q1(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
+template <int NS, int P, int SC>
+void launch_cell_q1_s(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
 {
   if (a.cells_per_thread == 2)
-    launch_cell_q1_z<NS, P, AT, 2>(map, a, n_items, stream);
+    launch_cell_q1_z<NS, P, SC, 2>(map, a, n_items, stream);
   else
-    launch_cell_q1_z<NS, P, AT, 1>(map, a, n_items, stream);
+    launch_cell_q1_z<NS, P, SC, 1>(map, a, n_items, stream);
+}
+
+// The schedule of a launch: a.atomic, else a.two_pass, else coloured.
+template <int NS, int P>
+void launch_cell_q1(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
+{
+  if (a.atomic)
+    launch_cell_q1_s<NS, P, SC_ATOMIC>(map, a, n_items, stream);
+  else if (a.two_pass)
+    launch_cell_q1_s<NS, P, SC_TWO_PASS>(map, a, n_items, stream);
+  else
+    launch_cell_q1_s<NS, P, SC_COLOURED>(map, a, n_items, stream);
 }
 
 } // namespace adm

@@ -53,6 +53,9 @@ Ensemble::Ensemble(adm_config const *cfgs, int n_members, int device, cudaStream
   za_.alloc(total);
   zb_.alloc(total);
   acc_.alloc(total);
+  // the two-pass schedule writes the accumulator at every node but the row
+  // padding, which the streaming update reads
+  ADM_CK(cudaMemset(acc_.p, 0, total * sizeof(double)));
   if (tab_.s > 1)
     s_.alloc(total);
   if (cfgs[0].time_method == 2)
@@ -198,6 +201,7 @@ void Ensemble::launch_step(double *solutions)
         ADM_CK(cudaGetLastError());
       }
       launch_two_pass_gather(deg_, a, n, stream_);
+      launch_stage_finalize(a, stride_, n, stream_);
       continue;
     }
     if (schedule_ == Thermal::kScheduleAtomic)

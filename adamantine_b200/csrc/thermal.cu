@@ -276,6 +276,36 @@ MaterialDesc make_material(adm_config const &cfg)
   return m;
 }
 
+// Neighbour-activity masks of every tile: bit (ox + 1) + 3 (oy + 1) + 9 (oz + 1)
+// is set when the tile at offset (ox, oy, oz) exists and is active (bit 13:
+// the tile itself). Inactive tiles get their neighbours' bits too (the
+// two-pass gather reads the mask of a node's owner tile, active or not).
+void neighbour_masks(Mesh const &mesh, std::vector<uint8_t> const &ta, std::vector<uint32_t> &nbr, bool &all_active)
+{
+  nbr.assign(mesh.n_tiles, 0u);
+  all_active = true;
+  for (int tz = 0; tz < mesh.nt[2]; ++tz)
+    for (int ty = 0; ty < mesh.nt[1]; ++ty)
+      for (int tx = 0; tx < mesh.nt[0]; ++tx)
+      {
+        size_t const tile = tx + (size_t)mesh.nt[0] * (ty + (size_t)mesh.nt[1] * tz);
+        if (!ta[tile])
+          all_active = false;
+        uint32_t mask = 0;
+        for (int oz = -1; oz <= 1; ++oz)
+          for (int oy = -1; oy <= 1; ++oy)
+            for (int ox = -1; ox <= 1; ++ox)
+            {
+              int const ax = tx + ox, ay = ty + oy, az = tz + oz;
+              if (ax < 0 || ay < 0 || az < 0 || ax >= mesh.nt[0] || ay >= mesh.nt[1] || az >= mesh.nt[2])
+                continue;
+              if (ta[ax + (size_t)mesh.nt[0] * (ay + (size_t)mesh.nt[1] * az)])
+                mask |= 1u << ((ox + 1) + 3 * (oy + 1) + 9 * (oz + 1));
+            }
+        nbr[tile] = mask;
+      }
+}
+
 CellTopology build_topology(Mesh const &mesh, std::vector<uint8_t> const &active,
                             std::vector<uint8_t> const &matid, bool need_slots,
                             std::vector<uint8_t> const *domain)
@@ -316,32 +346,7 @@ CellTopology build_topology(Mesh const &mesh, std::vector<uint8_t> const &active
           size_t const tile = (x / mesh.tx) + (size_t)mesh.nt[0] * ((y / mesh.ty) + (size_t)mesh.nt[1] * (z / mesh.tz));
           t.tile_active[tile] = 1;
         }
-  t.tile_nbr.assign(T, 0u);
-  t.all_tiles_active = true;
-  for (int tz = 0; tz < mesh.nt[2]; ++tz)
-    for (int ty = 0; ty < mesh.nt[1]; ++ty)
-      for (int tx = 0; tx < mesh.nt[0]; ++tx)
-      {
-        size_t const tile = tx + (size_t)mesh.nt[0] * (ty + (size_t)mesh.nt[1] * tz);
-        if (!t.tile_active[tile])
-        {
-          t.all_tiles_active = false;
-          continue;
-        }
-        uint32_t mask = 0;
-        for (int oz = -1; oz <= 1; ++oz)
-          for (int oy = -1; oy <= 1; ++oy)
-            for (int ox = -1; ox <= 1; ++ox)
-            {
-              int const ax = tx + ox, ay = ty + oy, az = tz + oz;
-              if (ax < 0 || ay < 0 || az < 0 || ax >= mesh.nt[0] || ay >= mesh.nt[1] || az >= mesh.nt[2])
-                continue;
-              size_t const nb = ax + (size_t)mesh.nt[0] * (ay + (size_t)mesh.nt[1] * az);
-              if (t.tile_active[nb])
-                mask |= 1u << ((ox + 1) + 3 * (oy + 1) + 9 * (oz + 1));
-            }
-        t.tile_nbr[tile] = mask;
-      }
+  neighbour_masks(mesh, t.tile_active, t.tile_nbr, t.all_tiles_active);
   if (need_slots)
   {
     t.face_slot.assign(C, -1);
@@ -574,6 +579,8 @@ void Thermal::rebuild()
   topo_ = build_topology(mesh_, active_, matid_, need_slots, domain_.empty() ? nullptr : &domain_);
   ADM_CK(cudaMemcpyAsync(cell_info_d_.p, topo_.cell_info.data(), C * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_));
   ADM_CK(cudaMemcpyAsync(tile_nbr_d_.p, topo_.tile_nbr.data(), mesh_.n_tiles * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_));
+  // the two-pass gather reads the halo arrays of inactive tiles as zeros
+  ADM_CK(cudaMemsetAsync(halo_d_.p, 0, halo_d_.n * sizeof(double), stream_));
   if (has_rotation_)
   {
     cos_d_.alloc(C);
@@ -868,7 +875,8 @@ void Thermal::launch_pass(KernelArgs a, double const *src)
   {
     // one launch over every tile (no atomics): each node's owner writes it,
     // the partial sums of nodes on a tile's upper faces go to its halo
-    // array, and the gather pass completes the shared nodes in a fixed order
+    // array, and the gather pass completes the shared nodes in a fixed
+    // order; a stage then applies the update over all nodes
     int const count = colour_off_[8];
     a.two_pass = 1;
     if (count > 0)
@@ -878,6 +886,8 @@ void Thermal::launch_pass(KernelArgs a, double const *src)
       ADM_CK(cudaGetLastError());
     }
     launch_two_pass_gather(mesh_.deg, a, 1, stream_);
+    if (a.mode == 2)
+      launch_stage_finalize(a, mesh_.n_nodes, 1, stream_);
     return;
   }
   if (schedule_ == kScheduleAtomic)
@@ -1403,30 +1413,7 @@ int64_t Thermal::activate_in_boxes(DeviceBoxes const &boxes, int64_t b0, int64_t
     int const x = c % mesh_.nc[0], y = (c / mesh_.nc[0]) % mesh_.nc[1], z = c / ((size_t)mesh_.nc[0] * mesh_.nc[1]);
     ta[(x / mesh_.tx) + (size_t)mesh_.nt[0] * ((y / mesh_.ty) + (size_t)mesh_.nt[1] * (z / mesh_.tz))] = 1;
   }
-  topo_.all_tiles_active = true;
-  for (int tz = 0; tz < mesh_.nt[2]; ++tz)
-    for (int ty = 0; ty < mesh_.nt[1]; ++ty)
-      for (int tx = 0; tx < mesh_.nt[0]; ++tx)
-      {
-        size_t const tile = tx + (size_t)mesh_.nt[0] * (ty + (size_t)mesh_.nt[1] * tz);
-        if (!ta[tile])
-        {
-          topo_.all_tiles_active = false;
-          continue;
-        }
-        uint32_t mask = 0;
-        for (int oz = -1; oz <= 1; ++oz)
-          for (int oy = -1; oy <= 1; ++oy)
-            for (int ox = -1; ox <= 1; ++ox)
-            {
-              int const ax = tx + ox, ay = ty + oy, az = tz + oz;
-              if (ax < 0 || ay < 0 || az < 0 || ax >= mesh_.nt[0] || ay >= mesh_.nt[1] || az >= mesh_.nt[2])
-                continue;
-              if (ta[ax + (size_t)mesh_.nt[0] * (ay + (size_t)mesh_.nt[1] * az)])
-                mask |= 1u << ((ox + 1) + 3 * (oy + 1) + 9 * (oz + 1));
-            }
-        topo_.tile_nbr[tile] = mask;
-      }
+  neighbour_masks(mesh_, ta, topo_.tile_nbr, topo_.all_tiles_active);
   work_.clear();
   for (int col = 0; col < 8; ++col)
   {
@@ -1450,6 +1437,7 @@ int64_t Thermal::activate_in_boxes(DeviceBoxes const &boxes, int64_t b0, int64_t
   ADM_CK(cudaMemcpyAsync(work_d_.p, work_.data(), work_.size() * sizeof(TileWork), cudaMemcpyHostToDevice, stream_));
   ADM_CK(cudaMemcpyAsync(tile_nbr_d_.p, topo_.tile_nbr.data(), mesh_.n_tiles * sizeof(uint32_t),
                          cudaMemcpyHostToDevice, stream_));
+  ADM_CK(cudaMemsetAsync(halo_d_.p, 0, halo_d_.n * sizeof(double), stream_));
   // add_material_end: the cell state goes back to the quadrature points
   get_state_from_material_properties();
   ADM_CK(cudaStreamSynchronize(stream_));

@@ -1,5 +1,5 @@
 // Instantiations of the FE_Q(1) cell kernel (one thread per cell), 1 material
-// state(s) and polynomial properties up to degree 2, in both launch
+// state(s) and polynomial properties up to degree 2, in the three launch
 // schedules; one translation unit per (degree, states, degree) so the build
 // runs in parallel.
 #include "cell_kernel_q1.cuh"
@@ -8,9 +8,6 @@ namespace adm
 {
 void launch_tile_d1_s1_p2(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
 {
-  if (a.atomic)
-    launch_cell_q1<1, 2, true>(map, a, n_items, stream);
-  else
-    launch_cell_q1<1, 2, false>(map, a, n_items, stream);
+  launch_cell_q1<1, 2>(map, a, n_items, stream);
 }
 } // namespace adm

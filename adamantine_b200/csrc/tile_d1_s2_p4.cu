@@ -1,5 +1,5 @@
 // Instantiations of the FE_Q(1) cell kernel (one thread per cell), 2 material
-// state(s) and polynomial properties up to degree 4, in both launch
+// state(s) and polynomial properties up to degree 4, in the three launch
 // schedules; one translation unit per (degree, states, degree) so the build
 // runs in parallel.
 #include "cell_kernel_q1.cuh"
@@ -8,9 +8,6 @@ namespace adm
 {
 void launch_tile_d1_s2_p4(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
 {
-  if (a.atomic)
-    launch_cell_q1<2, 4, true>(map, a, n_items, stream);
-  else
-    launch_cell_q1<2, 4, false>(map, a, n_items, stream);
+  launch_cell_q1<2, 4>(map, a, n_items, stream);
 }
 } // namespace adm

@@ -1,5 +1,5 @@
 // Instantiations of the fused tile kernel for FE degree 2, 2 material
-// state(s) and polynomial properties up to degree 2, in both launch
+// state(s) and polynomial properties up to degree 2, in the three launch
 // schedules; one translation unit per (degree, states, degree) so the build
 // runs in parallel.
 #include "tile_kernel.cuh"
@@ -8,9 +8,6 @@ namespace adm
 {
 void launch_tile_d2_s2_p2(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
 {
-  if (a.atomic)
-    launch_tile_t<2, 2, 2, true>(map, a, n_items, stream);
-  else
-    launch_tile_t<2, 2, 2, false>(map, a, n_items, stream);
+  launch_tile_t<2, 2, 2>(map, a, n_items, stream);
 }
 } // namespace adm

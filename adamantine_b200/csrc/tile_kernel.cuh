@@ -726,15 +726,8 @@ __device__ __noinline__ void face_terms(SmemPhys const &sp, MaterialDesc const *
 // (s0, s1, s2) (0 not shared, 1 shared with the lower neighbour tile, 2 with
 // the upper one), from the tile's neighbour-activity mask nbr and colour.
 // Coloured schedule: bit 1 first and bit 2 last toucher in colour order.
-// Two-pass schedule: 8 -- the node belongs to an upper neighbour tile (the
-// partial sum goes to this tile's halo array); 1 -- the node is this tile's:
-// its partial sum is stored here, and the gather pass adds the neighbours'
-// halo sums and applies the stage update (so the tile's write-out stores
-// only, with no loads to wait for).
-__device__ __forceinline__ int node_role(uint32_t nbr, int colour, int s0, int s1, int s2, bool two_pass)
+__device__ __forceinline__ int node_role(uint32_t nbr, int colour, int s0, int s1, int s2)
 {
-  if (two_pass)
-    return (s0 == 2 || s1 == 2 || s2 == 2) ? 8 : 1;
   int cmin = 8, cmax = -1;
 #pragma unroll
   for (int m = 0; m < 8; ++m)
@@ -756,40 +749,69 @@ __device__ __forceinline__ int node_role(uint32_t nbr, int colour, int s0, int s
 }
 
 // Two-pass schedule: the halo array of a tile holds one partial sum per node
-// on its upper brick faces (x = BX - 1, y = BY - 1 or z = BZ - 1, brick-local);
-// these nodes belong to the upper neighbours.
+// on its upper brick faces that an upper neighbour tile owns, in three full
+// faces: z (x = 0..BX-1, y = 0..BY-1), y (x, z) and x (y, z). A node shared
+// with the upper z neighbour sits in the z face, else one shared with the
+// upper y neighbour in the y face, else in the x face -- a rule both the
+// writing tile (from its sharing state) and the gather (from the offset of
+// the lower neighbour it reads) apply without looking at coordinates.
 template <int BX, int BY, int BZ>
 struct HaloLayout
 {
-  static constexpr int SIZE = BX * BY + BX * (BZ - 1) + (BY - 1) * (BZ - 1);
-  __host__ __device__ static int index(int X, int Y, int Z)
+  static constexpr int RZ = 0, RY = BX * BY, RX = BX * BY + BX * BZ;
+  static constexpr int SIZE = BX * BY + BX * BZ + BY * BZ;
+  // brick-local node (X, Y, Z), shared upward in z (uz), else y (uy), else x
+  __host__ __device__ static int index(bool uz, bool uy, int X, int Y, int Z)
   {
-    if (Z == BZ - 1)
-      return X + BX * Y;
-    if (Y == BY - 1)
-      return BX * BY + X + BX * Z;
-    return BX * BY + BX * (BZ - 1) + Y + (BY - 1) * Z; // X == BX - 1
+    return uz ? RZ + X + BX * Y : (uy ? RY + X + BX * Z : RX + Y + BY * Z);
   }
 };
 template <int DEG>
 using HaloOf = HaloLayout<TD<DEG>::BX, TD<DEG>::BY, TD<DEG>::BZ>;
 
-// Two-pass write-out of the nodes of a thread marked 8 (owned by an upper
-// neighbour): their partial sums into the tile's halo array; the mark is
-// cleared so write_nodes leaves them alone. XYZ[i] packs the node's
-// brick-local coordinates (X | Y << 8 | Z << 16).
-template <int DEG, int NV>
-__device__ __forceinline__ void send_halo(MemberData const &md, int tile, double const *res, int *rl,
-                                          int const *xyz)
+// Launch schedules of the tile kernels (template parameter SC).
+enum Schedule : int
 {
-  using HL = HaloOf<DEG>;
+  SC_COLOURED = 0,
+  SC_ATOMIC = 1,
+  SC_TWO_PASS = 2
+};
+
+// Two-pass role and halo slot of a node this thread writes, from its
+// brick-local coordinates and sharing state per direction (2: shared with
+// the upper neighbour tile, which owns it). Returns 8 (partial sum into the
+// halo array at *slot) or 4 (the tile's own node).
+template <class HL>
+__device__ __forceinline__ int two_pass_slot(int X, int Y, int Z, int sx, int sy, int sz, int *slot)
+{
+  if (sx != 2 && sy != 2 && sz != 2)
+    return 4;
+  *slot = HL::index(sz == 2, sy == 2, X, Y, Z);
+  return 8;
+}
+
+// Two-pass write-out (rl[i]: 4 own node, 8 halo node at slot[i], 0 none):
+// stores only (vmult mode 1 adds to dst). The owner's partial sum goes to
+// dst (vmult) or to the stage accumulator; the gather pass completes it.
+template <class HL, int NV>
+__device__ __forceinline__ void write_nodes_two_pass(KernelArgs const &args, MemberData const &md, int tile,
+                                                     double const *res, int const *rl, size_t const *gidx,
+                                                     int const *slot)
+{
+  double *const tgt = args.mode == 2 ? md.acc : args.vdst;
+  double *const halo = md.halo + (size_t)tile * HL::SIZE;
+  double old[NV];
 #pragma unroll
   for (int i = 0; i < NV; ++i)
-    if ((rl[i] & 12) == 12)
-    {
-      md.halo[(size_t)tile * HL::SIZE + HL::index(xyz[i] & 255, (xyz[i] >> 8) & 255, xyz[i] >> 16)] = res[i];
-      rl[i] = 0;
-    }
+    old[i] = (args.mode == 1 && rl[i] == 4) ? tgt[gidx[i]] : 0.0;
+#pragma unroll
+  for (int i = 0; i < NV; ++i)
+  {
+    if (rl[i] == 8)
+      halo[slot[i]] = res[i];
+    else if (rl[i] == 4)
+      tgt[gidx[i]] = old[i] + res[i];
+  }
 }
 
 // Write-out of the node sums res[i] of one thread (rl[i]: bit 4 the thread
@@ -914,7 +936,7 @@ __device__ __forceinline__ void load_member_constants(SmemPhys &sp, MemberData c
 // other buffer while the current item is computed.
 // FC: the problem has convective / radiative faces (instantiated apart so
 // that adiabatic problems carry no face code).
-template <int DEG, int NS, int P, bool AT, bool FC>
+template <int DEG, int NS, int P, int SC, bool FC>
 __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
     tile_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ KernelArgs args, int n_items)
 {
@@ -1049,12 +1071,12 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
       if (tid == 0)
         sp.member = w.member;
     }
-    if (!AT && tid < 27)
+    if (SC == SC_COLOURED && tid < 27)
     {
       // the role of the node class (tid % 3, tid / 3 % 3, tid / 9): sharing
       // state per direction, 0 not shared, 1 with the lower neighbour tile,
       // 2 with the upper one
-      sp.role[buf][tid] = node_role(md.tile_nbr[tile], colour, tid % 3, (tid / 3) % 3, tid / 9, args.two_pass != 0);
+      sp.role[buf][tid] = node_role(md.tile_nbr[tile], colour, tid % 3, (tid / 3) % 3, tid / 9);
     }
     if (slab == 0)
       changed[cl] = 0;
@@ -1432,7 +1454,7 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
     int const Z = DEG * lz + slab;
     int const gz = nz0 + Z;
     int const sz = (Z == 0 && tiz > 0) ? 1 : ((Z == DEG * TZ && tiz < args.nt[2] - 1) ? 2 : 0);
-    int rl[NQS], xyz[NQS];
+    int rl[NQS], slot[NQS];
     size_t gidx[NQS];
 #pragma unroll
     for (int i = 0; i < NQS; ++i)
@@ -1444,16 +1466,20 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
       bool const inside = gx < args.nn[0] && gy < nn1 && gz < args.nn[2];
       int const sx = (X == 0 && tix > 0) ? 1 : ((X == DEG * TX && tix < nt0 - 1) ? 2 : 0);
       int const sy = (Y == 0 && tiy > 0) ? 1 : ((Y == DEG * TY && tiy < nt1 - 1) ? 2 : 0);
-      rl[i] = (own && inside) ? (AT ? 4 : (sp.role[buf][sx + 3 * sy + 9 * sz] | 4)) : 0;
+      slot[i] = 0;
+      if constexpr (SC == SC_TWO_PASS)
+        rl[i] = (own && inside) ? two_pass_slot<HaloOf<DEG>>(X, Y, Z, sx, sy, sz, &slot[i]) : 0;
+      else
+        rl[i] = (own && inside) ? (SC == SC_ATOMIC ? 4 : (sp.role[buf][sx + 3 * sy + 9 * sz] | 4)) : 0;
       gidx[i] = gx + (size_t)pitch * (gy + (size_t)nn1 * gz);
-      xyz[i] = X | (Y << 8) | (Z << 16);
     }
-    if (!AT && args.two_pass)
-      send_halo<DEG, NQS>(md, tile, res, rl, xyz);
-    write_nodes<AT, NQS>(args, md, y, res, rl, gidx);
+    if constexpr (SC == SC_TWO_PASS)
+      write_nodes_two_pass<HaloOf<DEG>, NQS>(args, md, tile, res, rl, gidx, slot);
+    else
+      write_nodes<SC == SC_ATOMIC, NQS>(args, md, y, res, rl, gidx);
     // vmult writes zeros into the row padding of the node layout (the
     // two-pass gather does that itself)
-    if (!AT && !args.two_pass && args.mode == 0 && tix == nt0 - 1 && pitch > args.nn[0])
+    if (SC == SC_COLOURED && args.mode == 0 && tix == nt0 - 1 && pitch > args.nn[0])
     {
       int const npad = pitch - args.nn[0];
       for (int i = tid; i < npad * BY * BZ; i += NT)
@@ -1470,144 +1496,235 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
 
 // Launches the persistent tile kernel over n_items work items with at most
 // the number of CTAs that are resident at once on the device.
-template <int DEG, int NS, int P, bool AT, bool FC>
+template <int DEG, int NS, int P, int SC, bool FC>
 void launch_tile_f(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
 {
   static int grid_cap = 0;
   if (grid_cap == 0)
   {
-    cudaFuncSetAttribute(tile_kernel<DEG, NS, P, AT, FC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(tile_kernel<DEG, NS, P, SC, FC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)TD<DEG>::SMEM);
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_kernel<DEG, NS, P, AT, FC>, TD<DEG>::NT,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_kernel<DEG, NS, P, SC, FC>, TD<DEG>::NT,
                                                   TD<DEG>::SMEM);
     grid_cap = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
   }
   int const grid = n_items < grid_cap ? n_items : grid_cap;
-  tile_kernel<DEG, NS, P, AT, FC><<<grid, TD<DEG>::NT, TD<DEG>::SMEM, stream>>>(map, a, n_items);
+  tile_kernel<DEG, NS, P, SC, FC><<<grid, TD<DEG>::NT, TD<DEG>::SMEM, stream>>>(map, a, n_items);
 }
 
-template <int DEG, int NS, int P, bool AT>
-void launch_tile_t(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
+template <int DEG, int NS, int P, int SC>
+void launch_tile_s(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
 {
   if (a.faces)
-    launch_tile_f<DEG, NS, P, AT, true>(map, a, n_items, stream);
+    launch_tile_f<DEG, NS, P, SC, true>(map, a, n_items, stream);
   else
-    launch_tile_f<DEG, NS, P, AT, false>(map, a, n_items, stream);
+    launch_tile_f<DEG, NS, P, SC, false>(map, a, n_items, stream);
+}
+
+// The schedule of a launch: a.atomic, else a.two_pass, else coloured.
+template <int DEG, int NS, int P>
+void launch_tile_t(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
+{
+  if (a.atomic)
+    launch_tile_s<DEG, NS, P, SC_ATOMIC>(map, a, n_items, stream);
+  else if (a.two_pass)
+    launch_tile_s<DEG, NS, P, SC_TWO_PASS>(map, a, n_items, stream);
+  else
+    launch_tile_s<DEG, NS, P, SC_COLOURED>(map, a, n_items, stream);
 }
 
 } // namespace adm
 
 namespace adm
 {
-// Two-pass schedule, second pass, over every node of the padded layout of
-// every member (blockIdx.y). A node belongs to the tile whose half-open node
-// range holds it (the last tile per direction takes the upper end too). Its
-// sum is the owner's partial sum (when the owner is active) plus, in a fixed
-// order, the halo partial sums of the active lower neighbour tiles that
-// touch it -- no atomics, bit-reproducible. vmult: the owner's sum is in dst
-// already, the halo sums are added (nodes no active tile touches and the
-// row padding get zero); a stage: the inverse lumped mass and the
-// Runge-Kutta update for every node an active tile touches.
+// Two-pass schedule, second pass: one CTA per (tile, member) over the nodes
+// the tile owns -- its half-open node box, the last tile per direction
+// taking the upper end too. A node's sum is the owner's partial sum (when
+// the owner is active) plus, in a fixed order, the halo partial sums of the
+// lower neighbour tiles that touch it -- no atomics, bit-reproducible. The
+// halo arrays of inactive tiles hold zeros (cleared whenever the active set
+// changes), so a halo load waits for nothing but the node's position; the
+// neighbour mask only decides what is written. An active owner has written
+// all its nodes (dst for a vmult, the stage accumulator for a stage), so only
+// the nodes on the box's lower faces are visited; an inactive owner's whole
+// box is written (its nodes that no active tile touches get zero, except in
+// a vmult that adds to dst). A stage then runs the streaming update over all
+// nodes (stage_finalize_kernel), as the atomic schedule does.
 template <int DEG>
-__device__ __forceinline__ void two_pass_gather_node(KernelArgs const &a, MemberData const &md, int gx, int gy,
-                                                     int gz, size_t g)
+__device__ __forceinline__ void two_pass_gather_node(double *tgt, uint32_t w, bool keep, bool fill, bool const *lower,
+                                                     double const *hbase, size_t const *hstride, size_t g, int X,
+                                                     int Y, int Z)
 {
-  using T_ = TD<DEG>;
   using HL = HaloOf<DEG>;
-  constexpr int SX = DEG * T_::TX, SY = DEG * T_::TY, SZ = DEG * T_::TZ;
-  bool const vm = a.mode != 2;
-  if (gx >= a.nn[0])
-  {
-    if (a.mode == 0)
-      a.vdst[g] = 0.0;
-    return;
-  }
-  int const tx = min(gx / SX, a.nt[0] - 1), ty = min(gy / SY, a.nt[1] - 1), tz = min(gz / SZ, a.nt[2] - 1);
-  int const X = gx - SX * tx, Y = gy - SY * ty, Z = gz - SZ * tz;
-  bool const fx = X == 0 && tx > 0, fy = Y == 0 && ty > 0, fz = Z == 0 && tz > 0;
-  size_t const owner = tx + (size_t)a.nt[0] * (ty + (size_t)a.nt[1] * tz);
-  bool const owner_active = (md.tile_nbr[owner] >> 13) & 1u;
+  constexpr int SX = DEG * TD<DEG>::TX, SY = DEG * TD<DEG>::TY;
+  constexpr int BX = TD<DEG>::BX, BY = TD<DEG>::BY;
+  bool const fx = lower[0] && X == 0, fy = lower[1] && Y == 0, fz = lower[2] && Z == 0;
   double h = 0.0;
   bool any = false;
 #pragma unroll
   for (int m = 1; m < 8; ++m)
   {
     int const dx = m & 1, dy = (m >> 1) & 1, dz = m >> 2;
-    if ((dx && !fx) || (dy && !fy) || (dz && !fz))
-      continue;
-    size_t const c = owner - (size_t)dx - (size_t)a.nt[0] * ((size_t)dy + (size_t)a.nt[1] * (size_t)dz);
-    if (!((md.tile_nbr[c] >> 13) & 1u))
-      continue;
-    h += md.halo[c * HL::SIZE + HL::index(X + dx * SX, Y + dy * SY, Z + dz * SZ)];
-    any = true;
+    if ((!dx || fx) && (!dy || fy) && (!dz || fz))
+    {
+      // the node in the lower neighbour at -(dx, dy, dz) and its halo slot
+      // (shared upward in z if dz, else in y if dy, else in x)
+      int const slot = dz ? HL::RZ + (X + dx * SX) + BX * (Y + dy * SY)
+                          : (dy ? HL::RY + (X + dx * SX) + BX * Z : HL::RX + Y + BY * Z);
+      double const *const hp = hbase - (dx ? hstride[0] : 0) - (dy ? hstride[1] : 0) - (dz ? hstride[2] : 0);
+      h += hp[slot];
+      // its activity: bit (1 - dx) + 3 (1 - dy) + 9 (1 - dz) of the owner's mask
+      any = any || ((w >> ((1 - dx) + 3 * (1 - dy) + 9 * (1 - dz))) & 1u);
+    }
   }
-  if (vm && !any)
+  double const b = (keep && (fx || fy || fz)) ? tgt[g] : 0.0;
+  if (any || fill)
+    tgt[g] = b + h;
+}
+
+// Grid: x over the tiles, y over the members; 128 threads.
+template <int DEG>
+__global__ void __launch_bounds__(128) two_pass_gather_kernel(KernelArgs a)
+{
+  constexpr int SX = DEG * TD<DEG>::TX, SY = DEG * TD<DEG>::TY, SZ = DEG * TD<DEG>::TZ;
+  constexpr int NT = 128;
+  MemberData const &md = a.members[blockIdx.y];
+  int const nt0 = a.nt[0], nt1 = a.nt[1];
+  size_t const owner = blockIdx.x;
+  int const tx = (int)(owner % (size_t)nt0);
+  int const ty = (int)((owner / (size_t)nt0) % (size_t)nt1);
+  int const tz = (int)(owner / ((size_t)nt0 * (size_t)nt1));
+  uint32_t const w = md.tile_nbr[owner];
+  bool const owner_active = (w >> 13) & 1u;
+  // the owner's node box, which lower neighbours exist, the owner's halo
+  // array and the distances to its lower neighbours' arrays, its first node
+  int const ex = tx == nt0 - 1 ? a.nn[0] - SX * tx : SX;
+  int const ey = ty == nt1 - 1 ? a.nn[1] - SY * ty : SY;
+  int const ez = tz == a.nt[2] - 1 ? a.nn[2] - SZ * tz : SZ;
+  bool const lower[3] = {tx > 0, ty > 0, tz > 0};
+  constexpr size_t HS = HaloOf<DEG>::SIZE;
+  size_t const hstride[3] = {HS, HS * nt0, HS * nt0 * nt1};
+  double const *const hbase = md.halo + owner * HS;
+  size_t const pitch = (size_t)a.pitch, plane = (size_t)a.pitch * (size_t)a.nn[1];
+  size_t const rbase0 = (size_t)SX * tx + pitch * (size_t)(SY * ty) + plane * (size_t)(SZ * tz);
+  double *const tgt = a.mode == 2 ? md.acc : a.vdst;
+  // the target keeps its value where the owner wrote it, or where a vmult adds
+  bool const keep = owner_active || a.mode == 1;
+  if (owner_active)
   {
-    // complete in its owner's tile, or touched by no active tile
-    if (!owner_active && a.mode == 0)
-      a.vdst[g] = 0.0;
-    return;
-  }
-  if (!any && !owner_active)
-    return; // no active tile touches it: not a degree of freedom
-  if (vm)
-  {
-    // the owner's partial sum (or, mode 1, the caller's value plus it) is in
-    // dst already
-    if (owner_active || a.mode == 1)
-      a.vdst[g] += h;
-    else
-      a.vdst[g] = h;
-    return;
-  }
-  double *const y = a.y_override ? a.y_override : md.y;
-  double const total = (owner_active ? md.acc[g] : 0.0) + h;
-  double const dt = md.clock[1];
-  double const f = md.inv_mass[g] * total;
-  if (!isfinite(f))
-    atomicCAS(md.error, 0, (int)DERR_NONFINITE);
-  double const yv = y[g];
-  if (a.n_stages == 1)
-  {
-    y[g] = yv + dt * f;
-    return;
-  }
-  double const sv = a.stage > 0 ? md.s[g] : 0.0;
-  if (!a.last)
-  {
-    double zn = yv;
-    if (a.has_f0)
-      zn = zn + (dt * a.a_next_f0) * md.f0[g];
-    zn = zn + (dt * a.a_next) * f;
-    (a.dst_sel == 1 ? md.za : md.zb)[g] = zn;
-    double const sb = (dt * a.b_i) * f;
-    md.s[g] = a.stage == 0 ? sb : sv + sb;
-    if (a.store_f0)
-      md.f0[g] = f;
+    // the nodes on the lower faces: first those that only one lower
+    // neighbour touches (inside the z = 0, y = 0 and x = 0 faces: one halo
+    // load each), then the edges and the corner where faces meet
+    int const x0 = lower[0] ? 1 : 0, y0 = lower[1] ? 1 : 0, z0 = lower[2] ? 1 : 0;
+    int const wx = ex - x0, wy = ey - y0, wz = ez - z0;
+    int const nZ = lower[2] ? wx * wy : 0, nY = lower[1] ? wx * wz : 0, nX = lower[0] ? wy * wz : 0;
+    int const eXY = lower[0] && lower[1] ? wz : 0, eYZ = lower[1] && lower[2] ? wx : 0;
+    int const eXZ = lower[0] && lower[2] ? wy : 0, eC = lower[0] && lower[1] && lower[2] ? 1 : 0;
+    int const n1 = nZ + nY + nX, n = n1 + eXY + eYZ + eXZ + eC;
+    constexpr int BX = TD<DEG>::BX, BY = TD<DEG>::BY;
+    using HL = HaloOf<DEG>;
+    for (int k = threadIdx.x; k < n; k += NT)
+    {
+      if (k < n1)
+      {
+        int X, Y, Z, slot;
+        double const *hp;
+        uint32_t bit;
+        if (k < nZ)
+        {
+          int const r = k / wx;
+          X = x0 + (k - r * wx);
+          Y = y0 + r;
+          Z = 0;
+          slot = HL::RZ + X + BX * Y;
+          hp = hbase - hstride[2];
+          bit = 1u << (1 + 3 * 1 + 9 * 0);
+        }
+        else if (k < nZ + nY)
+        {
+          int const j = k - nZ, r = j / wx;
+          X = x0 + (j - r * wx);
+          Y = 0;
+          Z = z0 + r;
+          slot = HL::RY + X + BX * Z;
+          hp = hbase - hstride[1];
+          bit = 1u << (1 + 3 * 0 + 9 * 1);
+        }
+        else
+        {
+          int const j = k - nZ - nY, r = j / wy;
+          X = 0;
+          Y = y0 + (j - r * wy);
+          Z = z0 + r;
+          slot = HL::RX + Y + BY * Z;
+          hp = hbase - hstride[0];
+          bit = 1u << (0 + 3 * 1 + 9 * 1);
+        }
+        size_t const g = rbase0 + X + pitch * Y + plane * Z;
+        double const h = hp[slot];
+        double const b = tgt[g];
+        if (w & bit)
+          tgt[g] = b + h;
+      }
+      else
+      {
+        // edges: X = Y = 0 (along z), Y = Z = 0 (along x), X = Z = 0
+        // (along y), then the corner
+        int const j = k - n1;
+        int X, Y, Z;
+        if (j < eXY)
+        {
+          X = 0;
+          Y = 0;
+          Z = z0 + j;
+        }
+        else if (j < eXY + eYZ)
+        {
+          X = x0 + (j - eXY);
+          Y = 0;
+          Z = 0;
+        }
+        else if (j < eXY + eYZ + eXZ)
+        {
+          X = 0;
+          Y = y0 + (j - eXY - eYZ);
+          Z = 0;
+        }
+        else
+        {
+          X = 0;
+          Y = 0;
+          Z = 0;
+        }
+        two_pass_gather_node<DEG>(tgt, w, keep, false, lower, hbase, hstride, rbase0 + X + pitch * Y + plane * Z, X,
+                                  Y, Z);
+      }
+    }
   }
   else
   {
-    y[g] = yv + (sv + (dt * a.b_i) * f);
+    // the whole box: no active owner wrote it
+    bool const fill = a.mode != 1;
+    int const exy = ex * ey;
+    for (int k = threadIdx.x; k < exy * ez; k += NT)
+    {
+      int const Z = k / exy, r = k - Z * exy, Y = r / ex, X = r - Y * ex;
+      two_pass_gather_node<DEG>(tgt, w, keep, fill, lower, hbase, hstride, rbase0 + X + pitch * Y + plane * Z, X,
+                                Y, Z);
+    }
   }
-}
-
-// Grid: x over the padded row (pitch), y strided over the node rows
-// (nn[1] * nn[2] of them), z over the members; no 64-bit divisions.
-template <int DEG>
-__global__ void two_pass_gather_kernel(KernelArgs a)
-{
-  int const gx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gx >= a.pitch)
-    return;
-  MemberData const &md = a.members[blockIdx.z];
-  int const nn1 = a.nn[1], rows = nn1 * a.nn[2];
-  for (int r = blockIdx.y; r < rows; r += gridDim.y)
+  // vmult writes zeros into the row padding of the node layout
+  if (a.mode == 0 && tx == nt0 - 1 && a.pitch > a.nn[0])
   {
-    int const gz = r / nn1, gy = r - gz * nn1;
-    two_pass_gather_node<DEG>(a, md, gx, gy, gz, gx + (size_t)a.pitch * (size_t)r);
+    int const npad = a.pitch - a.nn[0];
+    for (int i = threadIdx.x; i < npad * ey * ez; i += NT)
+    {
+      int const row = i / npad, Z = row / ey, Y = row - Z * ey;
+      a.vdst[rbase0 + ex + (i - row * npad) + pitch * Y + plane * Z] = 0.0;
+    }
   }
 }
 } // namespace adm

@@ -7,12 +7,8 @@ namespace adm
 {
 void launch_two_pass_gather(int deg, KernelArgs const &a, int n_members, cudaStream_t stream)
 {
-  // 128 threads per block along a row; enough rows per launch to fill the
-  // device several times over, each block looping over the rest
-  int const rows = a.nn[1] * a.nn[2];
-  int const bx = (a.pitch + 127) / 128;
-  int const by = rows < 4096 / bx + 1 ? rows : 4096 / bx + 1;
-  dim3 const grid((unsigned)bx, (unsigned)(by < 65535 ? by : 65535), (unsigned)n_members);
+  // one CTA per (tile, member)
+  dim3 const grid((unsigned)(a.nt[0] * a.nt[1] * a.nt[2]), (unsigned)n_members);
   if (deg == 1)
     two_pass_gather_kernel<1><<<grid, 128, 0, stream>>>(a);
   else

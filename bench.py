@@ -52,7 +52,7 @@ TRAFFIC_NOTE = {"atomic": "ncu, one launch per vmult",
 # per schedule: the kernels of one vmult, their launch pattern and count
 KERNELS = {"coloured": ("adm::tile_kernel<2,3,2,0,0>", "8 colour launches", 8),
            "atomic": ("adm::tile_kernel<2,3,2,1,0>", "1 launch", 1),
-           "two_pass": ("adm::tile_kernel<2,3,2,0,0> (two-pass write-out) + adm::two_pass_gather_kernel<2>",
+           "two_pass": ("adm::tile_kernel<2,3,2,2,0> + adm::two_pass_gather_kernel<2>",
                         "1 tile launch + 1 gather launch", 2)}
 
 
