@@ -300,9 +300,11 @@ __device__ __forceinline__ void q1_cell(SmemPhys const &sp, MemberData const &md
           res[e + 4 * lev] += fo[e];
       }
     }
-    // state write-back: the liquid sum and, when a point of a uniform
-    // powder cell changed, the switch to per-point storage
-    if (NS > 1)
+    // state write-back: the liquid sum (read only by the state queries,
+    // which see the last evaluation: written by a vmult and by a step's
+    // last stage) and, when a point of a uniform powder cell changed, the
+    // switch to per-point storage
+    if (NS > 1 && (args.mode != 2 || args.last))
       md.liquid_sum[c] = liq;
     if (NS == 3 && pmode != 2 && cmask)
     {
@@ -427,8 +429,10 @@ __global__ void __launch_bounds__(Q1Cell<CZ>::NT, Q1Cell<CZ>::MINB)
         nx_info[j] = mk.cell_info[kc];
         if (NS == 3)
         {
+          // the uniform powder ratio matters only in mode 1
           nx_pmode[j] = mk.powder_mode[kc];
-          nx_pu[j] = mk.powder_cell[kc];
+          if (nx_pmode[j] == 1)
+            nx_pu[j] = mk.powder_cell[kc];
         }
       }
     }

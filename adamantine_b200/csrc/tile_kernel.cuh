@@ -1026,8 +1026,10 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
       nx_info = mk.cell_info[kc];
       if (NS == 3)
       {
+        // the uniform powder ratio matters only in mode 1
         nx_pmode = mk.powder_mode[kc];
-        nx_pu = mk.powder_cell[kc];
+        if (nx_pmode == 1)
+          nx_pu = mk.powder_cell[kc];
       }
     }
   };
@@ -1424,10 +1426,12 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
         res[i] += mbuf[i * NCELL + cl + TX * TY];
     }
 
-    // ---- state write-back
+    // ---- state write-back (the liquid sum is read only by the state
+    // queries, which see the last evaluation: written by a vmult and by a
+    // step's last stage)
     if (slab == 0 && active)
     {
-      if (NS > 1)
+      if (NS > 1 && (args.mode != 2 || args.last))
       {
         double l = 0.0;
         for (int s = 0; s < N; ++s)
