@@ -641,6 +641,289 @@ void launch_cell_q1_f(CUtensorMap const &map, KernelArgs const &a, int n_items, 
   cell_kernel_q1<NS, P, SC, FC, CZ><<<grid, Q::NT, Q::SMEM, stream>>>(map, a, n_items);
 }
 
+// ------------------------------------------------------------ column variant
+// One warp per CTA and per tile: thread (lx, ly) walks its column of TZ
+// cells bottom to top, carrying the node level two cells share in
+// registers; a node level is complete when the cell above it is done, and
+// it is merged across the warp with shuffles and written out then. The
+// warp's tiles need no CTA barrier (a warp vote before the first write and
+// __syncwarp for the shared state), so a warp whose tile is slow (cells in
+// the mushy range, the source) holds up no other warp; cell data are
+// prefetched one cell ahead.
+struct Q1Col
+{
+  static constexpr int TX = 8, TY = 4, TZ = 4;
+  static constexpr int NT = TX * TY; // one warp
+  static constexpr int MINB = 12;    // resident CTAs (warps) per SM the register budget targets
+  static constexpr int BRICKP = Q1Cell<1>::BRICKP;
+  static constexpr int NBUF = 3;
+  static constexpr size_t SMEM = sizeof(double) * NBUF * BRICKP;
+  static_assert(TX == TD<1>::TX && TY == TD<1>::TY && TZ == TD<1>::TZ,
+                "the Q1 column kernel uses the tiles of the Q1 tile kernel");
+};
+
+template <int NS, int P, int SC, bool FC>
+__global__ void __launch_bounds__(Q1Col::NT, Q1Col::MINB)
+    cell_kernel_q1_col(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ KernelArgs args,
+                       int n_items)
+{
+  using Q = Q1Col;
+  constexpr int TX = Q::TX, TY = Q::TY, TZ = Q::TZ, NT = Q::NT, NBUF = Q::NBUF;
+  constexpr int BXP = Q1Cell<1>::BXP, BY = Q1Cell<1>::BY, BZ = Q1Cell<1>::BZ;
+  constexpr unsigned kBoxBytes = sizeof(double) * BXP * BY * BZ;
+  unsigned const full = 0xffffffffu;
+  extern __shared__ __align__(128) double smem[];
+  __shared__ SmemPhys sp;
+  __shared__ __align__(8) uint64_t bars[NBUF];
+
+  int const lane = threadIdx.x;
+  int const lx = lane % TX, ly = lane / TX;
+  int const nt0 = args.nt[0], nt1 = args.nt[1];
+  int const pitch = args.pitch, nn1 = args.nn[1];
+
+  auto issue = [&](int b, int item) {
+    TileWork const wi = args.work[item];
+    int const tix = wi.xyz & 2047u, tiy = (wi.xyz >> 11) & 2047u, tiz = wi.xyz >> 22;
+    mbar_arrive_expect_tx(&bars[b], kBoxBytes);
+    tma_load_brick(smem + b * Q::BRICKP, &tmap, TX * tix, TY * tiy, TZ * tiz, wi.member, &bars[b]);
+  };
+  // the cell data of cell (lx, ly, kz) of item `item` (zeros outside the mesh)
+  auto load_cell = [&](int item, int kz, uint32_t &info, int &pmode, double &pu) {
+    TileWork const wk = args.work[item];
+    MemberData const &mk = args.members[wk.member];
+    int const kx = TX * (int)(wk.xyz & 2047u) + lx, ky = TY * (int)((wk.xyz >> 11) & 2047u) + ly;
+    int const kzz = TZ * (int)(wk.xyz >> 22) + kz;
+    info = 0u;
+    pmode = 0;
+    pu = 0.0;
+    if (kx < args.nc[0] && ky < args.nc[1] && kzz < args.nc[2])
+    {
+      size_t const kc = kx + (size_t)args.nc[0] * (ky + (size_t)args.nc[1] * kzz);
+      info = mk.cell_info[kc];
+      if (NS == 3)
+      {
+        pmode = mk.powder_mode[kc];
+        if (pmode == 1)
+          pu = mk.powder_cell[kc];
+      }
+    }
+  };
+
+  // work distribution as in cell_kernel_q1 (dynamic with args.claim, else
+  // strided or blocked)
+  bool const dyn = args.claim != nullptr && !args.blocked;
+  __shared__ int claimed[2];
+  int first, last, step;
+  if (dyn || !args.blocked)
+  {
+    first = blockIdx.x;
+    last = n_items;
+    step = gridDim.x;
+  }
+  else
+  {
+    int const per = (n_items + (int)gridDim.x - 1) / (int)gridDim.x;
+    first = (int)blockIdx.x * per;
+    last = min(first + per, n_items);
+    step = 1;
+  }
+  int second = first + step;
+  if (lane == 0)
+  {
+#pragma unroll
+    for (int b = 0; b < NBUF; ++b)
+      mbar_init(&bars[b], 1);
+    fence_mbar_init();
+    sp.member = -1;
+    if (dyn)
+    {
+      second = first < last ? atomicAdd(args.claim, 1) + (int)gridDim.x : last;
+      claimed[1] = second;
+    }
+    if (first < last)
+      issue(0, first);
+    if (second < last)
+      issue(1, second);
+  }
+  __syncwarp();
+  second = __shfl_sync(full, second, 0);
+
+  // cell data of the next cell to compute, one cell ahead
+  uint32_t nx_info = 0u;
+  int nx_pmode = 0;
+  double nx_pu = 0.0;
+  if (first < last)
+    load_cell(first, 0, nx_info, nx_pmode, nx_pu);
+
+  int it = 0, buf = 0;
+  unsigned phase = 0;
+  for (int item = first; item < last; ++it)
+  {
+    double const *brick = smem + buf * Q::BRICKP;
+    int const next = dyn ? claimed[(it + 1) & 1] : item + step;
+    int next2 = next + step;
+    if (dyn && lane == 0)
+    {
+      next2 = next < last ? atomicAdd(args.claim, 1) + (int)gridDim.x : last;
+      claimed[it & 1] = next2;
+    }
+    next2 = __shfl_sync(full, next2, 0);
+    TileWork const w = args.work[item];
+    MemberData const &md = args.members[w.member];
+    int const tile = w.tile;
+    int const tix = w.xyz & 2047u, tiy = (w.xyz >> 11) & 2047u, tiz = w.xyz >> 22;
+    int const colour = (tix & 1) | ((tiy & 1) << 1) | ((tiz & 1) << 2);
+    int const ncx0 = TX * tix, ncy0 = TY * tiy, ncz0 = TZ * tiz;
+    double *const y = args.y_override ? args.y_override : md.y;
+    if (sp.member != w.member)
+    {
+      __syncwarp();
+      load_member_constants<NT>(sp, md, lane);
+      __syncwarp();
+      if (lane == 0)
+        sp.member = w.member;
+    }
+    if (SC == SC_COLOURED && lane < 27)
+      sp.role[it & 1][lane] = node_role(md.tile_nbr[tile], colour, lane % 3, (lane / 3) % 3, lane / 9);
+    bool const do_src =
+        tile_meets_source<TX, TY, TZ>(args, sp.beams, sp.n_beams, tix, tiy, tiz);
+    // wait for this item's brick (bounded); if any lane's wait gave up the
+    // warp leaves before anything is written
+    bool const arrived = mbar_wait(&bars[buf], phase);
+    if (__any_sync(full, !arrived))
+    {
+      if (lane == 0)
+      {
+        atomicCAS(md.error, 0, (int)DERR_TMA_TIMEOUT);
+        mbar_wait(&bars[buf], phase);
+        if (next < last)
+          mbar_wait(&bars[buf == NBUF - 1 ? 0 : buf + 1], buf == NBUF - 1 ? phase ^ 1u : phase);
+      }
+      return;
+    }
+    __syncwarp(); // the roles and member constants are visible to the warp
+    // every lane has finished the previous item: its buffer takes the
+    // next-but-one brick
+    if (lane == 0 && next2 < last)
+    {
+      fence_proxy_async();
+      issue(buf == 0 ? NBUF - 1 : buf - 1, next2);
+    }
+
+    double carry[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 1
+    for (int k = 0; k <= TZ; ++k)
+    {
+      double lev[4];
+      if (k < TZ)
+      {
+        uint32_t const info = nx_info;
+        int const pmode = nx_pmode;
+        double const pu = nx_pu;
+        // prefetch the cell above (or the next item's first cell)
+        if (k + 1 < TZ)
+          load_cell(item, k + 1, nx_info, nx_pmode, nx_pu);
+        else if (next < last)
+          load_cell(next, 0, nx_info, nx_pmode, nx_pu);
+        double cres[8];
+        q1_cell<NS, P, FC>(sp, md, args, brick, lx, ly, k, ncx0, ncy0, ncz0, info, pmode, pu, true, do_src,
+                           cres);
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+        {
+          lev[e] = carry[e] + cres[e];
+          carry[e] = cres[e + 4];
+        }
+      }
+      else
+      {
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          lev[e] = carry[e];
+      }
+      // node level k: x then y neighbours' shares to the lower cell
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+      {
+        double const v = __shfl_down_sync(full, lev[2 * j], 1);
+        if (lx < TX - 1)
+          lev[1 + 2 * j] += v;
+      }
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+      {
+        double const v = __shfl_down_sync(full, lev[i], TX);
+        if (ly < TY - 1)
+          lev[i + 2] += v;
+      }
+      // write-out of the level's nodes this thread owns
+      int rl[4], slot[4];
+      size_t gidx[4];
+      int const Z = k, gzn = ncz0 + Z;
+      int const sz = (Z == 0 && tiz > 0) ? 1 : ((Z == TZ && tiz < args.nt[2] - 1) ? 2 : 0);
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+      {
+        int const a = e & 1, b = e >> 1;
+        int const X = lx + a, Y = ly + b;
+        int const gx = ncx0 + X, gy = ncy0 + Y;
+        bool const own = (a > 0 || lx == 0) && (b > 0 || ly == 0);
+        bool const inside = gx < args.nn[0] && gy < nn1 && gzn < args.nn[2];
+        int const sx = (X == 0 && tix > 0) ? 1 : ((X == TX && tix < nt0 - 1) ? 2 : 0);
+        int const sy = (Y == 0 && tiy > 0) ? 1 : ((Y == TY && tiy < nt1 - 1) ? 2 : 0);
+        slot[e] = 0;
+        if constexpr (SC == SC_TWO_PASS)
+          rl[e] = (own && inside) ? two_pass_slot<HaloOf<1>>(X, Y, Z, sx, sy, sz, &slot[e]) : 0;
+        else
+          rl[e] = (own && inside) ? (SC == SC_ATOMIC ? 4 : (sp.role[it & 1][sx + 3 * sy + 9 * sz] | 4)) : 0;
+        gidx[e] = gx + (size_t)pitch * (gy + (size_t)nn1 * gzn);
+      }
+      if constexpr (SC == SC_TWO_PASS)
+        write_nodes_two_pass<HaloOf<1>, 4>(args, md, tile, lev, rl, gidx, slot);
+      else
+        write_nodes<SC == SC_ATOMIC, 4>(args, md, y, lev, rl, gidx);
+    }
+    // vmult writes zeros into the row padding of the node layout (the
+    // two-pass gather does that itself)
+    if (SC == SC_COLOURED && args.mode == 0 && tix == nt0 - 1 && pitch > args.nn[0])
+    {
+      int const npad = pitch - args.nn[0];
+      for (int i = lane; i < npad * BY * BZ; i += NT)
+      {
+        int const X = i % npad, Y = (i / npad) % BY, Z = i / (npad * BY);
+        int const gy = ncy0 + Y, gzn = ncz0 + Z;
+        if (gy < nn1 && gzn < args.nn[2])
+          args.vdst[args.nn[0] + X + (size_t)pitch * (gy + (size_t)nn1 * gzn)] = 0.0;
+      }
+    }
+    if (++buf == NBUF)
+    {
+      buf = 0;
+      phase ^= 1u;
+    }
+    item = next;
+  }
+}
+
+template <int NS, int P, int SC, bool FC>
+void launch_cell_q1_col_f(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
+{
+  using Q = Q1Col;
+  static int grid_cap = 0;
+  if (grid_cap == 0)
+  {
+    cudaFuncSetAttribute(cell_kernel_q1_col<NS, P, SC, FC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)Q::SMEM);
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cell_kernel_q1_col<NS, P, SC, FC>, Q::NT, Q::SMEM);
+    grid_cap = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+  }
+  int const grid = n_items < grid_cap ? n_items : grid_cap;
+  cell_kernel_q1_col<NS, P, SC, FC><<<grid, Q::NT, Q::SMEM, stream>>>(map, a, n_items);
+}
+
 template <int NS, int P, int SC, int CZ>
 void launch_cell_q1_z(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
 {
@@ -650,11 +933,19 @@ void launch_cell_q1_z(CUtensorMap const &map, KernelArgs const &a, int n_items, 
     launch_cell_q1_f<NS, P, SC, false, CZ>(map, a, n_items, stream);
 }
 
-// a.cells_per_thread 2: two cells per thread (z), else one
+// a.cells_per_thread 4: the column variant (one warp per tile), 2: two
+// cells per thread (z), else one
 template <int NS, int P, int SC>
 void launch_cell_q1_s(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
 {
-  if (a.cells_per_thread == 2)
+  if (a.cells_per_thread == 4)
+  {
+    if (a.faces)
+      launch_cell_q1_col_f<NS, P, SC, true>(map, a, n_items, stream);
+    else
+      launch_cell_q1_col_f<NS, P, SC, false>(map, a, n_items, stream);
+  }
+  else if (a.cells_per_thread == 2)
     launch_cell_q1_z<NS, P, SC, 2>(map, a, n_items, stream);
   else
     launch_cell_q1_z<NS, P, SC, 1>(map, a, n_items, stream);

@@ -375,8 +375,10 @@ int Ensemble::autotune(double const *solutions, double dt, double *ms_out)
   int choice = saved, choice_cz = saved_cz;
   int const deg = members_.empty() ? 2 : members_[0]->mesh_.deg;
   for (int sch : {Thermal::kScheduleColoured, Thermal::kScheduleAtomic, Thermal::kScheduleTwoPass})
-    for (int cz = 1; cz <= (deg == 1 ? 2 : 1); ++cz)
+    for (int cz : {1, 2, 4})
   {
+    if (cz != 1 && deg != 1)
+      continue;
     schedule_ = sch;
     set_cells_per_thread(cz);
     ADM_CK(cudaMemcpyAsync(scratch.p, solutions, total * sizeof(double), cudaMemcpyDeviceToDevice, stream_));

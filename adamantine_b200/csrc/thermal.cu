@@ -1524,10 +1524,10 @@ void Thermal::build_atomic_list(std::vector<uint8_t> const &tile_active)
 
 void Thermal::set_cells_per_thread(int n)
 {
-  if (n != 1 && n != 2)
-    throw Error(ADM_ERR_INVALID, "cells per thread must be 1 or 2");
-  if (n == 2 && mesh_.deg != 1)
-    throw Error(ADM_ERR_UNSUPPORTED, "two cells per thread is a variant of the FE_Q(1) kernel");
+  if (n != 1 && n != 2 && n != 4)
+    throw Error(ADM_ERR_INVALID, "cells per thread must be 1, 2 or 4");
+  if (n != 1 && mesh_.deg != 1)
+    throw Error(ADM_ERR_UNSUPPORTED, "two or four cells per thread are variants of the FE_Q(1) kernel");
   if (n != cells_per_thread_ && step_graph_)
   {
     cudaGraphExecDestroy(step_graph_);
@@ -1614,8 +1614,10 @@ int Thermal::autotune(double const *field, double *ms_out)
   // launch schedules x (FE_Q(1)) cells per thread; ms_out[schedule] is the
   // schedule's best time
   for (int sch : {kScheduleColoured, kScheduleAtomic, kScheduleTwoPass})
-    for (int cz = 1; cz <= (mesh_.deg == 1 ? 2 : 1); ++cz)
+    for (int cz : {1, 2, 4})
     {
+      if (cz != 1 && mesh_.deg != 1)
+        continue;
       schedule_ = sch;
       cells_per_thread_ = cz;
       for (int r = 0; r < 2; ++r)

@@ -198,7 +198,7 @@ class Ensemble:
         _lib.check(self._L.adm_ensemble_set_schedule(self._h, int(schedule)))
 
     def set_cells_per_thread(self, n: int):
-        """FE_Q(1) kernel variant (1 or 2 cells per thread) of the batched
+        """FE_Q(1) kernel variant (1, 2 or 4 cells per thread) of the batched
         stages and the members' own launches."""
         _lib.check(self._L.adm_ensemble_set_cells_per_thread(self._h, int(n)))
 

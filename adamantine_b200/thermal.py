@@ -248,7 +248,7 @@ class ThermalPhysics:
 
     def set_cells_per_thread(self, n: int):
         """FE_Q(1) operator kernel variant: 1 or 2 cells (stacked in z) per
-        thread."""
+        thread, or 4 (one warp per tile, a thread per column of 4 cells)."""
         _lib.check(self._L.adm_set_cells_per_thread(self._h, int(n)))
 
     def cells_per_thread(self) -> int:

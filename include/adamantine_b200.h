@@ -217,9 +217,11 @@ int adm_set_schedule(adm_thermal *h, int32_t schedule);
 int adm_get_schedule(adm_thermal const *h, int32_t *schedule);
 /* Cells per thread of the FE_Q(1) operator kernel (no counterpart in the
  * reference): 1 (default) or 2 cells stacked in z per thread, the second
- * sharing the per-tile bookkeeping and one node level in registers. FE
- * degree 2 takes 1 only. Results agree to rounding; each variant is
- * bit-reproducible in the coloured schedule. */
+ * sharing the per-tile bookkeeping and one node level in registers; or 4,
+ * the column variant: one warp per tile, each thread walking its column of
+ * 4 cells and writing each node level out as it completes, with no CTA
+ * barrier. FE degree 2 takes 1 only. Results agree to rounding; each
+ * variant is bit-reproducible in the coloured and two-pass schedules. */
 int adm_set_cells_per_thread(adm_thermal *h, int32_t n);
 int adm_get_cells_per_thread(adm_thermal const *h, int32_t *n);
 /* Autotuner: times every schedule (and, for FE degree 1, both cells-per-

@@ -46,7 +46,8 @@ def test_ragged_members_have_distinct_work():
 
 
 @pytest.mark.parametrize("method,cells_per_thread", [("rk_fourth_order", 1), ("rk_third_order", 1),
-                                                     ("forward_euler", 1), ("rk_fourth_order", 2)])
+                                                     ("forward_euler", 1), ("rk_fourth_order", 2),
+                                                     ("rk_fourth_order", 4)])
 def test_batched_equals_looped_and_oracle(method, cells_per_thread):
     configs, params, grids = small_ensemble(method=method)
     e1 = Ensemble(configs)

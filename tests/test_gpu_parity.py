@@ -140,18 +140,20 @@ def test_activation_parity():
 Q1_CASES = [c for c in CASES if c.startswith("q1_")]
 
 
-@pytest.mark.parametrize("schedule", [0, 1])
+@pytest.mark.parametrize("cz", [2, 4])
+@pytest.mark.parametrize("schedule", [0, 1, 2])
 @pytest.mark.parametrize("name", Q1_CASES)
-def test_q1_two_cells_per_thread(name, schedule):
-    """The FE_Q(1) kernel variant with two cells (stacked in z) per thread:
-    the same bars against the oracle in both launch schedules (vmult with
-    its phase history over three applications, 12 time steps)."""
+def test_q1_cells_per_thread_variants(name, schedule, cz):
+    """The FE_Q(1) kernel variants with two cells (stacked in z) per thread
+    and with one warp per tile (a column of four cells per thread): the same
+    bars against the oracle in every launch schedule (vmult with its phase
+    history over three applications, 12 time steps)."""
     cfg, cells, T = make_case(name)
     o = make_oracle(cfg, cells)
     g = make_gpu(cfg, cells)
-    g.set_cells_per_thread(2)
+    g.set_cells_per_thread(cz)
     g.set_schedule(schedule)
-    assert g.cells_per_thread() == 2
+    assert g.cells_per_thread() == cz
     o.set_time(2e-4)
     g.set_time(2e-4)
     dst = g.initialize_dof_vector()
@@ -163,7 +165,7 @@ def test_q1_two_cells_per_thread(name, schedule):
         assert np.max(np.abs(g.get_qp_powder() - o.qp_powder())) < 1e-12
     o2 = make_oracle(cfg, cells)
     g2 = make_gpu(cfg, cells)
-    g2.set_cells_per_thread(2)
+    g2.set_cells_per_thread(cz)
     g2.set_schedule(schedule)
     y_ref = grid(T).copy()
     y = g2.from_grid(T)
@@ -180,5 +182,7 @@ def test_two_cells_per_thread_is_a_q1_variant():
     g = make_gpu(cfg, cells)
     with pytest.raises(Exception):
         g.set_cells_per_thread(2)
+    with pytest.raises(Exception):
+        g.set_cells_per_thread(4)
     with pytest.raises(Exception):
         g.set_cells_per_thread(3)
