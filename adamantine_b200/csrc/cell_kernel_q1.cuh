@@ -429,10 +429,10 @@ __global__ void __launch_bounds__(Q1Cell<CZ>::NT, Q1Cell<CZ>::MINB)
         nx_info[j] = mk.cell_info[kc];
         if (NS == 3)
         {
-          // the uniform powder ratio matters only in mode 1
+          // both loaded unconditionally: a load that waited for the mode
+          // would stall the thread here
           nx_pmode[j] = mk.powder_mode[kc];
-          if (nx_pmode[j] == 1)
-            nx_pu[j] = mk.powder_cell[kc];
+          nx_pu[j] = mk.powder_cell[kc];
         }
       }
     }
@@ -703,8 +703,7 @@ __global__ void __launch_bounds__(Q1Col::NT, Q1Col::MINB)
       if (NS == 3)
       {
         pmode = mk.powder_mode[kc];
-        if (pmode == 1)
-          pu = mk.powder_cell[kc];
+        pu = mk.powder_cell[kc];
       }
     }
   };

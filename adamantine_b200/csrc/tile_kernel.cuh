@@ -1026,10 +1026,10 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
       nx_info = mk.cell_info[kc];
       if (NS == 3)
       {
-        // the uniform powder ratio matters only in mode 1
+        // both loaded unconditionally: a load that waited for the mode
+        // would stall the thread here
         nx_pmode = mk.powder_mode[kc];
-        if (nx_pmode == 1)
-          nx_pu = mk.powder_cell[kc];
+        nx_pu = mk.powder_cell[kc];
       }
     }
   };
