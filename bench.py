@@ -252,14 +252,17 @@ def run_ensemble(args, dist, local_rank):
     assert e.device_error() == 0
     # the fair member loop: every member through its own single-member
     # handle and adm_evolve_n_steps (one CUDA graph per step), with the
-    # launch schedule the single-member autotuner picks on member 0
+    # launch schedule and kernel variant the single-member autotuner picks
+    # on member 0
     from adamantine_b200.thermal import ThermalPhysics
 
     singles = [ThermalPhysics(c, device=local_rank, stream=stream) for c in configs]
     ys = [singles[k].from_grid(grids[k]) for k in range(n)]
     single_schedule, _ = singles[0].autotune(ys[0])
+    single_cz = singles[0].cells_per_thread()
     for k, g in enumerate(singles):  # warm-up: graph capture of every handle
         g.set_schedule(single_schedule)
+        g.set_cells_per_thread(single_cz)
         g.evolve_n_steps(0.0, dt, 2, ys[k].clone())
     ys = [singles[k].from_grid(grids[k]) for k in range(n)]
     torch.cuda.synchronize()
@@ -348,7 +351,8 @@ def run_ensemble(args, dist, local_rank):
         "looped_member_steps_per_s": world * n * steps / (ms_g * 1e-3),
         "speedup": ms_g / ms_b, "batched_ms_per_step": ms_b / steps, "looped_ms_per_step": ms_g / steps,
         "looped_path": "32 single-member handles, adm_evolve_n_steps (one CUDA graph per step), "
-                       f"{['coloured', 'atomic'][single_schedule]} schedule (single-member autotuner)",
+                       f"{SCHEDULE_NAMES[single_schedule]} schedule, {single_cz} cell(s) per thread "
+                       "(single-member autotuner)",
         "max_rel_diff_batched_vs_graph_loop": graph_loop_diff,
         "per_step_loop": {"coloured_member_steps_per_s": world * n * steps / (ms_l * 1e-3),
                           "atomic_member_steps_per_s": world * n * steps / (ms_la * 1e-3),
@@ -356,6 +360,7 @@ def run_ensemble(args, dist, local_rank):
                           "path": "adm_ensemble_evolve_looped: each member's stages launched one by one"},
         "identical_results": identical, "max_rel_diff_batched_vs_looped": max_rel_diff,
         "batched_schedule": SCHEDULE_NAMES[schedule],
+        "batched_cells_per_thread": e.cells_per_thread(),
         "batched_path": "one CUDA graph per step (4 stages)",
         "work_items_per_sweep": e.n_work_items(),
         "enkf_analysis_ms": ms_a, "n_obs": int(idx.shape[1]), "augmented_params": 2,
