@@ -82,31 +82,71 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """Samples nvidia-smi SM clocks and throttle reasons during the timed region."""
+    """Samples the SM clock, its maximum and the active clock-event (throttle)
+    reasons during the timed region -- the fields of nvidia-smi's
+    clocks.sm, clocks.max.sm and clocks_event_reasons.* -- through NVML in
+    this process every 20 ms (a forked nvidia-smi could stall the launching
+    thread inside a region of a few milliseconds); nvidia-smi when NVML is
+    not importable."""
 
     QUERY = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, uuid):
         self.uuid = uuid
-        self.samples = []
+        self.samples = []  # (sm MHz, max sm MHz, set of active reason names)
         self._stop = threading.Event()
         self._thr = None
+        self._nvml = None
+        self._handle = None
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self._nvml = pynvml
+            want = uuid.replace("GPU-", "") if uuid else ""
+            for i in range(pynvml.nvmlDeviceGetCount()):
+                h = pynvml.nvmlDeviceGetHandleByIndex(i)
+                u = pynvml.nvmlDeviceGetUUID(h)
+                u = u.decode() if isinstance(u, bytes) else u
+                if not want or want in u:
+                    self._handle = h
+                    break
+        except Exception:
+            self._nvml = None
+
+    def _sample_nvml(self):
+        n, h = self._nvml, self._handle
+        sm = n.nvmlDeviceGetClockInfo(h, n.NVML_CLOCK_SM)
+        smax = n.nvmlDeviceGetMaxClockInfo(h, n.NVML_CLOCK_SM)
+        bits = n.nvmlDeviceGetCurrentClocksEventReasons(h)
+        masks = (n.nvmlClocksEventReasonHwSlowdown, n.nvmlClocksEventReasonHwThermalSlowdown,
+                 n.nvmlClocksEventReasonSwThermalSlowdown, n.nvmlClocksEventReasonSwPowerCap)
+        self.samples.append((float(sm), float(smax), {nm for nm, m in zip(self.NAMES, masks) if bits & m}))
+
+    def _sample_smi(self):
+        out = subprocess.run(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits"],
+                             capture_output=True, text=True, timeout=5).stdout
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if self.uuid and self.uuid not in f[0]:
+                continue
+            if f[1].replace(".", "").isdigit() and f[2].replace(".", "").isdigit():
+                act = {nm for nm, v in zip(self.NAMES, f[5:9]) if v.strip().lower() in ("active", "1", "yes")}
+                self.samples.append((float(f[1]), float(f[2]), act))
 
     def _run(self):
         while not self._stop.is_set():
             try:
-                out = subprocess.run(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits"],
-                                     capture_output=True, text=True, timeout=5).stdout
-                for line in out.strip().splitlines():
-                    f = [x.strip() for x in line.split(",")]
-                    if self.uuid and self.uuid not in f[0]:
-                        continue
-                    self.samples.append(f)
+                if self._handle is not None:
+                    self._sample_nvml()
+                else:
+                    self._sample_smi()
             except Exception:
                 pass
-            self._stop.wait(0.2)
+            self._stop.wait(0.02 if self._handle is not None else 0.2)
 
     def __enter__(self):
         self._thr = threading.Thread(target=self._run, daemon=True)
@@ -120,16 +160,12 @@ class ClockSampler:
     def summary(self):
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        smax = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = set()
-        for s in self.samples:
-            for n, v in zip(names, s[5:9]):
-                if v.strip().lower() in ("active", "1", "yes"):
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(self.samples)}
+        for _, _, act in self.samples:
+            reasons |= act
+        return {"sm_mhz": statistics.median(s[0] for s in self.samples),
+                "sm_max_mhz": max(s[1] for s in self.samples), "reasons": sorted(reasons),
+                "samples": len(self.samples), "source": "NVML" if self._handle is not None else "nvidia-smi"}
 
 
 SIZES = {"full": ((128, 128, 64), (20e-3, 20e-3, 10e-3), 16),
