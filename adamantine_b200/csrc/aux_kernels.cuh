@@ -35,6 +35,16 @@ __global__ void advance_clock_kernel(MemberData *members, int n)
 // GoldakHeatSource / ElectronBeamHeatSource / CubeHeatSource::update_time
 // (source/GoldakHeatSource.cc:24-44, source/ElectronBeamHeatSource.cc:24-45,
 // source/CubeHeatSource.cc:45-49). One block per member, one thread per beam.
+// Zeroes n doubles (p 16-byte aligned, n even) with the evict-last L2
+// policy: the atomic write-out that follows adds into lines still in L2.
+__global__ void zero_keep_kernel(double *p, size_t n)
+{
+  uint64_t const pol = l2_policy_evict_last();
+  size_t const n2 = n / 2;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n2; i += (size_t)gridDim.x * blockDim.x)
+    st_keep2(p + 2 * i, 0.0, 0.0, pol);
+}
+
 __global__ void stage_prepare_kernel(MemberData *members, int n_members, double c)
 {
   int const m = blockIdx.x;

@@ -191,4 +191,26 @@ struct KernelArgs
   double cw[27][4];
 };
 
+// L2 eviction priority for stores whose lines should outlive a streaming
+// read that follows: the zeroed target of the atomic write-out (its FP64
+// reductions then find the lines in L2 instead of fetching them from DRAM)
+// and the two-pass halo sums (read back by the gather pass).
+#ifdef __CUDACC__
+__device__ __forceinline__ uint64_t l2_policy_evict_last()
+{
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ void st_keep(double *p, double v, uint64_t pol)
+{
+  asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(p), "d"(v), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void st_keep2(double *p, double v0, double v1, uint64_t pol)
+{
+  asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(p), "d"(v0), "d"(v1), "l"(pol)
+               : "memory");
+}
+#endif
+
 } // namespace adm

@@ -210,7 +210,7 @@ void Ensemble::launch_step(double *solutions)
       // (and reloads the material constants) at most once or twice
       a.atomic = 1;
       a.blocked = 1;
-      ADM_CK(cudaMemsetAsync(acc_.p, 0, stride_ * (size_t)n * sizeof(double), stream_));
+      launch_zero_keep(acc_.p, stride_ * (size_t)n, stream_);
       if (!awork_.empty())
       {
         a.work = awork_d_.p;
@@ -374,6 +374,21 @@ int Ensemble::autotune(double const *solutions, double dt, double *ms_out)
   double best = 0.0;
   int choice = saved, choice_cz = saved_cz;
   int const deg = members_.empty() ? 2 : members_[0]->mesh_.deg;
+  // an untimed step of every variant first: the first launches of each
+  // kernel and the clock ramp of an idle GPU would otherwise fall on the
+  // first variant timed
+  for (int sch : {Thermal::kScheduleColoured, Thermal::kScheduleAtomic, Thermal::kScheduleTwoPass})
+    for (int cz : {1, 2, 4})
+    {
+      if (cz != 1 && deg != 1)
+        continue;
+      schedule_ = sch;
+      set_cells_per_thread(cz);
+      ADM_CK(cudaMemcpyAsync(scratch.p, solutions, total * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+      evolve_one_time_step(0.0, dt, scratch.p);
+      for (size_t k = 0; k < members_.size(); ++k)
+        members_[k]->restore_phase(snaps[k]);
+    }
   for (int sch : {Thermal::kScheduleColoured, Thermal::kScheduleAtomic, Thermal::kScheduleTwoPass})
     for (int cz : {1, 2, 4})
   {

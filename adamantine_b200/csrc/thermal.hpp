@@ -162,6 +162,9 @@ void launch_stage_prepare(MemberData *members, int n, double c, cudaStream_t str
 // Per-Gauss-point powder ratios [C][NN] from the sparse powder history.
 // Stage update of the atomic schedule for n_members members (a.members).
 void launch_stage_finalize(KernelArgs const &a, size_t n_nodes, int n_members, cudaStream_t stream);
+// Zeroes n doubles with the evict-last L2 policy (cudaMemsetAsync when p is
+// not 16-byte aligned or n is odd).
+void launch_zero_keep(double *p, size_t n, cudaStream_t stream);
 // two-pass schedule: the gather pass, and a tile's halo array length
 void launch_two_pass_gather(int deg, KernelArgs const &a, int n_members, cudaStream_t stream);
 size_t two_pass_halo_size(int deg);

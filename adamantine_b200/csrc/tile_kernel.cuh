@@ -800,6 +800,7 @@ __device__ __forceinline__ void write_nodes_two_pass(KernelArgs const &args, Mem
 {
   double *const tgt = args.mode == 2 ? md.acc : args.vdst;
   double *const halo = md.halo + (size_t)tile * HL::SIZE;
+  uint64_t const pol = l2_policy_evict_last(); // the gather pass reads the halo next
   double old[NV];
 #pragma unroll
   for (int i = 0; i < NV; ++i)
@@ -808,7 +809,7 @@ __device__ __forceinline__ void write_nodes_two_pass(KernelArgs const &args, Mem
   for (int i = 0; i < NV; ++i)
   {
     if (rl[i] == 8)
-      halo[slot[i]] = res[i];
+      st_keep(halo + slot[i], res[i], pol);
     else if (rl[i] == 4)
       tgt[gidx[i]] = old[i] + res[i];
   }

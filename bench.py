@@ -43,15 +43,20 @@ FP64_FLOP_PER_Q2_CELL = 2247
 
 # DRAM bytes (read + write) of one vmult of the 128x128x64 workload from ncu
 # captures (dram__bytes_read.sum + dram__bytes_write.sum): the atomic
-# schedule's single launch (mean of two launches), and the sum over the 8
-# colour launches of the coloured schedule (L2 flushed before every launch,
-# so re-reads that stay in L2 in the timed loop are counted).
-DRAM_BYTES_PER_VMULT_FULL = {"atomic": 211.8e6, "coloured": 327.0e6}
-TRAFFIC_NOTE = {"atomic": "ncu, one launch per vmult",
+# schedule's tile-kernel launch and the two-pass schedule's tile and gather
+# launches inside the timed loop with --cache-control none (L2 as the loop
+# leaves it; means over the loop's launches), and the sum over the 8 colour
+# launches of the coloured schedule (L2 flushed before every launch, so
+# re-reads that stay in L2 in the timed loop are counted).
+DRAM_BYTES_PER_VMULT_FULL = {"atomic": 189.9e6, "two_pass": 286.1e6, "coloured": 327.0e6}
+TRAFFIC_NOTE = {"atomic": "ncu --cache-control none, the tile-kernel launch of a timed-loop vmult",
+                "two_pass": "ncu --cache-control none, tile + gather launches of a timed-loop vmult",
                 "coloured": "ncu, L2 flushed before each of the 8 colour launches"}
-# per schedule: the kernels of one vmult, their launch pattern and count
+# per schedule: the dominant kernel of one vmult, its launch pattern, and
+# the number of launches of one vmult besides the beam preparation (the
+# atomic schedule zeroes its target with a kernel first)
 KERNELS = {"coloured": ("adm::tile_kernel<2,3,2,0,0>", "8 colour launches", 8),
-           "atomic": ("adm::tile_kernel<2,3,2,1,0>", "1 launch", 1),
+           "atomic": ("adm::tile_kernel<2,3,2,1,0>", "1 launch after adm::zero_keep_kernel", 2),
            "two_pass": ("adm::tile_kernel<2,3,2,2,0> + adm::two_pass_gather_kernel<2>",
                         "1 tile launch + 1 gather launch", 2)}
 
