@@ -37,8 +37,13 @@ __global__ void advance_clock_kernel(MemberData *members, int n)
 // source/CubeHeatSource.cc:45-49). One block per member, one thread per beam.
 // Zeroes n doubles (p 16-byte aligned, n even) with the evict-last L2
 // policy: the atomic write-out that follows adds into lines still in L2.
-__global__ void zero_keep_kernel(double *p, size_t n)
+// With members != nullptr, block m < n_members also prepares member m's beam
+// states for stage coefficient c (stage_prepare_kernel's work, folded into
+// the zeroing launch).
+__global__ void zero_keep_kernel(double *p, size_t n, MemberData *members, int n_members, double c)
 {
+  if (members != nullptr && (int)blockIdx.x < n_members && (int)threadIdx.x < members[blockIdx.x].n_beams)
+    prepare_beam(members[blockIdx.x], threadIdx.x, c);
   uint64_t const pol = l2_policy_evict_last();
   size_t const n2 = n / 2;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n2; i += (size_t)gridDim.x * blockDim.x)

@@ -179,7 +179,8 @@ void Ensemble::launch_step(double *solutions)
   int const n = n_members();
   for (int i = 0; i < tab_.s; ++i)
   {
-    if (any_source_)
+    // (the atomic schedule's zeroing launch prepares the beams itself)
+    if (any_source_ && schedule_ != Thermal::kScheduleAtomic)
     {
       launch_stage_prepare(md_d_.p, n, tab_.c[i], stream_);
     }
@@ -210,7 +211,7 @@ void Ensemble::launch_step(double *solutions)
       // (and reloads the material constants) at most once or twice
       a.atomic = 1;
       a.blocked = 1;
-      launch_zero_keep(acc_.p, stride_ * (size_t)n, stream_);
+      launch_zero_keep(acc_.p, stride_ * (size_t)n, stream_, any_source_ ? md_d_.p : nullptr, n, tab_.c[i]);
       if (!awork_.empty())
       {
         a.work = awork_d_.p;

@@ -898,7 +898,7 @@ void Thermal::launch_pass(KernelArgs a, double const *src)
     size_t const N = mesh_.n_nodes;
     a.atomic = 1;
     if (a.mode == 2)
-      launch_zero_keep(acc_p_, N, stream_);
+      launch_zero_keep(acc_p_, N, stream_, fold_prepare_c_ >= 0.0 ? member_d_.p : nullptr, 1, fold_prepare_c_);
     if (count > 0)
     {
       a.work = awork_d_.p;
@@ -946,15 +946,18 @@ void launch_stage_prepare(MemberData *members, int n, double c, cudaStream_t str
   ADM_CK(cudaGetLastError());
 }
 
-void launch_zero_keep(double *p, size_t n, cudaStream_t stream)
+void launch_zero_keep(double *p, size_t n, cudaStream_t stream, MemberData *members, int n_members, double c)
 {
   if ((reinterpret_cast<uintptr_t>(p) & 15u) != 0 || (n & 1u) != 0)
   {
     ADM_CK(cudaMemsetAsync(p, 0, n * sizeof(double), stream));
+    if (members != nullptr)
+      launch_stage_prepare(members, n_members, c, stream);
     return;
   }
-  size_t const blocks = std::min<size_t>((n / 2 + 255) / 256, 148 * 16);
-  zero_keep_kernel<<<(unsigned)std::max<size_t>(blocks, 1), 256, 0, stream>>>(p, n);
+  size_t blocks = std::min<size_t>((n / 2 + 255) / 256, 148 * 16);
+  blocks = std::max<size_t>(blocks, members != nullptr ? (size_t)n_members : 1);
+  zero_keep_kernel<<<(unsigned)blocks, 256, 0, stream>>>(p, n, members, n_members, c);
   ADM_CK(cudaGetLastError());
 }
 
@@ -1001,9 +1004,11 @@ void Thermal::vmult(double *dst, double const *src, bool add)
   // Nodes that only inactive tiles touch are not written by the tile kernel;
   // the atomic schedule adds into a zeroed vector.
   // (the two-pass gather writes every node itself)
+  // (the beam preparation rides along with the zeroing launch when there is one)
   if (!add && schedule_ != kScheduleTwoPass && (!topo_.all_tiles_active || schedule_ == kScheduleAtomic))
-    launch_zero_keep(dst, mesh_.n_nodes, stream_);
-  prepare_stage(0.0);
+    launch_zero_keep(dst, mesh_.n_nodes, stream_, cfg_.n_sources > 0 ? member_d_.p : nullptr, 1, 0.0);
+  else
+    prepare_stage(0.0);
   KernelArgs a = base_args();
   a.mode = add ? 1 : 0;
   a.vsrc = src;
@@ -1023,8 +1028,9 @@ void Thermal::vmult_stage(double *dst, double const *src, double c)
   if (!setup_done_)
     throw Error(ADM_ERR_INVALID, "setup() has not been called");
   if (schedule_ != kScheduleTwoPass && (!topo_.all_tiles_active || schedule_ == kScheduleAtomic))
-    launch_zero_keep(dst, mesh_.n_nodes, stream_);
-  prepare_stage(c);
+    launch_zero_keep(dst, mesh_.n_nodes, stream_, cfg_.n_sources > 0 ? member_d_.p : nullptr, 1, c);
+  else
+    prepare_stage(c);
   KernelArgs a = base_args();
   a.mode = 0;
   a.vsrc = src;
@@ -1065,10 +1071,15 @@ void Thermal::launch_step(double *solution)
 {
   for (int i = 0; i < tab_.s; ++i)
   {
-    prepare_stage(tab_.c[i]);
+    // the atomic schedule's zeroing launch prepares the beams itself
+    if (schedule_ == kScheduleAtomic && cfg_.n_sources > 0)
+      fold_prepare_c_ = tab_.c[i];
+    else
+      prepare_stage(tab_.c[i]);
     KernelArgs a = stage_args(i);
     a.y_override = solution;
     launch_pass(a, i == 0 ? solution : (a.src_sel == 1 ? za_p_ : zb_p_));
+    fold_prepare_c_ = -1.0;
   }
 }
 

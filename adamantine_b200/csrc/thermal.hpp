@@ -164,7 +164,10 @@ void launch_stage_prepare(MemberData *members, int n, double c, cudaStream_t str
 void launch_stage_finalize(KernelArgs const &a, size_t n_nodes, int n_members, cudaStream_t stream);
 // Zeroes n doubles with the evict-last L2 policy (cudaMemsetAsync when p is
 // not 16-byte aligned or n is odd).
-void launch_zero_keep(double *p, size_t n, cudaStream_t stream);
+// With members != nullptr the launch also prepares the beam states of
+// n_members members for stage coefficient c (launch_stage_prepare).
+void launch_zero_keep(double *p, size_t n, cudaStream_t stream, MemberData *members = nullptr, int n_members = 0,
+                      double c = 0.0);
 // two-pass schedule: the gather pass, and a tile's halo array length
 void launch_two_pass_gather(int deg, KernelArgs const &a, int n_members, cudaStream_t stream);
 size_t two_pass_halo_size(int deg);
@@ -340,6 +343,9 @@ private:
   DevBuf<uint8_t> powder_mode_, has_melted_d_;
   DevBuf<int32_t> face_slot_d_, error_d_;
   DevBuf<int32_t> claim_d_; // per-colour work counters of the tile launches (dynamic claiming)
+  // stage coefficient whose beam preparation the atomic schedule's zeroing
+  // launch does (negative: none pending)
+  double fold_prepare_c_ = -1.0;
   DevBuf<double> halo_d_;   // two-pass schedule: per-tile upper-face partial sums
   DevBuf<int64_t> cells_d_;
   // deposition: per-cell mark, append list, material ids

@@ -1461,14 +1461,20 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
     int const sz = (Z == 0 && tiz > 0) ? 1 : ((Z == DEG * TZ && tiz < args.nt[2] - 1) ? 2 : 0);
     int rl[NQS], slot[NQS];
     size_t gidx[NQS];
+    // the thread's first node and how many of its N x N nodes per row and
+    // column lie inside the mesh: one 64-bit index per thread, the nodes at
+    // constant offsets from it
+    int const gx0 = nx0 + DEG * lx, gy0 = ny0 + DEG * ly;
+    int const xin = args.nn[0] - gx0, yin = nn1 - gy0;
+    bool const zin = gz < args.nn[2];
+    size_t const g0 = gx0 + (size_t)pitch * (gy0 + (size_t)nn1 * gz);
 #pragma unroll
     for (int i = 0; i < NQS; ++i)
     {
       int const a = i % N, bb = i / N;
       int const X = DEG * lx + a, Y = DEG * ly + bb;
-      int const gx = nx0 + X, gy = ny0 + Y;
       bool const own = own_k && (a > 0 || lx == 0) && (bb > 0 || ly == 0);
-      bool const inside = gx < args.nn[0] && gy < nn1 && gz < args.nn[2];
+      bool const inside = a < xin && bb < yin && zin;
       int const sx = (X == 0 && tix > 0) ? 1 : ((X == DEG * TX && tix < nt0 - 1) ? 2 : 0);
       int const sy = (Y == 0 && tiy > 0) ? 1 : ((Y == DEG * TY && tiy < nt1 - 1) ? 2 : 0);
       slot[i] = 0;
@@ -1476,7 +1482,7 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
         rl[i] = (own && inside) ? two_pass_slot<HaloOf<DEG>>(X, Y, Z, sx, sy, sz, &slot[i]) : 0;
       else
         rl[i] = (own && inside) ? (SC == SC_ATOMIC ? 4 : (sp.role[buf][sx + 3 * sy + 9 * sz] | 4)) : 0;
-      gidx[i] = gx + (size_t)pitch * (gy + (size_t)nn1 * gz);
+      gidx[i] = g0 + a + (size_t)pitch * bb;
     }
     if constexpr (SC == SC_TWO_PASS)
       write_nodes_two_pass<HaloOf<DEG>, NQS>(args, md, tile, res, rl, gidx, slot);
