@@ -160,6 +160,7 @@ SIGNATURES = {
     "adm_mechanics_solve": [_VP, _VP, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double)],
     "adm_mechanics_n_dofs": [_VP, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)],
     "adm_mechanics_node_mask": [_VP, _VP],
+    "adm_mechanics_stress_state": [_VP, _VP, _VP, _VP],
     "adm_enkf_analysis": [_VP, ctypes.c_int32, _VP, ctypes.c_int64, ctypes.c_int64, _VP, ctypes.c_int32,
                           ctypes.c_int32, _VP, _VP, _VP, _VP, _VP, _VP],
 }

@@ -4,7 +4,9 @@
  * (assemble_rhs, :283-486: thermal expansion and gravity), the cell
  * selection of MechanicalPhysics::setup_dofs (source/MechanicalPhysics.cc
  * :280-440: thermally active cells with a solid ratio above 0.99) and the
- * CG solve of MechanicalPhysics::solve (:488-520), matrix-free on the GPU.
+ * CG solve of MechanicalPhysics::solve (:488-520), matrix-free on the GPU;
+ * then the J2 stress update of compute_stress (:542-634) at every Gauss
+ * point, one thread per point.
  *
  * Layout: the thermal handle's node layout (pitch, z-slabs); a displacement
  * vector is three node vectors (x, y, z components). Work: one warp per
@@ -56,6 +58,7 @@ struct MechArgs
   int thermoelastic, gravity;
   uint8_t const *melted;
   double const *tab; // the handle's reference-element tables (kTab* offsets)
+  double plastic_modulus[4], iso_hardening[4], elastic_limit[4];
 };
 
 __device__ __forceinline__ int64_t node_of(MechArgs const &a, int cx, int cy, int cz, int n)
@@ -63,6 +66,152 @@ __device__ __forceinline__ int64_t node_of(MechArgs const &a, int cx, int cy, in
   int const np = a.p + 1;
   int const i = n % np, j = (n / np) % np, k = n / (np * np);
   return (int64_t)(a.p * cx + i) + (int64_t)a.pitch * ((a.p * cy + j) + (int64_t)a.nn[1] * (a.p * cz + k));
+}
+
+// The stress state at the Gauss points: plastic internal variable [C N],
+// stress and back stress [6][C N] (xx, yy, zz, xy, xz, yz), point q of cell
+// c at c N + q.
+struct J2State
+{
+  double *kappa, *stress, *back;
+  int64_t cq; // C N
+};
+
+// A cell that starts carrying displacement: the elastic limit, zero stress
+// and back stress at its points (MechanicalPhysics::setup_dofs,
+// source/MechanicalPhysics.cc:366-378; the constructor, :76-98).
+__global__ void j2_init_kernel(MechArgs a, J2State s, int32_t const *cells, int n)
+{
+  int64_t const t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= (int64_t)n * a.N)
+    return;
+  int const c = cells[t / a.N], q = (int)(t % a.N);
+  int64_t const i = (int64_t)c * a.N + q;
+  s.kappa[i] = a.elastic_limit[a.matid[c]];
+  for (int k = 0; k < 6; ++k)
+  {
+    s.stress[k * s.cq + i] = 0.0;
+    s.back[k * s.cq + i] = 0.0;
+  }
+}
+
+// MechanicalPhysics::compute_stress (source/MechanicalPhysics.cc:542-634),
+// one thread per Gauss point of a cell that carries displacement: the
+// symmetric gradient of the displacement increment u - u_old (u_old NULL:
+// none yet), the trial stress sigma + lambda tr(eps) I + 2 mu eps, and where
+// |dev(sigma) - beta| reaches the plastic internal variable kappa the radial
+// return with increment (|eta| - kappa) / (2 mu + H) along n = eta / |eta|:
+// sigma -= 2 mu dgamma n, kappa += h H dgamma, beta += (1 - h) H^2 n (the
+// reference's back-stress update, :626-630, as written there: H^2 n, not
+// H dgamma n). |.| is the Frobenius norm (off-diagonal entries twice).
+__global__ void __launch_bounds__(128) j2_stress_kernel(MechArgs a, J2State s, double const *u,
+                                                        double const *u_old)
+{
+  int64_t const t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= (int64_t)a.n_cells * a.N)
+    return;
+  int const c = a.cells[t / a.N], q = (int)(t % a.N);
+  int const cx = c % a.nc[0], cy = (c / a.nc[0]) % a.nc[1], cz = c / (a.nc[0] * a.nc[1]);
+  int const mat = a.matid[c];
+  double const lam = a.lambda[mat], mu = a.mu[mat];
+  double G3[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+  for (int n = 0; n < a.N; ++n)
+  {
+    int64_t const g = node_of(a, cx, cy, cz, n);
+    double const *gr = a.tab + kTabGrad + (q * kMaxN + n) * 3;
+#pragma unroll
+    for (int comp = 0; comp < 3; ++comp)
+    {
+      double const d = u[comp * a.m + g] - (u_old ? u_old[comp * a.m + g] : 0.0);
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+        G3[comp][k] = fma(d, gr[k], G3[comp][k]);
+    }
+  }
+#pragma unroll
+  for (int comp = 0; comp < 3; ++comp)
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      G3[comp][k] *= a.inv_h[k];
+  // strain (symmetric gradient), xx yy zz xy xz yz
+  double const e[6] = {G3[0][0], G3[1][1], G3[2][2], 0.5 * (G3[0][1] + G3[1][0]), 0.5 * (G3[0][2] + G3[2][0]),
+                       0.5 * (G3[1][2] + G3[2][1])};
+  double const tr = e[0] + e[1] + e[2];
+  int64_t const i = (int64_t)c * a.N + q;
+  double sig[6], eta[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k)
+    sig[k] = s.stress[k * s.cq + i] + ((k < 3 ? lam * tr : 0.0) + 2.0 * mu * e[k]);
+  double const mean = (sig[0] + sig[1] + sig[2]) / 3.0;
+  double nrm2 = 0.0;
+#pragma unroll
+  for (int k = 0; k < 6; ++k)
+  {
+    eta[k] = (k < 3 ? sig[k] - mean : sig[k]) - s.back[k * s.cq + i];
+    nrm2 += (k < 3 ? 1.0 : 2.0) * eta[k] * eta[k];
+  }
+  double const nrm = sqrt(nrm2);
+  double const kap = s.kappa[i];
+  if (nrm < kap)
+  {
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+      s.stress[k * s.cq + i] = sig[k];
+    return;
+  }
+  double const H = a.plastic_modulus[mat], h = a.iso_hardening[mat];
+  double const dg = (nrm - kap) / (2.0 * mu + H);
+#pragma unroll
+  for (int k = 0; k < 6; ++k)
+  {
+    double const nk = eta[k] / nrm;
+    s.stress[k * s.cq + i] = sig[k] - 2.0 * mu * dg * nk;
+    s.back[k * s.cq + i] += (1.0 - h) * H * H * nk;
+  }
+  s.kappa[i] = kap + h * H * dg;
+}
+
+// The previous displacement after the cells that carry displacement changed
+// (MechanicalPhysics::setup_dofs, source/MechanicalPhysics.cc:296-337 and
+// :418-437): every cell that now carries displacement writes, in cell order,
+// its saved values -- the old displacement if it carried displacement
+// before, zeros if not -- so a node keeps its old value when the last such
+// cell touching it carried displacement before, else gets 0 (0 as well at
+// nodes of no such cell).
+__global__ void old_displacement_transfer_kernel(MechArgs a, uint8_t const *carry_prev, uint8_t const *carry_now,
+                                                 double *u_old)
+{
+  int64_t const g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (g >= a.m)
+    return;
+  int const gx = (int)(g % a.pitch);
+  int64_t const r = g / a.pitch;
+  int const gy = (int)(r % a.nn[1]), gz = (int)(r / a.nn[1]);
+  bool keep = false;
+  if (gx < a.nn[0])
+  {
+    // the cells around the node, in increasing cell index: the last one that
+    // carries displacement now decides
+    int64_t last = -1;
+    for (int dz = 1; dz >= 0; --dz)
+      for (int dy = 1; dy >= 0; --dy)
+        for (int dx = 1; dx >= 0; --dx)
+        {
+          // cell (cx, cy, cz) touches node (gx, gy, gz) when p cx <= gx <= p (cx + 1)
+          int const cx = gx / a.p - dx, cy = gy / a.p - dy, cz = gz / a.p - dz;
+          if (cx < 0 || cy < 0 || cz < 0 || cx >= a.nc[0] || cy >= a.nc[1] || cz >= a.nc[2])
+            continue;
+          if (gx > a.p * (cx + 1) || gy > a.p * (cy + 1) || gz > a.p * (cz + 1))
+            continue;
+          int64_t const c = cx + (int64_t)a.nc[0] * (cy + (int64_t)a.nc[1] * cz);
+          if (carry_now[c] && c > last)
+            last = c;
+        }
+    keep = last >= 0 && carry_prev[last];
+  }
+  for (int comp = 0; comp < 3; ++comp)
+    if (!keep)
+      u_old[comp * a.m + g] = 0.0;
 }
 
 // dst += A src on the free rows; 4 warps per block, 32 / N cells per warp
@@ -371,8 +520,13 @@ public:
     if (cfg_.clamped_faces < 0 || cfg_.clamped_faces > 63)
       throw Error(ADM_ERR_INVALID, "clamped_faces is a 6-bit mask");
     for (int k = 0; k < th_.cfg_.n_materials; ++k)
+    {
       if (!(cfg_.lame_second[k] > 0.0) || !(cfg_.lame_first[k] > -2.0 / 3.0 * cfg_.lame_second[k]))
         throw Error(ADM_ERR_INVALID, "Lame parameters must give a positive definite elasticity tensor");
+      if (std::isnan(cfg_.elastic_limit[k]) ||
+          (std::isfinite(cfg_.elastic_limit[k]) && !(2.0 * cfg_.lame_second[k] + cfg_.plastic_modulus[k] > 0.0)))
+        throw Error(ADM_ERR_INVALID, "J2 plasticity needs an elastic limit and 2 mu + plastic_modulus > 0");
+    }
     p_ = M.deg;
     N_ = (p_ + 1) * (p_ + 1) * (p_ + 1);
     // reference-element tables
@@ -422,6 +576,9 @@ public:
       if (t.active_[c] && st[c] > 0.99) // state 0: solid
         cells.push_back((int32_t)c);
     n_cells_ = (int64_t)cells.size();
+    std::vector<uint8_t> carry(C, 0);
+    for (int32_t c : cells)
+      carry[c] = 1;
     // nodes of those cells; clamped: on a clamped box face
     m_ = (int64_t)M.n_nodes;
     std::vector<uint8_t> mask(m_, 0);
@@ -459,6 +616,7 @@ public:
     ADM_CK(cudaMemcpyAsync(mask_.p, mask.data(), m_, cudaMemcpyHostToDevice, s));
     ADM_CK(cudaMemcpyAsync(matid_.p, t.matid_.data(), C, cudaMemcpyHostToDevice, s));
     ADM_CK(cudaMemcpyAsync(melted_.p, t.has_melted_.data(), C, cudaMemcpyHostToDevice, s));
+    setup_stress_state(carry, cells);
     // right-hand side and Jacobi diagonal
     rhs_.alloc(3 * m_);
     diag_.alloc(3 * m_);
@@ -544,6 +702,23 @@ public:
       *iterations = it;
     if (residual)
       *residual = res;
+    update_stress(x);
+  }
+
+  // stress state of the Gauss points into caller device arrays
+  void stress_state(double *stress, double *back, double *plastic)
+  {
+    require();
+    cudaStream_t const s = th_.stream_;
+    ADM_CK(cudaSetDevice(th_.device_));
+    int64_t const cq = (int64_t)th_.mesh_.n_cells * N_;
+    if (stress)
+      ADM_CK(cudaMemcpyAsync(stress, stress_.p, 6 * cq * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    if (back)
+      ADM_CK(cudaMemcpyAsync(back, back_.p, 6 * cq * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    if (plastic)
+      ADM_CK(cudaMemcpyAsync(plastic, kappa_.p, cq * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    ADM_CK(cudaStreamSynchronize(s));
   }
 
   int64_t n_dofs() const { return n_dofs_; }
@@ -555,6 +730,86 @@ private:
   {
     if (!ready_)
       throw Error(ADM_ERR_INVALID, "adm_mechanics_setup has not been called");
+  }
+
+  J2State j2() const { return J2State{kappa_.p, stress_.p, back_.p, (int64_t)th_.mesh_.n_cells * N_}; }
+
+  // The Gauss-point state and the previous displacement when the cells that
+  // carry displacement are (re)chosen: cells that start carrying it start
+  // from the elastic limit and zero stresses, and the previous displacement
+  // follows MechanicalPhysics::setup_dofs (old_displacement_transfer_kernel).
+  void setup_stress_state(std::vector<uint8_t> const &carry, std::vector<int32_t> const &cells)
+  {
+    cudaStream_t const s = th_.stream_;
+    size_t const C = th_.mesh_.n_cells;
+    bool const first = carry_prev_.empty();
+    std::vector<int32_t> fresh;
+    bool changed = first;
+    for (int32_t c : cells)
+      if (first || !carry_prev_[c])
+        fresh.push_back(c);
+    if (!first)
+      for (size_t c = 0; c < C; ++c)
+        changed = changed || (carry[c] != carry_prev_[c]);
+    if (first)
+    {
+      int64_t const cq = (int64_t)C * N_;
+      kappa_.alloc(std::max<int64_t>(1, cq));
+      stress_.alloc(std::max<int64_t>(1, 6 * cq));
+      back_.alloc(std::max<int64_t>(1, 6 * cq));
+      ADM_CK(cudaMemsetAsync(stress_.p, 0, 6 * cq * sizeof(double), s));
+      ADM_CK(cudaMemsetAsync(back_.p, 0, 6 * cq * sizeof(double), s));
+      // every cell starts at its material's elastic limit
+      std::vector<int32_t> all(C);
+      for (size_t c = 0; c < C; ++c)
+        all[c] = (int32_t)c;
+      init_points(all);
+      u_old_.alloc(3 * m_);
+      carry_d_.alloc(2 * C);
+    }
+    else if (!fresh.empty())
+      init_points(fresh);
+    if (!first && changed && has_old_)
+    {
+      ADM_CK(cudaMemcpyAsync(carry_d_.p, carry_prev_.data(), C, cudaMemcpyHostToDevice, s));
+      ADM_CK(cudaMemcpyAsync(carry_d_.p + C, carry.data(), C, cudaMemcpyHostToDevice, s));
+      old_displacement_transfer_kernel<<<(unsigned)((m_ + 255) / 256), 256, 0, s>>>(args(), carry_d_.p,
+                                                                                     carry_d_.p + C, u_old_.p);
+      ADM_CK(cudaGetLastError());
+    }
+    ADM_CK(cudaStreamSynchronize(s));
+    carry_prev_ = carry;
+  }
+
+  void init_points(std::vector<int32_t> const &list)
+  {
+    if (list.empty())
+      return;
+    cudaStream_t const s = th_.stream_;
+    DevBuf<int32_t> d;
+    d.alloc(list.size());
+    ADM_CK(cudaMemcpyAsync(d.p, list.data(), list.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    MechArgs a = args();
+    a.matid = matid_.p;
+    int64_t const n = (int64_t)list.size() * N_;
+    j2_init_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, j2(), d.p, (int)list.size());
+    ADM_CK(cudaGetLastError());
+    ADM_CK(cudaStreamSynchronize(s)); // d is released on return
+  }
+
+  // after a solve: stress from the displacement increment, then the
+  // displacement becomes the previous one
+  void update_stress(double const *u)
+  {
+    if (n_cells_ == 0)
+      return;
+    cudaStream_t const s = th_.stream_;
+    int64_t const n = n_cells_ * N_;
+    j2_stress_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(args(), j2(), u, has_old_ ? u_old_.p : nullptr);
+    ADM_CK(cudaGetLastError());
+    ADM_CK(cudaMemcpyAsync(u_old_.p, u, 3 * m_ * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    ADM_CK(cudaStreamSynchronize(s));
+    has_old_ = true;
   }
 
   MechArgs args() const
@@ -584,6 +839,9 @@ private:
       a.alpha[k] = cfg_.thermal_expansion[k];
       a.rho[k] = cfg_.density[k];
       a.tref[k] = cfg_.reference_temperature[k];
+      a.plastic_modulus[k] = cfg_.plastic_modulus[k];
+      a.iso_hardening[k] = cfg_.isotropic_hardening[k];
+      a.elastic_limit[k] = cfg_.elastic_limit[k];
     }
     a.tinit = cfg_.initial_temperature;
     a.thermoelastic = cfg_.thermoelastic;
@@ -643,6 +901,11 @@ private:
   DevBuf<uint8_t> mask_, matid_, melted_;
   DevBuf<double> tab_; // reference-element tables of this handle's degree
   DevBuf<double> rhs_, diag_, r_, z_, pv_, qv_, sc_;
+  // J2 state of the Gauss points and the previous displacement
+  DevBuf<double> kappa_, stress_, back_, u_old_;
+  DevBuf<uint8_t> carry_d_;              // [2][C]: carried before, carries now
+  std::vector<uint8_t> carry_prev_;      // cells that carried displacement at the last setup
+  bool has_old_ = false;                 // a solve has given a previous displacement
 };
 
 } // namespace adm
@@ -718,6 +981,14 @@ int adm_mechanics_node_mask(adm_mechanics const *h, uint8_t *mask)
   return adm::guard([&] {
     ADM_REQUIRE(h && mask, "null argument");
     std::copy(h->m->mask().begin(), h->m->mask().end(), mask);
+  });
+}
+
+int adm_mechanics_stress_state(adm_mechanics *h, double *stress, double *back_stress, double *plastic)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h, "null handle");
+    h->m->stress_state(stress, back_stress, plastic);
   });
 }
 

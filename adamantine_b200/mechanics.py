@@ -5,8 +5,11 @@ driver uses it after the thermal step (application/adamantine.hh:1289-1345):
 ``setup_dofs`` picks the cells that carry displacement (thermally active,
 solid ratio above 0.99) and forms the right-hand side from the temperature
 (thermal expansion from the reference temperature, gravity); ``solve`` runs
-CG on the elasticity operator and returns the displacement. Elastic only:
-the reference's J2 plasticity after the solve is not built.
+CG on the elasticity operator and returns the displacement, then updates
+the stress at the Gauss points from the displacement increment with the
+reference's combined isotropic-kinematic J2 model (compute_stress,
+source/MechanicalPhysics.cc:542-634); ``stress_state`` returns the stress,
+the back stress and the plastic internal variable.
 """
 from __future__ import annotations
 
@@ -36,6 +39,9 @@ class MechConfigStruct(ctypes.Structure):
         ("rel_tol", ctypes.c_double),
         ("max_iter", ctypes.c_int32),
         ("pad0", ctypes.c_int32),
+        ("plastic_modulus", ctypes.c_double * 4),
+        ("isotropic_hardening", ctypes.c_double * 4),
+        ("elastic_limit", ctypes.c_double * 4),
     ]
 
 
@@ -56,19 +62,23 @@ class MechanicalPhysics:
     for cells that have melted, initial_temperature for the others (the
     reference's reference_temperatures list with the initial temperature
     last); clamped: box faces with zero displacement ('x-' ... 'z+', boundary
-    ids 0..5)."""
+    ids 0..5). J2 plasticity per material: plastic_modulus,
+    isotropic_hardening and elastic_limit (infinite, the reference's
+    default, keeps the material elastic)."""
 
     def __init__(self, physics: ThermalPhysics, lame_first, lame_second, thermal_expansion=0.0, density=0.0,
                  reference_temperatures=None, initial_temperature: float = 300.0, thermoelastic: bool = True,
                  gravity: bool = True, clamped: Sequence[str] = ("z-",), rel_tol: float = 1e-12,
-                 max_iter: int = 0):
+                 max_iter: int = 0, plastic_modulus=0.0, isotropic_hardening=0.0, elastic_limit=float("inf")):
         self._L = _lib.load()
         self.physics = physics
         c = MechConfigStruct()
         for name, v in (("lame_first", lame_first), ("lame_second", lame_second),
                         ("thermal_expansion", thermal_expansion), ("density", density),
                         ("reference_temperature", reference_temperatures if reference_temperatures is not None
-                         else initial_temperature)):
+                         else initial_temperature),
+                        ("plastic_modulus", plastic_modulus), ("isotropic_hardening", isotropic_hardening),
+                        ("elastic_limit", elastic_limit)):
             arr = _per_material(v)
             for k in range(4):
                 getattr(c, name)[k] = arr[k]
@@ -137,3 +147,16 @@ class MechanicalPhysics:
         out = np.zeros(self.m, np.uint8)
         _lib.check(self._L.adm_mechanics_node_mask(self._h, out.ctypes.data_as(ctypes.c_void_p)))
         return out
+
+    def stress_state(self):
+        """(stress [6, n_cells, nq], back stress [6, n_cells, nq], plastic
+        internal variable [n_cells, nq]) at the nq = (degree + 1)^3 Gauss
+        points (x fastest) of every cell of the thermal mesh; components xx,
+        yy, zz, xy, xz, yz."""
+        C, nq = self.physics.n_cells, self.physics.n_qp
+        dev = self.physics.device
+        s = torch.empty((6, C, nq), dtype=torch.float64, device=dev)
+        b = torch.empty((6, C, nq), dtype=torch.float64, device=dev)
+        k = torch.empty((C, nq), dtype=torch.float64, device=dev)
+        _lib.check(self._L.adm_mechanics_stress_state(self._h, _dev(s), _dev(b), _dev(k)))
+        return s, b, k

@@ -22,8 +22,21 @@
  * The handle is bound to a thermal handle (same mesh, degree and node
  * layout): displacement vectors are 3 node vectors (x, y, z components)
  * of adm_n_nodes doubles each, consecutive; entries of nodes that carry no
- * displacement are 0. The elastic solve only: the reference's J2
- * plasticity after the solve (:520-634) is not built.
+ * displacement are 0.
+ *
+ * After each solve the stress is updated as MechanicalPhysics::solve and
+ * compute_stress do (:520-634): the displacement increment since the last
+ * solve gives the strain at every Gauss point of the cells that carry
+ * displacement, the trial stress adds C : strain to the stored stress, and
+ * where the norm of its deviator minus the back stress reaches the plastic
+ * internal variable (initially the elastic limit) the radial return of the
+ * combined isotropic-kinematic J2 model updates the stress, the plastic
+ * internal variable and the back stress. A cell that starts carrying
+ * displacement (material added, or solidified) starts from zero stress and
+ * back stress and the elastic limit; the previous displacement is carried
+ * over as MechanicalPhysics::setup_dofs does (:296-437: a node keeps it when
+ * the last cell touching it in cell order already carried displacement,
+ * else it restarts from 0).
  */
 #ifndef ADAMANTINE_B200_MECHANICS_H
 #define ADAMANTINE_B200_MECHANICS_H
@@ -59,6 +72,13 @@ typedef struct adm_mech_config
   double rel_tol;
   int32_t max_iter;
   int32_t pad0;
+  /* per material, the solid's plastic_modulus, isotropic_hardening (the
+   * isotropic share of the hardening, 0..1) and elastic_limit
+   * (MaterialProperty mechanical properties; +INFINITY, the reference's
+   * default when elastic_limit is not given, keeps the material elastic) */
+  double plastic_modulus[4];
+  double isotropic_hardening[4];
+  double elastic_limit[4];
 } adm_mech_config;
 
 typedef struct adm_mechanics adm_mechanics;
@@ -84,6 +104,15 @@ int adm_mechanics_solve(adm_mechanics *h, double *displacement, int32_t *iterati
 int adm_mechanics_n_dofs(adm_mechanics const *h, int64_t *n_dofs, int64_t *n_cells);
 /* Per node (adm_n_nodes bytes): 0 no displacement, 1 free, 2 clamped. */
 int adm_mechanics_node_mask(adm_mechanics const *h, uint8_t *mask);
+/* The stress state at the Gauss points (MechanicalPhysics::get_stress_tensor,
+ * the back stress and the plastic internal variable), device arrays indexed
+ * by q + nq (cell) with nq = (degree + 1)^3 Gauss points per cell
+ * (x fastest) and the thermal handle's cell index: stress and back_stress
+ * [6][n_cells nq] (components xx, yy, zz, xy, xz, yz), plastic
+ * [n_cells nq]; any may be NULL. Values of cells that carry no displacement
+ * are those they last had (zero stress and the elastic limit before they
+ * ever carried any). */
+int adm_mechanics_stress_state(adm_mechanics *h, double *stress, double *back_stress, double *plastic);
 
 #ifdef __cplusplus
 }

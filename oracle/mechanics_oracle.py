@@ -10,7 +10,15 @@ of the right-hand side of MechanicalOperator::assemble_rhs
 div phi_i + f . phi_i, f = (0, 0, -rho g)), the cell selection of
 MechanicalPhysics::setup_dofs (solid ratio > 0.99 among the thermally
 active cells) and the zero displacement on clamped box faces, solved by a
-dense direct solve. Small meshes only.
+dense direct solve; and the J2 stress update after a solve with the state
+carried over when the cells change (J2Points, transfer_old_displacement).
+Small meshes only.
+
+The elastic part is pinned to the reference's operator and Eshelby tests.
+The J2 part has no pin (parity unpinned): the reference's own elastoplastic
+test (tests/test_mechanical_physics.cc:559-617) computes the stress but
+checks nothing; the restatement follows compute_stress line by line and is
+checked against the yield-surface consistency of its isotropic case.
 
 Vectors are component-major over the plain node grid: index c * n_nodes +
 node, node = i + nn0 (j + nn1 k).
@@ -147,3 +155,94 @@ class Elasticity:
 def cells_with_displacement(active, solid_ratio):
     """MechanicalPhysics::setup_dofs: thermally active and solid > 0.99."""
     return [int(c) for c in np.nonzero((np.asarray(active) != 0) & (np.asarray(solid_ratio) > 0.99))[0]]
+
+
+class J2Points:
+    """The stress state at the Gauss points and its update after a solve,
+    restating MechanicalPhysics::compute_stress (source/MechanicalPhysics.cc
+    :542-634, combined isotropic-kinematic J2 plasticity after Borja,
+    Plasticity, ch. 3) and the state of cells that start carrying
+    displacement (setup_dofs, :366-378; constructor :76-98).
+
+    Arrays over every cell of the mesh: kappa[C, nq] (plastic internal
+    variable), stress[6, C, nq] and back[6, C, nq] with components xx, yy,
+    zz, xy, xz, yz; nq Gauss points per cell, x fastest."""
+
+    def __init__(self, e: Elasticity, plastic_modulus, isotropic_hardening, elastic_limit):
+        self.e = e
+        C = int(np.prod(e.nc))
+        nq = len(e.jxw)
+        self.H = np.broadcast_to(np.asarray(plastic_modulus, float), (4,)).copy()
+        self.h = np.broadcast_to(np.asarray(isotropic_hardening, float), (4,)).copy()
+        self.limit = np.broadcast_to(np.asarray(elastic_limit, float), (4,)).copy()
+        self.kappa = np.repeat(self.limit[e.matid][:, None], nq, axis=1)
+        self.stress = np.zeros((6, C, nq))
+        self.back = np.zeros((6, C, nq))
+
+    def start(self, cells):
+        """Cells that start carrying displacement: the elastic limit and zero
+        stresses."""
+        for c in cells:
+            self.kappa[c, :] = self.limit[self.e.matid[c]]
+            self.stress[:, c, :] = 0.0
+            self.back[:, c, :] = 0.0
+
+    def update(self, du):
+        """The stress update from the displacement increment du (3 n_nodes,
+        component-major plain grid) at the points of the cells that carry
+        displacement."""
+        e = self.e
+        n = e.n_nodes
+        for c in e.cells:
+            m = e.matid[c]
+            lam, mu, H, h = e.lam[m], e.mu[m], self.H[m], self.h[m]
+            nodes = e.cell_nodes(c)
+            U = np.stack([np.asarray(du)[comp * n + np.asarray(nodes)] for comp in range(3)])  # [comp, node]
+            for q in range(len(e.jxw)):
+                G = U @ e.grad[q]  # [comp, d] = d u_comp / d x_d
+                eps = 0.5 * (G + G.T)
+                sig = self._tensor(self.stress[:, c, q]) + lam * np.trace(eps) * np.eye(3) + 2.0 * mu * eps
+                dev = sig - np.trace(sig) / 3.0 * np.eye(3)
+                eta = dev - self._tensor(self.back[:, c, q])
+                nrm = np.sqrt(np.sum(eta * eta))
+                kap = self.kappa[c, q]
+                if nrm < kap:
+                    self.stress[:, c, q] = self._voigt(sig)
+                    continue
+                dg = (nrm - kap) / (2.0 * mu + H)
+                nflow = eta / nrm
+                self.stress[:, c, q] = self._voigt(sig - 2.0 * mu * dg * nflow)
+                self.kappa[c, q] = kap + h * H * dg
+                # the reference's back-stress update as written (:626-630)
+                self.back[:, c, q] = self._voigt(self._tensor(self.back[:, c, q]) + (1.0 - h) * H * H * nflow)
+
+    @staticmethod
+    def _tensor(v):
+        xx, yy, zz, xy, xz, yz = v
+        return np.array([[xx, xy, xz], [xy, yy, yz], [xz, yz, zz]])
+
+    @staticmethod
+    def _voigt(t):
+        return np.array([t[0, 0], t[1, 1], t[2, 2], t[0, 1], t[0, 2], t[1, 2]])
+
+
+def transfer_old_displacement(e: Elasticity, carry_prev, carry_now, u_old):
+    """The previous displacement after the cells that carry displacement
+    changed, as MechanicalPhysics::setup_dofs writes it
+    (source/MechanicalPhysics.cc:310-337, :418-437): each cell saves its
+    nodes' old values if it carried displacement, zeros if not; the vector is
+    cleared and every cell that carries displacement now writes its saved
+    values back, in cell order."""
+    n = e.n_nodes
+    saved = {}
+    for c in range(int(np.prod(e.nc))):
+        nodes = e.cell_nodes(c)
+        saved[c] = (np.stack([np.asarray(u_old)[comp * n + np.asarray(nodes)] for comp in range(3)])
+                    if carry_prev[c] else np.zeros((3, len(nodes))))
+    out = np.zeros(3 * n)
+    for c in range(int(np.prod(e.nc))):
+        if carry_now[c]:
+            nodes = np.asarray(e.cell_nodes(c))
+            for comp in range(3):
+                out[comp * n + nodes] = saved[c][comp]
+    return out

@@ -217,3 +217,97 @@ def test_handles_of_different_degrees_coexist():
         u2 = m2.solve()
         u1 = m1.solve()
         assert close(u1, alone[1][2], 1e-10) and close(u2, alone[2][2], 1e-10)
+
+
+def elastoplastic_box(degree, material_height=1e9):
+    """The reference's elastoplastic case (tests/test_mechanical_physics.cc
+    :559-617): a 12 x 6 x 6 box of 6 x 3 x 3 cells, one solid material."""
+    cfg = amr_test_config(degree=degree, n_cells=(6, 3, 3), n_states=1)
+    cfg.geometry = Geometry(dim=3, n_cells=(6, 3, 3), extent=(12.0, 6.0, 6.0), material_height=material_height)
+    cfg.sources = []
+    return cfg
+
+
+J2_PARAMS = dict(plastic_modulus=1.5, isotropic_hardening=0.5, elastic_limit=0.1)
+
+
+def assert_state_matches(mech, j):
+    from mechanics_oracle import J2Points  # noqa: F401  (the oracle's state j)
+
+    s, b, k = (x.cpu().numpy() for x in mech.stress_state())
+    for got, ref in ((s, j.stress), (b, j.back)):
+        scale = max(np.abs(ref).max(), 1e-300)
+        assert np.abs(got - ref).max() <= 1e-11 * scale
+    fin = np.isfinite(j.kappa)
+    assert (np.isfinite(k) == fin).all()
+    assert np.abs(k[fin] - j.kappa[fin]).max() <= 1e-11 * np.abs(j.kappa[fin]).max()
+
+
+@pytest.mark.parametrize("degree", [1, 2])
+def test_elastoplastic_stress_matches_the_j2_restatement(degree):
+    """Gravity on the clamped box (lambda = 2, mu = 3, rho = 1, plastic
+    modulus 1.5, isotropic hardening 0.5, elastic limit 0.1): after the CG
+    solve the stress, back stress and plastic internal variable at every
+    Gauss point equal the restatement's update from the same displacement
+    (plastic almost everywhere), and a second identical solve (increment 0)
+    updates both the same way."""
+    from mechanics_oracle import Elasticity, J2Points
+
+    cfg = elastoplastic_box(degree)
+    phys = ThermalPhysics(cfg)
+    mech = MechanicalPhysics(phys, 2.0, 3.0, density=1.0, thermoelastic=False, gravity=True, clamped=("z-",),
+                             **J2_PARAMS)
+    C = phys.n_cells
+    e = Elasticity((6, 3, 3), (12.0, 6.0, 6.0), degree, range(C), np.zeros(C, int), [2.0] * 4, [3.0] * 4,
+                   density=[1.0] * 4, clamped_faces=1 << 4)
+    j = J2Points(e, **J2_PARAMS)
+    u_prev = np.zeros(3 * e.n_nodes)
+    for _ in range(2):
+        mech.setup_dofs()
+        u = plain(phys, mech.solve())
+        j.update(u - u_prev)
+        u_prev = u
+        assert_state_matches(mech, j)
+    assert (j.kappa > 0.1).mean() > 0.5  # the plastic branch is exercised
+
+
+def test_cells_that_start_carrying_displacement():
+    """The box with its top layer inactive, solved; the layer added, solved
+    again: the new cells start from the elastic limit and zero stresses, and
+    the displacement increment uses the previous displacement as setup_dofs
+    carries it over (the nodes the new layer shares with the old one restart
+    from 0, the new cells coming later in cell order)."""
+    from mechanics_oracle import Elasticity, J2Points, transfer_old_displacement
+
+    cfg = elastoplastic_box(1, material_height=4.0)
+    phys = ThermalPhysics(cfg)
+    T = phys.initialize_dof_vector(300.0)
+    mech = MechanicalPhysics(phys, 2.0, 3.0, density=1.0, thermoelastic=False, gravity=True, clamped=("z-",),
+                             **J2_PARAMS)
+    C = phys.n_cells
+    active1 = phys.active_cells().astype(bool)
+    assert 0 < active1.sum() < C
+
+    def elasticity(active):
+        return Elasticity((6, 3, 3), (12.0, 6.0, 6.0), 1, np.nonzero(active)[0], np.zeros(C, int), [2.0] * 4,
+                          [3.0] * 4, density=[1.0] * 4, clamped_faces=1 << 4)
+
+    e1 = elasticity(active1)
+    j = J2Points(e1, **J2_PARAMS)
+    mech.setup_dofs()
+    u1 = plain(phys, mech.solve())
+    j.update(u1)
+    assert_state_matches(mech, j)
+    new = np.nonzero(~active1)[0]
+    phys.add_material(new, 300.0, T)
+    active2 = phys.active_cells().astype(bool)
+    assert active2.all()
+    mech.setup_dofs()
+    u2 = plain(phys, mech.solve())
+    e2 = elasticity(active2)
+    u_old = transfer_old_displacement(e2, active1.astype(np.uint8), active2.astype(np.uint8), u1)
+    assert (u_old != u1).any()  # the shared nodes restarted from 0
+    j.e = e2
+    j.start(new)
+    j.update(u2 - u_old)
+    assert_state_matches(mech, j)

@@ -88,3 +88,64 @@ def test_gravity_total_force_and_melted_reference():
 
 def test_cell_selection():
     assert cells_with_displacement([1, 1, 0, 1], [1.0, 0.5, 1.0, 0.995]) == [0, 3]
+
+
+def test_j2_isotropic_return_lands_on_the_yield_surface():
+    """Purely isotropic hardening (h = 1, no back stress): after a plastic
+    step the deviatoric stress norm equals the updated plastic internal
+    variable, kappa_new = kappa + H dgamma = |dev sigma|, at every point."""
+    from mechanics_oracle import Elasticity, J2Points
+
+    e = Elasticity((2, 1, 1), (2.0, 1.0, 1.0), 1, [0, 1], np.zeros(2, int), [2.0] * 4, [3.0] * 4)
+    j = J2Points(e, 1.5, 1.0, 0.1)
+    rng = np.random.default_rng(5)
+    plastic = 0
+    for _ in range(3):
+        k0 = j.kappa.copy()
+        j.update(rng.normal(size=3 * e.n_nodes) * 0.02)
+        for c in range(2):
+            for q in range(8):
+                s = j._tensor(j.stress[:, c, q])
+                dev = s - np.trace(s) / 3.0 * np.eye(3)
+                nrm = np.sqrt(np.sum(dev * dev))
+                assert (j.back[:, c, q] == 0.0).all()
+                if j.kappa[c, q] > k0[c, q]:  # yielded in this step
+                    plastic += 1
+                    assert abs(nrm - j.kappa[c, q]) <= 1e-14 * j.kappa[c, q]
+                else:  # elastic: inside the surface
+                    assert nrm < j.kappa[c, q]
+    assert plastic > 0
+
+
+def test_j2_elastic_steps_add_up():
+    """Below the elastic limit the stress is C : (sum of the strain
+    increments): two increments give the stress of their sum."""
+    from mechanics_oracle import Elasticity, J2Points
+
+    e = Elasticity((1, 1, 2), (1.0, 1.0, 2.0), 2, [0, 1], np.zeros(2, int), [2.0] * 4, [3.0] * 4)
+    a, b = J2Points(e, 1.5, 0.5, np.inf), J2Points(e, 1.5, 0.5, np.inf)
+    rng = np.random.default_rng(6)
+    d1, d2 = rng.normal(size=3 * e.n_nodes), rng.normal(size=3 * e.n_nodes)
+    a.update(d1)
+    a.update(d2)
+    b.update(d1 + d2)
+    assert np.abs(a.stress - b.stress).max() <= 1e-12 * np.abs(b.stress).max()
+    assert np.isinf(a.kappa).all() and (a.back == 0.0).all()
+
+
+def test_old_displacement_transfer_keeps_nodes_of_the_last_old_cell():
+    """setup_dofs's write-back in cell order: a node shared by a cell that
+    carried displacement and a later one that did not restarts from 0."""
+    from mechanics_oracle import Elasticity, transfer_old_displacement
+
+    e = Elasticity((3, 1, 1), (3.0, 1.0, 1.0), 1, [0, 1, 2], np.zeros(3, int), [2.0] * 4, [3.0] * 4)
+    u = np.arange(3 * e.n_nodes, dtype=float) + 1.0
+    prev = np.array([1, 0, 0], np.uint8)  # cell 0 carried displacement
+    now = np.array([1, 1, 0], np.uint8)   # cell 1 starts carrying it
+    out = transfer_old_displacement(e, prev, now, u)
+    n = e.n_nodes
+    for g in range(n):
+        i = g % e.nn[0]
+        want = 0.0 if i >= 1 else 1.0  # x = 1 is also cell 1's (written last): 0
+        for comp in range(3):
+            assert out[comp * n + g] == (u[comp * n + g] if want else 0.0), (g, comp)
