@@ -52,3 +52,26 @@ def run_amr(problem, dt=AMR_DT, duration=AMR_DURATION, every=AMR_EVERY, n_refine
             on_step(n, t)
         n += 1
     return t
+
+
+# demo_316_short_amr.info (test_integration_3d_amr.cc:60-88): forward Euler,
+# 1e-4 s steps to 4 ms, refinement every 5 steps (and before the first), one
+# level, coarsening after the beam; the reference expects 13005 DoFs at the
+# end and a finite field.
+DEMO_AMR_DT, DEMO_AMR_DURATION, DEMO_AMR_EVERY, DEMO_AMR_DOFS = 1e-4, 4e-3, 5, 13005
+
+
+def demo_316_short_amr_config(degree=2):
+    """demo_316_short_amr.info: 25 x 25 x 2 cells of a 5 x 5 x 0.5 mm plate
+    (x length, y width, z height), FE_Q(2), convective and radiative faces,
+    the amr_test material, a Goldak 400 W beam (absorption 0.3, 0.6 mm
+    diameter, 0.5 mm depth) along demo_316_short_scan_path_amr.txt. Its
+    material deposition adds no cell: the material height (0.75 mm) is above
+    the plate, so every cell is active from the start, and the deposition
+    boxes follow the scan path 0.95 mm up, above the mesh."""
+    cfg = amr_test_config(degree=degree, n_cells=(25, 25, 2), boundary="convective,radiative")
+    cfg.geometry = Geometry(dim=3, n_cells=(25, 25, 2), extent=(5e-3, 5e-3, 5e-4), material_height=0.75e-3)
+    seg = np.load(os.path.join(HERE, "golden", "demo_316_short_amr_scan_path.npy"))
+    cfg.sources = [Source(type="goldak", depth=0.5e-3, absorption_efficiency=0.3, diameter=0.6e-3,
+                          max_power=400.0, segments=seg)]
+    return cfg

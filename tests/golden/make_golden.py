@@ -29,6 +29,12 @@ variable ADAMANTINE_REFERENCE):
   FE_Q(3) cells of 5 x 5 x 0.5 mm, one refinement along the beam every 200
   steps, 250 forward Euler steps of 1 us; expected max 329.5 K, min 296.1 K),
   as (end_time, power_modifier, x, y, z) rows.
+* demo_316_short_amr_scan_path.npy -- the segments of
+  demo_316_short_scan_path_amr.txt, the scan path of demo_316_short_amr.info
+  (test_integration_3d_amr.cc:60-88: 25 x 25 x 2 FE_Q(2) cells of 5 x 5 x
+  0.5 mm, refinement every 5 steps with coarsening after the beam, 40
+  forward Euler steps of 1e-4 s; expected 13005 DoFs at the end), as
+  (end_time, power_modifier, x, y, z) rows.
 * integration_3d_gold_short.npz -- tests/data/integration_3d_gold_short.txt
   (229570 temperatures, 6 significant digits, stored as float32, exact to
   the printed digits) of demo_316_short.info (test_integration_3d.cc:117-120:
@@ -83,6 +89,9 @@ def main():
     np.save(os.path.join(HERE, "amr_test_scan_path.npy"),
             segments(open(os.path.join(data, "bare_plate_L_scan_path_fast.txt")).read()))
     print("wrote amr_test_scan_path.npy")
+    np.save(os.path.join(HERE, "demo_316_short_amr_scan_path.npy"),
+            segments(open(os.path.join(data, "demo_316_short_scan_path_amr.txt")).read()))
+    print("wrote demo_316_short_amr_scan_path.npy")
 
     for k in (1, 2):
         name = f"microstructure_G_R_gold_{k}.txt"

@@ -73,3 +73,24 @@ def test_constrained_operator_is_symmetric_for_linear_conduction(degree):
     assert abs(z @ ax - x @ az) <= 1e-12 * abs(z @ ax)
     # the constant field is in the kernel of the conduction operator
     assert np.abs(o.vmult(np.full(o.n_dofs, 700.0))).max() <= 1e-9 * np.abs(ax).max()
+
+
+def test_reference_demo_316_short_amr_dof_count():
+    """demo_316_short_amr.info (test_integration_3d_amr.cc:60-88): FE_Q(2),
+    refinement along the beam every 5 steps with coarsening after it, 40
+    forward Euler steps of 1e-4 s. The reference expects 13005 DoFs at the
+    end (the beam is off after 2.8 ms and the mesh has coarsened back to the
+    25 x 25 x 2 grid's 51 x 51 x 5 nodes) and a finite field; the refined
+    meshes on the way have more."""
+    from amr_cases import (DEMO_AMR_DOFS, DEMO_AMR_DT, DEMO_AMR_DURATION, DEMO_AMR_EVERY,
+                           demo_316_short_amr_config)
+
+    cfg = demo_316_short_amr_config()
+    o = amr_oracle.AmrProblem(cfg, 1, initial_state=cfg.geometry.initial_state())
+    o.setup(300.0)
+    seen = []
+    run_amr(o, dt=DEMO_AMR_DT, duration=DEMO_AMR_DURATION, every=DEMO_AMR_EVERY, n_refinements=1, coarsen=True,
+            on_step=lambda n, t: seen.append(o.n_dofs))
+    assert o.n_dofs == DEMO_AMR_DOFS
+    assert np.isfinite(o.y).all()
+    assert max(seen) > DEMO_AMR_DOFS  # it was refined on the way

@@ -200,3 +200,23 @@ def test_has_melted_follows_refinement():
             while src not in old:
                 src = (src[0] + 1, 2 * src[1], 2 * src[2], 2 * src[3])
         assert f == old[src], ((l, i, j, k), src)
+
+
+def test_demo_316_short_amr_run_matches_oracle():
+    """demo_316_short_amr.info's driver loop on the GPU: the same meshes as the
+    restatement at every refinement, the reference's 13005 DoFs at the end,
+    and the field within 1e-9 of the restatement's."""
+    from amr_cases import (DEMO_AMR_DOFS, DEMO_AMR_DT, DEMO_AMR_DURATION, DEMO_AMR_EVERY,
+                           demo_316_short_amr_config)
+
+    cfg = demo_316_short_amr_config()
+    g, o = both(cfg, 1)
+    run = lambda p: run_amr(p, dt=DEMO_AMR_DT, duration=DEMO_AMR_DURATION, every=DEMO_AMR_EVERY, n_refinements=1,
+                            coarsen=True)
+    run(g)
+    run(o)
+    assert g.n_dofs == o.n_dofs == DEMO_AMR_DOFS
+    assert (g.leaves() == np.array(o.forest.sorted_leaves())).all()
+    y = g.get_solution().cpu().numpy()
+    assert np.isfinite(y).all()
+    assert np.abs(y - o.y).max() <= 1e-9 * np.abs(o.y).max()
