@@ -44,13 +44,14 @@ FP64_FLOP_PER_Q2_CELL = 2247
 # DRAM bytes (read + write) of one vmult of the 128x128x64 workload from ncu
 # captures (dram__bytes_read.sum + dram__bytes_write.sum): the atomic
 # schedule's tile-kernel launch and the two-pass schedule's tile and gather
-# launches inside the timed loop with --cache-control none (L2 as the loop
-# leaves it; means over the loop's launches), and the sum over the 8 colour
+# launches of back-to-back vmults (the autotuner's timed trials) with
+# --cache-control none (L2 as the vmult loop leaves it; means over 7
+# launches), and the sum over the 8 colour
 # launches of the coloured schedule (L2 flushed before every launch, so
 # re-reads that stay in L2 in the timed loop are counted).
 DRAM_BYTES_PER_VMULT_FULL = {"atomic": 189.9e6, "two_pass": 286.1e6, "coloured": 327.0e6}
-TRAFFIC_NOTE = {"atomic": "ncu --cache-control none, the tile-kernel launch of a timed-loop vmult",
-                "two_pass": "ncu --cache-control none, tile + gather launches of a timed-loop vmult",
+TRAFFIC_NOTE = {"atomic": "ncu --cache-control none, the tile-kernel launch of back-to-back vmults",
+                "two_pass": "ncu --cache-control none, tile + gather launches of back-to-back vmults",
                 "coloured": "ncu, L2 flushed before each of the 8 colour launches"}
 # per schedule: the dominant kernel of one vmult, its launch pattern, and
 # the number of kernel launches of one vmult of this workload (one source):
