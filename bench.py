@@ -401,7 +401,10 @@ def run_ensemble(args, dist, local_rank):
                           "atomic_member_steps_per_s": world * n * steps / (ms_la * 1e-3),
                           "speedup_vs_coloured": ms_l / ms_b, "speedup_vs_atomic": ms_la / ms_b,
                           "path": "adm_ensemble_evolve_looped: each member's stages launched one by one"},
-        "identical_results": identical, "max_rel_diff_batched_vs_looped": max_rel_diff,
+        "bit_identical_to_loops": identical, "max_rel_diff_batched_vs_looped": max_rel_diff,
+        "bit_identity_note": "the atomic schedule's FP64 reductions round in launch order; the coloured and "
+                             "two-pass schedules give batched = looped bit for bit (tests/test_gpu_ensemble.py, "
+                             "tests/test_gpu_schedule.py)",
         "batched_schedule": SCHEDULE_NAMES[schedule],
         "batched_cells_per_thread": e.cells_per_thread(),
         "batched_path": "one CUDA graph per step (4 stages)",
