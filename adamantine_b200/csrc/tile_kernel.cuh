@@ -91,6 +91,24 @@ __device__ __forceinline__ void fence_proxy_async()
 {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
+// Barrier among the N threads (a multiple of 32) that execute it with the
+// same ID (1..15; 0 is __syncthreads'); compile-time ID and count, so that
+// the kernel reserves only the barriers it names.
+template <int ID, int N>
+__device__ __forceinline__ void named_barrier()
+{
+  asm volatile("bar.sync %0, %1;" ::"n"(ID), "n"(N) : "memory");
+}
+// The barrier of z-layer group g (warp-uniform) of a tile kernel: ID 1 + g.
+template <int NG, int N>
+__device__ __forceinline__ void group_barrier(int g)
+{
+  static_assert(NG == 2, "two z-layer groups (Q2 tiles of two cell layers)");
+  if (g == 0)
+    named_barrier<1, N>();
+  else
+    named_barrier<2, N>();
+}
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned bytes)
 {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
@@ -292,7 +310,6 @@ struct SmemPhys
   int n_materials, use_table, isotropic, n_beams;
   int has_rotation, sources_here;
   int member;
-  int src_on;      // the current item's tile meets a source
   int role[2][27]; // per item parity
 };
 
@@ -955,6 +972,7 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
   int *const changed_p = reinterpret_cast<int *>(lsum + N * NCELL); // [2][NCELL]
   __shared__ SmemPhys sp;
   __shared__ __align__(8) uint64_t bars[2];
+  __shared__ int src_on_g[TD<DEG>::TZ]; // per z-layer group: the item's tile meets a source
 
   int const tid = threadIdx.x;
   int const slab = tid / NCELL, cl = tid % NCELL;
@@ -1090,10 +1108,11 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
 
     // Tile-level source culling (exact: it skips only points where every
     // source is zero by its own cutoff rules), evaluated by the first warp
-    // and published through the level-exchange barrier. A thread that
-    // writes the flag for the next item has passed the flux barrier of this
-    // one, after which nobody reads it.
-    if (tid < 32)
+    // of each z-layer group (slab 0) for its group and published through
+    // the group's level-exchange barrier. A warp that writes its group's
+    // flag for the next item has passed the node barrier of this one, after
+    // which nobody reads it.
+    if (slab == 0)
     {
       bool do_src = false;
       double const x0 = args.origin[0] + ncx0 * args.h[0];
@@ -1121,8 +1140,8 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
           continue;
         do_src = true;
       }
-      if (tid == 0)
-        sp.src_on = do_src;
+      if ((tid & 31) == 0)
+        src_on_g[lz] = do_src;
     }
 
     // ---- the cell: thread (slab, cl) handles Gauss-point level qc = slab
@@ -1164,20 +1183,13 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
       }
     }
     // 2. exchange the levels: values T and z-gradients gz (G = D S) at this
-    //    thread's Gauss-point level
+    //    thread's Gauss-point level. The N level threads of a cell are in
+    //    the cell's z-layer group (its N warps), so the exchange needs only
+    //    that group's barrier; the other group goes on.
 #pragma unroll
     for (int i = 0; i < NQS; ++i)
       xbuf[(i + NQS * slab) * NCELL + cl] = wv[i];
-    if (__syncthreads_or(!arrived))
-    {
-      if (tid == 0)
-      {
-        atomicCAS(md.error, 0, (int)DERR_TMA_TIMEOUT);
-        // let the late copy land before the CTA leaves (bounded as well)
-        mbar_wait(&bars[buf], (unsigned)((it >> 1) & 1));
-      }
-      return;
-    }
+    group_barrier<TZ, NT / TZ>(lz);
     // prefetch the next item's brick into the other buffer, and claim the
     // item after it (read at the start of the next item, after this item's
     // flux and node barriers; the slot's previous value was read at the
@@ -1192,7 +1204,7 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
       if (dyn)
         claimed[it & 1] = next < last ? atomicAdd(args.claim, 1) + (int)gridDim.x : last;
     }
-    bool const do_src = sp.src_on != 0;
+    bool const do_src = src_on_g[lz] != 0;
     double Tq[NQS], az[NQS];
     // (a warp-uniform branch: a warp's threads share the level)
     if (slab == 0)
@@ -1367,7 +1379,7 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
       pzbuf[(i + NQS * slab) * NCELL + cl] = axy[i];
       pzbuf[(NN + i + NQS * slab) * NCELL + cl] = az[i];
     }
-    __syncthreads();
+    group_barrier<TZ, NT / TZ>(lz); // the flux exchange: the z-layer group
     double res[NQS];
     if (slab == 0)
       z_integrate<DEG, 0, NCELL>(args, axy, az, pzbuf, cl, res);
@@ -1419,7 +1431,22 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
       for (int i = 0; i < NQS; ++i)
         mbuf[i * NCELL + cl] = res[i];
     }
-    __syncthreads();
+    // the node barrier (the whole CTA) carries the brick-timeout vote: a
+    // thread whose wait gave up computed on whatever the buffer held, and
+    // the CTA ends here, before anything is written
+    if (__syncthreads_or(!arrived))
+    {
+      if (tid == 0)
+      {
+        atomicCAS(md.error, 0, (int)DERR_TMA_TIMEOUT);
+        // let the late copy, and the one requested for the next item, land
+        // before the CTA leaves (bounded as well)
+        mbar_wait(&bars[buf], (unsigned)((it >> 1) & 1));
+        if (next < last)
+          mbar_wait(&bars[buf ^ 1], (unsigned)(((it + 1) >> 1) & 1));
+      }
+      return;
+    }
     if (slab == DEG && lz < TZ - 1)
     {
 #pragma unroll
