@@ -687,9 +687,8 @@ __global__ void __launch_bounds__(Q1Col::NT, Q1Col::MINB)
     mbar_arrive_expect_tx(&bars[b], kBoxBytes);
     tma_load_brick(smem + b * Q::BRICKP, &tmap, TX * tix, TY * tiy, TZ * tiz, wi.member, &bars[b]);
   };
-  // the cell data of cell (lx, ly, kz) of item `item` (zeros outside the mesh)
-  auto load_cell = [&](int item, int kz, uint32_t &info, int &pmode, double &pu) {
-    TileWork const wk = args.work[item];
+  // the cell data of cell (lx, ly, kz) of work item wk (zeros outside the mesh)
+  auto load_cell = [&](TileWork const &wk, int kz, uint32_t &info, int &pmode, double &pu) {
     MemberData const &mk = args.members[wk.member];
     int const kx = TX * (int)(wk.xyz & 2047u) + lx, ky = TY * (int)((wk.xyz >> 11) & 2047u) + ly;
     int const kzz = TZ * (int)(wk.xyz >> 22) + kz;
@@ -747,12 +746,17 @@ __global__ void __launch_bounds__(Q1Col::NT, Q1Col::MINB)
   __syncwarp();
   second = __shfl_sync(full, second, 0);
 
-  // cell data of the next cell to compute, one cell ahead
+  // the work item (loaded one item ahead) and the cell data of the next
+  // cell to compute (one cell ahead)
+  TileWork w_cur{0, 0, 0u}, w_next{0, 0, 0u};
   uint32_t nx_info = 0u;
   int nx_pmode = 0;
   double nx_pu = 0.0;
   if (first < last)
-    load_cell(first, 0, nx_info, nx_pmode, nx_pu);
+  {
+    w_cur = args.work[first];
+    load_cell(w_cur, 0, nx_info, nx_pmode, nx_pu);
+  }
 
   int it = 0, buf = 0;
   unsigned phase = 0;
@@ -767,7 +771,9 @@ __global__ void __launch_bounds__(Q1Col::NT, Q1Col::MINB)
       claimed[it & 1] = next2;
     }
     next2 = __shfl_sync(full, next2, 0);
-    TileWork const w = args.work[item];
+    TileWork const w = w_cur;
+    if (next < last)
+      w_next = args.work[next]; // used by the last cell's prefetch and the next item
     MemberData const &md = args.members[w.member];
     int const tile = w.tile;
     int const tix = w.xyz & 2047u, tiy = (w.xyz >> 11) & 2047u, tiz = w.xyz >> 22;
@@ -821,9 +827,9 @@ __global__ void __launch_bounds__(Q1Col::NT, Q1Col::MINB)
         double const pu = nx_pu;
         // prefetch the cell above (or the next item's first cell)
         if (k + 1 < TZ)
-          load_cell(item, k + 1, nx_info, nx_pmode, nx_pu);
+          load_cell(w, k + 1, nx_info, nx_pmode, nx_pu);
         else if (next < last)
-          load_cell(next, 0, nx_info, nx_pmode, nx_pu);
+          load_cell(w_next, 0, nx_info, nx_pmode, nx_pu);
         double cres[8];
         q1_cell<NS, P, FC>(sp, md, args, brick, lx, ly, k, ncx0, ncy0, ncz0, info, pmode, pu, true, do_src,
                            cres);
@@ -900,6 +906,7 @@ __global__ void __launch_bounds__(Q1Col::NT, Q1Col::MINB)
       buf = 0;
       phase ^= 1u;
     }
+    w_cur = w_next;
     item = next;
   }
 }
