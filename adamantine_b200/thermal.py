@@ -257,8 +257,8 @@ class ThermalPhysics:
         return int(v.value)
 
     def autotune(self, field: torch.Tensor):
-        """Times every schedule (and, for FE degree 1, both cells-per-thread
-        variants) on vmults of field, keeps the fastest; returns (schedule,
+        """Times every schedule (and, for FE degree 1, every cells-per-thread
+        variant) on vmults of field, keeps the fastest; returns (schedule,
         [best ms coloured, atomic, two-pass])."""
         c = ctypes.c_int32()
         ms = np.zeros(3)

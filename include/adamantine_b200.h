@@ -224,8 +224,8 @@ int adm_get_schedule(adm_thermal const *h, int32_t *schedule);
  * variant is bit-reproducible in the coloured and two-pass schedules. */
 int adm_set_cells_per_thread(adm_thermal *h, int32_t n);
 int adm_get_cells_per_thread(adm_thermal const *h, int32_t *n);
-/* Autotuner: times every schedule (and, for FE degree 1, both cells-per-
- * thread variants) on vmults of the device field (the phase history is
+/* Autotuner: times every schedule (and, for FE degree 1, every cells-per-
+ * thread variant) on vmults of the device field (the phase history is
  * restored afterwards), keeps the fastest in the handle and returns its
  * schedule in *schedule; ms[2] (may be NULL) receives the best per-vmult
  * times of the coloured and atomic schedules. */
