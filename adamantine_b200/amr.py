@@ -249,9 +249,10 @@ class AmrThermalPhysics(_Common):
         return out
 
     def set_schedule(self, schedule: str):
-        """'atomic' (default: one launch per level and application) or
-        'coloured' (eight launches, a fixed order of additions)."""
-        self._call("set_schedule", {"coloured": 0, "atomic": 1}[schedule])
+        """'atomic' (default: one launch per level and application),
+        'coloured' (eight launches) or 'two_pass' (a tile launch and a
+        gather); the last two add in a fixed order."""
+        self._call("set_schedule", {"coloured": 0, "atomic": 1, "two_pass": 2}[schedule])
 
     def synchronize(self):
         self._call("synchronize")

@@ -869,10 +869,12 @@ public:
   }
 
   // Level-grid schedule (coloured: 8 launches per level and application,
-  // deterministic; atomic: 1 launch, additions in any order).
+  // deterministic; atomic: 1 launch, additions in any order; two-pass: a
+  // tile launch and a gather, deterministic).
   void set_schedule(int schedule)
   {
-    if (schedule != Thermal::kScheduleColoured && schedule != Thermal::kScheduleAtomic)
+    if (schedule != Thermal::kScheduleColoured && schedule != Thermal::kScheduleAtomic &&
+        schedule != Thermal::kScheduleTwoPass)
       throw Error(ADM_ERR_INVALID, "unknown schedule");
     schedule_ = schedule;
     drop_graph();

@@ -120,7 +120,8 @@ int adm_amr_level_layout(adm_amr *h, int level, int64_t nodes[3], int64_t *pitch
 int adm_amr_level_cell_state(adm_amr *h, int level, double *host);
 /* Launch schedule of the level grids (adm_set_schedule's values): the
  * atomic schedule (default) launches once per level and application, the
- * coloured one eight times and adds in a fixed order (bit-reproducible). */
+ * coloured one eight times and the two-pass one a tile launch and a gather,
+ * both adding in a fixed order (bit-reproducible). */
 int adm_amr_set_schedule(adm_amr *h, int schedule);
 /* ThermalPhysics::mark_has_melted on the refined mesh: every leaf whose
  * cell average of the solution exceeds threshold is flagged (flags stay

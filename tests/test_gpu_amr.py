@@ -52,11 +52,15 @@ def test_constrained_operator_and_mass_match_oracle(degree, boundary):
         g.vmult(dst, src)
         ref = o.vmult(y)
         assert np.abs(dst.cpu().numpy() - ref).max() <= 1e-10 * np.abs(ref).max()
-        g.set_schedule("coloured")
-        dst_c = torch.zeros_like(src)
-        g.vmult(dst_c, src)
+        for sch in ("coloured", "two_pass"):
+            g.set_schedule(sch)
+            dst_c = torch.zeros_like(src)
+            g.vmult(dst_c, src)
+            dst_r = torch.zeros_like(src)
+            g.vmult(dst_r, src)
+            assert torch.equal(dst_c, dst_r)  # a fixed order of additions
+            assert torch.abs(dst_c - dst).max().item() <= 1e-12 * np.abs(ref).max()
         g.set_schedule("atomic")
-        assert torch.abs(dst_c - dst).max().item() <= 1e-12 * np.abs(ref).max()
 
 
 @pytest.mark.parametrize("degree,method", [(2, "forward_euler"), (1, "forward_euler"), (2, "rk_third_order")])
