@@ -54,6 +54,8 @@ SIGNATURES = {
     "adm_autotune": [_VP, _VP, _I32, _D],
     "adm_autotune_schedules": [_VP, _VP, _I32, _D, ctypes.c_int32],
     "adm_set_cells_per_thread": [_VP, ctypes.c_int32],
+    "adm_set_cells_per_block": [_VP, ctypes.c_int32],
+    "adm_get_cells_per_block": [_VP, _I32],
     "adm_get_cells_per_thread": [_VP, _I32],
     "adm_save_checkpoint": [_VP, ctypes.c_char_p, ctypes.c_double, _VP],
     "adm_load_checkpoint": [_VP, ctypes.c_char_p, ctypes.c_int32, _D, _VP],

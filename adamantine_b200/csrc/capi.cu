@@ -293,6 +293,22 @@ int adm_get_cells_per_thread(adm_thermal const *h, int32_t *n)
   });
 }
 
+int adm_set_cells_per_block(adm_thermal *h, int32_t n)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h, "null handle");
+    as(h)->set_cells_per_block(n);
+  });
+}
+
+int adm_get_cells_per_block(adm_thermal const *h, int32_t *n)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && n, "null argument");
+    *n = as(h)->cells_per_block();
+  });
+}
+
 int adm_autotune_schedules(adm_thermal *h, double const *field, int32_t *schedule, double *ms, int32_t n_ms)
 {
   return adm::guard([&] {

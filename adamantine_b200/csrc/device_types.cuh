@@ -157,8 +157,9 @@ struct KernelArgs
   int blocked;  // 1: each CTA takes one contiguous run of work items
   int *claim;   // non-null: items after each CTA's first are claimed from this
                 // counter (zero at the launch), dynamic load balance
-  int cells_per_thread; // FE_Q(1) cell kernel: 1 or 2 cells (stacked in z) per thread
+  int cells_per_thread; // FE_Q(1) cell kernel: 1, 2 (stacked in z) or 4 (the column variant) per thread
   int two_pass;         // two-pass schedule: owners write, upper-face partial sums to md.halo
+  int tile_pairs;       // atomic FE_Q(2): work items are z-pairs of tiles (128-cell blocks)
   int stage;
   int last;     // last stage of the step (updates y)
   int n_stages; // 1 forward Euler

@@ -831,7 +831,7 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 // Tensor map of node vectors for the TMA brick loads: a 4D box of
 // (BXP, BY, BZ, 1) nodes over the (nn0, nn1, nn2, members) array with row
 // pitch `pitch` and member_stride doubles between members.
-CUtensorMap brick_map(Mesh const &m, double const *base, int n_members, size_t member_stride)
+CUtensorMap brick_map(Mesh const &m, double const *base, int n_members, size_t member_stride, int tz_cells)
 {
   CUtensorMap map;
   std::memset(&map, 0, sizeof(map));
@@ -857,7 +857,7 @@ CUtensorMap brick_map(Mesh const &m, double const *base, int n_members, size_t m
   {
     box[0] = TD<2>::BXP;
     box[1] = TD<2>::BY;
-    box[2] = TD<2>::BZ;
+    box[2] = tz_cells > 0 ? (cuuint32_t)(2 * tz_cells + 1) : (cuuint32_t)TD<2>::BZ;
   }
   cuuint32_t const elem[4] = {1, 1, 1, 1};
   CUresult const r = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double *>(base), dims,
@@ -893,16 +893,28 @@ void Thermal::launch_pass(KernelArgs a, double const *src)
   if (schedule_ == kScheduleAtomic)
   {
     // one launch over every tile (the ascending list), items strided over
-    // the CTAs (measured faster here than claiming them from a counter)
-    int const count = colour_off_[8];
+    // the CTAs (measured faster here than claiming them from a counter);
+    // with 128-cell blocks over the z-pairs of tiles
+    int count = colour_off_[8];
     size_t const N = mesh_.n_nodes;
     a.atomic = 1;
+    CUtensorMap map_used = map;
+    if (cells_per_block_ == 128)
+    {
+      build_pair_list();
+      count = (int)pwork_.size();
+      a.tile_pairs = 1;
+      a.nt[2] = (mesh_.nt[2] + 1) / 2;
+      a.work = pwork_d_.p;
+      map_used = brick_map(mesh_, src, 1, mesh_.n_nodes, 2 * mesh_.tz);
+    }
     if (a.mode == 2)
       launch_zero_keep(acc_p_, N, stream_, fold_prepare_c_ >= 0.0 ? member_d_.p : nullptr, 1, fold_prepare_c_);
     if (count > 0)
     {
-      a.work = awork_d_.p;
-      launch_tile(mesh_.deg, ns_, poly_p_, map, a, count, stream_);
+      if (!a.tile_pairs)
+        a.work = awork_d_.p;
+      launch_tile(mesh_.deg, ns_, poly_p_, map_used, a, count, stream_);
       ADM_CK(cudaGetLastError());
     }
     if (a.mode == 2)
@@ -1545,6 +1557,52 @@ void Thermal::build_atomic_list(std::vector<uint8_t> const &tile_active)
                            stream_));
 }
 
+void Thermal::set_cells_per_block(int n)
+{
+  int const tile = mesh_.tx * mesh_.ty * mesh_.tz;
+  if (n != tile && !(mesh_.deg == 2 && n == 2 * tile))
+    throw Error(ADM_ERR_INVALID, "cells per block: the tile's (64 for FE_Q(2), 128 for FE_Q(1)) or, for FE_Q(2), "
+                                 "128 (z-pairs of tiles)");
+  int const v = n == tile ? 0 : n;
+  if (v != cells_per_block_ && step_graph_)
+  {
+    cudaGraphExecDestroy(step_graph_);
+    step_graph_ = nullptr;
+  }
+  cells_per_block_ = v;
+}
+
+// The z-pairs (tiles at layers 2p and 2p + 1) that hold an active tile, for
+// the 128-cell blocks of the atomic schedule: x fastest, bottom pairs first
+// (the order of the atomic schedule's tile list).
+void Thermal::build_pair_list()
+{
+  if (pwork_version_ == work_version_ && !pwork_.empty())
+    return;
+  pwork_.clear();
+  int const nt0 = mesh_.nt[0], nt1 = mesh_.nt[1], nt2 = mesh_.nt[2];
+  std::vector<uint8_t> const &ta = topo_.tile_active;
+  for (int p = 0; 2 * p < nt2; ++p)
+    for (int ty = 0; ty < nt1; ++ty)
+      for (int tx = 0; tx < nt0; ++tx)
+      {
+        size_t const t0 = tx + (size_t)nt0 * (ty + (size_t)nt1 * (2 * p));
+        size_t const t1 = t0 + (size_t)nt0 * nt1;
+        if (!ta[t0] && !(2 * p + 1 < nt2 && ta[t1]))
+          continue;
+        TileWork w;
+        w.member = 0;
+        w.tile = (int32_t)t0;
+        w.xyz = pack_tile(tx, ty, p);
+        pwork_.push_back(w);
+      }
+  pwork_d_.alloc(std::max<size_t>(1, pwork_.size()));
+  if (!pwork_.empty())
+    ADM_CK(cudaMemcpyAsync(pwork_d_.p, pwork_.data(), pwork_.size() * sizeof(TileWork), cudaMemcpyHostToDevice,
+                           stream_));
+  pwork_version_ = work_version_;
+}
+
 void Thermal::set_cells_per_thread(int n)
 {
   if (n != 1 && n != 2 && n != 4)
@@ -1631,58 +1689,78 @@ int Thermal::autotune(double const *field, double *ms_out)
   cudaEvent_t e0, e1;
   ADM_CK(cudaEventCreate(&e0));
   ADM_CK(cudaEventCreate(&e1));
-  int const saved = schedule_, saved_cz = cells_per_thread_;
+  int const saved = schedule_, saved_cz = cells_per_thread_, saved_cpb = cells_per_block_;
   double best = 0.0;
-  int choice = saved, choice_cz = saved_cz;
-  // launch schedules x (FE_Q(1)) cells per thread; ms_out[schedule] is the
+  int choice = saved, choice_cz = saved_cz, choice_cpb = saved_cpb;
+  // launch schedules x kernel variants (FE_Q(1): cells per thread; FE_Q(2),
+  // atomic schedule: 64- or 128-cell blocks); ms_out[schedule] is the
   // schedule's best time. An untimed round over every variant first: the
   // first launches of each kernel and the clock ramp of an idle GPU would
   // otherwise fall on the first variant timed.
+  struct Variant
+  {
+    int sch, cz, cpb;
+  };
+  std::vector<Variant> variants;
   for (int sch : {kScheduleColoured, kScheduleAtomic, kScheduleTwoPass})
-    for (int cz : {1, 2, 4})
+  {
+    if (mesh_.deg == 1)
+      for (int cz : {1, 2, 4})
+        variants.push_back({sch, cz, 0});
+    else
     {
-      if (cz != 1 && mesh_.deg != 1)
-        continue;
-      schedule_ = sch;
-      cells_per_thread_ = cz;
-      for (int r = 0; r < 2; ++r)
-        vmult(dst.p, field, false);
+      variants.push_back({sch, 1, 0});
+      if (sch == kScheduleAtomic)
+        variants.push_back({sch, 1, 128});
     }
-  for (int sch : {kScheduleColoured, kScheduleAtomic, kScheduleTwoPass})
-    for (int cz : {1, 2, 4})
+  }
+  auto select = [&](Variant const &v) {
+    schedule_ = v.sch;
+    cells_per_thread_ = v.cz;
+    cells_per_block_ = v.cpb;
+  };
+  for (Variant const &v : variants)
+  {
+    select(v);
+    for (int r = 0; r < 2; ++r)
+      vmult(dst.p, field, false);
+  }
+  bool first_of[3] = {true, true, true}; // per schedule
+  for (Variant const &v : variants)
+  {
+    select(v);
+    for (int r = 0; r < 2; ++r)
+      vmult(dst.p, field, false);
+    ADM_CK(cudaEventRecord(e0, stream_));
+    int const reps = 5;
+    for (int r = 0; r < reps; ++r)
+      vmult(dst.p, field, false);
+    ADM_CK(cudaEventRecord(e1, stream_));
+    ADM_CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    ADM_CK(cudaEventElapsedTime(&ms, e0, e1));
+    double const per = ms / reps;
+    if (ms_out && (first_of[v.sch] || per < ms_out[v.sch]))
+      ms_out[v.sch] = per;
+    first_of[v.sch] = false;
+    if (best == 0.0 || per < best)
     {
-      if (cz != 1 && mesh_.deg != 1)
-        continue;
-      schedule_ = sch;
-      cells_per_thread_ = cz;
-      for (int r = 0; r < 2; ++r)
-        vmult(dst.p, field, false);
-      ADM_CK(cudaEventRecord(e0, stream_));
-      int const reps = 5;
-      for (int r = 0; r < reps; ++r)
-        vmult(dst.p, field, false);
-      ADM_CK(cudaEventRecord(e1, stream_));
-      ADM_CK(cudaEventSynchronize(e1));
-      float ms = 0.f;
-      ADM_CK(cudaEventElapsedTime(&ms, e0, e1));
-      double const per = ms / reps;
-      if (ms_out && (cz == 1 || per < ms_out[sch]))
-        ms_out[sch] = per;
-      if (best == 0.0 || per < best)
-      {
-        best = per;
-        choice = sch;
-        choice_cz = cz;
-      }
+      best = per;
+      choice = v.sch;
+      choice_cz = v.cz;
+      choice_cpb = v.cpb;
     }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   schedule_ = saved;
   cells_per_thread_ = saved_cz;
+  cells_per_block_ = saved_cpb;
   restore_phase(snap);
   ADM_CK(cudaStreamSynchronize(stream_));
   set_schedule(choice);
   set_cells_per_thread(choice_cz);
+  set_cells_per_block(choice_cpb == 0 ? mesh_.tx * mesh_.ty * mesh_.tz : choice_cpb);
   return choice;
 }
 

@@ -150,7 +150,8 @@ CellTopology build_topology(Mesh const &mesh, std::vector<uint8_t> const &active
 // Tensor map of n_members node vectors laid out member after member,
 // member_stride doubles apart (1 member: one vector), for the 4D TMA brick
 // loads of the tile kernel.
-CUtensorMap brick_map(Mesh const &m, double const *base, int n_members, size_t member_stride);
+// tz_cells: cell layers per block (0: the degree's tile depth)
+CUtensorMap brick_map(Mesh const &m, double const *base, int n_members, size_t member_stride, int tz_cells = 0);
 // Tile kernel launch for one colour's work list.
 void launch_tile(int deg, int ns, int p, CUtensorMap const &map, KernelArgs const &a, int n_items,
                  cudaStream_t stream);
@@ -268,10 +269,15 @@ public:
   static constexpr int kScheduleColoured = 0, kScheduleAtomic = 1, kScheduleTwoPass = 2;
   void set_schedule(int schedule);
   int schedule() const { return schedule_; }
-  // FE_Q(1) operator kernel: 1 or 2 cells (stacked in z) per thread
+  // FE_Q(1) operator kernel: 1, 2 (stacked in z) or 4 (the column variant)
+  // cells per thread
   void set_cells_per_thread(int n);
   void build_atomic_list(std::vector<uint8_t> const &tile_active);
   int cells_per_thread() const { return cells_per_thread_; }
+  // FE_Q(2) operator kernel: cells per block, 64 (one tile, every schedule)
+  // or 128 (a z-pair of tiles, the atomic schedule)
+  void set_cells_per_block(int n);
+  int cells_per_block() const { return cells_per_block_ ? cells_per_block_ : mesh_.tx * mesh_.ty * mesh_.tz; }
   // times both schedules on vmults of `field` (phase history restored) and
   // keeps the faster; ms_out[2] (may be null) receives the per-vmult times
   int autotune(double const *field, double *ms_out);
@@ -324,6 +330,7 @@ private:
   double op_time_ = 0.0;
   int schedule_ = kScheduleColoured;
   int cells_per_thread_ = 1;
+  int cells_per_block_ = 0; // 0: the tile (FE_Q(2): 64 cells)
   Tableau tab_;
 
   std::vector<uint8_t> active_, matid_, init_state_, has_melted_;
@@ -366,6 +373,11 @@ private:
   std::vector<TileWork> zwork_;
   DevBuf<TileWork> zwork_d_;
   uint64_t work_version_ = 0, zwork_version_ = ~0ull;
+  // 128-cell blocks: z-pairs of tiles with an active tile, bottom first
+  std::vector<TileWork> pwork_;
+  DevBuf<TileWork> pwork_d_;
+  uint64_t pwork_version_ = ~0ull;
+  void build_pair_list();
   cudaStream_t copy_in_ = nullptr, copy_out_ = nullptr;
   cudaEvent_t pipe_ev_[2 * kPipeChunks + 2] = {};
 

@@ -44,17 +44,20 @@ struct TileShape<2>
   static constexpr int TX = 8, TY = 4, TZ = 2;
 };
 
-template <int DEG>
+// Block dimensions of the tile kernels: the tile shape of the degree, or a
+// block of TZO cell layers (FE_Q(2): 4, a z-pair of tiles, in the atomic
+// schedule's 128-cell variant).
+template <int DEG, int TZO = TileShape<DEG>::TZ>
 struct TD
 {
   static constexpr int N = DEG + 1; // nodes / Gauss points per direction
-  static constexpr int TX = TileShape<DEG>::TX, TY = TileShape<DEG>::TY,
-                       TZ = TileShape<DEG>::TZ;
+  static constexpr int TX = TileShape<DEG>::TX, TY = TileShape<DEG>::TY, TZ = TZO;
   static constexpr int NCELL = TX * TY * TZ;
   // N threads per cell: thread (slab s, cell c) owns the Gauss points and the
   // nodes of z-level s of cell c
   static constexpr int NT = NCELL * N;
-  static constexpr int MINB = 2; // resident CTAs per SM the register budget targets
+  // resident CTAs per SM the register budget targets (168 registers)
+  static constexpr int MINB = NT > 256 ? 1 : 2;
   static constexpr int BX = DEG * TX + 1, BY = DEG * TY + 1, BZ = DEG * TZ + 1;
   // x extent of the TMA box: a multiple of 16 bytes
   static constexpr int BXP = (BX + 1) / 2 * 2;
@@ -103,11 +106,15 @@ __device__ __forceinline__ void named_barrier()
 template <int NG, int N>
 __device__ __forceinline__ void group_barrier(int g)
 {
-  static_assert(NG == 2, "two z-layer groups (Q2 tiles of two cell layers)");
+  static_assert(NG == 2 || NG == 4, "two or four z-layer groups");
   if (g == 0)
     named_barrier<1, N>();
-  else
+  else if (NG == 2 || g == 1)
     named_barrier<2, N>();
+  else if (g == 2)
+    named_barrier<3, N>();
+  else
+    named_barrier<4, N>();
 }
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned bytes)
 {
@@ -954,11 +961,11 @@ __device__ __forceinline__ void load_member_constants(SmemPhys &sp, MemberData c
 // other buffer while the current item is computed.
 // FC: the problem has convective / radiative faces (instantiated apart so
 // that adiabatic problems carry no face code).
-template <int DEG, int NS, int P, int SC, bool FC>
-__global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
+template <int DEG, int NS, int P, int SC, bool FC, int TZO = TileShape<DEG>::TZ>
+__global__ void __launch_bounds__(TD<DEG, TZO>::NT, TD<DEG, TZO>::MINB)
     tile_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ KernelArgs args, int n_items)
 {
-  using T_ = TD<DEG>;
+  using T_ = TD<DEG, TZO>;
   constexpr int N = T_::N, NN = T_::NN, NT = T_::NT, NCELL = T_::NCELL, NQS = T_::NQS;
   constexpr int TX = T_::TX, TY = T_::TY, TZ = T_::TZ;
   constexpr int BX = T_::BX, BY = T_::BY, BZ = T_::BZ, BXP = T_::BXP;
@@ -972,7 +979,7 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
   int *const changed_p = reinterpret_cast<int *>(lsum + N * NCELL); // [2][NCELL]
   __shared__ SmemPhys sp;
   __shared__ __align__(8) uint64_t bars[2];
-  __shared__ int src_on_g[TD<DEG>::TZ]; // per z-layer group: the item's tile meets a source
+  __shared__ int src_on_g[T_::TZ]; // per z-layer group: the item's tile meets a source
 
   int const tid = threadIdx.x;
   int const slab = tid / NCELL, cl = tid % NCELL;
@@ -1534,40 +1541,50 @@ __global__ void __launch_bounds__(TD<DEG>::NT, TD<DEG>::MINB)
 
 // Launches the persistent tile kernel over n_items work items with at most
 // the number of CTAs that are resident at once on the device.
-template <int DEG, int NS, int P, int SC, bool FC>
+template <int DEG, int NS, int P, int SC, bool FC, int TZO = TileShape<DEG>::TZ>
 void launch_tile_f(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
 {
+  using T_ = TD<DEG, TZO>;
   static int grid_cap = 0;
   if (grid_cap == 0)
   {
-    cudaFuncSetAttribute(tile_kernel<DEG, NS, P, SC, FC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)TD<DEG>::SMEM);
+    cudaFuncSetAttribute(tile_kernel<DEG, NS, P, SC, FC, TZO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)T_::SMEM);
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_kernel<DEG, NS, P, SC, FC>, TD<DEG>::NT,
-                                                  TD<DEG>::SMEM);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_kernel<DEG, NS, P, SC, FC, TZO>, T_::NT, T_::SMEM);
     grid_cap = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
   }
   int const grid = n_items < grid_cap ? n_items : grid_cap;
-  tile_kernel<DEG, NS, P, SC, FC><<<grid, TD<DEG>::NT, TD<DEG>::SMEM, stream>>>(map, a, n_items);
+  tile_kernel<DEG, NS, P, SC, FC, TZO><<<grid, T_::NT, T_::SMEM, stream>>>(map, a, n_items);
 }
 
-template <int DEG, int NS, int P, int SC>
+template <int DEG, int NS, int P, int SC, int TZO = TileShape<DEG>::TZ>
 void launch_tile_s(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
 {
   if (a.faces)
-    launch_tile_f<DEG, NS, P, SC, true>(map, a, n_items, stream);
+    launch_tile_f<DEG, NS, P, SC, true, TZO>(map, a, n_items, stream);
   else
-    launch_tile_f<DEG, NS, P, SC, false>(map, a, n_items, stream);
+    launch_tile_f<DEG, NS, P, SC, false, TZO>(map, a, n_items, stream);
 }
 
-// The schedule of a launch: a.atomic, else a.two_pass, else coloured.
+// The schedule of a launch: a.atomic, else a.two_pass, else coloured; an
+// atomic launch with a.tile_pairs runs 128-cell blocks over z-pairs of tiles
+// (FE_Q(2)).
 template <int DEG, int NS, int P>
 void launch_tile_t(CUtensorMap const &map, KernelArgs const &a, int n_items, cudaStream_t stream)
 {
   if (a.atomic)
+  {
+    if constexpr (DEG == 2)
+      if (a.tile_pairs)
+      {
+        launch_tile_s<DEG, NS, P, SC_ATOMIC, 2 * TileShape<DEG>::TZ>(map, a, n_items, stream);
+        return;
+      }
     launch_tile_s<DEG, NS, P, SC_ATOMIC>(map, a, n_items, stream);
+  }
   else if (a.two_pass)
     launch_tile_s<DEG, NS, P, SC_TWO_PASS>(map, a, n_items, stream);
   else

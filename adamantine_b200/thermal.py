@@ -256,6 +256,16 @@ class ThermalPhysics:
         _lib.check(self._L.adm_get_cells_per_thread(self._h, ctypes.byref(v)))
         return int(v.value)
 
+    def set_cells_per_block(self, n: int):
+        """FE_Q(2) operator kernel variant: 64 cells per block (one tile,
+        every schedule) or 128 (a z-pair of tiles, the atomic schedule)."""
+        _lib.check(self._L.adm_set_cells_per_block(self._h, int(n)))
+
+    def cells_per_block(self) -> int:
+        v = ctypes.c_int32()
+        _lib.check(self._L.adm_get_cells_per_block(self._h, ctypes.byref(v)))
+        return int(v.value)
+
     def autotune(self, field: torch.Tensor):
         """Times every schedule (and, for FE degree 1, every cells-per-thread
         variant) on vmults of field, keeps the fastest; returns (schedule,

@@ -224,8 +224,16 @@ int adm_get_schedule(adm_thermal const *h, int32_t *schedule);
  * variant is bit-reproducible in the coloured and two-pass schedules. */
 int adm_set_cells_per_thread(adm_thermal *h, int32_t n);
 int adm_get_cells_per_thread(adm_thermal const *h, int32_t *n);
-/* Autotuner: times every schedule (and, for FE degree 1, every cells-per-
- * thread variant) on vmults of the device field (the phase history is
+/* Cells per block of the FE_Q(2) operator kernel (no counterpart in the
+ * reference): 64 (default, one 8 x 4 x 2 tile per CTA of 192 threads, every
+ * schedule) or 128 (a z-pair of tiles per CTA of 384 threads, one CTA per
+ * SM, the atomic schedule; the other schedules keep 64). FE_Q(1) takes 128,
+ * its tile. */
+int adm_set_cells_per_block(adm_thermal *h, int32_t n);
+int adm_get_cells_per_block(adm_thermal const *h, int32_t *n);
+/* Autotuner: times every schedule and kernel variant (FE degree 1: cells per
+ * thread; FE degree 2, atomic schedule: cells per block) on vmults of the
+ * device field (the phase history is
  * restored afterwards), keeps the fastest in the handle and returns its
  * schedule in *schedule; ms[2] (may be NULL) receives the best per-vmult
  * times of the coloured and atomic schedules. */

@@ -186,3 +186,59 @@ def test_two_cells_per_thread_is_a_q1_variant():
         g.set_cells_per_thread(4)
     with pytest.raises(Exception):
         g.set_cells_per_thread(3)
+
+
+Q2_CASES = [c for c in CASES if c.startswith("q2_")]
+
+
+@pytest.mark.parametrize("name", Q2_CASES)
+def test_q2_128_cell_blocks(name):
+    """The FE_Q(2) kernel variant with 128-cell blocks (z-pairs of tiles, the
+    atomic schedule): the same bars against the oracle (three vmults with
+    their phase history, 12 time steps), with faces and partial activation
+    (pairs with one inactive tile) among the cases."""
+    cfg, cells, T = make_case(name)
+    o = make_oracle(cfg, cells)
+    g = make_gpu(cfg, cells)
+    g.set_schedule(1)
+    g.set_cells_per_block(128)
+    assert g.cells_per_block() == 128
+    o.set_time(2e-5)
+    g.set_time(2e-5)
+    dst = g.initialize_dof_vector()
+    for k in range(3):
+        Tk = T * (1.0 + 0.05 * k)
+        g.vmult(dst, g.from_grid(Tk))
+        assert rel_max(grid(g.to_grid(dst)), o.vmult(grid(Tk))) <= VMULT_TOL, k
+    if cfg.material.n_states == 3:
+        assert np.max(np.abs(g.get_qp_powder() - o.qp_powder())) < 1e-12
+    o2 = make_oracle(cfg, cells)
+    g2 = make_gpu(cfg, cells)
+    g2.set_schedule(1)
+    g2.set_cells_per_block(128)
+    y_ref = grid(T).copy()
+    y = g2.from_grid(T)
+    t_ref = t = 1e-5
+    for _ in range(12):
+        t_ref = o2.evolve_one_time_step(t_ref, 2e-6, y_ref)
+        t = g2.evolve_one_time_step(t, 2e-6, y)
+    assert rel_max(grid(g2.to_grid(y)), y_ref) <= STEP_TOL
+    assert g.device_error() == 0 and g2.device_error() == 0
+
+
+def test_cells_per_block_values():
+    cfg, cells, T = make_case("q2_slp_goldak")
+    g = make_gpu(cfg, cells)
+    assert g.cells_per_block() == 64
+    for bad in (32, 96, 256):
+        with pytest.raises(Exception):
+            g.set_cells_per_block(bad)
+    cfg1, cells1, _ = make_case("q1_solid_convective_goldak")
+    g1 = make_gpu(cfg1, cells1)
+    assert g1.cells_per_block() == 128
+    with pytest.raises(Exception):
+        g1.set_cells_per_block(256)
+    # the autotuner times the 128-cell blocks with the atomic schedule and
+    # keeps whichever variant is fastest
+    choice, ms = g.autotune(g.from_grid(T))
+    assert g.cells_per_block() in (64, 128) and min(ms) > 0
