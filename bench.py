@@ -881,6 +881,7 @@ def run_ours(args, rank, world, local_rank):
         "timing": {"l2": "two src/dst pairs alternate (272 MB working set > 126 MB L2)",
                    "events": "CUDA events on the handle's stream around the K vmults"},
         "schedule": sched_name,
+        "cells_per_block": g.cells_per_block(),
         "autotune_ms_per_vmult": dict(zip(SCHEDULE_NAMES, schedule_ms)),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,
