@@ -56,17 +56,21 @@ class AdjointProblem:
 
     base: configuration at theta = (1, 1, absorptivity, power) of its
     sources with unit scales; points: (n, 3) node coordinates (i, j, k) of
-    the observed nodes.
+    the observed nodes; material_id / deposition_cos / deposition_sin: per
+    cell, as ThermalPhysics takes them. Cube sources keep their value (the
+    source parameters act on Goldak and electron beams).
     """
 
     def __init__(self, base: ThermalConfig, y0_grid: np.ndarray, t0: float, dt: float, n_steps: int,
                  obs_steps: Sequence[int], points: np.ndarray, targets: Optional[np.ndarray] = None,
-                 device: int = 0, checkpoint_every: int = 0):
+                 device: int = 0, checkpoint_every: int = 0, material_id=None, deposition_cos=None,
+                 deposition_sin=None):
         self.base = base
         self.t0, self.dt, self.n_steps = float(t0), float(dt), int(n_steps)
         self.checkpoint_every = int(checkpoint_every)
         self.obs_steps = np.ascontiguousarray(obs_steps, np.int32)
-        self.phys = ThermalPhysics(base, device=device)
+        self.phys = ThermalPhysics(base, device=device, material_id=material_id, deposition_cos=deposition_cos,
+                                   deposition_sin=deposition_sin)
         pts = np.asarray(points, np.int64).reshape(-1, 3)
         self.points = pts
         self.node_index = np.ascontiguousarray(

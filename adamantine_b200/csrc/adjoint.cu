@@ -31,7 +31,7 @@ namespace adm
 {
 namespace
 {
-template <int DEG, int NS>
+template <int DEG, int NS, bool GEN>
 void launch_adj(CUtensorMap const &ymap, CUtensorMap const &mmap, AdjArgs const &a, int n_items,
                 cudaStream_t stream)
 {
@@ -40,15 +40,16 @@ void launch_adj(CUtensorMap const &ymap, CUtensorMap const &mmap, AdjArgs const 
   static int grid_cap = 0;
   if (grid_cap == 0)
   {
-    ADM_CK(cudaFuncSetAttribute(adjoint_kernel<DEG, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ADM_CK(cudaFuncSetAttribute(adjoint_kernel<DEG, NS, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem));
     int dev = 0, sms = 0, per_sm = 0;
     ADM_CK(cudaGetDevice(&dev));
     ADM_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    ADM_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_kernel<DEG, NS>, T_::NT, smem));
+    ADM_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_kernel<DEG, NS, GEN>, T_::NT, smem));
     grid_cap = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
   }
   int const grid = n_items < grid_cap ? n_items : grid_cap;
-  adjoint_kernel<DEG, NS><<<grid, T_::NT, smem, stream>>>(ymap, mmap, a, n_items);
+  adjoint_kernel<DEG, NS, GEN><<<grid, T_::NT, smem, stream>>>(ymap, mmap, a, n_items);
 }
 
 // the backward member data's stage clock
@@ -61,32 +62,43 @@ __global__ void bclock_kernel(double *clock, double t, double dt)
   }
 }
 
-void launch_adjoint(int deg, int ns, CUtensorMap const &ym, CUtensorMap const &mm, AdjArgs const &a, int n_items,
-                    cudaStream_t stream)
+template <bool GEN>
+void launch_adjoint_g(int deg, int ns, CUtensorMap const &ym, CUtensorMap const &mm, AdjArgs const &a, int n_items,
+                      cudaStream_t stream)
 {
   switch (deg * 10 + ns)
   {
   case 11:
-    launch_adj<1, 1>(ym, mm, a, n_items, stream);
+    launch_adj<1, 1, GEN>(ym, mm, a, n_items, stream);
     break;
   case 12:
-    launch_adj<1, 2>(ym, mm, a, n_items, stream);
+    launch_adj<1, 2, GEN>(ym, mm, a, n_items, stream);
     break;
   case 13:
-    launch_adj<1, 3>(ym, mm, a, n_items, stream);
+    launch_adj<1, 3, GEN>(ym, mm, a, n_items, stream);
     break;
   case 21:
-    launch_adj<2, 1>(ym, mm, a, n_items, stream);
+    launch_adj<2, 1, GEN>(ym, mm, a, n_items, stream);
     break;
   case 22:
-    launch_adj<2, 2>(ym, mm, a, n_items, stream);
+    launch_adj<2, 2, GEN>(ym, mm, a, n_items, stream);
     break;
   case 23:
-    launch_adj<2, 3>(ym, mm, a, n_items, stream);
+    launch_adj<2, 3, GEN>(ym, mm, a, n_items, stream);
     break;
   default:
     throw Error(ADM_ERR_INVALID, "no adjoint kernel for this degree / state count");
   }
+}
+
+// gen: the variant with rotation, faces and cube sources
+void launch_adjoint(int deg, int ns, bool gen, CUtensorMap const &ym, CUtensorMap const &mm, AdjArgs const &a,
+                    int n_items, cudaStream_t stream)
+{
+  if (gen)
+    launch_adjoint_g<true>(deg, ns, ym, mm, a, n_items, stream);
+  else
+    launch_adjoint_g<false>(deg, ns, ym, mm, a, n_items, stream);
 }
 
 // resid[p] = y[idx[p]] - target[p]; *J += sum_p resid[p]^2 (one block, fixed
@@ -266,19 +278,19 @@ class Adjoint
 public:
   explicit Adjoint(Thermal &t) : th_(t)
   {
-    if (t.cfg_.use_table)
-      throw Error(ADM_ERR_UNSUPPORTED, "the adjoint supports polynomial material properties only");
-    if (t.has_rotation_)
-      throw Error(ADM_ERR_UNSUPPORTED, "the adjoint does not support deposition-angle rotation");
-    if (!t.adiabatic_only_)
-      throw Error(ADM_ERR_UNSUPPORTED, "the adjoint supports adiabatic boundaries only");
     if (!t.setup_done_)
       throw Error(ADM_ERR_INVALID, "setup() has not been called");
     ADM_CK(cudaSetDevice(t.device_));
     C_ = t.mesh_.n_cells;
     NN_ = (t.mesh_.deg + 1) * (t.mesh_.deg + 1) * (t.mesh_.deg + 1);
     n_ = t.mesh_.n_nodes;
-    save_phase(init_mode_, init_cell_, init_q_);
+    gen_ = t.has_rotation_ || !t.adiabatic_only_;
+    for (int b = 0; b < t.cfg_.n_sources; ++b)
+      gen_ = gen_ || t.cfg_.sources[b].type == 2;
+    // the face points' powder history (three states with faces)
+    NFP_ = (t.ns_ == 3 && !t.adiabatic_only_) ? (size_t)t.topo_.n_slots * 6 * (t.mesh_.deg + 1) * (t.mesh_.deg + 1)
+                                               : 0;
+    save_phase(init_mode_, init_cell_, init_q_, init_face_);
   }
 
   void set_observations(int n_obs_steps, int32_t const *steps, int n_points, int64_t const *index,
@@ -324,11 +336,12 @@ public:
     Thermal &t = th_;
     ADM_CK(cudaSetDevice(t.device_));
     int const S = t.tab_.s;
-    double const per_step = 8.0 * S * ((double)n_ + (t.ns_ == 3 ? (double)C_ * NN_ : 0.0));
+    double const per_step = 8.0 * S * ((double)n_ + (t.ns_ == 3 ? (double)C_ * NN_ : 0.0) + (double)NFP_);
     size_t free_b = 0, total_b = 0;
     ADM_CK(cudaMemGetInfo(&free_b, &total_b));
     // the stores already held are released before the new ones are made
-    double const held = 8.0 * ((double)Ystore_.n + (double)Sstore_.n + (double)Ystore2_.n + (double)Sstore2_.n);
+    double const held = 8.0 * ((double)Ystore_.n + (double)Sstore_.n + (double)Ystore2_.n + (double)Sstore2_.n +
+                               (double)Fstore_.n + (double)Fstore2_.n);
     double const budget = 0.5 * ((double)free_b + held);
     double const fit = std::floor(budget / per_step);
     if (fit >= (double)n_steps)
@@ -359,16 +372,22 @@ public:
     Ystore_.alloc((size_t)K * S * n_);
     if (t.ns_ == 3)
       Sstore_.alloc((size_t)K * S * C_ * NN_);
+    if (NFP_)
+      Fstore_.alloc((size_t)K * S * NFP_);
     if (n_seg > 1)
     {
       Ystore2_.alloc((size_t)K * S * n_);
       if (t.ns_ == 3)
         Sstore2_.alloc((size_t)K * S * C_ * NN_);
+      if (NFP_)
+        Fstore2_.alloc((size_t)K * S * NFP_);
     }
     ystore_[0] = Ystore_.p;
     ystore_[1] = n_seg > 1 ? Ystore2_.p : Ystore_.p;
     sstore_[0] = Sstore_.p;
     sstore_[1] = n_seg > 1 ? Sstore2_.p : Sstore_.p;
+    fstore_[0] = Fstore_.p;
+    fstore_[1] = n_seg > 1 ? Fstore2_.p : Fstore_.p;
     rec_buf_ = (n_seg - 1) & 1;
     forward(t0, dt, n_steps, y0, K);
     double J = 0.0;
@@ -376,7 +395,7 @@ public:
     if (y_final)
       ADM_CK(cudaMemcpyAsync(y_final, y_.p, n_ * sizeof(double), cudaMemcpyDeviceToDevice, st));
     // final phase state of the forward run, restored at the end
-    save_phase(fin_mode_, fin_cell_, fin_q_);
+    save_phase(fin_mode_, fin_cell_, fin_q_, fin_face_);
 
     bool const ns3 = t.ns_ == 3;
     size_t const qn = C_ * NN_;
@@ -402,6 +421,7 @@ public:
       ADM_CK(cudaMemsetAsync(ls_a_.p, 0, qn * sizeof(double), st));
       ADM_CK(cudaMemsetAsync(ls_b_.p, 0, qn * sizeof(double), st));
     }
+    clear_face_adjoint(st);
     grad_d_.alloc(3);
     ADM_CK(cudaMemsetAsync(grad_d_.p, 0, 3 * sizeof(double), st));
     // the backward sweep runs on its own stream with its own member data
@@ -427,6 +447,7 @@ public:
       ADM_CK(cudaStreamWaitEvent(bs, ev_rec_[b], 0));
       double const *ys = ystore_[b];
       double *ss = sstore_[b];
+      double const *fs = fstore_[b];
       // backward sweep over the segment
       for (int n = n1 - 1; n >= n0; --n)
       {
@@ -482,6 +503,12 @@ public:
             A.lam_s_in = ls_b_.p;
             A.powder_start = init_mode_.p;
           }
+          if (NFP_)
+          {
+            A.sf_in = fs + rslot * NFP_;
+            A.lam_sf_out = lsf_a_.p;
+            A.lam_sf_in = lsf_b_.p;
+          }
           A.lam_y = lamYi;
           A.grad = grad_d_.p;
           A.mu_max = reinterpret_cast<double const *>(x.mu_max);
@@ -493,6 +520,8 @@ public:
           std::swap(act_cur_, act_next_);
           if (ns3)
             std::swap(ls_a_.p, ls_b_.p);
+          if (NFP_)
+            std::swap(lsf_a_.p, lsf_b_.p);
         }
         pending = true;
       }
@@ -531,6 +560,8 @@ public:
       ADM_CK(cudaMemcpyAsync(t.powder_cell_.p, fin_cell_.p, C_ * sizeof(double), cudaMemcpyDeviceToDevice, st));
       ADM_CK(cudaMemcpyAsync(t.powder_q_.p, fin_q_.p, qn * sizeof(double), cudaMemcpyDeviceToDevice, st));
     }
+    if (NFP_)
+      ADM_CK(cudaMemcpyAsync(t.face_powder_.p, fin_face_.p, NFP_ * sizeof(double), cudaMemcpyDeviceToDevice, st));
     ADM_CK(cudaStreamSynchronize(st));
     grad[0] = g[0];
     grad[1] = g[1];
@@ -568,6 +599,13 @@ public:
       A.s_in = Sstore_.p;
       A.lam_s_out = ls_a_.p;
       A.lam_s_in = ls_b_.p;
+    }
+    if (NFP_)
+    {
+      clear_face_adjoint(st);
+      A.sf_in = t.face_powder_.p;
+      A.lam_sf_out = lsf_a_.p;
+      A.lam_sf_in = lsf_b_.p;
     }
     A.lam_y = lam;
     A.grad = grad_d_.p;
@@ -608,7 +646,7 @@ private:
     A.k.work = work ? work : t.awork_d_.p;
     CUtensorMap const ym = brick_map(t.mesh_, A.yv, 1, n_);
     CUtensorMap const mm = brick_map(t.mesh_, A.mu, 1, n_);
-    launch_adjoint(t.mesh_.deg, t.ns_, ym, mm, A, count, stream ? stream : t.stream_);
+    launch_adjoint(t.mesh_.deg, t.ns_, gen_, ym, mm, A, count, stream ? stream : t.stream_);
     ADM_CK(cudaGetLastError());
   }
 
@@ -624,12 +662,28 @@ private:
     ADM_CK(cudaSetDevice(th_.device_));
   }
 
-  void save_phase(DevBuf<uint8_t> &mode, DevBuf<double> &cell, DevBuf<double> &q)
+  // both face-powder adjoint buffers allocated and zeroed
+  void clear_face_adjoint(cudaStream_t st)
+  {
+    if (!NFP_)
+      return;
+    lsf_a_.alloc(NFP_);
+    lsf_b_.alloc(NFP_);
+    ADM_CK(cudaMemsetAsync(lsf_a_.p, 0, NFP_ * sizeof(double), st));
+    ADM_CK(cudaMemsetAsync(lsf_b_.p, 0, NFP_ * sizeof(double), st));
+  }
+
+  void save_phase(DevBuf<uint8_t> &mode, DevBuf<double> &cell, DevBuf<double> &q, DevBuf<double> &face)
   {
     Thermal &t = th_;
     if (t.ns_ != 3)
       return;
     cudaStream_t const st = t.stream_;
+    if (NFP_)
+    {
+      face.alloc(NFP_);
+      ADM_CK(cudaMemcpyAsync(face.p, t.face_powder_.p, NFP_ * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    }
     mode.alloc(C_);
     cell.alloc(C_);
     q.alloc(C_ * NN_);
@@ -647,6 +701,9 @@ private:
                            cudaMemcpyDeviceToDevice, st));
     ADM_CK(cudaMemcpyAsync(t.powder_q_.p, ck_q_.p + (size_t)seg * C_ * NN_, C_ * NN_ * sizeof(double),
                            cudaMemcpyDeviceToDevice, st));
+    if (NFP_)
+      ADM_CK(cudaMemcpyAsync(t.face_powder_.p, ck_face_.p + (size_t)seg * NFP_, NFP_ * sizeof(double),
+                             cudaMemcpyDeviceToDevice, st));
   }
 
   void checkpoint(int seg)
@@ -662,6 +719,9 @@ private:
       ADM_CK(cudaMemcpyAsync(ck_q_.p + (size_t)seg * C_ * NN_, t.powder_q_.p, C_ * NN_ * sizeof(double),
                              cudaMemcpyDeviceToDevice, st));
     }
+    if (NFP_)
+      ADM_CK(cudaMemcpyAsync(ck_face_.p + (size_t)seg * NFP_, t.face_powder_.p, NFP_ * sizeof(double),
+                             cudaMemcpyDeviceToDevice, st));
   }
 
   // One step n of the forward run, stage by stage as Thermal::launch_step
@@ -686,6 +746,9 @@ private:
       if (t.ns_ == 3)
         launch_expand_powder(t.cell_info_d_.p, NN_, t.powder_mode_.p, t.powder_cell_.p, t.powder_q_.p,
                              sstore_[rec_buf_] + slot * qn, C_, st, init_mode_.p);
+      if (NFP_)
+        ADM_CK(cudaMemcpyAsync(fstore_[rec_buf_] + slot * NFP_, t.face_powder_.p, NFP_ * sizeof(double),
+                               cudaMemcpyDeviceToDevice, st));
       t.launch_pass(a, src);
     }
   }
@@ -727,6 +790,8 @@ private:
       ADM_CK(cudaMemcpyAsync(t.powder_cell_.p, init_cell_.p, C_ * sizeof(double), cudaMemcpyDeviceToDevice, st));
       ADM_CK(cudaMemcpyAsync(t.powder_q_.p, init_q_.p, C_ * NN_ * sizeof(double), cudaMemcpyDeviceToDevice, st));
     }
+    if (NFP_)
+      ADM_CK(cudaMemcpyAsync(t.face_powder_.p, init_face_.p, NFP_ * sizeof(double), cudaMemcpyDeviceToDevice, st));
     ADM_CK(cudaMemsetAsync(Jd_.p, 0, sizeof(double), st));
     if (K > 0)
     {
@@ -738,6 +803,8 @@ private:
         ck_cell_.alloc((size_t)n_seg * C_);
         ck_q_.alloc((size_t)n_seg * C_ * NN_);
       }
+      if (NFP_)
+        ck_face_.alloc((size_t)n_seg * NFP_);
     }
     times_.assign(n_steps + 1, 0.0);
     double tt = t0;
@@ -829,6 +896,12 @@ private:
   DevBuf<double> Ystore2_, Sstore2_, bclock_;
   double *ystore_[2] = {nullptr, nullptr};
   double *sstore_[2] = {nullptr, nullptr};
+  // face points' powder history (three states with faces): NFP_ values per
+  // phase state, their stores, checkpoints and adjoint buffers
+  size_t NFP_ = 0;
+  bool gen_ = false; // the kernel variant with rotation, faces and cube sources
+  DevBuf<double> Fstore_, Fstore2_, ck_face_, init_face_, fin_face_, lsf_a_, lsf_b_;
+  double *fstore_[2] = {nullptr, nullptr};
   int rec_buf_ = 0;
   DevBuf<MemberData> bmd_;
   DevBuf<BeamState> bbeam_;

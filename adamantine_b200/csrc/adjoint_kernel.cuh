@@ -14,18 +14,26 @@
 // specific-heat scale and the source strength (absorptivity or power):
 //   d/dlog k_scale   = sum_q JxW [ -sum_d a_d (dT/dx_d)(dmu/dx_d) ]
 //   d/dlog cp_scale  = -(c_p / c_p,eff) (that + JxW b mu)
-//   d/dlog Q         = sum_q JxW b mu
+//   d/dlog Q         = sum_q JxW b mu   (b from the Goldak and electron beams)
 // The derivative of the temperature dependence covers the polynomials of
 // every state, the liquid ratio (dl/dT = 1 / (T_l - T_s) inside the mushy
 // range) and the mixing with the powder history; the latent-heat indicator
 // l * solid > 0 is piecewise constant and contributes nothing.
 //
+// Properties are polynomials or 12-point tables (the derivative of a table
+// is the slope of its segment, 0 where it is clamped). A deposition angle
+// rotates the conductivity tensor in x-y: the gradients are rotated into the
+// frame of (k_x, k_y) before the point evaluation and the fluxes rotated
+// back. Convective / radiative faces (source/ThermalOperator.templates.hh:
+// 619-751) add the transpose of their flux density
+// B = -(1/(rho c_p)) [h_conv (T - T_conv) + h_rad (T - T_rad)] at the face
+// points, with the face points' own powder history (adj_face_terms).
+//
 // Same tiles and thread layout as the forward tile kernel (one thread per
 // cell and z-level); one launch covers the tiles of every colour, CTAs loop
 // over them, the two node bricks (T and mu) are staged with plain loads and
 // the per-node results are added with atomics (a node is shared by at most
-// eight tiles). Adiabatic faces only; polynomial properties; no
-// deposition-angle rotation.
+// eight tiles).
 #pragma once
 
 #include "tile_kernel.cuh"
@@ -48,6 +56,10 @@ struct AdjArgs
   double flush;            // tiles with |mu| <= flush * *mu_max and no powder adjoint are skipped
   int const *n_items_dev;  // number of work items (a selected list) in device memory, or null
   uint8_t *act_next;       // per tile: may hold a non-negligible adjoint next stage (set here), or null
+  // faces of three-state problems: [slot][6][NF] as MemberData::face_powder
+  double const *sf_in;     // powder ratio of the face points before the stage
+  double *lam_sf_out;      // adjoint of the face points' powder ratio after the stage
+  double *lam_sf_in;       // adjoint of the face points' powder ratio before the stage
 };
 
 // Horner value and derivative of sum_i c[i] T^i up to degree deg.
@@ -63,16 +75,52 @@ __device__ __forceinline__ void poly_vd(double const *c, int deg, double T, doub
   d = dd;
 }
 
+// Value and derivative of MaterialProperty::compute_property_from_table
+// (source/MaterialProperty.templates.hh:1158-1212; the value as
+// table_lookup computes it): the slope of the segment holding T, 0 where
+// the table is clamped (below the first point, from the next-to-last on).
+__device__ __forceinline__ void table_vd(MaterialDesc const *gm, int mat, int prop, int s, double T, double &v,
+                                         double &d)
+{
+  double const(*t)[2] = gm->table[mat][prop][s];
+  d = 0.0;
+  if (T <= t[0][0])
+  {
+    v = t[0][1];
+    return;
+  }
+  int i = 0;
+  for (; i < kTableSize; ++i)
+    if (T < t[i][0])
+      break;
+  if (i >= kTableSize - 1)
+  {
+    v = t[kTableSize - 1][1];
+    return;
+  }
+  v = t[i - 1][1] + (T - t[i - 1][0]) * (t[i][1] - t[i - 1][1]) / (t[i][0] - t[i - 1][0]);
+  d = (t[i][1] - t[i - 1][1]) / (t[i][0] - t[i - 1][0]);
+}
+
+// Value and T-derivative of one state's property (polynomial or table).
+__device__ __forceinline__ void prop_vd(SmemPhys const &sp, MaterialDesc const *gm, int mat, int prop, int s,
+                                        double T, double &v, double &d)
+{
+  if (sp.use_table)
+    table_vd(gm, mat, prop, s, T, v, d);
+  else
+    poly_vd(&sp.poly[mat][prop][s][0], sp.prop_deg[prop], T, v, d);
+}
+
 // Mixture value, T-derivative and s'-derivative of one state property.
 template <int NS>
-__device__ __forceinline__ void mix_prop(SmemPhys const &sp, int mat, int prop, double T, double const *r,
-                                         double ld, double &v, double &dT, double &ds)
+__device__ __forceinline__ void mix_prop(SmemPhys const &sp, MaterialDesc const *gm, int mat, int prop, double T,
+                                         double const *r, double ld, double &v, double &dT, double &ds)
 {
-  int const deg = sp.prop_deg[prop];
   double pv[NS], pd[NS];
 #pragma unroll
   for (int s = 0; s < NS; ++s)
-    poly_vd(&sp.poly[mat][prop][s][0], deg, T, pv[s], pd[s]);
+    prop_vd(sp, gm, mat, prop, s, T, pv[s], pd[s]);
   double a = 0.0, b = 0.0;
 #pragma unroll
   for (int s = 0; s < NS; ++s)
@@ -100,15 +148,17 @@ struct AdjQp
 // squared inverse cell sizes. Outputs: the reference-space fluxes and the
 // value term of the transposed operator, the adjoint of the powder ratio
 // before the stage and the three log-derivative contributions.
+// State ratios exactly as update_state_ratios computes them
+// (source/ThermalOperator.templates.hh:227-317), with dl/dT (ld) and which
+// side of s' = min(1 - l, s) is taken (br: s' = 1 - l).
 template <int NS>
-__device__ __forceinline__ AdjQp adj_qp(SmemPhys const &sp, int mat, double T, double mu, double gx, double gy,
-                                     double gz, double mx, double my, double mz, double s_in, double lam_out,
-                                     double JxW, double Q, double hx2, double hy2, double hz2)
+__device__ __forceinline__ void adj_ratios(SmemPhys const &sp, int mat, double T, double s_in, double *r,
+                                           double &ld, bool &br)
 {
-  // ratios exactly as update_state_ratios computes them
-  double r[3] = {1.0, 0.0, 0.0};
-  double ld = 0.0;
-  bool br = false; // s' = 1 - l (true) or s' = s (false)
+  r[0] = 1.0;
+  r[1] = r[2] = 0.0;
+  ld = 0.0;
+  br = false;
   if (NS > 1)
   {
     double const Ts = sp.props[mat][Q_SOLIDUS], Tl = sp.props[mat][Q_LIQUIDUS];
@@ -133,17 +183,41 @@ __device__ __forceinline__ AdjQp adj_qp(SmemPhys const &sp, int mat, double T, d
       r[0] = 1.0 - l - sp_new;
     }
   }
+}
+
+// 1/(rho c_p,eff) with its T- and s'-derivatives (get_inv_rho_cp,
+// source/ThermalOperator.templates.hh:415-477; the latent-heat indicator is
+// piecewise constant); cp / cp_eff for the specific-heat log-derivative.
+template <int NS>
+__device__ __forceinline__ void adj_inv_rho_cp(SmemPhys const &sp, MaterialDesc const *gm, int mat, double T,
+                                               double const *r, double ld, double &inv, double &inv_T,
+                                               double &inv_s, double &cp_frac)
+{
   double rho, rho_T, rho_s, cp, cp_T, cp_s;
-  mix_prop<NS>(sp, mat, P_DENSITY, T, r, ld, rho, rho_T, rho_s);
-  mix_prop<NS>(sp, mat, P_SPECIFIC_HEAT, T, r, ld, cp, cp_T, cp_s);
+  mix_prop<NS>(sp, gm, mat, P_DENSITY, T, r, ld, rho, rho_T, rho_s);
+  mix_prop<NS>(sp, gm, mat, P_SPECIFIC_HEAT, T, r, ld, cp, cp_T, cp_s);
   double cp_eff = cp;
   if (NS > 1 && r[1] * r[0] > 0.0)
     cp_eff += sp.latent_term[mat];
-  double const inv = recip(rho * cp_eff);
-  double const inv_T = -inv * inv * (rho_T * cp_eff + rho * cp_T);
-  double const inv_s = -inv * inv * (rho_s * cp_eff + rho * cp_s);
+  inv = recip(rho * cp_eff);
+  inv_T = -inv * inv * (rho_T * cp_eff + rho * cp_T);
+  inv_s = -inv * inv * (rho_s * cp_eff + rho * cp_s);
+  cp_frac = cp / cp_eff;
+}
+
+template <int NS>
+__device__ __forceinline__ AdjQp adj_qp(SmemPhys const &sp, MaterialDesc const *gm, int mat, double T, double mu,
+                                     double gx, double gy, double gz, double mx, double my, double mz,
+                                     double s_in, double lam_out, double JxW, double Q, double hx2, double hy2,
+                                     double hz2)
+{
+  double r[3], ld;
+  bool br;
+  adj_ratios<NS>(sp, mat, T, s_in, r, ld, br);
+  double inv, inv_T, inv_s, cp_frac;
+  adj_inv_rho_cp<NS>(sp, gm, mat, T, r, ld, inv, inv_T, inv_s, cp_frac);
   double kd[3], kd_T[3], kd_s[3];
-  mix_prop<NS>(sp, mat, P_KX, T, r, ld, kd[0], kd_T[0], kd_s[0]);
+  mix_prop<NS>(sp, gm, mat, P_KX, T, r, ld, kd[0], kd_T[0], kd_s[0]);
   if (sp.isotropic)
   {
     kd[1] = kd[2] = kd[0];
@@ -152,8 +226,8 @@ __device__ __forceinline__ AdjQp adj_qp(SmemPhys const &sp, int mat, double T, d
   }
   else
   {
-    mix_prop<NS>(sp, mat, P_KY, T, r, ld, kd[1], kd_T[1], kd_s[1]);
-    mix_prop<NS>(sp, mat, P_KZ, T, r, ld, kd[2], kd_T[2], kd_s[2]);
+    mix_prop<NS>(sp, gm, mat, P_KY, T, r, ld, kd[1], kd_T[1], kd_s[1]);
+    mix_prop<NS>(sp, gm, mat, P_KZ, T, r, ld, kd[2], kd_T[2], kd_s[2]);
   }
   // physical gradient products (reference gradients / h)
   double const uv[3] = {gx * mx * hx2, gy * my * hy2, gz * mz * hz2};
@@ -180,7 +254,7 @@ __device__ __forceinline__ AdjQp adj_qp(SmemPhys const &sp, int mat, double T, d
   }
   o.gk = JxW * (-dot_a);
   o.gq = JxW * b * mu;
-  o.gc = -(cp / cp_eff) * (o.gk + o.gq);
+  o.gc = -cp_frac * (o.gk + o.gq);
   // fluxes of the transposed diffusion term in reference coordinates
   double const cf = -inv * JxW;
   o.fx = cf * kd[0] * mx * hx2;
@@ -194,17 +268,17 @@ __device__ __forceinline__ AdjQp adj_qp(SmemPhys const &sp, int mat, double T, d
 // powder adjoint that does not propagate (the point is solid without powder
 // history, or untouched powder, whose s' = 1 - l follows T with
 // dl/dT = 0). One polynomial per property, inline.
-__device__ __forceinline__ AdjQp adj_qp_pure(SmemPhys const &sp, int mat, int st, double T, double mu, double gx,
-                                             double gy, double gz, double mx, double my, double mz, double JxW,
-                                             double Q, double hx2, double hy2, double hz2)
+__device__ __forceinline__ AdjQp adj_qp_pure(SmemPhys const &sp, MaterialDesc const *gm, int mat, int st, double T,
+                                             double mu, double gx, double gy, double gz, double mx, double my,
+                                             double mz, double JxW, double Q, double hx2, double hy2, double hz2)
 {
   double rho, rho_T, cp, cp_T;
-  poly_vd(&sp.poly[mat][P_DENSITY][st][0], sp.prop_deg[P_DENSITY], T, rho, rho_T);
-  poly_vd(&sp.poly[mat][P_SPECIFIC_HEAT][st][0], sp.prop_deg[P_SPECIFIC_HEAT], T, cp, cp_T);
+  prop_vd(sp, gm, mat, P_DENSITY, st, T, rho, rho_T);
+  prop_vd(sp, gm, mat, P_SPECIFIC_HEAT, st, T, cp, cp_T);
   double const inv = recip(rho * cp);
   double const inv_T = -inv * inv * (rho_T * cp + rho * cp_T);
   double kd[3], kd_T[3];
-  poly_vd(&sp.poly[mat][P_KX][st][0], sp.prop_deg[P_KX], T, kd[0], kd_T[0]);
+  prop_vd(sp, gm, mat, P_KX, st, T, kd[0], kd_T[0]);
   if (sp.isotropic)
   {
     kd[1] = kd[2] = kd[0];
@@ -212,8 +286,8 @@ __device__ __forceinline__ AdjQp adj_qp_pure(SmemPhys const &sp, int mat, int st
   }
   else
   {
-    poly_vd(&sp.poly[mat][P_KY][st][0], sp.prop_deg[P_KY], T, kd[1], kd_T[1]);
-    poly_vd(&sp.poly[mat][P_KZ][st][0], sp.prop_deg[P_KZ], T, kd[2], kd_T[2]);
+    prop_vd(sp, gm, mat, P_KY, st, T, kd[1], kd_T[1]);
+    prop_vd(sp, gm, mat, P_KZ, st, T, kd[2], kd_T[2]);
   }
   double const uv[3] = {gx * mx * hx2, gy * my * hy2, gz * mz * hz2};
   double dot_a = 0.0, dot_aT = 0.0;
@@ -243,19 +317,145 @@ __device__ __forceinline__ AdjQp adj_qp_pure(SmemPhys const &sp, int mat, int st
 // thread's level, and one copy of the code keeps the instruction footprint
 // small.
 template <int NS>
-__device__ __noinline__ AdjQp adj_point(SmemPhys const &sp, int mat, int pure, bool no_powder, double T,
-                                        double mu, double gx, double gy, double gz, double mx, double my,
-                                        double mz, double s_in, double lam_out, double JxW, double Q, double hx2,
-                                        double hy2, double hz2)
+__device__ __noinline__ AdjQp adj_point(SmemPhys const &sp, MaterialDesc const *gm, int mat, int pure,
+                                        bool no_powder, double T, double mu, double gx, double gy, double gz,
+                                        double mx, double my, double mz, double s_in, double lam_out, double JxW,
+                                        double Q, double hx2, double hy2, double hz2)
 {
   if (pure >= 0)
-    return adj_qp_pure(sp, mat, pure, T, mu, gx, gy, gz, mx, my, mz, JxW, Q, hx2, hy2, hz2);
+    return adj_qp_pure(sp, gm, mat, pure, T, mu, gx, gy, gz, mx, my, mz, JxW, Q, hx2, hy2, hz2);
   if (NS == 3 && no_powder)
-    return adj_qp<NS == 3 ? 2 : NS>(sp, mat, T, mu, gx, gy, gz, mx, my, mz, 0.0, 0.0, JxW, Q, hx2, hy2, hz2);
-  return adj_qp<NS>(sp, mat, T, mu, gx, gy, gz, mx, my, mz, s_in, lam_out, JxW, Q, hx2, hy2, hz2);
+    return adj_qp<NS == 3 ? 2 : NS>(sp, gm, mat, T, mu, gx, gy, gz, mx, my, mz, 0.0, 0.0, JxW, Q, hx2, hy2, hz2);
+  return adj_qp<NS>(sp, gm, mat, T, mu, gx, gy, gz, mx, my, mz, s_in, lam_out, JxW, Q, hx2, hy2, hz2);
 }
 
+// Transposed face terms of one cell for the node level `slab` (the
+// transpose of face_terms in tile_kernel.cuh, which every level thread of
+// a cell evaluates, keeping its own level's test functions). At a face
+// point with trace values T_f and mu_f, powder ratio s' = min(1 - l(T_f), s)
+// and flux density B(T_f, s') = -(1/(rho c_p)) [h_conv (T_f - T_conv) +
+// h_rad (T_f - T_rad)], h_rad = eps sigma (T_f + T_rad)(T_f^2 + T_rad^2):
+//   out[e]          += JxW mu_f dB/dT phi_e        (node e of this level)
+//   g                = lam_sf' + JxW mu_f dB/ds'   (to s, or -g dl/dT to T where s' = 1 - l)
+//   return value    += -(c_p / c_p,eff) JxW mu_f B (specific-heat log-derivative)
+// The powder adjoint and the return value come from one thread per face
+// point (the one that updates the face powder in the forward kernel).
 template <int DEG, int NS>
+__device__ __noinline__ double adj_face_terms(SmemPhys const &sp, MaterialDesc const *gm, AdjArgs const &A,
+                                              MemberData const &md, double const *yb, double const *mb, int lx,
+                                              int ly, int lz, int slab, uint32_t info, int mat, size_t c,
+                                              bool no_powder, double *out)
+{
+  constexpr int N = DEG + 1, NQS = N * N, NF = N * N;
+  constexpr int BXP = TD<DEG>::BXP, BY = TD<DEG>::BY;
+  KernelArgs const &args = A.k;
+  for (int e = 0; e < NQS; ++e)
+    out[e] = 0.0;
+  double gc = 0.0;
+  int const slot = (NS == 3 && !no_powder) ? md.face_slot[c] : -1;
+  for (int f = 0; f < 6; ++f)
+  {
+    if (!((info >> (CI_FACE_SHIFT + f)) & 1u))
+      continue;
+    int const d = f / 2, side = f % 2;
+    if (d == 2 && slab != (side ? N - 1 : 0))
+      continue; // a z face only touches one node level
+    bool const writer = d == 2 || slab == 0;
+    int const t0 = d == 0 ? 1 : 0, t1 = d == 2 ? 1 : 2;
+    int const btype =
+        ((info >> (CI_INTERFACE_SHIFT + f)) & 1u) ? args.interface_type : args.boundary_type[f];
+    double const ht0 = args.h[t0], ht1 = args.h[t1];
+    for (int fq = 0; fq < NF; ++fq)
+    {
+      int const qa = fq % N, qb = fq / N;
+      double T = 0.0, M = 0.0;
+      for (int j = 0; j < N; ++j)
+        for (int i = 0; i < N; ++i)
+        {
+          int loc[3];
+          loc[d] = side ? N - 1 : 0;
+          loc[t0] = i;
+          loc[t1] = j;
+          int const e = (DEG * lx + loc[0]) + BXP * ((DEG * ly + loc[1]) + BY * (DEG * lz + loc[2]));
+          double const phi = args.S[qa][i] * args.S[qb][j];
+          T += phi * yb[e];
+          M += phi * mb[e];
+        }
+      size_t const fi = ((size_t)(slot < 0 ? 0 : slot) * 6 + f) * NF + fq;
+      double const s_in = (slot >= 0 && A.sf_in) ? A.sf_in[fi] : 0.0;
+      double r[3], ld;
+      bool br;
+      adj_ratios<NS>(sp, mat, T, s_in, r, ld, br);
+      double inv, inv_T, inv_s, cp_frac;
+      adj_inv_rho_cp<NS>(sp, gm, mat, T, r, ld, inv, inv_T, inv_s, cp_frac);
+      double F = 0.0, F_T = 0.0, F_s = 0.0;
+      if (btype & B_CONVECTIVE)
+      {
+        double const Tc = sp.props[mat][Q_CONV_TINF];
+        double hc, hc_T, hc_s;
+        mix_prop<NS>(sp, gm, mat, P_CONV_COEF, T, r, ld, hc, hc_T, hc_s);
+        F += hc * (T - Tc);
+        F_T += hc_T * (T - Tc) + hc;
+        F_s += hc_s * (T - Tc);
+      }
+      if (btype & B_RADIATIVE)
+      {
+        double const Tr = sp.props[mat][Q_RAD_TINF];
+        double em, em_T, em_s;
+        mix_prop<NS>(sp, gm, mat, P_EMISSIVITY, T, r, ld, em, em_T, em_s);
+        double const sigma = 5.670374419e-8;
+        double const p = (T + Tr) * (T * T + Tr * Tr);
+        double const p_T = (T * T + Tr * Tr) + 2.0 * T * (T + Tr);
+        F += em * sigma * p * (T - Tr);
+        F_T += sigma * (em_T * p * (T - Tr) + em * (p_T * (T - Tr) + p));
+        F_s += em_s * sigma * p * (T - Tr);
+      }
+      double const B = -inv * F;
+      double const B_T = -(inv_T * F + inv * F_T);
+      double const w = args.qw[qa] * ht0 * args.qw[qb] * ht1 * M;
+      double val = w * B_T;
+      if (NS == 3 && slot >= 0)
+      {
+        double const lam_out = A.lam_sf_out ? A.lam_sf_out[fi] : 0.0;
+        double const gs = lam_out + w * (-(inv_s * F + inv * F_s));
+        if (br)
+          val -= ld * gs;
+        if (writer && A.lam_sf_in)
+          A.lam_sf_in[fi] = br ? 0.0 : gs;
+      }
+      if (writer)
+        gc -= cp_frac * w * B;
+      for (int j = 0; j < N; ++j)
+        for (int i = 0; i < N; ++i)
+        {
+          int const la = d == 0 ? (side ? N - 1 : 0) : i;
+          int const lb = d == 0 ? i : (d == 1 ? (side ? N - 1 : 0) : j);
+          int const lc = d == 2 ? (side ? N - 1 : 0) : j;
+          if (lc != slab)
+            continue;
+          out[la + N * lb] += val * (args.S[qa][i] * args.S[qb][j]);
+        }
+    }
+  }
+  return gc;
+}
+
+// The source at a point from the Goldak and electron beams only (the
+// beams the source-strength parameter scales; cube sources keep their
+// value).
+static __device__ __noinline__ double scaled_beam_sum(SmemPhys const &sp, double px, double py, double pz)
+{
+  double qs = 0.0;
+  for (int b = 0; b < sp.n_beams; ++b)
+    if (sp.beams[b].type != 2)
+      qs += beam_value(sp.beams[b], px, py, pz);
+  return qs;
+}
+
+// GEN: the problem has a deposition-angle rotation, boundary faces or a
+// cube source (instantiated apart so that the common case carries none of
+// that code).
+template <int DEG, int NS, bool GEN>
 __global__ void __launch_bounds__(TD<DEG>::NT, 2)
     adjoint_kernel(const __grid_constant__ CUtensorMap ymap, const __grid_constant__ CUtensorMap mmap,
                    const __grid_constant__ AdjArgs A, int n_items_max)
@@ -364,6 +564,12 @@ __global__ void __launch_bounds__(TD<DEG>::NT, 2)
       if (powder_cell)
         for (int i = 0; i < NQS; ++i)
           nz |= A.lam_s_out[sbase + i] != 0.0;
+      // the face points of the cell (level thread 0 of each cell)
+      int const fslot = (GEN && powder_cell && slab == 0 && A.lam_sf_out) ? md.face_slot[sc] : -1;
+      constexpr int NFS = 6 * (DEG + 1) * (DEG + 1);
+      if (fslot >= 0)
+        for (int i = 0; i < NFS; ++i)
+          nz |= A.lam_sf_out[(size_t)fslot * NFS + i] != 0.0;
       if (!__syncthreads_or(nz))
       {
         // the tile drops out of the list: both powder-adjoint buffers of
@@ -374,6 +580,12 @@ __global__ void __launch_bounds__(TD<DEG>::NT, 2)
           {
             A.lam_s_in[sbase + i] = 0.0;
             A.lam_s_out[sbase + i] = 0.0;
+          }
+        if (fslot >= 0)
+          for (int i = 0; i < NFS; ++i)
+          {
+            A.lam_sf_in[(size_t)fslot * NFS + i] = 0.0;
+            A.lam_sf_out[(size_t)fslot * NFS + i] = 0.0;
           }
         continue;
       }
@@ -388,7 +600,7 @@ __global__ void __launch_bounds__(TD<DEG>::NT, 2)
     }
 
     // tile-level source culling (as in the forward kernel)
-    bool do_src = false;
+    bool do_src = false, has_cube = false;
     {
       double const x0 = args.origin[0] + ncx0 * args.h[0];
       double const y0 = args.origin[1] + ncy0 * args.h[1];
@@ -403,7 +615,10 @@ __global__ void __launch_bounds__(TD<DEG>::NT, 2)
         {
           if (x1 >= bs.cube_min[0] && x0 <= bs.cube_max[0] && y1 >= bs.cube_min[1] && y0 <= bs.cube_max[1] &&
               z1 >= bs.cube_min[2] && z0 <= bs.cube_max[2])
+          {
             do_src = true;
+            has_cube = GEN;
+          }
           continue;
         }
         if ((z1 - bs.center[2]) + bs.depth < 0.0)
@@ -505,12 +720,23 @@ __global__ void __launch_bounds__(TD<DEG>::NT, 2)
       axy[i] = 0.0;
       az[i] = 0.0;
     }
+    MaterialDesc const *const gm = md.mat;
+    bool const no_powder = NS == 3 && A.powder_start && A.powder_start[c] == 0;
     if (active)
     {
       size_t const qbase = c * NN + (size_t)NQS * slab;
-      bool const no_powder = NS == 3 && A.powder_start && A.powder_start[c] == 0;
-      double const hx2 = args.inv_h[0] * args.inv_h[0], hy2 = args.inv_h[1] * args.inv_h[1],
-                   hz2 = args.inv_h[2] * args.inv_h[2];
+      double const hz2 = args.inv_h[2] * args.inv_h[2];
+      // a deposition angle rotates (k_x, k_y) (source/ThermalOperator.templates.hh:552-594):
+      // the point sees physical gradients in the frame of (k_x, k_y)
+      bool const rot = GEN && sp.has_rotation && !sp.isotropic;
+      double cs = 1.0, sn = 0.0;
+      if (rot)
+      {
+        cs = md.cosv[c];
+        sn = md.sinv[c];
+      }
+      double const hx2 = rot ? 1.0 : args.inv_h[0] * args.inv_h[0];
+      double const hy2 = rot ? 1.0 : args.inv_h[1] * args.inv_h[1];
   #pragma unroll
       for (int i = 0; i < NQS; ++i)
       {
@@ -526,13 +752,23 @@ __global__ void __launch_bounds__(TD<DEG>::NT, 2)
           my = fma(args.D[qb][k], Mq[qa + N * k], my);
         }
         double const gz = Tz[i], mz = Mz[i];
-        double Q = 0.0;
+        if (rot)
+        {
+          double const gxp = gx * args.inv_h[0], gyp = gy * args.inv_h[1];
+          double const mxp = mx * args.inv_h[0], myp = my * args.inv_h[1];
+          gx = cs * gxp + sn * gyp;
+          gy = cs * gyp - sn * gxp;
+          mx = cs * mxp + sn * myp;
+          my = cs * myp - sn * mxp;
+        }
+        double Q = 0.0, Qp = 0.0; // all sources; the scaled beams
         if (do_src)
         {
           double const px = (args.origin[0] + cx * args.h[0]) + args.qx[qa] * args.h[0];
           double const py = (args.origin[1] + cy * args.h[1]) + args.qx[qb] * args.h[1];
           double const pz = (args.origin[2] + cz * args.h[2]) + args.qx[slab] * args.h[2];
           Q = beam_sum(sp, px, py, pz);
+          Qp = has_cube ? scaled_beam_sum(sp, px, py, pz) : Q;
         }
         double const JxW = args.qw[qa] * args.qw[qb] * args.qw[slab] * args.vol;
         AdjQp o;
@@ -545,14 +781,22 @@ __global__ void __launch_bounds__(TD<DEG>::NT, 2)
         else if (T < sp.props[mat][Q_SOLIDUS])
           pure = !with_powder ? 0 : (s_in == 1.0 ? 2 : -1);
         double const lam_out = (with_powder && pure < 0) ? A.lam_s_out[qbase + i] : 0.0;
-        o = adj_point<NS>(sp, mat, pure, no_powder, T, mu, gx, gy, gz, mx, my, mz, s_in, lam_out, JxW, Q, hx2,
-                          hy2, hz2);
+        o = adj_point<NS>(sp, gm, mat, pure, no_powder, T, mu, gx, gy, gz, mx, my, mz, s_in, lam_out, JxW, Q,
+                          hx2, hy2, hz2);
         if (with_powder)
           A.lam_s_in[qbase + i] = o.lsin;
         g_k += o.gk;
-        g_q += o.gq;
+        g_q += (!GEN || Qp == Q) ? o.gq : (Q != 0.0 ? o.gq * (Qp / Q) : 0.0);
         g_c += o.gc;
-        double const fx = o.fx, fy = o.fy, val = o.val;
+        double fx = o.fx, fy = o.fy;
+        if (rot)
+        {
+          // back to the mesh frame, then to reference coordinates
+          double const fxp = cs * fx - sn * fy, fyp = sn * fx + cs * fy;
+          fx = fxp * args.inv_h[0];
+          fy = fyp * args.inv_h[1];
+        }
+        double const val = o.val;
         az[i] = o.fz;
   #pragma unroll
         for (int m = 0; m < N; ++m)
@@ -625,6 +869,15 @@ __global__ void __launch_bounds__(TD<DEG>::NT, 2)
         acc = fma(args.G[q][slab], vz, acc);
       }
       res[i] = active ? acc : 0.0;
+    }
+    // transposed face terms of the cells with active-boundary faces
+    if (GEN && args.faces && active && ((info >> CI_FACE_SHIFT) & 63u))
+    {
+      double fres[NQS];
+      g_c += adj_face_terms<DEG, NS>(sp, gm, A, md, yb, mb, lx, ly, lz, slab, info, mat, c, no_powder, fres);
+  #pragma unroll
+      for (int e = 0; e < NQS; ++e)
+        res[e] += fres[e];
     }
     // 6. per-node sums inside the tile (as in the forward kernel)
     static_assert(TX == 8 && TY == 4, "the node merge assumes 8 x 4 cell layers per warp");

@@ -5,16 +5,18 @@
  * forward being differentiated is adm_evolve_one_time_step
  * (ThermalPhysicsInterface::evolve_one_time_step,
  * source/ThermalPhysics.templates.hh:854-888) with the operator of
- * source/ThermalOperator.templates.hh:479-617.
+ * source/ThermalOperator.templates.hh:479-751 (cells and faces).
  *
  * Objective: J = sum_{k, p} (T_{n_k}[node_p] - target_{k,p})^2 over the
  * observation steps n_k and the observed nodes. Gradient: dJ/dlog(theta) for
  * theta = (conductivity scale, specific-heat scale, absorptivity, power),
  * i.e. theta * dJ/dtheta, where the conductivities of every state are
- * multiplied by the first, the specific heats by the second and every heat
- * source by the product of the last two. Supported: polynomial properties,
- * one to three material states (with the powder history), no deposition
- * rotation, adiabatic boundaries.
+ * multiplied by the first, the specific heats by the second and every
+ * Goldak / electron-beam source by the product of the last two (cube sources
+ * keep their value). Covered: polynomial and table properties, several
+ * materials, one to three material states (with the powder history of the
+ * cells' and the boundary faces' points), deposition-angle rotation,
+ * convective / radiative boundaries and active/inactive interfaces.
  */
 #ifndef ADAMANTINE_B200_ADJOINT_H
 #define ADAMANTINE_B200_ADJOINT_H
