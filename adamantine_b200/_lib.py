@@ -160,6 +160,8 @@ SIGNATURES = {
     "adm_mechanics_vmult": [_VP, _VP, _VP],
     "adm_mechanics_rhs": [_VP, _VP],
     "adm_mechanics_solve": [_VP, _VP, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double)],
+    "adm_mechanics_set_preconditioner": [_VP, ctypes.c_int32],
+    "adm_mechanics_multigrid_levels": [_VP, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int64)],
     "adm_mechanics_n_dofs": [_VP, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)],
     "adm_mechanics_node_mask": [_VP, _VP],
     "adm_mechanics_stress_state": [_VP, _VP, _VP, _VP],

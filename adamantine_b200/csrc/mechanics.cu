@@ -59,7 +59,24 @@ struct MechArgs
   uint8_t const *melted;
   double const *tab; // the handle's reference-element tables (kTab* offsets)
   double plastic_modulus[4], iso_hardening[4], elastic_limit[4];
+  double const *cell_coef; // multigrid levels: (lambda, mu) per cell instead of per material, or null
 };
+
+// Lame parameters of cell c
+__device__ __forceinline__ void cell_lame(MechArgs const &a, int c, double &lam, double &mu)
+{
+  if (a.cell_coef)
+  {
+    lam = a.cell_coef[2 * (int64_t)c];
+    mu = a.cell_coef[2 * (int64_t)c + 1];
+  }
+  else
+  {
+    int const mat = a.matid[c];
+    lam = a.lambda[mat];
+    mu = a.mu[mat];
+  }
+}
 
 __device__ __forceinline__ int64_t node_of(MechArgs const &a, int cx, int cy, int cz, int n)
 {
@@ -244,9 +261,7 @@ __global__ void __launch_bounds__(128) elastic_apply_kernel(MechArgs a, double c
     {
       int const c = a.cells[ci];
       int const cx = c % a.nc[0], cy = (c / a.nc[0]) % a.nc[1], cz = c / (a.nc[0] * a.nc[1]);
-      int const mat = a.matid[c];
-      lam = a.lambda[mat];
-      mu = a.mu[mat];
+      cell_lame(a, c, lam, mu);
       gidx = node_of(a, cx, cy, cz, l);
       freen = a.node_mask[gidx] == 1;
       for (int comp = 0; comp < 3; ++comp)
@@ -371,8 +386,8 @@ __global__ void __launch_bounds__(128) elastic_diag_kernel(MechArgs a, double *d
   {
     int const c = a.cells[ci];
     int const cx = c % a.nc[0], cy = (c / a.nc[0]) % a.nc[1], cz = c / (a.nc[0] * a.nc[1]);
-    int const mat = a.matid[c];
-    double const lam = a.lambda[mat], mu = a.mu[mat];
+    double lam, mu;
+    cell_lame(a, c, lam, mu);
     if (lane >= a.N)
       continue;
     int64_t const g = node_of(a, cx, cy, cz, lane);
@@ -459,6 +474,193 @@ __global__ void cg_direction_kernel(int64_t n, double const *s_new, double const
   p[i] = fma(s_new[0] / s_old[0], p[i], z[i]);
 }
 
+// ---- geometric multigrid preconditioner of the CG
+//
+// The reference preconditions its CG with algebraic multigrid
+// (MechanicalPhysics::solve, source/MechanicalPhysics.cc:488-520). Here: a
+// V-cycle over a hierarchy of structured levels, the finest the operator
+// itself (FE_Q(1) or FE_Q(2)), every coarser one FE_Q(1) rediscretized
+// on a box with half the cells per direction (per direction while that
+// count is even; an FE_Q(2) level first goes to FE_Q(1) on the same
+// cells), (lambda, mu) of a coarse cell the volume average over its
+// children (0 for children that carry no displacement); transfers are the
+// trilinear interpolation between the node lattices and its transpose;
+// the smoother is Chebyshev on diag^-1 A, the coarsest level is solved
+// exactly (dense inverse) when it is small. The same Chebyshev polynomial
+// before and after the coarse correction keeps the preconditioner
+// symmetric, as CG needs.
+
+// Node lattice of one level: x fastest with row pitch, m nodes per component.
+struct Lattice
+{
+  int nn[3];
+  int pitch;
+  int64_t m;
+};
+
+// 1-D interpolation stencil from the coarse lattice (ratio r: 1 same
+// index, 2 every other fine node coincides with a coarse one)
+__device__ __forceinline__ int mg_stencil(int i, int r, int *ci, double *cw)
+{
+  if (r == 1 || (i & 1) == 0)
+  {
+    ci[0] = i / r;
+    cw[0] = 1.0;
+    return 1;
+  }
+  ci[0] = i >> 1;
+  ci[1] = (i >> 1) + 1;
+  cw[0] = cw[1] = 0.5;
+  return 2;
+}
+
+// x_f += P x_c on the fine free rows (fine dinv != 0); the fine residual
+// buffer q_f is cleared on the way for the next operator application
+__global__ void mg_prolong_add_kernel(Lattice f, Lattice c, int r0, int r1, int r2, double const *dinv_f,
+                                      double const *xc, double *xf, double *qf)
+{
+  int64_t const t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= f.m)
+    return;
+  for (int comp = 0; comp < 3; ++comp)
+    qf[comp * f.m + t] = 0.0;
+  if (dinv_f[t] == 0.0 && dinv_f[f.m + t] == 0.0 && dinv_f[2 * f.m + t] == 0.0)
+    return;
+  int const i = (int)(t % f.pitch);
+  int64_t const rest = t / f.pitch;
+  int const j = (int)(rest % f.nn[1]), k = (int)(rest / f.nn[1]);
+  int ix[2], iy[2], iz[2];
+  double wx[2], wy[2], wz[2];
+  int const nx = mg_stencil(i, r0, ix, wx), ny = mg_stencil(j, r1, iy, wy), nz = mg_stencil(k, r2, iz, wz);
+  for (int comp = 0; comp < 3; ++comp)
+  {
+    if (dinv_f[comp * f.m + t] == 0.0)
+      continue;
+    double const *x = xc + comp * c.m;
+    double s = 0.0;
+    for (int cz = 0; cz < nz; ++cz)
+      for (int cy = 0; cy < ny; ++cy)
+        for (int cx = 0; cx < nx; ++cx)
+          s = fma(wx[cx] * wy[cy] * wz[cz], x[ix[cx] + (int64_t)c.pitch * (iy[cy] + (int64_t)c.nn[1] * iz[cz])], s);
+    xf[comp * f.m + t] += s;
+  }
+}
+
+// b_c = P^T r_f on the coarse free rows (coarse dinv != 0), 0 elsewhere;
+// only fine free rows carry residual (the others are 0)
+__global__ void mg_restrict_kernel(Lattice f, Lattice c, int r0, int r1, int r2, double const *dinv_c,
+                                   double const *rf, double *bc)
+{
+  int64_t const t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= c.m)
+    return;
+  int const I = (int)(t % c.pitch);
+  int64_t const rest = t / c.pitch;
+  int const J = (int)(rest % c.nn[1]), K = (int)(rest / c.nn[1]);
+  int const r[3] = {r0, r1, r2}, C[3] = {I, J, K};
+  int lo[3], hi[3];
+  for (int d = 0; d < 3; ++d)
+  {
+    int const cen = r[d] * C[d];
+    lo[d] = r[d] == 1 ? cen : max(cen - 1, 0);
+    hi[d] = r[d] == 1 ? cen : min(cen + 1, f.nn[d] - 1);
+  }
+  for (int comp = 0; comp < 3; ++comp)
+  {
+    double s = 0.0;
+    if (dinv_c[comp * c.m + t] != 0.0)
+    {
+      double const *x = rf + comp * f.m;
+      for (int k = lo[2]; k <= hi[2]; ++k)
+        for (int j = lo[1]; j <= hi[1]; ++j)
+          for (int i = lo[0]; i <= hi[0]; ++i)
+          {
+            double const w = (i == r0 * I ? 1.0 : 0.5) * (j == r1 * J ? 1.0 : 0.5) * (k == r2 * K ? 1.0 : 0.5);
+            s = fma(w, x[i + (int64_t)f.pitch * (j + (int64_t)f.nn[1] * k)], s);
+          }
+    }
+    bc[comp * c.m + t] = s;
+  }
+}
+
+// One Chebyshev step: d = cd d + cr dinv (b - q), x += d (first: x = d, no
+// q); q is cleared for the next operator application. Rows with dinv 0
+// (no displacement, clamped) stay 0.
+__global__ void mg_cheb_kernel(int64_t n, double const *b, double *q, double const *dinv, double *d, double *x,
+                               double cd, double cr, int first)
+{
+  int64_t const i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  double r = b[i];
+  if (!first)
+  {
+    r -= q[i];
+    q[i] = 0.0;
+  }
+  double const dn = (first ? 0.0 : cd * d[i]) + cr * dinv[i] * r;
+  d[i] = dn;
+  x[i] = first ? dn : x[i] + dn;
+}
+
+// r = b - q into rv; q cleared
+__global__ void mg_residual_kernel(int64_t n, double const *b, double *q, double *rv)
+{
+  int64_t const i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  rv[i] = b[i] - q[i];
+  q[i] = 0.0;
+}
+
+// x[idx[row]] = sum_j inv[row][j] b[idx[j]]: the coarsest level's exact
+// solve (one warp per row)
+__global__ void mg_dense_solve_kernel(int n, int64_t const *idx, double const *inv, double const *b, double *x)
+{
+  int const row = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  int const lane = threadIdx.x & 31;
+  if (row >= n)
+    return;
+  double s = 0.0;
+  for (int j = lane; j < n; j += 32)
+    s = fma(inv[(int64_t)row * n + j], b[idx[j]], s);
+  for (int o = 16; o > 0; o >>= 1)
+    s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0)
+    x[idx[row]] = s;
+}
+
+// dinv = 1 / diag on the free rows (diag != 0), 0 elsewhere
+__global__ void mg_invert_diag_kernel(int64_t n, double const *diag, double *dinv)
+{
+  int64_t const i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n)
+    dinv[i] = diag[i] != 0.0 ? 1.0 / diag[i] : 0.0;
+}
+
+// a seeded vector in [-1, 1] on the free rows (power iteration start)
+__global__ void mg_seed_kernel(int64_t n, double const *dinv, double *v)
+{
+  int64_t const i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  uint64_t h = (uint64_t)i * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull;
+  h ^= h >> 31;
+  h *= 0xBF58476D1CE4E5B9ull;
+  h ^= h >> 29;
+  v[i] = dinv[i] != 0.0 ? (double)(h >> 11) * (2.0 / 9007199254740992.0) - 1.0 : 0.0;
+}
+
+// v = dinv q / s (s on the device: a norm), q cleared
+__global__ void mg_power_kernel(int64_t n, double const *dinv, double *q, double const *s, double *v)
+{
+  int64_t const i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  v[i] = dinv[i] * q[i] / sqrt(*s);
+  q[i] = 0.0;
+}
+
 unsigned blocks_for(int64_t n) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16)); }
 
 // 1-D Gauss points / weights on [0, 1] and the Lagrange basis on the
@@ -529,33 +731,51 @@ public:
     }
     p_ = M.deg;
     N_ = (p_ + 1) * (p_ + 1) * (p_ + 1);
-    // reference-element tables
-    int const np = p_ + 1;
-    double x[3], w[3];
-    gauss_1d(np, x, w);
-    std::vector<double> val(kMaxN * kMaxN, 0.0), grad(kMaxN * kMaxN * 3, 0.0), wq(kMaxN, 0.0);
-    for (int q = 0; q < N_; ++q)
-    {
-      int const qi = q % np, qj = (q / np) % np, qk = q / (np * np);
-      wq[q] = w[qi] * w[qj] * w[qk];
-      for (int n = 0; n < N_; ++n)
-      {
-        int const ni = n % np, nj = (n / np) % np, nk = n / (np * np);
-        double const vx = lag(p_, ni, x[qi]), vy = lag(p_, nj, x[qj]), vz = lag(p_, nk, x[qk]);
-        val[q * kMaxN + n] = vx * vy * vz;
-        grad[(q * kMaxN + n) * 3 + 0] = lag_d(p_, ni, x[qi]) * vy * vz;
-        grad[(q * kMaxN + n) * 3 + 1] = vx * lag_d(p_, nj, x[qj]) * vz;
-        grad[(q * kMaxN + n) * 3 + 2] = vx * vy * lag_d(p_, nk, x[qk]);
-      }
-    }
     ADM_CK(cudaSetDevice(th_.device_));
-    std::vector<double> tab(kTabSize, 0.0);
-    std::copy(val.begin(), val.end(), tab.begin() + kTabVal);
-    std::copy(grad.begin(), grad.end(), tab.begin() + kTabGrad);
-    std::copy(wq.begin(), wq.end(), tab.begin() + kTabWq);
+    // reference-element tables of the degree, and of FE_Q(1) for the
+    // multigrid levels
+    std::vector<double> const tab = element_tables(p_);
     tab_.alloc(kTabSize);
     ADM_CK(cudaMemcpyAsync(tab_.p, tab.data(), kTabSize * sizeof(double), cudaMemcpyHostToDevice, th_.stream_));
+    tab1_h_ = element_tables(1);
+    tab1_.alloc(kTabSize);
+    ADM_CK(cudaMemcpyAsync(tab1_.p, tab1_h_.data(), kTabSize * sizeof(double), cudaMemcpyHostToDevice,
+                           th_.stream_));
     ADM_CK(cudaStreamSynchronize(th_.stream_));
+  }
+
+  ~Mechanics()
+  {
+    release_vcycle_graph();
+    if (cap_stream_)
+      cudaStreamDestroy(cap_stream_);
+  }
+  Mechanics(Mechanics const &) = delete;
+  Mechanics &operator=(Mechanics const &) = delete;
+
+  // values [q][n], reference gradients [q][n][d] and weights of the
+  // (p+1)^3 Gauss points of FE_Q(p) on [0, 1]^3, at the kTab* offsets
+  static std::vector<double> element_tables(int p)
+  {
+    int const np = p + 1, N = np * np * np;
+    double x[3], w[3];
+    gauss_1d(np, x, w);
+    std::vector<double> tab(kTabSize, 0.0);
+    for (int q = 0; q < N; ++q)
+    {
+      int const qi = q % np, qj = (q / np) % np, qk = q / (np * np);
+      tab[kTabWq + q] = w[qi] * w[qj] * w[qk];
+      for (int n = 0; n < N; ++n)
+      {
+        int const ni = n % np, nj = (n / np) % np, nk = n / (np * np);
+        double const vx = lag(p, ni, x[qi]), vy = lag(p, nj, x[qj]), vz = lag(p, nk, x[qk]);
+        tab[kTabVal + q * kMaxN + n] = vx * vy * vz;
+        tab[kTabGrad + (q * kMaxN + n) * 3 + 0] = lag_d(p, ni, x[qi]) * vy * vz;
+        tab[kTabGrad + (q * kMaxN + n) * 3 + 1] = vx * lag_d(p, nj, x[qj]) * vz;
+        tab[kTabGrad + (q * kMaxN + n) * 3 + 2] = vx * vy * lag_d(p, nk, x[qk]);
+      }
+    }
+    return tab;
   }
 
   void setup(double const *temperature)
@@ -633,6 +853,9 @@ public:
       ADM_CK(cudaGetLastError());
     }
     ADM_CK(cudaStreamSynchronize(s));
+    carry_now_ = carry;
+    release_vcycle_graph();
+    mg_.clear();
     ready_ = true;
   }
 
@@ -654,8 +877,8 @@ public:
     ADM_CK(cudaStreamSynchronize(th_.stream_));
   }
 
-  // Jacobi-preconditioned CG from x = 0 (the constrained and absent entries
-  // stay 0): stops at |r| <= rel_tol |rhs| (SolverControl of
+  // Preconditioned CG (multigrid V-cycle or Jacobi) from x = 0 (the
+  // constrained and absent entries stay 0): stops at |r| <= rel_tol |rhs| (SolverControl of
   // MechanicalPhysics::solve) or after max_iter iterations (an error).
   void solve(double *x, int32_t *iterations, double *residual)
   {
@@ -669,7 +892,10 @@ public:
     qv_.alloc(n);
     sc_.alloc(8);
     ADM_CK(cudaMemsetAsync(x, 0, n * sizeof(double), s));
+    ADM_CK(cudaMemsetAsync(z_.p, 0, n * sizeof(double), s));
     ADM_CK(cudaMemcpyAsync(r_.p, rhs_.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    if (precond_ == ADM_MECH_PRECONDITIONER_MULTIGRID && mg_.empty() && n_cells_ > 0)
+      setup_multigrid();
     double const rhs_norm = std::sqrt(dot(rhs_.p, rhs_.p, 0));
     double const tol = (cfg_.rel_tol > 0.0 ? cfg_.rel_tol : 1e-12) * rhs_norm;
     int const max_iter = cfg_.max_iter > 0 ? cfg_.max_iter : (int)std::max<int64_t>(1, n_dofs_);
@@ -719,6 +945,21 @@ public:
     if (plastic)
       ADM_CK(cudaMemcpyAsync(plastic, kappa_.p, cq * sizeof(double), cudaMemcpyDeviceToDevice, s));
     ADM_CK(cudaStreamSynchronize(s));
+  }
+
+  void set_preconditioner(int kind)
+  {
+    if (kind != ADM_MECH_PRECONDITIONER_JACOBI && kind != ADM_MECH_PRECONDITIONER_MULTIGRID)
+      throw Error(ADM_ERR_INVALID, "unknown preconditioner");
+    precond_ = kind;
+  }
+
+  void multigrid_levels(int32_t *n_levels, int64_t *coarsest) const
+  {
+    if (n_levels)
+      *n_levels = (int32_t)mg_.size();
+    if (coarsest)
+      *coarsest = mg_.empty() ? 0 : 3 * mg_.back()->n_free;
   }
 
   int64_t n_dofs() const { return n_dofs_; }
@@ -864,9 +1105,464 @@ private:
 
   void precondition(double const *r, double *z)
   {
+    if (precond_ == ADM_MECH_PRECONDITIONER_MULTIGRID)
+    {
+      // the V-cycle (some 20 launches per level) replays as one CUDA graph,
+      // captured on a stream of our own (the handle's may be the legacy
+      // default stream, which cannot be captured)
+      if (!vc_exec_ || vc_r_ != r || vc_z_ != z)
+      {
+        release_vcycle_graph();
+        if (!cap_stream_)
+          ADM_CK(cudaStreamCreateWithFlags(&cap_stream_, cudaStreamNonBlocking));
+        MgLevel &L = *mg_[0];
+        L.bp = const_cast<double *>(r);
+        L.xp = z;
+        cudaGraph_t graph;
+        ls_ = cap_stream_;
+        ADM_CK(cudaStreamBeginCapture(cap_stream_, cudaStreamCaptureModeThreadLocal));
+        try
+        {
+          mg_vcycle(0);
+        }
+        catch (...)
+        {
+          cudaStreamEndCapture(cap_stream_, &graph);
+          ls_ = nullptr;
+          throw;
+        }
+        cudaError_t const e = cudaStreamEndCapture(cap_stream_, &graph);
+        ls_ = nullptr;
+        ADM_CK(e);
+        ADM_CK(cudaGraphInstantiate(&vc_exec_, graph, 0));
+        cudaGraphDestroy(graph);
+        vc_r_ = r;
+        vc_z_ = z;
+      }
+      ADM_CK(cudaGraphLaunch(vc_exec_, th_.stream_));
+      return;
+    }
     int64_t const n = 3 * m_;
     jacobi_kernel<<<(unsigned)((n + 255) / 256), 256, 0, th_.stream_>>>(n, r, diag_.p, z);
     ADM_CK(cudaGetLastError());
+  }
+
+  // ---- geometric multigrid (the kernels' comment above tells the design)
+  static constexpr int kSmoothDegree = 3;   // Chebyshev steps before and after the coarse correction
+  static constexpr double kSmoothRange = 15.0; // smoothed part of the spectrum: [lmax / range, lmax]
+  static constexpr int kCoarseDegree = 12;  // Chebyshev steps on a coarsest level too large to invert
+  static constexpr int kDirectMax = 640;    // free DoFs of a coarsest level solved by a dense inverse
+  static constexpr int kPowerSteps = 16;    // power iterations for lmax(diag^-1 A)
+
+  struct MgLevel
+  {
+    int p = 1, N = 8;
+    int nc[3] = {0, 0, 0};
+    int r[3] = {1, 1, 1}; // node-lattice ratio to the next coarser level
+    double h[3] = {0, 0, 0};
+    Lattice lat{};
+    std::vector<uint8_t> carry; // per cell: carries displacement
+    std::vector<double> coef;   // per cell: (lambda, mu), 0 where it carries none
+    std::vector<uint8_t> mask;  // per node: 0 none, 1 free, 2 clamped
+    int64_t n_cells = 0, n_free = 0;
+    DevBuf<int32_t> cells;
+    DevBuf<uint8_t> maskd;
+    DevBuf<double> coefd, dinv, b, x, q, d;
+    double *bp = nullptr, *xp = nullptr; // right-hand side and solution (level 0: the CG's)
+    std::vector<double> cd, cr;          // Chebyshev step coefficients
+    double lmax = 0.0;
+    int n_direct = 0; // > 0: coarsest level solved by the dense inverse
+    DevBuf<int64_t> didx;
+    DevBuf<double> dinvm;
+    MechArgs a{};
+  };
+
+  int64_t count_free(std::vector<uint8_t> const &mask) const
+  {
+    int64_t n = 0;
+    for (uint8_t v : mask)
+      n += v == 1;
+    return n;
+  }
+
+  // node mask of a box level from the cells that carry displacement
+  std::vector<uint8_t> level_mask(MgLevel const &L) const
+  {
+    std::vector<uint8_t> mask(L.lat.m, 0);
+    int const np = L.p + 1;
+    for (int64_t c = 0; c < (int64_t)L.carry.size(); ++c)
+    {
+      if (!L.carry[c])
+        continue;
+      int const cx = (int)(c % L.nc[0]), cy = (int)((c / L.nc[0]) % L.nc[1]), cz = (int)(c / ((int64_t)L.nc[0] * L.nc[1]));
+      for (int n = 0; n < L.N; ++n)
+      {
+        int const ijk[3] = {L.p * cx + n % np, L.p * cy + (n / np) % np, L.p * cz + n / (np * np)};
+        bool clamped = false;
+        for (int f = 0; f < 6; ++f)
+          if ((cfg_.clamped_faces >> f) & 1)
+            clamped = clamped || ijk[f / 2] == ((f & 1) ? L.lat.nn[f / 2] - 1 : 0);
+        uint8_t &mk = mask[ijk[0] + (int64_t)L.lat.pitch * (ijk[1] + (int64_t)L.lat.nn[1] * ijk[2])];
+        mk = clamped ? 2 : std::max<uint8_t>(mk, 1);
+      }
+    }
+    return mask;
+  }
+
+  // the stream the V-cycle's launches go to (the capture stream while one
+  // is captured)
+  cudaStream_t ls() const { return ls_ ? ls_ : th_.stream_; }
+
+  void release_vcycle_graph()
+  {
+    if (vc_exec_)
+      cudaGraphExecDestroy(vc_exec_);
+    vc_exec_ = nullptr;
+    vc_r_ = nullptr;
+    vc_z_ = nullptr;
+  }
+
+  void mg_apply(MgLevel &L, double const *src)
+  {
+    if (L.n_cells == 0)
+      return;
+    int64_t const per_warp = 32 / L.N;
+    unsigned const nb =
+        (unsigned)std::max<int64_t>(1, std::min<int64_t>((L.n_cells + 4 * per_warp - 1) / (4 * per_warp), 148 * 16));
+    elastic_apply_kernel<<<nb, 128, 0, ls()>>>(L.a, src, L.q.p);
+    ADM_CK(cudaGetLastError());
+  }
+
+  void mg_smooth(MgLevel &L, bool zero_start)
+  {
+    cudaStream_t const s = ls();
+    int64_t const n = 3 * L.lat.m;
+    for (size_t j = 0; j < L.cd.size(); ++j)
+    {
+      bool const first = zero_start && j == 0;
+      if (!first)
+        mg_apply(L, L.xp);
+      mg_cheb_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, L.bp, L.q.p, L.dinv.p, L.d.p, L.xp, L.cd[j],
+                                                                  L.cr[j], first ? 1 : 0);
+      ADM_CK(cudaGetLastError());
+    }
+  }
+
+  void mg_vcycle(size_t l)
+  {
+    cudaStream_t const s = ls();
+    MgLevel &L = *mg_[l];
+    if (l + 1 == mg_.size())
+    {
+      if (L.n_direct > 0)
+      {
+        mg_dense_solve_kernel<<<(unsigned)((L.n_direct + 7) / 8), 256, 0, s>>>(L.n_direct, L.didx.p, L.dinvm.p,
+                                                                                L.bp, L.xp);
+        ADM_CK(cudaGetLastError());
+      }
+      else
+        mg_smooth(L, true);
+      return;
+    }
+    MgLevel &C = *mg_[l + 1];
+    int64_t const n = 3 * L.lat.m;
+    mg_smooth(L, true);
+    mg_apply(L, L.xp);
+    mg_residual_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, L.bp, L.q.p, L.d.p);
+    mg_restrict_kernel<<<(unsigned)((C.lat.m + 255) / 256), 256, 0, s>>>(L.lat, C.lat, L.r[0], L.r[1], L.r[2],
+                                                                         C.dinv.p, L.d.p, C.bp);
+    ADM_CK(cudaGetLastError());
+    mg_vcycle(l + 1);
+    mg_prolong_add_kernel<<<(unsigned)((L.lat.m + 255) / 256), 256, 0, s>>>(L.lat, C.lat, L.r[0], L.r[1], L.r[2],
+                                                                            L.dinv.p, C.xp, L.xp, L.q.p);
+    ADM_CK(cudaGetLastError());
+    mg_smooth(L, false);
+  }
+
+  // the level's device buffers, its operator arguments and diag^-1
+  void mg_device(MgLevel &L, bool finest)
+  {
+    cudaStream_t const s = th_.stream_;
+    int64_t const n = 3 * L.lat.m;
+    L.dinv.alloc(n);
+    L.q.alloc(n);
+    L.d.alloc(n);
+    ADM_CK(cudaMemsetAsync(L.q.p, 0, n * sizeof(double), s));
+    ADM_CK(cudaMemsetAsync(L.d.p, 0, n * sizeof(double), s));
+    if (finest)
+    {
+      L.a = args();
+      mg_invert_diag_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, diag_.p, L.dinv.p);
+      ADM_CK(cudaGetLastError());
+      return;
+    }
+    std::vector<int32_t> cells;
+    for (int64_t c = 0; c < (int64_t)L.carry.size(); ++c)
+      if (L.carry[c])
+        cells.push_back((int32_t)c);
+    L.n_cells = (int64_t)cells.size();
+    L.cells.alloc(std::max<size_t>(1, cells.size()));
+    L.maskd.alloc(L.lat.m);
+    L.coefd.alloc(std::max<size_t>(2, L.coef.size()));
+    L.b.alloc(n);
+    L.x.alloc(n);
+    ADM_CK(cudaMemsetAsync(L.x.p, 0, n * sizeof(double), s));
+    if (!cells.empty())
+      ADM_CK(cudaMemcpyAsync(L.cells.p, cells.data(), cells.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    ADM_CK(cudaMemcpyAsync(L.maskd.p, L.mask.data(), L.lat.m, cudaMemcpyHostToDevice, s));
+    ADM_CK(cudaMemcpyAsync(L.coefd.p, L.coef.data(), L.coef.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    L.bp = L.b.p;
+    L.xp = L.x.p;
+    MechArgs a = args();
+    a.p = 1;
+    a.N = 8;
+    for (int d = 0; d < 3; ++d)
+    {
+      a.nc[d] = L.nc[d];
+      a.nn[d] = L.lat.nn[d];
+      a.inv_h[d] = 1.0 / L.h[d];
+    }
+    a.pitch = L.lat.pitch;
+    a.m = L.lat.m;
+    a.jxw = L.h[0] * L.h[1] * L.h[2];
+    a.cells = L.cells.p;
+    a.n_cells = (int)L.n_cells;
+    a.node_mask = L.maskd.p;
+    a.cell_coef = L.coefd.p;
+    a.tab = tab1_.p;
+    L.a = a;
+    // diag^-1 (the diagonal kernel with these arguments; q serves as scratch)
+    unsigned const nb = (unsigned)std::max<int64_t>(1, std::min<int64_t>((L.n_cells + 3) / 4, 148 * 16));
+    if (L.n_cells > 0)
+      elastic_diag_kernel<<<nb, 128, 0, s>>>(a, L.q.p);
+    mg_invert_diag_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, L.q.p, L.dinv.p);
+    ADM_CK(cudaGetLastError());
+    ADM_CK(cudaMemsetAsync(L.q.p, 0, n * sizeof(double), s));
+  }
+
+  // lmax(diag^-1 A) by power iteration, then the Chebyshev coefficients
+  void mg_chebyshev(MgLevel &L, int degree)
+  {
+    cudaStream_t const s = th_.stream_;
+    int64_t const n = 3 * L.lat.m;
+    mg_seed_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, L.dinv.p, L.d.p);
+    ADM_CK(cudaGetLastError());
+    double nv = dot_n(L.d.p, L.d.p, n, 4);
+    double lmax = 0.0;
+    for (int it = 0; it < kPowerSteps && nv > 0.0; ++it)
+    {
+      mg_apply(L, L.d.p);
+      mg_power_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, L.dinv.p, L.q.p, sc_.p + 4, L.d.p);
+      ADM_CK(cudaGetLastError());
+      nv = dot_n(L.d.p, L.d.p, n, 4);
+      lmax = std::sqrt(nv);
+    }
+    ADM_CK(cudaMemsetAsync(L.d.p, 0, n * sizeof(double), s));
+    L.lmax = lmax;
+    double const upper = 1.2 * (lmax > 0.0 ? lmax : 1.0), lower = upper / kSmoothRange;
+    double const theta = 0.5 * (upper + lower), delta = 0.5 * (upper - lower), sigma = theta / delta;
+    L.cd.assign(1, 0.0);
+    L.cr.assign(1, 1.0 / theta);
+    double rho = 1.0 / sigma;
+    for (int j = 1; j < degree; ++j)
+    {
+      double const rn = 1.0 / (2.0 * sigma - rho);
+      L.cd.push_back(rn * rho);
+      L.cr.push_back(2.0 * rn / delta);
+      rho = rn;
+    }
+  }
+
+  // dense inverse of the coarsest FE_Q(1) level's operator on its free DoFs
+  void mg_direct(MgLevel &L)
+  {
+    std::vector<int64_t> idx;
+    std::vector<int64_t> pos(3 * L.lat.m, -1);
+    for (int comp = 0; comp < 3; ++comp)
+      for (int64_t g = 0; g < L.lat.m; ++g)
+        if (L.mask[g] == 1)
+        {
+          pos[comp * L.lat.m + g] = (int64_t)idx.size();
+          idx.push_back(comp * L.lat.m + g);
+        }
+    int const n = (int)idx.size();
+    std::vector<double> K((size_t)n * n, 0.0);
+    double const inv_h[3] = {1.0 / L.h[0], 1.0 / L.h[1], 1.0 / L.h[2]};
+    double const jxw = L.h[0] * L.h[1] * L.h[2];
+    for (int64_t c = 0; c < (int64_t)L.carry.size(); ++c)
+    {
+      if (!L.carry[c])
+        continue;
+      double const lam = L.coef[2 * c], mu = L.coef[2 * c + 1];
+      int const cx = (int)(c % L.nc[0]), cy = (int)((c / L.nc[0]) % L.nc[1]), cz = (int)(c / ((int64_t)L.nc[0] * L.nc[1]));
+      int64_t g[8];
+      for (int a = 0; a < 8; ++a)
+        g[a] = (cx + (a & 1)) + (int64_t)L.lat.pitch * ((cy + ((a >> 1) & 1)) + (int64_t)L.lat.nn[1] * (cz + (a >> 2)));
+      for (int q = 0; q < 8; ++q)
+      {
+        double const jw = jxw * tab1_h_[kTabWq + q];
+        double gr[8][3];
+        for (int a = 0; a < 8; ++a)
+          for (int d = 0; d < 3; ++d)
+            gr[a][d] = tab1_h_[kTabGrad + (q * kMaxN + a) * 3 + d] * inv_h[d];
+        for (int a = 0; a < 8; ++a)
+          for (int ca = 0; ca < 3; ++ca)
+          {
+            int64_t const ra = pos[ca * L.lat.m + g[a]];
+            if (ra < 0)
+              continue;
+            for (int b = 0; b < 8; ++b)
+              for (int cb = 0; cb < 3; ++cb)
+              {
+                int64_t const rb = pos[cb * L.lat.m + g[b]];
+                if (rb < 0)
+                  continue;
+                double v = lam * gr[a][ca] * gr[b][cb] + mu * gr[a][cb] * gr[b][ca];
+                if (ca == cb)
+                  v += mu * (gr[a][0] * gr[b][0] + gr[a][1] * gr[b][1] + gr[a][2] * gr[b][2]);
+                K[(size_t)ra * n + rb] += jw * v;
+              }
+          }
+      }
+    }
+    // Cholesky K = L L^T (lower, in place), then the inverse column by column
+    for (int j = 0; j < n; ++j)
+    {
+      double dsum = K[(size_t)j * n + j];
+      for (int k = 0; k < j; ++k)
+        dsum -= K[(size_t)j * n + k] * K[(size_t)j * n + k];
+      if (!(dsum > 0.0))
+        throw Error(ADM_ERR_DEVICE, "the coarsest multigrid level is not positive definite");
+      double const ljj = std::sqrt(dsum);
+      K[(size_t)j * n + j] = ljj;
+      for (int i = j + 1; i < n; ++i)
+      {
+        double v = K[(size_t)i * n + j];
+        for (int k = 0; k < j; ++k)
+          v -= K[(size_t)i * n + k] * K[(size_t)j * n + k];
+        K[(size_t)i * n + j] = v / ljj;
+      }
+    }
+    std::vector<double> inv((size_t)n * n, 0.0), col(n);
+    for (int e = 0; e < n; ++e)
+    {
+      for (int i = 0; i < n; ++i)
+      {
+        double v = i == e ? 1.0 : 0.0;
+        for (int k = 0; k < i; ++k)
+          v -= K[(size_t)i * n + k] * col[k];
+        col[i] = v / K[(size_t)i * n + i];
+      }
+      for (int i = n - 1; i >= 0; --i)
+      {
+        double v = col[i];
+        for (int k = i + 1; k < n; ++k)
+          v -= K[(size_t)k * n + i] * col[k];
+        col[i] = v / K[(size_t)i * n + i];
+      }
+      for (int i = 0; i < n; ++i)
+        inv[(size_t)i * n + e] = col[i];
+    }
+    cudaStream_t const s = th_.stream_;
+    L.n_direct = n;
+    L.didx.alloc(std::max(1, n));
+    L.dinvm.alloc(std::max<size_t>(1, (size_t)n * n));
+    if (n > 0)
+    {
+      ADM_CK(cudaMemcpyAsync(L.didx.p, idx.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+      ADM_CK(cudaMemcpyAsync(L.dinvm.p, inv.data(), (size_t)n * n * sizeof(double), cudaMemcpyHostToDevice, s));
+    }
+    ADM_CK(cudaStreamSynchronize(s));
+  }
+
+  // the level hierarchy for the current cells (built at the first
+  // multigrid solve after a setup)
+  void setup_multigrid()
+  {
+    Mesh const &M = th_.mesh_;
+    release_vcycle_graph();
+    mg_.clear();
+    sc_.alloc(8);
+    auto L0 = std::make_unique<MgLevel>();
+    L0->p = p_;
+    L0->N = N_;
+    for (int d = 0; d < 3; ++d)
+    {
+      L0->nc[d] = M.nc[d];
+      L0->h[d] = M.h[d];
+      L0->lat.nn[d] = M.nn[d];
+    }
+    L0->lat.pitch = M.pitch;
+    L0->lat.m = m_;
+    L0->carry = carry_now_;
+    L0->coef.assign(2 * carry_now_.size(), 0.0);
+    for (size_t c = 0; c < carry_now_.size(); ++c)
+      if (carry_now_[c])
+      {
+        L0->coef[2 * c] = cfg_.lame_first[th_.matid_[c]];
+        L0->coef[2 * c + 1] = cfg_.lame_second[th_.matid_[c]];
+      }
+    L0->mask = mask_h_;
+    L0->n_cells = n_cells_;
+    L0->n_free = count_free(mask_h_);
+    mg_device(*L0, true);
+    mg_.push_back(std::move(L0));
+    while (mg_.size() < 16)
+    {
+      MgLevel &F = *mg_.back();
+      int rc[3];
+      if (F.p == 2)
+        rc[0] = rc[1] = rc[2] = 1; // FE_Q(1) on the same cells
+      else
+      {
+        if (3 * F.n_free <= kDirectMax)
+          break;
+        for (int d = 0; d < 3; ++d)
+          rc[d] = (F.nc[d] % 2 == 0) ? 2 : 1;
+        if (rc[0] == 1 && rc[1] == 1 && rc[2] == 1)
+          break;
+      }
+      auto C = std::make_unique<MgLevel>();
+      for (int d = 0; d < 3; ++d)
+      {
+        C->nc[d] = F.nc[d] / rc[d];
+        C->h[d] = F.h[d] * rc[d];
+        C->lat.nn[d] = C->nc[d] + 1;
+        F.r[d] = F.p == 2 ? 2 : rc[d];
+      }
+      C->lat.pitch = C->lat.nn[0];
+      C->lat.m = (int64_t)C->lat.nn[0] * C->lat.nn[1] * C->lat.nn[2];
+      int64_t const nC = (int64_t)C->nc[0] * C->nc[1] * C->nc[2];
+      C->carry.assign(nC, 0);
+      C->coef.assign(2 * nC, 0.0);
+      double const share = 1.0 / (rc[0] * rc[1] * rc[2]);
+      for (int64_t c = 0; c < (int64_t)F.carry.size(); ++c)
+      {
+        if (!F.carry[c])
+          continue;
+        int const fx = (int)(c % F.nc[0]), fy = (int)((c / F.nc[0]) % F.nc[1]), fz = (int)(c / ((int64_t)F.nc[0] * F.nc[1]));
+        int64_t const cc = fx / rc[0] + (int64_t)C->nc[0] * (fy / rc[1] + (int64_t)C->nc[1] * (fz / rc[2]));
+        C->carry[cc] = 1;
+        C->coef[2 * cc] += share * F.coef[2 * c];
+        C->coef[2 * cc + 1] += share * F.coef[2 * c + 1];
+      }
+      C->mask = level_mask(*C);
+      C->n_free = count_free(C->mask);
+      mg_device(*C, false);
+      mg_.push_back(std::move(C));
+    }
+    // smoothers on every level but a coarsest one small enough to invert
+    MgLevel &last = *mg_.back();
+    bool const direct = last.p == 1 && 3 * last.n_free <= kDirectMax;
+    for (size_t l = 0; l < mg_.size(); ++l)
+    {
+      bool const coarsest = l + 1 == mg_.size();
+      if (coarsest && direct)
+        mg_direct(*mg_[l]);
+      else
+        mg_chebyshev(*mg_[l], coarsest ? kCoarseDegree : kSmoothDegree);
+    }
+    ADM_CK(cudaStreamSynchronize(th_.stream_));
   }
 
   // sc[slot] = x . y on the device (no read-back: the CG's scalars stay
@@ -878,6 +1574,19 @@ private:
     ADM_CK(cudaMemsetAsync(sc_.p + slot, 0, sizeof(double), s));
     dot_kernel<<<blocks_for(n), 256, 0, s>>>(n, x, y, sc_.p + slot);
     ADM_CK(cudaGetLastError());
+  }
+
+  // sc[slot] = x . y over n entries (device), also returned to the host
+  double dot_n(double const *x, double const *y, int64_t n, int slot)
+  {
+    cudaStream_t const s = th_.stream_;
+    ADM_CK(cudaMemsetAsync(sc_.p + slot, 0, sizeof(double), s));
+    dot_kernel<<<blocks_for(n), 256, 0, s>>>(n, x, y, sc_.p + slot);
+    ADM_CK(cudaGetLastError());
+    double v = 0.0;
+    ADM_CK(cudaMemcpyAsync(&v, sc_.p + slot, sizeof(double), cudaMemcpyDeviceToHost, s));
+    ADM_CK(cudaStreamSynchronize(s));
+    return v;
   }
 
   // sc[slot] = x . y (device), also returned to the host
@@ -899,7 +1608,16 @@ private:
   std::vector<uint8_t> mask_h_;
   DevBuf<int32_t> cells_;
   DevBuf<uint8_t> mask_, matid_, melted_;
-  DevBuf<double> tab_; // reference-element tables of this handle's degree
+  DevBuf<double> tab_;  // reference-element tables of this handle's degree
+  DevBuf<double> tab1_; // and of FE_Q(1) (multigrid levels)
+  std::vector<double> tab1_h_;
+  std::vector<uint8_t> carry_now_; // cells that carry displacement (last setup)
+  std::vector<std::unique_ptr<MgLevel>> mg_;
+  int precond_ = ADM_MECH_PRECONDITIONER_MULTIGRID;
+  cudaStream_t cap_stream_ = nullptr, ls_ = nullptr;
+  cudaGraphExec_t vc_exec_ = nullptr; // the captured V-cycle and the CG vectors it reads and writes
+  double const *vc_r_ = nullptr;
+  double *vc_z_ = nullptr;
   DevBuf<double> rhs_, diag_, r_, z_, pv_, qv_, sc_;
   // J2 state of the Gauss points and the previous displacement
   DevBuf<double> kappa_, stress_, back_, u_old_;
@@ -962,6 +1680,22 @@ int adm_mechanics_solve(adm_mechanics *h, double *displacement, int32_t *iterati
   return adm::guard([&] {
     ADM_REQUIRE(h && displacement, "null argument");
     h->m->solve(displacement, iterations, residual);
+  });
+}
+
+int adm_mechanics_set_preconditioner(adm_mechanics *h, int32_t kind)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h, "null handle");
+    h->m->set_preconditioner(kind);
+  });
+}
+
+int adm_mechanics_multigrid_levels(adm_mechanics const *h, int32_t *n_levels, int64_t *coarsest_dofs)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h, "null handle");
+    h->m->multigrid_levels(n_levels, coarsest_dofs);
   });
 }
 

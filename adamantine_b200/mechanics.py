@@ -5,7 +5,8 @@ driver uses it after the thermal step (application/adamantine.hh:1289-1345):
 ``setup_dofs`` picks the cells that carry displacement (thermally active,
 solid ratio above 0.99) and forms the right-hand side from the temperature
 (thermal expansion from the reference temperature, gravity); ``solve`` runs
-CG on the elasticity operator and returns the displacement, then updates
+CG on the elasticity operator (preconditioned by a geometric multigrid
+V-cycle, or by the diagonal) and returns the displacement, then updates
 the stress at the Gauss points from the displacement increment with the
 reference's combined isotropic-kinematic J2 model (compute_stress,
 source/MechanicalPhysics.cc:542-634); ``stress_state`` returns the stress,
@@ -130,6 +131,19 @@ class MechanicalPhysics:
         _lib.check(self._L.adm_mechanics_solve(self._h, _dev(x), ctypes.byref(it), ctypes.byref(res)))
         self.iterations, self.residual = int(it.value), float(res.value)
         return x
+
+    def set_preconditioner(self, kind: str):
+        """'multigrid' (the default: V-cycle over FE_Q(1) levels of the box,
+        Chebyshev smoothing, exact coarsest solve) or 'jacobi'."""
+        code = {"jacobi": 0, "multigrid": 1}[kind]
+        _lib.check(self._L.adm_mechanics_set_preconditioner(self._h, code))
+
+    def multigrid_levels(self):
+        """(levels, free DoFs of the coarsest level) of the hierarchy the
+        last multigrid solve built (0, 0 before one)."""
+        n, c = ctypes.c_int32(), ctypes.c_int64()
+        _lib.check(self._L.adm_mechanics_multigrid_levels(self._h, ctypes.byref(n), ctypes.byref(c)))
+        return int(n.value), int(c.value)
 
     @property
     def n_dofs(self) -> int:

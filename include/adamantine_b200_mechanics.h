@@ -83,6 +83,14 @@ typedef struct adm_mech_config
 
 typedef struct adm_mechanics adm_mechanics;
 
+/* Preconditioners of the CG (MechanicalPhysics::solve preconditions with
+ * algebraic multigrid): the diagonal, or a geometric multigrid V-cycle
+ * (the default) over FE_Q(1) levels of the box with half the cells per
+ * direction each, Chebyshev smoothing on diag^-1 A and an exact solve of
+ * the coarsest level. */
+#define ADM_MECH_PRECONDITIONER_JACOBI 0
+#define ADM_MECH_PRECONDITIONER_MULTIGRID 1
+
 /* Bound to a set-up thermal handle, which must outlive it. */
 int adm_mechanics_create(adm_thermal *thermal, adm_mech_config const *cfg, adm_mechanics **out);
 int adm_mechanics_destroy(adm_mechanics *h);
@@ -99,6 +107,11 @@ int adm_mechanics_rhs(adm_mechanics *h, double *dst);
 /* MechanicalPhysics::solve (elastic): displacement (device, 3 x
  * adm_n_nodes), CG iterations and final residual norm. */
 int adm_mechanics_solve(adm_mechanics *h, double *displacement, int32_t *iterations, double *residual);
+/* Selects the CG preconditioner (ADM_MECH_PRECONDITIONER_*). */
+int adm_mechanics_set_preconditioner(adm_mechanics *h, int32_t kind);
+/* Levels of the multigrid hierarchy (built at the first multigrid solve
+ * after a setup; 0 before) and the free DoFs of its coarsest level. */
+int adm_mechanics_multigrid_levels(adm_mechanics const *h, int32_t *n_levels, int64_t *coarsest_dofs);
 /* Counts: displacement DoFs (3 per node of a cell that carries
  * displacement, clamped ones included) and cells that carry displacement. */
 int adm_mechanics_n_dofs(adm_mechanics const *h, int64_t *n_dofs, int64_t *n_cells);
