@@ -137,6 +137,7 @@ SIGNATURES = {
     "adm_amr_refine_mesh": [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32],
     "adm_amr_execute": [_VP, _VP, _VP],
     "adm_amr_n_dofs": [_VP, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)],
+    "adm_amr_remesh_profile": [_VP, _VP],
     "adm_amr_n_leaves": [_VP, ctypes.POINTER(ctypes.c_int64)],
     "adm_amr_leaves": [_VP, _VP],
     "adm_amr_dof_lattice": [_VP, _VP],

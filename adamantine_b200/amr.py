@@ -181,6 +181,15 @@ class AmrThermalPhysics(_Common):
         r, c = self._flags(refine, lv), self._flags(coarsen, lv)
         self._call("execute", _p(r), _p(c))
 
+    REMESH_PHASES = ("snapshot", "flag_and_execute", "nodes_and_constraints", "level_setup", "cell_state_transfer",
+                     "prolongation_tables", "solution_transfer", "inverse_mass")
+
+    def remesh_profile(self) -> dict:
+        """Host wall time (ms) of the last refine_mesh / execute per phase."""
+        ms = np.zeros(len(self.REMESH_PHASES))
+        self._call("remesh_profile", _p(ms))
+        return dict(zip(self.REMESH_PHASES, ms.tolist()))
+
     # ---- vectors
     def new_vector(self) -> torch.Tensor:
         return torch.zeros(self.n_dofs, dtype=torch.float64, device=self.device)

@@ -45,6 +45,7 @@
 
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -54,6 +55,7 @@
 
 namespace adm
 {
+constexpr int kRemeshPhases = ADM_AMR_REMESH_PHASES;
 namespace
 {
 
@@ -227,7 +229,7 @@ struct AmrMesh
   int64_t NX[3] = {0, 0, 0};
   // composite DoFs (sorted lattice keys) and hanging constraints
   std::vector<int64_t> dof_key;
-  std::unordered_map<int64_t, int32_t> dof_of;
+  std::vector<uint8_t> node_map; // lattice byte map of the last build (1 node, 2 hanging)
   std::unordered_map<int64_t, std::vector<std::pair<int32_t, double>>> hanging;
   int64_t n_nodes_all = 0; // distinct node positions of the active leaves
 
@@ -358,9 +360,30 @@ struct AmrMesh
     double h[3];
     for (int d = 0; d < 3; ++d)
       h[d] = cfg.extent[d] / (double)forest.n(l, d);
-    for (int64_t k = 0; k < forest.n(l, 2); ++k)
-      for (int64_t j = 0; j < forest.n(l, 1); ++j)
-        for (int64_t i = 0; i < forest.n(l, 0); ++i)
+    // only the cells that meet the boxes' union can meet a box
+    double ulo[3] = {std::numeric_limits<double>::max(), std::numeric_limits<double>::max(),
+                     std::numeric_limits<double>::max()};
+    double uhi[3] = {std::numeric_limits<double>::lowest(), std::numeric_limits<double>::lowest(),
+                     std::numeric_limits<double>::lowest()};
+    for (auto const &bx : boxes)
+      for (int d = 0; d < 3; ++d)
+      {
+        ulo[d] = std::min(ulo[d], bx[d]);
+        uhi[d] = std::max(uhi[d], bx[3 + d]);
+      }
+    int64_t lo_i[3], hi_i[3];
+    for (int d = 0; d < 3; ++d)
+    {
+      // cells i with origin + i h <= uhi and origin + (i + 1) h >= ulo, one
+      // cell of margin against rounding (the exact test follows)
+      double const a = std::floor((ulo[d] - cfg.origin[d]) / h[d]) - 2.0;
+      double const b = std::floor((uhi[d] - cfg.origin[d]) / h[d]) + 2.0;
+      lo_i[d] = boxes.empty() ? 1 : (int64_t)std::max(0.0, std::min(a, (double)forest.n(l, d)));
+      hi_i[d] = boxes.empty() ? 0 : (int64_t)std::max(-1.0, std::min(b, (double)forest.n(l, d) - 1.0));
+    }
+    for (int64_t k = lo_i[2]; k <= hi_i[2]; ++k)
+      for (int64_t j = lo_i[1]; j <= hi_i[1]; ++j)
+        for (int64_t i = lo_i[0]; i <= hi_i[0]; ++i)
         {
           int64_t const c = forest.index(l, i, j, k);
           if (!forest.leaf[l][c])
@@ -453,26 +476,37 @@ struct AmrMesh
   void build()
   {
     int const L = forest.max_level;
-    std::unordered_map<int64_t, uint8_t> nodes; // key -> 1
-    {
-      int64_t n_leaf = 0;
-      for (int l = 0; l <= L; ++l)
-        n_leaf += n_active_leaves(l);
-      nodes.reserve((size_t)(n_leaf * (p + 1) * (p + 1) * 2));
-    }
+    // node positions of the active leaves on a dense byte map of the
+    // lattice (1: node, 2: hanging node); its scan in key order gives the
+    // sorted DoF keys
+    size_t const n_lat = (size_t)(NX[0] + 1) * (NX[1] + 1) * (NX[2] + 1);
+    node_map.assign(n_lat, 0);
+    int64_t n_all = 0;
+    int64_t const sx = 1, sy = NX[0] + 1, sz = (NX[0] + 1) * (NX[1] + 1); // key strides
     for (int l = 0; l <= L; ++l)
+    {
+      int64_t const fac = cell_size(l) / p; // lattice spacing of the level's nodes
       for (int64_t k = 0; k < forest.n(l, 2); ++k)
         for (int64_t j = 0; j < forest.n(l, 1); ++j)
+        {
+          uint8_t const *lf = &forest.leaf[l][forest.index(l, 0, j, k)];
           for (int64_t i = 0; i < forest.n(l, 0); ++i)
           {
-            if (!active_leaf(l, i, j, k))
+            if (!lf[i] || !in_domain(l, i, j, k))
               continue;
+            int64_t const k0 = key(lat(l, i, 0), lat(l, j, 0), lat(l, k, 0));
             for (int c = 0; c <= p; ++c)
               for (int b = 0; b <= p; ++b)
                 for (int a = 0; a <= p; ++a)
-                  nodes[key(lat(l, i, a), lat(l, j, b), lat(l, k, c))] = 1;
+                {
+                  uint8_t &v = node_map[k0 + fac * (a * sx + b * sy + c * sz)];
+                  n_all += v == 0;
+                  v = 1;
+                }
           }
-    n_nodes_all = (int64_t)nodes.size();
+        }
+    }
+    n_nodes_all = n_all;
     // hanging nodes: fine nodes on a face / edge of an active leaf whose
     // neighbour region across it is refined material, off the leaf's nodes
     std::unordered_map<int64_t, std::vector<std::pair<int64_t, double>>> hk;
@@ -535,16 +569,29 @@ struct AmrMesh
                   }
             }
           }
-    // masters: sorted keys of the non-hanging nodes
+    // masters: the keys of the non-hanging nodes, in key order (the map is
+    // scanned eight entries at a time, skipping empty words)
+    for (auto const &kv : hk)
+      node_map[kv.first] = 2;
     dof_key.clear();
-    for (auto const &kv : nodes)
-      if (!hk.count(kv.first))
-        dof_key.push_back(kv.first);
-    std::sort(dof_key.begin(), dof_key.end());
-    dof_of.clear();
-    dof_of.reserve(dof_key.size() * 2);
-    for (size_t d = 0; d < dof_key.size(); ++d)
-      dof_of[dof_key[d]] = (int32_t)d;
+    dof_key.reserve(n_all);
+    {
+      size_t const nw = n_lat / 8;
+      uint64_t const *w = reinterpret_cast<uint64_t const *>(node_map.data());
+      for (size_t q = 0; q < nw; ++q)
+      {
+        uint64_t x = 0;
+        std::memcpy(&x, w + q, 8);
+        if (!x)
+          continue;
+        for (int b = 0; b < 8; ++b)
+          if (node_map[8 * q + b] == 1)
+            dof_key.push_back((int64_t)(8 * q + b));
+      }
+      for (size_t q = 8 * nw; q < n_lat; ++q)
+        if (node_map[q] == 1)
+          dof_key.push_back((int64_t)q);
+    }
     // resolve chains (a master that is itself hanging)
     hanging.clear();
     for (auto const &kv : hk)
@@ -575,32 +622,39 @@ struct AmrMesh
       std::vector<std::pair<int32_t, double>> res;
       for (auto const &e : cur)
       {
-        auto it = dof_of.find(e.first);
-        if (it == dof_of.end())
+        int32_t const dof = find_dof(e.first);
+        if (dof < 0)
           throw Error(ADM_ERR_INVALID, "internal: constraint master is not a node of the mesh");
         bool merged = false;
         for (auto &r : res)
-          if (r.first == it->second)
+          if (r.first == dof)
           {
             r.second += e.second;
             merged = true;
           }
         if (!merged)
-          res.push_back({it->second, e.second});
+          res.push_back({dof, e.second});
       }
       std::sort(res.begin(), res.end());
       hanging[kv.first] = std::move(res);
     }
   }
 
+  // the DoF of a node key, or -1 (binary search of the sorted keys)
+  int32_t find_dof(int64_t k) const
+  {
+    auto const it = std::lower_bound(dof_key.begin(), dof_key.end(), k);
+    return (it != dof_key.end() && *it == k) ? (int32_t)(it - dof_key.begin()) : -1;
+  }
+
   // entries (dof, weight) of the value at a node key
   void entries(int64_t k, std::vector<std::pair<int32_t, double>> &out) const
   {
     out.clear();
-    auto it = dof_of.find(k);
-    if (it != dof_of.end())
+    int32_t const dof = find_dof(k);
+    if (dof >= 0)
     {
-      out.push_back({it->second, 1.0});
+      out.push_back({dof, 1.0});
       return;
     }
     auto h = hanging.find(k);
@@ -806,11 +860,21 @@ public:
       throw Error(ADM_ERR_INVALID, "setup() has not been called");
   }
 
+  // phase time since the last lap
+  void remesh_lap(int phase)
+  {
+    auto const now = std::chrono::steady_clock::now();
+    remesh_ms_[phase] = std::chrono::duration<double, std::milli>(now - remesh_clock_).count();
+    remesh_clock_ = now;
+  }
+
   // refine_and_transfer around an AmrMesh change (done by `change`)
   template <class F> void remesh(F &&change)
   {
     require_ready();
     Ordered ord(*this);
+    remesh_clock_ = std::chrono::steady_clock::now();
+    auto lap = [&](int phase) { remesh_lap(phase); };
     // the old field at the level nodes of the old leaves (constraints
     // resolved; only those nodes come back to the host) and the old cell
     // states (ThermalPhysics::set_state_to_material_properties)
@@ -841,32 +905,57 @@ public:
     old.melted.resize(levels_.size());
     old.pitch.assign(levels_.size(), 0);
     old.nn1.assign(levels_.size(), 0);
+    old.state_cells.resize(levels_.size());
     for (size_t l = 0; l < levels_.size(); ++l)
     {
       if (!alive(l))
         continue;
       levels_[l]->set_state_to_material_properties();
-      old.states[l].resize(levels_[l]->n_cells() * ns);
-      levels_[l]->get_cell_state(old.states[l].data());
+      // the states of the level's active leaves (ascending cell index)
+      std::vector<int32_t> &cells = old.state_cells[l];
+      for (int64_t k = 0; k < mesh_.forest.n((int)l, 2); ++k)
+        for (int64_t j = 0; j < mesh_.forest.n((int)l, 1); ++j)
+          for (int64_t i = 0; i < mesh_.forest.n((int)l, 0); ++i)
+            if (mesh_.active_leaf((int)l, i, j, k))
+              cells.push_back((int32_t)mesh_.forest.index((int)l, i, j, k));
+      old.states[l].resize(cells.size() * ns);
+      levels_[l]->get_cell_state_sparse(cells.data(), cells.size(), old.states[l].data());
       old.melted[l] = levels_[l]->has_melted_cells();
       old.pitch[l] = levels_[l]->mesh().pitch;
       old.nn1[l] = levels_[l]->mesh().nn[1];
     }
+    lap(0);
     change();
+    lap(1);
     mesh_.build();
-    build_levels(&old);
+    lap(2);
+    build_levels(&old); // phases 3-5
     // SolutionTransfer: the old field at the new nodes
+    // both key lists ascend: one walk through the old keys
     std::vector<double> y(n_dofs());
+    size_t at = 0;
     for (int64_t d = 0; d < n_dofs(); ++d)
     {
-      double v;
-      y[d] = old.dof_lookup(mesh_.dof_key[d], v) ? v : old.evaluate(mesh_, mesh_.dof_key[d]);
+      int64_t const key = mesh_.dof_key[d];
+      while (at < old.dof_key.size() && old.dof_key[at] < key)
+        ++at;
+      y[d] = (at < old.dof_key.size() && old.dof_key[at] == key) ? old.dof_val[at] : old.evaluate(mesh_, key);
     }
     y_.alloc(n_dofs());
     ADM_CK(cudaMemcpyAsync(y_.p, y.data(), y.size() * sizeof(double), cudaMemcpyHostToDevice, stream_));
     ADM_CK(cudaStreamSynchronize(stream_));
+    lap(6);
     compute_inverse_mass();
+    ADM_CK(cudaStreamSynchronize(stream_));
+    lap(7);
   }
+
+  // host wall time of the last remesh's phases: snapshot of the old field
+  // and states, flagging and execution, nodes and constraints, level-grid
+  // set-up, cell-state transfer, prolongation tables, solution transfer,
+  // inverse mass
+  double remesh_ms_[kRemeshPhases] = {0, 0, 0, 0, 0, 0, 0, 0};
+  std::chrono::steady_clock::time_point remesh_clock_;
 
   // Level-grid schedule (coloured: 8 launches per level and application,
   // deterministic; atomic: 1 launch, additions in any order; two-pass: a
@@ -1136,15 +1225,8 @@ private:
     std::vector<int64_t> row_pos, dof_key;
     std::vector<double> row_val, dof_val;
 
-    bool dof_lookup(int64_t key, double &v) const
-    {
-      auto it = std::lower_bound(dof_key.begin(), dof_key.end(), key);
-      if (it == dof_key.end() || *it != key)
-        return false;
-      v = dof_val[it - dof_key.begin()];
-      return true;
-    }
-    std::vector<std::vector<double>> states;
+    std::vector<std::vector<int32_t>> state_cells; // per level: the active leaves, ascending
+    std::vector<std::vector<double>> states;       // per level: their states [leaf][n_states]
     std::vector<std::vector<uint8_t>> melted;
     std::vector<int> pitch, nn1;
 
@@ -1219,10 +1301,12 @@ private:
           ++m;
         }
       }
-      int64_t const C = forest.cells(m);
       int64_t const cell = forest.index(m, a, b, c);
+      std::vector<int32_t> const &lc = state_cells[m];
+      auto const it = std::lower_bound(lc.begin(), lc.end(), (int32_t)cell);
+      bool const found = it != lc.end() && *it == (int32_t)cell;
       for (int q = 0; q < ns; ++q)
-        out[q] = states[m][q * C + cell];
+        out[q] = found ? states[m][(size_t)(it - lc.begin()) * ns + q] : 0.0;
       if (melt)
         *melt = melted[m].empty() ? 0 : melted[m][cell];
     }
@@ -1230,6 +1314,14 @@ private:
 
   void build_levels(Snapshot const *old)
   {
+    auto lap_ms = [&] {
+      auto const now = std::chrono::steady_clock::now();
+      double const ms = std::chrono::duration<double, std::milli>(now - remesh_clock_).count();
+      remesh_clock_ = now;
+      return ms;
+    };
+    double t_setup = 0.0, t_states = 0.0;
+    lap_ms();
     drop_graph();
     fork();
     int const L = mesh_.forest.max_level;
@@ -1270,9 +1362,12 @@ private:
       th->set_cells(act.data(), mat.data(), init.data(), nullptr, nullptr);
       th->set_domain(dom.data());
       th->setup();
+      t_setup += lap_ms();
       if (old)
       {
-        std::vector<double> st((size_t)C * ns, 0.0);
+        // the states of the active leaves only (CellDataTransfer)
+        std::vector<int32_t> cells;
+        std::vector<double> st;
         std::vector<uint8_t> melt(C, 0);
         for (int64_t k = 0; k < mesh_.forest.n(l, 2); ++k)
           for (int64_t j = 0; j < mesh_.forest.n(l, 1); ++j)
@@ -1283,14 +1378,17 @@ private:
                 continue;
               double v[3] = {0, 0, 0};
               old->state_of(l, i, j, k, ns, v, &melt[cell]);
-              for (int q = 0; q < ns; ++q)
-                st[(size_t)q * C + cell] = v[q];
+              cells.push_back((int32_t)cell);
+              st.insert(st.end(), v, v + ns);
             }
-        th->set_cell_state(st.data());
+        th->set_cell_state_sparse(cells.data(), st.data(), cells.size());
         th->get_state_from_material_properties();
         th->set_has_melted(melt.data());
+        t_states += lap_ms();
       }
     }
+    remesh_ms_[3] = t_setup;
+    remesh_ms_[4] = t_states;
     lev_off_.assign(L + 1, 0);
     int64_t off = 0;
     for (int l = 0; l <= L; ++l)
@@ -1315,27 +1413,58 @@ private:
       if (!alive(l))
         continue;
       Mesh const &lm = levels_[l]->mesh();
-      std::vector<int64_t> nodes;
+      // the level nodes of the active leaves, in ascending order: marked on
+      // a byte map of the level grid, then collected by a scan that skips
+      // empty 8-byte words
+      size_t const n_lev = lm.n_nodes;
+      node_mark_.assign(n_lev, 0);
+      int const p = mesh_.p;
       for (int64_t k = 0; k < mesh_.forest.n(l, 2); ++k)
         for (int64_t j = 0; j < mesh_.forest.n(l, 1); ++j)
+        {
+          uint8_t const *lf = &mesh_.forest.leaf[l][mesh_.forest.index(l, 0, j, k)];
           for (int64_t i = 0; i < mesh_.forest.n(l, 0); ++i)
           {
-            if (!mesh_.active_leaf(l, i, j, k))
+            if (!lf[i] || !mesh_.in_domain(l, i, j, k))
               continue;
-            int const p = mesh_.p;
             for (int c = 0; c <= p; ++c)
               for (int b = 0; b <= p; ++b)
                 for (int a = 0; a <= p; ++a)
-                  nodes.push_back((p * i + a) + (int64_t)lm.pitch * ((p * j + b) + (int64_t)lm.nn[1] * (p * k + c)));
+                  node_mark_[(p * i + a) + (int64_t)lm.pitch * ((p * j + b) + (int64_t)lm.nn[1] * (p * k + c))] = 1;
           }
-      std::sort(nodes.begin(), nodes.end());
-      nodes.erase(std::unique(nodes.begin(), nodes.end()), nodes.end());
+        }
+      std::vector<int64_t> nodes;
+      for (size_t q = 0; q < n_lev / 8; ++q)
+      {
+        uint64_t x = 0;
+        std::memcpy(&x, node_mark_.data() + 8 * q, 8);
+        if (!x)
+          continue;
+        for (int b = 0; b < 8; ++b)
+          if (node_mark_[8 * q + b])
+            nodes.push_back((int64_t)(8 * q + b));
+      }
+      for (size_t q = n_lev / 8 * 8; q < n_lev; ++q)
+        if (node_mark_[q])
+          nodes.push_back((int64_t)q);
+      // the nodes' lattice keys ascend with their level positions (both
+      // order by z, y, x), so the DoF keys are walked once alongside
+      size_t at = 0;
       for (int64_t nidx : nodes)
       {
         int64_t const x = nidx % lm.pitch, y = (nidx / lm.pitch) % lm.nn[1], z = nidx / ((int64_t)lm.pitch * lm.nn[1]);
         int const s = mesh_.forest.max_level - l;
         int64_t const f = ((int64_t)2 << s) / mesh_.p;
-        mesh_.entries(mesh_.key(x * f, y * f, z * f), ent);
+        int64_t const key = mesh_.key(x * f, y * f, z * f);
+        while (at < mesh_.dof_key.size() && mesh_.dof_key[at] < key)
+          ++at;
+        if (at < mesh_.dof_key.size() && mesh_.dof_key[at] == key)
+        {
+          ent.clear();
+          ent.push_back({(int32_t)at, 1.0});
+        }
+        else
+          mesh_.entries(key, ent);
         row_pos.push_back(lev_off_[l] + nidx);
         for (auto const &e : ent)
         {
@@ -1372,6 +1501,7 @@ private:
     upload(tpos_, tpos);
     upload(tw_, tw);
     ADM_CK(cudaStreamSynchronize(stream_));
+    remesh_lap(5);
   }
 
   template <class T> void upload(DevBuf<T> &buf, std::vector<T> const &v)
@@ -1438,6 +1568,7 @@ private:
   std::vector<std::unique_ptr<Thermal>> levels_;
   std::vector<uint8_t> alive_;
   std::vector<int64_t> row_pos_h_;
+  std::vector<uint8_t> node_mark_; // level-grid byte map (prolongation rows)
   int schedule_ = Thermal::kScheduleAtomic;
   std::vector<int64_t> lev_off_, row_lev_;
   int64_t lev_n_ = 0, n_rows_ = 0;
@@ -1690,6 +1821,15 @@ int adm_amr_execute(adm_amr *h, uint8_t const *refine, uint8_t const *coarsen)
     auto r = level_flags(h->a->mesh(), refine);
     auto c = level_flags(h->a->mesh(), coarsen);
     h->a->remesh([&] { h->a->mesh().execute(r, c); });
+  });
+}
+
+int adm_amr_remesh_profile(adm_amr const *h, double *ms)
+{
+  return adm::guard([&] {
+    ADM_REQUIRE(h && ms, "null argument");
+    for (int i = 0; i < adm::kRemeshPhases; ++i)
+      ms[i] = h->a->remesh_ms_[i];
   });
 }
 

@@ -554,6 +554,38 @@ __global__ void set_state_kernel(uint32_t const *cell_info, int ns, int NN,
   state[c] = 1.0 - l - p;
 }
 
+// MaterialProperty::set_initial_state: state[s][c] = (s == init[c])
+__global__ void init_state_kernel(uint8_t const *init, int ns, size_t C, double *state)
+{
+  size_t const c = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (c >= C)
+    return;
+  for (int s = 0; s < ns; ++s)
+    state[(size_t)s * C + c] = init[c] == s ? 1.0 : 0.0;
+}
+
+// state[s][cells[k]] = values[k][s] (the other cells were cleared before)
+__global__ void scatter_state_kernel(int32_t const *cells, double const *values, size_t n, int ns, size_t C,
+                                     double *state)
+{
+  size_t const k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (k >= n)
+    return;
+  for (int s = 0; s < ns; ++s)
+    state[(size_t)s * C + cells[k]] = values[k * ns + s];
+}
+
+// out[k][s] = state[s][cells[k]]
+__global__ void gather_state_kernel(int32_t const *cells, size_t n, int ns, size_t C, double const *state,
+                                    double *out)
+{
+  size_t const k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (k >= n)
+    return;
+  for (int s = 0; s < ns; ++s)
+    out[k * ns + s] = state[(size_t)s * C + cells[k]];
+}
+
 // get_state_from_material_properties (source/ThermalOperator.templates.hh:753-884):
 // broadcast the cell state to the quadrature-point (and face) tables.
 __global__ void get_state_kernel(uint32_t const *cell_info, int ns, int NN, int NF,

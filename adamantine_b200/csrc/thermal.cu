@@ -689,11 +689,16 @@ void Thermal::setup()
   ADM_CK(cudaSetDevice(device_));
   size_t const C = mesh_.n_cells;
   rebuild();
-  // MaterialProperty::set_initial_state
-  std::vector<double> st((size_t)ns_ * C, 0.0);
-  for (size_t c = 0; c < C; ++c)
-    st[(size_t)init_state_[c] * C + c] = 1.0;
-  ADM_CK(cudaMemcpyAsync(state_d_.p, st.data(), st.size() * sizeof(double), cudaMemcpyHostToDevice, stream_));
+  // MaterialProperty::set_initial_state (on the device from the per-cell
+  // state index)
+  {
+    DevBuf<uint8_t> init;
+    init.alloc(std::max<size_t>(1, C));
+    ADM_CK(cudaMemcpyAsync(init.p, init_state_.data(), C, cudaMemcpyHostToDevice, stream_));
+    init_state_kernel<<<(unsigned)((C + 255) / 256), 256, 0, stream_>>>(init.p, ns_, C, state_d_.p);
+    ADM_CK(cudaGetLastError());
+    ADM_CK(cudaStreamSynchronize(stream_)); // init is released on return
+  }
   if (ns_ == 3)
   {
     ADM_CK(cudaMemsetAsync(powder_mode_.p, 0, C, stream_));
@@ -1243,6 +1248,46 @@ void Thermal::set_cell_state(double const *host)
 {
   ADM_CK(cudaMemcpyAsync(state_d_.p, host, state_d_.n * sizeof(double), cudaMemcpyHostToDevice, stream_));
   ADM_CK(cudaStreamSynchronize(stream_));
+}
+
+void Thermal::get_cell_state_sparse(int32_t const *cells, size_t n, double *out)
+{
+  size_t const C = mesh_.n_cells;
+  for (size_t k = 0; k < n; ++k)
+    if (cells[k] < 0 || (size_t)cells[k] >= C)
+      throw Error(ADM_ERR_INVALID, "cell index out of range");
+  if (n == 0)
+    return;
+  DevBuf<int32_t> cd;
+  DevBuf<double> vd;
+  cd.alloc(n);
+  vd.alloc(n * ns_);
+  ADM_CK(cudaMemcpyAsync(cd.p, cells, n * sizeof(int32_t), cudaMemcpyHostToDevice, stream_));
+  gather_state_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream_>>>(cd.p, n, ns_, C, state_d_.p, vd.p);
+  ADM_CK(cudaGetLastError());
+  ADM_CK(cudaMemcpyAsync(out, vd.p, n * ns_ * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+  ADM_CK(cudaStreamSynchronize(stream_));
+}
+
+void Thermal::set_cell_state_sparse(int32_t const *cells, double const *values, size_t n)
+{
+  size_t const C = mesh_.n_cells;
+  for (size_t k = 0; k < n; ++k)
+    if (cells[k] < 0 || (size_t)cells[k] >= C)
+      throw Error(ADM_ERR_INVALID, "cell index out of range");
+  ADM_CK(cudaMemsetAsync(state_d_.p, 0, state_d_.n * sizeof(double), stream_));
+  DevBuf<int32_t> cd;
+  DevBuf<double> vd;
+  if (n > 0)
+  {
+    cd.alloc(n);
+    vd.alloc(n * ns_);
+    ADM_CK(cudaMemcpyAsync(cd.p, cells, n * sizeof(int32_t), cudaMemcpyHostToDevice, stream_));
+    ADM_CK(cudaMemcpyAsync(vd.p, values, n * ns_ * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    scatter_state_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream_>>>(cd.p, vd.p, n, ns_, C, state_d_.p);
+    ADM_CK(cudaGetLastError());
+  }
+  ADM_CK(cudaStreamSynchronize(stream_)); // cd and vd are released on return
 }
 
 void Thermal::get_qp_powder(double *host)

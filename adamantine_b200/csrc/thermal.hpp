@@ -235,6 +235,11 @@ public:
   void evaluate_material_properties(double const *temperature, double *pv);
   void get_cell_state(double *host);
   void set_cell_state(double const *host);
+  // the per-cell state of the listed cells (values [n][n_states]), every
+  // other cell's state 0 (as set_cell_state with zeros there)
+  void set_cell_state_sparse(int32_t const *cells, double const *values, size_t n);
+  // the per-cell state of the listed cells into out [n][n_states] (host)
+  void get_cell_state_sparse(int32_t const *cells, size_t n, double *out);
   void get_qp_powder(double *host);
   void mark_has_melted(double threshold, double const *temperature, uint8_t *host);
   // the has_melted flags per cell (host copy) and their replacement (a

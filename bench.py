@@ -686,6 +686,7 @@ def run_amr(args, local_rank):
     g.refine_mesh(t, t + K * dt, K, L, True)
     torch.cuda.synchronize()
     remesh_ms = 1e3 * (time.perf_counter() - t0)
+    remesh_phases = g.remesh_profile()
     g.close()
     # the uniform grid of the finest cells
     fine_cfg = copy.deepcopy(cfg)
@@ -706,7 +707,7 @@ def run_amr(args, local_rank):
         "workload": AMR_WORKLOAD, "max_level": L, "leaves_per_level": per_level, "dofs": n_dofs,
         "hanging_nodes": n_nodes - n_dofs, "steps": steps, "dt": dt, "ms_per_step": ms / steps,
         "mdofs_per_s": 4 * n_dofs * steps / (ms * 1e-3) / 1e6, "peak_temperature": float(y.max()),
-        "first_refine_mesh_ms": first_remesh_ms, "refine_mesh_ms": remesh_ms,
+        "first_refine_mesh_ms": first_remesh_ms, "refine_mesh_ms": remesh_ms, "refine_mesh_phases_ms": remesh_phases,
         "uniform_fine": {"nodes": fine_nodes, "ms_per_step": ms_fine / steps, "path": "evolve_n_steps (graphs)"},
         "speedup_vs_uniform_fine": ms_fine / ms,
     }

@@ -92,6 +92,13 @@ int adm_amr_refine_mesh(adm_amr *h, double time, double next_refinement_time, in
                         int coarsen_after_beam);
 int adm_amr_execute(adm_amr *h, uint8_t const *refine, uint8_t const *coarsen);
 int adm_amr_n_dofs(adm_amr const *h, int64_t *n_dofs, int64_t *n_nodes);
+/* Host wall time (ms) of the last refine_mesh / execute, per phase: the
+ * snapshot of the old field and cell states, flagging and executing the
+ * refinement, nodes and hanging-node constraints, the level grids' set-up,
+ * the cell-state transfer, the prolongation tables, the solution transfer,
+ * the inverse mass. */
+#define ADM_AMR_REMESH_PHASES 8
+int adm_amr_remesh_profile(adm_amr const *h, double *ms);
 int adm_amr_n_leaves(adm_amr const *h, int64_t *n);
 int adm_amr_leaves(adm_amr const *h, int32_t *lijk);
 int adm_amr_dof_lattice(adm_amr const *h, int64_t *xyz);
