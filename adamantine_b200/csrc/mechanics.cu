@@ -9,14 +9,16 @@
  * point, one thread per point.
  *
  * Layout: the thermal handle's node layout (pitch, z-slabs); a displacement
- * vector is three node vectors (x, y, z components). Work: one warp per
- * cell that carries displacement; the reference-element tables (values and
- * gradients of the (p+1)^3 nodal functions at the (p+1)^3 Gauss points)
- * sit in constant memory; each lane gathers one node's three components,
- * then evaluates one quadrature point's stress, then integrates one node's
- * three test functions and adds them into the result (FP64 atomics: a node
- * is shared by up to 8 cells). Clamped displacements are eliminated: their
- * columns are dropped and their rows are the identity.
+ * vector is three node vectors (x, y, z components). Work, FE_Q(2): one
+ * warp per cell that carries displacement; the reference-element tables
+ * (values and gradients of the (p+1)^3 nodal functions at the (p+1)^3
+ * Gauss points) sit in a per-handle device buffer; each lane gathers one
+ * node's three components, then evaluates one quadrature point's stress,
+ * then integrates one node's three test functions and adds them into the
+ * result (FP64 atomics: a node is shared by up to 8 cells). FE_Q(1): one
+ * thread per node gathers its row from the element matrices of its cells
+ * (elastic_gather_q1_kernel, no atomics). Clamped displacements are
+ * eliminated: their columns are dropped and their rows are the identity.
  */
 #include "capi_common.hpp"
 #include "thermal.hpp"
@@ -306,6 +308,99 @@ __global__ void __launch_bounds__(128) elastic_apply_kernel(MechArgs a, double c
     }
     __syncwarp();
   }
+}
+
+// FE_Q(1) element matrices of one level's cell size, passed by value (the
+// kernel-parameter bank): [2][8][8][3][3], K_lambda[a][b][ca][cb] =
+// int d_ca phi_a d_cb phi_b, then K_mu[a][b][ca][cb] = int (delta_ca,cb
+// grad phi_a . grad phi_b + d_cb phi_a d_ca phi_b).
+struct Q1Matrices
+{
+  double k[2 * 576];
+};
+
+// dst += A src on the free rows of an FE_Q(1) operator, one thread per
+// node and no atomics: the node's row gathers lambda K_lambda + mu K_mu of
+// its (up to eight) cells, (lambda, mu) per cell from a.cell_coef (0 for
+// the cells that carry no displacement); clamped and absent columns read
+// as 0. The loops are unrolled so that every matrix entry is a constant
+// operand of its FMA (no load), and the 27 neighbour values are read once:
+// the lower node layer and the middle one serve the four lower cells, then
+// the upper layer replaces the lower one for the four upper cells.
+__global__ void __launch_bounds__(128) elastic_gather_q1_kernel(MechArgs a, const __grid_constant__ Q1Matrices kq,
+                                                                double const *src, double *dst)
+{
+  int64_t const g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (g >= a.m || a.node_mask[g] != 1)
+    return;
+  int const i = (int)(g % a.pitch);
+  int64_t const rest = g / a.pitch;
+  int const j = (int)(rest % a.nn[1]), k = (int)(rest / a.nn[1]);
+  int64_t const sy = a.pitch, sz = (int64_t)a.pitch * a.nn[1];
+  // u[layer][dy + 1][dx + 1][component] of the two node layers in use
+  double u[2][3][3][3];
+  auto load_layer = [&](int slot, int dz) {
+#pragma unroll
+    for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+      for (int dx = -1; dx <= 1; ++dx)
+      {
+        bool const ok = i + dx >= 0 && i + dx < a.nn[0] && j + dy >= 0 && j + dy < a.nn[1] && k + dz >= 0 &&
+                        k + dz < a.nn[2];
+        int64_t const gn = g + dx + sy * dy + sz * dz;
+        bool const fr = ok && a.node_mask[gn] == 1;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          u[slot][dy + 1][dx + 1][c] = fr ? src[c * a.m + gn] : 0.0;
+      }
+  };
+  double acc[3] = {0.0, 0.0, 0.0};
+  load_layer(0, -1);
+  load_layer(1, 0);
+#pragma unroll
+  for (int oz = 0; oz < 2; ++oz)
+  {
+    if (oz == 1)
+      load_layer(0, 1); // slot 0 now holds the upper layer
+#pragma unroll
+    for (int oy = 0; oy < 2; ++oy)
+#pragma unroll
+      for (int ox = 0; ox < 2; ++ox)
+      {
+        int const cx = i - 1 + ox, cy = j - 1 + oy, cz = k - 1 + oz;
+        if (cx < 0 || cy < 0 || cz < 0 || cx >= a.nc[0] || cy >= a.nc[1] || cz >= a.nc[2])
+          continue;
+        int64_t const c = cx + (int64_t)a.nc[0] * (cy + (int64_t)a.nc[1] * cz);
+        double const lam = a.cell_coef[2 * c], mu = a.cell_coef[2 * c + 1];
+        if (lam == 0.0 && mu == 0.0)
+          continue;
+        int const la = (1 - ox) + 2 * (1 - oy) + 4 * (1 - oz); // the node's corner in the cell
+        double al[3] = {0.0, 0.0, 0.0}, am[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int b = 0; b < 8; ++b)
+        {
+          int const bx = b & 1, by = (b >> 1) & 1, bz = b >> 2;
+          // the cell node's layer: lower cells use slots 0 (dz -1) and 1
+          // (dz 0); upper cells slots 1 (dz 0) and 0 (dz +1)
+          int const slot = oz == 0 ? bz : 1 - bz;
+          double const *uv = u[slot][oy + by][ox + bx];
+          double const *Kl = &kq.k[(la * 8 + b) * 9];
+          double const *Km = Kl + 576;
+#pragma unroll
+          for (int ca = 0; ca < 3; ++ca)
+          {
+            al[ca] = fma(Kl[3 * ca], uv[0], fma(Kl[3 * ca + 1], uv[1], fma(Kl[3 * ca + 2], uv[2], al[ca])));
+            am[ca] = fma(Km[3 * ca], uv[0], fma(Km[3 * ca + 1], uv[1], fma(Km[3 * ca + 2], uv[2], am[ca])));
+          }
+        }
+#pragma unroll
+        for (int ca = 0; ca < 3; ++ca)
+          acc[ca] = fma(lam, al[ca], fma(mu, am[ca], acc[ca]));
+      }
+  }
+#pragma unroll
+  for (int ca = 0; ca < 3; ++ca)
+    dst[ca * a.m + g] += acc[ca];
 }
 
 // rhs += sum_q JxW ((3 lambda + 2 mu) alpha (T - T_ref) div v + f . v)
@@ -753,6 +848,37 @@ public:
   Mechanics(Mechanics const &) = delete;
   Mechanics &operator=(Mechanics const &) = delete;
 
+  // FE_Q(1) element matrices of a cell of size h: [2][8][8][3][3], the
+  // lambda part then the mu part (elastic_gather_q1_kernel)
+  Q1Matrices q1_element_matrices(double const h[3]) const
+  {
+    Q1Matrices M{};
+    double *K = M.k;
+    double const inv_h[3] = {1.0 / h[0], 1.0 / h[1], 1.0 / h[2]};
+    double const jxw = h[0] * h[1] * h[2];
+    for (int q = 0; q < 8; ++q)
+    {
+      double const jw = jxw * tab1_h_[kTabWq + q];
+      double gr[8][3];
+      for (int a = 0; a < 8; ++a)
+        for (int d = 0; d < 3; ++d)
+          gr[a][d] = tab1_h_[kTabGrad + (q * kMaxN + a) * 3 + d] * inv_h[d];
+      for (int a = 0; a < 8; ++a)
+        for (int b = 0; b < 8; ++b)
+        {
+          double const dot = gr[a][0] * gr[b][0] + gr[a][1] * gr[b][1] + gr[a][2] * gr[b][2];
+          for (int ca = 0; ca < 3; ++ca)
+            for (int cb = 0; cb < 3; ++cb)
+            {
+              size_t const e = (size_t)(a * 8 + b) * 9 + ca * 3 + cb;
+              K[e] += jw * gr[a][ca] * gr[b][cb];
+              K[576 + e] += jw * (gr[a][cb] * gr[b][ca] + (ca == cb ? dot : 0.0));
+            }
+        }
+    }
+    return M;
+  }
+
   // values [q][n], reference gradients [q][n][d] and weights of the
   // (p+1)^3 Gauss points of FE_Q(p) on [0, 1]^3, at the kTab* offsets
   static std::vector<double> element_tables(int p)
@@ -837,6 +963,22 @@ public:
     ADM_CK(cudaMemcpyAsync(matid_.p, t.matid_.data(), C, cudaMemcpyHostToDevice, s));
     ADM_CK(cudaMemcpyAsync(melted_.p, t.has_melted_.data(), C, cudaMemcpyHostToDevice, s));
     setup_stress_state(carry, cells);
+    // FE_Q(1): (lambda, mu) per cell (0 where no displacement) and the
+    // element matrices of the gather operator
+    if (p_ == 1)
+    {
+      std::vector<double> coef(2 * C, 0.0);
+      for (int32_t c : cells)
+      {
+        coef[2 * c] = cfg_.lame_first[t.matid_[c]];
+        coef[2 * c + 1] = cfg_.lame_second[t.matid_[c]];
+      }
+      coef0_d_.alloc(2 * C);
+      ADM_CK(cudaMemcpyAsync(coef0_d_.p, coef.data(), 2 * C * sizeof(double), cudaMemcpyHostToDevice, s));
+      double const h[3] = {M.h[0], M.h[1], M.h[2]};
+      kq0_ = q1_element_matrices(h);
+      ADM_CK(cudaStreamSynchronize(s));
+    }
     // right-hand side and Jacobi diagonal
     rhs_.alloc(3 * m_);
     diag_.alloc(3 * m_);
@@ -1089,6 +1231,7 @@ private:
     a.gravity = cfg_.gravity;
     a.melted = melted_.p;
     a.tab = tab_.p;
+    a.cell_coef = p_ == 1 ? coef0_d_.p : nullptr;
     return a;
   }
 
@@ -1096,6 +1239,12 @@ private:
   {
     if (n_cells_ == 0)
       return;
+    if (p_ == 1)
+    {
+      elastic_gather_q1_kernel<<<(unsigned)((m_ + 127) / 128), 128, 0, th_.stream_>>>(args(), kq0_, src, dst);
+      ADM_CK(cudaGetLastError());
+      return;
+    }
     int64_t const per_warp = 32 / N_;
     unsigned const nb =
         (unsigned)std::max<int64_t>(1, std::min<int64_t>((n_cells_ + 4 * per_warp - 1) / (4 * per_warp), 148 * 16));
@@ -1171,6 +1320,8 @@ private:
     double *bp = nullptr, *xp = nullptr; // right-hand side and solution (level 0: the CG's)
     std::vector<double> cd, cr;          // Chebyshev step coefficients
     double lmax = 0.0;
+    Q1Matrices kq{};                 // FE_Q(1) element matrices of the level's cells (gather apply)
+    Q1Matrices const *kqp = nullptr; // kq, or the finest level's
     int n_direct = 0; // > 0: coarsest level solved by the dense inverse
     DevBuf<int64_t> didx;
     DevBuf<double> dinvm;
@@ -1226,6 +1377,12 @@ private:
   {
     if (L.n_cells == 0)
       return;
+    if (L.p == 1)
+    {
+      elastic_gather_q1_kernel<<<(unsigned)((L.lat.m + 127) / 128), 128, 0, ls()>>>(L.a, *L.kqp, src, L.q.p);
+      ADM_CK(cudaGetLastError());
+      return;
+    }
     int64_t const per_warp = 32 / L.N;
     unsigned const nb =
         (unsigned)std::max<int64_t>(1, std::min<int64_t>((L.n_cells + 4 * per_warp - 1) / (4 * per_warp), 148 * 16));
@@ -1292,10 +1449,13 @@ private:
     if (finest)
     {
       L.a = args();
+      L.kqp = &kq0_;
       mg_invert_diag_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, diag_.p, L.dinv.p);
       ADM_CK(cudaGetLastError());
       return;
     }
+    L.kq = q1_element_matrices(L.h);
+    L.kqp = &L.kq;
     std::vector<int32_t> cells;
     for (int64_t c = 0; c < (int64_t)L.carry.size(); ++c)
       if (L.carry[c])
@@ -1610,6 +1770,8 @@ private:
   DevBuf<uint8_t> mask_, matid_, melted_;
   DevBuf<double> tab_;  // reference-element tables of this handle's degree
   DevBuf<double> tab1_; // and of FE_Q(1) (multigrid levels)
+  DevBuf<double> coef0_d_; // FE_Q(1): (lambda, mu) per cell
+  Q1Matrices kq0_{};       // and the element matrices
   std::vector<double> tab1_h_;
   std::vector<uint8_t> carry_now_; // cells that carry displacement (last setup)
   std::vector<std::unique_ptr<MgLevel>> mg_;
