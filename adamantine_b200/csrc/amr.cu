@@ -678,21 +678,43 @@ struct AmrMesh
 namespace
 {
 // y_lev[row_pos[r]] = sum_e w[e] y[dof[e]] over the row's entries
+// A composite vector given as y + dt sum_j a_j k_j (nk <= 3 terms; nk 0:
+// y itself): an RK stage input formed where it is read.
+struct StageSum
+{
+  double const *y;
+  double dt;
+  int nk;
+  double a[3];
+  double const *k[3];
+};
+
+__device__ __forceinline__ double stage_value(StageSum const &v, int64_t d)
+{
+  double x = v.y[d];
+  double s = 0.0;
+  for (int j = 0; j < v.nk; ++j)
+    s = fma(v.a[j], v.k[j][d], s);
+  return v.nk ? fma(v.dt, s, x) : x;
+}
+
+// lev[row_pos[r]] = sum_e w[e] v[dof[e]], v the composite vector
 __global__ void prolong_kernel(int64_t n_rows, int64_t const *row_pos, int64_t const *row_ptr, int32_t const *dof,
-                               double const *w, double const *y, double *lev)
+                               double const *w, StageSum v, double *lev)
 {
   int64_t const r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (r >= n_rows)
     return;
   double s = 0.0;
   for (int64_t e = row_ptr[r]; e < row_ptr[r + 1]; ++e)
-    s += w[e] * y[dof[e]];
+    s += w[e] * stage_value(v, dof[e]);
   lev[row_pos[r]] = s;
 }
 
-// out[d] = sum_e w[e] lev[pos[e]] (add: out[d] += ...)
+// out[d] = sum_e w[e] lev[pos[e]] (add: out[d] += ...; scale: times
+// scale[d], the inverse mass of an RK stage derivative)
 __global__ void restrict_kernel(int64_t n_dofs, int64_t const *ptr, int64_t const *pos, double const *w,
-                                double const *lev, double *out, int add)
+                                double const *lev, double *out, int add, double const *scale)
 {
   int64_t const d = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (d >= n_dofs)
@@ -700,6 +722,8 @@ __global__ void restrict_kernel(int64_t n_dofs, int64_t const *ptr, int64_t cons
   double s = 0.0;
   for (int64_t e = ptr[d]; e < ptr[d + 1]; ++e)
     s += w[e] * lev[pos[e]];
+  if (scale)
+    s *= scale[d];
   out[d] = add ? out[d] + s : s;
 }
 
@@ -745,13 +769,6 @@ __global__ void stage_input_kernel(int64_t n, double const *y, double dt, int nk
   if (nk > 2)
     s += a2 * k2[i];
   z[i] = y[i] + dt * s;
-}
-
-__global__ void scale_kernel(int64_t n, double const *inv_m, double *k)
-{
-  int64_t const i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i < n)
-    k[i] *= inv_m[i];
 }
 
 __global__ void fill_kernel(int64_t n, double v, double *y)
@@ -890,12 +907,12 @@ public:
     ADM_CK(cudaStreamSynchronize(stream_));
     if (n_rows_ > 0)
     {
-      DevBuf<double> rv;
-      rv.alloc(n_rows_);
-      gather_kernel<<<blocks(n_rows_), 256, 0, stream_>>>(n_rows_, row_pos_.p, src_lev_.p, rv.p);
+      snap_rows_.ensure(n_rows_);
+      gather_kernel<<<blocks(n_rows_), 256, 0, stream_>>>(n_rows_, row_pos_.p, src_lev_.p, snap_rows_.p);
       ADM_CK(cudaGetLastError());
       old.row_val.resize(n_rows_);
-      ADM_CK(cudaMemcpyAsync(old.row_val.data(), rv.p, n_rows_ * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+      ADM_CK(cudaMemcpyAsync(old.row_val.data(), snap_rows_.p, n_rows_ * sizeof(double), cudaMemcpyDeviceToHost,
+                             stream_));
       ADM_CK(cudaStreamSynchronize(stream_));
       old.row_pos = row_pos_h_; // ascending: levels in order, nodes sorted
     }
@@ -941,7 +958,7 @@ public:
         ++at;
       y[d] = (at < old.dof_key.size() && old.dof_key[at] == key) ? old.dof_val[at] : old.evaluate(mesh_, key);
     }
-    y_.alloc(n_dofs());
+    y_.ensure(n_dofs());
     ADM_CK(cudaMemcpyAsync(y_.p, y.data(), y.size() * sizeof(double), cudaMemcpyHostToDevice, stream_));
     ADM_CK(cudaStreamSynchronize(stream_));
     lap(6);
@@ -1031,12 +1048,14 @@ public:
     Ordered ord(*this);
     Thermal::Tableau const tab = Thermal::tableau(mesh_.cfg.time_method);
     int64_t const n = n_dofs();
-    double *const before = z_.p;
+    double *before[4];
+    for (int i = 0; i < 4; ++i)
+      before[i] = k_[i].p;
     for (int i = 0; i < tab.s; ++i)
-      k_[i].alloc(n);
-    z_.alloc(n);
-    if (z_.p != before)
-      drop_graph();
+      k_[i].ensure(n);
+    for (int i = 0; i < 4; ++i)
+      if (k_[i].p != before[i])
+        drop_graph(); // the graph holds the stage vectors' addresses
     // the level clocks, after the last replay and before this one
     fork();
     for (size_t l = 0; l < levels_.size(); ++l)
@@ -1155,15 +1174,24 @@ private:
   }
 
   // k = C^T (sum_l A_l) C src with the sources at stage c of the clocked step
-  void vmult_stage(double *dst, double const *src, double c)
+  // dst = (scale .) C^T sum_l A_l C v at the stage time t + c dt, v the
+  // composite vector (a stage input formed in the prolongation)
+  void vmult_stage(double *dst, StageSum const &v, double c, double const *scale = nullptr)
   {
-    prolong(src);
+    prolong(v);
     fork();
     for (size_t l = 0; l < levels_.size(); ++l)
       if (alive(l))
         levels_[l]->vmult_stage(dst_lev_.p + lev_off_[l], src_lev_.p + lev_off_[l], c);
     join();
-    restrict_to(dst, 0);
+    restrict_to(dst, 0, scale);
+  }
+
+  void vmult_stage(double *dst, double const *src, double c)
+  {
+    StageSum v{};
+    v.y = src;
+    vmult_stage(dst, v, c);
   }
 
   void step_body(double dt, Thermal::Tableau const &tab)
@@ -1171,28 +1199,21 @@ private:
     int64_t const n = n_dofs();
     for (int i = 0; i < tab.s; ++i)
     {
-      double const *in = y_.p;
-      if (i > 0)
-      {
-        // z = y + dt sum_{j<i} a_ij k_j
-        double a[3] = {0, 0, 0};
-        double const *kk[3] = {k_[0].p, k_[0].p, k_[0].p};
-        int nk = 0;
-        for (int j = 0; j < i; ++j)
-          if (tab.a[i][j] != 0.0)
-          {
-            a[nk] = tab.a[i][j];
-            kk[nk] = k_[j].p;
-            ++nk;
-          }
-        stage_input_kernel<<<blocks(n), 256, 0, stream_>>>(n, y_.p, dt, nk, a[0], kk[0], a[1], kk[1], a[2], kk[2],
-                                                            z_.p);
-        ADM_CK(cudaGetLastError());
-        in = z_.p;
-      }
-      vmult_stage(k_[i].p, in, tab.c[i]);
-      scale_kernel<<<blocks(n), 256, 0, stream_>>>(n, inv_m_.p, k_[i].p);
-      ADM_CK(cudaGetLastError());
+      // the stage input y + dt sum_{j<i} a_ij k_j is formed by the
+      // prolongation, and k_i = M^-1 (...) by the restriction
+      StageSum v{};
+      v.y = y_.p;
+      v.dt = dt;
+      for (int j = 0; j < i; ++j)
+        if (tab.a[i][j] != 0.0)
+        {
+          if (v.nk == 3)
+            throw Error(ADM_ERR_INVALID, "internal: more than three stage terms");
+          v.a[v.nk] = tab.a[i][j];
+          v.k[v.nk] = k_[j].p;
+          ++v.nk;
+        }
+      vmult_stage(k_[i].p, v, tab.c[i], inv_m_.p);
     }
     // y += dt sum_i b_i k_i
     double a[3] = {0, 0, 0};
@@ -1398,8 +1419,8 @@ private:
         off += (int64_t)((levels_[l]->m() + 31) / 32 * 32);
       }
     lev_n_ = off;
-    src_lev_.alloc(std::max<int64_t>(1, lev_n_));
-    dst_lev_.alloc(std::max<int64_t>(1, lev_n_));
+    src_lev_.ensure(std::max<int64_t>(1, lev_n_));
+    dst_lev_.ensure(std::max<int64_t>(1, lev_n_));
     ADM_CK(cudaMemsetAsync(src_lev_.p, 0, lev_n_ * sizeof(double), stream_));
     // prolongation rows (level nodes of active leaves) and their transpose
     std::vector<int64_t> row_pos, row_ptr{0};
@@ -1506,25 +1527,33 @@ private:
 
   template <class T> void upload(DevBuf<T> &buf, std::vector<T> const &v)
   {
-    buf.alloc(std::max<size_t>(1, v.size()));
+    buf.ensure(std::max<size_t>(1, v.size()));
     if (!v.empty())
       ADM_CK(cudaMemcpyAsync(buf.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream_));
     // the host vectors die with the caller: finish the copies first
     ADM_CK(cudaStreamSynchronize(stream_));
   }
 
-  void prolong(double const *y)
+  void prolong(StageSum const &v)
   {
     if (n_rows_ == 0)
       return;
-    prolong_kernel<<<blocks(n_rows_), 256, 0, stream_>>>(n_rows_, row_pos_.p, row_ptr_.p, ent_dof_.p, ent_w_.p, y,
+    prolong_kernel<<<blocks(n_rows_), 256, 0, stream_>>>(n_rows_, row_pos_.p, row_ptr_.p, ent_dof_.p, ent_w_.p, v,
                                                           src_lev_.p);
     ADM_CK(cudaGetLastError());
   }
 
-  void restrict_to(double *dst, int add)
+  void prolong(double const *y)
   {
-    restrict_kernel<<<blocks(n_dofs()), 256, 0, stream_>>>(n_dofs(), tptr_.p, tpos_.p, tw_.p, dst_lev_.p, dst, add);
+    StageSum v{};
+    v.y = y;
+    prolong(v);
+  }
+
+  void restrict_to(double *dst, int add, double const *scale = nullptr)
+  {
+    restrict_kernel<<<blocks(n_dofs()), 256, 0, stream_>>>(n_dofs(), tptr_.p, tpos_.p, tw_.p, dst_lev_.p, dst, add,
+                                                            scale);
     ADM_CK(cudaGetLastError());
   }
 
@@ -1532,7 +1561,7 @@ private:
   // masses of the leaves (the composite vector has no constrained entries)
   void compute_inverse_mass()
   {
-    inv_m_.alloc(std::max<int64_t>(1, n_dofs()));
+    inv_m_.ensure(std::max<int64_t>(1, n_dofs()));
     fork();
     for (size_t l = 0; l < levels_.size(); ++l)
       if (alive(l))
@@ -1569,6 +1598,7 @@ private:
   std::vector<uint8_t> alive_;
   std::vector<int64_t> row_pos_h_;
   std::vector<uint8_t> node_mark_; // level-grid byte map (prolongation rows)
+  DevBuf<double> snap_rows_;       // the old field at the old rows (remesh snapshot)
   int schedule_ = Thermal::kScheduleAtomic;
   std::vector<int64_t> lev_off_, row_lev_;
   int64_t lev_n_ = 0, n_rows_ = 0;
@@ -1576,7 +1606,7 @@ private:
   DevBuf<int64_t> row_pos_, row_ptr_, tptr_, tpos_;
   DevBuf<int32_t> ent_dof_;
   DevBuf<double> ent_w_, tw_;
-  DevBuf<double> y_, inv_m_, z_, k_[4];
+  DevBuf<double> y_, inv_m_, k_[4];
 };
 
 } // namespace adm

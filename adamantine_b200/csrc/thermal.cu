@@ -615,7 +615,7 @@ void Thermal::rebuild()
   colour_off_[8] = (int)work_.size();
   build_atomic_list(topo_.tile_active);
   ++work_version_;
-  work_d_.alloc(std::max<size_t>(1, work_.size()));
+  work_d_.ensure(std::max<size_t>(1, work_.size()));
   if (!work_.empty())
     ADM_CK(cudaMemcpyAsync(work_d_.p, work_.data(), work_.size() * sizeof(TileWork), cudaMemcpyHostToDevice, stream_));
   ADM_CK(cudaMemcpyAsync(has_melted_d_.p, has_melted_.data(), C, cudaMemcpyHostToDevice, stream_));
@@ -691,14 +691,10 @@ void Thermal::setup()
   rebuild();
   // MaterialProperty::set_initial_state (on the device from the per-cell
   // state index)
-  {
-    DevBuf<uint8_t> init;
-    init.alloc(std::max<size_t>(1, C));
-    ADM_CK(cudaMemcpyAsync(init.p, init_state_.data(), C, cudaMemcpyHostToDevice, stream_));
-    init_state_kernel<<<(unsigned)((C + 255) / 256), 256, 0, stream_>>>(init.p, ns_, C, state_d_.p);
-    ADM_CK(cudaGetLastError());
-    ADM_CK(cudaStreamSynchronize(stream_)); // init is released on return
-  }
+  scratch_u8_.ensure(std::max<size_t>(1, C));
+  ADM_CK(cudaMemcpyAsync(scratch_u8_.p, init_state_.data(), C, cudaMemcpyHostToDevice, stream_));
+  init_state_kernel<<<(unsigned)((C + 255) / 256), 256, 0, stream_>>>(scratch_u8_.p, ns_, C, state_d_.p);
+  ADM_CK(cudaGetLastError());
   if (ns_ == 3)
   {
     ADM_CK(cudaMemsetAsync(powder_mode_.p, 0, C, stream_));
@@ -1258,14 +1254,13 @@ void Thermal::get_cell_state_sparse(int32_t const *cells, size_t n, double *out)
       throw Error(ADM_ERR_INVALID, "cell index out of range");
   if (n == 0)
     return;
-  DevBuf<int32_t> cd;
-  DevBuf<double> vd;
-  cd.alloc(n);
-  vd.alloc(n * ns_);
-  ADM_CK(cudaMemcpyAsync(cd.p, cells, n * sizeof(int32_t), cudaMemcpyHostToDevice, stream_));
-  gather_state_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream_>>>(cd.p, n, ns_, C, state_d_.p, vd.p);
+  scratch_i32_.ensure(n);
+  scratch_f64_.ensure(n * ns_);
+  ADM_CK(cudaMemcpyAsync(scratch_i32_.p, cells, n * sizeof(int32_t), cudaMemcpyHostToDevice, stream_));
+  gather_state_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream_>>>(scratch_i32_.p, n, ns_, C, state_d_.p,
+                                                                       scratch_f64_.p);
   ADM_CK(cudaGetLastError());
-  ADM_CK(cudaMemcpyAsync(out, vd.p, n * ns_ * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+  ADM_CK(cudaMemcpyAsync(out, scratch_f64_.p, n * ns_ * sizeof(double), cudaMemcpyDeviceToHost, stream_));
   ADM_CK(cudaStreamSynchronize(stream_));
 }
 
@@ -1276,18 +1271,17 @@ void Thermal::set_cell_state_sparse(int32_t const *cells, double const *values, 
     if (cells[k] < 0 || (size_t)cells[k] >= C)
       throw Error(ADM_ERR_INVALID, "cell index out of range");
   ADM_CK(cudaMemsetAsync(state_d_.p, 0, state_d_.n * sizeof(double), stream_));
-  DevBuf<int32_t> cd;
-  DevBuf<double> vd;
   if (n > 0)
   {
-    cd.alloc(n);
-    vd.alloc(n * ns_);
-    ADM_CK(cudaMemcpyAsync(cd.p, cells, n * sizeof(int32_t), cudaMemcpyHostToDevice, stream_));
-    ADM_CK(cudaMemcpyAsync(vd.p, values, n * ns_ * sizeof(double), cudaMemcpyHostToDevice, stream_));
-    scatter_state_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream_>>>(cd.p, vd.p, n, ns_, C, state_d_.p);
+    scratch_i32_.ensure(n);
+    scratch_f64_.ensure(n * ns_);
+    ADM_CK(cudaMemcpyAsync(scratch_i32_.p, cells, n * sizeof(int32_t), cudaMemcpyHostToDevice, stream_));
+    ADM_CK(cudaMemcpyAsync(scratch_f64_.p, values, n * ns_ * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    scatter_state_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream_>>>(scratch_i32_.p, scratch_f64_.p, n, ns_,
+                                                                          C, state_d_.p);
     ADM_CK(cudaGetLastError());
   }
-  ADM_CK(cudaStreamSynchronize(stream_)); // cd and vd are released on return
+  ADM_CK(cudaStreamSynchronize(stream_)); // the host arrays may go once this returns
 }
 
 void Thermal::get_qp_powder(double *host)
@@ -1513,7 +1507,7 @@ int64_t Thermal::activate_in_boxes(DeviceBoxes const &boxes, int64_t b0, int64_t
   colour_off_[8] = (int)work_.size();
   build_atomic_list(ta);
   ++work_version_;
-  work_d_.alloc(std::max<size_t>(1, work_.size()));
+  work_d_.ensure(std::max<size_t>(1, work_.size()));
   ADM_CK(cudaMemcpyAsync(work_d_.p, work_.data(), work_.size() * sizeof(TileWork), cudaMemcpyHostToDevice, stream_));
   ADM_CK(cudaMemcpyAsync(tile_nbr_d_.p, topo_.tile_nbr.data(), mesh_.n_tiles * sizeof(uint32_t),
                          cudaMemcpyHostToDevice, stream_));
@@ -1596,7 +1590,7 @@ void Thermal::build_atomic_list(std::vector<uint8_t> const &tile_active)
           if (tile_active[tile])
             awork_.push_back(TileWork{0, (int32_t)tile, pack_tile(tx, ty, tz)});
         }
-  awork_d_.alloc(std::max<size_t>(1, awork_.size()));
+  awork_d_.ensure(std::max<size_t>(1, awork_.size()));
   if (!awork_.empty())
     ADM_CK(cudaMemcpyAsync(awork_d_.p, awork_.data(), awork_.size() * sizeof(TileWork), cudaMemcpyHostToDevice,
                            stream_));
@@ -1641,7 +1635,7 @@ void Thermal::build_pair_list()
         w.xyz = pack_tile(tx, ty, p);
         pwork_.push_back(w);
       }
-  pwork_d_.alloc(std::max<size_t>(1, pwork_.size()));
+  pwork_d_.ensure(std::max<size_t>(1, pwork_.size()));
   if (!pwork_.empty())
     ADM_CK(cudaMemcpyAsync(pwork_d_.p, pwork_.data(), pwork_.size() * sizeof(TileWork), cudaMemcpyHostToDevice,
                            stream_));

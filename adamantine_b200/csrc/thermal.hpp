@@ -51,10 +51,11 @@ struct DevBuf
   DevBuf() = default;
   DevBuf(DevBuf const &) = delete;
   DevBuf &operator=(DevBuf const &) = delete;
-  DevBuf(DevBuf &&o) noexcept : p(o.p), n(o.n)
+  DevBuf(DevBuf &&o) noexcept : p(o.p), n(o.n), cap(o.cap)
   {
     o.p = nullptr;
     o.n = 0;
+    o.cap = 0;
   }
   DevBuf &operator=(DevBuf &&o) noexcept
   {
@@ -63,8 +64,10 @@ struct DevBuf
       release();
       p = o.p;
       n = o.n;
+      cap = o.cap;
       o.p = nullptr;
       o.n = 0;
+      o.cap = 0;
     }
     return *this;
   }
@@ -75,6 +78,7 @@ struct DevBuf
       cudaFree(p);
     p = nullptr;
     n = 0;
+    cap = 0;
   }
   void alloc(size_t count)
   {
@@ -92,7 +96,22 @@ struct DevBuf
                                      " bytes failed: " + cudaGetErrorString(e));
     }
     n = count;
+    cap = count;
   }
+  // count elements, reusing the allocation when it is large enough (buffers
+  // whose size changes with every mesh change: no allocator call, with its
+  // implicit device synchronization, once they have grown)
+  void ensure(size_t count)
+  {
+    if (p && count <= cap)
+    {
+      n = count;
+      return;
+    }
+    alloc(count + count / 4);
+    n = count;
+  }
+  size_t cap = 0;
 };
 
 // 1D tables of one quadrature rule for FE_Q(deg) on Gauss-Lobatto nodes.
@@ -365,6 +384,11 @@ private:
   DevBuf<int64_t> list_d_;
   DevBuf<unsigned long long> count_d_;
   DevBuf<uint8_t> matid_d_;
+  // set-up and state-transfer scratch (grow-only: no allocator call per
+  // mesh change once grown)
+  DevBuf<uint8_t> scratch_u8_;
+  DevBuf<int32_t> scratch_i32_;
+  DevBuf<double> scratch_f64_;
   DevBuf<MaterialDesc> mat_d_;
   DevBuf<BeamState> beam_state_d_;
   DevBuf<MemberData> member_d_;
