@@ -284,13 +284,39 @@ public:
     C_ = t.mesh_.n_cells;
     NN_ = (t.mesh_.deg + 1) * (t.mesh_.deg + 1) * (t.mesh_.deg + 1);
     n_ = t.mesh_.n_nodes;
-    gen_ = t.has_rotation_ || !t.adiabatic_only_;
-    for (int b = 0; b < t.cfg_.n_sources; ++b)
-      gen_ = gen_ || t.cfg_.sources[b].type == 2;
-    // the face points' powder history (three states with faces)
-    NFP_ = (t.ns_ == 3 && !t.adiabatic_only_) ? (size_t)t.topo_.n_slots * 6 * (t.mesh_.deg + 1) * (t.mesh_.deg + 1)
-                                               : 0;
+    gen_ = general_kernel();
+    NFP_ = face_points();
     save_phase(init_mode_, init_cell_, init_q_, init_face_);
+  }
+
+  // the kernel variant with rotation, faces and cube sources is needed
+  bool general_kernel() const
+  {
+    Thermal const &t = th_;
+    bool g = t.has_rotation_ || !t.adiabatic_only_;
+    for (int b = 0; b < t.cfg_.n_sources; ++b)
+      g = g || t.cfg_.sources[b].type == 2;
+    return g;
+  }
+
+  // values of the face points' powder history (three states with faces)
+  size_t face_points() const
+  {
+    Thermal const &t = th_;
+    int const np = t.mesh_.deg + 1;
+    return (t.ns_ == 3 && !t.adiabatic_only_) ? (size_t)t.topo_.n_slots * 6 * np * np : 0;
+  }
+
+  // The stores and the captured initial phase state are sized by the
+  // handle's cells when the adjoint was created: cells activated since then
+  // (a new face-point layout, a deposition angle) need a new adjoint.
+  void check_handle() const
+  {
+    if (!th_.setup_done_)
+      throw Error(ADM_ERR_INVALID, "the thermal handle is not set up");
+    if (face_points() != NFP_ || general_kernel() != gen_)
+      throw Error(ADM_ERR_INVALID, "the thermal handle's cells changed after the adjoint was created; create a new "
+                                   "adjoint");
   }
 
   void set_observations(int n_obs_steps, int32_t const *steps, int n_points, int64_t const *index,
@@ -576,6 +602,7 @@ public:
   {
     Thermal &t = th_;
     cudaStream_t const st = t.stream_;
+    check_handle();
     ADM_CK(cudaSetDevice(t.device_));
     bool const ns3 = t.ns_ == 3;
     size_t const qn = C_ * NN_;
@@ -659,6 +686,7 @@ private:
     for (int s : obs_steps_)
       if (s < 0 || s > n_steps)
         throw Error(ADM_ERR_INVALID, "observation step outside [0, n_steps]");
+    check_handle();
     ADM_CK(cudaSetDevice(th_.device_));
   }
 

@@ -30,8 +30,11 @@ extern "C" {
 typedef struct adm_adjoint adm_adjoint;
 
 /* Adjoint driver over a set-up handle. The handle's phase state at this
- * call (the per-Gauss-point powder history) is the initial state of every
- * objective / gradient run. */
+ * call (the powder history of the Gauss points and of the boundary faces'
+ * points) is the initial state of every objective / gradient run. Cells
+ * activated on the handle afterwards (a new face-point layout or a
+ * deposition angle) make the later calls fail with ADM_ERR_INVALID: create
+ * a new adjoint then. */
 int adm_adjoint_create(adm_thermal *h, adm_adjoint **out);
 int adm_adjoint_destroy(adm_adjoint *a);
 /* Observations (host arrays): n_obs_steps step numbers in [0, n_steps],
