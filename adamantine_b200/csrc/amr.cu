@@ -175,9 +175,11 @@ struct Forest
       for (int l = max_level; l >= 2; --l)
         for (int64_t k = 0; k < n(l, 2); ++k)
           for (int64_t j = 0; j < n(l, 1); ++j)
+          {
+            uint8_t const *lf = &leaf[l][index(l, 0, j, k)];
             for (int64_t i = 0; i < n(l, 0); ++i)
             {
-              if (!leaf[l][index(l, i, j, k)])
+              if (!lf[i])
                 continue;
               for (int o = 0; o < kFaceEdge.n; ++o)
               {
@@ -193,6 +195,7 @@ struct Forest
                 }
               }
             }
+          }
     }
   }
 
@@ -456,16 +459,19 @@ struct AmrMesh
       for (int l = 0; l <= L; ++l)
       {
         std::vector<uint8_t> const hit = cells_to_refine(l, time, next_time, n_steps);
-        ref[l].assign(forest.cells(l), 0);
-        crs[l].assign(forest.cells(l), 0);
-        for (int64_t c = 0; c < forest.cells(l); ++c)
+        int64_t const nc = forest.cells(l);
+        ref[l].resize(nc);
+        crs[l].resize(nc);
+        uint8_t const *lf = forest.leaf[l].data(), *h = hit.data();
+        uint8_t *rf = ref[l].data(), *cr = crs[l].data();
+        uint8_t const do_crs = (coarsen_after_beam && l > 0) ? 1 : 0, do_ref = l < n_refinements ? 1 : 0;
+        // leaves: coarsen the ones the beam misses (above level 0), refine
+        // the ones it meets (below the refinement count)
+        for (int64_t c = 0; c < nc; ++c)
         {
-          if (!forest.leaf[l][c])
-            continue;
-          if (coarsen_after_beam && l > 0 && !hit[c])
-            crs[l][c] = 1;
-          if (hit[c] && l < n_refinements)
-            ref[l][c] = 1;
+          uint8_t const leaf = lf[c] != 0, hitc = h[c] != 0;
+          cr[c] = leaf & (hitc ^ 1) & do_crs;
+          rf[c] = leaf & hitc & do_ref;
         }
       }
       execute(ref, crs);
