@@ -15,10 +15,13 @@ carried over when the cells change (J2Points, transfer_old_displacement).
 Small meshes only.
 
 The elastic part is pinned to the reference's operator and Eshelby tests.
-The J2 part has no pin (parity unpinned): the reference's own elastoplastic
-test (tests/test_mechanical_physics.cc:559-617) computes the stress but
-checks nothing; the restatement follows compute_stress line by line and is
-checked against the yield-surface consistency of its isotropic case.
+The J2 part has no reference pin (parity unpinned against the reference):
+its own elastoplastic test (tests/test_mechanical_physics.cc:559-617)
+computes the stress but checks nothing. The restatement follows
+compute_stress line by line; its isotropic case is checked against the
+closed form of monotone simple shear with linear isotropic hardening and
+the yield-surface consistency of the return (the kinematic update as the
+reference writes it has no closed form to check against).
 
 Vectors are component-major over the plain node grid: index c * n_nodes +
 node, node = i + nn0 (j + nn1 k).

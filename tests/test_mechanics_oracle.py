@@ -149,3 +149,35 @@ def test_old_displacement_transfer_keeps_nodes_of_the_last_old_cell():
         want = 0.0 if i >= 1 else 1.0  # x = 1 is also cell 1's (written last): 0
         for comp in range(3):
             assert out[comp * n + g] == (u[comp * n + g] if want else 0.0), (g, comp)
+
+
+@pytest.mark.parametrize("degree", [1, 2])
+def test_j2_monotone_shear_matches_the_closed_form(degree):
+    """Simple shear u_x = gamma y applied in increments, linear isotropic
+    hardening (h = 1): the stress stays pure shear and, past the elastic
+    limit kappa_0, |dev sigma| = kappa_0 + H (sqrt(2) mu gamma - kappa_0) /
+    (2 mu + H), the closed form of the radial return under proportional
+    loading (Simo and Hughes, Computational Inelasticity, sec. 3.3), for
+    any split of the path into increments."""
+    from mechanics_oracle import Elasticity, J2Points
+
+    lam, mu, H, k0 = 2.0, 3.0, 1.5, 0.1
+    e = Elasticity((1, 1, 1), (1.0, 1.0, 1.0), degree, [0], np.zeros(1, int), [lam] * 4, [mu] * 4)
+    y = coords(e)[:, 1]
+    n = e.n_nodes
+    gamma_yield = k0 / (np.sqrt(2.0) * mu)
+    for steps in (1, 3, 10):
+        j = J2Points(e, H, 1.0, k0)
+        gamma = 0.0
+        for g in np.linspace(0.0, 5.0 * gamma_yield, steps + 1)[1:]:
+            du = np.zeros(3 * n)
+            du[:n] = (g - gamma) * y
+            j.update(du)
+            gamma = g
+        expect = k0 + H * (np.sqrt(2.0) * mu * gamma - k0) / (2.0 * mu + H)
+        for q in range(len(e.jxw)):
+            s = j._tensor(j.stress[:, 0, q])
+            assert abs(np.trace(s)) <= 1e-13 * expect
+            assert abs(s[0, 1] * np.sqrt(2.0) - expect) <= 1e-12 * expect  # |dev sigma| = sqrt(2) sigma_xy
+            assert abs(j.kappa[0, q] - expect) <= 1e-12 * expect
+            assert abs(s[0, 0]) + abs(s[1, 1]) + abs(s[2, 2]) + abs(s[0, 2]) + abs(s[1, 2]) <= 1e-13 * expect
