@@ -519,9 +519,11 @@ struct AmrMesh
     for (int l = 0; l < L; ++l)
       for (int64_t k = 0; k < forest.n(l, 2); ++k)
         for (int64_t j = 0; j < forest.n(l, 1); ++j)
+        {
+          uint8_t const *lf = &forest.leaf[l][forest.index(l, 0, j, k)];
           for (int64_t i = 0; i < forest.n(l, 0); ++i)
           {
-            if (!active_leaf(l, i, j, k))
+            if (!lf[i] || !in_domain(l, i, j, k))
               continue;
             int64_t const cc[3] = {i, j, k};
             for (int o = 0; o < kFaceEdge.n; ++o)
@@ -529,8 +531,12 @@ struct AmrMesh
               int64_t nb[3];
               for (int d = 0; d < 3; ++d)
                 nb[d] = cc[d] + kFaceEdge.o[o][d];
-              if (!forest.inside(l, nb[0], nb[1], nb[2]) || !in_domain(l, nb[0], nb[1], nb[2]) ||
-                  forest.status(l, nb[0], nb[1], nb[2]) != l + 1)
+              if (!forest.inside(l, nb[0], nb[1], nb[2]) || !in_domain(l, nb[0], nb[1], nb[2]))
+                continue;
+              // the neighbour region is refined (Forest::status == l + 1)
+              // exactly when its level-l cell exists and is not a leaf
+              int64_t const nbc = forest.index(l, nb[0], nb[1], nb[2]);
+              if (!forest.exists[l][nbc] || forest.leaf[l][nbc])
                 continue;
               // the shared entity: fixed coordinate (0 or p) along the
               // offset's nonzero directions, free along the others
@@ -575,6 +581,7 @@ struct AmrMesh
                   }
             }
           }
+        }
     // masters: the keys of the non-hanging nodes, in key order (the map is
     // scanned eight entries at a time, skipping empty words)
     for (auto const &kv : hk)
