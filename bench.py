@@ -933,12 +933,14 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_adjoint:
         line["adjoint"] = run_adjoint(args, local_rank)
     if args.deposition_steps > 0:
-        line["deposition"] = run_deposition(args, local_rank, rank == 0 and not args.no_cpu_baseline)
+        # the host-core baselines run at N = 1 only (rank 0 would keep the
+        # other ranks waiting at the closing barrier)
+        line["deposition"] = run_deposition(args, local_rank, world == 1 and not args.no_cpu_baseline)
     if args.amr_steps > 0:
         line["amr"] = run_amr(args, local_rank)
     if not args.no_mechanics:
         line["mechanics"] = run_mechanics(args, local_rank)
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, med, n, ref_out = cpu_vmult_rate(build_workload(args.size)[0], T, os.cpu_count() or 1,
                                                keep_result=True)
         line["cpu_baseline"] = {"value": rate, "unit": "GDoF/s", "cores": os.cpu_count() or 1, "kind": "port",
